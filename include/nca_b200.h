@@ -1,0 +1,184 @@
+/*
+ * nca_b200.h -- C ABI of the B200 batched NCA build and H^2 product.
+ *
+ * Every entry point returns an nca_status; on failure nca_last_error() holds a message
+ * (thread-local). No C++ exception or device trap crosses this boundary. Indices are
+ * 0-based; complex numbers are interleaved (re, im) doubles (or floats where stated);
+ * matrices are column-major, as in Julia.
+ *
+ * Each declaration names the reference interface of NestedCrossApproximation.jl (paths
+ * inside that project) that it replaces on the batched bottom-up build / H^2 product path.
+ */
+#ifndef NCA_B200_H
+#define NCA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    NCA_OK = 0,
+    NCA_ERR_SINGULAR = 1, /* SingularCrossMatrixError (src/utils/utils.jl:38-54) */
+    NCA_ERR_DIM = 2,      /* DimensionMismatch */
+    NCA_ERR_ARG = 3,      /* ArgumentError */
+    NCA_ERR_CUDA = 4,     /* CUDA runtime failure */
+    NCA_ERR_TIMEOUT = 5,  /* a bounded device wait gave up */
+    NCA_ERR_OOM = 6,      /* device allocation failed */
+    NCA_ERR_BUSY = 7      /* ConcurrentWorkspaceError (src/nca/petrovgalerkinnca.jl:210-218) */
+} nca_status;
+
+/* Kernel families of the entry generator (AdaptiveCrossApproximation.AbstractKernelMatrix
+ * for point kernels: README.md:100-108, test/testutils.jl:14-21). */
+typedef enum {
+    NCA_KERNEL_HELMHOLTZ = 0, /* cis(sign * k r) / (4 pi r); 0 where r == 0 or r < rmin */
+    NCA_KERNEL_LAPLACE = 1,   /* 1 / (4 pi r) */
+    NCA_KERNEL_MATRIX = 2     /* entry (i, j) of a given matrix (AdaptiveCrossApproximation.PointMatrix) */
+} nca_kernel_kind;
+
+typedef struct {
+    int32_t kind;          /* nca_kernel_kind */
+    int32_t sign;          /* +1: exp(+ikr), -1: exp(-ikr) */
+    double k;              /* wavenumber */
+    double rmin;           /* distances below rmin give 0 */
+    const double *matrix;  /* NCA_KERNEL_MATRIX: host matrix, ldmatrix x ntrial complex */
+    int64_t ldmatrix;
+} nca_kernel_desc;
+
+/* Apply modes of LinearMaps: A, transpose(A), adjoint(A) (src/nca/petrovgalerkinnca.jl:431-589). */
+typedef enum { NCA_MODE_N = 0, NCA_MODE_T = 1, NCA_MODE_C = 2 } nca_mode;
+
+/* Arithmetic of the product: complex FP64, or complex FP32 stores with FP32 arithmetic. */
+typedef enum { NCA_PREC_F64 = 0, NCA_PREC_F32 = 1 } nca_precision;
+
+typedef struct nca_tree nca_tree;
+typedef struct nca_partition nca_partition;
+typedef struct nca_core nca_core;
+typedef struct nca_workspace nca_workspace;
+
+int32_t nca_version(void);
+/* Copies the last error message of this thread into buf (always NUL-terminated). */
+int32_t nca_last_error(char *buf, size_t len);
+/* Details of the last NCA_ERR_SINGULAR on this thread: side (0 test, 1 trial), node,
+ * number of pivots and numerical rank (SingularCrossMatrixError(kind, npivots, rank)). */
+int32_t nca_last_singular(int32_t *side, int32_t *node, int32_t *npivots, int32_t *rank);
+
+/* ---- cluster trees (H2Trees.KMeansTree(points; builder=KMeansTreeBuilder(numberofclusters=2,
+ *      minvalues)), used by test/testutils.jl:27-39; the tree is an input of the reference's
+ *      PetrovGalerkinNCA, src/nca/petrovgalerkinnca.jl:138-142) ---- */
+int32_t nca_tree_kmeans(const double *points, int64_t npoints, int32_t minvalues,
+                        int32_t nclusters, nca_tree **out);
+void nca_tree_destroy(nca_tree *tree);
+int32_t nca_tree_sizes(const nca_tree *tree, int32_t *nnodes, int32_t *nlevels, int64_t *npoints);
+int32_t nca_tree_export(const nca_tree *tree, int32_t *perm, int32_t *begin, int32_t *end,
+                        int32_t *parent, int32_t *firstchild, int32_t *nchildren, int32_t *level,
+                        double *center, double *radius);
+
+/* ---- admissibility: interactions(tree, isnear(eta)) -> near/far CSR over test nodes
+ *      (AdaptiveCrossApproximation.interactions; consumed by src/nca/abstractnca.jl:148 and
+ *      src/admissibility/farinteractions.jl:66-92) ---- */
+int32_t nca_interactions(const nca_tree *test, const nca_tree *trial, double eta,
+                         nca_partition **out);
+void nca_partition_destroy(nca_partition *part);
+int32_t nca_partition_sizes(const nca_partition *part, int64_t *nnear, int64_t *nfar);
+int32_t nca_partition_export(const nca_partition *part, int32_t *nearptr, int32_t *nearnodes,
+                             int32_t *farptr, int32_t *farnodes, int32_t *trialfarptr,
+                             int32_t *trialfarnodes);
+
+/* ---- phase 1 for one cluster: _selectfarpivots with tree-mimicry pivoting
+ *      (src/compressors/batchedbottomup.jl:54-72) ---- */
+int32_t nca_select_farpivots(const nca_tree *fartree, const double *ownpoints,
+                             const double *farpoints, const int32_t *refidcs, int32_t nref,
+                             const int32_t *farnodes, int32_t nfar, int32_t maxrank,
+                             int32_t *pivots, int32_t *npivots);
+
+/* ---- the whole batched bottom-up build on one GPU: PetrovGalerkinNCACore(...) with
+ *      BatchedBottomUp(pivotselector=TreeMimicryPivoting, compressor=ACA(FullPivoting(),
+ *      FullPivoting(), FNormEstimator(tol))) on both sides
+ *      (src/nca/petrovgalerkinnca.jl:138-198 -> src/nca/abstractnca.jl:134-216 ->
+ *      src/compressors/batchedbottomup.jl:246-447 -> src/couplingmatrices.jl:11-53) ---- */
+typedef struct {
+    double tol_test, tol_trial; /* ACA tolerances of the two compressors */
+    int32_t maxrank;            /* maximum rank per cluster (default 50) */
+    int32_t sampled;            /* 1: sampled FNorm stop (batchedbottomup.jl:120-125) */
+    int32_t device;             /* CUDA device ordinal */
+    int32_t store_f32;          /* 1: also keep complex FP32 copies of all stores */
+} nca_build_opts;
+
+int32_t nca_core_build(const double *testpoints, int64_t ntest, const double *trialpoints,
+                       int64_t ntrial, const nca_tree *testtree, const nca_tree *trialtree,
+                       const nca_partition *part, const nca_kernel_desc *kernel,
+                       const nca_build_opts *opts, nca_core **out);
+void nca_core_destroy(nca_core *core);
+
+/* Sizes: number of nodes per side and the totals of the device stores. */
+typedef struct {
+    int64_t ntest, ntrial;
+    int32_t nnodes_test, nnodes_trial;
+    int64_t ncoeff_test, ncoeff_trial;  /* coefficient vector lengths (plan_from_pivots) */
+    int64_t near_entries, coupling_entries, basis_entries_test, basis_entries_trial,
+        transfer_entries_test, transfer_entries_trial;
+    int64_t nfarpairs, nnearpairs;
+    double build_seconds;             /* device build time (events) */
+    double build_seconds_host;        /* host planning time (tree mimicry, plans) */
+} nca_core_info;
+int32_t nca_core_get_info(const nca_core *core, nca_core_info *info);
+
+/* Pivots per node of one side (the third return value of testbases/trialbases,
+ * batchedbottomup.jl:344,446): ranks[nnodes], ptr[nnodes+1], idx[ptr[nnodes]]. */
+int32_t nca_core_export_pivots(const nca_core *core, int32_t side, int32_t *ranks, int32_t *nrows,
+                               int32_t *ptr, int32_t *idx);
+/* Far pivots of phase 1 per node of one side: ptr[nnodes+1], idx. */
+int32_t nca_core_farpivots_total(const nca_core *core, int32_t side, int64_t *total);
+int32_t nca_core_export_farpivots(const nca_core *core, int32_t side, int32_t *ptr, int32_t *idx);
+/* Interpolation operator X_t = A[rows, sigma] A[tau, sigma]^{-1} of every node (nrows x rank,
+ * column-major): the leaf basis (test: X, trial: X^T) or the stacked transfer matrices
+ * (nestedbasis.jl:43-57, transfermatrices.jl:183-211). off[nnodes+1] counts complex entries. */
+int32_t nca_core_export_x(const nca_core *core, int32_t side, int64_t *off, double *X);
+/* Coupling matrices in test-node CSR order (couplingmatrices.jl:11-53). */
+int32_t nca_core_export_couplings(const nca_core *core, int64_t *off, double *C);
+/* Near-field block rows per test node (abstractnca.jl:134-178). */
+int32_t nca_core_export_near(const nca_core *core, int64_t *off, int32_t *ncols, double *N);
+
+/* ---- the H^2 product: H2Workspace + _unsafe_mul!/_mul! (petrovgalerkinnca.jl:253-271,
+ *      :415-589). A workspace owns the coefficient buffers and a CUDA stream. ---- */
+int32_t nca_workspace_create(nca_core *core, int32_t max_nrhs, nca_workspace **out);
+void nca_workspace_destroy(nca_workspace *ws);
+/* y = alpha * op(H) x + beta * y for nrhs columns. memspace 0: x and y are host pointers
+ * (copies are part of the call); 1: device pointers. x, y are complex FP64 (interleaved). */
+int32_t nca_apply(nca_workspace *ws, int32_t mode, int32_t precision, const void *x, int64_t ldx,
+                  void *y, int64_t ldy, int64_t nrhs, double alpha_re, double alpha_im,
+                  double beta_re, double beta_im, int32_t memspace);
+/* Device time of the last nca_apply of this workspace (CUDA events), in seconds. */
+int32_t nca_workspace_last_time(const nca_workspace *ws, double *seconds);
+/* Kernel launches of the last nca_apply of this workspace. */
+int32_t nca_workspace_last_launches(const nca_workspace *ws, int32_t *launches);
+
+/* ---- level seams on caller-given blocks (batchedbottomup.jl:101-244, the CUDA extension's
+ *      ext/NestedCrossApproximationCUDAExt/compresslevel.jl:31-137): fully pivoted ACA and
+ *      the interpolation solve of every block of a packed level buffer
+ *      (rows rowoffsets[i]..rowoffsets[i+1]-1, columns 0..ncols[i]-1 of a (sum m) x ldcols
+ *      column-major complex FP64 host buffer). ---- */
+int32_t nca_blocks_aca(const double *buffer, int64_t ldbuffer, int32_t ldcols,
+                       const int64_t *rowoffsets, const int32_t *ncols, int32_t nblocks,
+                       int32_t maxrank, double tol, int32_t sampled, int32_t device,
+                       int32_t *ranks, int32_t *rowpivots, int32_t *colpivots);
+/* Z_i = X_i^T with X_i = L_i P_i^{-1}, L_i = A_i[:, colpivots], P_i = L_i[rowpivots, :]
+ * (compresslevel.jl:88-137). Z is rank_i x m_i per block at zoff[i] (complex entries).
+ * Singular cross matrices give NCA_ERR_SINGULAR and nca_last_singular(node = block). */
+int32_t nca_blocks_factors(const double *buffer, int64_t ldbuffer, int32_t ldcols,
+                           const int64_t *rowoffsets, int32_t nblocks, const int32_t *ranks,
+                           const int32_t *rowpivots, const int32_t *colpivots, int32_t maxrank,
+                           int32_t device, const int64_t *zoff, double *Z);
+
+/* ---- kernel entries: A(i, j) for index pairs (AbstractKernelMatrix entry evaluation) ---- */
+int32_t nca_entries(const nca_kernel_desc *kernel, const double *testpoints, int64_t ntest,
+                    const double *trialpoints, int64_t ntrial, const int64_t *ii,
+                    const int64_t *jj, int64_t n, int32_t device, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,69 @@
+// Argument blocks and launch declarations of the build and apply kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "entry.cuh"
+
+namespace nca {
+
+// One side of the batched build (side 0: test rows against trial far pivots; side 1: trial
+// rows, entries evaluated transposed, as assemble_level(...; transposed=true)).
+struct LevelArgs {
+    KernelParams K;
+    int side;
+    const double *own_pts;  // xyz of this side's points
+    const double *far_pts;  // xyz of the other side's points
+    const int32_t *perm, *begin, *end, *firstchild, *nchildren;
+    const int32_t *fpptr, *fpidx;  // phase-1 far pivots (CSR over nodes)
+    int32_t *rank, *nrows, *piv;   // outputs: rank, block rows, pivots (maxrank per node)
+    double2 *X;                    // interpolation operators, node slot at xoff[node]
+    const int64_t *xoff;
+    int maxrank;
+    double tol;
+    int sampled;
+    int32_t *status;  // [flag, node, npivots, rank] of the first singular cross matrix
+};
+
+size_t level_smem_bytes(int mcap, int ncap);
+__global__ void k_level_compress(LevelArgs a, const int32_t *nodes, int mcap, int ncap);
+
+struct CouplingArgs {
+    KernelParams K;
+    const double *test_pts, *trial_pts;
+    const int32_t *pair_t, *pair_s;
+    const int32_t *rank_t, *rank_s, *piv_t, *piv_s;
+    int maxrank;
+    const int64_t *coff;
+    int64_t npairs;
+    double2 *C;
+    float2 *C32;
+};
+__global__ void k_couplings(CouplingArgs a);
+
+struct NearArgs {
+    KernelParams K;
+    const double *test_pts, *trial_pts;
+    const int32_t *pair_t, *pair_s, *coloff;
+    const int32_t *t_perm, *t_begin, *t_end, *s_perm, *s_begin, *s_end;
+    const int64_t *noff;
+    int64_t npairs;
+    double2 *N;
+    float2 *N32;
+};
+__global__ void k_near(NearArgs a);
+
+__global__ void k_blocks_aca(const double2 *buf, int64_t ld, const int64_t *rowoff,
+                             const int32_t *ncols, int maxrank, double tol, int sampled, int mcap,
+                             int ncap, int32_t *ranks, int32_t *rowpiv, int32_t *colpiv);
+__global__ void k_blocks_factors(const double2 *buf, int64_t ld, const int64_t *rowoff,
+                                 const int32_t *ranks, const int32_t *rowpiv,
+                                 const int32_t *colpiv, int maxrank, const int64_t *zoff,
+                                 double2 *Z, int32_t *status);
+__global__ void k_entries(KernelParams K, const double *tp, const double *sp, const int64_t *ii,
+                          const int64_t *jj, int64_t n, double2 *out);
+__global__ void k_to_f32(const double2 *in, float2 *out, int64_t n);
+
+}  // namespace nca

@@ -1,0 +1,1074 @@
+// C ABI of the library (include/nca_b200.h): trees, partition, the device-resident batched
+// build and the H^2 product. Host orchestration only; the arithmetic is in build_kernels.cu
+// and apply_kernels.cu, the index planning in host_plan.cpp.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <type_traits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "apply_kernels.cuh"
+#include "build_kernels.cuh"
+#include "nca_internal.h"
+
+namespace nca {
+
+namespace {
+thread_local std::string g_error;
+thread_local int g_singular[4] = {0, 0, 0, 0};
+
+struct Failure : std::runtime_error {
+    int code;
+    Failure(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+void check(cudaError_t e, const char *what, int line) {
+    if (e != cudaSuccess) {
+        int code = e == cudaErrorMemoryAllocation ? NCA_ERR_OOM : NCA_ERR_CUDA;
+        throw Failure(code, std::string("CUDA error in ") + what + " (capi.cu:" + std::to_string(line) +
+                                "): " + cudaGetErrorString(e));
+    }
+}
+#define CK(call) check((call), #call, __LINE__)
+
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        release();
+        n = count;
+        CK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)));
+    }
+    void upload(const T *h, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) CK(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+    }
+    void upload(const std::vector<T> &v, cudaStream_t s) { upload(v.data(), v.size(), s); }
+    void zero(cudaStream_t s) { CK(cudaMemsetAsync(p, 0, sizeof(T) * std::max<size_t>(n, 1), s)); }
+    std::vector<T> download(cudaStream_t s) const {
+        std::vector<T> h(n);
+        if (n) CK(cudaMemcpyAsync(h.data(), p, sizeof(T) * n, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return h;
+    }
+};
+
+int fail(int code, const std::string &msg) {
+    g_error = msg;
+    return code;
+}
+
+template <typename F>
+int guarded(F &&f) {
+    try {
+        return f();
+    } catch (const Failure &e) {
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(NCA_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(NCA_ERR_ARG, e.what());
+    }
+}
+
+// Node lists grouped by level: nodes[ptr[l] .. ptr[l+1]) for level order as listed.
+struct LevelLists {
+    std::vector<int32_t> ptr, nodes;
+    std::vector<int> mcap;  // per group: capacity (rows) used for shared memory
+    DBuf<int32_t> d_nodes;
+};
+
+}  // namespace
+
+void set_error(const std::string &msg) { g_error = msg; }
+void set_singular(int side, int node, int npivots, int rank) {
+    g_singular[0] = side;
+    g_singular[1] = node;
+    g_singular[2] = npivots;
+    g_singular[3] = rank;
+}
+
+}  // namespace nca
+
+using namespace nca;
+
+struct DevSide {
+    int nnodes = 0, nlevels = 0;
+    int64_t npts = 0;
+    DBuf<double> pts;
+    DBuf<int32_t> perm, begin, end, firstchild, nchildren;
+    DBuf<int32_t> fpptr, fpidx;
+    DBuf<int32_t> rank, nrows, piv;
+    DBuf<int64_t> xoff, cptr;
+    DBuf<double2> X;
+    DBuf<float2> X32;
+    std::vector<int32_t> h_fpptr, h_fpidx, h_rank, h_nrows, h_piv;
+    std::vector<int64_t> h_xoff, h_cptr;
+    LevelLists up, down;
+    DBuf<int32_t> leaves;
+    int nleaves = 0, leafcap = 0;
+};
+
+struct nca_core {
+    int device = 0;
+    int maxrank = 50;
+    bool f32 = false;
+    nca::Tree tree[2];
+    nca::Partition part;
+    KernelParams K{};
+    DBuf<double2> kmat;
+    DevSide side[2];
+    // couplings in test-node CSR order
+    DBuf<int32_t> farptr, farnodes, tfarptr, tfarnodes, tfarpair;
+    DBuf<int64_t> coff;
+    DBuf<double2> C;
+    DBuf<float2> C32;
+    std::vector<int64_t> h_coff;
+    DBuf<int32_t> couple_fwd, couple_rev;
+    int n_couple_fwd = 0, n_couple_rev = 0;
+    // near field: one row block per test node
+    DBuf<int32_t> nearptr, nearnodes, near_coloff, tnearptr, tnearnodes, tnear_coloff;
+    DBuf<int64_t> noff;
+    DBuf<double2> N;
+    DBuf<float2> N32;
+    std::vector<int64_t> h_noff;
+    std::vector<int32_t> h_ncols;
+    nca_core_info info{};
+};
+
+struct nca_workspace {
+    nca_core *core = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int max_nrhs = 0;
+    DBuf<double2> xt, xhat, yhat, xstage, ystage;
+    std::atomic<bool> busy{false};
+    double last_seconds = 0.0;
+    int last_launches = 0;
+};
+
+namespace {
+
+constexpr int kApplyTile = 24 * 1024;  // bytes per operand tile in the product kernels
+constexpr int kMaxSmem = 227 * 1024;
+
+void set_kernel_params(nca_core *c, const nca_kernel_desc *k, int64_t ntest, int64_t ntrial,
+                       cudaStream_t s) {
+    c->K.kind = k->kind;
+    c->K.sign = k->sign < 0 ? -1 : 1;
+    c->K.k = k->k;
+    c->K.rmin = k->rmin;
+    c->K.mat = nullptr;
+    c->K.ldmat = 0;
+    if (k->kind == NCA_KERNEL_MATRIX) {
+        if (!k->matrix || k->ldmatrix < ntest) throw Failure(NCA_ERR_ARG, "matrix kernel needs ldmatrix >= ntest");
+        c->kmat.upload(reinterpret_cast<const double2 *>(k->matrix), size_t(k->ldmatrix) * ntrial, s);
+        c->K.mat = c->kmat.p;
+        c->K.ldmat = k->ldmatrix;
+    } else if (k->kind != NCA_KERNEL_HELMHOLTZ && k->kind != NCA_KERNEL_LAPLACE) {
+        throw Failure(NCA_ERR_ARG, "unknown kernel kind");
+    }
+}
+
+void upload_tree(DevSide &d, const nca::Tree &T, const double *pts, cudaStream_t s) {
+    d.nnodes = T.nnodes;
+    d.nlevels = T.nlevels;
+    d.npts = T.npoints;
+    d.pts.upload(pts, size_t(3 * T.npoints), s);
+    d.perm.upload(T.perm, s);
+    d.begin.upload(T.begin, s);
+    d.end.upload(T.end, s);
+    d.firstchild.upload(T.firstchild, s);
+    d.nchildren.upload(T.nchildren, s);
+}
+
+// Rows/rank bounds per node (bottom-up), X slot offsets and per-level active node lists.
+void plan_side(DevSide &d, const nca::Tree &T, int maxrank, std::vector<int32_t> &lv_ptr,
+               std::vector<int32_t> &lv_nodes, std::vector<int> &lv_mcap, std::vector<int> &lv_ncap) {
+    std::vector<int64_t> mb(T.nnodes, 0), rb(T.nnodes, 0);
+    for (int node = T.nnodes - 1; node >= 0; --node) {
+        int nfp = d.h_fpptr[node + 1] - d.h_fpptr[node];
+        if (nfp == 0) continue;
+        int64_t m = 0;
+        if (T.isleaf(node)) {
+            m = T.size(node);
+        } else {
+            for (int c = 0; c < T.nchildren[node]; ++c) m += rb[T.firstchild[node] + c];
+        }
+        mb[node] = m;
+        rb[node] = std::min<int64_t>({int64_t(maxrank), m, int64_t(nfp)});
+    }
+    d.h_xoff.assign(T.nnodes + 1, 0);
+    for (int node = 0; node < T.nnodes; ++node) d.h_xoff[node + 1] = d.h_xoff[node] + mb[node] * rb[node];
+    lv_ptr.assign(1, 0);
+    lv_nodes.clear();
+    lv_mcap.clear();
+    lv_ncap.clear();
+    for (int lev = T.nlevels - 1; lev >= 0; --lev) {
+        int mc = 0, nc = 0;
+        for (int node = T.levelptr[lev]; node < T.levelptr[lev + 1]; ++node) {
+            int nfp = d.h_fpptr[node + 1] - d.h_fpptr[node];
+            if (nfp == 0) continue;
+            lv_nodes.push_back(node);
+            mc = std::max<int>(mc, int(mb[node]));
+            nc = std::max(nc, nfp);
+        }
+        lv_ptr.push_back(int32_t(lv_nodes.size()));
+        lv_mcap.push_back(mc);
+        lv_ncap.push_back(nc);
+    }
+}
+
+// Apply plans of one side once the ranks are known.
+void plan_apply(DevSide &d, const nca::Tree &T, cudaStream_t s) {
+    d.up.ptr.assign(1, 0);
+    d.up.nodes.clear();
+    d.up.mcap.clear();
+    for (int lev = T.nlevels - 1; lev >= 0; --lev) {
+        int mc = 0;
+        for (int node = T.levelptr[lev]; node < T.levelptr[lev + 1]; ++node)
+            if (d.h_rank[node] > 0) {
+                d.up.nodes.push_back(node);
+                mc = std::max(mc, d.h_rank[node]);
+            }
+        d.up.ptr.push_back(int32_t(d.up.nodes.size()));
+        d.up.mcap.push_back(mc);
+    }
+    d.up.d_nodes.upload(d.up.nodes, s);
+    d.down.ptr.assign(1, 0);
+    d.down.nodes.clear();
+    d.down.mcap.clear();
+    for (int lev = 0; lev < T.nlevels; ++lev) {
+        int mc = 0;
+        for (int node = T.levelptr[lev]; node < T.levelptr[lev + 1]; ++node)
+            if (d.h_rank[node] > 0 && !T.isleaf(node)) {
+                d.down.nodes.push_back(node);
+                mc = std::max(mc, d.h_nrows[node]);
+            }
+        d.down.ptr.push_back(int32_t(d.down.nodes.size()));
+        d.down.mcap.push_back(mc);
+    }
+    d.down.d_nodes.upload(d.down.nodes, s);
+    std::vector<int32_t> leaves;
+    d.leafcap = 0;
+    for (int node = 0; node < T.nnodes; ++node)
+        if (T.isleaf(node)) {
+            leaves.push_back(node);
+            d.leafcap = std::max(d.leafcap, T.size(node));
+        }
+    d.nleaves = int(leaves.size());
+    d.leaves.upload(leaves, s);
+    d.h_cptr.assign(T.nnodes + 1, 0);
+    for (int node = 0; node < T.nnodes; ++node) d.h_cptr[node + 1] = d.h_cptr[node] + d.h_rank[node];
+    d.cptr.upload(d.h_cptr, s);
+}
+
+int launch_grid(int64_t work, int per_sm) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return int(std::max<int64_t>(1, std::min<int64_t>(work, int64_t(sms) * per_sm)));
+}
+
+void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int64_t ns,
+                const nca_build_opts *o) {
+    const int maxrank = c->maxrank;
+    auto h0 = std::chrono::steady_clock::now();
+    cudaStream_t s;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } sg{s};
+    upload_tree(c->side[0], c->tree[0], tp, s);
+    upload_tree(c->side[1], c->tree[1], sp, s);
+    const nca::Partition &P = c->part;
+    // phase 1 on the host (tree mimicry); far field = own far nodes + ancestors'
+    all_farpivots(c->tree[0], c->tree[1], tp, sp, P.farptr, P.farnodes, maxrank, c->side[0].h_fpptr,
+                  c->side[0].h_fpidx);
+    all_farpivots(c->tree[1], c->tree[0], sp, tp, P.tfarptr, P.tfarnodes, maxrank, c->side[1].h_fpptr,
+                  c->side[1].h_fpidx);
+    auto h1 = std::chrono::steady_clock::now();
+    cudaEvent_t ev0, ev1;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } eg{ev0, ev1};
+    DBuf<int32_t> status;
+    status.alloc(4);
+    CK(cudaEventRecord(ev0, s));
+    for (int sd = 0; sd < 2; ++sd) {
+        DevSide &d = c->side[sd];
+        const nca::Tree &T = c->tree[sd];
+        d.fpptr.upload(d.h_fpptr, s);
+        d.fpidx.upload(d.h_fpidx, s);
+        std::vector<int32_t> lv_ptr, lv_nodes;
+        std::vector<int> lv_mcap, lv_ncap;
+        plan_side(d, T, maxrank, lv_ptr, lv_nodes, lv_mcap, lv_ncap);
+        d.xoff.upload(d.h_xoff, s);
+        d.X.alloc(size_t(d.h_xoff.back()));
+        d.rank.alloc(T.nnodes);
+        d.rank.zero(s);
+        d.nrows.alloc(T.nnodes);
+        d.nrows.zero(s);
+        d.piv.alloc(size_t(T.nnodes) * maxrank);
+        DBuf<int32_t> nodes;
+        nodes.upload(lv_nodes, s);
+        status.zero(s);
+        LevelArgs a;
+        a.K = c->K;
+        a.side = sd;
+        a.own_pts = d.pts.p;
+        a.far_pts = c->side[1 - sd].pts.p;
+        a.perm = d.perm.p;
+        a.begin = d.begin.p;
+        a.end = d.end.p;
+        a.firstchild = d.firstchild.p;
+        a.nchildren = d.nchildren.p;
+        a.fpptr = d.fpptr.p;
+        a.fpidx = d.fpidx.p;
+        a.rank = d.rank.p;
+        a.nrows = d.nrows.p;
+        a.piv = d.piv.p;
+        a.X = d.X.p;
+        a.xoff = d.xoff.p;
+        a.maxrank = maxrank;
+        a.tol = sd == 0 ? o->tol_test : o->tol_trial;
+        a.sampled = o->sampled;
+        a.status = status.p;
+        size_t maxsm = 0;
+        for (size_t l = 0; l + 1 < lv_ptr.size(); ++l)
+            maxsm = std::max(maxsm, level_smem_bytes(lv_mcap[l], lv_ncap[l]));
+        if (maxsm > size_t(kMaxSmem))
+            throw Failure(NCA_ERR_ARG, "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
+        CK(cudaFuncSetAttribute(k_level_compress, cudaFuncAttributeMaxDynamicSharedMemorySize, int(maxsm)));
+        for (size_t l = 0; l + 1 < lv_ptr.size(); ++l) {
+            int cnt = lv_ptr[l + 1] - lv_ptr[l];
+            if (cnt == 0) continue;
+            size_t sm = level_smem_bytes(lv_mcap[l], lv_ncap[l]);
+            k_level_compress<<<cnt, 256, sm, s>>>(a, nodes.p + lv_ptr[l], lv_mcap[l], lv_ncap[l]);
+            CK(cudaGetLastError());
+        }
+        std::vector<int32_t> st = status.download(s);
+        if (st[0] == 1) {
+            set_singular(sd, st[1], st[2], st[3]);
+            throw Failure(NCA_ERR_SINGULAR,
+                          "SingularCrossMatrixError: the cross matrix of " + std::string(sd == 0 ? "test" : "trial") +
+                              " node " + std::to_string(st[1]) + " is singular - " + std::to_string(st[2]) +
+                              " pivots were selected but only " + std::to_string(st[3]) +
+                              " of them are linearly independent (coincident points?)");
+        }
+        if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: level block exceeds its planned capacity");
+        d.h_rank = d.rank.download(s);
+        d.h_nrows = d.nrows.download(s);
+        d.h_piv = d.piv.download(s);
+        plan_apply(d, T, s);
+        if (c->f32) {
+            d.X32.alloc(d.X.n);
+            if (d.X.n) k_to_f32<<<launch_grid(int64_t(d.X.n) / 256 + 1, 8), 256, 0, s>>>(d.X.p, d.X32.p, int64_t(d.X.n));
+            CK(cudaGetLastError());
+        }
+    }
+    // couplings S_ts = K[tau_t, sigma_s] in test CSR order
+    const nca::Tree &Tt = c->tree[0], &Ts = c->tree[1];
+    const int64_t npairs = P.farnodes.size();
+    std::vector<int32_t> pair_t(npairs), pair_s(P.farnodes.begin(), P.farnodes.end());
+    c->h_coff.assign(npairs + 1, 0);
+    for (int t = 0; t < Tt.nnodes; ++t)
+        for (int i = P.farptr[t]; i < P.farptr[t + 1]; ++i) {
+            pair_t[i] = t;
+            c->h_coff[i + 1] = c->h_coff[i] + int64_t(c->side[0].h_rank[t]) * c->side[1].h_rank[P.farnodes[i]];
+        }
+    c->farptr.upload(P.farptr, s);
+    c->farnodes.upload(P.farnodes, s);
+    c->tfarptr.upload(P.tfarptr, s);
+    c->tfarnodes.upload(P.tfarnodes, s);
+    std::vector<int32_t> tfarpair(P.tfarnodes.size());
+    for (int sn = 0; sn < Ts.nnodes; ++sn)
+        for (int k = P.tfarptr[sn]; k < P.tfarptr[sn + 1]; ++k) {
+            int t = P.tfarnodes[k];
+            auto it = std::lower_bound(P.farnodes.begin() + P.farptr[t], P.farnodes.begin() + P.farptr[t + 1], sn);
+            tfarpair[k] = int32_t(it - P.farnodes.begin());
+        }
+    c->tfarpair.upload(tfarpair, s);
+    c->coff.upload(c->h_coff, s);
+    c->C.alloc(size_t(c->h_coff.back()));
+    if (c->f32) c->C32.alloc(c->C.n);
+    {
+        DBuf<int32_t> dpt, dps;
+        dpt.upload(pair_t, s);
+        dps.upload(pair_s, s);
+        CouplingArgs a;
+        a.K = c->K;
+        a.test_pts = c->side[0].pts.p;
+        a.trial_pts = c->side[1].pts.p;
+        a.pair_t = dpt.p;
+        a.pair_s = dps.p;
+        a.rank_t = c->side[0].rank.p;
+        a.rank_s = c->side[1].rank.p;
+        a.piv_t = c->side[0].piv.p;
+        a.piv_s = c->side[1].piv.p;
+        a.maxrank = maxrank;
+        a.coff = c->coff.p;
+        a.npairs = npairs;
+        a.C = c->C.p;
+        a.C32 = c->f32 ? c->C32.p : nullptr;
+        if (npairs > 0) {
+            k_couplings<<<launch_grid(npairs, 16), 256, 0, s>>>(a);
+            CK(cudaGetLastError());
+        }
+        CK(cudaStreamSynchronize(s));
+    }
+    std::vector<int32_t> fwd, rev;
+    for (int t = 0; t < Tt.nnodes; ++t)
+        if (c->side[0].h_rank[t] > 0) fwd.push_back(t);
+    for (int sn = 0; sn < Ts.nnodes; ++sn)
+        if (c->side[1].h_rank[sn] > 0) rev.push_back(sn);
+    c->n_couple_fwd = int(fwd.size());
+    c->n_couple_rev = int(rev.size());
+    c->couple_fwd.upload(fwd, s);
+    c->couple_rev.upload(rev, s);
+    // near field: one row block per test leaf, columns = its near trial leaves in list order
+    const int64_t nnear = P.nearnodes.size();
+    c->h_noff.assign(Tt.nnodes + 1, 0);
+    c->h_ncols.assign(Tt.nnodes, 0);
+    std::vector<int32_t> near_coloff(nnear), near_t(nnear);
+    for (int t = 0; t < Tt.nnodes; ++t) {
+        int col = 0;
+        for (int i = P.nearptr[t]; i < P.nearptr[t + 1]; ++i) {
+            near_coloff[i] = col;
+            near_t[i] = t;
+            col += Ts.size(P.nearnodes[i]);
+        }
+        c->h_ncols[t] = col;
+        c->h_noff[t + 1] = c->h_noff[t] + int64_t(Tt.size(t)) * col;
+    }
+    std::vector<int32_t> tnear_coloff(P.tnearnodes.size());
+    for (int sn = 0; sn < Ts.nnodes; ++sn)
+        for (int k = P.tnearptr[sn]; k < P.tnearptr[sn + 1]; ++k) {
+            int t = P.tnearnodes[k];
+            auto it = std::lower_bound(P.nearnodes.begin() + P.nearptr[t], P.nearnodes.begin() + P.nearptr[t + 1], sn);
+            tnear_coloff[k] = near_coloff[it - P.nearnodes.begin()];
+        }
+    c->nearptr.upload(P.nearptr, s);
+    c->nearnodes.upload(P.nearnodes, s);
+    c->near_coloff.upload(near_coloff, s);
+    c->tnearptr.upload(P.tnearptr, s);
+    c->tnearnodes.upload(P.tnearnodes, s);
+    c->tnear_coloff.upload(tnear_coloff, s);
+    c->noff.upload(c->h_noff, s);
+    c->N.alloc(size_t(c->h_noff.back()));
+    if (c->f32) c->N32.alloc(c->N.n);
+    {
+        DBuf<int32_t> dnt;
+        dnt.upload(near_t, s);
+        NearArgs a;
+        a.K = c->K;
+        a.test_pts = c->side[0].pts.p;
+        a.trial_pts = c->side[1].pts.p;
+        a.pair_t = dnt.p;
+        a.pair_s = c->nearnodes.p;
+        a.coloff = c->near_coloff.p;
+        a.t_perm = c->side[0].perm.p;
+        a.t_begin = c->side[0].begin.p;
+        a.t_end = c->side[0].end.p;
+        a.s_perm = c->side[1].perm.p;
+        a.s_begin = c->side[1].begin.p;
+        a.s_end = c->side[1].end.p;
+        a.noff = c->noff.p;
+        a.npairs = nnear;
+        a.N = c->N.p;
+        a.N32 = c->f32 ? c->N32.p : nullptr;
+        if (nnear > 0) {
+            k_near<<<launch_grid(nnear, 16), 256, 0, s>>>(a);
+            CK(cudaGetLastError());
+        }
+        CK(cudaEventRecord(ev1, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    auto h2 = std::chrono::steady_clock::now();
+    nca_core_info &I = c->info;
+    I.ntest = nt;
+    I.ntrial = ns;
+    I.nnodes_test = Tt.nnodes;
+    I.nnodes_trial = Ts.nnodes;
+    I.ncoeff_test = c->side[0].h_cptr.back();
+    I.ncoeff_trial = c->side[1].h_cptr.back();
+    I.near_entries = c->h_noff.back();
+    I.coupling_entries = c->h_coff.back();
+    for (int sd = 0; sd < 2; ++sd) {
+        int64_t basis = 0, transfer = 0;
+        const nca::Tree &T = c->tree[sd];
+        for (int node = 0; node < T.nnodes; ++node) {
+            int64_t e = int64_t(c->side[sd].h_nrows[node]) * c->side[sd].h_rank[node];
+            (T.isleaf(node) ? basis : transfer) += e;
+        }
+        (sd == 0 ? I.basis_entries_test : I.basis_entries_trial) = basis;
+        (sd == 0 ? I.transfer_entries_test : I.transfer_entries_trial) = transfer;
+    }
+    I.nfarpairs = npairs;
+    I.nnearpairs = nnear;
+    I.build_seconds = ms * 1e-3;
+    I.build_seconds_host = std::chrono::duration<double>(h1 - h0).count() +
+                           std::chrono::duration<double>(h2 - h1).count() - ms * 1e-3;
+}
+
+int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_t ldx, void *y,
+               int64_t ldy, int64_t nrhs, double2 alpha, double2 beta, int memspace) {
+    nca_core *c = ws->core;
+    if (mode < 0 || mode > 2) return fail(NCA_ERR_ARG, "mode must be 0 (N), 1 (T) or 2 (C)");
+    if (precision != NCA_PREC_F64 && precision != NCA_PREC_F32) return fail(NCA_ERR_ARG, "unknown precision");
+    if (precision == NCA_PREC_F32 && !c->f32)
+        return fail(NCA_ERR_ARG, "complex FP32 product requested but the core was built without store_f32");
+    const int in = mode == 0 ? 1 : 0, out = 1 - in;
+    const int64_t nin = c->side[in].npts, nout = c->side[out].npts;
+    if (nrhs < 0 || ldx < nin || ldy < nout) return fail(NCA_ERR_DIM, "DimensionMismatch: leading dimension smaller than the operator size");
+    if (nrhs == 0) return NCA_OK;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t s = ws->stream;
+    const int b = int(nrhs);
+    DevSide &I = c->side[in], &O = c->side[out];
+    if (b > ws->max_nrhs) {
+        ws->xt.alloc(size_t(std::max(c->side[0].npts, c->side[1].npts)) * b);
+        ws->xhat.alloc(size_t(std::max(c->side[0].h_cptr.back(), c->side[1].h_cptr.back())) * b);
+        ws->yhat.alloc(ws->xhat.n);
+        ws->max_nrhs = b;
+    }
+    const double2 *xd = reinterpret_cast<const double2 *>(x);
+    double2 *yd = reinterpret_cast<double2 *>(y);
+    int64_t lx = ldx, ly = ldy;
+    const bool usebeta = beta.x != 0.0 || beta.y != 0.0;
+    if (memspace == 0) {
+        if (ws->xstage.n < size_t(nin) * b) ws->xstage.alloc(size_t(nin) * b);
+        if (ws->ystage.n < size_t(nout) * b) ws->ystage.alloc(size_t(nout) * b);
+    }
+    int launches = 0;
+    CK(cudaEventRecord(ws->e0, s));
+    if (memspace == 0) {
+        CK(cudaMemcpy2DAsync(ws->xstage.p, sizeof(double2) * nin, xd, sizeof(double2) * ldx,
+                             sizeof(double2) * nin, b, cudaMemcpyHostToDevice, s));
+        if (usebeta)
+            CK(cudaMemcpy2DAsync(ws->ystage.p, sizeof(double2) * nout, yd, sizeof(double2) * ldy,
+                                 sizeof(double2) * nout, b, cudaMemcpyHostToDevice, s));
+        xd = ws->xstage.p;
+        yd = ws->ystage.p;
+        lx = nin;
+        ly = nout;
+    }
+    k_gather<<<launch_grid(nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, I.perm.p, nin, b, ws->xt.p);
+    ++launches;
+    CK(cudaMemsetAsync(ws->yhat.p, 0, sizeof(double2) * size_t(O.h_cptr.back()) * b, s));
+    const bool conj = mode == 2;
+    const int bc = std::min(b, 16);
+    auto run = [&](auto tag) {
+        using S = decltype(tag);
+        const S *Xi = nullptr, *Xo = nullptr, *Cm = nullptr, *Nm = nullptr;
+        if constexpr (std::is_same<S, double2>::value) {
+            Xi = I.X.p;
+            Xo = O.X.p;
+            Cm = c->C.p;
+            Nm = c->N.p;
+        } else {
+            Xi = I.X32.p;
+            Xo = O.X32.p;
+            Cm = c->C32.p;
+            Nm = c->N32.p;
+        }
+        const int tile = kApplyTile;
+        // upward sweep (leaves at any level take x, others their children's xhat)
+        SweepArgs<S> up{I.begin.p, I.firstchild.p, I.nchildren.p, I.rank.p, I.nrows.p, I.xoff.p, I.cptr.p,
+                        Xi, ws->xt.p, ws->xhat.p, b, conj && in == 0};
+        for (size_t l = 0; l + 1 < I.up.ptr.size(); ++l) {
+            int cnt = I.up.ptr[l + 1] - I.up.ptr[l];
+            if (!cnt) continue;
+            int mc = std::max(I.up.mcap[l], bc);
+            launch_up<S>(up, I.up.d_nodes.p + I.up.ptr[l], cnt, mc, tile, s);
+            ++launches;
+        }
+        // coupling
+        CoupleArgs<S> cp;
+        if (mode == 0) {
+            cp = CoupleArgs<S>{c->farptr.p, c->farnodes.p, nullptr, c->side[0].rank.p, c->side[1].rank.p,
+                               c->side[0].cptr.p, c->side[1].cptr.p, c->coff.p, Cm, ws->xhat.p, ws->yhat.p,
+                               b, false, false};
+        } else {
+            cp = CoupleArgs<S>{c->tfarptr.p, c->tfarnodes.p, c->tfarpair.p, c->side[1].rank.p, c->side[0].rank.p,
+                               c->side[1].cptr.p, c->side[0].cptr.p, c->coff.p, Cm, ws->xhat.p, ws->yhat.p,
+                               b, true, conj};
+        }
+        int ncp = mode == 0 ? c->n_couple_fwd : c->n_couple_rev;
+        if (ncp > 0) {
+            int mc = std::max(c->maxrank, bc);
+            launch_couple<S>(cp, mode == 0 ? c->couple_fwd.p : c->couple_rev.p, ncp, mc, tile, s);
+            ++launches;
+        }
+        // downward sweep
+        SweepArgs<S> dn{O.begin.p, O.firstchild.p, O.nchildren.p, O.rank.p, O.nrows.p, O.xoff.p, O.cptr.p,
+                        Xo, ws->xt.p, ws->yhat.p, b, conj && out == 1};
+        for (size_t l = 0; l + 1 < O.down.ptr.size(); ++l) {
+            int cnt = O.down.ptr[l + 1] - O.down.ptr[l];
+            if (!cnt) continue;
+            int mc = std::max(O.down.mcap[l], bc);
+            launch_down<S>(dn, O.down.d_nodes.p + O.down.ptr[l], cnt, mc, tile, s);
+            ++launches;
+        }
+        // leaves: op(X_t) yhat_t + near field, scattered into y
+        LeafArgs<S> lf;
+        lf.perm = O.perm.p;
+        lf.begin = O.begin.p;
+        lf.end = O.end.p;
+        lf.rank = O.rank.p;
+        lf.nrows = O.nrows.p;
+        lf.xoff = O.xoff.p;
+        lf.cptr = O.cptr.p;
+        lf.X = Xo;
+        lf.yhat = ws->yhat.p;
+        if (mode == 0) {
+            lf.nptr = c->nearptr.p;
+            lf.nnodes = c->nearnodes.p;
+            lf.coloff = c->near_coloff.p;
+        } else {
+            lf.nptr = c->tnearptr.p;
+            lf.nnodes = c->tnearnodes.p;
+            lf.coloff = c->tnear_coloff.p;
+        }
+        lf.o_begin = I.begin.p;
+        lf.o_end = I.end.p;
+        lf.noff = c->noff.p;
+        lf.N = Nm;
+        lf.xt = ws->xt.p;
+        lf.y = yd;
+        lf.ldy = ly;
+        lf.alpha = alpha;
+        lf.beta = usebeta ? beta : make_double2(0.0, 0.0);
+        lf.b = b;
+        lf.reverse = mode != 0;
+        lf.conj = conj && out == 1;
+        int mc = std::max(O.leafcap, bc);
+        launch_leaves<S>(lf, O.leaves.p, O.nleaves, mc, tile, s);
+        ++launches;
+    };
+    if (precision == NCA_PREC_F64)
+        run(double2{});
+    else
+        run(float2{});
+    CK(cudaGetLastError());
+    if (memspace == 0)
+        CK(cudaMemcpy2DAsync(y, sizeof(double2) * ldy, ws->ystage.p, sizeof(double2) * nout,
+                             sizeof(double2) * nout, b, cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(ws->e1, s));
+    CK(cudaEventSynchronize(ws->e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ws->e0, ws->e1));
+    ws->last_seconds = ms * 1e-3;
+    ws->last_launches = launches;
+    return NCA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t nca_version(void) { return 1; }
+
+int32_t nca_last_error(char *buf, size_t len) {
+    if (!buf || len == 0) return NCA_ERR_ARG;
+    size_t n = std::min(len - 1, g_error.size());
+    std::memcpy(buf, g_error.data(), n);
+    buf[n] = '\0';
+    return NCA_OK;
+}
+
+int32_t nca_last_singular(int32_t *side, int32_t *node, int32_t *npivots, int32_t *rank) {
+    *side = g_singular[0];
+    *node = g_singular[1];
+    *npivots = g_singular[2];
+    *rank = g_singular[3];
+    return NCA_OK;
+}
+
+int32_t nca_tree_kmeans(const double *points, int64_t npoints, int32_t minvalues, int32_t nclusters,
+                        nca_tree **out) {
+    return guarded([&] {
+        if (!out || (npoints > 0 && !points)) return fail(NCA_ERR_ARG, "null argument");
+        if (nclusters != 2) return fail(NCA_ERR_ARG, "only numberofclusters = 2 is supported");
+        if (minvalues < 1) return fail(NCA_ERR_ARG, "minvalues must be positive");
+        if (npoints >= (int64_t(1) << 31)) return fail(NCA_ERR_ARG, "too many points for 32-bit indices");
+        auto *t = new nca_tree;
+        t->t = build_kmeans_tree(points, npoints, minvalues);
+        *out = t;
+        return int(NCA_OK);
+    });
+}
+
+void nca_tree_destroy(nca_tree *tree) { delete tree; }
+
+int32_t nca_tree_sizes(const nca_tree *tree, int32_t *nnodes, int32_t *nlevels, int64_t *npoints) {
+    if (!tree) return fail(NCA_ERR_ARG, "null tree");
+    *nnodes = tree->t.nnodes;
+    *nlevels = tree->t.nlevels;
+    *npoints = tree->t.npoints;
+    return NCA_OK;
+}
+
+int32_t nca_tree_export(const nca_tree *tree, int32_t *perm, int32_t *begin, int32_t *end,
+                        int32_t *parent, int32_t *firstchild, int32_t *nchildren, int32_t *level,
+                        double *center, double *radius) {
+    if (!tree) return fail(NCA_ERR_ARG, "null tree");
+    const nca::Tree &T = tree->t;
+    std::copy(T.perm.begin(), T.perm.end(), perm);
+    std::copy(T.begin.begin(), T.begin.end(), begin);
+    std::copy(T.end.begin(), T.end.end(), end);
+    std::copy(T.parent.begin(), T.parent.end(), parent);
+    std::copy(T.firstchild.begin(), T.firstchild.end(), firstchild);
+    std::copy(T.nchildren.begin(), T.nchildren.end(), nchildren);
+    std::copy(T.level.begin(), T.level.end(), level);
+    std::copy(T.center.begin(), T.center.end(), center);
+    std::copy(T.radius.begin(), T.radius.end(), radius);
+    return NCA_OK;
+}
+
+int32_t nca_interactions(const nca_tree *test, const nca_tree *trial, double eta, nca_partition **out) {
+    return guarded([&] {
+        if (!test || !trial || !out) return fail(NCA_ERR_ARG, "null argument");
+        auto *p = new nca_partition;
+        p->p = build_partition(test->t, trial->t, eta);
+        *out = p;
+        return int(NCA_OK);
+    });
+}
+
+void nca_partition_destroy(nca_partition *part) { delete part; }
+
+int32_t nca_partition_sizes(const nca_partition *part, int64_t *nnear, int64_t *nfar) {
+    if (!part) return fail(NCA_ERR_ARG, "null partition");
+    *nnear = int64_t(part->p.nearnodes.size());
+    *nfar = int64_t(part->p.farnodes.size());
+    return NCA_OK;
+}
+
+int32_t nca_partition_export(const nca_partition *part, int32_t *nearptr, int32_t *nearnodes,
+                             int32_t *farptr, int32_t *farnodes, int32_t *trialfarptr,
+                             int32_t *trialfarnodes) {
+    if (!part) return fail(NCA_ERR_ARG, "null partition");
+    const nca::Partition &P = part->p;
+    std::copy(P.nearptr.begin(), P.nearptr.end(), nearptr);
+    std::copy(P.nearnodes.begin(), P.nearnodes.end(), nearnodes);
+    std::copy(P.farptr.begin(), P.farptr.end(), farptr);
+    std::copy(P.farnodes.begin(), P.farnodes.end(), farnodes);
+    std::copy(P.tfarptr.begin(), P.tfarptr.end(), trialfarptr);
+    std::copy(P.tfarnodes.begin(), P.tfarnodes.end(), trialfarnodes);
+    return NCA_OK;
+}
+
+int32_t nca_select_farpivots(const nca_tree *fartree, const double *ownpoints, const double *farpoints,
+                             const int32_t *refidcs, int32_t nref, const int32_t *farnodes, int32_t nfar,
+                             int32_t maxrank, int32_t *pivots, int32_t *npivots) {
+    return guarded([&] {
+        if (!fartree || !npivots) return fail(NCA_ERR_ARG, "null argument");
+        if (maxrank < 0) return fail(NCA_ERR_ARG, "maxrank must be non-negative");
+        for (int i = 0; i < nfar; ++i)
+            if (farnodes[i] < 0 || farnodes[i] >= fartree->t.nnodes) return fail(NCA_ERR_ARG, "far node out of range");
+        *npivots = select_farpivots(fartree->t, ownpoints, farpoints, refidcs, nref, farnodes, nfar, maxrank, pivots);
+        return int(NCA_OK);
+    });
+}
+
+int32_t nca_core_build(const double *testpoints, int64_t ntest, const double *trialpoints, int64_t ntrial,
+                       const nca_tree *testtree, const nca_tree *trialtree, const nca_partition *part,
+                       const nca_kernel_desc *kernel, const nca_build_opts *opts, nca_core **out) {
+    return guarded([&] {
+        if (!testtree || !trialtree || !part || !kernel || !opts || !out) return fail(NCA_ERR_ARG, "null argument");
+        if (testtree->t.npoints != ntest || trialtree->t.npoints != ntrial)
+            return fail(NCA_ERR_DIM, "DimensionMismatch: tree and point counts differ");
+        if (opts->maxrank < 1 || opts->maxrank > 128) return fail(NCA_ERR_ARG, "maxrank must be in 1..128");
+        if (!(opts->tol_test >= 0.0) || !(opts->tol_trial >= 0.0)) return fail(NCA_ERR_ARG, "tolerances must be non-negative");
+        if (int64_t(part->p.nearptr.size()) != testtree->t.nnodes + 1 ||
+            int64_t(part->p.tfarptr.size()) != trialtree->t.nnodes + 1)
+            return fail(NCA_ERR_DIM, "partition does not match the trees");
+        CK(cudaSetDevice(opts->device));
+        auto c = std::make_unique<nca_core>();
+        c->device = opts->device;
+        c->maxrank = opts->maxrank;
+        c->f32 = opts->store_f32 != 0;
+        c->tree[0] = testtree->t;
+        c->tree[1] = trialtree->t;
+        c->part = part->p;
+        set_kernel_params(c.get(), kernel, ntest, ntrial, nullptr);
+        build_core(c.get(), testpoints, ntest, trialpoints, ntrial, opts);
+        *out = c.release();
+        return int(NCA_OK);
+    });
+}
+
+void nca_core_destroy(nca_core *core) {
+    if (!core) return;
+    cudaSetDevice(core->device);
+    delete core;
+}
+
+int32_t nca_core_get_info(const nca_core *core, nca_core_info *info) {
+    if (!core || !info) return fail(NCA_ERR_ARG, "null argument");
+    *info = core->info;
+    return NCA_OK;
+}
+
+int32_t nca_core_export_pivots(const nca_core *core, int32_t side, int32_t *ranks, int32_t *nrows,
+                               int32_t *ptr, int32_t *idx) {
+    if (!core || side < 0 || side > 1) return fail(NCA_ERR_ARG, "bad argument");
+    const DevSide &d = core->side[side];
+    int nn = d.nnodes;
+    std::copy(d.h_rank.begin(), d.h_rank.end(), ranks);
+    std::copy(d.h_nrows.begin(), d.h_nrows.end(), nrows);
+    ptr[0] = 0;
+    for (int t = 0; t < nn; ++t) {
+        ptr[t + 1] = ptr[t] + d.h_rank[t];
+        std::copy(d.h_piv.begin() + int64_t(t) * core->maxrank,
+                  d.h_piv.begin() + int64_t(t) * core->maxrank + d.h_rank[t], idx + ptr[t]);
+    }
+    return NCA_OK;
+}
+
+int32_t nca_core_farpivots_total(const nca_core *core, int32_t side, int64_t *total) {
+    if (!core || side < 0 || side > 1) return fail(NCA_ERR_ARG, "bad argument");
+    *total = core->side[side].h_fpptr.back();
+    return NCA_OK;
+}
+
+int32_t nca_core_export_farpivots(const nca_core *core, int32_t side, int32_t *ptr, int32_t *idx) {
+    if (!core || side < 0 || side > 1) return fail(NCA_ERR_ARG, "bad argument");
+    const DevSide &d = core->side[side];
+    std::copy(d.h_fpptr.begin(), d.h_fpptr.end(), ptr);
+    std::copy(d.h_fpidx.begin(), d.h_fpidx.end(), idx);
+    return NCA_OK;
+}
+
+int32_t nca_core_export_x(const nca_core *core, int32_t side, int64_t *off, double *X) {
+    return guarded([&] {
+        if (!core || side < 0 || side > 1) return fail(NCA_ERR_ARG, "bad argument");
+        const DevSide &d = core->side[side];
+        CK(cudaSetDevice(core->device));
+        std::vector<double2> all(d.X.n);
+        if (d.X.n) CK(cudaMemcpy(all.data(), d.X.p, sizeof(double2) * d.X.n, cudaMemcpyDeviceToHost));
+        off[0] = 0;
+        for (int t = 0; t < d.nnodes; ++t) {
+            int64_t e = int64_t(d.h_nrows[t]) * d.h_rank[t];
+            off[t + 1] = off[t] + e;
+            std::memcpy(X + 2 * off[t], all.data() + d.h_xoff[t], sizeof(double2) * e);
+        }
+        return int(NCA_OK);
+    });
+}
+
+int32_t nca_core_export_couplings(const nca_core *core, int64_t *off, double *C) {
+    return guarded([&] {
+        if (!core) return fail(NCA_ERR_ARG, "null core");
+        CK(cudaSetDevice(core->device));
+        std::copy(core->h_coff.begin(), core->h_coff.end(), off);
+        if (core->C.n) CK(cudaMemcpy(C, core->C.p, sizeof(double2) * core->C.n, cudaMemcpyDeviceToHost));
+        return int(NCA_OK);
+    });
+}
+
+int32_t nca_core_export_near(const nca_core *core, int64_t *off, int32_t *ncols, double *N) {
+    return guarded([&] {
+        if (!core) return fail(NCA_ERR_ARG, "null core");
+        CK(cudaSetDevice(core->device));
+        std::copy(core->h_noff.begin(), core->h_noff.end(), off);
+        std::copy(core->h_ncols.begin(), core->h_ncols.end(), ncols);
+        if (core->N.n) CK(cudaMemcpy(N, core->N.p, sizeof(double2) * core->N.n, cudaMemcpyDeviceToHost));
+        return int(NCA_OK);
+    });
+}
+
+int32_t nca_workspace_create(nca_core *core, int32_t max_nrhs, nca_workspace **out) {
+    return guarded([&] {
+        if (!core || !out) return fail(NCA_ERR_ARG, "null argument");
+        CK(cudaSetDevice(core->device));
+        auto ws = std::make_unique<nca_workspace>();
+        ws->core = core;
+        CK(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&ws->e0));
+        CK(cudaEventCreate(&ws->e1));
+        int b = std::max(1, max_nrhs);
+        ws->xt.alloc(size_t(std::max(core->side[0].npts, core->side[1].npts)) * b);
+        ws->xhat.alloc(size_t(std::max(core->side[0].h_cptr.back(), core->side[1].h_cptr.back())) * b);
+        ws->yhat.alloc(ws->xhat.n);
+        ws->max_nrhs = b;
+        *out = ws.release();
+        return int(NCA_OK);
+    });
+}
+
+void nca_workspace_destroy(nca_workspace *ws) {
+    if (!ws) return;
+    cudaSetDevice(ws->core->device);
+    if (ws->stream) cudaStreamDestroy(ws->stream);
+    if (ws->e0) cudaEventDestroy(ws->e0);
+    if (ws->e1) cudaEventDestroy(ws->e1);
+    delete ws;
+}
+
+int32_t nca_apply(nca_workspace *ws, int32_t mode, int32_t precision, const void *x, int64_t ldx, void *y,
+                  int64_t ldy, int64_t nrhs, double alpha_re, double alpha_im, double beta_re, double beta_im,
+                  int32_t memspace) {
+    if (!ws) return fail(NCA_ERR_ARG, "null workspace");
+    bool expected = false;
+    if (!ws->busy.compare_exchange_strong(expected, true))
+        return fail(NCA_ERR_BUSY, "ConcurrentWorkspaceError: the workspace is in use by another matrix-vector product");
+    int st = guarded([&] {
+        return apply_impl(ws, mode, precision, x, ldx, y, ldy, nrhs, make_double2(alpha_re, alpha_im),
+                          make_double2(beta_re, beta_im), memspace);
+    });
+    ws->busy.store(false);
+    return st;
+}
+
+int32_t nca_workspace_last_time(const nca_workspace *ws, double *seconds) {
+    if (!ws || !seconds) return fail(NCA_ERR_ARG, "null argument");
+    *seconds = ws->last_seconds;
+    return NCA_OK;
+}
+
+int32_t nca_workspace_last_launches(const nca_workspace *ws, int32_t *launches) {
+    if (!ws || !launches) return fail(NCA_ERR_ARG, "null argument");
+    *launches = ws->last_launches;
+    return NCA_OK;
+}
+
+int32_t nca_blocks_aca(const double *buffer, int64_t ldbuffer, int32_t ldcols, const int64_t *rowoffsets,
+                       const int32_t *ncols, int32_t nblocks, int32_t maxrank, double tol, int32_t sampled,
+                       int32_t device, int32_t *ranks, int32_t *rowpivots, int32_t *colpivots) {
+    return guarded([&] {
+        if (nblocks < 0 || maxrank < 1 || maxrank > 128) return fail(NCA_ERR_ARG, "bad block arguments");
+        if (nblocks == 0) return int(NCA_OK);
+        CK(cudaSetDevice(device));
+        int mcap = 0, ncap = 1;
+        for (int i = 0; i < nblocks; ++i) {
+            mcap = std::max<int>(mcap, int(rowoffsets[i + 1] - rowoffsets[i]));
+            if (ncols[i] > ldcols) return fail(NCA_ERR_ARG, "ncols exceeds the buffer width");
+            ncap = std::max(ncap, ncols[i]);
+        }
+        mcap = std::max(mcap, 1);
+        size_t sm = sizeof(double2) * (size_t(mcap) * ncap + mcap + ncap) + sizeof(int32_t) * 2 * ncap + 16;
+        if (sm > size_t(kMaxSmem)) return fail(NCA_ERR_ARG, "block does not fit in shared memory");
+        cudaStream_t s = nullptr;
+        DBuf<double2> dbuf;
+        dbuf.upload(reinterpret_cast<const double2 *>(buffer), size_t(ldbuffer) * ldcols, s);
+        DBuf<int64_t> doff;
+        doff.upload(rowoffsets, size_t(nblocks) + 1, s);
+        DBuf<int32_t> dn, dr, drp, dcp;
+        dn.upload(ncols, nblocks, s);
+        dr.alloc(nblocks);
+        drp.alloc(size_t(nblocks) * maxrank);
+        dcp.alloc(size_t(nblocks) * maxrank);
+        CK(cudaFuncSetAttribute(k_blocks_aca, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        k_blocks_aca<<<nblocks, 256, sm, s>>>(dbuf.p, ldbuffer, doff.p, dn.p, maxrank, tol, sampled, mcap, ncap,
+                                              dr.p, drp.p, dcp.p);
+        CK(cudaGetLastError());
+        CK(cudaMemcpy(ranks, dr.p, sizeof(int32_t) * nblocks, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(rowpivots, drp.p, sizeof(int32_t) * nblocks * maxrank, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(colpivots, dcp.p, sizeof(int32_t) * nblocks * maxrank, cudaMemcpyDeviceToHost));
+        return int(NCA_OK);
+    });
+}
+
+int32_t nca_blocks_factors(const double *buffer, int64_t ldbuffer, int32_t ldcols, const int64_t *rowoffsets,
+                           int32_t nblocks, const int32_t *ranks, const int32_t *rowpivots,
+                           const int32_t *colpivots, int32_t maxrank, int32_t device, const int64_t *zoff,
+                           double *Z) {
+    return guarded([&] {
+        if (nblocks < 0 || maxrank < 1 || maxrank > 128) return fail(NCA_ERR_ARG, "bad block arguments");
+        if (nblocks == 0) return int(NCA_OK);
+        CK(cudaSetDevice(device));
+        int mcap = 1;
+        for (int i = 0; i < nblocks; ++i) {
+            int m = int(rowoffsets[i + 1] - rowoffsets[i]);
+            mcap = std::max(mcap, m);
+            if (ranks[i] < 0 || ranks[i] > maxrank || ranks[i] > m) return fail(NCA_ERR_ARG, "rank out of range");
+            for (int k = 0; k < ranks[i]; ++k) {
+                int rp = rowpivots[int64_t(i) * maxrank + k], cp = colpivots[int64_t(i) * maxrank + k];
+                if (rp < 0 || rp >= m || cp < 0 || cp >= ldcols) return fail(NCA_ERR_ARG, "pivot out of range");
+            }
+        }
+        size_t sm = sizeof(double2) * size_t(maxrank) * maxrank + sizeof(int32_t) * maxrank + 16;
+        if (sm > size_t(kMaxSmem)) return fail(NCA_ERR_ARG, "block does not fit in shared memory");
+        cudaStream_t s = nullptr;
+        DBuf<double2> dbuf, dz;
+        dbuf.upload(reinterpret_cast<const double2 *>(buffer), size_t(ldbuffer) * ldcols, s);
+        DBuf<int64_t> doff, dzoff;
+        doff.upload(rowoffsets, size_t(nblocks) + 1, s);
+        dzoff.upload(zoff, size_t(nblocks) + 1, s);
+        DBuf<int32_t> dr, drp, dcp, st;
+        dr.upload(ranks, nblocks, s);
+        drp.upload(rowpivots, size_t(nblocks) * maxrank, s);
+        dcp.upload(colpivots, size_t(nblocks) * maxrank, s);
+        st.alloc(4);
+        st.zero(s);
+        dz.alloc(size_t(zoff[nblocks]));
+        CK(cudaFuncSetAttribute(k_blocks_factors, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        k_blocks_factors<<<nblocks, 256, sm, s>>>(dbuf.p, ldbuffer, doff.p, dr.p, drp.p, dcp.p, maxrank,
+                                                  dzoff.p, dz.p, st.p);
+        CK(cudaGetLastError());
+        std::vector<int32_t> h = st.download(s);
+        if (h[0] == 1) {
+            set_singular(0, h[1], h[2], h[3]);
+            return fail(NCA_ERR_SINGULAR, "SingularCrossMatrixError: block " + std::to_string(h[1]) + " has " +
+                                              std::to_string(h[2]) + " pivots but rank " + std::to_string(h[3]));
+        }
+        if (dz.n) CK(cudaMemcpy(Z, dz.p, sizeof(double2) * dz.n, cudaMemcpyDeviceToHost));
+        return int(NCA_OK);
+    });
+}
+
+int32_t nca_entries(const nca_kernel_desc *kernel, const double *testpoints, int64_t ntest,
+                    const double *trialpoints, int64_t ntrial, const int64_t *ii, const int64_t *jj, int64_t n,
+                    int32_t device, double *out) {
+    return guarded([&] {
+        if (!kernel || n < 0) return fail(NCA_ERR_ARG, "bad argument");
+        if (n == 0) return int(NCA_OK);
+        for (int64_t e = 0; e < n; ++e)
+            if (ii[e] < 0 || ii[e] >= ntest || jj[e] < 0 || jj[e] >= ntrial) return fail(NCA_ERR_ARG, "index out of range");
+        CK(cudaSetDevice(device));
+        nca_core tmp;
+        set_kernel_params(&tmp, kernel, ntest, ntrial, nullptr);
+        DBuf<double> tp, sp;
+        tp.upload(testpoints, size_t(3 * ntest), nullptr);
+        sp.upload(trialpoints, size_t(3 * ntrial), nullptr);
+        DBuf<int64_t> di, dj;
+        di.upload(ii, size_t(n), nullptr);
+        dj.upload(jj, size_t(n), nullptr);
+        DBuf<double2> dout;
+        dout.alloc(size_t(n));
+        k_entries<<<launch_grid(n / 256 + 1, 8), 256>>>(tmp.K, tp.p, sp.p, di.p, dj.p, n, dout.p);
+        CK(cudaGetLastError());
+        CK(cudaMemcpy(out, dout.p, sizeof(double2) * n, cudaMemcpyDeviceToHost));
+        return int(NCA_OK);
+    });
+}
+
+}  // extern "C"

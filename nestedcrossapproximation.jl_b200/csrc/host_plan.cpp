@@ -1,0 +1,380 @@
+// Host planner of the batched build: cluster tree, admissible partition, phase-1 far pivots.
+//
+// These steps run on the host in the reference too (they decide index sets, not entries):
+//   - the k-means tree (H2Trees.KMeansTree with numberofclusters = 2; an input of
+//     PetrovGalerkinNCA, src/nca/petrovgalerkinnca.jl:138-142),
+//   - interactions(tree, isnear(eta)) with the ball admissibility
+//     2 max(r_t, r_s) > eta max(|c_t - c_s| - r_t - r_s, 0)  ->  near
+//     (the low-frequency branch of src/admissibility/nearinteractions.jl:84-95),
+//   - FarData and its test->trial transpose (src/admissibility/farinteractions.jl:16-92),
+//   - farfield: own far nodes, then each ancestor's (farinteractions.jl:38-60),
+//   - _selectfarpivots with tree mimicry (src/compressors/batchedbottomup.jl:54-72).
+//
+// Rules fixed by this project where the reference's dependencies are not available
+// (AdaptiveCrossApproximation.jl, H2Trees.jl): 2-means splits seeded by the point farthest
+// from the centroid and the point farthest from that one, Lloyd iterations with ties to the
+// first cluster, stable partition; tree mimicry picks, for each pivot, the far node whose
+// centre maximises dmin^2/|y - c_t|^2 (dmin: distance to the pivots chosen so far), descends
+// by the same score to a leaf and takes the best untaken point there; ties go to the first
+// candidate. Compiled with -ffp-contract=off: every fused multiply-add is an explicit
+// std::fma, so results are reproducible bit for bit.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <thread>
+
+#include "nca_internal.h"
+
+namespace nca {
+
+namespace {
+
+inline double dist2(const double *a, const double *b) {
+    double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+    return std::fma(dx, dx, std::fma(dy, dy, dz * dz));
+}
+
+constexpr int kLloydIterations = 50;
+
+struct Splitter {
+    const double *pts;
+    std::vector<int32_t> side, scratch;
+
+    // Reorders ids[0:cnt) into two stable groups; returns the size of the first one.
+    int split(int32_t *ids, int cnt) {
+        side.assign(cnt, -1);
+        scratch.resize(cnt);
+        double g[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < cnt; ++i) {
+            const double *p = pts + 3 * int64_t(ids[i]);
+            g[0] += p[0];
+            g[1] += p[1];
+            g[2] += p[2];
+        }
+        for (double &v : g) v /= cnt;
+        auto farthest = [&](const double *from) {
+            int arg = 0;
+            double best = -1.0;
+            for (int i = 0; i < cnt; ++i) {
+                double d = dist2(pts + 3 * int64_t(ids[i]), from);
+                if (d > best) {
+                    best = d;
+                    arg = i;
+                }
+            }
+            return std::make_pair(arg, best);
+        };
+        int a = farthest(g).first;
+        auto [b, spread] = farthest(pts + 3 * int64_t(ids[a]));
+        int first = 0;
+        if (spread > 0.0) {
+            double c[2][3];
+            std::memcpy(c[0], pts + 3 * int64_t(ids[a]), sizeof(c[0]));
+            std::memcpy(c[1], pts + 3 * int64_t(ids[b]), sizeof(c[1]));
+            for (int it = 0; it < kLloydIterations; ++it) {
+                bool changed = false;
+                for (int i = 0; i < cnt; ++i) {
+                    const double *p = pts + 3 * int64_t(ids[i]);
+                    int32_t s = dist2(p, c[1]) < dist2(p, c[0]) ? 1 : 0;
+                    if (s != side[i]) {
+                        side[i] = s;
+                        changed = true;
+                    }
+                }
+                if (!changed) break;
+                double sum[2][3] = {{0, 0, 0}, {0, 0, 0}};
+                int num[2] = {0, 0};
+                for (int i = 0; i < cnt; ++i) {
+                    const double *p = pts + 3 * int64_t(ids[i]);
+                    for (int d = 0; d < 3; ++d) sum[side[i]][d] += p[d];
+                    ++num[side[i]];
+                }
+                if (num[0] == 0 || num[1] == 0) break;
+                for (int k = 0; k < 2; ++k)
+                    for (int d = 0; d < 3; ++d) c[k][d] = sum[k][d] / num[k];
+            }
+            first = int(std::count(side.begin(), side.end(), 0));
+        }
+        if (first == 0 || first == cnt) {
+            first = (cnt + 1) / 2;
+            for (int i = 0; i < cnt; ++i) side[i] = i < first ? 0 : 1;
+        }
+        int k = 0;
+        for (int grp = 0; grp < 2; ++grp)
+            for (int i = 0; i < cnt; ++i)
+                if (side[i] == grp) scratch[k++] = ids[i];
+        std::copy(scratch.begin(), scratch.end(), ids);
+        return first;
+    }
+};
+
+}  // namespace
+
+Tree build_kmeans_tree(const double *pts, int64_t n, int minvalues) {
+    Tree T;
+    T.npoints = n;
+    T.perm.resize(n);
+    for (int64_t i = 0; i < n; ++i) T.perm[i] = int32_t(i);
+    T.begin.push_back(0);
+    T.end.push_back(int32_t(n));
+    T.parent.push_back(-1);
+    T.level.push_back(0);
+    Splitter sp{pts, {}, {}};
+    for (size_t node = 0; node < T.begin.size(); ++node) {
+        int b = T.begin[node], e = T.end[node];
+        int cnt = e - b;
+        if (cnt > minvalues && cnt >= 2) {
+            int first = sp.split(T.perm.data() + b, cnt);
+            T.firstchild.push_back(int32_t(T.begin.size()));
+            T.nchildren.push_back(2);
+            int bounds[3] = {b, b + first, e};
+            for (int c = 0; c < 2; ++c) {
+                T.begin.push_back(bounds[c]);
+                T.end.push_back(bounds[c + 1]);
+                T.parent.push_back(int32_t(node));
+                T.level.push_back(T.level[node] + 1);
+            }
+        } else {
+            T.firstchild.push_back(-1);
+            T.nchildren.push_back(0);
+        }
+    }
+    T.nnodes = int(T.begin.size());
+    T.center.resize(3 * size_t(T.nnodes));
+    T.radius.resize(T.nnodes);
+    for (int node = 0; node < T.nnodes; ++node) {
+        double s[3] = {0, 0, 0};
+        for (int i = T.begin[node]; i < T.end[node]; ++i)
+            for (int d = 0; d < 3; ++d) s[d] += pts[3 * int64_t(T.perm[i]) + d];
+        int cnt = T.size(node);
+        double *c = &T.center[3 * size_t(node)];
+        for (int d = 0; d < 3; ++d) c[d] = cnt > 0 ? s[d] / cnt : 0.0;
+        double m = 0.0;
+        for (int i = T.begin[node]; i < T.end[node]; ++i)
+            m = std::max(m, dist2(pts + 3 * int64_t(T.perm[i]), c));
+        T.radius[node] = std::sqrt(m);
+    }
+    T.nlevels = T.level.back() + 1;
+    T.levelptr.assign(T.nlevels + 1, T.nnodes);
+    for (int node = T.nnodes - 1; node >= 0; --node) T.levelptr[T.level[node]] = node;
+    T.iperm.resize(n);
+    for (int64_t i = 0; i < n; ++i) T.iperm[T.perm[i]] = int32_t(i);
+    return T;
+}
+
+namespace {
+
+bool isnear(const Tree &A, const Tree &B, int a, int b, double eta) {
+    double ra = A.radius[a], rb = B.radius[b];
+    double gap = std::sqrt(dist2(&A.center[3 * size_t(a)], &B.center[3 * size_t(b)])) - (ra + rb);
+    double sep = gap > 0.0 ? gap : 0.0;
+    return 2.0 * std::max(ra, rb) > eta * sep;
+}
+
+struct PairSink {
+    std::vector<int32_t> nt, ns, ft, fs;
+};
+
+void traverse(const Tree &T, const Tree &S, int t, int s, double eta, PairSink &out) {
+    if (!isnear(T, S, t, s, eta)) {
+        out.ft.push_back(t);
+        out.fs.push_back(s);
+        return;
+    }
+    bool lt = T.isleaf(t), ls = S.isleaf(s);
+    if (lt && ls) {
+        out.nt.push_back(t);
+        out.ns.push_back(s);
+    } else if (lt) {
+        for (int c = 0; c < S.nchildren[s]; ++c) traverse(T, S, t, S.firstchild[s] + c, eta, out);
+    } else if (ls) {
+        for (int c = 0; c < T.nchildren[t]; ++c) traverse(T, S, T.firstchild[t] + c, s, eta, out);
+    } else {
+        for (int c = 0; c < T.nchildren[t]; ++c)
+            for (int d = 0; d < S.nchildren[s]; ++d)
+                traverse(T, S, T.firstchild[t] + c, S.firstchild[s] + d, eta, out);
+    }
+}
+
+void to_csr(const std::vector<int32_t> &key, const std::vector<int32_t> &val, int nrows,
+            std::vector<int32_t> &ptr, std::vector<int32_t> &idx) {
+    ptr.assign(nrows + 1, 0);
+    for (int32_t k : key) ++ptr[k + 1];
+    for (int r = 0; r < nrows; ++r) ptr[r + 1] += ptr[r];
+    idx.resize(key.size());
+    std::vector<int32_t> cursor(ptr.begin(), ptr.end() - 1);
+    for (size_t i = 0; i < key.size(); ++i) idx[cursor[key[i]]++] = val[i];
+    for (int r = 0; r < nrows; ++r) std::sort(idx.begin() + ptr[r], idx.begin() + ptr[r + 1]);
+}
+
+}  // namespace
+
+Partition build_partition(const Tree &test, const Tree &trial, double eta) {
+    PairSink sink;
+    if (test.nnodes > 0 && trial.nnodes > 0) traverse(test, trial, 0, 0, eta, sink);
+    Partition P;
+    to_csr(sink.nt, sink.ns, test.nnodes, P.nearptr, P.nearnodes);
+    to_csr(sink.ft, sink.fs, test.nnodes, P.farptr, P.farnodes);
+    to_csr(sink.ns, sink.nt, trial.nnodes, P.tnearptr, P.tnearnodes);
+    to_csr(sink.fs, sink.ft, trial.nnodes, P.tfarptr, P.tfarnodes);
+    return P;
+}
+
+namespace {
+
+// Greedy tree-mimicry selection state for one cluster.
+class Mimicry {
+  public:
+    Mimicry(const Tree &far, const double *farpts, const double *centroid, const int32_t *roots,
+            int nroots, int capacity)
+        : F_(far), pts_(farpts), roots_(roots), nroots_(nroots) {
+        std::memcpy(c_, centroid, sizeof(c_));
+        chosen_xyz_.reserve(3 * size_t(capacity));
+        chosen_pos_.reserve(capacity);
+        root_dmin_.assign(nroots, 1.0);
+        root_taken_.assign(nroots, 0);
+    }
+
+    int32_t next() {
+        int node = -1;
+        double best = -1.0;
+        for (int i = 0; i < nroots_; ++i) {
+            int f = roots_[i];
+            if (F_.size(f) - root_taken_[i] <= 0) continue;
+            double sc = score(&F_.center[3 * size_t(f)], root_dmin_[i]);
+            if (sc > best) {
+                best = sc;
+                node = f;
+            }
+        }
+        while (!F_.isleaf(node)) {
+            int pick = -1;
+            double pbest = -1.0;
+            for (int c = 0; c < F_.nchildren[node]; ++c) {
+                int ch = F_.firstchild[node] + c;
+                if (F_.size(ch) - taken_inside(ch) <= 0) continue;
+                const double *cc = &F_.center[3 * size_t(ch)];
+                double sc = score(cc, dmin(cc));
+                if (sc > pbest) {
+                    pbest = sc;
+                    pick = ch;
+                }
+            }
+            node = pick;
+        }
+        int bestpos = -1;
+        best = -1.0;
+        for (int pos = F_.begin[node]; pos < F_.end[node]; ++pos) {
+            if (std::find(chosen_pos_.begin(), chosen_pos_.end(), pos) != chosen_pos_.end()) continue;
+            const double *y = pts_ + 3 * int64_t(F_.perm[pos]);
+            double sc = score(y, dmin(y));
+            if (sc > best) {
+                best = sc;
+                bestpos = pos;
+            }
+        }
+        int32_t id = F_.perm[bestpos];
+        const double *y = pts_ + 3 * int64_t(id);
+        bool firstpick = chosen_pos_.empty();
+        chosen_pos_.push_back(bestpos);
+        chosen_xyz_.insert(chosen_xyz_.end(), y, y + 3);
+        for (int i = 0; i < nroots_; ++i) {
+            int f = roots_[i];
+            double d = dist2(&F_.center[3 * size_t(f)], y);
+            if (firstpick || d < root_dmin_[i]) root_dmin_[i] = d;
+            if (bestpos >= F_.begin[f] && bestpos < F_.end[f]) ++root_taken_[i];
+        }
+        return id;
+    }
+
+  private:
+    double score(const double *y, double dmin2) const {
+        double d2 = dist2(y, c_);
+        if (d2 < 1e-300) d2 = 1e-300;
+        return dmin2 / d2;
+    }
+    double dmin(const double *y) const {
+        if (chosen_pos_.empty()) return 1.0;
+        double m = INFINITY;
+        for (size_t q = 0; q < chosen_pos_.size(); ++q) m = std::min(m, dist2(y, &chosen_xyz_[3 * q]));
+        return m;
+    }
+    int taken_inside(int node) const {
+        int k = 0;
+        for (int pos : chosen_pos_) k += (pos >= F_.begin[node] && pos < F_.end[node]);
+        return k;
+    }
+
+    const Tree &F_;
+    const double *pts_;
+    const int32_t *roots_;
+    int nroots_;
+    double c_[3];
+    std::vector<double> chosen_xyz_;
+    std::vector<int> chosen_pos_;
+    std::vector<double> root_dmin_;
+    std::vector<int> root_taken_;
+};
+
+}  // namespace
+
+int select_farpivots(const Tree &far, const double *ownpts, const double *farpts,
+                     const int32_t *refidcs, int nref, const int32_t *farnodes, int nfar,
+                     int maxrank, int32_t *out) {
+    int limit = std::min(maxrank, nref);
+    int n = 0;
+    for (int i = 0; i < nfar && limit - n > 0; ++i) {
+        n += std::min(limit - n, far.size(farnodes[i]));
+    }
+    if (n <= 0) return 0;
+    double s[3] = {0, 0, 0};
+    for (int i = 0; i < nref; ++i)
+        for (int d = 0; d < 3; ++d) s[d] += ownpts[3 * int64_t(refidcs[i]) + d];
+    double c[3];
+    for (int d = 0; d < 3; ++d) c[d] = s[d] / nref;
+    Mimicry M(far, farpts, c, farnodes, nfar, n);
+    for (int p = 0; p < n; ++p) out[p] = M.next();
+    return n;
+}
+
+int host_threads() {
+    unsigned hc = std::thread::hardware_concurrency();
+    return hc == 0 ? 1 : int(std::min(hc, 64u));
+}
+
+void all_farpivots(const Tree &own, const Tree &far, const double *ownpts, const double *farpts,
+                   const std::vector<int32_t> &ptr, const std::vector<int32_t> &nodes,
+                   int maxrank, std::vector<int32_t> &fpptr, std::vector<int32_t> &fpidx) {
+    int nn = own.nnodes;
+    std::vector<int32_t> count(nn, 0);
+    std::vector<int32_t> buf(size_t(nn) * std::max(maxrank, 1));
+    std::atomic<int> cursor{0};
+    auto work = [&]() {
+        std::vector<int32_t> ff;
+        for (;;) {
+            int t = cursor.fetch_add(1);
+            if (t >= nn) break;
+            ff.clear();
+            for (int a = t; a >= 0; a = own.parent[a])
+                ff.insert(ff.end(), nodes.begin() + ptr[a], nodes.begin() + ptr[a + 1]);
+            if (ff.empty()) continue;
+            count[t] = select_farpivots(far, ownpts, farpts, own.perm.data() + own.begin[t],
+                                        own.size(t), ff.data(), int(ff.size()), maxrank,
+                                        buf.data() + size_t(t) * maxrank);
+        }
+    };
+    int nth = std::max(1, std::min(host_threads(), nn));
+    std::vector<std::thread> pool;
+    for (int i = 1; i < nth; ++i) pool.emplace_back(work);
+    work();
+    for (auto &th : pool) th.join();
+    fpptr.assign(nn + 1, 0);
+    for (int t = 0; t < nn; ++t) fpptr[t + 1] = fpptr[t] + count[t];
+    fpidx.resize(fpptr[nn]);
+    for (int t = 0; t < nn; ++t)
+        std::copy(buf.begin() + size_t(t) * maxrank, buf.begin() + size_t(t) * maxrank + count[t],
+                  fpidx.begin() + fpptr[t]);
+}
+
+}  // namespace nca

@@ -1,0 +1,59 @@
+// Internal declarations shared by the host planner (host_plan.cpp) and the CUDA sources.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "nca_b200.h"
+
+namespace nca {
+
+// Thread-local error state behind nca_last_error / nca_last_singular.
+void set_error(const std::string &msg);
+void set_singular(int side, int node, int npivots, int rank);
+
+// k-means cluster tree, node ids in breadth-first order (root 0, siblings consecutive,
+// every level a contiguous id range).
+struct Tree {
+    int64_t npoints = 0;
+    int nnodes = 0, nlevels = 0;
+    std::vector<int32_t> perm, iperm;
+    std::vector<int32_t> begin, end, parent, firstchild, nchildren, level;
+    std::vector<double> center, radius;
+    std::vector<int32_t> levelptr;
+    bool isleaf(int n) const { return nchildren[n] == 0; }
+    int size(int n) const { return end[n] - begin[n]; }
+};
+
+Tree build_kmeans_tree(const double *pts, int64_t n, int minvalues);
+
+// Near/far interaction lists over test nodes, plus the trial-side transposes.
+struct Partition {
+    std::vector<int32_t> nearptr, nearnodes, farptr, farnodes;
+    std::vector<int32_t> tnearptr, tnearnodes, tfarptr, tfarnodes;
+};
+
+Partition build_partition(const Tree &test, const Tree &trial, double eta);
+
+// Phase 1 of the batched compressor for one cluster (tree mimicry on the far tree).
+int select_farpivots(const Tree &far, const double *ownpts, const double *farpts,
+                     const int32_t *refidcs, int nref, const int32_t *farnodes, int nfar,
+                     int maxrank, int32_t *out);
+
+// Phase 1 for every node of one side, in parallel over nodes: CSR of far pivots.
+void all_farpivots(const Tree &own, const Tree &far, const double *ownpts, const double *farpts,
+                   const std::vector<int32_t> &ptr, const std::vector<int32_t> &nodes,
+                   int maxrank, std::vector<int32_t> &fpptr, std::vector<int32_t> &fpidx);
+
+// Worker count of the host planner.
+int host_threads();
+
+}  // namespace nca
+
+struct nca_tree {
+    nca::Tree t;
+};
+struct nca_partition {
+    nca::Partition p;
+};

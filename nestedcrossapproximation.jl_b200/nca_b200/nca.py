@@ -1,0 +1,458 @@
+"""PetrovGalerkinNCA: the H^2 matrix as a linear map (src/nca/petrovgalerkinnca.jl).
+
+`PetrovGalerkinNCACore` runs the whole batched bottom-up build on the GPU
+(`nca_core_build`); `H2Workspace` owns the device coefficient buffers and a CUDA stream and
+is the linear map: `A @ x`, `mul(y, A, x, alpha, beta)`, `transpose(A)`, `adjoint(A)`,
+vectors or blocks of right-hand sides, host (numpy) or device (torch.cuda) arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+
+import numpy as np
+
+from ._lib import (ArgumentError, BuildOpts, ConcurrentWorkspaceError, CoreInfo, DimensionMismatch, check, lib,
+                   ptr)
+from .admissibility import IsNear, Partition, isnear as _isnear
+from .compressors import ACA, BatchedBottomUp
+from .trees import BlockTree
+from .utils import CoefficientPlan
+
+PREC_F64, PREC_F32 = 0, 1
+MODE_N, MODE_T, MODE_C = 0, 1, 2
+
+
+class BasisStore:
+    """Leaf bases of one side: blocks[i] belongs to plan_nodes[i] ((points, rank) on the test
+    side, (rank, points) on the trial side)."""
+
+    def __init__(self, nodes, blocks):
+        self.nodes, self.blocks = nodes, blocks
+
+
+class TransferStore:
+    """Transfer matrices level by level: (parent, child, block) with blocks (child rank, parent
+    rank) on the test side and (parent rank, child rank) on the trial side."""
+
+    def __init__(self, levelidcs, leveltoidcsptr, idxtochdsptr, chdsidcs, blocks):
+        self.levelidcs, self.leveltoidcsptr = levelidcs, leveltoidcsptr
+        self.idxtochdsptr, self.chdsidcs, self.blocks = idxtochdsptr, chdsidcs, blocks
+
+
+class CouplingStore:
+    def __init__(self, nodetofarnodesptr, farnodes, blocks):
+        self.nodetofarnodesptr, self.farnodes, self.blocks = nodetofarnodesptr, farnodes, blocks
+
+
+class PetrovGalerkinNCACore:
+    """Read-only H^2 matrix built by the batched bottom-up NCA on one GPU."""
+
+    def __init__(self, operator, testspace, trialspace, tree: BlockTree, *, testcompressor: BatchedBottomUp,
+                 trialcompressor: BatchedBottomUp, isnear: IsNear | None = None, maxrank: int = 50,
+                 ntasks: int | None = None, store_f32: bool = False, device: int = 0, sampled: bool = True,
+                 partition: Partition | None = None, verbose: bool = False):
+        if ntasks is not None and ntasks < 1:
+            raise ArgumentError(f"ntasks must be positive, got {ntasks}")
+        for comp in (testcompressor, trialcompressor):
+            if not isinstance(comp, BatchedBottomUp) or not isinstance(comp.compressor, ACA):
+                raise ArgumentError("compressors must be BatchedBottomUp(pivotselector=TreeMimicryPivoting, "
+                                    "compressor=ACA(FullPivoting(), FullPivoting(), FNormEstimator(tol)))")
+        self.operator = operator
+        self.testpoints = np.ascontiguousarray(testspace, dtype=np.float64).reshape(-1, 3)
+        self.trialpoints = np.ascontiguousarray(trialspace, dtype=np.float64).reshape(-1, 3)
+        self.tree = tree
+        self.isnear = isnear or _isnear()
+        self.partition = partition or Partition(tree, self.isnear)
+        self.maxrank = int(maxrank)
+        self.device = int(device)
+        self.f32 = bool(store_f32)
+        opts = BuildOpts()
+        opts.tol_test, opts.tol_trial = testcompressor.compressor.tol, trialcompressor.compressor.tol
+        opts.maxrank, opts.sampled, opts.device, opts.store_f32 = self.maxrank, int(sampled), self.device, int(self.f32)
+        desc = operator.desc()
+        h = C.c_void_p()
+        check(lib().nca_core_build(ptr(self.testpoints), len(self.testpoints), ptr(self.trialpoints),
+                                   len(self.trialpoints), tree.test._h, tree.trial._h, self.partition._h,
+                                   C.byref(desc), C.byref(opts), C.byref(h)))
+        self._h = h
+        info = CoreInfo()
+        check(lib().nca_core_get_info(h, C.byref(info)))
+        self.info = info
+        self.dim = (len(self.testpoints), len(self.trialpoints))
+        self._cache = {}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().nca_core_destroy(h)
+            self._h = None
+
+    @property
+    def shape(self):
+        return self.dim
+
+    # ---- exports (host copies of the device stores) ----
+    def pivots(self, side: int):
+        """Pivots per node (None for nodes without far field), ranks and block rows."""
+        key = ("piv", side)
+        if key not in self._cache:
+            tr = self.tree.test if side == 0 else self.tree.trial
+            n = tr.nnodes
+            ranks, nrows, p = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n + 1, np.int32)
+            idx = np.zeros(max(self.maxrank * n, 1), np.int32)
+            check(lib().nca_core_export_pivots(self._h, side, ptr(ranks), ptr(nrows), ptr(p), ptr(idx)))
+            fp = self.farpivots(side)
+            piv = [idx[p[i]:p[i + 1]].copy() if len(fp[i]) else None for i in range(n)]
+            self._cache[key] = (piv, ranks, nrows)
+        return self._cache[key]
+
+    def farpivots(self, side: int):
+        key = ("fp", side)
+        if key not in self._cache:
+            tr = self.tree.test if side == 0 else self.tree.trial
+            tot = C.c_int64()
+            check(lib().nca_core_farpivots_total(self._h, side, C.byref(tot)))
+            p = np.zeros(tr.nnodes + 1, np.int32)
+            idx = np.zeros(max(tot.value, 1), np.int32)
+            check(lib().nca_core_export_farpivots(self._h, side, ptr(p), ptr(idx)))
+            self._cache[key] = [idx[p[i]:p[i + 1]].copy() for i in range(tr.nnodes)]
+        return self._cache[key]
+
+    def interpolation(self, side: int):
+        """X_t = A[rows, sigma] A[tau, sigma]^{-1} per node (nrows x rank)."""
+        key = ("X", side)
+        if key not in self._cache:
+            piv, ranks, nrows = self.pivots(side)
+            n = len(ranks)
+            off = np.zeros(n + 1, np.int64)
+            X = np.zeros(max(int(np.dot(ranks.astype(np.int64), nrows)), 1), np.complex128)
+            check(lib().nca_core_export_x(self._h, side, ptr(off), ptr(X)))
+            self._cache[key] = [X[off[i]:off[i + 1]].reshape((nrows[i], ranks[i]), order="F") for i in range(n)]
+        return self._cache[key]
+
+    def _bases(self, side):
+        tr = self.tree.test if side == 0 else self.tree.trial
+        piv, _, _ = self.pivots(side)
+        Xs = self.interpolation(side)
+        nodes = [t for t in range(tr.nnodes) if tr.isleaf(t) and piv[t] is not None]
+        blocks = [Xs[t] if side == 0 else Xs[t].T for t in nodes]
+        return BasisStore(nodes, blocks)
+
+    def _transfers(self, side):
+        tr = self.tree.test if side == 0 else self.tree.trial
+        piv, ranks, _ = self.pivots(side)
+        Xs = self.interpolation(side)
+        levelidcs, lptr, cptr, chds, blocks = [], [0], [0], [], []
+        for lev in tr.levels():
+            for t in tr.levelnodes(lev):
+                if tr.isleaf(t) or piv[t] is None:
+                    continue
+                levelidcs.append(t)
+                row = 0
+                for ch in tr.children(t):
+                    k = int(ranks[ch])
+                    E = Xs[t][row:row + k, :]
+                    blocks.append(E if side == 0 else E.T)
+                    chds.append(ch)
+                    row += k
+                cptr.append(len(chds))
+            lptr.append(len(levelidcs))
+        return TransferStore(levelidcs, lptr, cptr, chds, blocks)
+
+    @property
+    def nestedtestbases(self):
+        return self._bases(0)
+
+    @property
+    def nestedtrialbases(self):
+        return self._bases(1)
+
+    @property
+    def testtransfermatrices(self):
+        return self._transfers(0)
+
+    @property
+    def trialtransfermatrices(self):
+        return self._transfers(1)
+
+    @property
+    def couplingmatrices(self):
+        if "C" not in self._cache:
+            part = self.partition
+            off = np.zeros(len(part.farnodes) + 1, np.int64)
+            Cf = np.zeros(max(self.info.coupling_entries, 1), np.complex128)
+            check(lib().nca_core_export_couplings(self._h, ptr(off), ptr(Cf)))
+            _, rt, _ = self.pivots(0)
+            _, rs, _ = self.pivots(1)
+            blocks = []
+            for t in range(self.tree.test.nnodes):
+                for i in range(part.farptr[t], part.farptr[t + 1]):
+                    s = part.farnodes[i]
+                    blocks.append(Cf[off[i]:off[i + 1]].reshape((rt[t], rs[s]), order="F"))
+            self._cache["C"] = CouplingStore(part.farptr, part.farnodes, blocks)
+        return self._cache["C"]
+
+    @property
+    def nearblocks(self):
+        """Near-field block rows: list of (rows, cols, block) per test node with near blocks."""
+        if "N" not in self._cache:
+            part, tt, st = self.partition, self.tree.test, self.tree.trial
+            n = tt.nnodes
+            off = np.zeros(n + 1, np.int64)
+            ncols = np.zeros(n, np.int32)
+            Nf = np.zeros(max(self.info.near_entries, 1), np.complex128)
+            check(lib().nca_core_export_near(self._h, ptr(off), ptr(ncols), ptr(Nf)))
+            out = []
+            for t in range(n):
+                if part.nearptr[t + 1] == part.nearptr[t]:
+                    continue
+                rows = tt.values(t)
+                cols = np.concatenate([st.values(s) for s in part.nearnodes[part.nearptr[t]:part.nearptr[t + 1]]])
+                out.append((rows, cols, Nf[off[t]:off[t + 1]].reshape((len(rows), ncols[t]), order="F")))
+            self._cache["N"] = out
+        return self._cache["N"]
+
+    @property
+    def aggregationplan(self):
+        return CoefficientPlan(np.concatenate([[0], np.cumsum(self.pivots(1)[1])]))
+
+    @property
+    def disaggregationplan(self):
+        return CoefficientPlan(np.concatenate([[0], np.cumsum(self.pivots(0)[1])]))
+
+
+class LinearMap:
+    """Minimal LinearMaps algebra: sums, scalar multiples and products of maps."""
+
+    shape = (0, 0)
+
+    def _apply(self, x, mode):
+        raise NotImplementedError
+
+    def __matmul__(self, x):
+        if isinstance(x, LinearMap):
+            return _Composed(self, x)
+        return self._apply(x, MODE_N)
+
+    __mul__ = __matmul__
+
+    def __rmul__(self, a):
+        return _Scaled(self, a)
+
+    def __add__(self, other):
+        return _Sum(self, other)
+
+    def __sub__(self, other):
+        return _Sum(self, _Scaled(other, -1.0))
+
+    @property
+    def T(self):
+        return _Transposed(self, MODE_T)
+
+    @property
+    def H(self):
+        return _Transposed(self, MODE_C)
+
+
+class _Scaled(LinearMap):
+    def __init__(self, A, a):
+        self.A, self.a, self.shape = A, a, A.shape
+
+    def _apply(self, x, mode):
+        a = np.conj(self.a) if mode == MODE_C else self.a
+        return a * self.A._apply(x, mode)
+
+
+class _Sum(LinearMap):
+    def __init__(self, A, B):
+        self.A, self.B, self.shape = A, B, A.shape
+
+    def _apply(self, x, mode):
+        return self.A._apply(x, mode) + self.B._apply(x, mode)
+
+
+class _Composed(LinearMap):
+    def __init__(self, A, B):
+        self.A, self.B, self.shape = A, B, (A.shape[0], B.shape[1])
+
+    def _apply(self, x, mode):
+        if mode == MODE_N:
+            return self.A._apply(self.B._apply(x, MODE_N), MODE_N)
+        return self.B._apply(self.A._apply(x, mode), mode)
+
+
+class _Transposed(LinearMap):
+    def __init__(self, A, mode):
+        self.A, self.mode = A, mode
+        self.shape = (A.shape[1], A.shape[0])
+
+    def _apply(self, x, mode):
+        if mode != MODE_N:
+            raise ArgumentError("nested transposes are not supported")
+        return self.A._apply(x, self.mode)
+
+    @property
+    def lmap(self):
+        return self.A
+
+
+class H2Workspace(LinearMap):
+    """H^2 matrix as a linear map: a shared read-only core plus this workspace's device
+    buffers and stream. One product at a time per workspace (ConcurrentWorkspaceError)."""
+
+    def __init__(self, core: PetrovGalerkinNCACore, dtype=np.complex128, *, max_nrhs: int = 16,
+                 parts: str = "all"):
+        self.core = core
+        self.dtype = np.dtype(dtype)
+        if self.dtype not in (np.dtype(np.complex128), np.dtype(np.complex64)):
+            raise ArgumentError("H2Workspace element type must be complex128 or complex64")
+        self.precision = PREC_F32 if self.dtype == np.complex64 else PREC_F64
+        if self.precision == PREC_F32 and not core.f32:
+            raise ArgumentError("a complex64 workspace needs a core built with store_f32=True")
+        self.parts = parts
+        h = C.c_void_p()
+        check(lib().nca_workspace_create(core._h, int(max_nrhs), C.byref(h)))
+        self._h = h
+        self._lock = threading.Lock()
+        self.shape = core.dim
+        self.last_seconds = 0.0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().nca_workspace_destroy(h)
+            self._h = None
+
+    @property
+    def busy(self):
+        return self._lock.locked()
+
+    def __getattr__(self, name):
+        core = self.__dict__.get("core")
+        if core is None:
+            raise AttributeError(name)
+        return getattr(core, name)
+
+    def _apply(self, x, mode):
+        return mul(None, self if mode == MODE_N else _Transposed(self, mode), x)
+
+
+def withworkspace(f, ws: H2Workspace):
+    """Run f as the only product on ws; fails instead of waiting (petrovgalerkinnca.jl:293-300)."""
+    if not ws._lock.acquire(blocking=False):
+        raise ConcurrentWorkspaceError()
+    try:
+        return f()
+    finally:
+        ws._lock.release()
+
+
+def _unwrap(A):
+    if isinstance(A, H2Workspace):
+        return A, MODE_N
+    if isinstance(A, _Transposed) and isinstance(A.A, H2Workspace):
+        return A.A, A.mode
+    raise ArgumentError("mul needs an H2Workspace, its transpose or its adjoint")
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+def mul(y, A, x, alpha=1.0, beta=0.0):
+    """y = alpha op(A) x + beta y (LinearMaps' 5-argument mul!). y None allocates it."""
+    ws, mode = _unwrap(A)
+    core = ws.core
+    nin = core.dim[1] if mode == MODE_N else core.dim[0]
+    nout = core.dim[0] if mode == MODE_N else core.dim[1]
+    if _is_torch(x) and x.is_cuda:
+        import torch
+        vec = x.dim() == 1
+        Xr = x.reshape(x.shape[0], -1).to(torch.complex128).t().contiguous()  # (nrhs, nin): column-major block
+        if Xr.shape[1] != nin:
+            raise DimensionMismatch(f"x has {Xr.shape[1]} rows, the operator {nin} columns")
+        nrhs = Xr.shape[0]
+        if y is None:
+            Yr = torch.zeros((nrhs, nout), dtype=torch.complex128, device=x.device)
+            beta = 0.0
+        else:
+            Yr = y.reshape(nout, -1).t().contiguous()
+        if not ws._lock.acquire(blocking=False):
+            raise ConcurrentWorkspaceError()
+        try:
+            al, be = complex(alpha), complex(beta)
+            check(lib().nca_apply(ws._h, mode, ws.precision, C.c_void_p(Xr.data_ptr()), nin,
+                                  C.c_void_p(Yr.data_ptr()), nout, nrhs, al.real, al.imag, be.real, be.imag, 1))
+        finally:
+            ws._lock.release()
+        out = Yr.t()
+        if y is not None:
+            y.copy_(out.reshape(y.shape))
+            return y
+        return out.reshape(-1) if vec else out
+    if _is_torch(x):
+        x = x.numpy()
+    x = np.asarray(x)
+    vec = x.ndim == 1
+    X = np.asfortranarray(x.reshape(x.shape[0], -1), dtype=np.complex128)
+    if X.shape[0] != nin:
+        raise DimensionMismatch(f"x has {X.shape[0]} rows, the operator {nin} columns")
+    nrhs = X.shape[1]
+    if y is None:
+        Y = np.zeros((nout, nrhs), dtype=np.complex128, order="F")
+        beta = 0.0
+        target = None
+    else:
+        if y.shape[0] != nout:
+            raise DimensionMismatch(f"y has {y.shape[0]} rows, the operator {nout} rows")
+        Y = np.asfortranarray(y.reshape(nout, -1), dtype=np.complex128)
+        target = y
+    if not ws._lock.acquire(blocking=False):
+        raise ConcurrentWorkspaceError()
+    try:
+        al, be = complex(alpha), complex(beta)
+        check(lib().nca_apply(ws._h, mode, ws.precision, ptr(X), nin, ptr(Y), nout, nrhs, al.real, al.imag,
+                              be.real, be.imag, 0))
+        t = C.c_double()
+        lib().nca_workspace_last_time(ws._h, C.byref(t))
+        ws.last_seconds = t.value
+    finally:
+        ws._lock.release()
+    out = Y[:, 0] if vec else Y
+    if target is not None:
+        target[...] = out.reshape(target.shape).astype(target.dtype, copy=False)
+        return target
+    return out.astype(ws.dtype, copy=False) if ws.dtype != np.complex128 else out
+
+
+def PetrovGalerkinNCA(operator, testspace, trialspace, tree, **kwargs) -> H2Workspace:
+    """Build the core and one workspace over it (petrovgalerkinnca.jl:327-331)."""
+    dtype = kwargs.pop("dtype", np.complex128)
+    return H2Workspace(PetrovGalerkinNCACore(operator, testspace, trialspace, tree, **kwargs), dtype)
+
+
+def core(A):
+    ws, _ = _unwrap(A)
+    return ws.core
+
+
+def transpose(A):
+    return A.T
+
+
+def adjoint(A):
+    return A.H
+
+
+def storage(h2mat, verbose: bool = True) -> float:
+    """Stored entries of near field, couplings, transfers and bases in GB (petrovgalerkinnca.jl:386-411)."""
+    c = h2mat.core if isinstance(h2mat, H2Workspace) else h2mat
+    i = c.info
+    n = (i.near_entries + i.coupling_entries + i.transfer_entries_test + i.transfer_entries_trial +
+         i.basis_entries_test + i.basis_entries_trial)
+    gb = n * 16 * 1e-9
+    if verbose:
+        print("storage:", gb, "GB")
+        print("compression ratio:", n / (c.dim[0] * c.dim[1]))
+    return gb

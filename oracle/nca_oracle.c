@@ -1,0 +1,1477 @@
+/*
+ * nca_oracle.c -- CPU restatement of NestedCrossApproximation.jl's batched bottom-up
+ * NCA build and its H^2 matrix-vector product.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is the checker for the sm_100a library: only the
+ * tests, the smoke check and the CPU-baseline leg of the benchmark load it. The library
+ * never links, calls or falls back to it.
+ *
+ * Reference files restated here (paths inside the reference project):
+ *   src/compressors/batchedbottomup.jl      phase 1/2/3 level loop           (:54-72, :101-116, :145-244, :246-447)
+ *   src/pivoting/pivots.jl                  capped cluster size               (:15-25)
+ *   src/nestedbasis.jl                      leaf bases                        (:43-57)
+ *   src/transfermatrices.jl                 transfer matrices, level order    (:58-95, :183-211)
+ *   src/utils/utils.jl                      ptrfromcounts, singular check     (:2-9, :57-80)
+ *   src/couplingmatrices.jl                 coupling store                    (:11-53)
+ *   src/nca/abstractnca.jl                  coefficient plan, near field      (:110-119, :134-178)
+ *   src/admissibility/farinteractions.jl    FarData, farfield, CSR transpose  (:38-92)
+ *   src/admissibility/nearinteractions.jl   ball admissibility (LF branch)    (:84-95)
+ *   src/nca/aggregate.jl, couple.jl, disaggregate.jl   the five apply stages
+ *   src/nca/petrovgalerkinnca.jl            forward / transpose / adjoint     (:431-589)
+ *
+ * Parts of the path live in packages that are not in the reference tree
+ * (AdaptiveCrossApproximation.jl 0.4: fully pivoted ACA, FNormEstimator, tree-mimicry
+ * pivoting, `interactions`, `isnear`; H2Trees.jl 0.4 + ParallelKMeans 1.1: the k-means
+ * tree). Their published algorithms are restated with the project's fixed rules:
+ *   - fully pivoted ACA: argmax of |R_ij|^2, ties to the lowest column-major index; row and
+ *     column of each pivot zeroed after the rank-1 update; stop after r crosses when
+ *     ||R_r||_F^2 * s/(s-r) <= tol^2 ||A||_F^2 (sampled, s = block columns) or
+ *     ||R_r||_F^2 <= tol^2 ||A||_F^2 (unsampled). Pinned by the reference KATs
+ *     test/compressors/test_batchedbottomup.jl:43-52 and test/gpu/test_compresslevel.jl:127-189.
+ *   - the squared Frobenius norms are summed in one fixed order (256 strided partial sums,
+ *     then halving trees inside groups of 32 and over the 8 group totals); the device kernel
+ *     uses the same order, so both decide convergence identically.
+ *   - k-means tree: 2 clusters, farthest-point seeds, Lloyd iterations, stable partition.
+ *   - tree mimicry: greedy descent of the far tree maximising dmin^2(y)/|y-c_t|^2.
+ *   - kernel entries: sin/cos by Cody-Waite reduction with a three-part pi/2 and Taylor
+ *     polynomials on [-pi/4, pi/4] (Horner with fused multiply-add); every floating-point
+ *     step is written out, so the device code reproduces each entry bit for bit.
+ * Compile with -ffp-contract=off: every fused multiply-add here is an explicit fma().
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct {
+    double re, im;
+} oc;
+
+static inline oc oc_make(double re, double im) {
+    oc r;
+    r.re = re;
+    r.im = im;
+    return r;
+}
+/* (a.re + i a.im)(b.re + i b.im) with the project's fixed rounding sequence. */
+static inline oc oc_mul(oc a, oc b) {
+    oc r;
+    r.re = fma(a.re, b.re, -(a.im * b.im));
+    r.im = fma(a.re, b.im, a.im * b.re);
+    return r;
+}
+static inline oc oc_conj(oc a) { return oc_make(a.re, -a.im); }
+static inline double oc_abs2(oc a) { return fma(a.re, a.re, a.im * a.im); }
+
+/* ------------------------------------------------------------------------------------ */
+/* Kernel entries                                                                        */
+/* ------------------------------------------------------------------------------------ */
+
+enum {
+    OK_HELMHOLTZ = 0, /* cis(s k r) / (4 pi r), s = +1 or -1 */
+    OK_LAPLACE = 1,   /* 1 / (4 pi r) */
+    OK_MATRIX = 2     /* entry (i, j) of a given column-major complex matrix */
+};
+
+typedef struct {
+    int kind;
+    int sign;
+    double k;
+    double rmin;
+    const double *mat;
+    long ldmat;
+} okern;
+
+static const double PIO2_1 = 0x1.921fb54442d18p+0;
+static const double PIO2_2 = 0x1.1a62633145c07p-54;
+static const double PIO2_3 = -0x1.f1976b7ed8fbcp-110;
+static const double TWO_OVER_PI = 0x1.45f306dc9c883p-1;
+static const double FOUR_PI = 0x1.921fb54442d18p+3;
+
+/* sin and cos of x (|x| < 2^20): x = q pi/2 + y, |y| <= pi/4, then Taylor series of
+ * degree 17 (sin) and 18 (cos) in Horner form. Coefficients are (-1)^k/(2k+1)! and
+ * (-1)^k/(2k)!, each rounded to the nearest double. */
+void oracle_sincos(double x, double *s, double *c) {
+    double q = rint(x * TWO_OVER_PI);
+    double y = fma(-q, PIO2_1, x);
+    y = fma(-q, PIO2_2, y);
+    y = fma(-q, PIO2_3, y);
+    double y2 = y * y;
+    double ps = 0x1.952c77030ad4ap-49;
+    ps = fma(ps, y2, -0x1.ae7f3e733b81fp-41);
+    ps = fma(ps, y2, 0x1.6124613a86d09p-33);
+    ps = fma(ps, y2, -0x1.ae64567f544e4p-26);
+    ps = fma(ps, y2, 0x1.71de3a556c734p-19);
+    ps = fma(ps, y2, -0x1.a01a01a01a01ap-13);
+    ps = fma(ps, y2, 0x1.1111111111111p-7);
+    ps = fma(ps, y2, -0x1.5555555555555p-3);
+    double sn = fma(y * y2, ps, y);
+    double pc = -0x1.6827863b97d97p-53;
+    pc = fma(pc, y2, 0x1.ae7f3e733b81fp-45);
+    pc = fma(pc, y2, -0x1.93974a8c07c9dp-37);
+    pc = fma(pc, y2, 0x1.1eed8eff8d898p-29);
+    pc = fma(pc, y2, -0x1.27e4fb7789f5cp-22);
+    pc = fma(pc, y2, 0x1.a01a01a01a01ap-16);
+    pc = fma(pc, y2, -0x1.6c16c16c16c17p-10);
+    pc = fma(pc, y2, 0x1.5555555555555p-5);
+    pc = fma(pc, y2, -0x1.0000000000000p-1);
+    double cs = fma(y2, pc, 1.0);
+    long iq = (long)q;
+    int quadrant = (int)(((iq % 4) + 4) % 4);
+    switch (quadrant) {
+    case 0: *s = sn; *c = cs; break;
+    case 1: *s = cs; *c = -sn; break;
+    case 2: *s = -sn; *c = -cs; break;
+    default: *s = -cs; *c = sn; break;
+    }
+}
+
+/* Entry of the kernel matrix for test point x (global index i) and trial point y (j). */
+static inline oc okern_entry(const okern *K, const double *x, const double *y, long i, long j) {
+    if (K->kind == OK_MATRIX) {
+        const double *e = K->mat + 2 * (i + j * K->ldmat);
+        return oc_make(e[0], e[1]);
+    }
+    double dx = x[0] - y[0], dy = x[1] - y[1], dz = x[2] - y[2];
+    double d2 = fma(dx, dx, fma(dy, dy, dz * dz));
+    double r = sqrt(d2);
+    if (r == 0.0 || r < K->rmin)
+        return oc_make(0.0, 0.0);
+    double inv = 1.0 / (FOUR_PI * r);
+    if (K->kind == OK_LAPLACE)
+        return oc_make(inv, 0.0);
+    double s, c;
+    oracle_sincos(K->k * r, &s, &c);
+    if (K->sign < 0)
+        return oc_make(c * inv, -(s * inv));
+    return oc_make(c * inv, s * inv);
+}
+
+void oracle_entries(int kind, int sign, double k, double rmin, const double *mat, long ldmat,
+                    const double *xs, const double *ys, const long *ii, const long *jj, long n,
+                    double *out) {
+    okern K = {kind, sign, k, rmin, mat, ldmat};
+    for (long e = 0; e < n; ++e) {
+        oc v = okern_entry(&K, xs + 3 * ii[e], ys + 3 * jj[e], ii[e], jj[e]);
+        out[2 * e] = v.re;
+        out[2 * e + 1] = v.im;
+    }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* k-means cluster tree (restates H2Trees.KMeansTree with numberofclusters = 2)           */
+/* ------------------------------------------------------------------------------------ */
+
+typedef struct {
+    long n;
+    int nnodes, nlevels;
+    int *perm, *iperm;
+    int *begin, *end, *parent, *firstchild, *nchildren, *level;
+    double *center, *radius;
+    int *levelptr;
+} otree;
+
+static double d2pts(const double *a, const double *b) {
+    double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+    return fma(dx, dx, fma(dy, dy, dz * dz));
+}
+
+#define KMEANS_MAXIT 50
+
+/* Split perm[b:e) into two stable parts; returns the size of the first part. */
+static int kmeans_split(const double *pts, int *perm, int b, int e, int *assign, int *tmp) {
+    int cnt = e - b;
+    double g[3] = {0, 0, 0};
+    for (int i = b; i < e; ++i) {
+        const double *p = pts + 3 * (long)perm[i];
+        g[0] += p[0];
+        g[1] += p[1];
+        g[2] += p[2];
+    }
+    g[0] /= cnt;
+    g[1] /= cnt;
+    g[2] /= cnt;
+    int ia = b;
+    double best = -1.0;
+    for (int i = b; i < e; ++i) {
+        double d = d2pts(pts + 3 * (long)perm[i], g);
+        if (d > best) {
+            best = d;
+            ia = i;
+        }
+    }
+    int ib = b;
+    best = -1.0;
+    for (int i = b; i < e; ++i) {
+        double d = d2pts(pts + 3 * (long)perm[i], pts + 3 * (long)perm[ia]);
+        if (d > best) {
+            best = d;
+            ib = i;
+        }
+    }
+    int n0 = 0;
+    if (best > 0.0) {
+        double c0[3], c1[3];
+        memcpy(c0, pts + 3 * (long)perm[ia], sizeof c0);
+        memcpy(c1, pts + 3 * (long)perm[ib], sizeof c1);
+        for (int i = 0; i < cnt; ++i)
+            assign[i] = -1;
+        for (int it = 0; it < KMEANS_MAXIT; ++it) {
+            int changed = 0;
+            for (int i = 0; i < cnt; ++i) {
+                const double *p = pts + 3 * (long)perm[b + i];
+                int a = d2pts(p, c1) < d2pts(p, c0) ? 1 : 0;
+                if (a != assign[i]) {
+                    changed = 1;
+                    assign[i] = a;
+                }
+            }
+            if (!changed)
+                break;
+            double s0[3] = {0, 0, 0}, s1[3] = {0, 0, 0};
+            int m0 = 0, m1 = 0;
+            for (int i = 0; i < cnt; ++i) {
+                const double *p = pts + 3 * (long)perm[b + i];
+                if (assign[i] == 0) {
+                    s0[0] += p[0]; s0[1] += p[1]; s0[2] += p[2];
+                    ++m0;
+                } else {
+                    s1[0] += p[0]; s1[1] += p[1]; s1[2] += p[2];
+                    ++m1;
+                }
+            }
+            if (m0 == 0 || m1 == 0)
+                break;
+            for (int d = 0; d < 3; ++d) {
+                c0[d] = s0[d] / m0;
+                c1[d] = s1[d] / m1;
+            }
+        }
+        for (int i = 0; i < cnt; ++i)
+            n0 += assign[i] == 0;
+    }
+    if (n0 == 0 || n0 == cnt) {
+        n0 = (cnt + 1) / 2;
+        for (int i = 0; i < cnt; ++i)
+            assign[i] = i < n0 ? 0 : 1;
+    }
+    int k = 0;
+    for (int i = 0; i < cnt; ++i)
+        if (assign[i] == 0)
+            tmp[k++] = perm[b + i];
+    for (int i = 0; i < cnt; ++i)
+        if (assign[i] == 1)
+            tmp[k++] = perm[b + i];
+    memcpy(perm + b, tmp, sizeof(int) * cnt);
+    return n0;
+}
+
+static void node_ball(const double *pts, const int *perm, int b, int e, double *c, double *r) {
+    double s[3] = {0, 0, 0};
+    for (int i = b; i < e; ++i) {
+        const double *p = pts + 3 * (long)perm[i];
+        s[0] += p[0];
+        s[1] += p[1];
+        s[2] += p[2];
+    }
+    int cnt = e - b;
+    for (int d = 0; d < 3; ++d)
+        c[d] = cnt > 0 ? s[d] / cnt : 0.0;
+    double m = 0.0;
+    for (int i = b; i < e; ++i) {
+        double d = d2pts(pts + 3 * (long)perm[i], c);
+        if (d > m)
+            m = d;
+    }
+    *r = sqrt(m);
+}
+
+otree *oracle_tree_build(const double *pts, long n, int minvalues) {
+    otree *T = calloc(1, sizeof(otree));
+    T->n = n;
+    long cap = 2 * n + 1;
+    T->perm = malloc(sizeof(int) * (n > 0 ? n : 1));
+    T->iperm = malloc(sizeof(int) * (n > 0 ? n : 1));
+    T->begin = malloc(sizeof(int) * cap);
+    T->end = malloc(sizeof(int) * cap);
+    T->parent = malloc(sizeof(int) * cap);
+    T->firstchild = malloc(sizeof(int) * cap);
+    T->nchildren = malloc(sizeof(int) * cap);
+    T->level = malloc(sizeof(int) * cap);
+    T->center = malloc(sizeof(double) * 3 * cap);
+    T->radius = malloc(sizeof(double) * cap);
+    for (long i = 0; i < n; ++i)
+        T->perm[i] = (int)i;
+    int *assign = malloc(sizeof(int) * (n > 0 ? n : 1));
+    int *tmp = malloc(sizeof(int) * (n > 0 ? n : 1));
+    T->begin[0] = 0;
+    T->end[0] = (int)n;
+    T->parent[0] = -1;
+    T->level[0] = 0;
+    int nn = 1;
+    for (int node = 0; node < nn; ++node) {
+        int b = T->begin[node], e = T->end[node];
+        int cnt = e - b;
+        if (cnt > minvalues && cnt >= 2) {
+            int n0 = kmeans_split(pts, T->perm, b, e, assign, tmp);
+            T->firstchild[node] = nn;
+            T->nchildren[node] = 2;
+            for (int c = 0; c < 2; ++c) {
+                int id = nn + c;
+                T->begin[id] = c == 0 ? b : b + n0;
+                T->end[id] = c == 0 ? b + n0 : e;
+                T->parent[id] = node;
+                T->level[id] = T->level[node] + 1;
+            }
+            nn += 2;
+        } else {
+            T->firstchild[node] = -1;
+            T->nchildren[node] = 0;
+        }
+    }
+    for (int node = 0; node < nn; ++node)
+        node_ball(pts, T->perm, T->begin[node], T->end[node], T->center + 3 * node,
+                  T->radius + node);
+    T->nnodes = nn;
+    T->nlevels = T->level[nn - 1] + 1;
+    T->levelptr = malloc(sizeof(int) * (T->nlevels + 1));
+    int l = 0;
+    T->levelptr[0] = 0;
+    for (int node = 0; node < nn; ++node)
+        while (T->level[node] > l)
+            T->levelptr[++l] = node;
+    T->levelptr[T->nlevels] = nn;
+    for (long i = 0; i < n; ++i)
+        T->iperm[T->perm[i]] = (int)i;
+    free(assign);
+    free(tmp);
+    return T;
+}
+
+void oracle_tree_free(otree *T) {
+    if (!T)
+        return;
+    free(T->perm); free(T->iperm); free(T->begin); free(T->end); free(T->parent);
+    free(T->firstchild); free(T->nchildren); free(T->level); free(T->center);
+    free(T->radius); free(T->levelptr);
+    free(T);
+}
+
+int oracle_tree_nnodes(const otree *T) { return T->nnodes; }
+int oracle_tree_nlevels(const otree *T) { return T->nlevels; }
+void oracle_tree_export(const otree *T, int *perm, int *begin, int *end, int *parent,
+                        int *firstchild, int *nchildren, int *level, double *center,
+                        double *radius) {
+    memcpy(perm, T->perm, sizeof(int) * T->n);
+    memcpy(begin, T->begin, sizeof(int) * T->nnodes);
+    memcpy(end, T->end, sizeof(int) * T->nnodes);
+    memcpy(parent, T->parent, sizeof(int) * T->nnodes);
+    memcpy(firstchild, T->firstchild, sizeof(int) * T->nnodes);
+    memcpy(nchildren, T->nchildren, sizeof(int) * T->nnodes);
+    memcpy(level, T->level, sizeof(int) * T->nnodes);
+    memcpy(center, T->center, sizeof(double) * 3 * T->nnodes);
+    memcpy(radius, T->radius, sizeof(double) * T->nnodes);
+}
+
+static inline int isleaf(const otree *T, int node) { return T->nchildren[node] == 0; }
+
+/* ------------------------------------------------------------------------------------ */
+/* Admissibility and interaction lists                                                   */
+/* ------------------------------------------------------------------------------------ */
+
+/* Ball admissibility (the low-frequency branch of nearinteractions.jl:84-95). */
+static int isnear_ball(const otree *A, const otree *B, int a, int b, double eta) {
+    double ra = A->radius[a], rb = B->radius[b];
+    double dist = sqrt(d2pts(A->center + 3 * a, B->center + 3 * b)) - (ra + rb);
+    double sep = dist > 0.0 ? dist : 0.0;
+    double rmax = ra > rb ? ra : rb;
+    return 2.0 * rmax > eta * sep;
+}
+
+typedef struct {
+    int *t, *s;
+    long n, cap;
+} pairlist;
+
+static void pl_push(pairlist *p, int t, int s) {
+    if (p->n == p->cap) {
+        p->cap = p->cap ? 2 * p->cap : 1024;
+        p->t = realloc(p->t, sizeof(int) * p->cap);
+        p->s = realloc(p->s, sizeof(int) * p->cap);
+    }
+    p->t[p->n] = t;
+    p->s[p->n] = s;
+    p->n++;
+}
+
+static void dual_visit(const otree *T, const otree *S, int t, int s, double eta, pairlist *nearp,
+                       pairlist *farp) {
+    if (!isnear_ball(T, S, t, s, eta)) {
+        pl_push(farp, t, s);
+    } else if (isleaf(T, t) && isleaf(S, s)) {
+        pl_push(nearp, t, s);
+    } else if (isleaf(T, t)) {
+        for (int c = 0; c < S->nchildren[s]; ++c)
+            dual_visit(T, S, t, S->firstchild[s] + c, eta, nearp, farp);
+    } else if (isleaf(S, s)) {
+        for (int c = 0; c < T->nchildren[t]; ++c)
+            dual_visit(T, S, T->firstchild[t] + c, s, eta, nearp, farp);
+    } else {
+        for (int c = 0; c < T->nchildren[t]; ++c)
+            for (int d = 0; d < S->nchildren[s]; ++d)
+                dual_visit(T, S, T->firstchild[t] + c, S->firstchild[s] + d, eta, nearp, farp);
+    }
+}
+
+static int cmp_int(const void *a, const void *b) {
+    int x = *(const int *)a, y = *(const int *)b;
+    return (x > y) - (x < y);
+}
+
+/* CSR over `nrows` keys with each row's entries sorted ascending. */
+static void pairs_to_csr(const int *key, const int *val, long n, int nrows, int **ptr_out,
+                         int **idx_out) {
+    int *ptr = calloc(nrows + 1, sizeof(int));
+    int *idx = malloc(sizeof(int) * (n > 0 ? n : 1));
+    for (long i = 0; i < n; ++i)
+        ptr[key[i] + 1]++;
+    for (int r = 0; r < nrows; ++r)
+        ptr[r + 1] += ptr[r];
+    int *cur = malloc(sizeof(int) * (nrows > 0 ? nrows : 1));
+    memcpy(cur, ptr, sizeof(int) * nrows);
+    for (long i = 0; i < n; ++i)
+        idx[cur[key[i]]++] = val[i];
+    for (int r = 0; r < nrows; ++r)
+        qsort(idx + ptr[r], ptr[r + 1] - ptr[r], sizeof(int), cmp_int);
+    free(cur);
+    *ptr_out = ptr;
+    *idx_out = idx;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Phase 1: geometric far pivots (tree mimicry)                                         */
+/* ------------------------------------------------------------------------------------ */
+
+/* min(limit, number of points of node), as the capped _clustersize (pivots.jl:15-25). */
+static int clustersize_capped(const otree *T, int node, int limit) {
+    if (limit <= 0)
+        return 0;
+    int c = T->end[node] - T->begin[node];
+    return c < limit ? c : limit;
+}
+
+typedef struct {
+    const otree *F;       /* far tree */
+    const double *fpts;   /* far-side points */
+    double c[3];          /* centroid of the cluster's own points */
+    const int *nodes;     /* far nodes */
+    int nnodes;
+    int *chosen;          /* chosen far points (global ids) */
+    double *chosenxyz;
+    int *chosenpos;       /* their positions in F->perm */
+    int nchosen;
+    double *rootdmin;     /* per far node: min squared distance of its centre to the chosen */
+    int *rootcnt;         /* per far node: chosen points inside it */
+} mimicry;
+
+static double mim_score(const mimicry *M, const double *y, double dmin2) {
+    double d2 = d2pts(y, M->c);
+    if (d2 < 1e-300)
+        d2 = 1e-300;
+    return dmin2 / d2;
+}
+
+static double mim_dmin(const mimicry *M, const double *y) {
+    if (M->nchosen == 0)
+        return 1.0;
+    double m = INFINITY;
+    for (int q = 0; q < M->nchosen; ++q) {
+        double d = d2pts(y, M->chosenxyz + 3 * q);
+        if (d < m)
+            m = d;
+    }
+    return m;
+}
+
+static int mim_inside(const mimicry *M, int node) {
+    int b = M->F->begin[node], e = M->F->end[node], k = 0;
+    for (int q = 0; q < M->nchosen; ++q)
+        k += (M->chosenpos[q] >= b && M->chosenpos[q] < e);
+    return k;
+}
+
+static int mim_next(mimicry *M) {
+    const otree *F = M->F;
+    int best = -1;
+    double bests = -1.0;
+    for (int i = 0; i < M->nnodes; ++i) {
+        int f = M->nodes[i];
+        if (F->end[f] - F->begin[f] - M->rootcnt[i] <= 0)
+            continue;
+        double sc = mim_score(M, F->center + 3 * f, M->rootdmin[i]);
+        if (sc > bests) {
+            bests = sc;
+            best = f;
+        }
+    }
+    int node = best;
+    while (!isleaf(F, node)) {
+        int bc = -1;
+        double bs = -1.0;
+        for (int c = 0; c < F->nchildren[node]; ++c) {
+            int ch = F->firstchild[node] + c;
+            if (F->end[ch] - F->begin[ch] - mim_inside(M, ch) <= 0)
+                continue;
+            const double *cc = F->center + 3 * ch;
+            double sc = mim_score(M, cc, mim_dmin(M, cc));
+            if (sc > bs) {
+                bs = sc;
+                bc = ch;
+            }
+        }
+        node = bc;
+    }
+    int bp = -1;
+    double bs = -1.0;
+    for (int pos = F->begin[node]; pos < F->end[node]; ++pos) {
+        int taken = 0;
+        for (int q = 0; q < M->nchosen; ++q)
+            if (M->chosenpos[q] == pos) {
+                taken = 1;
+                break;
+            }
+        if (taken)
+            continue;
+        const double *y = M->fpts + 3 * (long)F->perm[pos];
+        double sc = mim_score(M, y, mim_dmin(M, y));
+        if (sc > bs) {
+            bs = sc;
+            bp = pos;
+        }
+    }
+    int pid = F->perm[bp];
+    int q = M->nchosen++;
+    M->chosen[q] = pid;
+    M->chosenpos[q] = bp;
+    memcpy(M->chosenxyz + 3 * q, M->fpts + 3 * (long)pid, 3 * sizeof(double));
+    for (int i = 0; i < M->nnodes; ++i) {
+        int f = M->nodes[i];
+        double d = d2pts(F->center + 3 * f, M->chosenxyz + 3 * q);
+        if (q == 0 || d < M->rootdmin[i])
+            M->rootdmin[i] = d;
+        if (bp >= F->begin[f] && bp < F->end[f])
+            M->rootcnt[i]++;
+    }
+    return pid;
+}
+
+/* _selectfarpivots (batchedbottomup.jl:54-72): up to min(maxrank, |refidcs|) far points. */
+int oracle_select_farpivots(const otree *F, const double *ownpts, const double *farpts,
+                            const int *refidcs, int nref, const int *farnodes, int nfar,
+                            int maxrank, int *out) {
+    int limit = maxrank < nref ? maxrank : nref;
+    int n = 0;
+    for (int i = 0; i < nfar; ++i) {
+        n += clustersize_capped(F, farnodes[i], limit - n);
+        if (n == limit)
+            break;
+    }
+    if (n <= 0)
+        return 0;
+    mimicry M;
+    M.F = F;
+    M.fpts = farpts;
+    double s[3] = {0, 0, 0};
+    for (int i = 0; i < nref; ++i) {
+        const double *p = ownpts + 3 * (long)refidcs[i];
+        s[0] += p[0];
+        s[1] += p[1];
+        s[2] += p[2];
+    }
+    for (int d = 0; d < 3; ++d)
+        M.c[d] = s[d] / nref;
+    M.nodes = farnodes;
+    M.nnodes = nfar;
+    M.chosen = out;
+    M.chosenxyz = malloc(sizeof(double) * 3 * n);
+    M.chosenpos = malloc(sizeof(int) * n);
+    M.nchosen = 0;
+    M.rootdmin = malloc(sizeof(double) * (nfar > 0 ? nfar : 1));
+    M.rootcnt = calloc(nfar > 0 ? nfar : 1, sizeof(int));
+    for (int i = 0; i < nfar; ++i)
+        M.rootdmin[i] = 1.0;
+    for (int p = 0; p < n; ++p)
+        mim_next(&M);
+    free(M.chosenxyz);
+    free(M.chosenpos);
+    free(M.rootdmin);
+    free(M.rootcnt);
+    return n;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Fixed-order squared Frobenius norm and argmax                                        */
+/* ------------------------------------------------------------------------------------ */
+
+#define NRED 256
+
+/* Sum of |R_e|^2 over e < len in the fixed order; argmax with lowest-index ties. */
+static double fixed_norm2(const oc *R, long len, double *vmax, long *emax) {
+    double part[NRED];
+    double bv = -1.0;
+    long be = -1;
+    for (int k = 0; k < NRED; ++k) {
+        double acc = 0.0;
+        for (long e = k; e < len; e += NRED) {
+            double a = oc_abs2(R[e]);
+            acc = acc + a;
+        }
+        part[k] = acc;
+    }
+    for (long e = 0; e < len; ++e) {
+        double a = oc_abs2(R[e]);
+        if (a > bv) {
+            bv = a;
+            be = e;
+        }
+    }
+    double warp[NRED / 32];
+    for (int w = 0; w < NRED / 32; ++w) {
+        double *p = part + 32 * w;
+        for (int off = 16; off >= 1; off >>= 1)
+            for (int k = 0; k < off; ++k)
+                p[k] = p[k] + p[k + off];
+        warp[w] = p[0];
+    }
+    for (int off = NRED / 64; off >= 1; off >>= 1)
+        for (int k = 0; k < off; ++k)
+            warp[k] = warp[k] + warp[k + off];
+    *vmax = bv;
+    *emax = be;
+    return warp[0];
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Fully pivoted ACA on an m x n block (column-major). Overwrites R.                     */
+/* ------------------------------------------------------------------------------------ */
+
+int oracle_aca_block(oc *R, int m, int n, int maxrank, double tol, int sampled, int *rowpiv,
+                     int *colpiv) {
+    int limit = maxrank;
+    if (m < limit)
+        limit = m;
+    if (n < limit)
+        limit = n;
+    if (limit <= 0)
+        return 0;
+    long len = (long)m * n;
+    double vmax;
+    long emax;
+    double normA2 = fixed_norm2(R, len, &vmax, &emax);
+    double normR2 = normA2;
+    double tol2 = tol * tol;
+    double rhs = tol2 * normA2;
+    oc *u = malloc(sizeof(oc) * m);
+    oc *v = malloc(sizeof(oc) * n);
+    int r = 0;
+    while (r < limit) {
+        if (!(vmax > 0.0))
+            break;
+        double lhs = sampled ? (normR2 * (double)n) / (double)(n - r) : normR2;
+        if (lhs <= rhs)
+            break;
+        int ip = (int)(emax % m), jp = (int)(emax / m);
+        rowpiv[r] = ip;
+        colpiv[r] = jp;
+        oc p = R[ip + (long)jp * m];
+        double d = oc_abs2(p);
+        oc w = oc_make(p.re / d, -(p.im / d));
+        for (int i = 0; i < m; ++i)
+            u[i] = R[i + (long)jp * m];
+        for (int j = 0; j < n; ++j)
+            v[j] = oc_mul(R[ip + (long)j * m], w);
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < m; ++i) {
+                oc t = oc_mul(u[i], v[j]);
+                oc *x = R + i + (long)j * m;
+                x->re = x->re - t.re;
+                x->im = x->im - t.im;
+            }
+        for (int j = 0; j < n; ++j)
+            R[ip + (long)j * m] = oc_make(0.0, 0.0);
+        for (int i = 0; i < m; ++i)
+            R[i + (long)jp * m] = oc_make(0.0, 0.0);
+        ++r;
+        normR2 = fixed_norm2(R, len, &vmax, &emax);
+    }
+    free(u);
+    free(v);
+    return r;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Cross factorization (utils.jl:57-80) and X = L P^{-1}                                */
+/* ------------------------------------------------------------------------------------ */
+
+/* LU with partial pivoting of the r x r matrix P (column-major, in place), the singular
+ * check of _crossfactorization, then X <- X P^{-1} for the m x r matrix X.
+ * Returns 0, or the numerical rank (< r) when the cross matrix is singular. */
+static int cross_solve(oc *P, int r, oc *X, int m, int *rank_out) {
+    if (r == 0) {
+        *rank_out = 0;
+        return 0;
+    }
+    int *ipiv = malloc(sizeof(int) * r);
+    int zero_pivot = 0;
+    for (int k = 0; k < r; ++k) {
+        int pr = k;
+        double bv = -1.0;
+        for (int i = k; i < r; ++i) {
+            double a = oc_abs2(P[i + (long)k * r]);
+            if (a > bv) {
+                bv = a;
+                pr = i;
+            }
+        }
+        ipiv[k] = pr;
+        if (pr != k)
+            for (int j = 0; j < r; ++j) {
+                oc t = P[k + (long)j * r];
+                P[k + (long)j * r] = P[pr + (long)j * r];
+                P[pr + (long)j * r] = t;
+            }
+        oc piv = P[k + (long)k * r];
+        double d = oc_abs2(piv);
+        if (d == 0.0) {
+            zero_pivot = 1;
+            continue;
+        }
+        oc w = oc_make(piv.re / d, -(piv.im / d));
+        for (int i = k + 1; i < r; ++i)
+            P[i + (long)k * r] = oc_mul(P[i + (long)k * r], w);
+        for (int j = k + 1; j < r; ++j) {
+            oc a = P[k + (long)j * r];
+            for (int i = k + 1; i < r; ++i) {
+                oc t = oc_mul(P[i + (long)k * r], a);
+                P[i + (long)j * r].re -= t.re;
+                P[i + (long)j * r].im -= t.im;
+            }
+        }
+    }
+    double d2max = 0.0, d2min = INFINITY;
+    for (int i = 0; i < r; ++i) {
+        double d2 = oc_abs2(P[i + (long)i * r]);
+        if (d2 > d2max)
+            d2max = d2;
+        if (d2 < d2min)
+            d2min = d2;
+    }
+    double eps = 0x1p-52;
+    double tol2 = (10.0 * eps) * (10.0 * eps) * d2max;
+    if (zero_pivot || !(d2min > tol2)) {
+        int rank = 0;
+        for (int i = 0; i < r; ++i)
+            rank += oc_abs2(P[i + (long)i * r]) > tol2;
+        *rank_out = rank;
+        free(ipiv);
+        return 1;
+    }
+    /* X P = L with P = Pi^T L U: solve row by row. */
+    oc *z = malloc(sizeof(oc) * r);
+    for (int row = 0; row < m; ++row) {
+        for (int j = 0; j < r; ++j)
+            z[j] = X[row + (long)j * m];
+        for (int j = 0; j < r; ++j) {
+            oc acc = z[j];
+            for (int i = 0; i < j; ++i) {
+                oc t = oc_mul(z[i], P[i + (long)j * r]);
+                acc.re -= t.re;
+                acc.im -= t.im;
+            }
+            oc u = P[j + (long)j * r];
+            double d = oc_abs2(u);
+            z[j] = oc_mul(acc, oc_make(u.re / d, -(u.im / d)));
+        }
+        for (int j = r - 1; j >= 0; --j) {
+            oc acc = z[j];
+            for (int i = j + 1; i < r; ++i) {
+                oc t = oc_mul(z[i], P[i + (long)j * r]);
+                acc.re -= t.re;
+                acc.im -= t.im;
+            }
+            z[j] = acc;
+        }
+        for (int k = r - 1; k >= 0; --k)
+            if (ipiv[k] != k) {
+                oc t = z[k];
+                z[k] = z[ipiv[k]];
+                z[ipiv[k]] = t;
+            }
+        for (int j = 0; j < r; ++j)
+            X[row + (long)j * m] = z[j];
+    }
+    free(z);
+    free(ipiv);
+    *rank_out = r;
+    return 0;
+}
+
+/* X = L[:, 0:r] P^{-1} with P = L[rows, 0:r]; L is m x r column-major (interleaved complex).
+ * Returns 0 or 1 (singular; *rank set). Used by the nested basis KATs. */
+int oracle_cross_solve(const double *L, int m, int r, const int *rows, double *X, int *rank) {
+    oc *P = malloc(sizeof(oc) * (r > 0 ? r * r : 1));
+    for (int j = 0; j < r; ++j)
+        for (int i = 0; i < r; ++i) {
+            const double *e = L + 2 * (rows[i] + (long)j * m);
+            P[i + (long)j * r] = oc_make(e[0], e[1]);
+        }
+    memcpy(X, L, sizeof(oc) * (size_t)m * r);
+    int st = cross_solve(P, r, (oc *)X, m, rank);
+    free(P);
+    return st;
+}
+
+int oracle_aca(const double *A, int m, int n, int maxrank, double tol, int sampled, int *rowpiv,
+               int *colpiv) {
+    oc *R = malloc(sizeof(oc) * ((size_t)m * n > 0 ? (size_t)m * n : 1));
+    memcpy(R, A, sizeof(oc) * (size_t)m * n);
+    int r = oracle_aca_block(R, m, n, maxrank, tol, sampled, rowpiv, colpiv);
+    free(R);
+    return r;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Whole batched bottom-up build                                                        */
+/* ------------------------------------------------------------------------------------ */
+
+typedef struct {
+    okern K;
+    double *mat_copy;
+    long npts[2];
+    double *pts[2];
+    otree *tree[2];
+    double eta;
+    int maxrank, sampled;
+    double tol[2];
+    /* partition, indexed by test nodes (near/far) and trial nodes (transposes) */
+    int *nearptr, *nearnodes, *farptr, *farnodes;
+    int *tnearptr, *tnearnodes, *tfarptr, *tfarnodes;
+    /* per side: far pivots CSR, ranks, pivots, row counts, X blocks */
+    int *fpptr[2], *fpidx[2];
+    int *rank[2], *nrows[2];
+    int *pivptr[2], *pividx[2]; /* pivots in CSR form once the build is done */
+    int *pivtmp[2];             /* nnodes x maxrank during the build */
+    long *xoff[2];
+    oc *X[2];
+    long *cptr[2]; /* coefficient plan (0-based) */
+    /* couplings: per far pair in test CSR order */
+    long *coff;
+    oc *C;
+    /* near: per test node, row block |t| x ncols (offset -1 if none) */
+    long *noff;
+    int *ncols;
+    oc *N;
+    /* trial-side near transpose: for each entry of tnear lists, column offset in row block */
+    int *tnear_coloff;
+    int status, bad_side, bad_node, bad_npiv, bad_rank;
+    int nthreads;
+} ohandle;
+
+static const double *side_pt(const ohandle *H, int side, long idx) {
+    return H->pts[side] + 3 * idx;
+}
+
+/* Entry of the level block of `side` for own point `own` and far point `far`. */
+static inline oc level_entry(const ohandle *H, int side, long own, long far) {
+    if (side == 0)
+        return okern_entry(&H->K, side_pt(H, 0, own), side_pt(H, 1, far), own, far);
+    return okern_entry(&H->K, side_pt(H, 0, far), side_pt(H, 1, own), far, own);
+}
+
+static void build_side(ohandle *H, int side) {
+    const otree *T = H->tree[side];
+    const otree *F = H->tree[1 - side];
+    int nn = T->nnodes;
+    int maxrank = H->maxrank;
+    /* phase 1: far field = own far nodes + ancestors' far nodes */
+    const int *ptr = side == 0 ? H->farptr : H->tfarptr;
+    const int *nodes = side == 0 ? H->farnodes : H->tfarnodes;
+    int *cnt = calloc(nn, sizeof(int));
+    int *tmpfp = malloc(sizeof(int) * (size_t)nn * (maxrank > 0 ? maxrank : 1));
+#pragma omp parallel for schedule(dynamic, 4) num_threads(H->nthreads)
+    for (int t = 0; t < nn; ++t) {
+        int total = 0;
+        for (int a = t; a >= 0; a = T->parent[a])
+            total += ptr[a + 1] - ptr[a];
+        if (total == 0)
+            continue;
+        int *ff = malloc(sizeof(int) * total);
+        int k = 0;
+        for (int a = t; a >= 0; a = T->parent[a])
+            for (int i = ptr[a]; i < ptr[a + 1]; ++i)
+                ff[k++] = nodes[i];
+        int nref = T->end[t] - T->begin[t];
+        cnt[t] = oracle_select_farpivots(F, H->pts[side], H->pts[1 - side], T->perm + T->begin[t],
+                                         nref, ff, total, maxrank, tmpfp + (size_t)t * maxrank);
+        free(ff);
+    }
+    H->fpptr[side] = malloc(sizeof(int) * (nn + 1));
+    H->fpptr[side][0] = 0;
+    for (int t = 0; t < nn; ++t)
+        H->fpptr[side][t + 1] = H->fpptr[side][t] + cnt[t];
+    H->fpidx[side] = malloc(sizeof(int) * (H->fpptr[side][nn] > 0 ? H->fpptr[side][nn] : 1));
+    for (int t = 0; t < nn; ++t)
+        memcpy(H->fpidx[side] + H->fpptr[side][t], tmpfp + (size_t)t * maxrank,
+               sizeof(int) * cnt[t]);
+    free(tmpfp);
+    free(cnt);
+
+    /* per-node row counts and X sizes need the children's ranks: run level by level */
+    H->rank[side] = calloc(nn, sizeof(int));
+    H->nrows[side] = calloc(nn, sizeof(int));
+    H->pivtmp[side] = malloc(sizeof(int) * (size_t)nn * (maxrank > 0 ? maxrank : 1));
+    oc **Xn = calloc(nn, sizeof(oc *));
+    double tol = H->tol[side];
+    int failed = 0;
+    for (int lev = T->nlevels - 1; lev >= 0 && !failed; --lev) {
+        int lb = T->levelptr[lev], le = T->levelptr[lev + 1];
+#pragma omp parallel for schedule(dynamic, 1) num_threads(H->nthreads)
+        for (int t = lb; t < le; ++t) {
+            int n = H->fpptr[side][t + 1] - H->fpptr[side][t];
+            if (n == 0)
+                continue;
+            const int *fp = H->fpidx[side] + H->fpptr[side][t];
+            int m;
+            int *rows;
+            if (isleaf(T, t)) {
+                m = T->end[t] - T->begin[t];
+                rows = malloc(sizeof(int) * (m > 0 ? m : 1));
+                memcpy(rows, T->perm + T->begin[t], sizeof(int) * m);
+            } else {
+                m = 0;
+                for (int c = 0; c < T->nchildren[t]; ++c)
+                    m += H->rank[side][T->firstchild[t] + c];
+                rows = malloc(sizeof(int) * (m > 0 ? m : 1));
+                int k = 0;
+                for (int c = 0; c < T->nchildren[t]; ++c) {
+                    int ch = T->firstchild[t] + c;
+                    memcpy(rows + k, H->pivtmp[side] + (size_t)ch * maxrank,
+                           sizeof(int) * H->rank[side][ch]);
+                    k += H->rank[side][ch];
+                }
+            }
+            H->nrows[side][t] = m;
+            oc *A = malloc(sizeof(oc) * ((size_t)m * n > 0 ? (size_t)m * n : 1));
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < m; ++i)
+                    A[i + (long)j * m] = level_entry(H, side, rows[i], fp[j]);
+            oc *R = malloc(sizeof(oc) * ((size_t)m * n > 0 ? (size_t)m * n : 1));
+            memcpy(R, A, sizeof(oc) * (size_t)m * n);
+            int rp[256], cp[256];
+            int r = oracle_aca_block(R, m, n, maxrank, tol, H->sampled, rp, cp);
+            free(R);
+            H->rank[side][t] = r;
+            for (int k = 0; k < r; ++k)
+                H->pivtmp[side][(size_t)t * maxrank + k] = rows[rp[k]];
+            oc *X = malloc(sizeof(oc) * ((size_t)m * r > 0 ? (size_t)m * r : 1));
+            oc *P = malloc(sizeof(oc) * (r > 0 ? (size_t)r * r : 1));
+            for (int j = 0; j < r; ++j) {
+                for (int i = 0; i < m; ++i)
+                    X[i + (long)j * m] = A[i + (long)cp[j] * m];
+                for (int i = 0; i < r; ++i)
+                    P[i + (long)j * r] = A[rp[i] + (long)cp[j] * m];
+            }
+            int rk;
+            int st = cross_solve(P, r, X, m, &rk);
+            free(P);
+            free(A);
+            free(rows);
+            Xn[t] = X;
+            if (st) {
+#pragma omp critical
+                {
+                    if (!failed || t < H->bad_node) {
+                        failed = 1;
+                        H->bad_side = side;
+                        H->bad_node = t;
+                        H->bad_npiv = r;
+                        H->bad_rank = rk;
+                    }
+                }
+            }
+        }
+    }
+    if (failed)
+        H->status = 1;
+    /* flatten pivots and X */
+    H->pivptr[side] = malloc(sizeof(int) * (nn + 1));
+    H->pivptr[side][0] = 0;
+    for (int t = 0; t < nn; ++t)
+        H->pivptr[side][t + 1] = H->pivptr[side][t] + H->rank[side][t];
+    H->pividx[side] = malloc(sizeof(int) * (H->pivptr[side][nn] > 0 ? H->pivptr[side][nn] : 1));
+    for (int t = 0; t < nn; ++t)
+        memcpy(H->pividx[side] + H->pivptr[side][t], H->pivtmp[side] + (size_t)t * maxrank,
+               sizeof(int) * H->rank[side][t]);
+    H->xoff[side] = malloc(sizeof(long) * (nn + 1));
+    H->xoff[side][0] = 0;
+    for (int t = 0; t < nn; ++t)
+        H->xoff[side][t + 1] = H->xoff[side][t] + (long)H->nrows[side][t] * H->rank[side][t];
+    H->X[side] = malloc(sizeof(oc) * (H->xoff[side][nn] > 0 ? H->xoff[side][nn] : 1));
+    for (int t = 0; t < nn; ++t) {
+        if (Xn[t])
+            memcpy(H->X[side] + H->xoff[side][t], Xn[t],
+                   sizeof(oc) * (H->xoff[side][t + 1] - H->xoff[side][t]));
+        free(Xn[t]);
+    }
+    free(Xn);
+    /* coefficient plan (plan_from_pivots, abstractnca.jl:110-119), 0-based */
+    H->cptr[side] = malloc(sizeof(long) * (nn + 1));
+    H->cptr[side][0] = 0;
+    for (int t = 0; t < nn; ++t)
+        H->cptr[side][t + 1] = H->cptr[side][t] + H->rank[side][t];
+}
+
+static void build_couplings(ohandle *H) {
+    const otree *T = H->tree[0];
+    int nn = T->nnodes;
+    long npairs = H->farptr[nn];
+    H->coff = malloc(sizeof(long) * (npairs + 1));
+    H->coff[0] = 0;
+    for (int t = 0; t < nn; ++t)
+        for (int i = H->farptr[t]; i < H->farptr[t + 1]; ++i) {
+            int s = H->farnodes[i];
+            H->coff[i + 1] = H->coff[i] + (long)H->rank[0][t] * H->rank[1][s];
+        }
+    H->C = malloc(sizeof(oc) * (H->coff[npairs] > 0 ? H->coff[npairs] : 1));
+#pragma omp parallel for schedule(dynamic, 16) num_threads(H->nthreads)
+    for (long i = 0; i < npairs; ++i) {
+        int t = -1;
+        /* find t with farptr[t] <= i < farptr[t+1] */
+        int lo = 0, hi = nn;
+        while (hi - lo > 1) {
+            int mid = (lo + hi) / 2;
+            if (H->farptr[mid] <= i)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        t = lo;
+        int s = H->farnodes[i];
+        int kt = H->rank[0][t], ks = H->rank[1][s];
+        const int *tp = H->pividx[0] + H->pivptr[0][t];
+        const int *sp = H->pividx[1] + H->pivptr[1][s];
+        oc *S = H->C + H->coff[i];
+        for (int j = 0; j < ks; ++j)
+            for (int a = 0; a < kt; ++a)
+                S[a + (long)j * kt] = okern_entry(&H->K, side_pt(H, 0, tp[a]), side_pt(H, 1, sp[j]),
+                                                  tp[a], sp[j]);
+    }
+}
+
+static void build_near(ohandle *H) {
+    const otree *T = H->tree[0], *S = H->tree[1];
+    int nn = T->nnodes;
+    H->noff = malloc(sizeof(long) * (nn + 1));
+    H->ncols = calloc(nn, sizeof(int));
+    H->noff[0] = 0;
+    for (int t = 0; t < nn; ++t) {
+        int nc = 0;
+        for (int i = H->nearptr[t]; i < H->nearptr[t + 1]; ++i) {
+            int s = H->nearnodes[i];
+            nc += S->end[s] - S->begin[s];
+        }
+        H->ncols[t] = nc;
+        H->noff[t + 1] = H->noff[t] + (long)(T->end[t] - T->begin[t]) * nc;
+    }
+    H->N = malloc(sizeof(oc) * (H->noff[nn] > 0 ? H->noff[nn] : 1));
+#pragma omp parallel for schedule(dynamic, 4) num_threads(H->nthreads)
+    for (int t = 0; t < nn; ++t) {
+        int mt = T->end[t] - T->begin[t];
+        oc *B = H->N + H->noff[t];
+        int col = 0;
+        for (int i = H->nearptr[t]; i < H->nearptr[t + 1]; ++i) {
+            int s = H->nearnodes[i];
+            for (int pos = S->begin[s]; pos < S->end[s]; ++pos, ++col) {
+                long j = S->perm[pos];
+                for (int a = 0; a < mt; ++a) {
+                    long ii = T->perm[T->begin[t] + a];
+                    B[a + (long)col * mt] = okern_entry(&H->K, side_pt(H, 0, ii), side_pt(H, 1, j),
+                                                        ii, j);
+                }
+            }
+        }
+    }
+    /* column offset of block (t, s) inside row block t, indexed like the trial near lists */
+    int ns = S->nnodes;
+    H->tnear_coloff = malloc(sizeof(int) * (H->tnearptr[ns] > 0 ? H->tnearptr[ns] : 1));
+    for (int s = 0; s < ns; ++s)
+        for (int k = H->tnearptr[s]; k < H->tnearptr[s + 1]; ++k) {
+            int t = H->tnearnodes[k];
+            int col = 0;
+            for (int i = H->nearptr[t]; i < H->nearptr[t + 1]; ++i) {
+                int s2 = H->nearnodes[i];
+                if (s2 == s)
+                    break;
+                col += S->end[s2] - S->begin[s2];
+            }
+            H->tnear_coloff[k] = col;
+        }
+}
+
+ohandle *oracle_build(const double *tp, long nt, const double *sp, long ns, int minvalues,
+                      double eta, int kind, int sign, double k, double rmin, const double *mat,
+                      long ldmat, double tol_test, double tol_trial, int maxrank, int sampled,
+                      int nthreads) {
+    ohandle *H = calloc(1, sizeof(ohandle));
+    H->nthreads = nthreads > 0 ? nthreads : 1;
+    H->npts[0] = nt;
+    H->npts[1] = ns;
+    H->pts[0] = malloc(sizeof(double) * 3 * (nt > 0 ? nt : 1));
+    H->pts[1] = malloc(sizeof(double) * 3 * (ns > 0 ? ns : 1));
+    memcpy(H->pts[0], tp, sizeof(double) * 3 * nt);
+    memcpy(H->pts[1], sp, sizeof(double) * 3 * ns);
+    if (kind == OK_MATRIX) {
+        H->mat_copy = malloc(sizeof(double) * 2 * ldmat * ns);
+        memcpy(H->mat_copy, mat, sizeof(double) * 2 * ldmat * ns);
+    }
+    okern K = {kind, sign, k, rmin, H->mat_copy, ldmat};
+    H->K = K;
+    H->eta = eta;
+    H->maxrank = maxrank;
+    H->sampled = sampled;
+    H->tol[0] = tol_test;
+    H->tol[1] = tol_trial;
+    H->tree[0] = oracle_tree_build(tp, nt, minvalues);
+    H->tree[1] = oracle_tree_build(sp, ns, minvalues);
+    pairlist nearp = {0}, farp = {0};
+    dual_visit(H->tree[0], H->tree[1], 0, 0, eta, &nearp, &farp);
+    int nnt = H->tree[0]->nnodes, nns = H->tree[1]->nnodes;
+    pairs_to_csr(nearp.t, nearp.s, nearp.n, nnt, &H->nearptr, &H->nearnodes);
+    pairs_to_csr(farp.t, farp.s, farp.n, nnt, &H->farptr, &H->farnodes);
+    pairs_to_csr(nearp.s, nearp.t, nearp.n, nns, &H->tnearptr, &H->tnearnodes);
+    pairs_to_csr(farp.s, farp.t, farp.n, nns, &H->tfarptr, &H->tfarnodes);
+    free(nearp.t); free(nearp.s); free(farp.t); free(farp.s);
+    build_side(H, 0);
+    if (H->status == 0)
+        build_side(H, 1);
+    if (H->status == 0) {
+        build_couplings(H);
+        build_near(H);
+    }
+    return H;
+}
+
+void oracle_free(ohandle *H) {
+    if (!H)
+        return;
+    for (int s = 0; s < 2; ++s) {
+        free(H->pts[s]); oracle_tree_free(H->tree[s]);
+        free(H->fpptr[s]); free(H->fpidx[s]); free(H->rank[s]); free(H->nrows[s]);
+        free(H->pivptr[s]); free(H->pividx[s]); free(H->pivtmp[s]); free(H->xoff[s]);
+        free(H->X[s]); free(H->cptr[s]);
+    }
+    free(H->mat_copy);
+    free(H->nearptr); free(H->nearnodes); free(H->farptr); free(H->farnodes);
+    free(H->tnearptr); free(H->tnearnodes); free(H->tfarptr); free(H->tfarnodes);
+    free(H->coff); free(H->C); free(H->noff); free(H->ncols); free(H->N);
+    free(H->tnear_coloff);
+    free(H);
+}
+
+/* ---- getters (ctypes) ---- */
+int oracle_status(const ohandle *H, int *side, int *node, int *npiv, int *rank) {
+    *side = H->bad_side;
+    *node = H->bad_node;
+    *npiv = H->bad_npiv;
+    *rank = H->bad_rank;
+    return H->status;
+}
+const otree *oracle_tree(const ohandle *H, int side) { return H->tree[side]; }
+void oracle_partition_sizes(const ohandle *H, long *nnear, long *nfar) {
+    *nnear = H->nearptr[H->tree[0]->nnodes];
+    *nfar = H->farptr[H->tree[0]->nnodes];
+}
+void oracle_partition(const ohandle *H, int *nearptr, int *nearnodes, int *farptr, int *farnodes,
+                      int *tfarptr, int *tfarnodes) {
+    int nt = H->tree[0]->nnodes, ns = H->tree[1]->nnodes;
+    memcpy(nearptr, H->nearptr, sizeof(int) * (nt + 1));
+    memcpy(nearnodes, H->nearnodes, sizeof(int) * H->nearptr[nt]);
+    memcpy(farptr, H->farptr, sizeof(int) * (nt + 1));
+    memcpy(farnodes, H->farnodes, sizeof(int) * H->farptr[nt]);
+    memcpy(tfarptr, H->tfarptr, sizeof(int) * (ns + 1));
+    memcpy(tfarnodes, H->tfarnodes, sizeof(int) * H->tfarptr[ns]);
+}
+int oracle_farpivots_total(const ohandle *H, int side) {
+    return H->fpptr[side][H->tree[side]->nnodes];
+}
+void oracle_farpivots(const ohandle *H, int side, int *ptr, int *idx) {
+    int nn = H->tree[side]->nnodes;
+    memcpy(ptr, H->fpptr[side], sizeof(int) * (nn + 1));
+    memcpy(idx, H->fpidx[side], sizeof(int) * H->fpptr[side][nn]);
+}
+int oracle_pivots_total(const ohandle *H, int side) {
+    return H->pivptr[side][H->tree[side]->nnodes];
+}
+void oracle_pivots(const ohandle *H, int side, int *rank, int *nrows, int *ptr, int *idx) {
+    int nn = H->tree[side]->nnodes;
+    memcpy(rank, H->rank[side], sizeof(int) * nn);
+    memcpy(nrows, H->nrows[side], sizeof(int) * nn);
+    memcpy(ptr, H->pivptr[side], sizeof(int) * (nn + 1));
+    memcpy(idx, H->pividx[side], sizeof(int) * H->pivptr[side][nn]);
+}
+long oracle_x_total(const ohandle *H, int side) { return H->xoff[side][H->tree[side]->nnodes]; }
+void oracle_x(const ohandle *H, int side, long *off, double *X) {
+    int nn = H->tree[side]->nnodes;
+    memcpy(off, H->xoff[side], sizeof(long) * (nn + 1));
+    memcpy(X, H->X[side], sizeof(oc) * H->xoff[side][nn]);
+}
+long oracle_coupling_total(const ohandle *H) { return H->coff[H->farptr[H->tree[0]->nnodes]]; }
+void oracle_couplings(const ohandle *H, long *off, double *C) {
+    long np = H->farptr[H->tree[0]->nnodes];
+    memcpy(off, H->coff, sizeof(long) * (np + 1));
+    memcpy(C, H->C, sizeof(oc) * H->coff[np]);
+}
+long oracle_near_total(const ohandle *H) { return H->noff[H->tree[0]->nnodes]; }
+void oracle_near(const ohandle *H, long *off, int *ncols, double *N) {
+    int nn = H->tree[0]->nnodes;
+    memcpy(off, H->noff, sizeof(long) * (nn + 1));
+    memcpy(ncols, H->ncols, sizeof(int) * nn);
+    memcpy(N, H->N, sizeof(oc) * H->noff[nn]);
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* H^2 matrix-vector product: the five stages and the near field                        */
+/* ------------------------------------------------------------------------------------ */
+
+/* op(A) applied to a vector: mode 0 = A, 1 = transpose(A), 2 = adjoint(A). */
+static inline oc opentry(oc a, int conj) { return conj ? oc_conj(a) : a; }
+
+/* y[0:nr] += op(B) x where B is stored column-major as nrow x ncol with leading dim ld.
+ * trans = 0: y (nrow) += B x (ncol); trans = 1: y (ncol) += B^T x (nrow) (conjugated if conj). */
+static void small_gemv(const oc *B, int nrow, int ncol, long ld, int trans, int conj, const oc *x,
+                       oc *y) {
+    if (!trans) {
+        for (int j = 0; j < ncol; ++j) {
+            oc xj = x[j];
+            for (int i = 0; i < nrow; ++i) {
+                oc t = oc_mul(B[i + (long)j * ld], xj);
+                y[i].re += t.re;
+                y[i].im += t.im;
+            }
+        }
+    } else {
+        for (int j = 0; j < ncol; ++j) {
+            oc acc = y[j];
+            for (int i = 0; i < nrow; ++i) {
+                oc t = oc_mul(opentry(B[i + (long)j * ld], conj), x[i]);
+                acc.re += t.re;
+                acc.im += t.im;
+            }
+            y[j] = acc;
+        }
+    }
+}
+
+/* One right-hand side: x has npts[in] entries, y npts[out] entries (interleaved complex). */
+static void apply_one(const ohandle *H, int mode, const oc *x, oc *y) {
+    int conj = mode == 2;
+    /* forward: trial side aggregates (in = trial), test side disaggregates (out = test).
+     * transpose/adjoint: test side aggregates, trial side disaggregates. */
+    int in = mode == 0 ? 1 : 0, out = 1 - in;
+    const otree *Ti = H->tree[in], *To = H->tree[out];
+    long nin = H->cptr[in][Ti->nnodes], nout = H->cptr[out][To->nnodes];
+    oc *xhat = calloc(nin > 0 ? nin : 1, sizeof(oc));
+    oc *yhat = calloc(nout > 0 ? nout : 1, sizeof(oc));
+    for (long i = 0; i < H->npts[out]; ++i)
+        y[i] = oc_make(0.0, 0.0);
+    /* basis op on the aggregation side: trial basis V = X^T applied as is (forward), test basis
+     * U = X applied as U^T / U^H (transpose / adjoint): both read X with trans = 1 */
+    int cin = in == 1 ? 0 : conj; /* forward: V_s = X_s^T, no conjugation */
+    /* 1. leaf projection (aggregate.jl:1-19) */
+#pragma omp parallel for schedule(dynamic, 8) num_threads(H->nthreads)
+    for (int s = 0; s < Ti->nnodes; ++s) {
+        if (!isleaf(Ti, s) || H->fpptr[in][s + 1] == H->fpptr[in][s])
+            continue;
+        int m = H->nrows[in][s], r = H->rank[in][s];
+        oc *xs = malloc(sizeof(oc) * (m > 0 ? m : 1));
+        for (int a = 0; a < m; ++a)
+            xs[a] = x[Ti->perm[Ti->begin[s] + a]];
+        small_gemv(H->X[in] + H->xoff[in][s], m, r, m, 1, cin, xs, xhat + H->cptr[in][s]);
+        free(xs);
+    }
+    /* 2. upward sweep, levels leaf -> root (aggregate.jl:44-67) */
+    for (int lev = Ti->nlevels - 1; lev >= 0; --lev) {
+#pragma omp parallel for schedule(dynamic, 8) num_threads(H->nthreads)
+        for (int p = Ti->levelptr[lev]; p < Ti->levelptr[lev + 1]; ++p) {
+            if (isleaf(Ti, p) || H->fpptr[in][p + 1] == H->fpptr[in][p])
+                continue;
+            int m = H->nrows[in][p], r = H->rank[in][p];
+            const oc *Xp = H->X[in] + H->xoff[in][p];
+            int row = 0;
+            for (int c = 0; c < Ti->nchildren[p]; ++c) {
+                int ch = Ti->firstchild[p] + c;
+                int kc = H->rank[in][ch];
+                /* transfer of child c: rows [row, row + kc) of X_p */
+                small_gemv(Xp + row, kc, r, m, 1, cin, xhat + H->cptr[in][ch],
+                           xhat + H->cptr[in][p]);
+                row += kc;
+            }
+        }
+    }
+    /* 3. coupling (couple.jl) */
+    if (mode == 0) {
+#pragma omp parallel for schedule(dynamic, 8) num_threads(H->nthreads)
+        for (int t = 0; t < To->nnodes; ++t)
+            for (int i = H->farptr[t]; i < H->farptr[t + 1]; ++i) {
+                int s = H->farnodes[i];
+                small_gemv(H->C + H->coff[i], H->rank[0][t], H->rank[1][s], H->rank[0][t], 0, 0,
+                           xhat + H->cptr[1][s], yhat + H->cptr[0][t]);
+            }
+    } else {
+        /* serial, as _couple_reverse! (couple.jl:52-100) */
+        for (int t = 0; t < Ti->nnodes; ++t)
+            for (int i = H->farptr[t]; i < H->farptr[t + 1]; ++i) {
+                int s = H->farnodes[i];
+                small_gemv(H->C + H->coff[i], H->rank[0][t], H->rank[1][s], H->rank[0][t], 1, conj,
+                           xhat + H->cptr[0][t], yhat + H->cptr[1][s]);
+            }
+    }
+    /* 4. downward sweep, levels root -> leaf (disaggregate.jl:1-23) */
+    int cout = out == 0 ? 0 : conj;
+    for (int lev = 0; lev < To->nlevels; ++lev) {
+#pragma omp parallel for schedule(dynamic, 8) num_threads(H->nthreads)
+        for (int p = To->levelptr[lev]; p < To->levelptr[lev + 1]; ++p) {
+            if (isleaf(To, p) || H->fpptr[out][p + 1] == H->fpptr[out][p])
+                continue;
+            int m = H->nrows[out][p], r = H->rank[out][p];
+            const oc *Xp = H->X[out] + H->xoff[out][p];
+            int row = 0;
+            for (int c = 0; c < To->nchildren[p]; ++c) {
+                int ch = To->firstchild[p] + c;
+                int kc = H->rank[out][ch];
+                if (!cout) {
+                    small_gemv(Xp + row, kc, r, m, 0, 0, yhat + H->cptr[out][p],
+                               yhat + H->cptr[out][ch]);
+                } else {
+                    /* conj(X) applied without transpose */
+                    for (int j = 0; j < r; ++j) {
+                        oc xj = yhat[H->cptr[out][p] + j];
+                        for (int a = 0; a < kc; ++a) {
+                            oc t = oc_mul(oc_conj(Xp[row + a + (long)j * m]), xj);
+                            yhat[H->cptr[out][ch] + a].re += t.re;
+                            yhat[H->cptr[out][ch] + a].im += t.im;
+                        }
+                    }
+                }
+                row += kc;
+            }
+        }
+    }
+    /* 5. leaf expansion (disaggregate.jl:62-80) */
+#pragma omp parallel for schedule(dynamic, 8) num_threads(H->nthreads)
+    for (int t = 0; t < To->nnodes; ++t) {
+        if (!isleaf(To, t) || H->fpptr[out][t + 1] == H->fpptr[out][t])
+            continue;
+        int m = H->nrows[out][t], r = H->rank[out][t];
+        const oc *Xt = H->X[out] + H->xoff[out][t];
+        const oc *yh = yhat + H->cptr[out][t];
+        for (int a = 0; a < m; ++a) {
+            oc acc = oc_make(0.0, 0.0);
+            for (int j = 0; j < r; ++j) {
+                oc t2 = oc_mul(opentry(Xt[a + (long)j * m], cout), yh[j]);
+                acc.re += t2.re;
+                acc.im += t2.im;
+            }
+            long gi = To->perm[To->begin[t] + a];
+            y[gi].re += acc.re;
+            y[gi].im += acc.im;
+        }
+    }
+    /* 6. near field (petrovgalerkinnca.jl:474, :531, :587) */
+    const otree *Tt = H->tree[0], *Ts = H->tree[1];
+    if (mode == 0) {
+#pragma omp parallel for schedule(dynamic, 4) num_threads(H->nthreads)
+        for (int t = 0; t < Tt->nnodes; ++t) {
+            int mt = Tt->end[t] - Tt->begin[t];
+            int nc = H->ncols[t];
+            if (nc == 0)
+                continue;
+            const oc *B = H->N + H->noff[t];
+            oc *acc = calloc(mt, sizeof(oc));
+            int col = 0;
+            for (int i = H->nearptr[t]; i < H->nearptr[t + 1]; ++i) {
+                int s = H->nearnodes[i];
+                for (int pos = Ts->begin[s]; pos < Ts->end[s]; ++pos, ++col) {
+                    oc xj = x[Ts->perm[pos]];
+                    for (int a = 0; a < mt; ++a) {
+                        oc t2 = oc_mul(B[a + (long)col * mt], xj);
+                        acc[a].re += t2.re;
+                        acc[a].im += t2.im;
+                    }
+                }
+            }
+            for (int a = 0; a < mt; ++a) {
+                long gi = Tt->perm[Tt->begin[t] + a];
+                y[gi].re += acc[a].re;
+                y[gi].im += acc[a].im;
+            }
+            free(acc);
+        }
+    } else {
+#pragma omp parallel for schedule(dynamic, 4) num_threads(H->nthreads)
+        for (int s = 0; s < Ts->nnodes; ++s) {
+            int ms = Ts->end[s] - Ts->begin[s];
+            for (int k = H->tnearptr[s]; k < H->tnearptr[s + 1]; ++k) {
+                int t = H->tnearnodes[k];
+                int mt = Tt->end[t] - Tt->begin[t];
+                const oc *B = H->N + H->noff[t] + (long)H->tnear_coloff[k] * mt;
+                for (int j = 0; j < ms; ++j) {
+                    oc acc = oc_make(0.0, 0.0);
+                    for (int a = 0; a < mt; ++a) {
+                        oc t2 = oc_mul(opentry(B[a + (long)j * mt], conj),
+                                       x[Tt->perm[Tt->begin[t] + a]]);
+                        acc.re += t2.re;
+                        acc.im += t2.im;
+                    }
+                    long gj = Ts->perm[Ts->begin[s] + j];
+                    y[gj].re += acc.re;
+                    y[gj].im += acc.im;
+                }
+            }
+        }
+    }
+    free(xhat);
+    free(yhat);
+}
+
+/* y = op(H) x for nrhs columns (column-major, interleaved complex), one column at a time as
+ * LinearMaps applies a vector-only map to a matrix. */
+void oracle_apply(const ohandle *H, int mode, const double *x, long ldx, double *y, long ldy,
+                  long nrhs) {
+    for (long q = 0; q < nrhs; ++q)
+        apply_one(H, mode, (const oc *)(x + 2 * q * ldx), (oc *)(y + 2 * q * ldy));
+}
+
+/* Dense FP64 reference rows: y[r] = sum_j A(rows[r], j) x[j], long double accumulation. */
+void oracle_dense_rows(int kind, int sign, double k, double rmin, const double *mat, long ldmat,
+                       const double *tp, const double *sp, long ns, const long *rows, long nrows,
+                       int transposed, const double *x, double *y, int nthreads) {
+    okern K = {kind, sign, k, rmin, mat, ldmat};
+#pragma omp parallel for schedule(static) num_threads(nthreads > 0 ? nthreads : 1)
+    for (long r = 0; r < nrows; ++r) {
+        long double re = 0.0L, im = 0.0L;
+        long i = rows[r];
+        for (long j = 0; j < ns; ++j) {
+            oc a = transposed ? okern_entry(&K, tp + 3 * j, sp + 3 * i, j, i)
+                              : okern_entry(&K, tp + 3 * i, sp + 3 * j, i, j);
+            long double xr = x[2 * j], xi = x[2 * j + 1];
+            re += (long double)a.re * xr - (long double)a.im * xi;
+            im += (long double)a.re * xi + (long double)a.im * xr;
+        }
+        y[2 * r] = (double)re;
+        y[2 * r + 1] = (double)im;
+    }
+}
