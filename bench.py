@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark: batched bottom-up NCA build + H^2 block products on one B200 (per rank).
+
+Workload (Galerkin, low frequency): 65,536 points uniform on the unit sphere (seeded),
+Helmholtz cis(kr)/(4 pi r) with k = 1.0 (zero on the diagonal), k-means tree minvalues 64,
+batched bottom-up ACA tol 1e-5, maxrank 50. One step = y = H X and y = H^H X for a block of
+16 seeded complex Gaussian right-hand sides (complex FP64). The metric is the product's
+algorithmic HBM bytes (stores read once per block + vectors) per second; the build time is
+reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--precision f64|f32]
+
+With --gpus N > 1 it runs under torchrun, one independent replica per GPU (the path has no
+exchange step); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "nestedcrossapproximation.jl_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "H² build+matvec time & matvec HBM GB/s, chosen vs plain FP64 at rel err 1e-4"
+WORKLOAD = "galerkin-sphere-65536-k1-tol1e-5-16rhs"
+E = 16  # bytes per complex FP64 entry
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="f64", choices=["f64", "f32"])
+    p.add_argument("--npoints", type=int, default=65536)
+    p.add_argument("--nrhs", type=int, default=16)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile-stages", action="store_true", help="print per-stage times to stderr")
+    return p.parse_args()
+
+
+def sphere(n, seed=1234):
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((n, 3))
+    return g / np.linalg.norm(g, axis=1, keepdims=True)
+
+
+def rhs(n, b, seed=99):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((n, b)) + 1j * rng.standard_normal((n, b))
+
+
+def store_entries(info):
+    return (info["near_entries"] + info["coupling_entries"] + info["transfer_entries_test"] +
+            info["transfer_entries_trial"] + info["basis_entries_test"] + info["basis_entries_trial"])
+
+
+def product_bytes(info, b, e=E):
+    """Algorithmic bytes of one product with b right-hand sides: every stored entry once, x read,
+    y read and written, coefficient vectors written and read once."""
+    vec = e * b * (info["ntrial"] + 2 * info["ntest"]) + 2 * e * b * (info["ncoeff_test"] + info["ncoeff_trial"])
+    return e * store_entries(info) + vec
+
+
+def stage_bytes(info, b, e=E):
+    """Algorithmic bytes per launch of the leaf stage (near field + leaf bases + scatter), the
+    dominant kernel: near entries and output-side leaf bases once, x slices, y written."""
+    return e * (info["near_entries"] + info["basis_entries_test"]) + e * b * (
+        info["ntrial"] + info["ntest"] + info["ncoeff_test"])
+
+
+def info_dict(core):
+    i = core.info
+    return {k: getattr(i, k) for k, _ in type(i)._fields_}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_from_profiles():
+    """DRAM bytes per launch of the leaf kernel from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "k_leaves_galerkin_sphere.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (clocks and throttle reasons)."""
+
+    def __init__(self, index):
+        self.proc, self.path = None, os.path.join(ROOT, "gpurun_out", f"clocks_bench_{index}.csv")
+        self.index = index
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem(N, n, device, store_f32):
+    pts = sphere(n)
+    tree = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=64))
+    bt = N.BlockTree(tree, tree)
+    aca = N.ACA(N.FullPivoting(), N.FullPivoting(), N.FNormEstimator(1e-5))
+    comp = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(pts, pts, tree), compressor=aca)
+    t0 = time.perf_counter()
+    core = N.PetrovGalerkinNCACore(N.HelmholtzKernel(1.0), pts, pts, bt, testcompressor=comp, trialcompressor=comp,
+                                   maxrank=50, store_f32=store_f32, device=device)
+    wall = time.perf_counter() - t0
+    return pts, core, wall
+
+
+def dense_rows_error(N, pts, core, ws, X, nrows=64):
+    """Relative error of H X against rows of the dense FP64 matrix evaluated on the device."""
+    rng = np.random.default_rng(7)
+    rows = rng.choice(len(pts), nrows, replace=False)
+    ii = np.repeat(rows, len(pts))
+    jj = np.tile(np.arange(len(pts)), nrows)
+    D = N.seams.entries(N.HelmholtzKernel(1.0), pts, pts, ii, jj, device=core.device).reshape(nrows, len(pts))
+    Y = N.mul(None, ws, X[:, :2])
+    ref = D @ X[:, :2]
+    return float(np.linalg.norm(Y[rows] - ref) / np.linalg.norm(ref))
+
+
+def cpu_baseline_sample(b_sample, nrhs):
+    """The oracle (C restatement, OpenMP on the host cores) on the same workload: its own build,
+    then one forward and one adjoint product on b_sample right-hand sides; the product time is
+    scaled to nrhs (the oracle applies one right-hand side at a time)."""
+    from oracle import oracle as O
+    pts = sphere(65536)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    H = O.H2(pts, pts, O.Kernel(O.KIND_HELMHOLTZ, k=1.0), minvalues=64, tol=1e-5, maxrank=50, nthreads=cores)
+    tb = time.perf_counter() - t0
+    X = rhs(len(pts), b_sample)
+    t0 = time.perf_counter()
+    H.apply(X, 0)
+    H.apply(X, 2)
+    tp = (time.perf_counter() - t0) * nrhs / b_sample
+    info = {"near_entries": sum(a.size for a in H.near), "coupling_entries": sum(a.size for a in H.couplings),
+            "transfer_entries_test": sum(H.X[0][t].size for t in range(H.trees[0].nnodes) if not H.trees[0].isleaf(t)),
+            "transfer_entries_trial": sum(H.X[1][t].size for t in range(H.trees[1].nnodes) if not H.trees[1].isleaf(t)),
+            "basis_entries_test": sum(H.X[0][t].size for t in range(H.trees[0].nnodes) if H.trees[0].isleaf(t)),
+            "basis_entries_trial": sum(H.X[1][t].size for t in range(H.trees[1].nnodes) if H.trees[1].isleaf(t)),
+            "ntest": len(pts), "ntrial": len(pts), "ncoeff_test": int(H.ranks[0].sum()),
+            "ncoeff_trial": int(H.ranks[1].sum())}
+    step_bytes = 2 * product_bytes(info, nrhs)
+    return {"value": step_bytes / tp / 1e9, "unit": "GB/s", "cores": cores, "kind": "port",
+            "sample": f"oracle build ({tb:.1f} s) + one forward and one adjoint product on {b_sample} of the "
+                      f"{nrhs} right-hand sides, time scaled x{nrhs // b_sample}",
+            "build_s": tb, "step_s": tp}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    pts = sphere(args.npoints)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    H = O.H2(pts, pts, O.Kernel(O.KIND_HELMHOLTZ, k=1.0), minvalues=64, tol=1e-5, maxrank=50, nthreads=cores)
+    tb = time.perf_counter() - t0
+    b_sample = 2
+    X = rhs(len(pts), b_sample)
+    for _ in range(args.warmup):
+        H.apply(X, 0)
+        H.apply(X, 2)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        H.apply(X, 0)
+        H.apply(X, 2)
+    el = (time.perf_counter() - t0) * args.nrhs / b_sample
+    info = {"near_entries": sum(a.size for a in H.near), "coupling_entries": sum(a.size for a in H.couplings),
+            "transfer_entries_test": sum(H.X[0][t].size for t in range(H.trees[0].nnodes) if not H.trees[0].isleaf(t)),
+            "transfer_entries_trial": sum(H.X[1][t].size for t in range(H.trees[1].nnodes) if not H.trees[1].isleaf(t)),
+            "basis_entries_test": sum(H.X[0][t].size for t in range(H.trees[0].nnodes) if H.trees[0].isleaf(t)),
+            "basis_entries_trial": sum(H.X[1][t].size for t in range(H.trees[1].nnodes) if H.trees[1].isleaf(t)),
+            "ntest": len(pts), "ntrial": len(pts), "ncoeff_test": int(H.ranks[0].sum()),
+            "ncoeff_trial": int(H.ranks[1].sum())}
+    step_bytes = 2 * product_bytes(info, args.nrhs)
+    value = step_bytes * args.steps / el / 1e9
+    sample = (f"CPU oracle (C restatement, OpenMP, {cores} threads); each step one forward and one adjoint product "
+              f"on {b_sample} of {args.nrhs} right-hand sides, time scaled x{args.nrhs // b_sample}")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "complex-f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "npoints": args.npoints, "nrhs": args.nrhs, "build_s": tb,
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    import nca_b200 as N
+
+    f32 = args.precision == "f32"
+    pts, core, build_wall = build_problem(N, args.npoints, local, f32)
+    info = info_dict(core)
+    n = args.npoints
+    b = args.nrhs
+    ws = N.H2Workspace(core, np.complex64 if f32 else np.complex128, max_nrhs=b)
+    prec = 1 if f32 else 0
+    L = N.lib()
+    X = rhs(n, b)
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(f"cuda:{local}")  # column-major n x b
+    Yd = torch.zeros((b, n), dtype=torch.complex128, device=f"cuda:{local}")
+
+    def step_device():
+        for mode in (0, 2):
+            st = L.nca_apply(ws._h, mode, prec, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Yd.data_ptr()), n, b,
+                             1.0, 0.0, 0.0, 0.0, 1)
+            if st:
+                N._lib.check(st)
+
+    launches = C.c_int32()
+    ws.set_profiling(True)
+    clocks = Clocks(local)
+    clocks.start()
+    t_end = time.perf_counter() + 1.0
+    w = 0
+    while w < max(args.warmup, 3) or time.perf_counter() < t_end:
+        step_device()
+        w += 1
+    stage_sum = {k: 0.0 for k in ("gather", "upward", "coupling", "downward", "leaves")}
+    stage_n = {k: 0 for k in stage_sum}
+    total_launches = 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        for mode in (0, 2):
+            st = L.nca_apply(ws._h, mode, prec, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Yd.data_ptr()), n, b,
+                             1.0, 0.0, 0.0, 0.0, 1)
+            if st:
+                N._lib.check(st)
+            L.nca_workspace_last_launches(ws._h, C.byref(launches))
+            total_launches += launches.value
+            for k, (t, cnt) in ws.stage_times().items():
+                stage_sum[k] += t
+                stage_n[k] += cnt
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    elapsed = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        t = torch.tensor([elapsed], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    step_bytes = 2 * product_bytes(info, b, 8 if f32 else E)
+    value = world * step_bytes * args.steps / elapsed / 1e9
+    # end to end: the same products through the C ABI with pinned host buffers
+    Xh = torch.from_numpy(np.ascontiguousarray(X.T)).pin_memory()
+    Yh = torch.zeros((b, n), dtype=torch.complex128).pin_memory()
+    for _ in range(2):
+        for mode in (0, 2):
+            N._lib.check(L.nca_apply(ws._h, mode, prec, C.c_void_p(Xh.data_ptr()), n, C.c_void_p(Yh.data_ptr()), n,
+                                     b, 1.0, 0.0, 0.0, 0.0, 0))
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for mode in (0, 2):
+            N._lib.check(L.nca_apply(ws._h, mode, prec, C.c_void_p(Xh.data_ptr()), n, C.c_void_p(Yh.data_ptr()), n,
+                                     b, 1.0, 0.0, 0.0, 0.0, 0))
+    e2e_el = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_el], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_el = float(t.item())
+    e2e = {"value": world * step_bytes * args.steps / e2e_el / 1e9, "unit": "GB/s",
+           "h2d_bytes_per_step": 2 * n * b * E, "d2h_bytes_per_step": 2 * n * b * E}
+    err = dense_rows_error(N, pts, core, ws, X) if rank == 0 else None
+    # roofline of the dominant stage (CUDA events on the workspace stream, in the timed region)
+    top = max(stage_sum, key=lambda k: stage_sum[k])
+    peak, peak_kind = peaks()
+    leaves_avg = stage_sum["leaves"] / max(stage_n["leaves"], 1)
+    achieved = stage_bytes(info, b, 8 if f32 else E) / leaves_avg / 1e9 if leaves_avg > 0 else None
+    roofline = {"kernel": "k_leaves (near field + leaf bases + scatter)", "bound": "hbm", "achieved": achieved,
+                "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                "traffic": traffic_from_profiles(), "launch_ms": 1e3 * leaves_avg,
+                "share_of_step": stage_sum["leaves"] / max(sum(stage_sum.values()), 1e-30), "top_stage": top}
+    if args.profile_stages and rank == 0:
+        print(json.dumps({k: (1e3 * stage_sum[k] / args.steps, stage_n[k]) for k in stage_sum}), file=sys.stderr)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(2, b)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex-f32" if f32 else "complex-f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "npoints": n, "nrhs": b, "step": "H X and H^H X (16-column block)",
+                       "l2": "inputs larger than L2 (stores 1.7 GB per product)",
+                       "build_s": build_wall, "build_device_s": info["build_seconds"],
+                       "build_host_s": info["build_seconds_host"], "stored_gb": E * store_entries(info) / 1e9,
+                       "relerr_vs_dense_rows": err, "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": total_launches,
+            "clocks": clk,
+        }), flush=True)
+    del ws, core
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

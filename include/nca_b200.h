@@ -155,6 +155,15 @@ int32_t nca_apply(nca_workspace *ws, int32_t mode, int32_t precision, const void
 int32_t nca_workspace_last_time(const nca_workspace *ws, double *seconds);
 /* Kernel launches of the last nca_apply of this workspace. */
 int32_t nca_workspace_last_launches(const nca_workspace *ws, int32_t *launches);
+/* Which parts the workspace applies: the far field (nested bases, transfers, couplings) and/or
+ * the near field. farmatrix / nearmatrix of the reference (petrovgalerkinnca.jl:344-371). */
+int32_t nca_workspace_set_parts(nca_workspace *ws, int32_t far, int32_t near);
+/* Stage timers (CUDA events around each stage on the workspace stream). With profiling on,
+ * nca_workspace_stage_times returns the device seconds and launches of the last nca_apply per
+ * stage: 0 gather of x, 1 upward sweep, 2 coupling, 3 downward sweep, 4 leaves + near field. */
+int32_t nca_workspace_set_profiling(nca_workspace *ws, int32_t on);
+int32_t nca_workspace_stage_times(const nca_workspace *ws, double *seconds, int32_t *launches,
+                                  int32_t nstages);
 
 /* ---- level seams on caller-given blocks (batchedbottomup.jl:101-244, the CUDA extension's
  *      ext/NestedCrossApproximationCUDAExt/compresslevel.jl:31-137): fully pivoted ACA and

@@ -1,21 +1,31 @@
-// Device kernels of the H^2 matrix-vector product (src/nca/aggregate.jl, couple.jl,
-// disaggregate.jl and the near-field product of src/nca/petrovgalerkinnca.jl:431-589),
-// for a block of b right-hand sides.
+// Device kernel of the H^2 matrix-vector product (src/nca/aggregate.jl, couple.jl,
+// disaggregate.jl and the near-field product of src/nca/petrovgalerkinnca.jl:431-589) for a
+// block of b right-hand sides.
 //
-// Storage per side: one interpolation operator X_p (nrows x rank, column-major) per node;
-// the leaf basis is X (test) or X^T (trial), and the transfer matrices of p's children are
-// the row slices of X_p in child order. Siblings have consecutive node ids, so the children's
-// coefficients form one contiguous slice and every transfer step is a single small GEMM:
-//   upward   xhat_p = op(X_p)^T [xhat_c1; xhat_c2; ...]   (leaf: the gathered x slice)
-//   coupling yhat_t = sum_s S_ts xhat_s        (reverse: yhat_s = sum_t op(S_ts)^T xhat_t)
-//   downward [yhat_c1; ...] += op(X_p) yhat_p
-//   leaves   y_t = op(X_t) yhat_t + sum_s op(N_ts) x_s, written straight to the user layout.
-// Every stage is a gather (the reverse coupling and the transposed near field read the
-// trial-side CSR transposes), so no atomics are used and results are bitwise reproducible.
-// Vectors are laid out point-major with the right-hand sides contiguous: v[i * b + q].
+// Every stage is the same operation: for each output node o (one CTA),
+//     out_o (R x b) = sum over segments  op(M_seg) (R x w_seg) * v_seg (w_seg x b)
+// with every matrix block M_seg contiguous (column-major, leading dimension R) and every vector
+// slice v_seg contiguous (rows of b right-hand sides, v[i * b + q]). The stores keep transposed
+// copies where a product needs them, so each stage reads R x w tiles:
+//   upward   xhat_p = X_p^T [xhat_c1; xhat_c2; ...] (leaf: the gathered x slice)   from XT
+//   coupling yhat_t = sum_s S_ts xhat_s      (reverse: from the transposed couplings CT)
+//   downward [yhat_c1; ...] += X_p yhat_p
+//   leaves   y_t = X_t yhat_t + sum_s N_ts x_s (reverse: from the transposed near blocks NT),
+//            scattered straight into the caller's layout.
+//
+// CTA = 8 consumer warps + 1 producer warp. The producer streams tiles through a 4-stage
+// shared-memory ring with cp.async.bulk (bulk copies completing on a "full" mbarrier); the
+// consumers release stages on an "empty" mbarrier. Complex FP64 tiles go through the FP64
+// tensor-core MMA (mma.m8n8k4.f64) with three real products per complex product
+// (Re = ArBr - AiBi, Im = (Ar+Ai)(Br+Bi) - ArBr - AiBi); complex FP32 tiles use FMA. Output
+// tiles of 8 rows x 8 right-hand sides are spread over the warps; when a node has fewer
+// tiles than warps the columns are split between warps and summed in shared memory. Every
+// wait is bounded: on timeout the CTA records an error, drains its copies (bounded) and
+// returns. Every stage gathers (no atomics), so products are bitwise reproducible.
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "apply_kernels.cuh"
 
@@ -23,278 +33,550 @@ namespace nca {
 
 namespace {
 
-constexpr int NT = 256;
+constexpr int NCONS = 8;              // consumer warps
+constexpr int NT = (NCONS + 1) * 32;  // + one producer warp
+constexpr int NSTAGE = 3;
+constexpr int CAPM = 18432;  // bytes of matrix tile per stage
+constexpr int CAPV = 5120;   // bytes of vector tile per stage
+constexpr int STAGE_BYTES = CAPM + CAPV;
 
-__device__ __forceinline__ double2 ld_c(const double2 *p) { return *p; }
-__device__ __forceinline__ double2 ld_c(const float2 *p) {
-    float2 v = *p;
-    return make_double2(v.x, v.y);
+// Shared-memory strides (in 16-byte elements) that are 2 mod 4: the four lanes of an MMA
+// fragment row then hit four different bank groups.
+__host__ __device__ __forceinline__ int conflict_free(int n) { return n + ((6 - n % 4) % 4); }
+constexpr unsigned kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    for (unsigned it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
 }
 
-template <typename C>
-struct Cx;
-template <>
-struct Cx<double2> {
-    __device__ static double2 zero() { return make_double2(0.0, 0.0); }
-    __device__ static double2 from(double2 v) { return v; }
-    __device__ static double2 fma(double2 a, double2 b, double2 c) {
-        return make_double2(::fma(a.x, b.x, ::fma(-a.y, b.y, c.x)), ::fma(a.x, b.y, ::fma(a.y, b.x, c.y)));
-    }
-};
-template <>
-struct Cx<float2> {
-    __device__ static float2 zero() { return make_float2(0.f, 0.f); }
-    __device__ static float2 from(double2 v) { return make_float2(float(v.x), float(v.y)); }
-    __device__ static float2 fma(float2 a, float2 b, float2 c) {
-        return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
-    }
-};
-
-__device__ __forceinline__ double2 to_d(double2 v) { return v; }
-__device__ __forceinline__ double2 to_d(float2 v) { return make_double2(v.x, v.y); }
-
-template <typename C>
-__device__ __forceinline__ C conj_if(C a, bool c) {
-    if (c) a.y = -a.y;
-    return a;
+// D = A (8x4, row) * B (4x8, col) + D on the FP64 tensor cores.
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
 }
 
-// Shared-memory plan of one block product: output accumulator M x bc (double2), a tile of the
-// matrix (element type C) and a tile of the right operand (C).
-struct Smem {
-    double2 *acc;
-    unsigned char *a;
-    unsigned char *b;
-    int kc;  // columns of the inner dimension per tile
+__device__ __forceinline__ void cfma(float2 &acc, float2 m, float2 x) {
+    acc.x = fmaf(m.x, x.x, fmaf(-m.y, x.y, acc.x));
+    acc.y = fmaf(m.x, x.y, fmaf(m.y, x.x, acc.y));
+}
+
+template <typename S>
+struct Seg {
+    const S *M;
+    const double2 *v;
+    int w;
 };
 
-// acc(row, q) += sum_k opA(row, k) * B(k, q), rows < M, inner < K, q < bc.
-// A (element S, global memory): TRANS ? A[k + row * lda] : A[row + k * lda]; conj if conjA.
-// B (global, double2): B[k * bstride + q].
-template <typename S, typename C, bool TRANS>
-__device__ void block_gemm(const S *A, int64_t lda, int M, int K, bool conjA, const double2 *B,
-                           int bstride, int bc, const Smem &sm) {
-    C *As = reinterpret_cast<C *>(sm.a);
-    C *Bs = reinterpret_cast<C *>(sm.b);
-    const int tid = threadIdx.x;
-    for (int k0 = 0; k0 < K; k0 += sm.kc) {
-        const int kc = min(sm.kc, K - k0);
-        // tile of A as M x kc column-major in smem (opA(row, k0 + kk) at As[row + kk * M])
-        if (!TRANS) {
-            for (int e = tid; e < M * kc; e += NT) {
-                int row = e % M, kk = e / M;
-                As[e] = conj_if(Cx<C>::from(ld_c(A + row + (k0 + kk) * lda)), conjA);
-            }
+template <typename S, int STAGE>
+__device__ __forceinline__ int out_rows(const RowArgs<S> &a, int o) {
+    if (STAGE == STAGE_UP) return a.rank[o];
+    if (STAGE == STAGE_DOWN) return a.nrows[o];
+    if (STAGE == STAGE_COUPLE) return a.rank_out[o];
+    return a.end[o] - a.begin[o];
+}
+
+template <typename S, int STAGE>
+__device__ __forceinline__ int own_segment(const RowArgs<S> &a, int o) {
+    return (STAGE == STAGE_LEAVES && a.X && a.rank[o] > 0) ? 1 : 0;
+}
+
+template <typename S, int STAGE>
+__device__ __forceinline__ int nsegs(const RowArgs<S> &a, int o) {
+    if (STAGE == STAGE_UP || STAGE == STAGE_DOWN) return 1;
+    const int list = a.ptr ? a.ptr[o + 1] - a.ptr[o] : 0;
+    return own_segment<S, STAGE>(a, o) + list;
+}
+
+template <typename S, int STAGE>
+__device__ __forceinline__ Seg<S> segment(const RowArgs<S> &a, int o, int k) {
+    Seg<S> g;
+    if (STAGE == STAGE_UP) {
+        g.M = a.M + a.moff[o];
+        g.w = a.nrows[o];
+        g.v = a.nchildren[o] == 0 ? a.src + int64_t(a.begin[o]) * a.vs : a.coef + a.cptr[a.firstchild[o]] * a.vs;
+    } else if (STAGE == STAGE_DOWN) {
+        g.M = a.M + a.moff[o];
+        g.w = a.rank[o];
+        g.v = a.coef + a.cptr[o] * a.vs;
+    } else if (STAGE == STAGE_COUPLE) {
+        const int e = a.ptr[o] + k;
+        const int other = a.other[e];
+        g.M = a.M + a.moff[e];
+        g.w = a.rank_in[other];
+        g.v = a.src + a.cptr_in[other] * a.vs;
+    } else {
+        const int own = own_segment<S, STAGE>(a, o);
+        if (k < own) {
+            g.M = a.X + a.xoff[o];
+            g.w = a.rank[o];
+            g.v = a.coef + a.cptr[o] * a.vs;
         } else {
-            for (int e = tid; e < M * kc; e += NT) {
-                int kk = e % kc, row = e / kc;
-                As[row + kk * M] = conj_if(Cx<C>::from(ld_c(A + (k0 + kk) + row * lda)), conjA);
+            const int e = a.ptr[o] + k - own;
+            const int other = a.other[e];
+            g.M = a.M + a.moff[e];
+            g.w = a.o_end[other] - a.o_begin[other];
+            g.v = a.src + int64_t(a.o_begin[other]) * a.vs;
+        }
+    }
+    return g;
+}
+
+// Shared control block of one CTA.
+struct Ctl {
+    uint64_t full[NSTAGE];
+    uint64_t empty[NSTAGE];
+    int w[NSTAGE];
+    int abort;
+    int err;
+};
+
+// Per-warp accumulators (MAXT output tiles of 8 x 8): three real products per tile for
+// FP64, complex FMA for FP32.
+template <typename S, int MAXT>
+struct Acc;
+template <int MAXT>
+struct Acc<double2, MAXT> {
+    // with few tiles per warp, two independent sets (even / odd k-steps) double the chains in flight
+    static constexpr int NSET = MAXT <= 2 ? 2 : 1;
+    double c1[NSET][MAXT][2], c2[NSET][MAXT][2], c3[NSET][MAXT][2];
+    __device__ void zero() {
+#pragma unroll
+        for (int p = 0; p < NSET; ++p)
+#pragma unroll
+            for (int u = 0; u < MAXT; ++u)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) c1[p][u][h] = c2[p][u][h] = c3[p][u][h] = 0.0;
+    }
+    __device__ double2 value(int u, int h) const {
+        double r1 = 0.0, r2 = 0.0, r3 = 0.0;
+#pragma unroll
+        for (int p = 0; p < NSET; ++p) {
+            r1 += c1[p][u][h];
+            r2 += c2[p][u][h];
+            r3 += c3[p][u][h];
+        }
+        return make_double2(r1 - r2, r3 - r1 - r2);
+    }
+};
+
+template <int MAXT>
+struct Acc<float2, MAXT> {
+    float2 c[MAXT][2];
+    __device__ void zero() {
+#pragma unroll
+        for (int u = 0; u < MAXT; ++u) c[u][0] = c[u][1] = make_float2(0.f, 0.f);
+    }
+    __device__ double2 value(int u, int h) const { return make_double2(c[u][h].x, c[u][h].y); }
+};
+
+// Output tiles of one consumer warp. The R x bc output is cut into 8 x 8 tiles spread over the
+// 8 consumer warps; when there are fewer tiles than warps, the columns are split into kgroups
+// interleaved groups of k-steps and the groups are summed at the end.
+template <int MAXT>
+struct TileMap {
+    int n, kgroups, mykg;
+    int arow[MAXT];  // output row of this lane's A fragment (or -1 past the block)
+    int bcol[MAXT];  // right-hand side of this lane's B fragment (or -1)
+    int ocol[MAXT];              // first right-hand side of the tile
+    bool reuse[MAXT];            // same A rows as the previous tile
+    __device__ void init(int R, int bc, int warp, int g) {
+        const int MT = (R + 7) >> 3, NTL = (bc + 7) >> 3;
+        const int tiles = MT * NTL;
+        kgroups = tiles >= NCONS ? 1 : NCONS / (tiles > 0 ? tiles : 1);
+        const int ntw = (tiles + NCONS - 1) / NCONS;
+        mykg = kgroups > 1 ? warp / (tiles > 0 ? tiles : 1) : 0;
+        const bool busy = kgroups > 1 ? warp < tiles * kgroups : warp < tiles;
+        n = 0;
+#pragma unroll
+        for (int u = 0; u < MAXT; ++u) {
+            const int t = kgroups > 1 ? warp % (tiles > 0 ? tiles : 1) : warp + u * NCONS;
+            const bool ok = busy && u < (kgroups > 1 ? 1 : ntw) && t < tiles;
+            const int mt = ok ? t % MT : 0, nt = ok ? t / MT : 0;
+            ocol[u] = nt * 8;
+            arow[u] = (ok && mt * 8 + g < R) ? mt * 8 + g : -1;
+            bcol[u] = (ok && nt * 8 + g < bc) ? nt * 8 + g : -1;
+            reuse[u] = u > 0 && ok && kgroups == 1 && ((t - NCONS) % MT) == mt;
+            if (ok) n = u + 1;
+        }
+    }
+};
+
+// One chunk (w columns) of the consumer warp's tiles.
+template <typename S, int MAXT>
+__device__ __forceinline__ void consume(Acc<S, MAXT> &acc, const TileMap<MAXT> &tm, const unsigned char *tile, int w,
+                                        int R, int ldm, int bc, int ldv, int g, int tq, double sgn) {
+    if constexpr (std::is_same<S, double2>::value) {
+        const double2 *Ms = reinterpret_cast<const double2 *>(tile);
+        const double2 *Vs = reinterpret_cast<const double2 *>(tile + CAPM);
+        constexpr int NSET = Acc<S, MAXT>::NSET;
+        const int step = 4 * tm.kgroups;
+        for (int k0 = tm.mykg * 4; k0 < w; k0 += NSET * step) {
+#pragma unroll
+            for (int p = 0; p < NSET; ++p) {
+                const int kk = k0 + p * step + tq;
+                const bool in = kk < w;
+                double2 av = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int u = 0; u < MAXT; ++u) {
+                    if (u >= tm.n) break;
+                    if (!tm.reuse[u]) av = (in && tm.arow[u] >= 0) ? Ms[tm.arow[u] + kk * ldm] : make_double2(0.0, 0.0);
+                    const double2 bv = (in && tm.bcol[u] >= 0) ? Vs[kk * ldv + tm.bcol[u]] : make_double2(0.0, 0.0);
+                    const double ai = sgn < 0.0 ? -av.y : av.y;  // a select, not an FP64 multiply
+                    dmma(acc.c1[p][u][0], acc.c1[p][u][1], av.x, bv.x);
+                    dmma(acc.c2[p][u][0], acc.c2[p][u][1], ai, bv.y);
+                    dmma(acc.c3[p][u][0], acc.c3[p][u][1], av.x + ai, bv.x + bv.y);
+                }
             }
         }
-        for (int e = tid; e < kc * bc; e += NT) {
-            int kk = e / bc, q = e % bc;
-            Bs[e] = Cx<C>::from(B[int64_t(k0 + kk) * bstride + q]);
+    } else {
+        const float2 *Ms = reinterpret_cast<const float2 *>(tile);
+        const double2 *Vs = reinterpret_cast<const double2 *>(tile + CAPM);
+        const float fs = float(sgn);
+        for (int k = tm.mykg; k < w; k += tm.kgroups) {
+#pragma unroll
+            for (int u = 0; u < MAXT; ++u) {
+                if (u >= tm.n) break;
+                const int row = tm.arow[u];
+                float2 m = row >= 0 ? Ms[row + k * ldm] : make_float2(0.f, 0.f);
+                m.y *= fs;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int col = tm.ocol[u] + 2 * tq + h;
+                    const double2 xv = col < bc ? Vs[k * ldv + col] : make_double2(0.0, 0.0);
+                    cfma(acc.c[u][h], m, make_float2(float(xv.x), float(xv.y)));
+                }
+            }
         }
-        __syncthreads();
-        for (int e = tid; e < M * bc; e += NT) {
-            int row = e / bc, q = e % bc;
-            C s = Cx<C>::zero();
-            for (int kk = 0; kk < kc; ++kk) s = Cx<C>::fma(As[row + kk * M], Bs[kk * bc + q], s);
-            double2 d = to_d(s);
-            sm.acc[e].x += d.x;
-            sm.acc[e].y += d.y;
-        }
-        __syncthreads();
     }
-}
-
-__device__ Smem carve(unsigned char *base, int mcap, int bc, int tile_bytes, int elem) {
-    Smem s;
-    s.acc = reinterpret_cast<double2 *>(base);
-    size_t off = sizeof(double2) * size_t(mcap) * bc;
-    s.a = base + off;
-    s.b = s.a + tile_bytes;
-    s.kc = tile_bytes / (elem * (mcap > bc ? mcap : bc));
-    if (s.kc < 1) s.kc = 1;
-    return s;
-}
-
-__device__ void zero_acc(double2 *acc, int n) {
-    for (int e = threadIdx.x; e < n; e += NT) acc[e] = make_double2(0.0, 0.0);
-    __syncthreads();
 }
 
 }  // namespace
 
-size_t apply_smem_bytes(int mcap, int bc, int tile_bytes) {
-    return sizeof(double2) * size_t(mcap) * bc + 2 * size_t(tile_bytes);
+int rows_capacity(int bc) {
+    // at most 8 tiles of 8 x 8 per warp over 8 warps (R * ceil(bc / 8) <= 512); 4 padded complex
+    // FP64 columns must fit one matrix tile; the partial sums (R x bc) must fit the ring
+    const int ntl = (bc + 7) / 8;
+    const int by_tiles = 512 / (ntl > 0 ? ntl : 1);
+    const int by_tile_bytes = CAPM / (4 * 16) - 2;
+    const int by_ring = NSTAGE * STAGE_BYTES / (16 * (bc > 0 ? bc : 1));
+    int cap = by_tiles < by_tile_bytes ? by_tiles : by_tile_bytes;
+    return cap < by_ring ? cap : by_ring;
 }
 
-__global__ void k_gather(const double2 *x, int64_t ldx, const int32_t *perm, int64_t n, int b,
-                         double2 *xt) {
-    int64_t total = n * b;
-    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
-         e += int64_t(gridDim.x) * blockDim.x) {
-        int64_t i = e / b;
-        int q = int(e % b);
-        xt[e] = x[perm[i] + q * ldx];
-    }
-}
+template <typename S, int STAGE, int MAXT>
+__device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *nodes) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ Ctl ctl;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int o = nodes[blockIdx.x];
+    const int R = out_rows<S, STAGE>(a, o);
+    const int bc = a.bc;
+    const int elem = int(sizeof(S));
+    constexpr bool f64 = std::is_same<S, double2>::value;
+    // FP64 tiles are copied column by column into padded shared-memory columns; FP32 tiles in one
+    // piece. Vector rows keep the buffers' padded stride when a pass covers all right-hand sides.
+    const int ldm = f64 ? conflict_free(R) : R;
+    const bool vwhole = bc == a.b;
+    const int ldv = vwhole ? a.vs : conflict_free(bc);
+    int wmax = R > 0 ? CAPM / (ldm * elem) : CAPV;
+    const int wv = CAPV / (ldv * 16);
+    if (wv < wmax) wmax = wv;
+    if (!f64) wmax &= ~3;  // FP32: whole k-steps keep interior chunks 16-byte multiples
+    if (wmax < 4) wmax = 4;
 
-template <typename S, typename C>
-__global__ void __launch_bounds__(NT) k_up(SweepArgs<S> a, const int32_t *nodes, int mcap,
-                                           int tile_bytes) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int p = nodes[blockIdx.x];
-    const int m = a.nrows[p], r = a.rank[p];
-    const double2 *src = a.nchildren[p] == 0 ? a.xt + int64_t(a.begin[p]) * a.b
-                                             : a.coef + a.cptr[a.firstchild[p]] * a.b;
-    double2 *dst = a.coef + a.cptr[p] * a.b;
-    const S *X = a.X + a.xoff[p];
-    for (int q0 = 0; q0 < a.b; q0 += 16) {
-        const int bc = min(16, a.b - q0);
-        Smem sm = carve(smem, mcap, bc, tile_bytes, sizeof(C));
-        zero_acc(sm.acc, r * bc);
-        block_gemm<S, C, true>(X, m, r, m, a.conj, src + q0, a.b, bc, sm);
-        for (int e = threadIdx.x; e < r * bc; e += NT) dst[int64_t(e / bc) * a.b + q0 + e % bc] = sm.acc[e];
-        __syncthreads();
-    }
-}
-
-template <typename S, typename C>
-__global__ void __launch_bounds__(NT) k_down(SweepArgs<S> a, const int32_t *nodes, int mcap,
-                                             int tile_bytes) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int p = nodes[blockIdx.x];
-    const int m = a.nrows[p], r = a.rank[p];
-    const double2 *src = a.coef + a.cptr[p] * a.b;
-    double2 *dst = a.coef + a.cptr[a.firstchild[p]] * a.b;
-    const S *X = a.X + a.xoff[p];
-    for (int q0 = 0; q0 < a.b; q0 += 16) {
-        const int bc = min(16, a.b - q0);
-        Smem sm = carve(smem, mcap, bc, tile_bytes, sizeof(C));
-        for (int e = threadIdx.x; e < m * bc; e += NT) sm.acc[e] = dst[int64_t(e / bc) * a.b + q0 + e % bc];
-        __syncthreads();
-        block_gemm<S, C, false>(X, m, m, r, a.conj, src + q0, a.b, bc, sm);
-        for (int e = threadIdx.x; e < m * bc; e += NT) dst[int64_t(e / bc) * a.b + q0 + e % bc] = sm.acc[e];
-        __syncthreads();
-    }
-}
-
-template <typename S, typename C>
-__global__ void __launch_bounds__(NT) k_couple(CoupleArgs<S> a, const int32_t *nodes, int mcap,
-                                               int tile_bytes) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int o = nodes[blockIdx.x];  // output node (test node forward, trial node reverse)
-    const int ko = a.rank_out[o];
-    double2 *dst = a.yhat + a.cptr_out[o] * a.b;
-    for (int q0 = 0; q0 < a.b; q0 += 16) {
-        const int bc = min(16, a.b - q0);
-        Smem sm = carve(smem, mcap, bc, tile_bytes, sizeof(C));
-        zero_acc(sm.acc, ko * bc);
-        for (int k = a.ptr[o]; k < a.ptr[o + 1]; ++k) {
-            const int pair = a.pairs ? a.pairs[k] : k;
-            const int other = a.other[k];
-            const int ki = a.rank_in[other];
-            if (ki == 0) continue;
-            const S *Cm = a.C + a.coff[pair];
-            const double2 *src = a.xhat + a.cptr_in[other] * a.b + q0;
-            if (!a.reverse)
-                block_gemm<S, C, false>(Cm, ko, ko, ki, false, src, a.b, bc, sm);
-            else
-                block_gemm<S, C, true>(Cm, ki, ko, ki, a.conj, src, a.b, bc, sm);
+    if (tid == 0) {
+        for (int s = 0; s < NSTAGE; ++s) {
+            mbar_init(&ctl.full[s], 1);
+            mbar_init(&ctl.empty[s], NCONS);
         }
-        for (int e = threadIdx.x; e < ko * bc; e += NT) dst[int64_t(e / bc) * a.b + q0 + e % bc] = sm.acc[e];
-        __syncthreads();
+        ctl.abort = 0;
+        ctl.err = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-}
+    __syncthreads();
 
-template <typename S, typename C>
-__global__ void __launch_bounds__(NT) k_leaves(LeafArgs<S> a, const int32_t *leaves, int mcap,
-                                               int tile_bytes) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int t = leaves[blockIdx.x];
-    const int mt = a.end[t] - a.begin[t];
-    const int r = a.rank[t];
-    for (int q0 = 0; q0 < a.b; q0 += 16) {
-        const int bc = min(16, a.b - q0);
-        Smem sm = carve(smem, mcap, bc, tile_bytes, sizeof(C));
-        zero_acc(sm.acc, mt * bc);
-        if (r > 0 && a.nrows[t] == mt)
-            block_gemm<S, C, false>(a.X + a.xoff[t], mt, mt, r, a.conj, a.yhat + a.cptr[t] * a.b + q0,
-                                    a.b, bc, sm);
-        for (int k = a.nptr[t]; k < a.nptr[t + 1]; ++k) {
-            const int o = a.nnodes[k];
-            const int mo = a.o_end[o] - a.o_begin[o];
-            const double2 *src = a.xt + int64_t(a.o_begin[o]) * a.b + q0;
-            if (!a.reverse) {
-                // forward: N_ts is mt x ms at column offset coloff of t's row block
-                const S *Nm = a.N + a.noff[t] + int64_t(a.coloff[k]) * mt;
-                block_gemm<S, C, false>(Nm, mt, mt, mo, false, src, a.b, bc, sm);
-            } else {
-                // transposed: N_{o,t} is mo x mt at column offset coloff of o's row block
-                const S *Nm = a.N + a.noff[o] + int64_t(a.coloff[k]) * mo;
-                block_gemm<S, C, true>(Nm, mo, mt, mo, a.conj, src, a.b, bc, sm);
+    const int g = lane >> 2, tq = lane & 3;
+    volatile int *abort_flag = &ctl.abort;
+    Acc<S, MAXT> acc;
+    acc.zero();
+    TileMap<MAXT> tm;
+    tm.init(R, bc, warp < NCONS ? warp : 0, g);
+    const double sgn = a.conj ? -1.0 : 1.0;
+
+    if (warp == NCONS) {
+        // ---------------- producer warp ----------------
+        if (lane == 0) {
+            const int nseg = nsegs<S, STAGE>(a, o);
+            int k = 0, c0 = 0;
+            // the next segment's descriptor is loaded one segment ahead, so the dependent index
+            // loads (CSR entry -> partner node -> its range) overlap the current segment's copies
+            Seg<S> gs, gnext;
+            gs.w = 0;
+            gnext.w = 0;
+            if (nseg > 0) gs = segment<S, STAGE>(a, o, 0);
+            if (nseg > 1) gnext = segment<S, STAGE>(a, o, 1);
+            for (int chunk = 0;; ++chunk) {
+                const int s = chunk % NSTAGE;
+                if (chunk >= NSTAGE && !mbar_wait_bounded(&ctl.empty[s], ((chunk / NSTAGE) - 1) & 1)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                if (*abort_flag) break;
+                while (k < nseg && c0 >= gs.w) {
+                    ++k;
+                    c0 = 0;
+                    gs = gnext;
+                    if (k + 1 < nseg) gnext = segment<S, STAGE>(a, o, k + 1);
+                }
+                if (k >= nseg) {
+                    ctl.w[s] = -1;
+                    mbar_arrive(&ctl.full[s]);
+                    break;
+                }
+                int w = gs.w - c0;
+                if (w > wmax) w = wmax;
+                const S *msrc = gs.M + int64_t(c0) * R;
+                const double2 *vsrc = gs.v + int64_t(c0) * a.vs + a.q0;
+                c0 += w;
+                const uint32_t mbytes = (uint32_t(R) * uint32_t(w) * uint32_t(elem) + 15u) & ~15u;
+                const uint32_t vrow = uint32_t(bc) * 16u;
+                const uint32_t vbytes = vwhole ? uint32_t(w) * uint32_t(a.vs) * 16u : vrow * uint32_t(w);
+                unsigned char *tile = smem + s * STAGE_BYTES;
+                if (((reinterpret_cast<uintptr_t>(msrc) | reinterpret_cast<uintptr_t>(vsrc)) & 15u) != 0) {
+                    ctl.err = 1;  // never issue an unaligned bulk copy: skip this chunk
+                    ctl.w[s] = 0;
+                    mbar_arrive(&ctl.full[s]);
+                    continue;
+                }
+                ctl.w[s] = w;
+                if (f64) {
+                    const uint32_t col = uint32_t(R) * 16u;
+                    mbar_expect_tx(&ctl.full[s], col * uint32_t(w) + vbytes);
+                    for (int j = 0; j < w; ++j)
+                        bulk_g2s(tile + j * ldm * 16, msrc + int64_t(j) * R, col, &ctl.full[s]);
+                } else {
+                    mbar_expect_tx(&ctl.full[s], mbytes + vbytes);
+                    if (mbytes) bulk_g2s(tile, msrc, mbytes, &ctl.full[s]);
+                }
+                if (vwhole) {
+                    bulk_g2s(tile + CAPM, vsrc, vbytes, &ctl.full[s]);
+                } else {
+                    for (int j = 0; j < w; ++j)
+                        bulk_g2s(tile + CAPM + j * ldv * 16, vsrc + int64_t(j) * a.vs, vrow, &ctl.full[s]);
+                }
             }
         }
-        const double2 al = a.alpha, be = a.beta;
-        const bool usebeta = be.x != 0.0 || be.y != 0.0;
-        for (int e = threadIdx.x; e < mt * bc; e += NT) {
-            const int i = e / bc, q = q0 + e % bc;
-            double2 v = sm.acc[e];
-            double2 out = make_double2(al.x * v.x - al.y * v.y, al.x * v.y + al.y * v.x);
-            double2 *yp = a.y + a.perm[a.begin[t] + i] + int64_t(q) * a.ldy;
-            if (usebeta) {
-                double2 yo = *yp;
-                out.x += be.x * yo.x - be.y * yo.y;
-                out.y += be.x * yo.y + be.y * yo.x;
+        __syncwarp();
+    } else {
+        // ---------------- consumer warps ----------------
+        for (int chunk = 0;; ++chunk) {
+            const int s = chunk % NSTAGE;
+            if (!mbar_wait_bounded(&ctl.full[s], (chunk / NSTAGE) & 1)) {
+                *abort_flag = 1;
+                break;
+            }
+            const int w = ctl.w[s];
+            if (w < 0 || *abort_flag) break;
+            if (tm.n > 0) consume<S, MAXT>(acc, tm, smem + s * STAGE_BYTES, w, R, ldm, bc, ldv, g, tq, sgn);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ctl.empty[s]);
+        }
+    }
+    __syncthreads();  // every role is done with the ring
+    const bool aborted = *abort_flag != 0;
+    double2 *red = reinterpret_cast<double2 *>(smem);
+    if (!aborted && warp < NCONS) {
+#pragma unroll
+        for (int u = 0; u < MAXT; ++u) {
+            if (u >= tm.n) break;
+            const int row = tm.arow[u];  // C fragment rows equal the A fragment rows (g)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int col = tm.ocol[u] + 2 * tq + h;
+                if (row >= 0 && col < bc) red[(tm.mykg * R + row) * bc + col] = acc.value(u, h);
+            }
+        }
+    }
+    __syncthreads();  // partial sums visible
+    if (aborted) {
+        // a wait gave up: wait (bounded) for copies that may still land in the ring, then leave
+        if (tid == 0) {
+            for (int s = 0; s < NSTAGE; ++s) {
+                mbar_wait_bounded(&ctl.full[s], 0);
+                mbar_wait_bounded(&ctl.full[s], 1);
+            }
+            atomicCAS(a.error, 0, 2);
+        }
+        return;
+    }
+    if (tid == 0 && ctl.err) atomicCAS(a.error, 0, ctl.err);
+    for (int e = tid; e < R * bc; e += NT) {
+        // coefficients: right-hand sides fastest (contiguous rows); y: rows fastest (the caller's columns)
+        const int i = STAGE == STAGE_LEAVES ? e % R : e / bc;
+        const int qq = STAGE == STAGE_LEAVES ? e / R : e % bc;
+        double2 v = red[i * bc + qq];
+        for (int kg = 1; kg < tm.kgroups; ++kg) {
+            const double2 p = red[(kg * R + i) * bc + qq];
+            v.x += p.x;
+            v.y += p.y;
+        }
+        const int col = a.q0 + qq;
+        if (STAGE == STAGE_UP) {
+            a.coef[(a.cptr[o] + i) * a.vs + col] = v;
+        } else if (STAGE == STAGE_COUPLE) {
+            a.dst[(a.cptr_out[o] + i) * a.vs + col] = v;
+        } else if (STAGE == STAGE_DOWN) {
+            double2 *d = a.coef + (a.cptr[a.firstchild[o]] + i) * a.vs + col;
+            const double2 old = *d;
+            *d = make_double2(old.x + v.x, old.y + v.y);
+        } else {
+            double2 *yp = a.y + a.perm[a.begin[o] + i] + int64_t(col) * a.ldy;
+            double2 out = make_double2(a.alpha.x * v.x - a.alpha.y * v.y, a.alpha.x * v.y + a.alpha.y * v.x);
+            if (a.usebeta) {
+                const double2 yo = *yp;
+                out.x += a.beta.x * yo.x - a.beta.y * yo.y;
+                out.y += a.beta.x * yo.y + a.beta.y * yo.x;
             }
             *yp = out;
         }
-        __syncthreads();
     }
 }
 
+// One kernel symbol per stage (the profiler and the launch list name them apart); MAXT is the
+// number of 8 x 8 output tiles a consumer warp keeps in registers.
+template <typename S, int MAXT>
+__global__ void __launch_bounds__(NT, MAXT <= 2 ? 3 : 1) k_rows_up(RowArgs<S> a, const int32_t *nodes) {
+    rows_body<S, STAGE_UP, MAXT>(a, nodes);
+}
+template <typename S, int MAXT>
+__global__ void __launch_bounds__(NT, MAXT <= 2 ? 3 : 1) k_rows_couple(RowArgs<S> a, const int32_t *nodes) {
+    rows_body<S, STAGE_COUPLE, MAXT>(a, nodes);
+}
+template <typename S, int MAXT>
+__global__ void __launch_bounds__(NT, MAXT <= 2 ? 3 : 1) k_rows_down(RowArgs<S> a, const int32_t *nodes) {
+    rows_body<S, STAGE_DOWN, MAXT>(a, nodes);
+}
+template <typename S, int MAXT>
+__global__ void __launch_bounds__(NT, MAXT <= 2 ? 3 : 1) k_rows_leaves(RowArgs<S> a, const int32_t *nodes) {
+    rows_body<S, STAGE_LEAVES, MAXT>(a, nodes);
+}
+
+size_t rows_smem_bytes() { return size_t(NSTAGE) * STAGE_BYTES; }
+
+__global__ void k_gather(const double2 *x, int64_t ldx, const int32_t *perm, int64_t n, int b, int vs,
+                         double2 *xt) {
+    const int64_t total = n * b;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+         e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = e / b;
+        const int q = int(e % b);
+        xt[i * vs + q] = x[perm[i] + q * ldx];
+    }
+}
+
+int vector_stride(int b) { return conflict_free(b); }
+
 namespace {
-// The attribute is per device and per kernel; setting it costs far less than a launch.
-template <typename K>
-void raise_smem(K kernel, size_t bytes) {
-    if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+template <typename S, int MAXT>
+void launch_maxt(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
+    const size_t sm = rows_smem_bytes();
+    switch (a.stage) {
+    case STAGE_UP:
+        cudaFuncSetAttribute(k_rows_up<S, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        k_rows_up<S, MAXT><<<count, NT, sm, s>>>(a, nodes);
+        break;
+    case STAGE_COUPLE:
+        cudaFuncSetAttribute(k_rows_couple<S, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        k_rows_couple<S, MAXT><<<count, NT, sm, s>>>(a, nodes);
+        break;
+    case STAGE_DOWN:
+        cudaFuncSetAttribute(k_rows_down<S, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        k_rows_down<S, MAXT><<<count, NT, sm, s>>>(a, nodes);
+        break;
+    default:
+        cudaFuncSetAttribute(k_rows_leaves<S, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        k_rows_leaves<S, MAXT><<<count, NT, sm, s>>>(a, nodes);
+    }
 }
 }  // namespace
 
 template <typename S>
-void launch_up(const SweepArgs<S> &a, const int32_t *nodes, int count, int mcap, int tile, cudaStream_t s) {
-    size_t sm = apply_smem_bytes(mcap, a.b < 16 ? a.b : 16, tile);
-    raise_smem(k_up<S, S>, sm);
-    k_up<S, S><<<count, NT, sm, s>>>(a, nodes, mcap, tile);
-}
-template <typename S>
-void launch_down(const SweepArgs<S> &a, const int32_t *nodes, int count, int mcap, int tile, cudaStream_t s) {
-    size_t sm = apply_smem_bytes(mcap, a.b < 16 ? a.b : 16, tile);
-    raise_smem(k_down<S, S>, sm);
-    k_down<S, S><<<count, NT, sm, s>>>(a, nodes, mcap, tile);
-}
-template <typename S>
-void launch_couple(const CoupleArgs<S> &a, const int32_t *nodes, int count, int mcap, int tile, cudaStream_t s) {
-    size_t sm = apply_smem_bytes(mcap, a.b < 16 ? a.b : 16, tile);
-    raise_smem(k_couple<S, S>, sm);
-    k_couple<S, S><<<count, NT, sm, s>>>(a, nodes, mcap, tile);
-}
-template <typename S>
-void launch_leaves(const LeafArgs<S> &a, const int32_t *nodes, int count, int mcap, int tile, cudaStream_t s) {
-    size_t sm = apply_smem_bytes(mcap, a.b < 16 ? a.b : 16, tile);
-    raise_smem(k_leaves<S, S>, sm);
-    k_leaves<S, S><<<count, NT, sm, s>>>(a, nodes, mcap, tile);
+void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
+    if (count <= 0) return;
+    const int tiles = ((a.maxrows + 7) / 8) * ((a.bc + 7) / 8);
+    const int per_warp = (tiles + NCONS - 1) / NCONS;
+    if (per_warp <= 2)
+        launch_maxt<S, 2>(a, nodes, count, s);
+    else if (per_warp <= 4)
+        launch_maxt<S, 4>(a, nodes, count, s);
+    else
+        launch_maxt<S, 8>(a, nodes, count, s);
 }
 
-template void launch_up<double2>(const SweepArgs<double2> &, const int32_t *, int, int, int, cudaStream_t);
-template void launch_up<float2>(const SweepArgs<float2> &, const int32_t *, int, int, int, cudaStream_t);
-template void launch_down<double2>(const SweepArgs<double2> &, const int32_t *, int, int, int, cudaStream_t);
-template void launch_down<float2>(const SweepArgs<float2> &, const int32_t *, int, int, int, cudaStream_t);
-template void launch_couple<double2>(const CoupleArgs<double2> &, const int32_t *, int, int, int, cudaStream_t);
-template void launch_couple<float2>(const CoupleArgs<float2> &, const int32_t *, int, int, int, cudaStream_t);
-template void launch_leaves<double2>(const LeafArgs<double2> &, const int32_t *, int, int, int, cudaStream_t);
-template void launch_leaves<float2>(const LeafArgs<float2> &, const int32_t *, int, int, int, cudaStream_t);
+template void launch_rows<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
+template void launch_rows<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+
+namespace {
+template <typename S>
+__global__ void k_transpose_blocks(const S *in, const int64_t *inoff, const int32_t *rows, const int32_t *cols,
+                                   const int64_t *outoff, int64_t nblocks, S *out) {
+    for (int64_t blk = blockIdx.x; blk < nblocks; blk += gridDim.x) {
+        const int R = rows[blk], Cc = cols[blk];
+        const S *src = in + inoff[blk];
+        S *dst = out + outoff[blk];
+        for (int e = threadIdx.x; e < R * Cc; e += blockDim.x) {
+            const int i = e % R, j = e / R;
+            dst[j + int64_t(i) * Cc] = src[e];
+        }
+    }
+}
+}  // namespace
+
+template <typename S>
+void launch_transpose_blocks(const S *in, const int64_t *inoff, const int32_t *rows, const int32_t *cols,
+                             const int64_t *outoff, int64_t nblocks, S *out, cudaStream_t s) {
+    if (nblocks <= 0) return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = int(nblocks < int64_t(sms) * 16 ? nblocks : int64_t(sms) * 16);
+    k_transpose_blocks<S><<<grid, 256, 0, s>>>(in, inoff, rows, cols, outoff, nblocks, out);
+}
+template void launch_transpose_blocks<double2>(const double2 *, const int64_t *, const int32_t *, const int32_t *,
+                                               const int64_t *, int64_t, double2 *, cudaStream_t);
+template void launch_transpose_blocks<float2>(const float2 *, const int64_t *, const int32_t *, const int32_t *,
+                                              const int64_t *, int64_t, float2 *, cudaStream_t);
 
 }  // namespace nca

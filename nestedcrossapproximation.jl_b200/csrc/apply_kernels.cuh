@@ -1,4 +1,4 @@
-// Argument blocks of the H^2 product kernels.
+// Argument block of the H^2 product kernel (one kernel for every stage).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -7,64 +7,57 @@
 
 namespace nca {
 
-// Upward / downward sweep over one side's interpolation operators.
-template <typename S>
-struct SweepArgs {
-    const int32_t *begin, *firstchild, *nchildren, *rank, *nrows;
-    const int64_t *xoff, *cptr;
-    const S *X;
-    const double2 *xt;  // tree-ordered input (upward sweep at the leaves)
-    double2 *coef;      // xhat (upward) or yhat (downward)
-    int b;
-    bool conj;
-};
+enum { STAGE_UP = 0, STAGE_COUPLE = 1, STAGE_DOWN = 2, STAGE_LEAVES = 3 };
 
-// Coupling stage: forward gathers over the test node's far list, reverse over the trial
-// node's transposed list (pairs[] maps it to the coupling block).
+// out_o = sum over segments op(M_seg) v_seg for every output node o of a launch.
+//   STAGE_UP:     o a node of the input side; one segment XT_o (rank x nrows) times the gathered
+//                 input slice (leaf) or the children's xhat; writes xhat_o.
+//   STAGE_COUPLE: o a node of the output side; segments over its far list (CSR ptr/other),
+//                 blocks M + moff[e] (rank_out x rank_in), vectors xhat of the partner; writes yhat_o.
+//   STAGE_DOWN:   o a node of the output side; one segment X_o (nrows x rank) times yhat_o, added
+//                 to the children's yhat.
+//   STAGE_LEAVES: o a leaf of the output side; segments X_o yhat_o (if ranked) and the near
+//                 blocks M + moff[e] times the partner's input slice; scattered into y.
 template <typename S>
-struct CoupleArgs {
-    const int32_t *ptr, *other, *pairs;
-    const int32_t *rank_out, *rank_in;
-    const int64_t *cptr_out, *cptr_in, *coff;
-    const S *C;
-    const double2 *xhat;
-    double2 *yhat;
-    int b;
-    bool reverse, conj;
-};
-
-// Leaf stage: op(X_t) yhat_t plus the near field, scattered to the caller's layout.
-template <typename S>
-struct LeafArgs {
-    const int32_t *perm, *begin, *end, *rank, *nrows;
-    const int64_t *xoff, *cptr;
+struct RowArgs {
+    int stage;
+    const int32_t *begin, *end, *firstchild, *nchildren, *rank, *nrows, *perm;
+    const int64_t *cptr;
+    const S *M;
+    const int64_t *moff;
     const S *X;
-    const double2 *yhat;
-    const int32_t *nptr, *nnodes, *coloff;  // near lists of the output leaves
-    const int32_t *o_begin, *o_end;         // the other side's nodes (input points)
-    const int64_t *noff;                    // near row-block offsets (test nodes)
-    const S *N;
-    const double2 *xt;  // tree-ordered input
+    const int64_t *xoff;
+    const int32_t *ptr, *other;
+    const int32_t *rank_in, *rank_out;
+    const int64_t *cptr_in, *cptr_out;
+    const int32_t *o_begin, *o_end;
+    const double2 *src;
+    double2 *coef;
+    double2 *dst;
     double2 *y;
     int64_t ldy;
     double2 alpha, beta;
-    int b;
-    bool reverse, conj;
+    int usebeta;
+    int b, bc, q0;
+    int vs;           // row stride of the vector buffers (>= b)
+    int conj;
+    int maxrows;      // largest output block of the launch (picks the register tile)
+    int32_t *error;   // 1: misaligned copy skipped, 2: a bounded wait gave up
 };
 
-size_t apply_smem_bytes(int mcap, int bc, int tile_bytes);
+size_t rows_smem_bytes();
+int rows_capacity(int bc);  // largest output block one CTA computes for bc right-hand sides
 
-__global__ void k_gather(const double2 *x, int64_t ldx, const int32_t *perm, int64_t n, int b,
+__global__ void k_gather(const double2 *x, int64_t ldx, const int32_t *perm, int64_t n, int b, int vs,
                          double2 *xt);
+int vector_stride(int b);  // row stride of the internal vector buffers for b right-hand sides
 
-// Host launchers (one per stage); each raises the kernel's dynamic shared-memory limit once.
 template <typename S>
-void launch_up(const SweepArgs<S> &a, const int32_t *nodes, int count, int mcap, int tile, cudaStream_t s);
+void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
+
+// out block e = (in block e)^T for R_e x C_e column-major blocks.
 template <typename S>
-void launch_down(const SweepArgs<S> &a, const int32_t *nodes, int count, int mcap, int tile, cudaStream_t s);
-template <typename S>
-void launch_couple(const CoupleArgs<S> &a, const int32_t *nodes, int count, int mcap, int tile, cudaStream_t s);
-template <typename S>
-void launch_leaves(const LeafArgs<S> &a, const int32_t *nodes, int count, int mcap, int tile, cudaStream_t s);
+void launch_transpose_blocks(const S *in, const int64_t *inoff, const int32_t *rows, const int32_t *cols,
+                             const int64_t *outoff, int64_t nblocks, S *out, cudaStream_t s);
 
 }  // namespace nca

@@ -481,9 +481,7 @@ __global__ void __launch_bounds__(256) k_near(NearArgs a) {
         int t = a.pair_t[pair], s = a.pair_s[pair];
         int tb = a.t_begin[t], mt = a.t_end[t] - tb;
         int sb = a.s_begin[s], ms = a.s_end[s] - sb;
-        int64_t off = a.noff[t] + int64_t(a.coloff[pair]) * mt;
-        double2 *N = a.N + off;
-        float2 *N32 = a.N32 ? a.N32 + off : nullptr;
+        double2 *N = a.N + a.poff[pair];
         for (int e = threadIdx.x; e < mt * ms; e += blockDim.x) {
             int i = e % mt, j = e / mt;
             int64_t gi = a.t_perm[tb + i], gj = a.s_perm[sb + j];
@@ -491,7 +489,6 @@ __global__ void __launch_bounds__(256) k_near(NearArgs a) {
             const double *y = a.trial_pts + 3 * gj;
             double2 v = kernel_entry(a.K, x[0], x[1], x[2], y[0], y[1], y[2], gi, gj);
             N[e] = v;
-            if (N32) N32[e] = make_float2(float(v.x), float(v.y));
         }
     }
 }

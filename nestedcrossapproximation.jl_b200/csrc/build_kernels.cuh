@@ -46,12 +46,11 @@ __global__ void k_couplings(CouplingArgs a);
 struct NearArgs {
     KernelParams K;
     const double *test_pts, *trial_pts;
-    const int32_t *pair_t, *pair_s, *coloff;
+    const int32_t *pair_t, *pair_s;
     const int32_t *t_perm, *t_begin, *t_end, *s_perm, *s_begin, *s_end;
-    const int64_t *noff;
+    const int64_t *poff;  // block offset of each near pair
     int64_t npairs;
     double2 *N;
-    float2 *N32;
 };
 __global__ void k_near(NearArgs a);
 

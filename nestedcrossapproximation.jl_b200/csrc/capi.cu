@@ -117,8 +117,8 @@ struct DevSide {
     DBuf<int32_t> fpptr, fpidx;
     DBuf<int32_t> rank, nrows, piv;
     DBuf<int64_t> xoff, cptr;
-    DBuf<double2> X;
-    DBuf<float2> X32;
+    DBuf<double2> X, XT;  // interpolation operators and their transposes (same padded offsets)
+    DBuf<float2> X32, XT32;
     std::vector<int32_t> h_fpptr, h_fpidx, h_rank, h_nrows, h_piv;
     std::vector<int64_t> h_xoff, h_cptr;
     LevelLists up, down;
@@ -137,18 +137,21 @@ struct nca_core {
     DevSide side[2];
     // couplings in test-node CSR order
     DBuf<int32_t> farptr, farnodes, tfarptr, tfarnodes, tfarpair;
-    DBuf<int64_t> coff;
-    DBuf<double2> C;
-    DBuf<float2> C32;
-    std::vector<int64_t> h_coff;
+    // padded block offsets: S_ts per test-CSR pair (cfoff), S_ts^T per trial-CSR entry (ctoff)
+    DBuf<int64_t> cfoff, ctoff;
+    DBuf<double2> C, CT;
+    DBuf<float2> C32, CT32;
+    std::vector<int64_t> h_cfoff;
     DBuf<int32_t> couple_fwd, couple_rev;
     int n_couple_fwd = 0, n_couple_rev = 0;
     // near field: one row block per test node
-    DBuf<int32_t> nearptr, nearnodes, near_coloff, tnearptr, tnearnodes, tnear_coloff;
-    DBuf<int64_t> noff;
-    DBuf<double2> N;
-    DBuf<float2> N32;
-    std::vector<int64_t> h_noff;
+    DBuf<int32_t> nearptr, nearnodes, tnearptr, tnearnodes;
+    // padded block offsets: N_ts per test-CSR near pair (nfoff), N_ts^T per trial-CSR entry (ntoff)
+    DBuf<int64_t> nfoff, ntoff;
+    DBuf<double2> N, NT;
+    DBuf<float2> N32, NT32;
+    std::vector<int64_t> h_nfoff;
+    std::vector<int64_t> h_noff;  // compact row-block offsets per test node (exports)
     std::vector<int32_t> h_ncols;
     nca_core_info info{};
 };
@@ -160,14 +163,24 @@ struct nca_workspace {
     int max_nrhs = 0;
     DBuf<double2> xt, xhat, yhat, xstage, ystage;
     std::atomic<bool> busy{false};
+    DBuf<int32_t> error;
+    int32_t *error_host = nullptr;  // pinned
     double last_seconds = 0.0;
     int last_launches = 0;
+    bool far = true, near = true;
+    bool profiling = false;
+    cudaEvent_t stage_ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    double stage_seconds[5] = {0, 0, 0, 0, 0};
+    int stage_launches[5] = {0, 0, 0, 0, 0};
 };
 
 namespace {
 
-constexpr int kApplyTile = 24 * 1024;  // bytes per operand tile in the product kernels
 constexpr int kMaxSmem = 227 * 1024;
+
+// Block sizes rounded up to an even number of entries: every block then starts on a 32-byte
+// (FP64) or 16-byte (FP32) boundary, as the bulk copies of the product require.
+inline int64_t pad2(int64_t n) { return (n + 1) & ~int64_t(1); }
 
 void set_kernel_params(nca_core *c, const nca_kernel_desc *k, int64_t ntest, int64_t ntrial,
                        cudaStream_t s) {
@@ -216,7 +229,7 @@ void plan_side(DevSide &d, const nca::Tree &T, int maxrank, std::vector<int32_t>
         rb[node] = std::min<int64_t>({int64_t(maxrank), m, int64_t(nfp)});
     }
     d.h_xoff.assign(T.nnodes + 1, 0);
-    for (int node = 0; node < T.nnodes; ++node) d.h_xoff[node + 1] = d.h_xoff[node] + mb[node] * rb[node];
+    for (int node = 0; node < T.nnodes; ++node) d.h_xoff[node + 1] = d.h_xoff[node] + pad2(mb[node] * rb[node]);
     lv_ptr.assign(1, 0);
     lv_nodes.clear();
     lv_mcap.clear();
@@ -385,39 +398,50 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         d.h_nrows = d.nrows.download(s);
         d.h_piv = d.piv.download(s);
         plan_apply(d, T, s);
-        if (c->f32) {
-            d.X32.alloc(d.X.n);
-            if (d.X.n) k_to_f32<<<launch_grid(int64_t(d.X.n) / 256 + 1, 8), 256, 0, s>>>(d.X.p, d.X32.p, int64_t(d.X.n));
-            CK(cudaGetLastError());
-        }
+        d.XT.alloc(d.X.n);
+        launch_transpose_blocks<double2>(d.X.p, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, T.nnodes, d.XT.p, s);
+        CK(cudaGetLastError());
     }
-    // couplings S_ts = K[tau_t, sigma_s] in test CSR order
+    // couplings S_ts = K[tau_t, sigma_s] in test CSR order, and their transposes in trial CSR order
     const nca::Tree &Tt = c->tree[0], &Ts = c->tree[1];
+    const std::vector<int32_t> &rk_t = c->side[0].h_rank, &rk_s = c->side[1].h_rank;
     const int64_t npairs = P.farnodes.size();
     std::vector<int32_t> pair_t(npairs), pair_s(P.farnodes.begin(), P.farnodes.end());
-    c->h_coff.assign(npairs + 1, 0);
+    c->h_cfoff.assign(npairs + 1, 0);
+    int64_t coupling_entries = 0;
     for (int t = 0; t < Tt.nnodes; ++t)
         for (int i = P.farptr[t]; i < P.farptr[t + 1]; ++i) {
             pair_t[i] = t;
-            c->h_coff[i + 1] = c->h_coff[i] + int64_t(c->side[0].h_rank[t]) * c->side[1].h_rank[P.farnodes[i]];
+            const int64_t e = int64_t(rk_t[t]) * rk_s[P.farnodes[i]];
+            coupling_entries += e;
+            c->h_cfoff[i + 1] = c->h_cfoff[i] + pad2(e);
         }
     c->farptr.upload(P.farptr, s);
     c->farnodes.upload(P.farnodes, s);
     c->tfarptr.upload(P.tfarptr, s);
     c->tfarnodes.upload(P.tfarnodes, s);
-    std::vector<int32_t> tfarpair(P.tfarnodes.size());
+    const int64_t ntf = P.tfarnodes.size();
+    std::vector<int32_t> tfarpair(ntf), tr_rows(ntf), tr_cols(ntf);
+    std::vector<int64_t> tr_in(ntf), h_ctoff(ntf + 1, 0);
     for (int sn = 0; sn < Ts.nnodes; ++sn)
         for (int k = P.tfarptr[sn]; k < P.tfarptr[sn + 1]; ++k) {
-            int t = P.tfarnodes[k];
+            const int t = P.tfarnodes[k];
             auto it = std::lower_bound(P.farnodes.begin() + P.farptr[t], P.farnodes.begin() + P.farptr[t + 1], sn);
-            tfarpair[k] = int32_t(it - P.farnodes.begin());
+            const int pair = int(it - P.farnodes.begin());
+            tfarpair[k] = pair;
+            tr_in[k] = c->h_cfoff[pair];
+            tr_rows[k] = rk_t[t];
+            tr_cols[k] = rk_s[sn];
+            h_ctoff[k + 1] = h_ctoff[k] + pad2(int64_t(rk_t[t]) * rk_s[sn]);
         }
     c->tfarpair.upload(tfarpair, s);
-    c->coff.upload(c->h_coff, s);
-    c->C.alloc(size_t(c->h_coff.back()));
-    if (c->f32) c->C32.alloc(c->C.n);
+    c->cfoff.upload(c->h_cfoff, s);
+    c->ctoff.upload(h_ctoff, s);
+    c->C.alloc(size_t(c->h_cfoff.back()));
+    c->CT.alloc(size_t(h_ctoff.back()));
     {
-        DBuf<int32_t> dpt, dps;
+        DBuf<int32_t> dpt, dps, drows, dcols;
+        DBuf<int64_t> din;
         dpt.upload(pair_t, s);
         dps.upload(pair_s, s);
         CouplingArgs a;
@@ -431,58 +455,101 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         a.piv_t = c->side[0].piv.p;
         a.piv_s = c->side[1].piv.p;
         a.maxrank = maxrank;
-        a.coff = c->coff.p;
+        a.coff = c->cfoff.p;
         a.npairs = npairs;
         a.C = c->C.p;
-        a.C32 = c->f32 ? c->C32.p : nullptr;
+        a.C32 = nullptr;
         if (npairs > 0) {
             k_couplings<<<launch_grid(npairs, 16), 256, 0, s>>>(a);
             CK(cudaGetLastError());
         }
+        din.upload(tr_in, s);
+        drows.upload(tr_rows, s);
+        dcols.upload(tr_cols, s);
+        launch_transpose_blocks<double2>(c->C.p, din.p, drows.p, dcols.p, c->ctoff.p, ntf, c->CT.p, s);
+        CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s));
     }
+    // output nodes of the coupling stage, largest work first (shorter tail of the last wave)
     std::vector<int32_t> fwd, rev;
-    for (int t = 0; t < Tt.nnodes; ++t)
-        if (c->side[0].h_rank[t] > 0) fwd.push_back(t);
-    for (int sn = 0; sn < Ts.nnodes; ++sn)
-        if (c->side[1].h_rank[sn] > 0) rev.push_back(sn);
+    std::vector<int64_t> wf(Tt.nnodes, 0), wr(Ts.nnodes, 0);
+    for (int t = 0; t < Tt.nnodes; ++t) {
+        if (rk_t[t] <= 0) continue;
+        fwd.push_back(t);
+        for (int i = P.farptr[t]; i < P.farptr[t + 1]; ++i) wf[t] += int64_t(rk_t[t]) * rk_s[P.farnodes[i]];
+    }
+    for (int sn = 0; sn < Ts.nnodes; ++sn) {
+        if (rk_s[sn] <= 0) continue;
+        rev.push_back(sn);
+        for (int k = P.tfarptr[sn]; k < P.tfarptr[sn + 1]; ++k) wr[sn] += int64_t(rk_s[sn]) * rk_t[P.tfarnodes[k]];
+    }
+    std::stable_sort(fwd.begin(), fwd.end(), [&](int a, int b) { return wf[a] > wf[b]; });
+    std::stable_sort(rev.begin(), rev.end(), [&](int a, int b) { return wr[a] > wr[b]; });
     c->n_couple_fwd = int(fwd.size());
     c->n_couple_rev = int(rev.size());
     c->couple_fwd.upload(fwd, s);
     c->couple_rev.upload(rev, s);
-    // near field: one row block per test leaf, columns = its near trial leaves in list order
+    // near field: one block per near pair (test CSR order) and its transpose (trial CSR order)
     const int64_t nnear = P.nearnodes.size();
     c->h_noff.assign(Tt.nnodes + 1, 0);
     c->h_ncols.assign(Tt.nnodes, 0);
-    std::vector<int32_t> near_coloff(nnear), near_t(nnear);
+    c->h_nfoff.assign(nnear + 1, 0);
+    std::vector<int32_t> near_t(nnear);
+    int64_t near_entries = 0;
     for (int t = 0; t < Tt.nnodes; ++t) {
         int col = 0;
         for (int i = P.nearptr[t]; i < P.nearptr[t + 1]; ++i) {
-            near_coloff[i] = col;
             near_t[i] = t;
-            col += Ts.size(P.nearnodes[i]);
+            const int ms = Ts.size(P.nearnodes[i]);
+            col += ms;
+            const int64_t e = int64_t(Tt.size(t)) * ms;
+            near_entries += e;
+            c->h_nfoff[i + 1] = c->h_nfoff[i] + pad2(e);
         }
         c->h_ncols[t] = col;
         c->h_noff[t + 1] = c->h_noff[t] + int64_t(Tt.size(t)) * col;
     }
-    std::vector<int32_t> tnear_coloff(P.tnearnodes.size());
+    const int64_t ntn = P.tnearnodes.size();
+    std::vector<int32_t> ntr_rows(ntn), ntr_cols(ntn);
+    std::vector<int64_t> ntr_in(ntn), h_ntoff(ntn + 1, 0);
     for (int sn = 0; sn < Ts.nnodes; ++sn)
         for (int k = P.tnearptr[sn]; k < P.tnearptr[sn + 1]; ++k) {
-            int t = P.tnearnodes[k];
+            const int t = P.tnearnodes[k];
             auto it = std::lower_bound(P.nearnodes.begin() + P.nearptr[t], P.nearnodes.begin() + P.nearptr[t + 1], sn);
-            tnear_coloff[k] = near_coloff[it - P.nearnodes.begin()];
+            ntr_in[k] = c->h_nfoff[it - P.nearnodes.begin()];
+            ntr_rows[k] = Tt.size(t);
+            ntr_cols[k] = Ts.size(sn);
+            h_ntoff[k + 1] = h_ntoff[k] + pad2(int64_t(Tt.size(t)) * Ts.size(sn));
         }
+    // leaves of both sides, largest work (near columns + own basis) first
+    for (int sd = 0; sd < 2; ++sd) {
+        const nca::Tree &T = c->tree[sd];
+        const std::vector<int32_t> &ptr = sd == 0 ? P.nearptr : P.tnearptr;
+        const std::vector<int32_t> &nodes = sd == 0 ? P.nearnodes : P.tnearnodes;
+        const nca::Tree &F = c->tree[1 - sd];
+        std::vector<int64_t> work(T.nnodes, 0);
+        std::vector<int32_t> leaves;
+        for (int t = 0; t < T.nnodes; ++t) {
+            if (!T.isleaf(t)) continue;
+            leaves.push_back(t);
+            work[t] = c->side[sd].h_rank[t];
+            for (int i = ptr[t]; i < ptr[t + 1]; ++i) work[t] += F.size(nodes[i]);
+            work[t] *= T.size(t);
+        }
+        std::stable_sort(leaves.begin(), leaves.end(), [&](int a, int b) { return work[a] > work[b]; });
+        c->side[sd].leaves.upload(leaves, s);
+    }
     c->nearptr.upload(P.nearptr, s);
     c->nearnodes.upload(P.nearnodes, s);
-    c->near_coloff.upload(near_coloff, s);
     c->tnearptr.upload(P.tnearptr, s);
     c->tnearnodes.upload(P.tnearnodes, s);
-    c->tnear_coloff.upload(tnear_coloff, s);
-    c->noff.upload(c->h_noff, s);
-    c->N.alloc(size_t(c->h_noff.back()));
-    if (c->f32) c->N32.alloc(c->N.n);
+    c->nfoff.upload(c->h_nfoff, s);
+    c->ntoff.upload(h_ntoff, s);
+    c->N.alloc(size_t(c->h_nfoff.back()));
+    c->NT.alloc(size_t(h_ntoff.back()));
     {
-        DBuf<int32_t> dnt;
+        DBuf<int32_t> dnt, drows, dcols;
+        DBuf<int64_t> din;
         dnt.upload(near_t, s);
         NearArgs a;
         a.K = c->K;
@@ -490,20 +557,38 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         a.trial_pts = c->side[1].pts.p;
         a.pair_t = dnt.p;
         a.pair_s = c->nearnodes.p;
-        a.coloff = c->near_coloff.p;
         a.t_perm = c->side[0].perm.p;
         a.t_begin = c->side[0].begin.p;
         a.t_end = c->side[0].end.p;
         a.s_perm = c->side[1].perm.p;
         a.s_begin = c->side[1].begin.p;
         a.s_end = c->side[1].end.p;
-        a.noff = c->noff.p;
+        a.poff = c->nfoff.p;
         a.npairs = nnear;
         a.N = c->N.p;
-        a.N32 = c->f32 ? c->N32.p : nullptr;
         if (nnear > 0) {
             k_near<<<launch_grid(nnear, 16), 256, 0, s>>>(a);
             CK(cudaGetLastError());
+        }
+        din.upload(ntr_in, s);
+        drows.upload(ntr_rows, s);
+        dcols.upload(ntr_cols, s);
+        launch_transpose_blocks<double2>(c->N.p, din.p, drows.p, dcols.p, c->ntoff.p, ntn, c->NT.p, s);
+        CK(cudaGetLastError());
+        if (c->f32) {
+            auto down = [&](DBuf<double2> &src, DBuf<float2> &dst) {
+                dst.alloc(src.n);
+                if (src.n) k_to_f32<<<launch_grid(int64_t(src.n) / 256 + 1, 8), 256, 0, s>>>(src.p, dst.p, int64_t(src.n));
+                CK(cudaGetLastError());
+            };
+            for (int sd = 0; sd < 2; ++sd) {
+                down(c->side[sd].X, c->side[sd].X32);
+                down(c->side[sd].XT, c->side[sd].XT32);
+            }
+            down(c->C, c->C32);
+            down(c->CT, c->CT32);
+            down(c->N, c->N32);
+            down(c->NT, c->NT32);
         }
         CK(cudaEventRecord(ev1, s));
         CK(cudaStreamSynchronize(s));
@@ -518,8 +603,8 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
     I.nnodes_trial = Ts.nnodes;
     I.ncoeff_test = c->side[0].h_cptr.back();
     I.ncoeff_trial = c->side[1].h_cptr.back();
-    I.near_entries = c->h_noff.back();
-    I.coupling_entries = c->h_coff.back();
+    I.near_entries = near_entries;
+    I.coupling_entries = coupling_entries;
     for (int sd = 0; sd < 2; ++sd) {
         int64_t basis = 0, transfer = 0;
         const nca::Tree &T = c->tree[sd];
@@ -546,15 +631,18 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
         return fail(NCA_ERR_ARG, "complex FP32 product requested but the core was built without store_f32");
     const int in = mode == 0 ? 1 : 0, out = 1 - in;
     const int64_t nin = c->side[in].npts, nout = c->side[out].npts;
-    if (nrhs < 0 || ldx < nin || ldy < nout) return fail(NCA_ERR_DIM, "DimensionMismatch: leading dimension smaller than the operator size");
+    if (nrhs < 0 || ldx < nin || ldy < nout)
+        return fail(NCA_ERR_DIM, "DimensionMismatch: leading dimension smaller than the operator size");
     if (nrhs == 0) return NCA_OK;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = ws->stream;
     const int b = int(nrhs);
+    const int vs = vector_stride(b);
     DevSide &I = c->side[in], &O = c->side[out];
     if (b > ws->max_nrhs) {
-        ws->xt.alloc(size_t(std::max(c->side[0].npts, c->side[1].npts)) * b);
-        ws->xhat.alloc(size_t(std::max(c->side[0].h_cptr.back(), c->side[1].h_cptr.back())) * b);
+        const int vsm = b + 2;  // >= vector_stride(b') for every b' <= b
+        ws->xt.alloc(size_t(std::max(c->side[0].npts, c->side[1].npts)) * vsm);
+        ws->xhat.alloc(size_t(std::max(c->side[0].h_cptr.back(), c->side[1].h_cptr.back())) * vsm);
         ws->yhat.alloc(ws->xhat.n);
         ws->max_nrhs = b;
     }
@@ -567,7 +655,12 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
         if (ws->ystage.n < size_t(nout) * b) ws->ystage.alloc(size_t(nout) * b);
     }
     int launches = 0;
+    int stage_launch[5] = {0, 0, 0, 0, 0};
+    auto mark = [&](int k) {
+        if (ws->profiling) CK(cudaEventRecord(ws->stage_ev[k], s));
+    };
     CK(cudaEventRecord(ws->e0, s));
+    CK(cudaMemsetAsync(ws->error.p, 0, sizeof(int32_t), s));
     if (memspace == 0) {
         CK(cudaMemcpy2DAsync(ws->xstage.p, sizeof(double2) * nin, xd, sizeof(double2) * ldx,
                              sizeof(double2) * nin, b, cudaMemcpyHostToDevice, s));
@@ -579,104 +672,163 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
         lx = nin;
         ly = nout;
     }
-    k_gather<<<launch_grid(nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, I.perm.p, nin, b, ws->xt.p);
+    mark(0);
+    k_gather<<<launch_grid(nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, I.perm.p, nin, b, vs, ws->xt.p);
     ++launches;
-    CK(cudaMemsetAsync(ws->yhat.p, 0, sizeof(double2) * size_t(O.h_cptr.back()) * b, s));
+    ++stage_launch[0];
+    mark(1);
     const bool conj = mode == 2;
-    const int bc = std::min(b, 16);
     auto run = [&](auto tag) {
         using S = decltype(tag);
-        const S *Xi = nullptr, *Xo = nullptr, *Cm = nullptr, *Nm = nullptr;
-        if constexpr (std::is_same<S, double2>::value) {
-            Xi = I.X.p;
-            Xo = O.X.p;
-            Cm = c->C.p;
-            Nm = c->N.p;
-        } else {
-            Xi = I.X32.p;
-            Xo = O.X32.p;
-            Cm = c->C32.p;
-            Nm = c->N32.p;
-        }
-        const int tile = kApplyTile;
-        // upward sweep (leaves at any level take x, others their children's xhat)
-        SweepArgs<S> up{I.begin.p, I.firstchild.p, I.nchildren.p, I.rank.p, I.nrows.p, I.xoff.p, I.cptr.p,
-                        Xi, ws->xt.p, ws->xhat.p, b, conj && in == 0};
-        for (size_t l = 0; l + 1 < I.up.ptr.size(); ++l) {
-            int cnt = I.up.ptr[l + 1] - I.up.ptr[l];
-            if (!cnt) continue;
-            int mc = std::max(I.up.mcap[l], bc);
-            launch_up<S>(up, I.up.d_nodes.p + I.up.ptr[l], cnt, mc, tile, s);
-            ++launches;
-        }
-        // coupling
-        CoupleArgs<S> cp;
+        constexpr bool f64 = std::is_same<S, double2>::value;
+        const S *XTi = f64 ? (const S *)I.XT.p : (const S *)I.XT32.p;
+        const S *Xo = f64 ? (const S *)O.X.p : (const S *)O.X32.p;
+        const S *Cm = nullptr, *Nm = nullptr;
         if (mode == 0) {
-            cp = CoupleArgs<S>{c->farptr.p, c->farnodes.p, nullptr, c->side[0].rank.p, c->side[1].rank.p,
-                               c->side[0].cptr.p, c->side[1].cptr.p, c->coff.p, Cm, ws->xhat.p, ws->yhat.p,
-                               b, false, false};
+            Cm = f64 ? (const S *)c->C.p : (const S *)c->C32.p;
+            Nm = f64 ? (const S *)c->N.p : (const S *)c->N32.p;
         } else {
-            cp = CoupleArgs<S>{c->tfarptr.p, c->tfarnodes.p, c->tfarpair.p, c->side[1].rank.p, c->side[0].rank.p,
-                               c->side[1].cptr.p, c->side[0].cptr.p, c->coff.p, Cm, ws->xhat.p, ws->yhat.p,
-                               b, true, conj};
+            Cm = f64 ? (const S *)c->CT.p : (const S *)c->CT32.p;
+            Nm = f64 ? (const S *)c->NT.p : (const S *)c->NT32.p;
         }
-        int ncp = mode == 0 ? c->n_couple_fwd : c->n_couple_rev;
-        if (ncp > 0) {
-            int mc = std::max(c->maxrank, bc);
-            launch_couple<S>(cp, mode == 0 ? c->couple_fwd.p : c->couple_rev.p, ncp, mc, tile, s);
+        for (int q0 = 0; q0 < b; q0 += 16) {
+            const int bc = std::min(16, b - q0);
+            if (ws->far) {
+                // upward sweep: xhat_p = XT_p [leaf x slice | children's xhat], deepest level first
+                for (size_t l = 0; l + 1 < I.up.ptr.size(); ++l) {
+                    const int cnt = I.up.ptr[l + 1] - I.up.ptr[l];
+                    if (!cnt) continue;
+                    RowArgs<S> a{};
+                    a.stage = STAGE_UP;
+                    a.begin = I.begin.p;
+                    a.firstchild = I.firstchild.p;
+                    a.nchildren = I.nchildren.p;
+                    a.rank = I.rank.p;
+                    a.nrows = I.nrows.p;
+                    a.cptr = I.cptr.p;
+                    a.M = XTi;
+                    a.moff = I.xoff.p;
+                    a.src = ws->xt.p;
+                    a.coef = ws->xhat.p;
+                    a.b = b;
+                    a.bc = bc;
+                    a.q0 = q0;
+                    a.vs = vs;
+                    a.conj = conj && in == 0;
+                    a.maxrows = I.up.mcap[l];
+                    a.error = ws->error.p;
+                    launch_rows<S>(a, I.up.d_nodes.p + I.up.ptr[l], cnt, s);
+                    ++launches;
+                    ++stage_launch[1];
+                }
+            }
+            if (q0 == 0) mark(2);
+            const int ncp = mode == 0 ? c->n_couple_fwd : c->n_couple_rev;
+            if (ws->far && ncp > 0) {
+                RowArgs<S> a{};
+                a.stage = STAGE_COUPLE;
+                a.M = Cm;
+                if (mode == 0) {
+                    a.moff = c->cfoff.p;
+                    a.ptr = c->farptr.p;
+                    a.other = c->farnodes.p;
+                } else {
+                    a.moff = c->ctoff.p;
+                    a.ptr = c->tfarptr.p;
+                    a.other = c->tfarnodes.p;
+                }
+                a.rank_in = I.rank.p;
+                a.rank_out = O.rank.p;
+                a.cptr_in = I.cptr.p;
+                a.cptr_out = O.cptr.p;
+                a.src = ws->xhat.p;
+                a.dst = ws->yhat.p;
+                a.b = b;
+                a.bc = bc;
+                a.q0 = q0;
+                a.vs = vs;
+                a.conj = conj;
+                a.maxrows = c->maxrank;
+                a.error = ws->error.p;
+                launch_rows<S>(a, mode == 0 ? c->couple_fwd.p : c->couple_rev.p, ncp, s);
+                ++launches;
+                ++stage_launch[2];
+            }
+            if (q0 == 0) mark(3);
+            if (ws->far) {
+                // downward sweep: [yhat_children] += X_p yhat_p, root level first
+                for (size_t l = 0; l + 1 < O.down.ptr.size(); ++l) {
+                    const int cnt = O.down.ptr[l + 1] - O.down.ptr[l];
+                    if (!cnt) continue;
+                    RowArgs<S> a{};
+                    a.stage = STAGE_DOWN;
+                    a.firstchild = O.firstchild.p;
+                    a.rank = O.rank.p;
+                    a.nrows = O.nrows.p;
+                    a.cptr = O.cptr.p;
+                    a.M = Xo;
+                    a.moff = O.xoff.p;
+                    a.coef = ws->yhat.p;
+                    a.b = b;
+                    a.bc = bc;
+                    a.q0 = q0;
+                    a.vs = vs;
+                    a.conj = conj && out == 1;
+                    a.maxrows = O.down.mcap[l];
+                    a.error = ws->error.p;
+                    launch_rows<S>(a, O.down.d_nodes.p + O.down.ptr[l], cnt, s);
+                    ++launches;
+                    ++stage_launch[3];
+                }
+            }
+            if (q0 == 0) mark(4);
+            // leaves: y_t = X_t yhat_t + sum_s N_ts x_s, scattered into y
+            RowArgs<S> a{};
+            a.stage = STAGE_LEAVES;
+            a.begin = O.begin.p;
+            a.end = O.end.p;
+            a.perm = O.perm.p;
+            a.rank = O.rank.p;
+            a.cptr = O.cptr.p;
+            a.X = ws->far ? Xo : nullptr;
+            a.xoff = O.xoff.p;
+            a.coef = ws->yhat.p;
+            if (ws->near) {
+                a.M = Nm;
+                a.moff = mode == 0 ? c->nfoff.p : c->ntoff.p;
+                a.ptr = mode == 0 ? c->nearptr.p : c->tnearptr.p;
+                a.other = mode == 0 ? c->nearnodes.p : c->tnearnodes.p;
+            }
+            a.o_begin = I.begin.p;
+            a.o_end = I.end.p;
+            a.src = ws->xt.p;
+            a.y = yd;
+            a.ldy = ly;
+            a.alpha = alpha;
+            a.beta = beta;
+            a.usebeta = usebeta;
+            a.b = b;
+            a.bc = bc;
+            a.q0 = q0;
+            a.vs = vs;
+            a.conj = conj;
+            a.maxrows = O.leafcap;
+            a.error = ws->error.p;
+            launch_rows<S>(a, O.leaves.p, O.nleaves, s);
             ++launches;
+            ++stage_launch[4];
         }
-        // downward sweep
-        SweepArgs<S> dn{O.begin.p, O.firstchild.p, O.nchildren.p, O.rank.p, O.nrows.p, O.xoff.p, O.cptr.p,
-                        Xo, ws->xt.p, ws->yhat.p, b, conj && out == 1};
-        for (size_t l = 0; l + 1 < O.down.ptr.size(); ++l) {
-            int cnt = O.down.ptr[l + 1] - O.down.ptr[l];
-            if (!cnt) continue;
-            int mc = std::max(O.down.mcap[l], bc);
-            launch_down<S>(dn, O.down.d_nodes.p + O.down.ptr[l], cnt, mc, tile, s);
-            ++launches;
-        }
-        // leaves: op(X_t) yhat_t + near field, scattered into y
-        LeafArgs<S> lf;
-        lf.perm = O.perm.p;
-        lf.begin = O.begin.p;
-        lf.end = O.end.p;
-        lf.rank = O.rank.p;
-        lf.nrows = O.nrows.p;
-        lf.xoff = O.xoff.p;
-        lf.cptr = O.cptr.p;
-        lf.X = Xo;
-        lf.yhat = ws->yhat.p;
-        if (mode == 0) {
-            lf.nptr = c->nearptr.p;
-            lf.nnodes = c->nearnodes.p;
-            lf.coloff = c->near_coloff.p;
-        } else {
-            lf.nptr = c->tnearptr.p;
-            lf.nnodes = c->tnearnodes.p;
-            lf.coloff = c->tnear_coloff.p;
-        }
-        lf.o_begin = I.begin.p;
-        lf.o_end = I.end.p;
-        lf.noff = c->noff.p;
-        lf.N = Nm;
-        lf.xt = ws->xt.p;
-        lf.y = yd;
-        lf.ldy = ly;
-        lf.alpha = alpha;
-        lf.beta = usebeta ? beta : make_double2(0.0, 0.0);
-        lf.b = b;
-        lf.reverse = mode != 0;
-        lf.conj = conj && out == 1;
-        int mc = std::max(O.leafcap, bc);
-        launch_leaves<S>(lf, O.leaves.p, O.nleaves, mc, tile, s);
-        ++launches;
+        mark(5);
     };
+    const int cap = rows_capacity(std::min(b, 16));
+    if (O.leafcap > cap || I.leafcap > cap || 2 * c->maxrank > cap)
+        return fail(NCA_ERR_ARG, "a leaf or transfer block has more rows than one product CTA holds");
     if (precision == NCA_PREC_F64)
         run(double2{});
     else
         run(float2{});
     CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ws->error_host, ws->error.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     if (memspace == 0)
         CK(cudaMemcpy2DAsync(y, sizeof(double2) * ldy, ws->ystage.p, sizeof(double2) * nout,
                              sizeof(double2) * nout, b, cudaMemcpyDeviceToHost, s));
@@ -686,6 +838,16 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     CK(cudaEventElapsedTime(&ms, ws->e0, ws->e1));
     ws->last_seconds = ms * 1e-3;
     ws->last_launches = launches;
+    if (ws->profiling) {
+        for (int k = 0; k < 5; ++k) {
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, ws->stage_ev[k], ws->stage_ev[k + 1]));
+            ws->stage_seconds[k] = t * 1e-3;
+            ws->stage_launches[k] = stage_launch[k];
+        }
+    }
+    if (*ws->error_host == 2) return fail(NCA_ERR_TIMEOUT, "a bounded wait in the product kernel gave up");
+    if (*ws->error_host != 0) return fail(NCA_ERR_CUDA, "internal: a product copy was misaligned and skipped");
     return NCA_OK;
 }
 
@@ -888,8 +1050,16 @@ int32_t nca_core_export_couplings(const nca_core *core, int64_t *off, double *C)
     return guarded([&] {
         if (!core) return fail(NCA_ERR_ARG, "null core");
         CK(cudaSetDevice(core->device));
-        std::copy(core->h_coff.begin(), core->h_coff.end(), off);
-        if (core->C.n) CK(cudaMemcpy(C, core->C.p, sizeof(double2) * core->C.n, cudaMemcpyDeviceToHost));
+        std::vector<double2> all(core->C.n);
+        if (core->C.n) CK(cudaMemcpy(all.data(), core->C.p, sizeof(double2) * core->C.n, cudaMemcpyDeviceToHost));
+        const nca::Partition &P = core->part;
+        off[0] = 0;
+        for (int t = 0; t < core->tree[0].nnodes; ++t)
+            for (int i = P.farptr[t]; i < P.farptr[t + 1]; ++i) {
+                const int64_t e = int64_t(core->side[0].h_rank[t]) * core->side[1].h_rank[P.farnodes[i]];
+                off[i + 1] = off[i] + e;
+                std::memcpy(C + 2 * off[i], all.data() + core->h_cfoff[i], sizeof(double2) * e);
+            }
         return int(NCA_OK);
     });
 }
@@ -898,9 +1068,19 @@ int32_t nca_core_export_near(const nca_core *core, int64_t *off, int32_t *ncols,
     return guarded([&] {
         if (!core) return fail(NCA_ERR_ARG, "null core");
         CK(cudaSetDevice(core->device));
+        std::vector<double2> all(core->N.n);
+        if (core->N.n) CK(cudaMemcpy(all.data(), core->N.p, sizeof(double2) * core->N.n, cudaMemcpyDeviceToHost));
+        const nca::Partition &P = core->part;
         std::copy(core->h_noff.begin(), core->h_noff.end(), off);
         std::copy(core->h_ncols.begin(), core->h_ncols.end(), ncols);
-        if (core->N.n) CK(cudaMemcpy(N, core->N.p, sizeof(double2) * core->N.n, cudaMemcpyDeviceToHost));
+        for (int t = 0; t < core->tree[0].nnodes; ++t) {
+            int64_t pos = core->h_noff[t];
+            for (int i = P.nearptr[t]; i < P.nearptr[t + 1]; ++i) {
+                const int64_t e = int64_t(core->tree[0].size(t)) * core->tree[1].size(P.nearnodes[i]);
+                std::memcpy(N + 2 * pos, all.data() + core->h_nfoff[i], sizeof(double2) * e);
+                pos += e;
+            }
+        }
         return int(NCA_OK);
     });
 }
@@ -915,10 +1095,12 @@ int32_t nca_workspace_create(nca_core *core, int32_t max_nrhs, nca_workspace **o
         CK(cudaEventCreate(&ws->e0));
         CK(cudaEventCreate(&ws->e1));
         int b = std::max(1, max_nrhs);
-        ws->xt.alloc(size_t(std::max(core->side[0].npts, core->side[1].npts)) * b);
-        ws->xhat.alloc(size_t(std::max(core->side[0].h_cptr.back(), core->side[1].h_cptr.back())) * b);
+        ws->xt.alloc(size_t(std::max(core->side[0].npts, core->side[1].npts)) * (b + 2));
+        ws->xhat.alloc(size_t(std::max(core->side[0].h_cptr.back(), core->side[1].h_cptr.back())) * (b + 2));
         ws->yhat.alloc(ws->xhat.n);
         ws->max_nrhs = b;
+        ws->error.alloc(1);
+        CK(cudaMallocHost(&ws->error_host, sizeof(int32_t)));
         *out = ws.release();
         return int(NCA_OK);
     });
@@ -930,6 +1112,9 @@ void nca_workspace_destroy(nca_workspace *ws) {
     if (ws->stream) cudaStreamDestroy(ws->stream);
     if (ws->e0) cudaEventDestroy(ws->e0);
     if (ws->e1) cudaEventDestroy(ws->e1);
+    for (cudaEvent_t &e : ws->stage_ev)
+        if (e) cudaEventDestroy(e);
+    if (ws->error_host) cudaFreeHost(ws->error_host);
     delete ws;
 }
 
@@ -957,6 +1142,33 @@ int32_t nca_workspace_last_time(const nca_workspace *ws, double *seconds) {
 int32_t nca_workspace_last_launches(const nca_workspace *ws, int32_t *launches) {
     if (!ws || !launches) return fail(NCA_ERR_ARG, "null argument");
     *launches = ws->last_launches;
+    return NCA_OK;
+}
+
+int32_t nca_workspace_set_parts(nca_workspace *ws, int32_t far, int32_t near) {
+    if (!ws) return fail(NCA_ERR_ARG, "null workspace");
+    ws->far = far != 0;
+    ws->near = near != 0;
+    return NCA_OK;
+}
+
+int32_t nca_workspace_set_profiling(nca_workspace *ws, int32_t on) {
+    return guarded([&] {
+        if (!ws) return fail(NCA_ERR_ARG, "null workspace");
+        CK(cudaSetDevice(ws->core->device));
+        for (cudaEvent_t &e : ws->stage_ev)
+            if (!e) CK(cudaEventCreate(&e));
+        ws->profiling = on != 0;
+        return int(NCA_OK);
+    });
+}
+
+int32_t nca_workspace_stage_times(const nca_workspace *ws, double *seconds, int32_t *launches, int32_t nstages) {
+    if (!ws || nstages < 0) return fail(NCA_ERR_ARG, "bad argument");
+    for (int k = 0; k < std::min(nstages, 5); ++k) {
+        if (seconds) seconds[k] = ws->stage_seconds[k];
+        if (launches) launches[k] = ws->stage_launches[k];
+    }
     return NCA_OK;
 }
 

@@ -12,8 +12,8 @@ from .admissibility import FarData, fardata, farfield, farinteractions, farnodes
 from .compressors import ACA, BatchedBottomUp, FNormEstimator, FullPivoting, TreeMimicryPivoting, _clustersize, \
     _selectfarpivots
 from .kernels import HelmholtzKernel, LaplaceKernel, MatrixKernel
-from .nca import (H2Workspace, PetrovGalerkinNCA, PetrovGalerkinNCACore, adjoint, core, mul, storage, transpose,
-                  withworkspace)
+from .nca import (H2Workspace, PetrovGalerkinNCA, PetrovGalerkinNCACore, adjoint, core, farmatrix, mul, nearmatrix,
+                  storage, transpose, withworkspace)
 from .trees import BlockTree, KMeansTree, KMeansTreeBuilder, testtree, trialtree
 from .utils import collect_assigned, plan_from_pivots, ptrfromcounts
 

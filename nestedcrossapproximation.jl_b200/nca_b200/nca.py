@@ -310,10 +310,13 @@ class H2Workspace(LinearMap):
         self.precision = PREC_F32 if self.dtype == np.complex64 else PREC_F64
         if self.precision == PREC_F32 and not core.f32:
             raise ArgumentError("a complex64 workspace needs a core built with store_f32=True")
+        if parts not in ("all", "far", "near"):
+            raise ArgumentError("parts must be 'all', 'far' or 'near'")
         self.parts = parts
         h = C.c_void_p()
         check(lib().nca_workspace_create(core._h, int(max_nrhs), C.byref(h)))
         self._h = h
+        check(lib().nca_workspace_set_parts(h, int(parts != "near"), int(parts != "far")))
         self._lock = threading.Lock()
         self.shape = core.dim
         self.last_seconds = 0.0
@@ -336,6 +339,36 @@ class H2Workspace(LinearMap):
 
     def _apply(self, x, mode):
         return mul(None, self if mode == MODE_N else _Transposed(self, mode), x)
+
+
+    def set_profiling(self, on: bool = True):
+        """Record CUDA events around each stage of every product (see stage_times)."""
+        check(lib().nca_workspace_set_profiling(self._h, int(on)))
+
+    def stage_times(self):
+        """Device seconds and launches of the last product per stage: gather, upward sweep,
+        coupling, downward sweep, leaves + near field."""
+        t = (C.c_double * 5)()
+        n = (C.c_int32 * 5)()
+        check(lib().nca_workspace_stage_times(self._h, t, n, 5))
+        names = ("gather", "upward", "coupling", "downward", "leaves")
+        return {k: (t[i], n[i]) for i, k in enumerate(names)}
+
+    def launches(self):
+        n = C.c_int32()
+        check(lib().nca_workspace_last_launches(self._h, C.byref(n)))
+        return n.value
+
+
+def farmatrix(h2mat: H2Workspace) -> H2Workspace:
+    """The far field of h2mat as a workspace with an empty near field; the stores are shared,
+    the buffers are not (petrovgalerkinnca.jl:344-362)."""
+    return H2Workspace(h2mat.core, h2mat.dtype, parts="far")
+
+
+def nearmatrix(h2mat: H2Workspace) -> H2Workspace:
+    """The near field of h2mat as a linear map (its dense blocks: core.nearblocks)."""
+    return H2Workspace(h2mat.core, h2mat.dtype, parts="near")
 
 
 def withworkspace(f, ws: H2Workspace):
