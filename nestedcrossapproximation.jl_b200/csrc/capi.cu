@@ -181,6 +181,9 @@ constexpr int kMaxSmem = 227 * 1024;
 // Block sizes rounded up to an even number of entries: every block then starts on a 32-byte
 // (FP64) or 16-byte (FP32) boundary, as the bulk copies of the product require.
 inline int64_t pad2(int64_t n) { return (n + 1) & ~int64_t(1); }
+// Row slots of a vector buffer that serves every b' <= b right-hand sides: vector_stride(b') is
+// b' plus at most 3 padding slots.
+inline int vector_slots(int b) { return b + 3; }
 
 void set_kernel_params(nca_core *c, const nca_kernel_desc *k, int64_t ntest, int64_t ntrial,
                        cudaStream_t s) {
@@ -622,60 +625,42 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
                            std::chrono::duration<double>(h2 - h1).count() - ms * 1e-3;
 }
 
-int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_t ldx, void *y,
-               int64_t ldy, int64_t nrhs, double2 alpha, double2 beta, int memspace) {
-    nca_core *c = ws->core;
-    if (mode < 0 || mode > 2) return fail(NCA_ERR_ARG, "mode must be 0 (N), 1 (T) or 2 (C)");
-    if (precision != NCA_PREC_F64 && precision != NCA_PREC_F32) return fail(NCA_ERR_ARG, "unknown precision");
-    if (precision == NCA_PREC_F32 && !c->f32)
-        return fail(NCA_ERR_ARG, "complex FP32 product requested but the core was built without store_f32");
+// Device buffers one product runs on: the gathered input (nin x vs), the input side's
+// coefficients xhat and the output side's yhat (coefficient rows x vs), and the error word the
+// kernels raise (must be zero when the product starts).
+struct ProductBuffers {
+    double2 *xt, *xhat, *yhat;
+    int32_t *error;
+    bool far, near;
+};
+
+// Launch counts of one product: total and per stage (gather, up, couple, down, leaves).
+struct ProductLaunches {
+    int total = 0;
+    int stage[5] = {0, 0, 0, 0, 0};
+};
+
+// Enqueues the gather and the four product stages of y = alpha op(A) x + beta y on stream s.
+// x, y are device arrays (ldx, ldy leading dimensions); stage_ev (nullable) receives six events
+// that bracket the stages.
+int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int64_t lx, double2 *yd,
+                    int64_t ly, int b, double2 alpha, double2 beta, const ProductBuffers &buf,
+                    cudaStream_t s, cudaEvent_t *stage_ev, ProductLaunches &count) {
     const int in = mode == 0 ? 1 : 0, out = 1 - in;
-    const int64_t nin = c->side[in].npts, nout = c->side[out].npts;
-    if (nrhs < 0 || ldx < nin || ldy < nout)
-        return fail(NCA_ERR_DIM, "DimensionMismatch: leading dimension smaller than the operator size");
-    if (nrhs == 0) return NCA_OK;
-    CK(cudaSetDevice(c->device));
-    cudaStream_t s = ws->stream;
-    const int b = int(nrhs);
-    const int vs = vector_stride(b);
+    const int64_t nin = c->side[in].npts;
     DevSide &I = c->side[in], &O = c->side[out];
-    if (b > ws->max_nrhs) {
-        const int vsm = b + 2;  // >= vector_stride(b') for every b' <= b
-        ws->xt.alloc(size_t(std::max(c->side[0].npts, c->side[1].npts)) * vsm);
-        ws->xhat.alloc(size_t(std::max(c->side[0].h_cptr.back(), c->side[1].h_cptr.back())) * vsm);
-        ws->yhat.alloc(ws->xhat.n);
-        ws->max_nrhs = b;
-    }
-    const double2 *xd = reinterpret_cast<const double2 *>(x);
-    double2 *yd = reinterpret_cast<double2 *>(y);
-    int64_t lx = ldx, ly = ldy;
+    const int vs = vector_stride(b);
     const bool usebeta = beta.x != 0.0 || beta.y != 0.0;
-    if (memspace == 0) {
-        if (ws->xstage.n < size_t(nin) * b) ws->xstage.alloc(size_t(nin) * b);
-        if (ws->ystage.n < size_t(nout) * b) ws->ystage.alloc(size_t(nout) * b);
-    }
-    int launches = 0;
-    int stage_launch[5] = {0, 0, 0, 0, 0};
+    const int cap = rows_capacity(std::min(b, 16));
+    if (O.leafcap > cap || I.leafcap > cap || 2 * c->maxrank > cap)
+        return fail(NCA_ERR_ARG, "a leaf or transfer block has more rows than one product CTA holds");
     auto mark = [&](int k) {
-        if (ws->profiling) CK(cudaEventRecord(ws->stage_ev[k], s));
+        if (stage_ev) CK(cudaEventRecord(stage_ev[k], s));
     };
-    CK(cudaEventRecord(ws->e0, s));
-    CK(cudaMemsetAsync(ws->error.p, 0, sizeof(int32_t), s));
-    if (memspace == 0) {
-        CK(cudaMemcpy2DAsync(ws->xstage.p, sizeof(double2) * nin, xd, sizeof(double2) * ldx,
-                             sizeof(double2) * nin, b, cudaMemcpyHostToDevice, s));
-        if (usebeta)
-            CK(cudaMemcpy2DAsync(ws->ystage.p, sizeof(double2) * nout, yd, sizeof(double2) * ldy,
-                                 sizeof(double2) * nout, b, cudaMemcpyHostToDevice, s));
-        xd = ws->xstage.p;
-        yd = ws->ystage.p;
-        lx = nin;
-        ly = nout;
-    }
     mark(0);
-    k_gather<<<launch_grid(nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, I.perm.p, nin, b, vs, ws->xt.p);
-    ++launches;
-    ++stage_launch[0];
+    k_gather<<<launch_grid(nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, I.perm.p, nin, b, vs, buf.xt);
+    ++count.total;
+    ++count.stage[0];
     mark(1);
     const bool conj = mode == 2;
     auto run = [&](auto tag) {
@@ -693,7 +678,7 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
         }
         for (int q0 = 0; q0 < b; q0 += 16) {
             const int bc = std::min(16, b - q0);
-            if (ws->far) {
+            if (buf.far) {
                 // upward sweep: xhat_p = XT_p [leaf x slice | children's xhat], deepest level first
                 for (size_t l = 0; l + 1 < I.up.ptr.size(); ++l) {
                     const int cnt = I.up.ptr[l + 1] - I.up.ptr[l];
@@ -708,23 +693,23 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
                     a.cptr = I.cptr.p;
                     a.M = XTi;
                     a.moff = I.xoff.p;
-                    a.src = ws->xt.p;
-                    a.coef = ws->xhat.p;
+                    a.src = buf.xt;
+                    a.coef = buf.xhat;
                     a.b = b;
                     a.bc = bc;
                     a.q0 = q0;
                     a.vs = vs;
                     a.conj = conj && in == 0;
                     a.maxrows = I.up.mcap[l];
-                    a.error = ws->error.p;
+                    a.error = buf.error;
                     launch_rows<S>(a, I.up.d_nodes.p + I.up.ptr[l], cnt, s);
-                    ++launches;
-                    ++stage_launch[1];
+                    ++count.total;
+                    ++count.stage[1];
                 }
             }
             if (q0 == 0) mark(2);
             const int ncp = mode == 0 ? c->n_couple_fwd : c->n_couple_rev;
-            if (ws->far && ncp > 0) {
+            if (buf.far && ncp > 0) {
                 RowArgs<S> a{};
                 a.stage = STAGE_COUPLE;
                 a.M = Cm;
@@ -741,21 +726,21 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
                 a.rank_out = O.rank.p;
                 a.cptr_in = I.cptr.p;
                 a.cptr_out = O.cptr.p;
-                a.src = ws->xhat.p;
-                a.dst = ws->yhat.p;
+                a.src = buf.xhat;
+                a.dst = buf.yhat;
                 a.b = b;
                 a.bc = bc;
                 a.q0 = q0;
                 a.vs = vs;
                 a.conj = conj;
                 a.maxrows = c->maxrank;
-                a.error = ws->error.p;
+                a.error = buf.error;
                 launch_rows<S>(a, mode == 0 ? c->couple_fwd.p : c->couple_rev.p, ncp, s);
-                ++launches;
-                ++stage_launch[2];
+                ++count.total;
+                ++count.stage[2];
             }
             if (q0 == 0) mark(3);
-            if (ws->far) {
+            if (buf.far) {
                 // downward sweep: [yhat_children] += X_p yhat_p, root level first
                 for (size_t l = 0; l + 1 < O.down.ptr.size(); ++l) {
                     const int cnt = O.down.ptr[l + 1] - O.down.ptr[l];
@@ -768,17 +753,17 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
                     a.cptr = O.cptr.p;
                     a.M = Xo;
                     a.moff = O.xoff.p;
-                    a.coef = ws->yhat.p;
+                    a.coef = buf.yhat;
                     a.b = b;
                     a.bc = bc;
                     a.q0 = q0;
                     a.vs = vs;
                     a.conj = conj && out == 1;
                     a.maxrows = O.down.mcap[l];
-                    a.error = ws->error.p;
+                    a.error = buf.error;
                     launch_rows<S>(a, O.down.d_nodes.p + O.down.ptr[l], cnt, s);
-                    ++launches;
-                    ++stage_launch[3];
+                    ++count.total;
+                    ++count.stage[3];
                 }
             }
             if (q0 == 0) mark(4);
@@ -790,10 +775,10 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
             a.perm = O.perm.p;
             a.rank = O.rank.p;
             a.cptr = O.cptr.p;
-            a.X = ws->far ? Xo : nullptr;
+            a.X = buf.far ? Xo : nullptr;
             a.xoff = O.xoff.p;
-            a.coef = ws->yhat.p;
-            if (ws->near) {
+            a.coef = buf.yhat;
+            if (buf.near) {
                 a.M = Nm;
                 a.moff = mode == 0 ? c->nfoff.p : c->ntoff.p;
                 a.ptr = mode == 0 ? c->nearptr.p : c->tnearptr.p;
@@ -801,7 +786,7 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
             }
             a.o_begin = I.begin.p;
             a.o_end = I.end.p;
-            a.src = ws->xt.p;
+            a.src = buf.xt;
             a.y = yd;
             a.ldy = ly;
             a.alpha = alpha;
@@ -813,21 +798,76 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
             a.vs = vs;
             a.conj = conj;
             a.maxrows = O.leafcap;
-            a.error = ws->error.p;
+            a.error = buf.error;
             launch_rows<S>(a, O.leaves.p, O.nleaves, s);
-            ++launches;
-            ++stage_launch[4];
+            ++count.total;
+            ++count.stage[4];
         }
         mark(5);
     };
-    const int cap = rows_capacity(std::min(b, 16));
-    if (O.leafcap > cap || I.leafcap > cap || 2 * c->maxrank > cap)
-        return fail(NCA_ERR_ARG, "a leaf or transfer block has more rows than one product CTA holds");
     if (precision == NCA_PREC_F64)
         run(double2{});
     else
         run(float2{});
     CK(cudaGetLastError());
+    return NCA_OK;
+}
+
+// Argument checks shared by the product entry points.
+int check_product_args(nca_core *c, int mode, int precision, int64_t ldx, int64_t ldy, int64_t nrhs) {
+    if (mode < 0 || mode > 2) return fail(NCA_ERR_ARG, "mode must be 0 (N), 1 (T) or 2 (C)");
+    if (precision != NCA_PREC_F64 && precision != NCA_PREC_F32) return fail(NCA_ERR_ARG, "unknown precision");
+    if (precision == NCA_PREC_F32 && !c->f32)
+        return fail(NCA_ERR_ARG, "complex FP32 product requested but the core was built without store_f32");
+    const int in = mode == 0 ? 1 : 0, out = 1 - in;
+    if (nrhs < 0 || ldx < c->side[in].npts || ldy < c->side[out].npts)
+        return fail(NCA_ERR_DIM, "DimensionMismatch: leading dimension smaller than the operator size");
+    return NCA_OK;
+}
+
+int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_t ldx, void *y,
+               int64_t ldy, int64_t nrhs, double2 alpha, double2 beta, int memspace) {
+    nca_core *c = ws->core;
+    if (int st = check_product_args(c, mode, precision, ldx, ldy, nrhs)) return st;
+    const int in = mode == 0 ? 1 : 0, out = 1 - in;
+    const int64_t nin = c->side[in].npts, nout = c->side[out].npts;
+    if (nrhs == 0) return NCA_OK;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t s = ws->stream;
+    const int b = int(nrhs);
+    if (b > ws->max_nrhs) {
+        const int vsm = vector_slots(b);
+        ws->xt.alloc(size_t(std::max(c->side[0].npts, c->side[1].npts)) * vsm);
+        ws->xhat.alloc(size_t(std::max(c->side[0].h_cptr.back(), c->side[1].h_cptr.back())) * vsm);
+        ws->yhat.alloc(ws->xhat.n);
+        ws->max_nrhs = b;
+    }
+    const double2 *xd = reinterpret_cast<const double2 *>(x);
+    double2 *yd = reinterpret_cast<double2 *>(y);
+    int64_t lx = ldx, ly = ldy;
+    const bool usebeta = beta.x != 0.0 || beta.y != 0.0;
+    if (memspace == 0) {
+        if (ws->xstage.n < size_t(nin) * b) ws->xstage.alloc(size_t(nin) * b);
+        if (ws->ystage.n < size_t(nout) * b) ws->ystage.alloc(size_t(nout) * b);
+    }
+    CK(cudaEventRecord(ws->e0, s));
+    CK(cudaMemsetAsync(ws->error.p, 0, sizeof(int32_t), s));
+    if (memspace == 0) {
+        CK(cudaMemcpy2DAsync(ws->xstage.p, sizeof(double2) * nin, xd, sizeof(double2) * ldx,
+                             sizeof(double2) * nin, b, cudaMemcpyHostToDevice, s));
+        if (usebeta)
+            CK(cudaMemcpy2DAsync(ws->ystage.p, sizeof(double2) * nout, yd, sizeof(double2) * ldy,
+                                 sizeof(double2) * nout, b, cudaMemcpyHostToDevice, s));
+        xd = ws->xstage.p;
+        yd = ws->ystage.p;
+        lx = nin;
+        ly = nout;
+    }
+    const ProductBuffers buf{ws->xt.p, ws->xhat.p, ws->yhat.p, ws->error.p, ws->far, ws->near};
+    ProductLaunches count;
+    if (int st = enqueue_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, buf, s,
+                                 ws->profiling ? ws->stage_ev : nullptr, count))
+        return st;
     CK(cudaMemcpyAsync(ws->error_host, ws->error.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     if (memspace == 0)
         CK(cudaMemcpy2DAsync(y, sizeof(double2) * ldy, ws->ystage.p, sizeof(double2) * nout,
@@ -837,13 +877,13 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ws->e0, ws->e1));
     ws->last_seconds = ms * 1e-3;
-    ws->last_launches = launches;
+    ws->last_launches = count.total;
     if (ws->profiling) {
         for (int k = 0; k < 5; ++k) {
             float t = 0.f;
             CK(cudaEventElapsedTime(&t, ws->stage_ev[k], ws->stage_ev[k + 1]));
             ws->stage_seconds[k] = t * 1e-3;
-            ws->stage_launches[k] = stage_launch[k];
+            ws->stage_launches[k] = count.stage[k];
         }
     }
     if (*ws->error_host == 2) return fail(NCA_ERR_TIMEOUT, "a bounded wait in the product kernel gave up");
@@ -1095,8 +1135,8 @@ int32_t nca_workspace_create(nca_core *core, int32_t max_nrhs, nca_workspace **o
         CK(cudaEventCreate(&ws->e0));
         CK(cudaEventCreate(&ws->e1));
         int b = std::max(1, max_nrhs);
-        ws->xt.alloc(size_t(std::max(core->side[0].npts, core->side[1].npts)) * (b + 2));
-        ws->xhat.alloc(size_t(std::max(core->side[0].h_cptr.back(), core->side[1].h_cptr.back())) * (b + 2));
+        ws->xt.alloc(size_t(std::max(core->side[0].npts, core->side[1].npts)) * vector_slots(b));
+        ws->xhat.alloc(size_t(std::max(core->side[0].h_cptr.back(), core->side[1].h_cptr.back())) * vector_slots(b));
         ws->yhat.alloc(ws->xhat.n);
         ws->max_nrhs = b;
         ws->error.alloc(1);

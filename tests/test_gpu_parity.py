@@ -193,6 +193,22 @@ def test_concurrency_guard(c1):
     assert np.array_equal(A @ x, expected)
 
 
+def test_small_workspaces_padded_strides(c1):
+    """Right-hand-side counts whose padded vector stride is b + 3 (b = 3 mod 4), from workspaces
+    sized exactly for them and from one that grows."""
+    test, trial, A, H = c1
+    N = _n()
+    for b in (3, 7, 1, 2):
+        W = N.H2Workspace(N.core(A), max_nrhs=b)
+        X = cgauss((1024, b), 50 + b)
+        assert relerr(W @ X, H.apply(X, 0)) < REL
+        assert relerr(W.H @ X, H.apply(X, 2)) < REL
+    W = N.H2Workspace(N.core(A), max_nrhs=1)
+    X = cgauss((1024, 19), 60)
+    assert relerr(W @ X, H.apply(X, 0)) < REL
+    assert relerr(W.T @ X[:, :11], H.apply(X[:, :11], 1)) < REL
+
+
 def test_device_arrays(c1):
     import torch
     test, trial, A, H = c1
