@@ -151,6 +151,21 @@ void nca_workspace_destroy(nca_workspace *ws);
 int32_t nca_apply(nca_workspace *ws, int32_t mode, int32_t precision, const void *x, int64_t ldx,
                   void *y, int64_t ldy, int64_t nrhs, double alpha_re, double alpha_im,
                   double beta_re, double beta_im, int32_t memspace);
+/* Allocation-free product (no counterpart in the reference, whose products always run on an
+ * H2Workspace's own buffers): y = alpha * op(H) x + beta * y with x, y DEVICE arrays (16-byte
+ * aligned) on the caller's stream (NULL: the legacy default stream), every intermediate buffer
+ * in one fixed device array of NCA_STATIC_SCRATCH_BYTES per device that the library's module
+ * holds. The call makes no cudaMalloc/cudaFree or other allocation, for callers whose own pool
+ * owns device memory. It needs (nin + input coefficients + output coefficients) *
+ * (nrhs + 3) * 16 bytes + 1 KiB at most; larger products return NCA_ERR_ARG naming the size.
+ * The first call on a device does the one-time setup (module load, symbol lookup): make it
+ * before any stream capture on that device. The scratch is shared by every core on the device,
+ * so overlapping calls would race on it: a call made while another is in progress on the same
+ * device returns NCA_ERR_BUSY. The call waits for the stream and returns the kernels' status. */
+#define NCA_STATIC_SCRATCH_BYTES (32ull << 20)
+int32_t nca_apply_static(nca_core *core, int32_t mode, int32_t precision, const void *x, int64_t ldx,
+                         void *y, int64_t ldy, int64_t nrhs, double alpha_re, double alpha_im,
+                         double beta_re, double beta_im, void *stream);
 /* Device time of the last nca_apply of this workspace (CUDA events), in seconds. */
 int32_t nca_workspace_last_time(const nca_workspace *ws, double *seconds);
 /* Kernel launches of the last nca_apply of this workspace. */

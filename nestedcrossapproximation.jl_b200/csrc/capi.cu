@@ -8,6 +8,7 @@
 #include <chrono>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <type_traits>
 #include <stdexcept>
@@ -891,6 +892,87 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     return NCA_OK;
 }
 
+// ---- allocation-free product ------------------------------------------------------------
+// Callers that cannot allocate device memory: a host whose own pool (Julia's CUDA.jl, PyTorch's
+// caching allocator) has reserved nearly all of HBM, so a cudaMalloc inside the library fails or
+// fragments the pool, and callers on a path that must not synchronise on cudaMalloc/cudaFree.
+// nca_apply_static keeps every intermediate buffer of the product (gathered input, xhat, yhat,
+// error word) in this file-scope array instead: NCA_STATIC_SCRATCH_BYTES per device, allocated
+// once when the module is loaded, never by the call.
+static __device__ __align__(256) unsigned char g_static_scratch[NCA_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_static_setup;
+void *g_static_base[kMaxStaticDevices] = {};
+std::atomic<bool> g_static_busy[kMaxStaticDevices];
+
+inline size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+// Device address of this device's scratch array; the first call per device looks it up (with
+// that device current), which loads the module holding the array.
+int static_scratch_base(int device, unsigned char **base) {
+    std::lock_guard<std::mutex> lock(g_static_setup);
+    if (!g_static_base[device]) {
+        void *p = nullptr;
+        const cudaError_t rc = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (rc != cudaSuccess)
+            return fail(NCA_ERR_CUDA, std::string("cudaGetSymbolAddress(static product scratch): ") +
+                                          cudaGetErrorString(rc));
+        g_static_base[device] = p;
+    }
+    *base = static_cast<unsigned char *>(g_static_base[device]);
+    return NCA_OK;
+}
+
+int apply_static_impl(nca_core *c, int mode, int precision, const void *x, int64_t ldx, void *y, int64_t ldy,
+                      int64_t nrhs, double2 alpha, double2 beta, cudaStream_t s) {
+    if (int st = check_product_args(c, mode, precision, ldx, ldy, nrhs)) return st;
+    if (nrhs == 0) return NCA_OK;
+    if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15)
+        return fail(NCA_ERR_ARG, "x and y must be 16-byte aligned device arrays");
+    const int in = mode == 0 ? 1 : 0, out = 1 - in;
+    const int b = int(std::min<int64_t>(nrhs, 1 << 30));
+    const size_t vs = size_t(vector_stride(b));
+    // layout: error word | xt (nin x vs) | xhat (input coefficients x vs) | yhat (output coefficients x vs)
+    const size_t o_xt = 256;
+    const size_t o_xhat = o_xt + align256(sizeof(double2) * size_t(c->side[in].npts) * vs);
+    const size_t o_yhat = o_xhat + align256(sizeof(double2) * size_t(c->side[in].h_cptr.back()) * vs);
+    const size_t need = o_yhat + align256(sizeof(double2) * size_t(c->side[out].h_cptr.back()) * vs);
+    if (nrhs != b || need > size_t(NCA_STATIC_SCRATCH_BYTES))
+        return fail(NCA_ERR_ARG, "nca_apply_static: " + std::to_string(nrhs) + " right-hand sides need " +
+                                     std::to_string(need) + " bytes of scratch, more than the fixed " +
+                                     std::to_string(size_t(NCA_STATIC_SCRATCH_BYTES)) +
+                                     " (NCA_STATIC_SCRATCH_BYTES); use nca_apply or fewer right-hand sides");
+    if (c->device < 0 || c->device >= kMaxStaticDevices)
+        return fail(NCA_ERR_ARG, "nca_apply_static supports devices 0..63");
+    CK(cudaSetDevice(c->device));
+    unsigned char *base = nullptr;
+    if (int st = static_scratch_base(c->device, &base)) return st;
+    bool expected = false;
+    if (!g_static_busy[c->device].compare_exchange_strong(expected, true))
+        return fail(NCA_ERR_BUSY, "nca_apply_static: another call on this device is using the static scratch");
+    struct Release {
+        std::atomic<bool> &flag;
+        ~Release() { flag.store(false); }
+    } release{g_static_busy[c->device]};
+    const ProductBuffers buf{reinterpret_cast<double2 *>(base + o_xt), reinterpret_cast<double2 *>(base + o_xhat),
+                             reinterpret_cast<double2 *>(base + o_yhat), reinterpret_cast<int32_t *>(base), true,
+                             true};
+    // Only the error word must start at zero: every xt row is gathered, every xhat / yhat block
+    // is written (up sweep, coupling) before it is read.
+    CK(cudaMemsetAsync(buf.error, 0, sizeof(int32_t), s));
+    ProductLaunches count;
+    if (int st = enqueue_product(c, mode, precision, reinterpret_cast<const double2 *>(x), ldx,
+                                 reinterpret_cast<double2 *>(y), ldy, b, alpha, beta, buf, s, nullptr, count))
+        return st;
+    int32_t err = 0;
+    CK(cudaMemcpyAsync(&err, buf.error, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (err == 2) return fail(NCA_ERR_TIMEOUT, "a bounded wait in the product kernel gave up");
+    if (err != 0) return fail(NCA_ERR_CUDA, "internal: a product copy was misaligned and skipped");
+    return NCA_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1171,6 +1253,16 @@ int32_t nca_apply(nca_workspace *ws, int32_t mode, int32_t precision, const void
     });
     ws->busy.store(false);
     return st;
+}
+
+int32_t nca_apply_static(nca_core *core, int32_t mode, int32_t precision, const void *x, int64_t ldx, void *y,
+                         int64_t ldy, int64_t nrhs, double alpha_re, double alpha_im, double beta_re,
+                         double beta_im, void *stream) {
+    if (!core) return fail(NCA_ERR_ARG, "null core");
+    return guarded([&] {
+        return apply_static_impl(core, mode, precision, x, ldx, y, ldy, nrhs, make_double2(alpha_re, alpha_im),
+                                 make_double2(beta_re, beta_im), static_cast<cudaStream_t>(stream));
+    });
 }
 
 int32_t nca_workspace_last_time(const nca_workspace *ws, double *seconds) {

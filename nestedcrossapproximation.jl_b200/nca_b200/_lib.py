@@ -93,6 +93,7 @@ SIGNATURES = {
     "nca_workspace_create": (I32, [P, I32, P]),
     "nca_workspace_destroy": (None, [P]),
     "nca_apply": (I32, [P, I32, I32, P, I64, P, I64, I64, D, D, D, D, I32]),
+    "nca_apply_static": (I32, [P, I32, I32, P, I64, P, I64, I64, D, D, D, D, P]),
     "nca_workspace_last_time": (I32, [P, P]),
     "nca_workspace_last_launches": (I32, [P, P]),
     "nca_workspace_set_parts": (I32, [P, I32, I32]),
