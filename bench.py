@@ -95,7 +95,7 @@ def peaks():
 
 def traffic_from_profiles():
     """DRAM bytes per launch of the leaf kernel from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "k_leaves_galerkin_sphere.md")
+    path = os.path.join(ROOT, "profiles", "k_rows_leaves_galerkin_sphere.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -348,7 +348,7 @@ def main():
     peak, peak_kind = peaks()
     leaves_avg = stage_sum["leaves"] / max(stage_n["leaves"], 1)
     achieved = stage_bytes(info, b, 8 if f32 else E) / leaves_avg / 1e9 if leaves_avg > 0 else None
-    roofline = {"kernel": "k_leaves (near field + leaf bases + scatter)", "bound": "hbm", "achieved": achieved,
+    roofline = {"kernel": "k_rows_leaves (near field + leaf bases + scatter)", "bound": "hbm", "achieved": achieved,
                 "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                 "traffic": traffic_from_profiles(), "launch_ms": 1e3 * leaves_avg,
                 "share_of_step": stage_sum["leaves"] / max(sum(stage_sum.values()), 1e-30), "top_stage": top}
