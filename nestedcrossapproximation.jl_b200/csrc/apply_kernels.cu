@@ -13,9 +13,10 @@
 //   leaves   y_t = X_t yhat_t + sum_s N_ts x_s (reverse: from the transposed near blocks NT),
 //            scattered straight into the caller's layout.
 //
-// CTA = 8 consumer warps + 1 producer warp. The producer streams tiles through a 4-stage
-// shared-memory ring with cp.async.bulk (bulk copies completing on a "full" mbarrier); the
-// consumers release stages on an "empty" mbarrier. Complex FP64 tiles go through the FP64
+// CTA = 8 consumer warps + 1 producer warp. The producer streams tiles through a 3-stage
+// shared-memory ring with cp.async.bulk (bulk copies completing on a "full" mbarrier), filling
+// each stage with columns of successive segments; the consumers release stages on an "empty"
+// mbarrier. Complex FP64 tiles go through the FP64
 // tensor-core MMA (mma.m8n8k4.f64) with three real products per complex product
 // (Re = ArBr - AiBi, Im = (Ar+Ai)(Br+Bi) - ArBr - AiBi); complex FP32 tiles use FMA. Output
 // tiles of 8 rows x 8 right-hand sides are spread over the warps; when a node has fewer
@@ -36,9 +37,7 @@ namespace {
 constexpr int NCONS = 8;              // consumer warps
 constexpr int NT = (NCONS + 1) * 32;  // + one producer warp
 constexpr int NSTAGE = 3;
-constexpr int CAPM = 18432;  // bytes of matrix tile per stage
-constexpr int CAPV = 5120;   // bytes of vector tile per stage
-constexpr int STAGE_BYTES = CAPM + CAPV;
+constexpr int STAGE_BYTES = 23552;  // one ring stage: w matrix columns, then w vector rows
 
 // Shared-memory strides (in 16-byte elements) that are 2 mod 4: the four lanes of an MMA
 // fragment row then hit four different bank groups.
@@ -54,9 +53,8 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
+__device__ __forceinline__ void mbar_expect_tx_only(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
     asm volatile(
@@ -201,50 +199,58 @@ struct Acc<float2, MAXT> {
     __device__ double2 value(int u, int h) const { return make_double2(c[u][h].x, c[u][h].y); }
 };
 
-// Output tiles of one consumer warp. The R x bc output is cut into 8 x 8 tiles spread over the
-// 8 consumer warps; when there are fewer tiles than warps, the columns are split into kgroups
-// interleaved groups of k-steps and the groups are summed at the end.
+// Output tiles of one consumer warp. The R x bc output is cut into row tiles of 8 rows; a warp
+// owns whole row tiles (all column tiles of 8 right-hand sides, so one A fragment serves them
+// all): row tiles w, w + 8, ... When there are fewer row tiles than warps, the columns are split
+// into kgroups interleaved groups of k-steps and the groups are summed at the end.
 template <int MAXT>
 struct TileMap {
     int n, kgroups, mykg;
     int arow[MAXT];  // output row of this lane's A fragment (or -1 past the block)
     int bcol[MAXT];  // right-hand side of this lane's B fragment (or -1)
-    int ocol[MAXT];              // first right-hand side of the tile
-    bool reuse[MAXT];            // same A rows as the previous tile
+    int ocol[MAXT];  // first right-hand side of the tile
+    bool reuse[MAXT];  // same A rows as the previous tile
     __device__ void init(int R, int bc, int warp, int g) {
         const int MT = (R + 7) >> 3, NTL = (bc + 7) >> 3;
-        const int tiles = MT * NTL;
-        kgroups = tiles >= NCONS ? 1 : NCONS / (tiles > 0 ? tiles : 1);
-        const int ntw = (tiles + NCONS - 1) / NCONS;
-        mykg = kgroups > 1 ? warp / (tiles > 0 ? tiles : 1) : 0;
-        const bool busy = kgroups > 1 ? warp < tiles * kgroups : warp < tiles;
+        const int mt1 = MT > 0 ? MT : 1, ntl1 = NTL > 0 ? NTL : 1;
+        kgroups = MT >= NCONS ? 1 : NCONS / mt1;
+        mykg = kgroups > 1 ? warp / mt1 : 0;
+        const int rt0 = kgroups > 1 ? warp % mt1 : warp;
+        const bool busy = MT > 0 && NTL > 0 && (kgroups > 1 ? warp < MT * kgroups : warp < MT);
         n = 0;
 #pragma unroll
         for (int u = 0; u < MAXT; ++u) {
-            const int t = kgroups > 1 ? warp % (tiles > 0 ? tiles : 1) : warp + u * NCONS;
-            const bool ok = busy && u < (kgroups > 1 ? 1 : ntw) && t < tiles;
-            const int mt = ok ? t % MT : 0, nt = ok ? t / MT : 0;
+            const int j = u / ntl1, nt = u % ntl1;
+            const int rt = rt0 + j * NCONS;
+            const bool ok = busy && (kgroups == 1 || j == 0) && rt < MT;
             ocol[u] = nt * 8;
-            arow[u] = (ok && mt * 8 + g < R) ? mt * 8 + g : -1;
+            arow[u] = (ok && rt * 8 + g < R) ? rt * 8 + g : -1;
             bcol[u] = (ok && nt * 8 + g < bc) ? nt * 8 + g : -1;
-            reuse[u] = u > 0 && ok && kgroups == 1 && ((t - NCONS) % MT) == mt;
+            reuse[u] = ok && nt > 0;
             if (ok) n = u + 1;
         }
     }
 };
 
+// Output tiles a consumer warp holds for R rows and bc right-hand sides (picks MAXT).
+inline int tiles_per_warp(int R, int bc) {
+    const int MT = (R + 7) / 8, NTL = (bc + 7) / 8;
+    return ((MT + NCONS - 1) / NCONS) * NTL;
+}
+
 // One chunk (w columns) of the consumer warp's tiles.
 template <typename S, int MAXT>
 __device__ __forceinline__ void consume(Acc<S, MAXT> &acc, const TileMap<MAXT> &tm, const unsigned char *tile, int w,
-                                        int R, int ldm, int bc, int ldv, int g, int tq, double sgn) {
+                                        int voff, int R, int ldm, int bc, int ldv, int g, int tq, double sgn) {
     if constexpr (std::is_same<S, double2>::value) {
         const double2 *Ms = reinterpret_cast<const double2 *>(tile);
-        const double2 *Vs = reinterpret_cast<const double2 *>(tile + CAPM);
+        const double2 *Vs = reinterpret_cast<const double2 *>(tile + voff);
         constexpr int NSET = Acc<S, MAXT>::NSET;
         const int step = 4 * tm.kgroups;
         for (int k0 = tm.mykg * 4; k0 < w; k0 += NSET * step) {
 #pragma unroll
             for (int p = 0; p < NSET; ++p) {
+                if (k0 + p * step >= w) break;  // warp-uniform: no MMA on columns past the chunk
                 const int kk = k0 + p * step + tq;
                 const bool in = kk < w;
                 double2 av = make_double2(0.0, 0.0);
@@ -262,7 +268,7 @@ __device__ __forceinline__ void consume(Acc<S, MAXT> &acc, const TileMap<MAXT> &
         }
     } else {
         const float2 *Ms = reinterpret_cast<const float2 *>(tile);
-        const double2 *Vs = reinterpret_cast<const double2 *>(tile + CAPM);
+        const double2 *Vs = reinterpret_cast<const double2 *>(tile + voff);
         const float fs = float(sgn);
         for (int k = tm.mykg; k < w; k += tm.kgroups) {
 #pragma unroll
@@ -286,10 +292,11 @@ __device__ __forceinline__ void consume(Acc<S, MAXT> &acc, const TileMap<MAXT> &
 
 int rows_capacity(int bc) {
     // at most 8 tiles of 8 x 8 per warp over 8 warps (R * ceil(bc / 8) <= 512); 4 padded complex
-    // FP64 columns must fit one matrix tile; the partial sums (R x bc) must fit the ring
+    // FP64 columns and their vector rows must fit one stage; the partial sums (R x bc) must fit
+    // the ring
     const int ntl = (bc + 7) / 8;
     const int by_tiles = 512 / (ntl > 0 ? ntl : 1);
-    const int by_tile_bytes = CAPM / (4 * 16) - 2;
+    const int by_tile_bytes = STAGE_BYTES / (4 * 16) - conflict_free(bc) - 3;
     const int by_ring = NSTAGE * STAGE_BYTES / (16 * (bc > 0 ? bc : 1));
     int cap = by_tiles < by_tile_bytes ? by_tiles : by_tile_bytes;
     return cap < by_ring ? cap : by_ring;
@@ -310,11 +317,17 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
     const int ldm = f64 ? conflict_free(R) : R;
     const bool vwhole = bc == a.b;
     const int ldv = vwhole ? a.vs : conflict_free(bc);
-    int wmax = R > 0 ? CAPM / (ldm * elem) : CAPV;
-    const int wv = CAPV / (ldv * 16);
-    if (wv < wmax) wmax = wv;
-    if (!f64) wmax &= ~3;  // FP32: whole k-steps keep interior chunks 16-byte multiples
+    // columns per stage: matrix columns first, the vector rows at voff (16-byte aligned). FP64
+    // chunks are whole groups of 8 columns (two k-steps of 4, one per accumulator set); FP32
+    // chunks whole k-steps, so interior chunks stay 16-byte multiples.
+    int wmax = STAGE_BYTES / (ldm * elem + ldv * 16);
+    wmax &= f64 ? (wmax >= 8 ? ~7 : ~0) : ~3;
     if (wmax < 4) wmax = 4;
+    int voff = (wmax * ldm * elem + 15) & ~15;
+    while (wmax > 4 && voff + wmax * ldv * 16 > STAGE_BYTES) {
+        wmax -= 4;
+        voff = (wmax * ldm * elem + 15) & ~15;
+    }
 
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; ++s) {
@@ -354,48 +367,57 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
                     break;
                 }
                 if (*abort_flag) break;
-                while (k < nseg && c0 >= gs.w) {
-                    ++k;
-                    c0 = 0;
-                    gs = gnext;
-                    if (k + 1 < nseg) gnext = segment<S, STAGE>(a, o, k + 1);
+                unsigned char *tile = smem + s * STAGE_BYTES;
+                // FP64: the stage is filled with columns of successive segments (one copy per
+                // matrix column, so pieces pack at any column); FP32 tiles are one piece each.
+                int filled = 0;
+                while (filled < wmax) {
+                    while (k < nseg && c0 >= gs.w) {
+                        ++k;
+                        c0 = 0;
+                        gs = gnext;
+                        if (k + 1 < nseg) gnext = segment<S, STAGE>(a, o, k + 1);
+                    }
+                    if (k >= nseg) break;
+                    int w = gs.w - c0;
+                    if (w > wmax - filled) w = wmax - filled;
+                    const S *msrc = gs.M + int64_t(c0) * R;
+                    const double2 *vsrc = gs.v + int64_t(c0) * a.vs + a.q0;
+                    c0 += w;
+                    if (((reinterpret_cast<uintptr_t>(msrc) | reinterpret_cast<uintptr_t>(vsrc)) & 15u) != 0) {
+                        ctl.err = 1;  // never issue an unaligned bulk copy: skip this piece
+                        continue;
+                    }
+                    const uint32_t vrow = uint32_t(bc) * 16u;
+                    const uint32_t vbytes = vwhole ? uint32_t(w) * uint32_t(a.vs) * 16u : vrow * uint32_t(w);
+                    unsigned char *mdst = tile + filled * ldm * elem;
+                    unsigned char *vdst = tile + voff + filled * ldv * 16;
+                    if (f64) {
+                        const uint32_t col = uint32_t(R) * 16u;
+                        mbar_expect_tx_only(&ctl.full[s], col * uint32_t(w) + vbytes);
+                        for (int j = 0; j < w; ++j)
+                            bulk_g2s(mdst + j * ldm * 16, msrc + int64_t(j) * R, col, &ctl.full[s]);
+                    } else {
+                        const uint32_t mbytes = (uint32_t(R) * uint32_t(w) * uint32_t(elem) + 15u) & ~15u;
+                        mbar_expect_tx_only(&ctl.full[s], mbytes + vbytes);
+                        if (mbytes) bulk_g2s(mdst, msrc, mbytes, &ctl.full[s]);
+                    }
+                    if (vwhole) {
+                        bulk_g2s(vdst, vsrc, vbytes, &ctl.full[s]);
+                    } else {
+                        for (int j = 0; j < w; ++j)
+                            bulk_g2s(vdst + j * ldv * 16, vsrc + int64_t(j) * a.vs, vrow, &ctl.full[s]);
+                    }
+                    filled += w;
+                    if (!f64) break;
                 }
-                if (k >= nseg) {
+                if (filled == 0 && k >= nseg) {
                     ctl.w[s] = -1;
                     mbar_arrive(&ctl.full[s]);
                     break;
                 }
-                int w = gs.w - c0;
-                if (w > wmax) w = wmax;
-                const S *msrc = gs.M + int64_t(c0) * R;
-                const double2 *vsrc = gs.v + int64_t(c0) * a.vs + a.q0;
-                c0 += w;
-                const uint32_t mbytes = (uint32_t(R) * uint32_t(w) * uint32_t(elem) + 15u) & ~15u;
-                const uint32_t vrow = uint32_t(bc) * 16u;
-                const uint32_t vbytes = vwhole ? uint32_t(w) * uint32_t(a.vs) * 16u : vrow * uint32_t(w);
-                unsigned char *tile = smem + s * STAGE_BYTES;
-                if (((reinterpret_cast<uintptr_t>(msrc) | reinterpret_cast<uintptr_t>(vsrc)) & 15u) != 0) {
-                    ctl.err = 1;  // never issue an unaligned bulk copy: skip this chunk
-                    ctl.w[s] = 0;
-                    mbar_arrive(&ctl.full[s]);
-                    continue;
-                }
-                ctl.w[s] = w;
-                if (f64) {
-                    const uint32_t col = uint32_t(R) * 16u;
-                    mbar_expect_tx(&ctl.full[s], col * uint32_t(w) + vbytes);
-                    for (int j = 0; j < w; ++j)
-                        bulk_g2s(tile + j * ldm * 16, msrc + int64_t(j) * R, col, &ctl.full[s]);
-                } else {
-                    mbar_expect_tx(&ctl.full[s], mbytes + vbytes);
-                    if (mbytes) bulk_g2s(tile, msrc, mbytes, &ctl.full[s]);
-                }
-                if (vwhole) {
-                    bulk_g2s(tile + CAPM, vsrc, vbytes, &ctl.full[s]);
-                } else {
-                    for (int j = 0; j < w; ++j)
-                        bulk_g2s(tile + CAPM + j * ldv * 16, vsrc + int64_t(j) * a.vs, vrow, &ctl.full[s]);
-                }
+                ctl.w[s] = filled;
+                mbar_arrive(&ctl.full[s]);
             }
         }
         __syncwarp();
@@ -409,7 +431,7 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
             }
             const int w = ctl.w[s];
             if (w < 0 || *abort_flag) break;
-            if (tm.n > 0) consume<S, MAXT>(acc, tm, smem + s * STAGE_BYTES, w, R, ldm, bc, ldv, g, tq, sgn);
+            if (tm.n > 0) consume<S, MAXT>(acc, tm, smem + s * STAGE_BYTES, w, voff, R, ldm, bc, ldv, g, tq, sgn);
             __syncwarp();
             if (lane == 0) mbar_arrive(&ctl.empty[s]);
         }
@@ -535,8 +557,7 @@ void launch_maxt(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStrea
 template <typename S>
 void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
     if (count <= 0) return;
-    const int tiles = ((a.maxrows + 7) / 8) * ((a.bc + 7) / 8);
-    const int per_warp = (tiles + NCONS - 1) / NCONS;
+    const int per_warp = tiles_per_warp(a.maxrows, a.bc);
     if (per_warp <= 2)
         launch_maxt<S, 2>(a, nodes, count, s);
     else if (per_warp <= 4)
