@@ -160,24 +160,27 @@ struct Ctl {
     int err;
 };
 
-// Per-warp accumulators (MAXT output tiles of 8 x 8): three real products per tile for
-// FP64, complex FMA for FP32.
-template <typename S, int MAXT>
+// Per-warp accumulators: NRT row tiles x NTL column tiles of 8 x 8 outputs. FP64: the three
+// real products of the 3M complex product per tile (c1 = Ar Br, c2 = Ai Bi, c3 = (Ar + s Ai)
+// (Br + Bi) with s = -1 for the conjugate), in two independent sets (even / odd k-steps) when a
+// warp holds a single tile. FP32: complex FMA.
+template <typename S, int NRT, int NTL>
 struct Acc;
-template <int MAXT>
-struct Acc<double2, MAXT> {
-    // with few tiles per warp, two independent sets (even / odd k-steps) double the chains in flight
-    static constexpr int NSET = MAXT <= 2 ? 2 : 1;
-    double c1[NSET][MAXT][2], c2[NSET][MAXT][2], c3[NSET][MAXT][2];
+template <int NRT, int NTL>
+struct Acc<double2, NRT, NTL> {
+    static constexpr int T = NRT * NTL;
+    static constexpr int NSET = T <= 1 ? 2 : 1;
+    double c1[NSET][T][2], c2[NSET][T][2], c3[NSET][T][2];
     __device__ void zero() {
 #pragma unroll
         for (int p = 0; p < NSET; ++p)
 #pragma unroll
-            for (int u = 0; u < MAXT; ++u)
+            for (int u = 0; u < T; ++u)
 #pragma unroll
                 for (int h = 0; h < 2; ++h) c1[p][u][h] = c2[p][u][h] = c3[p][u][h] = 0.0;
     }
-    __device__ double2 value(int u, int h) const {
+    // Re = c1 - s c2, Im = c3 - c1 - s c2 (s = +1: A B; s = -1: conj(A) B)
+    __device__ double2 value(int u, int h, double sgn) const {
         double r1 = 0.0, r2 = 0.0, r3 = 0.0;
 #pragma unroll
         for (int p = 0; p < NSET; ++p) {
@@ -185,86 +188,96 @@ struct Acc<double2, MAXT> {
             r2 += c2[p][u][h];
             r3 += c3[p][u][h];
         }
-        return make_double2(r1 - r2, r3 - r1 - r2);
+        const double t = sgn * r2;
+        return make_double2(r1 - t, r3 - r1 - t);
     }
 };
 
-template <int MAXT>
-struct Acc<float2, MAXT> {
-    float2 c[MAXT][2];
+template <int NRT, int NTL>
+struct Acc<float2, NRT, NTL> {
+    static constexpr int T = NRT * NTL;
+    float2 c[T][2];
     __device__ void zero() {
 #pragma unroll
-        for (int u = 0; u < MAXT; ++u) c[u][0] = c[u][1] = make_float2(0.f, 0.f);
+        for (int u = 0; u < T; ++u) c[u][0] = c[u][1] = make_float2(0.f, 0.f);
     }
-    __device__ double2 value(int u, int h) const { return make_double2(c[u][h].x, c[u][h].y); }
+    __device__ double2 value(int u, int h, double) const { return make_double2(c[u][h].x, c[u][h].y); }
 };
 
 // Output tiles of one consumer warp. The R x bc output is cut into row tiles of 8 rows; a warp
-// owns whole row tiles (all column tiles of 8 right-hand sides, so one A fragment serves them
-// all): row tiles w, w + 8, ... When there are fewer row tiles than warps, the columns are split
-// into kgroups interleaved groups of k-steps and the groups are summed at the end.
-template <int MAXT>
+// owns whole row tiles (all NTL column tiles of 8 right-hand sides, so one A fragment serves
+// them all): row tiles rt0, rt0 + 8, ... (nrt of them, at most NRT). When there are fewer row
+// tiles than warps, the columns are split into kgroups interleaved groups of k-steps and the
+// groups are summed at the end.
 struct TileMap {
-    int n, kgroups, mykg;
-    int arow[MAXT];  // output row of this lane's A fragment (or -1 past the block)
-    int bcol[MAXT];  // right-hand side of this lane's B fragment (or -1)
-    int ocol[MAXT];  // first right-hand side of the tile
-    bool reuse[MAXT];  // same A rows as the previous tile
-    __device__ void init(int R, int bc, int warp, int g) {
-        const int MT = (R + 7) >> 3, NTL = (bc + 7) >> 3;
-        const int mt1 = MT > 0 ? MT : 1, ntl1 = NTL > 0 ? NTL : 1;
+    int kgroups, mykg, rt0, nrt;
+    __device__ void init(int R, int warp) {
+        const int MT = (R + 7) >> 3;
+        const int mt1 = MT > 0 ? MT : 1;
         kgroups = MT >= NCONS ? 1 : NCONS / mt1;
         mykg = kgroups > 1 ? warp / mt1 : 0;
-        const int rt0 = kgroups > 1 ? warp % mt1 : warp;
-        const bool busy = MT > 0 && NTL > 0 && (kgroups > 1 ? warp < MT * kgroups : warp < MT);
-        n = 0;
-#pragma unroll
-        for (int u = 0; u < MAXT; ++u) {
-            const int j = u / ntl1, nt = u % ntl1;
-            const int rt = rt0 + j * NCONS;
-            const bool ok = busy && (kgroups == 1 || j == 0) && rt < MT;
-            ocol[u] = nt * 8;
-            arow[u] = (ok && rt * 8 + g < R) ? rt * 8 + g : -1;
-            bcol[u] = (ok && nt * 8 + g < bc) ? nt * 8 + g : -1;
-            reuse[u] = ok && nt > 0;
-            if (ok) n = u + 1;
-        }
+        rt0 = kgroups > 1 ? warp % mt1 : warp;
+        const bool busy = MT > 0 && (kgroups > 1 ? warp < MT * kgroups : warp < MT);
+        nrt = !busy ? 0 : kgroups > 1 ? 1 : (MT - rt0 + NCONS - 1) / NCONS;
     }
+    __device__ int row(int j, int g) const { return (rt0 + j * NCONS) * 8 + g; }
 };
 
-// Output tiles a consumer warp holds for R rows and bc right-hand sides (picks MAXT).
-inline int tiles_per_warp(int R, int bc) {
-    const int MT = (R + 7) / 8, NTL = (bc + 7) / 8;
-    return ((MT + NCONS - 1) / NCONS) * NTL;
-}
-
-// One chunk (w columns) of the consumer warp's tiles.
-template <typename S, int MAXT>
-__device__ __forceinline__ void consume(Acc<S, MAXT> &acc, const TileMap<MAXT> &tm, const unsigned char *tile, int w,
+// One chunk (w columns, tile at smem offset 0, vectors at voff) of the consumer warp's tiles.
+// FP64 operands of full k-steps are loaded without checks: A rows past R and B columns past bc
+// only reach outputs that are never stored (each C row / column depends on its own A row / B
+// column alone), so their addresses are clamped into the block. Only k-steps that cross the
+// chunk end need zeros (a k past w would reach every output).
+template <typename S, int NRT, int NTL>
+__device__ __forceinline__ void consume(Acc<S, NRT, NTL> &acc, const TileMap &tm, const unsigned char *tile, int w,
                                         int voff, int R, int ldm, int bc, int ldv, int g, int tq, double sgn) {
     if constexpr (std::is_same<S, double2>::value) {
         const double2 *Ms = reinterpret_cast<const double2 *>(tile);
         const double2 *Vs = reinterpret_cast<const double2 *>(tile + voff);
-        constexpr int NSET = Acc<S, MAXT>::NSET;
+        constexpr int NSET = Acc<S, NRT, NTL>::NSET;
         const int step = 4 * tm.kgroups;
-        for (int k0 = tm.mykg * 4; k0 < w; k0 += NSET * step) {
+        int ar[NRT], bcl[NTL];
 #pragma unroll
-            for (int p = 0; p < NSET; ++p) {
-                if (k0 + p * step >= w) break;  // warp-uniform: no MMA on columns past the chunk
-                const int kk = k0 + p * step + tq;
-                const bool in = kk < w;
-                double2 av = make_double2(0.0, 0.0);
+        for (int j = 0; j < NRT; ++j) {
+            const int r = tm.row(j, g);
+            ar[j] = r < R ? r : R - 1;
+        }
 #pragma unroll
-                for (int u = 0; u < MAXT; ++u) {
-                    if (u >= tm.n) break;
-                    if (!tm.reuse[u]) av = (in && tm.arow[u] >= 0) ? Ms[tm.arow[u] + kk * ldm] : make_double2(0.0, 0.0);
-                    const double2 bv = (in && tm.bcol[u] >= 0) ? Vs[kk * ldv + tm.bcol[u]] : make_double2(0.0, 0.0);
-                    const double ai = sgn < 0.0 ? -av.y : av.y;  // a select, not an FP64 multiply
-                    dmma(acc.c1[p][u][0], acc.c1[p][u][1], av.x, bv.x);
-                    dmma(acc.c2[p][u][0], acc.c2[p][u][1], ai, bv.y);
-                    dmma(acc.c3[p][u][0], acc.c3[p][u][1], av.x + ai, bv.x + bv.y);
+        for (int t = 0; t < NTL; ++t) bcl[t] = t * 8 + g < bc ? t * 8 + g : bc - 1;
+        auto kstep = [&](int p, int kk, bool full) {
+            double2 bv[NTL];
+            double bs[NTL];
+#pragma unroll
+            for (int t = 0; t < NTL; ++t) {
+                bv[t] = (full || kk < w) ? Vs[kk * ldv + bcl[t]] : make_double2(0.0, 0.0);
+                bs[t] = bv[t].x + bv[t].y;
+            }
+#pragma unroll
+            for (int j = 0; j < NRT; ++j) {
+                if (NRT > 1 && j >= tm.nrt) break;
+                const double2 av = (full || kk < w) ? Ms[ar[j] + kk * ldm] : make_double2(0.0, 0.0);
+                const double as = fma(sgn, av.y, av.x);
+#pragma unroll
+                for (int t = 0; t < NTL; ++t) {
+                    const int u = j * NTL + t;
+                    dmma(acc.c1[p][u][0], acc.c1[p][u][1], av.x, bv[t].x);
+                    dmma(acc.c2[p][u][0], acc.c2[p][u][1], av.y, bv[t].y);
+                    dmma(acc.c3[p][u][0], acc.c3[p][u][1], as, bs[t]);
                 }
             }
+        };
+        int k0 = tm.mykg * 4;
+        // whole sets: every set of the group ends inside the chunk
+        for (; k0 + (NSET - 1) * step + 4 <= w; k0 += NSET * step) {
+#pragma unroll
+            for (int p = 0; p < NSET; ++p) kstep(p, k0 + p * step + tq, true);
+        }
+        // the rest of the chunk: sets that start inside it, with zeros past w
+#pragma unroll
+        for (int p = 0; p < NSET; ++p) {
+            const int kb = k0 + p * step;
+            if (kb >= w) break;
+            kstep(p, kb + tq, kb + 4 <= w);
         }
     } else {
         const float2 *Ms = reinterpret_cast<const float2 *>(tile);
@@ -272,16 +285,19 @@ __device__ __forceinline__ void consume(Acc<S, MAXT> &acc, const TileMap<MAXT> &
         const float fs = float(sgn);
         for (int k = tm.mykg; k < w; k += tm.kgroups) {
 #pragma unroll
-            for (int u = 0; u < MAXT; ++u) {
-                if (u >= tm.n) break;
-                const int row = tm.arow[u];
-                float2 m = row >= 0 ? Ms[row + k * ldm] : make_float2(0.f, 0.f);
+            for (int j = 0; j < NRT; ++j) {
+                if (j >= tm.nrt) break;
+                const int row = tm.row(j, g);
+                float2 m = row < R ? Ms[row + k * ldm] : make_float2(0.f, 0.f);
                 m.y *= fs;
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int col = tm.ocol[u] + 2 * tq + h;
-                    const double2 xv = col < bc ? Vs[k * ldv + col] : make_double2(0.0, 0.0);
-                    cfma(acc.c[u][h], m, make_float2(float(xv.x), float(xv.y)));
+                for (int t = 0; t < NTL; ++t) {
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int col = t * 8 + 2 * tq + h;
+                        const double2 xv = col < bc ? Vs[k * ldv + col] : make_double2(0.0, 0.0);
+                        cfma(acc.c[j * NTL + t][h], m, make_float2(float(xv.x), float(xv.y)));
+                    }
                 }
             }
         }
@@ -302,7 +318,7 @@ int rows_capacity(int bc) {
     return cap < by_ring ? cap : by_ring;
 }
 
-template <typename S, int STAGE, int MAXT>
+template <typename S, int STAGE, int NRT, int NTL>
 __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *nodes) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ Ctl ctl;
@@ -342,10 +358,10 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
 
     const int g = lane >> 2, tq = lane & 3;
     volatile int *abort_flag = &ctl.abort;
-    Acc<S, MAXT> acc;
+    Acc<S, NRT, NTL> acc;
     acc.zero();
-    TileMap<MAXT> tm;
-    tm.init(R, bc, warp < NCONS ? warp : 0, g);
+    TileMap tm;
+    tm.init(R, warp < NCONS ? warp : 0);
     const double sgn = a.conj ? -1.0 : 1.0;
 
     if (warp == NCONS) {
@@ -431,7 +447,7 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
             }
             const int w = ctl.w[s];
             if (w < 0 || *abort_flag) break;
-            if (tm.n > 0) consume<S, MAXT>(acc, tm, smem + s * STAGE_BYTES, w, voff, R, ldm, bc, ldv, g, tq, sgn);
+            if (tm.nrt > 0) consume<S, NRT, NTL>(acc, tm, smem + s * STAGE_BYTES, w, voff, R, ldm, bc, ldv, g, tq, sgn);
             __syncwarp();
             if (lane == 0) mbar_arrive(&ctl.empty[s]);
         }
@@ -441,14 +457,17 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
     double2 *red = reinterpret_cast<double2 *>(smem);
     if (!aborted && warp < NCONS) {
 #pragma unroll
-        for (int u = 0; u < MAXT; ++u) {
-            if (u >= tm.n) break;
-            const int row = tm.arow[u];  // C fragment rows equal the A fragment rows (g)
+        for (int j = 0; j < NRT; ++j) {
+            if (j >= tm.nrt) break;
+            const int row = tm.row(j, g);  // C fragment rows equal the A fragment rows (g)
+            if (row >= R) continue;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int col = tm.ocol[u] + 2 * tq + h;
-                if (row >= 0 && col < bc) red[(tm.mykg * R + row) * bc + col] = acc.value(u, h);
-            }
+            for (int t = 0; t < NTL; ++t)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int col = t * 8 + 2 * tq + h;
+                    if (col < bc) red[(tm.mykg * R + row) * bc + col] = acc.value(j * NTL + t, h, sgn);
+                }
         }
     }
     __syncthreads();  // partial sums visible
@@ -496,24 +515,18 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
     }
 }
 
-// One kernel symbol per stage (the profiler and the launch list name them apart); MAXT is the
-// number of 8 x 8 output tiles a consumer warp keeps in registers.
-template <typename S, int MAXT>
-__global__ void __launch_bounds__(NT, MAXT <= 2 ? 3 : 1) k_rows_up(RowArgs<S> a, const int32_t *nodes) {
-    rows_body<S, STAGE_UP, MAXT>(a, nodes);
-}
-template <typename S, int MAXT>
-__global__ void __launch_bounds__(NT, MAXT <= 2 ? 3 : 1) k_rows_couple(RowArgs<S> a, const int32_t *nodes) {
-    rows_body<S, STAGE_COUPLE, MAXT>(a, nodes);
-}
-template <typename S, int MAXT>
-__global__ void __launch_bounds__(NT, MAXT <= 2 ? 3 : 1) k_rows_down(RowArgs<S> a, const int32_t *nodes) {
-    rows_body<S, STAGE_DOWN, MAXT>(a, nodes);
-}
-template <typename S, int MAXT>
-__global__ void __launch_bounds__(NT, MAXT <= 2 ? 3 : 1) k_rows_leaves(RowArgs<S> a, const int32_t *nodes) {
-    rows_body<S, STAGE_LEAVES, MAXT>(a, nodes);
-}
+// One kernel symbol per stage (the profiler and the launch list name them apart); a consumer
+// warp keeps NRT row tiles x NTL column tiles of 8 x 8 outputs in registers.
+#define NCA_ROWS_KERNEL(NAME, STAGE_ID)                                                           \
+    template <typename S, int NRT, int NTL>                                                       \
+    __global__ void __launch_bounds__(NT, NRT * NTL <= 2 ? 3 : 1) NAME(RowArgs<S> a, const int32_t *nodes) { \
+        rows_body<S, STAGE_ID, NRT, NTL>(a, nodes);                                               \
+    }
+NCA_ROWS_KERNEL(k_rows_up, STAGE_UP)
+NCA_ROWS_KERNEL(k_rows_couple, STAGE_COUPLE)
+NCA_ROWS_KERNEL(k_rows_down, STAGE_DOWN)
+NCA_ROWS_KERNEL(k_rows_leaves, STAGE_LEAVES)
+#undef NCA_ROWS_KERNEL
 
 size_t rows_smem_bytes() { return size_t(NSTAGE) * STAGE_BYTES; }
 
@@ -531,39 +544,52 @@ __global__ void k_gather(const double2 *x, int64_t ldx, const int32_t *perm, int
 int vector_stride(int b) { return conflict_free(b); }
 
 namespace {
-template <typename S, int MAXT>
-void launch_maxt(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
+template <typename S, int NRT, int NTL>
+void launch_tiles(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
     const size_t sm = rows_smem_bytes();
     switch (a.stage) {
     case STAGE_UP:
-        cudaFuncSetAttribute(k_rows_up<S, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        k_rows_up<S, MAXT><<<count, NT, sm, s>>>(a, nodes);
+        cudaFuncSetAttribute(k_rows_up<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        k_rows_up<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
         break;
     case STAGE_COUPLE:
-        cudaFuncSetAttribute(k_rows_couple<S, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        k_rows_couple<S, MAXT><<<count, NT, sm, s>>>(a, nodes);
+        cudaFuncSetAttribute(k_rows_couple<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        k_rows_couple<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
         break;
     case STAGE_DOWN:
-        cudaFuncSetAttribute(k_rows_down<S, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        k_rows_down<S, MAXT><<<count, NT, sm, s>>>(a, nodes);
+        cudaFuncSetAttribute(k_rows_down<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        k_rows_down<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
         break;
     default:
-        cudaFuncSetAttribute(k_rows_leaves<S, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        k_rows_leaves<S, MAXT><<<count, NT, sm, s>>>(a, nodes);
+        cudaFuncSetAttribute(k_rows_leaves<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        k_rows_leaves<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
     }
+}
+
+// Row tiles per warp for the largest block of the launch: 1, 2, 4 or (one column tile only) 8;
+// rows_capacity keeps R * ceil(bc / 8) <= 512, so the tiles of a warp never exceed 8.
+template <typename S, int NTL>
+void launch_ntl(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
+    const int MT = (a.maxrows + 7) / 8;
+    const int nrt = (MT + NCONS - 1) / NCONS;
+    if (nrt <= 1)
+        launch_tiles<S, 1, NTL>(a, nodes, count, s);
+    else if (nrt <= 2)
+        launch_tiles<S, 2, NTL>(a, nodes, count, s);
+    else if (nrt <= 4 || NTL == 2)
+        launch_tiles<S, 4, NTL>(a, nodes, count, s);
+    else
+        launch_tiles<S, (NTL == 1 ? 8 : 4), NTL>(a, nodes, count, s);
 }
 }  // namespace
 
 template <typename S>
 void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
     if (count <= 0) return;
-    const int per_warp = tiles_per_warp(a.maxrows, a.bc);
-    if (per_warp <= 2)
-        launch_maxt<S, 2>(a, nodes, count, s);
-    else if (per_warp <= 4)
-        launch_maxt<S, 4>(a, nodes, count, s);
+    if (a.bc > 8)
+        launch_ntl<S, 2>(a, nodes, count, s);
     else
-        launch_maxt<S, 8>(a, nodes, count, s);
+        launch_ntl<S, 1>(a, nodes, count, s);
 }
 
 template void launch_rows<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
