@@ -328,9 +328,12 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
     const int bc = a.bc;
     const int elem = int(sizeof(S));
     constexpr bool f64 = std::is_same<S, double2>::value;
-    // FP64 tiles are copied column by column into padded shared-memory columns; FP32 tiles in one
-    // piece. Vector rows keep the buffers' padded stride when a pass covers all right-hand sides.
-    const int ldm = f64 ? conflict_free(R) : R;
+    // FP64 blocks of 32 rows or more are copied column by column into padded shared-memory
+    // columns (conflict-free A fragments); smaller blocks, whose many short columns would make
+    // the producer the bottleneck, and FP32 tiles are copied in one piece per segment. Vector
+    // rows keep the buffers' padded stride when a pass covers all right-hand sides.
+    const bool percol = f64 && R >= 32;
+    const int ldm = percol ? conflict_free(R) : R;
     const bool vwhole = bc == a.b;
     const int ldv = vwhole ? a.vs : conflict_free(bc);
     // columns per stage: matrix columns first, the vector rows at voff (16-byte aligned). FP64
@@ -384,8 +387,9 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
                 }
                 if (*abort_flag) break;
                 unsigned char *tile = smem + s * STAGE_BYTES;
-                // FP64: the stage is filled with columns of successive segments (one copy per
-                // matrix column, so pieces pack at any column); FP32 tiles are one piece each.
+                // FP64: the stage is filled with columns of successive segments (complex FP64
+                // pieces are whole 16-byte multiples, so they pack at any column); FP32 tiles are
+                // one piece each.
                 int filled = 0;
                 while (filled < wmax) {
                     while (k < nseg && c0 >= gs.w) {
@@ -408,7 +412,7 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
                     const uint32_t vbytes = vwhole ? uint32_t(w) * uint32_t(a.vs) * 16u : vrow * uint32_t(w);
                     unsigned char *mdst = tile + filled * ldm * elem;
                     unsigned char *vdst = tile + voff + filled * ldv * 16;
-                    if (f64) {
+                    if (percol) {
                         const uint32_t col = uint32_t(R) * 16u;
                         mbar_expect_tx_only(&ctl.full[s], col * uint32_t(w) + vbytes);
                         for (int j = 0; j < w; ++j)
@@ -425,7 +429,7 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
                             bulk_g2s(vdst + j * ldv * 16, vsrc + int64_t(j) * a.vs, vrow, &ctl.full[s]);
                     }
                     filled += w;
-                    if (!f64) break;
+                    if (!f64) break;  // FP32 pieces may end off a 16-byte boundary
                 }
                 if (filled == 0 && k >= nseg) {
                     ctl.w[s] = -1;
