@@ -16,9 +16,10 @@
 // CTA = 8 consumer warps + 1 producer warp. The producer streams tiles through a 3-stage
 // shared-memory ring with cp.async.bulk (bulk copies completing on a "full" mbarrier), filling
 // each stage with columns of successive segments; the consumers release stages on an "empty"
-// mbarrier. Complex FP64 tiles go through the FP64
-// tensor-core MMA (mma.m8n8k4.f64) with three real products per complex product
-// (Re = ArBr - AiBi, Im = (Ar+Ai)(Br+Bi) - ArBr - AiBi); complex FP32 tiles use FMA. Output
+// mbarrier. Tiles go through the FP64 tensor-core MMA (mma.m8n8k4.f64) with three real
+// products per complex product (Re = ArBr - AiBi, Im = (Ar+Ai)(Br+Bi) - ArBr - AiBi); stored
+// complex FP32 blocks are widened to FP64 as they are loaded, so both precisions accumulate in
+// FP64 and FP32 storage halves the bytes streamed without changing the arithmetic. Output
 // tiles of 8 rows x 8 right-hand sides are spread over the warps; when a node has fewer
 // tiles than warps the columns are split between warps and summed in shared memory. Every
 // wait is bounded: on timeout the CTA records an error, drains its copies (bounded) and
@@ -83,11 +84,6 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
-}
-
-__device__ __forceinline__ void cfma(float2 &acc, float2 m, float2 x) {
-    acc.x = fmaf(m.x, x.x, fmaf(-m.y, x.y, acc.x));
-    acc.y = fmaf(m.x, x.y, fmaf(m.y, x.x, acc.y));
 }
 
 template <typename S>
@@ -160,14 +156,12 @@ struct Ctl {
     int err;
 };
 
-// Per-warp accumulators: NRT row tiles x NTL column tiles of 8 x 8 outputs. FP64: the three
-// real products of the 3M complex product per tile (c1 = Ar Br, c2 = Ai Bi, c3 = (Ar + s Ai)
+// Per-warp accumulators: NRT row tiles x NTL column tiles of 8 x 8 outputs, the three real
+// products of the 3M complex product per tile (c1 = Ar Br, c2 = Ai Bi, c3 = (Ar + s Ai)
 // (Br + Bi) with s = -1 for the conjugate), in two independent sets (even / odd k-steps) when a
-// warp holds a single tile. FP32: complex FMA.
-template <typename S, int NRT, int NTL>
-struct Acc;
+// warp holds a single tile. Both stored precisions accumulate in FP64.
 template <int NRT, int NTL>
-struct Acc<double2, NRT, NTL> {
+struct Acc {
     static constexpr int T = NRT * NTL;
     static constexpr int NSET = T <= 1 ? 2 : 1;
     double c1[NSET][T][2], c2[NSET][T][2], c3[NSET][T][2];
@@ -193,16 +187,8 @@ struct Acc<double2, NRT, NTL> {
     }
 };
 
-template <int NRT, int NTL>
-struct Acc<float2, NRT, NTL> {
-    static constexpr int T = NRT * NTL;
-    float2 c[T][2];
-    __device__ void zero() {
-#pragma unroll
-        for (int u = 0; u < T; ++u) c[u][0] = c[u][1] = make_float2(0.f, 0.f);
-    }
-    __device__ double2 value(int u, int h, double) const { return make_double2(c[u][h].x, c[u][h].y); }
-};
+__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.y); }
 
 // Output tiles of one consumer warp. The R x bc output is cut into row tiles of 8 rows; a warp
 // owns whole row tiles (all NTL column tiles of 8 right-hand sides, so one A fragment serves
@@ -223,84 +209,61 @@ struct TileMap {
     __device__ int row(int j, int g) const { return (rt0 + j * NCONS) * 8 + g; }
 };
 
-// One chunk (w columns, tile at smem offset 0, vectors at voff) of the consumer warp's tiles.
-// FP64 operands of full k-steps are loaded without checks: A rows past R and B columns past bc
-// only reach outputs that are never stored (each C row / column depends on its own A row / B
-// column alone), so their addresses are clamped into the block. Only k-steps that cross the
-// chunk end need zeros (a k past w would reach every output).
+// One chunk (w columns, tile at smem offset 0, vectors at voff) of the consumer warp's tiles,
+// on the FP64 tensor cores for both stored precisions (complex FP32 blocks are widened to FP64
+// as their fragments are loaded). Operands of full k-steps are loaded without checks: A rows
+// past R and B columns past bc only reach outputs that are never stored (each C row / column
+// depends on its own A row / B column alone), so their addresses are clamped into the block.
+// Only k-steps that cross the chunk end need zeros (a k past w would reach every output).
 template <typename S, int NRT, int NTL>
-__device__ __forceinline__ void consume(Acc<S, NRT, NTL> &acc, const TileMap &tm, const unsigned char *tile, int w,
+__device__ __forceinline__ void consume(Acc<NRT, NTL> &acc, const TileMap &tm, const unsigned char *tile, int w,
                                         int voff, int R, int ldm, int bc, int ldv, int g, int tq, double sgn) {
-    if constexpr (std::is_same<S, double2>::value) {
-        const double2 *Ms = reinterpret_cast<const double2 *>(tile);
-        const double2 *Vs = reinterpret_cast<const double2 *>(tile + voff);
-        constexpr int NSET = Acc<S, NRT, NTL>::NSET;
-        const int step = 4 * tm.kgroups;
-        int ar[NRT], bcl[NTL];
+    const S *Ms = reinterpret_cast<const S *>(tile);
+    const double2 *Vs = reinterpret_cast<const double2 *>(tile + voff);
+    constexpr int NSET = Acc<NRT, NTL>::NSET;
+    const int step = 4 * tm.kgroups;
+    int ar[NRT], bcl[NTL];
+#pragma unroll
+    for (int j = 0; j < NRT; ++j) {
+        const int r = tm.row(j, g);
+        ar[j] = r < R ? r : R - 1;
+    }
+#pragma unroll
+    for (int t = 0; t < NTL; ++t) bcl[t] = t * 8 + g < bc ? t * 8 + g : bc - 1;
+    auto kstep = [&](int p, int kk, bool full) {
+        double2 bv[NTL];
+        double bs[NTL];
+#pragma unroll
+        for (int t = 0; t < NTL; ++t) {
+            bv[t] = (full || kk < w) ? Vs[kk * ldv + bcl[t]] : make_double2(0.0, 0.0);
+            bs[t] = bv[t].x + bv[t].y;
+        }
 #pragma unroll
         for (int j = 0; j < NRT; ++j) {
-            const int r = tm.row(j, g);
-            ar[j] = r < R ? r : R - 1;
-        }
-#pragma unroll
-        for (int t = 0; t < NTL; ++t) bcl[t] = t * 8 + g < bc ? t * 8 + g : bc - 1;
-        auto kstep = [&](int p, int kk, bool full) {
-            double2 bv[NTL];
-            double bs[NTL];
+            if (NRT > 1 && j >= tm.nrt) break;
+            const double2 av = (full || kk < w) ? to_d2(Ms[ar[j] + kk * ldm]) : make_double2(0.0, 0.0);
+            const double as = fma(sgn, av.y, av.x);
 #pragma unroll
             for (int t = 0; t < NTL; ++t) {
-                bv[t] = (full || kk < w) ? Vs[kk * ldv + bcl[t]] : make_double2(0.0, 0.0);
-                bs[t] = bv[t].x + bv[t].y;
-            }
-#pragma unroll
-            for (int j = 0; j < NRT; ++j) {
-                if (NRT > 1 && j >= tm.nrt) break;
-                const double2 av = (full || kk < w) ? Ms[ar[j] + kk * ldm] : make_double2(0.0, 0.0);
-                const double as = fma(sgn, av.y, av.x);
-#pragma unroll
-                for (int t = 0; t < NTL; ++t) {
-                    const int u = j * NTL + t;
-                    dmma(acc.c1[p][u][0], acc.c1[p][u][1], av.x, bv[t].x);
-                    dmma(acc.c2[p][u][0], acc.c2[p][u][1], av.y, bv[t].y);
-                    dmma(acc.c3[p][u][0], acc.c3[p][u][1], as, bs[t]);
-                }
-            }
-        };
-        int k0 = tm.mykg * 4;
-        // whole sets: every set of the group ends inside the chunk
-        for (; k0 + (NSET - 1) * step + 4 <= w; k0 += NSET * step) {
-#pragma unroll
-            for (int p = 0; p < NSET; ++p) kstep(p, k0 + p * step + tq, true);
-        }
-        // the rest of the chunk: sets that start inside it, with zeros past w
-#pragma unroll
-        for (int p = 0; p < NSET; ++p) {
-            const int kb = k0 + p * step;
-            if (kb >= w) break;
-            kstep(p, kb + tq, kb + 4 <= w);
-        }
-    } else {
-        const float2 *Ms = reinterpret_cast<const float2 *>(tile);
-        const double2 *Vs = reinterpret_cast<const double2 *>(tile + voff);
-        const float fs = float(sgn);
-        for (int k = tm.mykg; k < w; k += tm.kgroups) {
-#pragma unroll
-            for (int j = 0; j < NRT; ++j) {
-                if (j >= tm.nrt) break;
-                const int row = tm.row(j, g);
-                float2 m = row < R ? Ms[row + k * ldm] : make_float2(0.f, 0.f);
-                m.y *= fs;
-#pragma unroll
-                for (int t = 0; t < NTL; ++t) {
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int col = t * 8 + 2 * tq + h;
-                        const double2 xv = col < bc ? Vs[k * ldv + col] : make_double2(0.0, 0.0);
-                        cfma(acc.c[j * NTL + t][h], m, make_float2(float(xv.x), float(xv.y)));
-                    }
-                }
+                const int u = j * NTL + t;
+                dmma(acc.c1[p][u][0], acc.c1[p][u][1], av.x, bv[t].x);
+                dmma(acc.c2[p][u][0], acc.c2[p][u][1], av.y, bv[t].y);
+                dmma(acc.c3[p][u][0], acc.c3[p][u][1], as, bs[t]);
             }
         }
+    };
+    int k0 = tm.mykg * 4;
+    // whole sets: every set of the group ends inside the chunk
+    for (; k0 + (NSET - 1) * step + 4 <= w; k0 += NSET * step) {
+#pragma unroll
+        for (int p = 0; p < NSET; ++p) kstep(p, k0 + p * step + tq, true);
+    }
+    // the rest of the chunk: sets that start inside it, with zeros past w
+#pragma unroll
+    for (int p = 0; p < NSET; ++p) {
+        const int kb = k0 + p * step;
+        if (kb >= w) break;
+        kstep(p, kb + tq, kb + 4 <= w);
     }
 }
 
@@ -336,11 +299,11 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
     const int ldm = percol ? conflict_free(R) : R;
     const bool vwhole = bc == a.b;
     const int ldv = vwhole ? a.vs : conflict_free(bc);
-    // columns per stage: matrix columns first, the vector rows at voff (16-byte aligned). FP64
-    // chunks are whole groups of 8 columns (two k-steps of 4, one per accumulator set); FP32
-    // chunks whole k-steps, so interior chunks stay 16-byte multiples.
+    // columns per stage: matrix columns first, the vector rows at voff (16-byte aligned). Chunks
+    // are whole groups of 8 columns (two k-steps of 4, one per accumulator set), so interior
+    // FP32 chunks stay 16-byte multiples.
     int wmax = STAGE_BYTES / (ldm * elem + ldv * 16);
-    wmax &= f64 ? (wmax >= 8 ? ~7 : ~0) : ~3;
+    wmax &= wmax >= 8 ? ~7 : ~3;
     if (wmax < 4) wmax = 4;
     int voff = (wmax * ldm * elem + 15) & ~15;
     while (wmax > 4 && voff + wmax * ldv * 16 > STAGE_BYTES) {
@@ -361,7 +324,7 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
 
     const int g = lane >> 2, tq = lane & 3;
     volatile int *abort_flag = &ctl.abort;
-    Acc<S, NRT, NTL> acc;
+    Acc<NRT, NTL> acc;
     acc.zero();
     TileMap tm;
     tm.init(R, warp < NCONS ? warp : 0);
@@ -387,9 +350,9 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
                 }
                 if (*abort_flag) break;
                 unsigned char *tile = smem + s * STAGE_BYTES;
-                // FP64: the stage is filled with columns of successive segments (complex FP64
-                // pieces are whole 16-byte multiples, so they pack at any column); FP32 tiles are
-                // one piece each.
+                // The stage is filled with columns of successive segments: complex FP64 pieces
+                // (and FP32 pieces of an even number of rows) are whole 16-byte multiples, so
+                // they pack at any column; odd-row FP32 tiles are one piece each.
                 int filled = 0;
                 while (filled < wmax) {
                     while (k < nseg && c0 >= gs.w) {
@@ -429,7 +392,7 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
                             bulk_g2s(vdst + j * ldv * 16, vsrc + int64_t(j) * a.vs, vrow, &ctl.full[s]);
                     }
                     filled += w;
-                    if (!f64) break;  // FP32 pieces may end off a 16-byte boundary
+                    if (!f64 && (R & 1)) break;  // odd-row FP32 pieces may end off a 16-byte boundary
                 }
                 if (filled == 0 && k >= nseg) {
                     ctl.w[s] = -1;
