@@ -50,7 +50,7 @@ typedef struct {
 /* Apply modes of LinearMaps: A, transpose(A), adjoint(A) (src/nca/petrovgalerkinnca.jl:431-589). */
 typedef enum { NCA_MODE_N = 0, NCA_MODE_T = 1, NCA_MODE_C = 2 } nca_mode;
 
-/* Arithmetic of the product: complex FP64, or complex FP32 stores with FP32 arithmetic. */
+/* Stores the product reads: complex FP64, or complex FP32 copies (FP64 arithmetic either way). */
 typedef enum { NCA_PREC_F64 = 0, NCA_PREC_F32 = 1 } nca_precision;
 
 typedef struct nca_tree nca_tree;
@@ -124,6 +124,12 @@ typedef struct {
     double build_seconds;             /* device build time (events) */
     double build_seconds_host;        /* host planning time (tree mimicry, plans) */
 } nca_core_info;
+/* Batched uneven problems (no counterpart in the reference, which applies one H^2 at a time):
+ * one block-diagonal core over ncores built cores of one device, so a product covers all of them
+ * in one launch per stage level. x and y are the members' vectors stacked in member order. The
+ * batch copies the members' stores; the members may be destroyed afterwards. Exports of a batch
+ * list the members' nodes, points and pairs renumbered in member order. */
+int32_t nca_core_batch(const nca_core *const *cores, int32_t ncores, nca_core **out);
 int32_t nca_core_get_info(const nca_core *core, nca_core_info *info);
 
 /* Pivots per node of one side (the third return value of testbases/trialbases,

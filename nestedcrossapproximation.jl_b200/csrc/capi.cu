@@ -892,6 +892,340 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     return NCA_OK;
 }
 
+// ---- batches: one block-diagonal core from several built cores ------------------------------
+// Many independent problems of uneven size are applied as one operator: the batch renumbers the
+// members' nodes, points, pairs and store offsets into one forest and copies the stores back to
+// back, so every product stage (one launch per level of the deepest member, one coupling and one
+// leaf launch) covers all members at once. x and y are the members' vectors stacked in order.
+
+template <typename T>
+std::vector<T> download_now(const DBuf<T> &b, size_t n) {
+    std::vector<T> h(n);
+    if (n) CK(cudaMemcpy(h.data(), b.p, sizeof(T) * n, cudaMemcpyDeviceToHost));
+    return h;
+}
+
+// dst = concatenation of counts[i] elements of parts[i]
+template <typename T>
+void concat_device(DBuf<T> &dst, const std::vector<const DBuf<T> *> &parts, const std::vector<size_t> &counts,
+                   cudaStream_t s) {
+    size_t total = 0;
+    for (size_t c : counts) total += c;
+    dst.alloc(total);
+    size_t off = 0;
+    for (size_t i = 0; i < parts.size(); ++i) {
+        if (counts[i]) CK(cudaMemcpyAsync(dst.p + off, parts[i]->p, sizeof(T) * counts[i], cudaMemcpyDeviceToDevice, s));
+        off += counts[i];
+    }
+}
+
+// appends v[0..n) + add to out (entries < 0 kept: "no node")
+template <typename T, typename U>
+void append_offset(std::vector<T> &out, const std::vector<U> &v, size_t n, int64_t add, bool keep_negative = false) {
+    for (size_t i = 0; i < n; ++i) out.push_back(T(keep_negative && v[i] < 0 ? v[i] : v[i] + add));
+}
+
+// CSR pointer arrays: ptr of each member without its last entry, shifted; final total at the end
+template <typename T>
+void append_ptr(std::vector<T> &out, const std::vector<T> &ptr, int64_t add) {
+    for (size_t i = 0; i + 1 < ptr.size(); ++i) out.push_back(T(ptr[i] + add));
+}
+
+void merge_trees(const std::vector<const nca_core *> &cs, int sd, nca::Tree &T) {
+    T = nca::Tree{};
+    int64_t poff = 0;
+    int noff = 0;
+    for (const nca_core *c : cs) {
+        const nca::Tree &M = c->tree[sd];
+        append_offset(T.perm, M.perm, M.perm.size(), poff);
+        append_offset(T.iperm, M.iperm, M.iperm.size(), poff);
+        append_offset(T.begin, M.begin, M.begin.size(), poff);
+        append_offset(T.end, M.end, M.end.size(), poff);
+        append_offset(T.parent, M.parent, M.parent.size(), noff, true);
+        append_offset(T.firstchild, M.firstchild, M.firstchild.size(), noff, true);
+        T.nchildren.insert(T.nchildren.end(), M.nchildren.begin(), M.nchildren.end());
+        T.level.insert(T.level.end(), M.level.begin(), M.level.end());
+        T.center.insert(T.center.end(), M.center.begin(), M.center.end());
+        T.radius.insert(T.radius.end(), M.radius.begin(), M.radius.end());
+        T.nlevels = std::max(T.nlevels, M.nlevels);
+        poff += M.npoints;
+        noff += M.nnodes;
+    }
+    T.npoints = poff;
+    T.nnodes = noff;
+    T.levelptr.clear();  // members' nodes are not level-contiguous in a forest
+}
+
+void merge_core(const std::vector<const nca_core *> &cs, nca_core *m, cudaStream_t s) {
+    const size_t n = cs.size();
+    m->device = cs[0]->device;
+    m->maxrank = 0;
+    m->f32 = true;
+    for (const nca_core *c : cs) {
+        m->maxrank = std::max(m->maxrank, c->maxrank);
+        m->f32 = m->f32 && c->f32;
+    }
+    m->K = cs[0]->K;
+    m->K.mat = nullptr;
+    std::vector<int> noff[2], poff[2];
+    for (int sd = 0; sd < 2; ++sd) {
+        merge_trees(cs, sd, m->tree[sd]);
+        int no = 0, po = 0;
+        for (const nca_core *c : cs) {
+            noff[sd].push_back(no);
+            poff[sd].push_back(po);
+            no += c->tree[sd].nnodes;
+            po += int(c->tree[sd].npoints);
+        }
+    }
+    // partition (test-node CSR and trial-node transposes)
+    nca::Partition &P = m->part;
+    int64_t nearoff = 0, faroff = 0, tnearoff = 0, tfaroff = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const nca::Partition &Q = cs[i]->part;
+        append_ptr(P.nearptr, Q.nearptr, nearoff);
+        append_ptr(P.farptr, Q.farptr, faroff);
+        append_ptr(P.tnearptr, Q.tnearptr, tnearoff);
+        append_ptr(P.tfarptr, Q.tfarptr, tfaroff);
+        append_offset(P.nearnodes, Q.nearnodes, Q.nearnodes.size(), noff[1][i]);
+        append_offset(P.farnodes, Q.farnodes, Q.farnodes.size(), noff[1][i]);
+        append_offset(P.tnearnodes, Q.tnearnodes, Q.tnearnodes.size(), noff[0][i]);
+        append_offset(P.tfarnodes, Q.tfarnodes, Q.tfarnodes.size(), noff[0][i]);
+        nearoff += Q.nearnodes.size();
+        faroff += Q.farnodes.size();
+        tnearoff += Q.tnearnodes.size();
+        tfaroff += Q.tfarnodes.size();
+    }
+    P.nearptr.push_back(int32_t(nearoff));
+    P.farptr.push_back(int32_t(faroff));
+    P.tnearptr.push_back(int32_t(tnearoff));
+    P.tfarptr.push_back(int32_t(tfaroff));
+    // sides: node arrays, bases, plans
+    for (int sd = 0; sd < 2; ++sd) {
+        DevSide &d = m->side[sd];
+        const nca::Tree &T = m->tree[sd];
+        d.nnodes = T.nnodes;
+        d.nlevels = T.nlevels;
+        d.npts = T.npoints;
+        d.perm.upload(T.perm, s);
+        d.begin.upload(T.begin, s);
+        d.end.upload(T.end, s);
+        d.firstchild.upload(T.firstchild, s);
+        d.nchildren.upload(T.nchildren, s);
+        std::vector<const DBuf<double> *> pts;
+        std::vector<size_t> npts;
+        for (const nca_core *c : cs) {
+            pts.push_back(&c->side[sd].pts);
+            npts.push_back(size_t(3 * c->side[sd].npts));
+        }
+        concat_device(d.pts, pts, npts, s);
+        d.h_rank.clear();
+        d.h_nrows.clear();
+        d.h_fpptr.clear();
+        d.h_fpidx.clear();
+        d.h_xoff.clear();
+        d.h_cptr.clear();
+        d.h_piv.assign(size_t(T.nnodes) * m->maxrank, 0);
+        int64_t xo = 0, co = 0, fo = 0;
+        std::vector<const DBuf<double2> *> X, XT;
+        std::vector<const DBuf<float2> *> X32, XT32;
+        std::vector<size_t> xn;
+        for (size_t i = 0; i < n; ++i) {
+            const DevSide &e = cs[i]->side[sd];
+            const int nn = e.nnodes;
+            d.h_rank.insert(d.h_rank.end(), e.h_rank.begin(), e.h_rank.end());
+            d.h_nrows.insert(d.h_nrows.end(), e.h_nrows.begin(), e.h_nrows.end());
+            append_ptr(d.h_fpptr, e.h_fpptr, fo);
+            append_offset(d.h_fpidx, e.h_fpidx, e.h_fpidx.size(), poff[sd][i]);
+            append_ptr(d.h_xoff, e.h_xoff, xo);
+            append_ptr(d.h_cptr, e.h_cptr, co);
+            for (int t = 0; t < nn; ++t)
+                for (int r = 0; r < e.h_rank[t]; ++r)
+                    d.h_piv[size_t(noff[sd][i] + t) * m->maxrank + r] =
+                        e.h_piv[size_t(t) * cs[i]->maxrank + r] + poff[sd][i];
+            fo += e.h_fpptr.back();
+            xo += e.h_xoff.back();
+            co += e.h_cptr.back();
+            X.push_back(&e.X);
+            XT.push_back(&e.XT);
+            X32.push_back(&e.X32);
+            XT32.push_back(&e.XT32);
+            xn.push_back(size_t(e.h_xoff.back()));
+        }
+        d.h_fpptr.push_back(int32_t(fo));
+        d.h_xoff.push_back(xo);
+        d.h_cptr.push_back(co);
+        d.rank.upload(d.h_rank, s);
+        d.nrows.upload(d.h_nrows, s);
+        d.xoff.upload(d.h_xoff, s);
+        d.cptr.upload(d.h_cptr, s);
+        concat_device(d.X, X, xn, s);
+        concat_device(d.XT, XT, xn, s);
+        if (m->f32) {
+            concat_device(d.X32, X32, xn, s);
+            concat_device(d.XT32, XT32, xn, s);
+        }
+        // level lists by depth: up deepest first, down root first, over all members
+        d.up.ptr.assign(1, 0);
+        d.up.nodes.clear();
+        d.up.mcap.clear();
+        d.down.ptr.assign(1, 0);
+        d.down.nodes.clear();
+        d.down.mcap.clear();
+        for (int pass = 0; pass < 2; ++pass) {
+            LevelLists &L = pass == 0 ? d.up : d.down;
+            for (int g = 0; g < T.nlevels; ++g) {
+                const int depth = pass == 0 ? T.nlevels - 1 - g : g;
+                int mc = 0;
+                for (size_t i = 0; i < n; ++i) {
+                    const DevSide &e = cs[i]->side[sd];
+                    const LevelLists &Le = pass == 0 ? e.up : e.down;
+                    const int ge = pass == 0 ? e.nlevels - 1 - depth : depth;  // member's group
+                    if (ge < 0 || ge + 1 >= int(Le.ptr.size())) continue;
+                    for (int k = Le.ptr[ge]; k < Le.ptr[ge + 1]; ++k) L.nodes.push_back(Le.nodes[k] + noff[sd][i]);
+                    mc = std::max(mc, Le.mcap[ge]);
+                }
+                L.ptr.push_back(int32_t(L.nodes.size()));
+                L.mcap.push_back(mc);
+            }
+            L.d_nodes.upload(L.nodes, s);
+        }
+        std::vector<int32_t> leaves;
+        d.leafcap = 0;
+        for (int node = 0; node < T.nnodes; ++node)
+            if (T.isleaf(node)) {
+                leaves.push_back(node);
+                d.leafcap = std::max(d.leafcap, T.size(node));
+            }
+        d.nleaves = int(leaves.size());
+        d.leaves.upload(leaves, s);
+    }
+    // couplings: test-CSR blocks (cfoff) and their trial-CSR transposes (ctoff)
+    {
+        std::vector<int64_t> ctoff;
+        std::vector<const DBuf<double2> *> Cp, CTp;
+        std::vector<const DBuf<float2> *> C32p, CT32p;
+        std::vector<size_t> cn, ctn;
+        int64_t co = 0, cto = 0;
+        m->h_cfoff.clear();
+        for (size_t i = 0; i < n; ++i) {
+            const nca_core *c = cs[i];
+            const size_t npair = c->part.farnodes.size(), ntp = c->part.tfarnodes.size();
+            append_ptr(m->h_cfoff, c->h_cfoff, co);
+            const std::vector<int64_t> h_ctoff = download_now(c->ctoff, ntp + 1);
+            append_ptr(ctoff, h_ctoff, cto);
+            co += c->h_cfoff[npair];
+            cto += h_ctoff[ntp];
+            Cp.push_back(&c->C);
+            CTp.push_back(&c->CT);
+            C32p.push_back(&c->C32);
+            CT32p.push_back(&c->CT32);
+            cn.push_back(size_t(c->h_cfoff[npair]));
+            ctn.push_back(size_t(h_ctoff[ntp]));
+        }
+        m->h_cfoff.push_back(co);
+        ctoff.push_back(cto);
+        m->cfoff.upload(m->h_cfoff, s);
+        m->ctoff.upload(ctoff, s);
+        concat_device(m->C, Cp, cn, s);
+        concat_device(m->CT, CTp, ctn, s);
+        if (m->f32) {
+            concat_device(m->C32, C32p, cn, s);
+            concat_device(m->CT32, CT32p, ctn, s);
+        }
+        m->farptr.upload(P.farptr, s);
+        m->farnodes.upload(P.farnodes, s);
+        m->tfarptr.upload(P.tfarptr, s);
+        m->tfarnodes.upload(P.tfarnodes, s);
+        // coupling output nodes of all members, largest work first
+        const std::vector<int32_t> &rt = m->side[0].h_rank, &rs = m->side[1].h_rank;
+        std::vector<int32_t> fwd, rev;
+        std::vector<int64_t> wf(rt.size(), 0), wr(rs.size(), 0);
+        for (size_t t = 0; t < rt.size(); ++t) {
+            if (rt[t] <= 0) continue;
+            fwd.push_back(int32_t(t));
+            for (int k = P.farptr[t]; k < P.farptr[t + 1]; ++k) wf[t] += int64_t(rt[t]) * rs[P.farnodes[k]];
+        }
+        for (size_t u = 0; u < rs.size(); ++u) {
+            if (rs[u] <= 0) continue;
+            rev.push_back(int32_t(u));
+            for (int k = P.tfarptr[u]; k < P.tfarptr[u + 1]; ++k) wr[u] += int64_t(rs[u]) * rt[P.tfarnodes[k]];
+        }
+        std::stable_sort(fwd.begin(), fwd.end(), [&](int a, int b) { return wf[a] > wf[b]; });
+        std::stable_sort(rev.begin(), rev.end(), [&](int a, int b) { return wr[a] > wr[b]; });
+        m->n_couple_fwd = int(fwd.size());
+        m->n_couple_rev = int(rev.size());
+        m->couple_fwd.upload(fwd, s);
+        m->couple_rev.upload(rev, s);
+    }
+    // near field
+    {
+        std::vector<int64_t> ntoff;
+        std::vector<const DBuf<double2> *> Np, NTp;
+        std::vector<const DBuf<float2> *> N32p, NT32p;
+        std::vector<size_t> nn, ntn;
+        int64_t no = 0, nto = 0, ro = 0;
+        m->h_nfoff.clear();
+        m->h_noff.clear();
+        m->h_ncols.clear();
+        for (size_t i = 0; i < n; ++i) {
+            const nca_core *c = cs[i];
+            const size_t npair = c->part.nearnodes.size(), ntp = c->part.tnearnodes.size();
+            append_ptr(m->h_nfoff, c->h_nfoff, no);
+            append_ptr(m->h_noff, c->h_noff, ro);
+            m->h_ncols.insert(m->h_ncols.end(), c->h_ncols.begin(), c->h_ncols.end());
+            const std::vector<int64_t> h_ntoff = download_now(c->ntoff, ntp + 1);
+            append_ptr(ntoff, h_ntoff, nto);
+            no += c->h_nfoff[npair];
+            nto += h_ntoff[ntp];
+            ro += c->h_noff.back();
+            Np.push_back(&c->N);
+            NTp.push_back(&c->NT);
+            N32p.push_back(&c->N32);
+            NT32p.push_back(&c->NT32);
+            nn.push_back(size_t(c->h_nfoff[npair]));
+            ntn.push_back(size_t(h_ntoff[ntp]));
+        }
+        m->h_nfoff.push_back(no);
+        m->h_noff.push_back(ro);
+        ntoff.push_back(nto);
+        m->nfoff.upload(m->h_nfoff, s);
+        m->ntoff.upload(ntoff, s);
+        concat_device(m->N, Np, nn, s);
+        concat_device(m->NT, NTp, ntn, s);
+        if (m->f32) {
+            concat_device(m->N32, N32p, nn, s);
+            concat_device(m->NT32, NT32p, ntn, s);
+        }
+        m->nearptr.upload(P.nearptr, s);
+        m->nearnodes.upload(P.nearnodes, s);
+        m->tnearptr.upload(P.tnearptr, s);
+        m->tnearnodes.upload(P.tnearnodes, s);
+    }
+    // storage summary: sums of the members'
+    nca_core_info &I = m->info;
+    I = nca_core_info{};
+    for (const nca_core *c : cs) {
+        const nca_core_info &J = c->info;
+        I.ntest += J.ntest;
+        I.ntrial += J.ntrial;
+        I.nnodes_test += J.nnodes_test;
+        I.nnodes_trial += J.nnodes_trial;
+        I.ncoeff_test += J.ncoeff_test;
+        I.ncoeff_trial += J.ncoeff_trial;
+        I.near_entries += J.near_entries;
+        I.coupling_entries += J.coupling_entries;
+        I.basis_entries_test += J.basis_entries_test;
+        I.basis_entries_trial += J.basis_entries_trial;
+        I.transfer_entries_test += J.transfer_entries_test;
+        I.transfer_entries_trial += J.transfer_entries_trial;
+        I.nfarpairs += J.nfarpairs;
+        I.nnearpairs += J.nnearpairs;
+        I.build_seconds += J.build_seconds;
+        I.build_seconds_host += J.build_seconds_host;
+    }
+}
+
 // ---- allocation-free product ------------------------------------------------------------
 // Callers that cannot allocate device memory: a host whose own pool (Julia's CUDA.jl, PyTorch's
 // caching allocator) has reserved nearly all of HBM, so a cudaMalloc inside the library fails or
@@ -1113,6 +1447,28 @@ void nca_core_destroy(nca_core *core) {
     if (!core) return;
     cudaSetDevice(core->device);
     delete core;
+}
+
+int32_t nca_core_batch(const nca_core *const *cores, int32_t ncores, nca_core **out) {
+    return guarded([&] {
+        if (!cores || !out || ncores < 1) return fail(NCA_ERR_ARG, "a batch needs at least one core");
+        std::vector<const nca_core *> cs(cores, cores + ncores);
+        int64_t nt = 0, ns = 0;
+        for (const nca_core *c : cs) {
+            if (!c) return fail(NCA_ERR_ARG, "null core in the batch");
+            if (c->device != cs[0]->device) return fail(NCA_ERR_ARG, "the cores of a batch must share one device");
+            nt += c->side[0].npts;
+            ns += c->side[1].npts;
+        }
+        if (nt >= (int64_t(1) << 31) || ns >= (int64_t(1) << 31))
+            return fail(NCA_ERR_ARG, "too many points in the batch for 32-bit indices");
+        CK(cudaSetDevice(cs[0]->device));
+        auto m = std::make_unique<nca_core>();
+        merge_core(cs, m.get(), nullptr);
+        CK(cudaStreamSynchronize(nullptr));
+        *out = m.release();
+        return int(NCA_OK);
+    });
 }
 
 int32_t nca_core_get_info(const nca_core *core, nca_core_info *info) {

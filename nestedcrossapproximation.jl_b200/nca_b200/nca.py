@@ -459,6 +459,43 @@ def mul(y, A, x, alpha=1.0, beta=0.0):
     return out.astype(ws.dtype, copy=False) if ws.dtype != np.complex128 else out
 
 
+class BatchCore(PetrovGalerkinNCACore):
+    """Block-diagonal H^2 operator over several built cores (many problems of uneven size in one
+    product). Vectors are the members' vectors stacked in member order: test offsets
+    `testoffsets`, trial offsets `trialoffsets`. The members may be released afterwards; the batch
+    owns copies of their stores. Exports of the members' blocks are taken from the members."""
+
+    def __init__(self, cores):
+        cores = list(cores)
+        if not cores:
+            raise ArgumentError("a batch needs at least one core")
+        arr = (C.c_void_p * len(cores))(*[c._h.value for c in cores])
+        h = C.c_void_p()
+        check(lib().nca_core_batch(arr, len(cores), C.byref(h)))
+        self._h = h
+        info = CoreInfo()
+        check(lib().nca_core_get_info(h, C.byref(info)))
+        self.info = info
+        self.members = len(cores)
+        self.testoffsets = np.concatenate([[0], np.cumsum([c.dim[0] for c in cores])]).astype(np.int64)
+        self.trialoffsets = np.concatenate([[0], np.cumsum([c.dim[1] for c in cores])]).astype(np.int64)
+        self.dim = (int(self.testoffsets[-1]), int(self.trialoffsets[-1]))
+        self.f32 = all(c.f32 for c in cores)
+        self.device = cores[0].device
+        self.maxrank = max(c.maxrank for c in cores)
+        self._cache = {}
+
+    def _member_export(self, *args, **kwargs):
+        raise ArgumentError("export the member cores of a batch")
+
+    pivots = farpivots = interpolation = _member_export
+
+
+def batch(cores) -> BatchCore:
+    """One block-diagonal core over several built cores (see BatchCore)."""
+    return BatchCore([c.core if isinstance(c, H2Workspace) else c for c in cores])
+
+
 def PetrovGalerkinNCA(operator, testspace, trialspace, tree, **kwargs) -> H2Workspace:
     """Build the core and one workspace over it (petrovgalerkinnca.jl:327-331)."""
     dtype = kwargs.pop("dtype", np.complex128)

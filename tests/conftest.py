@@ -50,3 +50,20 @@ def sphere(n, seed):
 def cgauss(shape, seed):
     rng = np.random.default_rng(seed)
     return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+def cube_surface(n, seed):
+    """n points uniform on the surface of the unit cube [0, 1]^3 (face chosen uniformly, then a
+    uniform point on it), seeded."""
+    rng = np.random.default_rng(seed)
+    face = rng.integers(0, 6, n)
+    uv = rng.uniform(0.0, 1.0, (n, 2))
+    pts = np.empty((n, 3))
+    axis = face // 2
+    for a in range(3):
+        sel = axis == a
+        others = [b for b in range(3) if b != a]
+        pts[sel, a] = (face[sel] % 2).astype(float)
+        pts[sel, others[0]] = uv[sel, 0]
+        pts[sel, others[1]] = uv[sel, 1]
+    return pts
