@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--nrhs", type=int, default=16)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-stages", action="store_true", help="print per-stage times to stderr")
+    p.add_argument("--workload", default="galerkin-sphere", choices=["galerkin-sphere", "batched-uneven"],
+                   help="batched-uneven: 64 problems of uneven size, one batched product vs 64 calls")
     return p.parse_args()
 
 
@@ -288,10 +290,129 @@ def run_reference(args):
     }), flush=True)
 
 
+def cube_surface(n, seed):
+    rng = np.random.default_rng(seed)
+    face = rng.integers(0, 6, n)
+    uv = rng.uniform(0.0, 1.0, (n, 2))
+    pts = np.empty((n, 3))
+    for a in range(3):
+        sel = face // 2 == a
+        o = [c for c in range(3) if c != a]
+        pts[sel, a] = (face[sel] % 2).astype(float)
+        pts[sel, o[0]], pts[sel, o[1]] = uv[sel, 0], uv[sel, 1]
+    return pts
+
+
+def run_batched(args):
+    """64 independent problems, N log-uniform in [4096, 65536], sphere / cube surface alternating,
+    k uniform in [0.5, 4], FP64 build at tol 1e-4 (minvalues 64); step = y = H X with 8
+    right-hand sides per problem. Timed: 64 plain per-problem FP64 products, one batched FP64
+    product and one batched mixed-precision product (complex-FP32 stores, FP64 accumulation)."""
+    import torch
+    import nca_b200 as N
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(2024)
+    nprob, b = 64, 8
+    sizes = np.exp(rng.uniform(np.log(4096), np.log(65536), nprob)).astype(int)
+    ks = rng.uniform(0.5, 4.0, nprob)
+    L = N.lib()
+    t0 = time.perf_counter()
+    members = []
+    for i in range(nprob):
+        pts = sphere(int(sizes[i]), 500 + i) if i % 2 == 0 else cube_surface(int(sizes[i]), 500 + i)
+        tree = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=64))
+        aca = N.ACA(N.FullPivoting(), N.FullPivoting(), N.FNormEstimator(1e-4))
+        comp = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(pts, pts, tree), compressor=aca)
+        members.append(N.PetrovGalerkinNCACore(N.HelmholtzKernel(float(ks[i]), rmin=1e-12), pts, pts,
+                                               N.BlockTree(tree, tree), testcompressor=comp, trialcompressor=comp,
+                                               store_f32=True, device=local))
+    build_wall = time.perf_counter() - t0
+    ntot = int(sizes.sum())
+    X = rhs(ntot, b, seed=77)
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(f"cuda:{local}")
+    off = np.concatenate([[0], np.cumsum(sizes)])
+
+    def timed(fn, steps):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3 / steps
+
+    # 64 plain per-problem FP64 calls (each on its own slice of the stacked vectors)
+    Yp = torch.zeros_like(Xd)
+    Xs = [Xd[:, off[i]:off[i + 1]].contiguous() for i in range(nprob)]
+    Ys = [torch.zeros_like(x) for x in Xs]
+    wss = [N.H2Workspace(m, max_nrhs=b) for m in members]
+
+    def plain():
+        for i in range(nprob):
+            n = int(sizes[i])
+            N._lib.check(L.nca_apply(wss[i]._h, 0, 0, C.c_void_p(Xs[i].data_ptr()), n, C.c_void_p(Ys[i].data_ptr()),
+                                     n, b, 1.0, 0.0, 0.0, 0.0, 1))
+    t_plain = timed(plain, args.steps)
+    info_m = [info_dict(m) for m in members]
+    del wss
+    batch = N.batch(members, move=True)
+    members.clear()
+    import gc
+    gc.collect()
+    info = info_dict(batch)
+    W64 = N.H2Workspace(batch, max_nrhs=b)
+    W32 = N.H2Workspace(batch, np.complex64, max_nrhs=b)
+    Y64 = torch.zeros_like(Xd)
+    Y32 = torch.zeros_like(Xd)
+
+    def batched(W, prec, Y):
+        return lambda: N._lib.check(L.nca_apply(W._h, 0, prec, C.c_void_p(Xd.data_ptr()), ntot,
+                                                C.c_void_p(Y.data_ptr()), ntot, b, 1.0, 0.0, 0.0, 0.0, 1))
+    clocks = Clocks(local)
+    clocks.start()
+    t64 = timed(batched(W64, 0, Y64), args.steps)
+    t32 = timed(batched(W32, 1, Y32), args.steps)
+    clk = clocks.stop()
+    launches = C.c_int32()
+    L.nca_workspace_last_launches(W32._h, C.byref(launches))
+    # the plain per-problem results agree with the batched FP64 product; FP32 error vs FP64
+    rel_plain = max(float((Y64[:, off[i]:off[i + 1]] - Ys[i]).norm() / Ys[i].norm()) for i in range(nprob))
+    rel32 = float((Y32 - Y64).norm() / Y64.norm())
+    bytes64 = product_bytes(info, b)
+    bytes32 = product_bytes(info, b, 8)
+    peak, peak_kind = peaks()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": bytes32 / t32 / 1e9, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t32, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "complex-f32 stores, f64 accumulation", "data": "synthetic",
+            "config": {"workload": "batched-uneven-64-tol1e-4-8rhs", "problems": nprob, "npoints_total": ntot,
+                       "npoints_min": int(sizes.min()), "npoints_max": int(sizes.max()), "nrhs": b,
+                       "step": "y = H X for every problem (one batched product)",
+                       "l2": "inputs larger than L2", "build_s_64_problems": build_wall,
+                       "stored_gb_f64": E * store_entries(info) / 1e9},
+            "plain_per_problem_f64": {"ms_per_step": 1e3 * t_plain, "value": bytes64 / t_plain / 1e9},
+            "batched_f64": {"ms_per_step": 1e3 * t64, "value": bytes64 / t64 / 1e9,
+                            "relerr_vs_per_problem": rel_plain},
+            "speedup_vs_plain_per_problem_f64": t_plain / t32, "relerr_f32_vs_f64": rel32,
+            "roofline": {"bound": "hbm", "achieved": bytes32 / t32 / 1e9, "peak": peak, "peak_source": peak_kind,
+                         "unit": "GB/s", "frac": bytes32 / t32 / 1e9 / peak, "traffic": None,
+                         "note": "whole product (all stages), algorithmic bytes"},
+            "gpu_launches": launches.value, "clocks": clk}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "batched-uneven":
+        run_batched(args)
         return
     import torch
     import torch.distributed as dist

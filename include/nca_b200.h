@@ -127,9 +127,13 @@ typedef struct {
 /* Batched uneven problems (no counterpart in the reference, which applies one H^2 at a time):
  * one block-diagonal core over ncores built cores of one device, so a product covers all of them
  * in one launch per stage level. x and y are the members' vectors stacked in member order. The
- * batch copies the members' stores; the members may be destroyed afterwards. Exports of a batch
- * list the members' nodes, points and pairs renumbered in member order. */
-int32_t nca_core_batch(const nca_core *const *cores, int32_t ncores, nca_core **out);
+ * batch copies the members' stores (the members may be destroyed afterwards); with
+ * NCA_BATCH_MOVE_STORES each member's device stores are released as soon as they are copied, so
+ * the peak stays near one copy, and the members may afterwards only be destroyed (every other
+ * call on them returns NCA_ERR_ARG). Exports of a batch list the members' nodes, points and
+ * pairs renumbered in member order. */
+#define NCA_BATCH_MOVE_STORES 1
+int32_t nca_core_batch(nca_core *const *cores, int32_t ncores, int32_t flags, nca_core **out);
 int32_t nca_core_get_info(const nca_core *core, nca_core_info *info);
 
 /* Pivots per node of one side (the third return value of testbases/trialbases,

@@ -155,6 +155,7 @@ struct nca_core {
     std::vector<int64_t> h_noff;  // compact row-block offsets per test node (exports)
     std::vector<int32_t> h_ncols;
     nca_core_info info{};
+    bool moved = false;  // stores moved into a batch: the core may only be destroyed
 };
 
 struct nca_workspace {
@@ -829,6 +830,7 @@ int check_product_args(nca_core *c, int mode, int precision, int64_t ldx, int64_
 int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_t ldx, void *y,
                int64_t ldy, int64_t nrhs, double2 alpha, double2 beta, int memspace) {
     nca_core *c = ws->core;
+    if (c->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
     if (int st = check_product_args(c, mode, precision, ldx, ldy, nrhs)) return st;
     const int in = mode == 0 ? 1 : 0, out = 1 - in;
     const int64_t nin = c->side[in].npts, nout = c->side[out].npts;
@@ -905,10 +907,11 @@ std::vector<T> download_now(const DBuf<T> &b, size_t n) {
     return h;
 }
 
-// dst = concatenation of counts[i] elements of parts[i]
+// dst = concatenation of counts[i] elements of parts[i]; with release, each part is freed once
+// its copy has completed (moving the members' stores keeps the peak near one copy)
 template <typename T>
-void concat_device(DBuf<T> &dst, const std::vector<const DBuf<T> *> &parts, const std::vector<size_t> &counts,
-                   cudaStream_t s) {
+void concat_device(DBuf<T> &dst, const std::vector<DBuf<T> *> &parts, const std::vector<size_t> &counts,
+                   cudaStream_t s, bool release = false) {
     size_t total = 0;
     for (size_t c : counts) total += c;
     dst.alloc(total);
@@ -916,6 +919,10 @@ void concat_device(DBuf<T> &dst, const std::vector<const DBuf<T> *> &parts, cons
     for (size_t i = 0; i < parts.size(); ++i) {
         if (counts[i]) CK(cudaMemcpyAsync(dst.p + off, parts[i]->p, sizeof(T) * counts[i], cudaMemcpyDeviceToDevice, s));
         off += counts[i];
+        if (release) {
+            CK(cudaStreamSynchronize(s));
+            parts[i]->release();
+        }
     }
 }
 
@@ -931,7 +938,7 @@ void append_ptr(std::vector<T> &out, const std::vector<T> &ptr, int64_t add) {
     for (size_t i = 0; i + 1 < ptr.size(); ++i) out.push_back(T(ptr[i] + add));
 }
 
-void merge_trees(const std::vector<const nca_core *> &cs, int sd, nca::Tree &T) {
+void merge_trees(const std::vector<nca_core *> &cs, int sd, nca::Tree &T) {
     T = nca::Tree{};
     int64_t poff = 0;
     int noff = 0;
@@ -956,7 +963,7 @@ void merge_trees(const std::vector<const nca_core *> &cs, int sd, nca::Tree &T) 
     T.levelptr.clear();  // members' nodes are not level-contiguous in a forest
 }
 
-void merge_core(const std::vector<const nca_core *> &cs, nca_core *m, cudaStream_t s) {
+void merge_core(const std::vector<nca_core *> &cs, nca_core *m, bool move, cudaStream_t s) {
     const size_t n = cs.size();
     m->device = cs[0]->device;
     m->maxrank = 0;
@@ -1012,13 +1019,13 @@ void merge_core(const std::vector<const nca_core *> &cs, nca_core *m, cudaStream
         d.end.upload(T.end, s);
         d.firstchild.upload(T.firstchild, s);
         d.nchildren.upload(T.nchildren, s);
-        std::vector<const DBuf<double> *> pts;
+        std::vector<DBuf<double> *> pts;
         std::vector<size_t> npts;
-        for (const nca_core *c : cs) {
+        for (nca_core *c : cs) {
             pts.push_back(&c->side[sd].pts);
             npts.push_back(size_t(3 * c->side[sd].npts));
         }
-        concat_device(d.pts, pts, npts, s);
+        concat_device(d.pts, pts, npts, s, move);
         d.h_rank.clear();
         d.h_nrows.clear();
         d.h_fpptr.clear();
@@ -1027,11 +1034,11 @@ void merge_core(const std::vector<const nca_core *> &cs, nca_core *m, cudaStream
         d.h_cptr.clear();
         d.h_piv.assign(size_t(T.nnodes) * m->maxrank, 0);
         int64_t xo = 0, co = 0, fo = 0;
-        std::vector<const DBuf<double2> *> X, XT;
-        std::vector<const DBuf<float2> *> X32, XT32;
+        std::vector<DBuf<double2> *> X, XT;
+        std::vector<DBuf<float2> *> X32, XT32;
         std::vector<size_t> xn;
         for (size_t i = 0; i < n; ++i) {
-            const DevSide &e = cs[i]->side[sd];
+            DevSide &e = cs[i]->side[sd];
             const int nn = e.nnodes;
             d.h_rank.insert(d.h_rank.end(), e.h_rank.begin(), e.h_rank.end());
             d.h_nrows.insert(d.h_nrows.end(), e.h_nrows.begin(), e.h_nrows.end());
@@ -1059,11 +1066,11 @@ void merge_core(const std::vector<const nca_core *> &cs, nca_core *m, cudaStream
         d.nrows.upload(d.h_nrows, s);
         d.xoff.upload(d.h_xoff, s);
         d.cptr.upload(d.h_cptr, s);
-        concat_device(d.X, X, xn, s);
-        concat_device(d.XT, XT, xn, s);
+        concat_device(d.X, X, xn, s, move);
+        concat_device(d.XT, XT, xn, s, move);
         if (m->f32) {
-            concat_device(d.X32, X32, xn, s);
-            concat_device(d.XT32, XT32, xn, s);
+            concat_device(d.X32, X32, xn, s, move);
+            concat_device(d.XT32, XT32, xn, s, move);
         }
         // level lists by depth: up deepest first, down root first, over all members
         d.up.ptr.assign(1, 0);
@@ -1103,13 +1110,13 @@ void merge_core(const std::vector<const nca_core *> &cs, nca_core *m, cudaStream
     // couplings: test-CSR blocks (cfoff) and their trial-CSR transposes (ctoff)
     {
         std::vector<int64_t> ctoff;
-        std::vector<const DBuf<double2> *> Cp, CTp;
-        std::vector<const DBuf<float2> *> C32p, CT32p;
+        std::vector<DBuf<double2> *> Cp, CTp;
+        std::vector<DBuf<float2> *> C32p, CT32p;
         std::vector<size_t> cn, ctn;
         int64_t co = 0, cto = 0;
         m->h_cfoff.clear();
         for (size_t i = 0; i < n; ++i) {
-            const nca_core *c = cs[i];
+            nca_core *c = cs[i];
             const size_t npair = c->part.farnodes.size(), ntp = c->part.tfarnodes.size();
             append_ptr(m->h_cfoff, c->h_cfoff, co);
             const std::vector<int64_t> h_ctoff = download_now(c->ctoff, ntp + 1);
@@ -1127,11 +1134,11 @@ void merge_core(const std::vector<const nca_core *> &cs, nca_core *m, cudaStream
         ctoff.push_back(cto);
         m->cfoff.upload(m->h_cfoff, s);
         m->ctoff.upload(ctoff, s);
-        concat_device(m->C, Cp, cn, s);
-        concat_device(m->CT, CTp, ctn, s);
+        concat_device(m->C, Cp, cn, s, move);
+        concat_device(m->CT, CTp, ctn, s, move);
         if (m->f32) {
-            concat_device(m->C32, C32p, cn, s);
-            concat_device(m->CT32, CT32p, ctn, s);
+            concat_device(m->C32, C32p, cn, s, move);
+            concat_device(m->CT32, CT32p, ctn, s, move);
         }
         m->farptr.upload(P.farptr, s);
         m->farnodes.upload(P.farnodes, s);
@@ -1161,15 +1168,15 @@ void merge_core(const std::vector<const nca_core *> &cs, nca_core *m, cudaStream
     // near field
     {
         std::vector<int64_t> ntoff;
-        std::vector<const DBuf<double2> *> Np, NTp;
-        std::vector<const DBuf<float2> *> N32p, NT32p;
+        std::vector<DBuf<double2> *> Np, NTp;
+        std::vector<DBuf<float2> *> N32p, NT32p;
         std::vector<size_t> nn, ntn;
         int64_t no = 0, nto = 0, ro = 0;
         m->h_nfoff.clear();
         m->h_noff.clear();
         m->h_ncols.clear();
         for (size_t i = 0; i < n; ++i) {
-            const nca_core *c = cs[i];
+            nca_core *c = cs[i];
             const size_t npair = c->part.nearnodes.size(), ntp = c->part.tnearnodes.size();
             append_ptr(m->h_nfoff, c->h_nfoff, no);
             append_ptr(m->h_noff, c->h_noff, ro);
@@ -1191,17 +1198,19 @@ void merge_core(const std::vector<const nca_core *> &cs, nca_core *m, cudaStream
         ntoff.push_back(nto);
         m->nfoff.upload(m->h_nfoff, s);
         m->ntoff.upload(ntoff, s);
-        concat_device(m->N, Np, nn, s);
-        concat_device(m->NT, NTp, ntn, s);
+        concat_device(m->N, Np, nn, s, move);
+        concat_device(m->NT, NTp, ntn, s, move);
         if (m->f32) {
-            concat_device(m->N32, N32p, nn, s);
-            concat_device(m->NT32, NT32p, ntn, s);
+            concat_device(m->N32, N32p, nn, s, move);
+            concat_device(m->NT32, NT32p, ntn, s, move);
         }
         m->nearptr.upload(P.nearptr, s);
         m->nearnodes.upload(P.nearnodes, s);
         m->tnearptr.upload(P.tnearptr, s);
         m->tnearnodes.upload(P.tnearnodes, s);
     }
+    if (move)
+        for (nca_core *c : cs) c->moved = true;
     // storage summary: sums of the members'
     nca_core_info &I = m->info;
     I = nca_core_info{};
@@ -1260,6 +1269,7 @@ int static_scratch_base(int device, unsigned char **base) {
 
 int apply_static_impl(nca_core *c, int mode, int precision, const void *x, int64_t ldx, void *y, int64_t ldy,
                       int64_t nrhs, double2 alpha, double2 beta, cudaStream_t s) {
+    if (c->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
     if (int st = check_product_args(c, mode, precision, ldx, ldy, nrhs)) return st;
     if (nrhs == 0) return NCA_OK;
     if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15)
@@ -1449,13 +1459,18 @@ void nca_core_destroy(nca_core *core) {
     delete core;
 }
 
-int32_t nca_core_batch(const nca_core *const *cores, int32_t ncores, nca_core **out) {
+int32_t nca_core_batch(nca_core *const *cores, int32_t ncores, int32_t flags, nca_core **out) {
     return guarded([&] {
         if (!cores || !out || ncores < 1) return fail(NCA_ERR_ARG, "a batch needs at least one core");
-        std::vector<const nca_core *> cs(cores, cores + ncores);
+        if (flags & ~int32_t(NCA_BATCH_MOVE_STORES)) return fail(NCA_ERR_ARG, "unknown batch flags");
+        std::vector<nca_core *> cs(cores, cores + ncores);
         int64_t nt = 0, ns = 0;
-        for (const nca_core *c : cs) {
+        for (size_t i = 0; i < cs.size(); ++i) {
+            const nca_core *c = cs[i];
             if (!c) return fail(NCA_ERR_ARG, "null core in the batch");
+            if (c->moved) return fail(NCA_ERR_ARG, "a core of the batch was moved into another batch");
+            for (size_t j = 0; j < i; ++j)
+                if (cs[j] == c) return fail(NCA_ERR_ARG, "a core appears twice in the batch");
             if (c->device != cs[0]->device) return fail(NCA_ERR_ARG, "the cores of a batch must share one device");
             nt += c->side[0].npts;
             ns += c->side[1].npts;
@@ -1464,7 +1479,7 @@ int32_t nca_core_batch(const nca_core *const *cores, int32_t ncores, nca_core **
             return fail(NCA_ERR_ARG, "too many points in the batch for 32-bit indices");
         CK(cudaSetDevice(cs[0]->device));
         auto m = std::make_unique<nca_core>();
-        merge_core(cs, m.get(), nullptr);
+        merge_core(cs, m.get(), (flags & NCA_BATCH_MOVE_STORES) != 0, nullptr);
         CK(cudaStreamSynchronize(nullptr));
         *out = m.release();
         return int(NCA_OK);
@@ -1510,6 +1525,7 @@ int32_t nca_core_export_farpivots(const nca_core *core, int32_t side, int32_t *p
 int32_t nca_core_export_x(const nca_core *core, int32_t side, int64_t *off, double *X) {
     return guarded([&] {
         if (!core || side < 0 || side > 1) return fail(NCA_ERR_ARG, "bad argument");
+        if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
         const DevSide &d = core->side[side];
         CK(cudaSetDevice(core->device));
         std::vector<double2> all(d.X.n);
@@ -1527,6 +1543,7 @@ int32_t nca_core_export_x(const nca_core *core, int32_t side, int64_t *off, doub
 int32_t nca_core_export_couplings(const nca_core *core, int64_t *off, double *C) {
     return guarded([&] {
         if (!core) return fail(NCA_ERR_ARG, "null core");
+        if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
         CK(cudaSetDevice(core->device));
         std::vector<double2> all(core->C.n);
         if (core->C.n) CK(cudaMemcpy(all.data(), core->C.p, sizeof(double2) * core->C.n, cudaMemcpyDeviceToHost));
@@ -1545,6 +1562,7 @@ int32_t nca_core_export_couplings(const nca_core *core, int64_t *off, double *C)
 int32_t nca_core_export_near(const nca_core *core, int64_t *off, int32_t *ncols, double *N) {
     return guarded([&] {
         if (!core) return fail(NCA_ERR_ARG, "null core");
+        if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
         CK(cudaSetDevice(core->device));
         std::vector<double2> all(core->N.n);
         if (core->N.n) CK(cudaMemcpy(all.data(), core->N.p, sizeof(double2) * core->N.n, cudaMemcpyDeviceToHost));
@@ -1566,6 +1584,7 @@ int32_t nca_core_export_near(const nca_core *core, int64_t *off, int32_t *ncols,
 int32_t nca_workspace_create(nca_core *core, int32_t max_nrhs, nca_workspace **out) {
     return guarded([&] {
         if (!core || !out) return fail(NCA_ERR_ARG, "null argument");
+        if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
         CK(cudaSetDevice(core->device));
         auto ws = std::make_unique<nca_workspace>();
         ws->core = core;

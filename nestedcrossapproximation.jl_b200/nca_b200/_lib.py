@@ -83,7 +83,7 @@ SIGNATURES = {
     "nca_select_farpivots": (I32, [P, P, P, P, I32, P, I32, I32, P, P]),
     "nca_core_build": (I32, [P, I64, P, I64, P, P, P, P, P, P]),
     "nca_core_destroy": (None, [P]),
-    "nca_core_batch": (I32, [P, I32, P]),
+    "nca_core_batch": (I32, [P, I32, I32, P]),
     "nca_core_get_info": (I32, [P, P]),
     "nca_core_export_pivots": (I32, [P, I32, P, P, P, P]),
     "nca_core_farpivots_total": (I32, [P, I32, P]),

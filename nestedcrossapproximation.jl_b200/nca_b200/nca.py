@@ -83,7 +83,7 @@ class PetrovGalerkinNCACore:
         self._cache = {}
 
     def __del__(self):
-        h = getattr(self, "_h", None)
+        h = self.__dict__.get("_h")
         if h is not None and h.value:
             lib().nca_core_destroy(h)
             self._h = None
@@ -322,7 +322,8 @@ class H2Workspace(LinearMap):
         self.last_seconds = 0.0
 
     def __del__(self):
-        h = getattr(self, "_h", None)
+        # the instance's own handle only (a failed __init__ leaves none; never the core's)
+        h = self.__dict__.get("_h")
         if h is not None and h.value:
             lib().nca_workspace_destroy(h)
             self._h = None
@@ -333,7 +334,7 @@ class H2Workspace(LinearMap):
 
     def __getattr__(self, name):
         core = self.__dict__.get("core")
-        if core is None:
+        if core is None or name.startswith("_"):
             raise AttributeError(name)
         return getattr(core, name)
 
@@ -462,16 +463,17 @@ def mul(y, A, x, alpha=1.0, beta=0.0):
 class BatchCore(PetrovGalerkinNCACore):
     """Block-diagonal H^2 operator over several built cores (many problems of uneven size in one
     product). Vectors are the members' vectors stacked in member order: test offsets
-    `testoffsets`, trial offsets `trialoffsets`. The members may be released afterwards; the batch
-    owns copies of their stores. Exports of the members' blocks are taken from the members."""
+    `testoffsets`, trial offsets `trialoffsets`. The batch owns copies of the members' stores
+    (with move=True the members' device stores are released as they are copied). Exports of the
+    members' blocks are taken from the members."""
 
-    def __init__(self, cores):
+    def __init__(self, cores, move: bool = False):
         cores = list(cores)
         if not cores:
             raise ArgumentError("a batch needs at least one core")
         arr = (C.c_void_p * len(cores))(*[c._h.value for c in cores])
         h = C.c_void_p()
-        check(lib().nca_core_batch(arr, len(cores), C.byref(h)))
+        check(lib().nca_core_batch(arr, len(cores), 1 if move else 0, C.byref(h)))
         self._h = h
         info = CoreInfo()
         check(lib().nca_core_get_info(h, C.byref(info)))
@@ -491,9 +493,10 @@ class BatchCore(PetrovGalerkinNCACore):
     pivots = farpivots = interpolation = _member_export
 
 
-def batch(cores) -> BatchCore:
-    """One block-diagonal core over several built cores (see BatchCore)."""
-    return BatchCore([c.core if isinstance(c, H2Workspace) else c for c in cores])
+def batch(cores, move: bool = False) -> BatchCore:
+    """One block-diagonal core over several built cores (see BatchCore). move=True releases each
+    member's device stores as soon as they are copied; the members are then unusable."""
+    return BatchCore([c.core if isinstance(c, H2Workspace) else c for c in cores], move)
 
 
 def PetrovGalerkinNCA(operator, testspace, trialspace, tree, **kwargs) -> H2Workspace:

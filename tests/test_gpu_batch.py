@@ -110,3 +110,20 @@ def test_batch_survives_members_and_static_path():
     N._lib.check(N.lib().nca_apply_static(B._h, 0, 0, C.c_void_p(Xd.data_ptr()), 1300, C.c_void_p(Yd.data_ptr()),
                                           1300, 3, 1.0, 0.0, 0.0, 0.0, None))
     assert relerr(Yd.cpu().numpy().T, Y) < 1e-13
+
+
+def test_batch_move_releases_members():
+    N = _n()
+    ms = [member(n, 30 + i, 2.0, 32) for i, n in enumerate((500, 800))]
+    X = cgauss((1300, 2), 12)
+    refs = [ms[0][2] @ X[:500], ms[1][2] @ X[500:]]
+    B = N.batch([A for _, _, A in ms], move=True)
+    # moved members refuse products and new workspaces
+    with pytest.raises(N.ArgumentError):
+        ms[0][2] @ X[:500]
+    with pytest.raises(N.ArgumentError):
+        N.H2Workspace(N.core(ms[1][2]))
+    with pytest.raises(N.ArgumentError):
+        N.batch([A for _, _, A in ms])
+    Y = N.H2Workspace(B) @ X
+    assert relerr(Y[:500], refs[0]) < 1e-13 and relerr(Y[500:], refs[1]) < 1e-13
