@@ -124,6 +124,17 @@ typedef struct {
     double build_seconds;             /* device build time (events) */
     double build_seconds_host;        /* host planning time (tree mimicry, plans) */
 } nca_core_info;
+/* ---- differentiation on frozen skeletons (no counterpart in the reference, which has no
+ *      gradients): the tree, partition, ranks and row/column pivots of a build stay fixed. ---- */
+/* Refills every store at wavenumber k with the frozen skeleton: X = K[rows, sigma] K[tau, sigma]^{-1},
+ * couplings, near field (and FP32 copies); bit-identical to the build at the build's own k. A
+ * singular frozen cross matrix returns NCA_ERR_SINGULAR and leaves the core unchanged. Drops
+ * the d/dk stores. */
+int32_t nca_core_set_wavenumber(nca_core *core, double k);
+/* Prepares the d/dk stores at the core's wavenumber: dX = (dK[rows, sigma] - X dK[tau, sigma])
+ * K[tau, sigma]^{-1} per node, dS and dN from the derivative entries (as much memory as the
+ * complex FP64 stores). */
+int32_t nca_core_prepare_dk(nca_core *core);
 /* Batched uneven problems (no counterpart in the reference, which applies one H^2 at a time):
  * one block-diagonal core over ncores built cores of one device, so a product covers all of them
  * in one launch per stage level. x and y are the members' vectors stacked in member order. The
@@ -176,6 +187,12 @@ int32_t nca_apply(nca_workspace *ws, int32_t mode, int32_t precision, const void
 int32_t nca_apply_static(nca_core *core, int32_t mode, int32_t precision, const void *x, int64_t ldx,
                          void *y, int64_t ldy, int64_t nrhs, double alpha_re, double alpha_im,
                          double beta_re, double beta_im, void *stream);
+/* Tangent product y = alpha (dH/dk) x + beta y (forward mode, complex FP64, after
+ * nca_core_prepare_dk): the sweeps of nca_apply carried as dual numbers. With the adjoint product
+ * it gives the gradients of a loss through y = H(k) x: x_bar = H^H y_bar (nca_apply mode C) and
+ * k_bar = Re(y_bar^H (dH/dk) x). No counterpart in the reference. */
+int32_t nca_apply_dk(nca_workspace *ws, const void *x, int64_t ldx, void *y, int64_t ldy, int64_t nrhs,
+                     double alpha_re, double alpha_im, double beta_re, double beta_im, int32_t memspace);
 /* Device time of the last nca_apply of this workspace (CUDA events), in seconds. */
 int32_t nca_workspace_last_time(const nca_workspace *ws, double *seconds);
 /* Kernel launches of the last nca_apply of this workspace. */
@@ -211,6 +228,12 @@ int32_t nca_blocks_factors(const double *buffer, int64_t ldbuffer, int32_t ldcol
 int32_t nca_entries(const nca_kernel_desc *kernel, const double *testpoints, int64_t ntest,
                     const double *trialpoints, int64_t ntrial, const int64_t *ii,
                     const int64_t *jj, int64_t n, int32_t device, double *out);
+
+/* d/dk of the point-kernel entries (Helmholtz: (-sin(kr) + i sign cos(kr)) / (4 pi); Laplace: 0);
+ * no counterpart in the reference. Matrix kernels return NCA_ERR_ARG. */
+int32_t nca_entries_dk(const nca_kernel_desc *kernel, const double *testpoints, int64_t ntest,
+                       const double *trialpoints, int64_t ntrial, const int64_t *ii,
+                       const int64_t *jj, int64_t n, int32_t device, double *out);
 
 #ifdef __cplusplus
 }

@@ -287,6 +287,7 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
     __shared__ Ctl ctl;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int o = nodes[blockIdx.x];
+    if (STAGE == STAGE_UP && a.skip_leaves && a.nchildren[o] == 0) return;  // whole CTA, before any barrier
     const int R = out_rows<S, STAGE>(a, o);
     const int bc = a.bc;
     const int elem = int(sizeof(S));
@@ -461,12 +462,16 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
             v.y += p.y;
         }
         const int col = a.q0 + qq;
-        if (STAGE == STAGE_UP) {
-            a.coef[(a.cptr[o] + i) * a.vs + col] = v;
-        } else if (STAGE == STAGE_COUPLE) {
-            a.dst[(a.cptr_out[o] + i) * a.vs + col] = v;
+        if (STAGE == STAGE_UP || STAGE == STAGE_COUPLE) {
+            double2 *d = STAGE == STAGE_UP ? (a.coef_out ? a.coef_out : a.coef) + (a.cptr[o] + i) * a.vs + col
+                                           : a.dst + (a.cptr_out[o] + i) * a.vs + col;
+            if (a.accumulate) {
+                const double2 old = *d;
+                v = make_double2(old.x + v.x, old.y + v.y);
+            }
+            *d = v;
         } else if (STAGE == STAGE_DOWN) {
-            double2 *d = a.coef + (a.cptr[a.firstchild[o]] + i) * a.vs + col;
+            double2 *d = (a.coef_out ? a.coef_out : a.coef) + (a.cptr[a.firstchild[o]] + i) * a.vs + col;
             const double2 old = *d;
             *d = make_double2(old.x + v.x, old.y + v.y);
         } else {

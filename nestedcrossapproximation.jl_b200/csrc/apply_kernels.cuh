@@ -43,6 +43,10 @@ struct RowArgs {
     int conj;
     int maxrows;      // largest output block of the launch (picks the register tile)
     int32_t *error;   // 1: misaligned copy skipped, 2: a bounded wait gave up
+    // tangent products: UP / DOWN write into coef_out (nullptr: coef) while reading coef;
+    // UP and COUPLE add to the existing output with accumulate; UP skips leaves with skip_leaves
+    double2 *coef_out;
+    int accumulate, skip_leaves;
 };
 
 size_t rows_smem_bytes();

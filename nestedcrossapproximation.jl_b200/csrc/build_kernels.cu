@@ -349,6 +349,8 @@ __global__ void __launch_bounds__(NT) k_level_compress(LevelArgs a, const int32_
     // phase 3a: pivots
     const int r = aca_smem(R, m, n, a.maxrank, a.tol, a.sampled, u, v, rp, cp, wsum, wmax, widx);
     for (int k = tid; k < r; k += NT) a.piv[int64_t(node) * a.maxrank + k] = rowid[rp[k]];
+    if (a.cpiv)
+        for (int k = tid; k < r; k += NT) a.cpiv[int64_t(node) * a.maxrank + k] = colid[cp[k]];
     if (tid == 0) {
         a.rank[node] = r;
         a.nrows[node] = m;
@@ -374,6 +376,121 @@ __global__ void __launch_bounds__(NT) k_level_compress(LevelArgs a, const int32_
     __syncthreads();
     double2 *X = a.X + a.xoff[node];
     for (int e = tid; e < m * r; e += NT) X[e] = R[e];
+}
+
+size_t values_smem_bytes(int mcap, int rcap, int mode) {
+    size_t b = sizeof(double2) * (size_t(mcap) * rcap + size_t(rcap) * rcap * (mode ? 2 : 1));
+    b += sizeof(double) * 3 * (size_t(mcap) + 2 * rcap);
+    b += sizeof(int32_t) * (size_t(mcap) + 3 * rcap);
+    return (b + 15) & ~size_t(15);
+}
+
+namespace {
+// K(row point i, column point j) with the side's orientation (test rows / trial columns on side 0)
+__device__ __forceinline__ double2 oriented_entry(const KernelParams &K, int side, const double *rowxyz,
+                                                  const int32_t *rowid, const double *colxyz,
+                                                  const int32_t *colid, int i, int j) {
+    const double *p = rowxyz + 3 * i;
+    const double *q = colxyz + 3 * j;
+    if (side == 0) return kernel_entry(K, p[0], p[1], p[2], q[0], q[1], q[2], rowid[i], colid[j]);
+    return kernel_entry(K, q[0], q[1], q[2], p[0], p[1], p[2], colid[j], rowid[i]);
+}
+}  // namespace
+
+__global__ void __launch_bounds__(NT) k_level_values(ValueArgs a, const int32_t *nodes, int mcap, int rcap) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2 *L = reinterpret_cast<double2 *>(smem);
+    double2 *P = L + size_t(mcap) * rcap;
+    double2 *dP = P + size_t(rcap) * rcap;
+    double *rowxyz = reinterpret_cast<double *>(dP + (a.mode ? size_t(rcap) * rcap : 0));
+    double *colxyz = rowxyz + 3 * mcap;
+    double *tauxyz = colxyz + 3 * rcap;
+    int32_t *rowid = reinterpret_cast<int32_t *>(tauxyz + 3 * rcap);
+    int32_t *colid = rowid + mcap;
+    int32_t *tauid = colid + rcap;
+    int32_t *ipiv = tauid + rcap;
+    __shared__ int s_m, s_flag;
+    const int tid = threadIdx.x;
+    const int node = nodes[blockIdx.x];
+    const int r = a.rank[node];
+    if (r <= 0) return;
+    const bool leaf = a.nchildren[node] == 0;
+    if (tid == 0) {
+        int m = 0;
+        if (leaf) {
+            m = a.end[node] - a.begin[node];
+        } else {
+            for (int c = 0; c < a.nchildren[node]; ++c) m += a.rank[a.firstchild[node] + c];
+        }
+        s_m = m;
+    }
+    __syncthreads();
+    const int m = s_m;
+    if (m > mcap || r > rcap) {
+        if (tid == 0 && atomicCAS(a.status, 0, 2) == 0) {
+            a.status[1] = node;
+            a.status[2] = m;
+            a.status[3] = r;
+        }
+        return;
+    }
+    if (leaf) {
+        for (int i = tid; i < m; i += NT) rowid[i] = a.perm[a.begin[node] + i];
+    } else {
+        int off = 0;
+        for (int c = 0; c < a.nchildren[node]; ++c) {
+            const int ch = a.firstchild[node] + c;
+            const int kc = a.rank[ch];
+            for (int k = tid; k < kc; k += NT) rowid[off + k] = a.piv[int64_t(ch) * a.maxrank + k];
+            off += kc;
+        }
+    }
+    for (int j = tid; j < r; j += NT) {
+        colid[j] = a.cpiv[int64_t(node) * a.maxrank + j];
+        tauid[j] = a.piv[int64_t(node) * a.maxrank + j];
+    }
+    __syncthreads();
+    for (int e = tid; e < 3 * m; e += NT) rowxyz[e] = a.own_pts[3 * int64_t(rowid[e / 3]) + e % 3];
+    for (int e = tid; e < 3 * r; e += NT) {
+        colxyz[e] = a.far_pts[3 * int64_t(colid[e / 3]) + e % 3];
+        tauxyz[e] = a.own_pts[3 * int64_t(tauid[e / 3]) + e % 3];
+    }
+    __syncthreads();
+    const KernelParams &KL = a.mode ? a.dK : a.K;
+    for (int e = tid; e < m * r; e += NT) L[e] = oriented_entry(KL, a.side, rowxyz, rowid, colxyz, colid, e % m, e / m);
+    for (int e = tid; e < r * r; e += NT) {
+        P[e] = oriented_entry(a.K, a.side, tauxyz, tauid, colxyz, colid, e % r, e / r);
+        if (a.mode) dP[e] = oriented_entry(a.dK, a.side, tauxyz, tauid, colxyz, colid, e % r, e / r);
+    }
+    __syncthreads();
+    if (a.mode) {
+        // M = dL - X dP, row by row into L
+        const double2 *X = a.Xin + a.xoff[node];
+        for (int e = tid; e < m * r; e += NT) {
+            const int i = e % m, j = e / m;
+            double2 acc = L[e];
+            for (int l = 0; l < r; ++l) {
+                const double2 t = cmul_rn(X[i + int64_t(l) * m], dP[l + j * r]);
+                acc.x -= t.x;
+                acc.y -= t.y;
+            }
+            L[e] = acc;
+        }
+        __syncthreads();
+    }
+    int rank = 0;
+    if (cross_factor_smem(P, r, ipiv, &s_flag, &rank)) {
+        if (tid == 0 && atomicCAS(a.status, 0, 1) == 0) {
+            a.status[1] = node;
+            a.status[2] = r;
+            a.status[3] = rank;
+        }
+        return;
+    }
+    for (int i = tid; i < m; i += NT) solve_row(L + i, m, r, P, ipiv);
+    __syncthreads();
+    double2 *X = a.Xout + a.xoff[node];
+    for (int e = tid; e < m * r; e += NT) X[e] = L[e];
 }
 
 // Level seam on caller-given blocks: block i holds rows rowoff[i]..rowoff[i+1]-1 and

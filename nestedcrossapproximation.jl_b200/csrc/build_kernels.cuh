@@ -19,6 +19,7 @@ struct LevelArgs {
     const int32_t *perm, *begin, *end, *firstchild, *nchildren;
     const int32_t *fpptr, *fpidx;  // phase-1 far pivots (CSR over nodes)
     int32_t *rank, *nrows, *piv;   // outputs: rank, block rows, pivots (maxrank per node)
+    int32_t *cpiv;                 // optional output: column pivots (far-side point ids)
     double2 *X;                    // interpolation operators, node slot at xoff[node]
     const int64_t *xoff;
     int maxrank;
@@ -29,6 +30,24 @@ struct LevelArgs {
 
 size_t level_smem_bytes(int mcap, int ncap);
 __global__ void k_level_compress(LevelArgs a, const int32_t *nodes, int mcap, int ncap);
+
+// Frozen-skeleton values of the interpolation operators: with the row pivots tau (piv) and
+// column pivots sigma (cpiv) of a finished build, mode 0 recomputes X = K[rows, sigma]
+// K[tau, sigma]^{-1} for the kernel K (a new wavenumber; bit-identical to the build at the same
+// one), mode 1 computes dX/dk = (dK[rows, sigma] - X dK[tau, sigma]) K[tau, sigma]^{-1} from X.
+struct ValueArgs {
+    KernelParams K, dK;
+    int side, mode;
+    const double *own_pts, *far_pts;
+    const int32_t *perm, *begin, *end, *firstchild, *nchildren, *rank, *piv, *cpiv;
+    int maxrank;
+    const double2 *Xin;  // mode 1: X at the wavenumber of K
+    double2 *Xout;
+    const int64_t *xoff;
+    int32_t *status;  // [flag, node, npivots, rank]: 1 singular cross matrix, 2 capacity
+};
+size_t values_smem_bytes(int mcap, int rcap, int mode);
+__global__ void k_level_values(ValueArgs a, const int32_t *nodes, int mcap, int rcap);
 
 struct CouplingArgs {
     KernelParams K;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <chrono>
 #include <cstring>
@@ -120,6 +121,8 @@ struct DevSide {
     DBuf<int64_t> xoff, cptr;
     DBuf<double2> X, XT;  // interpolation operators and their transposes (same padded offsets)
     DBuf<float2> X32, XT32;
+    DBuf<int32_t> cpiv;     // column pivots sigma of every node (far-side point ids, maxrank per node)
+    DBuf<double2> dX, dXT;  // dX/dk on the frozen skeleton (prepared on demand)
     std::vector<int32_t> h_fpptr, h_fpidx, h_rank, h_nrows, h_piv;
     std::vector<int64_t> h_xoff, h_cptr;
     LevelLists up, down;
@@ -154,6 +157,14 @@ struct nca_core {
     std::vector<int64_t> h_nfoff;
     std::vector<int64_t> h_noff;  // compact row-block offsets per test node (exports)
     std::vector<int32_t> h_ncols;
+    // pair lists and transposition plans of the coupling and near stores (refills at another
+    // wavenumber and the d/dk stores reuse them)
+    DBuf<int32_t> cpair_t, ctr_rows, ctr_cols, near_t, ntr_rows, ntr_cols;
+    DBuf<int64_t> ctr_in, ntr_in;
+    int64_t n_ctr = 0, n_ntr = 0;
+    DBuf<double2> dC, dCT, dN, dNT;  // dS/dk and dN/dk on the frozen skeleton
+    bool has_dk = false;
+    bool batch = false;  // block-diagonal batch of several cores (one wavenumber per member)
     nca_core_info info{};
     bool moved = false;  // stores moved into a batch: the core may only be destroyed
 };
@@ -164,6 +175,7 @@ struct nca_workspace {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int max_nrhs = 0;
     DBuf<double2> xt, xhat, yhat, xstage, ystage;
+    DBuf<double2> dxhat, dyhat;  // tangent products (d/dk)
     std::atomic<bool> busy{false};
     DBuf<int32_t> error;
     int32_t *error_host = nullptr;  // pinned
@@ -305,6 +317,131 @@ int launch_grid(int64_t work, int per_sm) {
     return int(std::max<int64_t>(1, std::min<int64_t>(work, int64_t(sms) * per_sm)));
 }
 
+// Couplings S_ts = K[tau_t, tau_s] of every admissible pair (test CSR order) into C and their
+// transposes (trial CSR order) into CT, for the kernel K (values or d/dk entries).
+void fill_couplings(nca_core *c, const KernelParams &K, double2 *C, double2 *CT, cudaStream_t s) {
+    const int64_t npairs = int64_t(c->part.farnodes.size());
+    CouplingArgs a;
+    a.K = K;
+    a.test_pts = c->side[0].pts.p;
+    a.trial_pts = c->side[1].pts.p;
+    a.pair_t = c->cpair_t.p;
+    a.pair_s = c->farnodes.p;
+    a.rank_t = c->side[0].rank.p;
+    a.rank_s = c->side[1].rank.p;
+    a.piv_t = c->side[0].piv.p;
+    a.piv_s = c->side[1].piv.p;
+    a.maxrank = c->maxrank;
+    a.coff = c->cfoff.p;
+    a.npairs = npairs;
+    a.C = C;
+    a.C32 = nullptr;
+    if (npairs > 0) {
+        k_couplings<<<launch_grid(npairs, 16), 256, 0, s>>>(a);
+        CK(cudaGetLastError());
+    }
+    launch_transpose_blocks<double2>(C, c->ctr_in.p, c->ctr_rows.p, c->ctr_cols.p, c->ctoff.p, c->n_ctr, CT, s);
+    CK(cudaGetLastError());
+}
+
+// Near blocks K[t, s] of every near pair (test CSR order) into N and their transposes into NT.
+void fill_near(nca_core *c, const KernelParams &K, double2 *N, double2 *NT, cudaStream_t s) {
+    const int64_t nnear = int64_t(c->part.nearnodes.size());
+    NearArgs a;
+    a.K = K;
+    a.test_pts = c->side[0].pts.p;
+    a.trial_pts = c->side[1].pts.p;
+    a.pair_t = c->near_t.p;
+    a.pair_s = c->nearnodes.p;
+    a.t_perm = c->side[0].perm.p;
+    a.t_begin = c->side[0].begin.p;
+    a.t_end = c->side[0].end.p;
+    a.s_perm = c->side[1].perm.p;
+    a.s_begin = c->side[1].begin.p;
+    a.s_end = c->side[1].end.p;
+    a.poff = c->nfoff.p;
+    a.npairs = nnear;
+    a.N = N;
+    if (nnear > 0) {
+        k_near<<<launch_grid(nnear, 16), 256, 0, s>>>(a);
+        CK(cudaGetLastError());
+    }
+    launch_transpose_blocks<double2>(N, c->ntr_in.p, c->ntr_rows.p, c->ntr_cols.p, c->ntoff.p, c->n_ntr, NT, s);
+    CK(cudaGetLastError());
+}
+
+// Complex FP32 copies of every store (the mixed-precision product reads them).
+void make_f32_copies(nca_core *c, cudaStream_t s) {
+    auto down = [&](DBuf<double2> &src, DBuf<float2> &dst) {
+        if (dst.n != src.n) dst.alloc(src.n);
+        if (src.n) k_to_f32<<<launch_grid(int64_t(src.n) / 256 + 1, 8), 256, 0, s>>>(src.p, dst.p, int64_t(src.n));
+        CK(cudaGetLastError());
+    };
+    for (int sd = 0; sd < 2; ++sd) {
+        down(c->side[sd].X, c->side[sd].X32);
+        down(c->side[sd].XT, c->side[sd].XT32);
+    }
+    down(c->C, c->C32);
+    down(c->CT, c->CT32);
+    down(c->N, c->N32);
+    down(c->NT, c->NT32);
+}
+
+// Interpolation operators of one side on the frozen skeleton (k_level_values): mode 0 the values
+// for kernel K into Xout, mode 1 dX/dk (dK: derivative entries) from the side's X; transposes
+// into XTout. A singular cross matrix raises NCA_ERR_SINGULAR and leaves Xout partly written.
+void fill_bases(nca_core *c, int sd, int mode, const KernelParams &K, const KernelParams &dK, double2 *Xout,
+                double2 *XTout, cudaStream_t s) {
+    DevSide &d = c->side[sd];
+    if (d.up.nodes.empty()) return;
+    int mcap = 1, rcap = 1;
+    for (int node = 0; node < d.nnodes; ++node)
+        if (d.h_rank[node] > 0) {
+            mcap = std::max(mcap, d.h_nrows[node]);
+            rcap = std::max(rcap, d.h_rank[node]);
+        }
+    const size_t sm = values_smem_bytes(mcap, rcap, mode);
+    if (sm > size_t(kMaxSmem))
+        throw Failure(NCA_ERR_ARG, "a cross block of the frozen skeleton does not fit in shared memory");
+    CK(cudaFuncSetAttribute(k_level_values, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    DBuf<int32_t> status;
+    status.alloc(4);
+    status.zero(s);
+    ValueArgs a;
+    a.K = K;
+    a.dK = dK;
+    a.side = sd;
+    a.mode = mode;
+    a.own_pts = d.pts.p;
+    a.far_pts = c->side[1 - sd].pts.p;
+    a.perm = d.perm.p;
+    a.begin = d.begin.p;
+    a.end = d.end.p;
+    a.firstchild = d.firstchild.p;
+    a.nchildren = d.nchildren.p;
+    a.rank = d.rank.p;
+    a.piv = d.piv.p;
+    a.cpiv = d.cpiv.p;
+    a.maxrank = c->maxrank;
+    a.Xin = d.X.p;
+    a.Xout = Xout;
+    a.xoff = d.xoff.p;
+    a.status = status.p;
+    k_level_values<<<int(d.up.nodes.size()), 256, sm, s>>>(a, d.up.d_nodes.p, mcap, rcap);
+    CK(cudaGetLastError());
+    const std::vector<int32_t> st = status.download(s);
+    CK(cudaStreamSynchronize(s));
+    if (st[0] == 1) {
+        set_singular(sd, st[1], st[2], st[3]);
+        throw Failure(NCA_ERR_SINGULAR, "SingularCrossMatrixError: the frozen cross matrix of " +
+                                            std::string(sd == 0 ? "test" : "trial") + " node " +
+                                            std::to_string(st[1]) + " is singular at this wavenumber");
+    }
+    if (st[0] == 2) throw Failure(NCA_ERR_CUDA, "internal: a frozen cross block exceeds its planned capacity");
+    launch_transpose_blocks<double2>(Xout, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, d.nnodes, XTout, s);
+    CK(cudaGetLastError());
+}
+
 void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int64_t ns,
                 const nca_build_opts *o) {
     const int maxrank = c->maxrank;
@@ -352,6 +489,7 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         d.nrows.alloc(T.nnodes);
         d.nrows.zero(s);
         d.piv.alloc(size_t(T.nnodes) * maxrank);
+        d.cpiv.alloc(size_t(T.nnodes) * maxrank);
         DBuf<int32_t> nodes;
         nodes.upload(lv_nodes, s);
         status.zero(s);
@@ -370,6 +508,7 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         a.rank = d.rank.p;
         a.nrows = d.nrows.p;
         a.piv = d.piv.p;
+        a.cpiv = d.cpiv.p;
         a.X = d.X.p;
         a.xoff = d.xoff.p;
         a.maxrank = maxrank;
@@ -444,37 +583,13 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
     c->ctoff.upload(h_ctoff, s);
     c->C.alloc(size_t(c->h_cfoff.back()));
     c->CT.alloc(size_t(h_ctoff.back()));
-    {
-        DBuf<int32_t> dpt, dps, drows, dcols;
-        DBuf<int64_t> din;
-        dpt.upload(pair_t, s);
-        dps.upload(pair_s, s);
-        CouplingArgs a;
-        a.K = c->K;
-        a.test_pts = c->side[0].pts.p;
-        a.trial_pts = c->side[1].pts.p;
-        a.pair_t = dpt.p;
-        a.pair_s = dps.p;
-        a.rank_t = c->side[0].rank.p;
-        a.rank_s = c->side[1].rank.p;
-        a.piv_t = c->side[0].piv.p;
-        a.piv_s = c->side[1].piv.p;
-        a.maxrank = maxrank;
-        a.coff = c->cfoff.p;
-        a.npairs = npairs;
-        a.C = c->C.p;
-        a.C32 = nullptr;
-        if (npairs > 0) {
-            k_couplings<<<launch_grid(npairs, 16), 256, 0, s>>>(a);
-            CK(cudaGetLastError());
-        }
-        din.upload(tr_in, s);
-        drows.upload(tr_rows, s);
-        dcols.upload(tr_cols, s);
-        launch_transpose_blocks<double2>(c->C.p, din.p, drows.p, dcols.p, c->ctoff.p, ntf, c->CT.p, s);
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(s));
-    }
+    c->cpair_t.upload(pair_t, s);
+    c->ctr_in.upload(tr_in, s);
+    c->ctr_rows.upload(tr_rows, s);
+    c->ctr_cols.upload(tr_cols, s);
+    c->n_ctr = ntf;
+    fill_couplings(c, c->K, c->C.p, c->CT.p, s);
+    CK(cudaStreamSynchronize(s));
     // output nodes of the coupling stage, largest work first (shorter tail of the last wave)
     std::vector<int32_t> fwd, rev;
     std::vector<int64_t> wf(Tt.nnodes, 0), wr(Ts.nnodes, 0);
@@ -552,52 +667,15 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
     c->ntoff.upload(h_ntoff, s);
     c->N.alloc(size_t(c->h_nfoff.back()));
     c->NT.alloc(size_t(h_ntoff.back()));
-    {
-        DBuf<int32_t> dnt, drows, dcols;
-        DBuf<int64_t> din;
-        dnt.upload(near_t, s);
-        NearArgs a;
-        a.K = c->K;
-        a.test_pts = c->side[0].pts.p;
-        a.trial_pts = c->side[1].pts.p;
-        a.pair_t = dnt.p;
-        a.pair_s = c->nearnodes.p;
-        a.t_perm = c->side[0].perm.p;
-        a.t_begin = c->side[0].begin.p;
-        a.t_end = c->side[0].end.p;
-        a.s_perm = c->side[1].perm.p;
-        a.s_begin = c->side[1].begin.p;
-        a.s_end = c->side[1].end.p;
-        a.poff = c->nfoff.p;
-        a.npairs = nnear;
-        a.N = c->N.p;
-        if (nnear > 0) {
-            k_near<<<launch_grid(nnear, 16), 256, 0, s>>>(a);
-            CK(cudaGetLastError());
-        }
-        din.upload(ntr_in, s);
-        drows.upload(ntr_rows, s);
-        dcols.upload(ntr_cols, s);
-        launch_transpose_blocks<double2>(c->N.p, din.p, drows.p, dcols.p, c->ntoff.p, ntn, c->NT.p, s);
-        CK(cudaGetLastError());
-        if (c->f32) {
-            auto down = [&](DBuf<double2> &src, DBuf<float2> &dst) {
-                dst.alloc(src.n);
-                if (src.n) k_to_f32<<<launch_grid(int64_t(src.n) / 256 + 1, 8), 256, 0, s>>>(src.p, dst.p, int64_t(src.n));
-                CK(cudaGetLastError());
-            };
-            for (int sd = 0; sd < 2; ++sd) {
-                down(c->side[sd].X, c->side[sd].X32);
-                down(c->side[sd].XT, c->side[sd].XT32);
-            }
-            down(c->C, c->C32);
-            down(c->CT, c->CT32);
-            down(c->N, c->N32);
-            down(c->NT, c->NT32);
-        }
-        CK(cudaEventRecord(ev1, s));
-        CK(cudaStreamSynchronize(s));
-    }
+    c->near_t.upload(near_t, s);
+    c->ntr_in.upload(ntr_in, s);
+    c->ntr_rows.upload(ntr_rows, s);
+    c->ntr_cols.upload(ntr_cols, s);
+    c->n_ntr = ntn;
+    fill_near(c, c->K, c->N.p, c->NT.p, s);
+    if (c->f32) make_f32_copies(c, s);
+    CK(cudaEventRecord(ev1, s));
+    CK(cudaStreamSynchronize(s));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
     auto h2 = std::chrono::steady_clock::now();
@@ -815,6 +893,148 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
     return NCA_OK;
 }
 
+// Enqueues y = alpha (dH/dk) x + beta y (forward mode, complex FP64) on the frozen skeleton:
+// the product's sweeps carried as dual numbers (xhat, dxhat) and (yhat, dyhat):
+//   up       xhat_p = X_p^T src_p,   dxhat_p = dX_p^T src_p + X_p^T dxhat_children
+//   coupling yhat = S xhat,          dyhat = S dxhat + dS xhat
+//   down     yhat_c += X_p yhat_p,   dyhat_c += X_p dyhat_p + dX_p yhat_p
+//   leaves   dy_t = X_t dyhat_t + dX_t yhat_t + sum_s dN_ts x_s
+// dxhat and dyhat have the shapes of xhat and yhat.
+int enqueue_tangent(nca_core *c, const double2 *xd, int64_t lx, double2 *yd, int64_t ly, int b, double2 alpha,
+                    double2 beta, const ProductBuffers &buf, double2 *dxhat, double2 *dyhat, cudaStream_t s,
+                    ProductLaunches &count) {
+    DevSide &I = c->side[1], &O = c->side[0];
+    const int64_t nin = I.npts;
+    const int vs = vector_stride(b);
+    const int cap = rows_capacity(std::min(b, 16));
+    if (O.leafcap > cap || I.leafcap > cap || 2 * c->maxrank > cap)
+        return fail(NCA_ERR_ARG, "a leaf or transfer block has more rows than one product CTA holds");
+    k_gather<<<launch_grid(nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, I.perm.p, nin, b, vs, buf.xt);
+    ++count.total;
+    auto go = [&](RowArgs<double2> &a, const int32_t *nodes, int cnt) {
+        a.error = buf.error;
+        a.b = b;
+        a.vs = vs;
+        launch_rows<double2>(a, nodes, cnt, s);
+        ++count.total;
+    };
+    for (int q0 = 0; q0 < b; q0 += 16) {
+        const int bc = std::min(16, b - q0);
+        for (size_t l = 0; l + 1 < I.up.ptr.size(); ++l) {
+            const int cnt = I.up.ptr[l + 1] - I.up.ptr[l];
+            if (!cnt) continue;
+            const int32_t *nodes = I.up.d_nodes.p + I.up.ptr[l];
+            for (int pass = 0; pass < 3; ++pass) {
+                RowArgs<double2> a{};
+                a.stage = STAGE_UP;
+                a.begin = I.begin.p;
+                a.firstchild = I.firstchild.p;
+                a.nchildren = I.nchildren.p;
+                a.rank = I.rank.p;
+                a.nrows = I.nrows.p;
+                a.cptr = I.cptr.p;
+                a.moff = I.xoff.p;
+                a.src = buf.xt;
+                a.bc = bc;
+                a.q0 = q0;
+                a.maxrows = I.up.mcap[l];
+                if (pass == 0) {  // xhat_p = X_p^T src
+                    a.M = I.XT.p;
+                    a.coef = buf.xhat;
+                } else if (pass == 1) {  // dxhat_p = dX_p^T src
+                    a.M = I.dXT.p;
+                    a.coef = buf.xhat;
+                    a.coef_out = dxhat;
+                } else {  // dxhat_p += X_p^T dxhat_children
+                    a.M = I.XT.p;
+                    a.coef = dxhat;
+                    a.accumulate = 1;
+                    a.skip_leaves = 1;
+                }
+                go(a, nodes, cnt);
+            }
+        }
+        const int ncp = c->n_couple_fwd;
+        if (ncp > 0)
+            for (int pass = 0; pass < 3; ++pass) {
+                RowArgs<double2> a{};
+                a.stage = STAGE_COUPLE;
+                a.M = pass == 2 ? c->dC.p : c->C.p;
+                a.moff = c->cfoff.p;
+                a.ptr = c->farptr.p;
+                a.other = c->farnodes.p;
+                a.rank_in = I.rank.p;
+                a.rank_out = O.rank.p;
+                a.cptr_in = I.cptr.p;
+                a.cptr_out = O.cptr.p;
+                a.src = pass == 1 ? dxhat : buf.xhat;
+                a.dst = pass == 0 ? buf.yhat : dyhat;
+                a.accumulate = pass == 2;
+                a.bc = bc;
+                a.q0 = q0;
+                a.maxrows = c->maxrank;
+                go(a, c->couple_fwd.p, ncp);
+            }
+        for (size_t l = 0; l + 1 < O.down.ptr.size(); ++l) {
+            const int cnt = O.down.ptr[l + 1] - O.down.ptr[l];
+            if (!cnt) continue;
+            for (int pass = 0; pass < 3; ++pass) {
+                RowArgs<double2> a{};
+                a.stage = STAGE_DOWN;
+                a.firstchild = O.firstchild.p;
+                a.rank = O.rank.p;
+                a.nrows = O.nrows.p;
+                a.cptr = O.cptr.p;
+                a.moff = O.xoff.p;
+                a.M = pass == 2 ? O.dX.p : O.X.p;
+                a.coef = pass == 1 ? dyhat : buf.yhat;
+                a.coef_out = pass == 2 ? dyhat : nullptr;
+                a.bc = bc;
+                a.q0 = q0;
+                a.maxrows = O.down.mcap[l];
+                go(a, O.down.d_nodes.p + O.down.ptr[l], cnt);
+            }
+        }
+        for (int pass = 0; pass < 2; ++pass) {
+            RowArgs<double2> a{};
+            a.stage = STAGE_LEAVES;
+            a.begin = O.begin.p;
+            a.end = O.end.p;
+            a.perm = O.perm.p;
+            a.rank = O.rank.p;
+            a.cptr = O.cptr.p;
+            a.xoff = O.xoff.p;
+            a.o_begin = I.begin.p;
+            a.o_end = I.end.p;
+            a.src = buf.xt;
+            a.y = yd;
+            a.ldy = ly;
+            a.alpha = alpha;
+            if (pass == 0) {  // y = alpha (X dyhat + dN x) + beta y
+                a.X = O.X.p;
+                a.coef = dyhat;
+                a.M = c->dN.p;
+                a.moff = c->nfoff.p;
+                a.ptr = c->nearptr.p;
+                a.other = c->nearnodes.p;
+                a.beta = beta;
+                a.usebeta = beta.x != 0.0 || beta.y != 0.0;
+            } else {  // y += alpha dX yhat
+                a.X = O.dX.p;
+                a.coef = buf.yhat;
+                a.beta = make_double2(1.0, 0.0);
+                a.usebeta = 1;
+            }
+            a.bc = bc;
+            a.q0 = q0;
+            a.maxrows = O.leafcap;
+            go(a, O.leaves.p, O.nleaves);
+        }
+    }
+    CK(cudaGetLastError());
+    return NCA_OK;
+}
+
 // Argument checks shared by the product entry points.
 int check_product_args(nca_core *c, int mode, int precision, int64_t ldx, int64_t ldy, int64_t nrhs) {
     if (mode < 0 || mode > 2) return fail(NCA_ERR_ARG, "mode must be 0 (N), 1 (T) or 2 (C)");
@@ -828,10 +1048,13 @@ int check_product_args(nca_core *c, int mode, int precision, int64_t ldx, int64_
 }
 
 int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_t ldx, void *y,
-               int64_t ldy, int64_t nrhs, double2 alpha, double2 beta, int memspace) {
+               int64_t ldy, int64_t nrhs, double2 alpha, double2 beta, int memspace, bool tangent = false) {
     nca_core *c = ws->core;
     if (c->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
     if (int st = check_product_args(c, mode, precision, ldx, ldy, nrhs)) return st;
+    if (tangent && (mode != 0 || precision != NCA_PREC_F64))
+        return fail(NCA_ERR_ARG, "the d/dk product is forward mode and complex FP64");
+    if (tangent && !c->has_dk) return fail(NCA_ERR_ARG, "call nca_core_prepare_dk before the d/dk product");
     const int in = mode == 0 ? 1 : 0, out = 1 - in;
     const int64_t nin = c->side[in].npts, nout = c->side[out].npts;
     if (nrhs == 0) return NCA_OK;
@@ -866,11 +1089,19 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
         lx = nin;
         ly = nout;
     }
+    if (tangent && ws->dxhat.n < ws->xhat.n) {
+        ws->dxhat.alloc(ws->xhat.n);
+        ws->dyhat.alloc(ws->xhat.n);
+    }
     const ProductBuffers buf{ws->xt.p, ws->xhat.p, ws->yhat.p, ws->error.p, ws->far, ws->near};
     ProductLaunches count;
-    if (int st = enqueue_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, buf, s,
-                                 ws->profiling ? ws->stage_ev : nullptr, count))
+    if (tangent) {
+        if (int st = enqueue_tangent(c, xd, lx, yd, ly, b, alpha, beta, buf, ws->dxhat.p, ws->dyhat.p, s, count))
+            return st;
+    } else if (int st = enqueue_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, buf, s,
+                                        ws->profiling ? ws->stage_ev : nullptr, count)) {
         return st;
+    }
     CK(cudaMemcpyAsync(ws->error_host, ws->error.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     if (memspace == 0)
         CK(cudaMemcpy2DAsync(y, sizeof(double2) * ldy, ws->ystage.p, sizeof(double2) * nout,
@@ -881,7 +1112,7 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     CK(cudaEventElapsedTime(&ms, ws->e0, ws->e1));
     ws->last_seconds = ms * 1e-3;
     ws->last_launches = count.total;
-    if (ws->profiling) {
+    if (ws->profiling && !tangent) {
         for (int k = 0; k < 5; ++k) {
             float t = 0.f;
             CK(cudaEventElapsedTime(&t, ws->stage_ev[k], ws->stage_ev[k + 1]));
@@ -1209,6 +1440,7 @@ void merge_core(const std::vector<nca_core *> &cs, nca_core *m, bool move, cudaS
         m->tnearptr.upload(P.tnearptr, s);
         m->tnearnodes.upload(P.tnearnodes, s);
     }
+    m->batch = true;
     if (move)
         for (nca_core *c : cs) c->moved = true;
     // storage summary: sums of the members'
@@ -1316,6 +1548,10 @@ int apply_static_impl(nca_core *c, int mode, int precision, const void *x, int64
     if (err != 0) return fail(NCA_ERR_CUDA, "internal: a product copy was misaligned and skipped");
     return NCA_OK;
 }
+
+int entries_impl(const nca_kernel_desc *kernel, const double *testpoints, int64_t ntest, const double *trialpoints,
+                 int64_t ntrial, const int64_t *ii, const int64_t *jj, int64_t n, int32_t device, double *out,
+                 int deriv);
 
 }  // namespace
 
@@ -1457,6 +1693,84 @@ void nca_core_destroy(nca_core *core) {
     if (!core) return;
     cudaSetDevice(core->device);
     delete core;
+}
+
+int32_t nca_core_set_wavenumber(nca_core *core, double k) {
+    return guarded([&] {
+        if (!core) return fail(NCA_ERR_ARG, "null core");
+        if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
+        if (core->batch) return fail(NCA_ERR_ARG, "a batch has one wavenumber per member: refill the members");
+        if (core->K.kind == NCA_KERNEL_MATRIX) return fail(NCA_ERR_ARG, "a matrix kernel has no wavenumber");
+        if (!std::isfinite(k)) return fail(NCA_ERR_ARG, "the wavenumber must be finite");
+        CK(cudaSetDevice(core->device));
+        cudaStream_t s;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() { cudaStreamDestroy(s); }
+        } sg{s};
+        KernelParams K = core->K;
+        K.k = k;
+        K.deriv = 0;
+        // new bases first (a singular frozen cross matrix leaves the core unchanged)
+        DBuf<double2> X[2], XT[2];
+        for (int sd = 0; sd < 2; ++sd) {
+            X[sd].alloc(core->side[sd].X.n);
+            XT[sd].alloc(core->side[sd].X.n);
+            fill_bases(core, sd, 0, K, K, X[sd].p, XT[sd].p, s);
+        }
+        for (int sd = 0; sd < 2; ++sd) {
+            std::swap(core->side[sd].X.p, X[sd].p);
+            std::swap(core->side[sd].XT.p, XT[sd].p);
+            core->side[sd].dX.release();
+            core->side[sd].dXT.release();
+        }
+        core->K.k = k;
+        fill_couplings(core, K, core->C.p, core->CT.p, s);
+        fill_near(core, K, core->N.p, core->NT.p, s);
+        if (core->f32) make_f32_copies(core, s);
+        core->dC.release();
+        core->dCT.release();
+        core->dN.release();
+        core->dNT.release();
+        core->has_dk = false;
+        CK(cudaStreamSynchronize(s));
+        return int(NCA_OK);
+    });
+}
+
+int32_t nca_core_prepare_dk(nca_core *core) {
+    return guarded([&] {
+        if (!core) return fail(NCA_ERR_ARG, "null core");
+        if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
+        if (core->batch) return fail(NCA_ERR_ARG, "prepare the d/dk stores of the members, not of a batch");
+        if (core->K.kind == NCA_KERNEL_MATRIX) return fail(NCA_ERR_ARG, "a matrix kernel has no wavenumber derivative");
+        if (core->has_dk) return int(NCA_OK);
+        CK(cudaSetDevice(core->device));
+        cudaStream_t s;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() { cudaStreamDestroy(s); }
+        } sg{s};
+        KernelParams dK = core->K;
+        dK.deriv = 1;
+        for (int sd = 0; sd < 2; ++sd) {
+            DevSide &d = core->side[sd];
+            d.dX.alloc(d.X.n);
+            d.dXT.alloc(d.X.n);
+            fill_bases(core, sd, 1, core->K, dK, d.dX.p, d.dXT.p, s);
+        }
+        core->dC.alloc(core->C.n);
+        core->dCT.alloc(core->CT.n);
+        fill_couplings(core, dK, core->dC.p, core->dCT.p, s);
+        core->dN.alloc(core->N.n);
+        core->dNT.alloc(core->NT.n);
+        fill_near(core, dK, core->dN.p, core->dNT.p, s);
+        CK(cudaStreamSynchronize(s));
+        core->has_dk = true;
+        return int(NCA_OK);
+    });
 }
 
 int32_t nca_core_batch(nca_core *const *cores, int32_t ncores, int32_t flags, nca_core **out) {
@@ -1640,6 +1954,20 @@ int32_t nca_apply_static(nca_core *core, int32_t mode, int32_t precision, const 
     });
 }
 
+int32_t nca_apply_dk(nca_workspace *ws, const void *x, int64_t ldx, void *y, int64_t ldy, int64_t nrhs,
+                     double alpha_re, double alpha_im, double beta_re, double beta_im, int32_t memspace) {
+    if (!ws) return fail(NCA_ERR_ARG, "null workspace");
+    bool expected = false;
+    if (!ws->busy.compare_exchange_strong(expected, true))
+        return fail(NCA_ERR_BUSY, "ConcurrentWorkspaceError: the workspace is in use by another matrix-vector product");
+    int st = guarded([&] {
+        return apply_impl(ws, 0, NCA_PREC_F64, x, ldx, y, ldy, nrhs, make_double2(alpha_re, alpha_im),
+                          make_double2(beta_re, beta_im), memspace, true);
+    });
+    ws->busy.store(false);
+    return st;
+}
+
 int32_t nca_workspace_last_time(const nca_workspace *ws, double *seconds) {
     if (!ws || !seconds) return fail(NCA_ERR_ARG, "null argument");
     *seconds = ws->last_seconds;
@@ -1767,6 +2095,22 @@ int32_t nca_blocks_factors(const double *buffer, int64_t ldbuffer, int32_t ldcol
 int32_t nca_entries(const nca_kernel_desc *kernel, const double *testpoints, int64_t ntest,
                     const double *trialpoints, int64_t ntrial, const int64_t *ii, const int64_t *jj, int64_t n,
                     int32_t device, double *out) {
+    return entries_impl(kernel, testpoints, ntest, trialpoints, ntrial, ii, jj, n, device, out, 0);
+}
+
+int32_t nca_entries_dk(const nca_kernel_desc *kernel, const double *testpoints, int64_t ntest,
+                       const double *trialpoints, int64_t ntrial, const int64_t *ii, const int64_t *jj, int64_t n,
+                       int32_t device, double *out) {
+    if (kernel && kernel->kind == NCA_KERNEL_MATRIX) return fail(NCA_ERR_ARG, "a matrix kernel has no wavenumber derivative");
+    return entries_impl(kernel, testpoints, ntest, trialpoints, ntrial, ii, jj, n, device, out, 1);
+}
+
+}  // extern "C"
+
+namespace {
+int entries_impl(const nca_kernel_desc *kernel, const double *testpoints, int64_t ntest, const double *trialpoints,
+                 int64_t ntrial, const int64_t *ii, const int64_t *jj, int64_t n, int32_t device, double *out,
+                 int deriv) {
     return guarded([&] {
         if (!kernel || n < 0) return fail(NCA_ERR_ARG, "bad argument");
         if (n == 0) return int(NCA_OK);
@@ -1783,6 +2127,7 @@ int32_t nca_entries(const nca_kernel_desc *kernel, const double *testpoints, int
         dj.upload(jj, size_t(n), nullptr);
         DBuf<double2> dout;
         dout.alloc(size_t(n));
+        tmp.K.deriv = deriv;
         k_entries<<<launch_grid(n / 256 + 1, 8), 256>>>(tmp.K, tp.p, sp.p, di.p, dj.p, n, dout.p);
         CK(cudaGetLastError());
         CK(cudaMemcpy(out, dout.p, sizeof(double2) * n, cudaMemcpyDeviceToHost));
@@ -1790,4 +2135,5 @@ int32_t nca_entries(const nca_kernel_desc *kernel, const double *testpoints, int
     });
 }
 
-}  // extern "C"
+}  // namespace
+

@@ -1,5 +1,6 @@
 // Device kernel-entry generator: Helmholtz cis(sign k r)/(4 pi r), Laplace 1/(4 pi r), and a
-// matrix-backed kernel (AdaptiveCrossApproximation.PointMatrix, test/test_couplingmatrices.jl:15).
+// matrix-backed kernel (AdaptiveCrossApproximation.PointMatrix, test/test_couplingmatrices.jl:15),
+// plus the wavenumber derivatives of the point kernels (gradients on frozen skeletons).
 //
 // The pivots of the batched build are argmax decisions on these values, so every rounding
 // step is spelled out with _rn intrinsics (no contraction, no library sin/cos): the host
@@ -23,6 +24,7 @@ struct KernelParams {
     double rmin;
     const double2 *mat;  // NCA_KERNEL_MATRIX: device copy, column-major
     int64_t ldmat;
+    int deriv;           // 1: entries of dK/dk instead of K (Helmholtz and Laplace only)
 };
 
 __device__ __forceinline__ void sincos_cw(double x, double *s, double *c) {
@@ -74,6 +76,15 @@ __device__ __forceinline__ double2 kernel_entry(const KernelParams &K, double x0
     double r = __dsqrt_rn(d2);
     if (r == 0.0 || r < K.rmin) return make_double2(0.0, 0.0);
     const double FOUR_PI = 0x1.921fb54442d18p+3;
+    if (K.deriv) {
+        // d/dk cis(sign k r) / (4 pi r) = (-sin(k r) + i sign cos(k r)) / (4 pi); Laplace: 0
+        if (K.kind == 1) return make_double2(0.0, 0.0);
+        double s, c;
+        sincos_cw(__dmul_rn(K.k, r), &s, &c);
+        const double inv4pi = __ddiv_rn(1.0, FOUR_PI);
+        const double re = -__dmul_rn(s, inv4pi), im = __dmul_rn(c, inv4pi);
+        return make_double2(re, K.sign < 0 ? -im : im);
+    }
     double inv = __ddiv_rn(1.0, __dmul_rn(FOUR_PI, r));
     if (K.kind == 1) return make_double2(inv, 0.0);
     double s, c;

@@ -12,7 +12,7 @@ from .admissibility import FarData, fardata, farfield, farinteractions, farnodes
 from .compressors import ACA, BatchedBottomUp, FNormEstimator, FullPivoting, TreeMimicryPivoting, _clustersize, \
     _selectfarpivots
 from .kernels import HelmholtzKernel, LaplaceKernel, MatrixKernel
-from .nca import (BatchCore, H2Workspace, PetrovGalerkinNCA, PetrovGalerkinNCACore, adjoint, batch, core, farmatrix, mul, nearmatrix,
+from .nca import (BatchCore, H2Workspace, dHdk, rrule_mul, PetrovGalerkinNCA, PetrovGalerkinNCACore, adjoint, batch, core, farmatrix, mul, nearmatrix,
                   storage, transpose, withworkspace)
 from .trees import BlockTree, KMeansTree, KMeansTreeBuilder, testtree, trialtree
 from .utils import collect_assigned, plan_from_pivots, ptrfromcounts

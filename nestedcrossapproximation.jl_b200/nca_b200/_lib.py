@@ -103,6 +103,10 @@ SIGNATURES = {
     "nca_blocks_aca": (I32, [P, I64, I32, P, P, I32, I32, D, I32, I32, P, P, P]),
     "nca_blocks_factors": (I32, [P, I64, I32, P, I32, P, P, P, I32, I32, P, P]),
     "nca_entries": (I32, [P, P, I64, P, I64, P, P, I64, I32, P]),
+    "nca_entries_dk": (I32, [P, P, I64, P, I64, P, P, I64, I32, P]),
+    "nca_core_set_wavenumber": (I32, [P, D]),
+    "nca_core_prepare_dk": (I32, [P]),
+    "nca_apply_dk": (I32, [P, P, I64, P, I64, I64, D, D, D, D, I32]),
 }
 
 _lib = None

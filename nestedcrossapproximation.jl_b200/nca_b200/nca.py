@@ -92,6 +92,23 @@ class PetrovGalerkinNCACore:
     def shape(self):
         return self.dim
 
+    # ---- frozen-skeleton refills and derivatives ----
+    @property
+    def wavenumber(self):
+        return getattr(self.operator, "k", None)
+
+    def set_wavenumber(self, k: float):
+        """Refill every store at wavenumber k with the frozen skeleton (tree, ranks and pivots of
+        the build); bit-identical to the build at the build's own k."""
+        check(lib().nca_core_set_wavenumber(self._h, float(k)))
+        op = self.operator
+        self.operator = type(op)(float(k), sign=op.sign, rmin=op.rmin)
+        self._cache = {}
+
+    def prepare_dk(self):
+        """Device stores of dX/dk, dS/dk and dN/dk on the frozen skeleton (for dHdk products)."""
+        check(lib().nca_core_prepare_dk(self._h))
+
     # ---- exports (host copies of the device stores) ----
     def pivots(self, side: int):
         """Pivots per node (None for nodes without far field), ranks and block rows."""
@@ -394,9 +411,18 @@ def _is_torch(x):
     return type(x).__module__.startswith("torch")
 
 
-def mul(y, A, x, alpha=1.0, beta=0.0):
+def _product(ws, mode, xp, nin, yp, nout, nrhs, al, be, memspace, tangent):
+    if tangent:
+        return lib().nca_apply_dk(ws._h, xp, nin, yp, nout, nrhs, al.real, al.imag, be.real, be.imag, memspace)
+    return lib().nca_apply(ws._h, mode, ws.precision, xp, nin, yp, nout, nrhs, al.real, al.imag, be.real, be.imag,
+                           memspace)
+
+
+def mul(y, A, x, alpha=1.0, beta=0.0, _tangent=False):
     """y = alpha op(A) x + beta y (LinearMaps' 5-argument mul!). y None allocates it."""
     ws, mode = _unwrap(A)
+    if _tangent and (mode != MODE_N or ws.precision != PREC_F64):
+        raise ArgumentError("the d/dk product is forward mode on a complex FP64 workspace")
     core = ws.core
     nin = core.dim[1] if mode == MODE_N else core.dim[0]
     nout = core.dim[0] if mode == MODE_N else core.dim[1]
@@ -416,8 +442,8 @@ def mul(y, A, x, alpha=1.0, beta=0.0):
             raise ConcurrentWorkspaceError()
         try:
             al, be = complex(alpha), complex(beta)
-            check(lib().nca_apply(ws._h, mode, ws.precision, C.c_void_p(Xr.data_ptr()), nin,
-                                  C.c_void_p(Yr.data_ptr()), nout, nrhs, al.real, al.imag, be.real, be.imag, 1))
+            check(_product(ws, mode, C.c_void_p(Xr.data_ptr()), nin, C.c_void_p(Yr.data_ptr()), nout, nrhs, al, be,
+                           1, _tangent))
         finally:
             ws._lock.release()
         out = Yr.t()
@@ -446,8 +472,7 @@ def mul(y, A, x, alpha=1.0, beta=0.0):
         raise ConcurrentWorkspaceError()
     try:
         al, be = complex(alpha), complex(beta)
-        check(lib().nca_apply(ws._h, mode, ws.precision, ptr(X), nin, ptr(Y), nout, nrhs, al.real, al.imag,
-                              be.real, be.imag, 0))
+        check(_product(ws, mode, ptr(X), nin, ptr(Y), nout, nrhs, al, be, 0, _tangent))
         t = C.c_double()
         lib().nca_workspace_last_time(ws._h, C.byref(t))
         ws.last_seconds = t.value
@@ -458,6 +483,47 @@ def mul(y, A, x, alpha=1.0, beta=0.0):
         target[...] = out.reshape(target.shape).astype(target.dtype, copy=False)
         return target
     return out.astype(ws.dtype, copy=False) if ws.dtype != np.complex128 else out
+
+
+class _DHDK(LinearMap):
+    """dH/dk of an FP64 workspace on its frozen skeleton, forward mode (y = dH/dk x)."""
+
+    def __init__(self, ws):
+        self.ws = ws
+        self.shape = ws.shape
+
+    def _apply(self, x, mode):
+        if mode != MODE_N:
+            raise ArgumentError("dH/dk is applied in forward mode only (use the real part of y_bar^H dH/dk x)")
+        self.ws.core.prepare_dk()
+        return mul(None, self.ws, x, _tangent=True)
+
+
+def dHdk(A) -> LinearMap:
+    """dH/dk as a forward-mode linear map on the frozen skeleton of A's core."""
+    ws, mode = _unwrap(A)
+    if mode != MODE_N:
+        raise ArgumentError("dH/dk is taken of H itself (forward mode); use Re(y_bar^H dH/dk x) for transposes")
+    return _DHDK(ws)
+
+
+def rrule_mul(A, x):
+    """ChainRulesCore-style rrule of y = H(k) x: returns (y, pullback) with
+    pullback(y_bar) = (k_bar, x_bar), x_bar = H^H y_bar (the adjoint product) and
+    k_bar = Re(y_bar^H dH/dk x) (the tangent product on the frozen skeleton). Cotangents follow
+    ChainRules' convention dJ = Re<y_bar, dy>, so J = ||y - b||^2 gives y_bar = 2 (y - b)."""
+    ws, mode = _unwrap(A)
+    if mode != MODE_N:
+        raise ArgumentError("rrule_mul differentiates y = H x")
+    y = A @ x
+    x_saved = x.copy() if hasattr(x, "copy") else x
+
+    def pullback(ybar):
+        xbar = ws.H @ ybar
+        dy = dHdk(ws) @ x_saved
+        kbar = float(np.real(np.vdot(np.asarray(ybar), np.asarray(dy))))
+        return kbar, xbar
+    return y, pullback
 
 
 class BatchCore(PetrovGalerkinNCACore):

@@ -54,8 +54,8 @@ def blocks_factors(blocks, ranks, rowpivots, colpivots, maxrank, device=0, width
     return [Z[zoff[i]:zoff[i + 1]].reshape((int(rk[i]), blocks[i].shape[0]), order="F") for i in range(nb)]
 
 
-def entries(kernel, testpoints, trialpoints, ii, jj, device=0):
-    """Kernel entries A(ii[e], jj[e]) evaluated on the device."""
+def entries(kernel, testpoints, trialpoints, ii, jj, device=0, dk=False):
+    """Kernel entries A(ii[e], jj[e]) evaluated on the device (dk=True: their d/dk)."""
     tp = np.ascontiguousarray(testpoints, dtype=np.float64).reshape(-1, 3)
     sp = np.ascontiguousarray(trialpoints, dtype=np.float64).reshape(-1, 3)
     ii = np.ascontiguousarray(ii, dtype=np.int64)
@@ -63,6 +63,6 @@ def entries(kernel, testpoints, trialpoints, ii, jj, device=0):
     out = np.zeros(max(len(ii), 1), dtype=np.complex128)
     d = kernel.desc()
     import ctypes as C
-    check(lib().nca_entries(C.byref(d), ptr(tp), len(tp), ptr(sp), len(sp), ptr(ii), ptr(jj), len(ii), int(device),
-                            ptr(out)))
+    f = lib().nca_entries_dk if dk else lib().nca_entries
+    check(f(C.byref(d), ptr(tp), len(tp), ptr(sp), len(sp), ptr(ii), ptr(jj), len(ii), int(device), ptr(out)))
     return out[:len(ii)]
