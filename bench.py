@@ -46,8 +46,9 @@ def parse():
     p.add_argument("--nrhs", type=int, default=16)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-stages", action="store_true", help="print per-stage times to stderr")
-    p.add_argument("--workload", default="galerkin-sphere", choices=["galerkin-sphere", "batched-uneven"],
-                   help="batched-uneven: 64 problems of uneven size, one batched product vs 64 calls")
+    p.add_argument("--workload", default="galerkin-sphere", choices=["galerkin-sphere", "batched-uneven", "gradients"],
+                   help="batched-uneven: 64 problems of uneven size, one batched product vs 64 calls; "
+                        "gradients: dJ/dx and dJ/dk of J = ||H(k) x - b||^2 on a perturbed sphere")
     return p.parse_args()
 
 
@@ -406,6 +407,128 @@ def run_batched(args):
             "gpu_launches": launches.value, "clocks": clk}), flush=True)
 
 
+def perturbed_sphere(n, seed):
+    """r(theta, phi) = 1 + 0.1 sin(3 theta) cos(2 phi), (cos theta, phi) uniform."""
+    rng = np.random.default_rng(seed)
+    ct = rng.uniform(-1.0, 1.0, n)
+    ph = rng.uniform(0.0, 2 * np.pi, n)
+    th = np.arccos(ct)
+    r = 1.0 + 0.1 * np.sin(3 * th) * np.cos(2 * ph)
+    st = np.sqrt(1.0 - ct * ct)
+    return np.stack([r * st * np.cos(ph), r * st * np.sin(ph), r * ct], axis=1)
+
+
+def run_gradients(args):
+    """131,072 points on a perturbed sphere, Helmholtz k = 20, tol 1e-5 (standard admissibility,
+    maxrank 50), skeleton frozen after the build; J = ||H(k) x - b||^2 with 4 right-hand sides.
+    One step = one gradient: y = H x, x_bar = H^H (2 (y - b)), k_bar = Re(y_bar^H dH/dk x)
+    (forward, adjoint and tangent products). The d/dk stores are prepared once per skeleton and
+    timed separately. k_bar is checked against central differences (h = 1e-6 k) of frozen refills."""
+    import torch
+    import nca_b200 as N
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    n, b, k = 131072, 4, 20.0
+    pts = perturbed_sphere(n, 4242)
+    tree = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=64))
+    aca = N.ACA(N.FullPivoting(), N.FullPivoting(), N.FNormEstimator(1e-5))
+    comp = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(pts, pts, tree), compressor=aca)
+    t0 = time.perf_counter()
+    core = N.PetrovGalerkinNCACore(N.HelmholtzKernel(k, rmin=1e-12), pts, pts, N.BlockTree(tree, tree),
+                                   testcompressor=comp, trialcompressor=comp, device=local)
+    build_wall = time.perf_counter() - t0
+    info = info_dict(core)
+    ws = N.H2Workspace(core, max_nrhs=b)
+    L = N.lib()
+    X = rhs(n, b, seed=5)
+    B = rhs(n, b, seed=6)
+    dev = f"cuda:{local}"
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(dev)
+    Bd = torch.from_numpy(np.ascontiguousarray(B.T)).to(dev)
+    Yd, Rd, Xb, Dy = (torch.zeros_like(Xd) for _ in range(4))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    core.prepare_dk()
+    torch.cuda.synchronize()
+    prep = time.perf_counter() - t0
+
+    def grad():
+        N._lib.check(L.nca_apply(ws._h, 0, 0, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Yd.data_ptr()), n, b,
+                                 1.0, 0.0, 0.0, 0.0, 1))
+        torch.sub(Yd, Bd, out=Rd)
+        Rd.mul_(2.0)
+        N._lib.check(L.nca_apply(ws._h, 2, 0, C.c_void_p(Rd.data_ptr()), n, C.c_void_p(Xb.data_ptr()), n, b,
+                                 1.0, 0.0, 0.0, 0.0, 1))
+        N._lib.check(L.nca_apply_dk(ws._h, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Dy.data_ptr()), n, b,
+                                    1.0, 0.0, 0.0, 0.0, 1))
+        return torch.vdot(Rd.reshape(-1), Dy.reshape(-1)).real
+    for _ in range(max(args.warmup, 3)):
+        grad()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        kbar = grad()
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    el = e0.elapsed_time(e1) * 1e-3 / args.steps
+    kbar = float(kbar.item())
+    # central differences of J on the frozen skeleton
+    h = 1e-6 * k
+
+    def J():
+        N._lib.check(L.nca_apply(ws._h, 0, 0, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Yd.data_ptr()), n, b,
+                                 1.0, 0.0, 0.0, 0.0, 1))
+        return float(((Yd - Bd).abs() ** 2).sum().item())
+    core.set_wavenumber(k + h)
+    jp = J()
+    core.set_wavenumber(k - h)
+    jm = J()
+    core.set_wavenumber(k)
+    fd = (jp - jm) / (2 * h)
+    err = dense_rows_error_k(N, pts, core, ws, X, k) if rank == 0 else None
+    step_bytes = 2 * product_bytes(info, b) + tangent_bytes(info, b)
+    peak, peak_kind = peaks()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": step_bytes / el / 1e9, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "complex-f64", "data": "synthetic",
+            "config": {"workload": "gradients-perturbed-sphere-131072-k20-tol1e-5-4rhs", "npoints": n, "nrhs": b,
+                       "k": k, "admissibility": "standard isnear (eta 1), maxrank 50",
+                       "step": "one gradient: H x, H^H (2 (Hx - b)), dH/dk x",
+                       "l2": "inputs larger than L2", "build_s": build_wall, "prepare_dk_s": prep,
+                       "stored_gb": E * store_entries(info) / 1e9, "relerr_vs_dense_rows": err},
+            "gradients_per_s": 1.0 / el, "k_bar": kbar, "k_bar_central_difference": fd,
+            "k_bar_relerr_vs_fd": abs(kbar - fd) / abs(fd),
+            "roofline": {"bound": "hbm", "achieved": step_bytes / el / 1e9, "peak": peak, "peak_source": peak_kind,
+                         "unit": "GB/s", "frac": step_bytes / el / 1e9 / peak, "traffic": None,
+                         "note": "whole gradient step (three products), algorithmic bytes"},
+            "clocks": clk}), flush=True)
+
+
+def tangent_bytes(info, b, e=E):
+    """Algorithmic bytes of one tangent product: every stored entry and its d/dk twice as many
+    stores (X, dX, S, dS, N, dN), x read, y written, four coefficient vectors written and read."""
+    vec = e * b * (info["ntrial"] + 2 * info["ntest"]) + 4 * e * b * (info["ncoeff_test"] + info["ncoeff_trial"])
+    return 2 * e * store_entries(info) + vec
+
+
+def dense_rows_error_k(N, pts, core, ws, X, k, nrows=64):
+    rng = np.random.default_rng(7)
+    rows = rng.choice(len(pts), nrows, replace=False)
+    ii = np.repeat(rows, len(pts))
+    jj = np.tile(np.arange(len(pts)), nrows)
+    D = N.seams.entries(N.HelmholtzKernel(k, rmin=1e-12), pts, pts, ii, jj, device=core.device).reshape(nrows, len(pts))
+    Y = N.mul(None, ws, X[:, :1])
+    ref = D @ X[:, :1]
+    return float(np.linalg.norm(Y[rows] - ref) / np.linalg.norm(ref))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -413,6 +536,9 @@ def main():
         return
     if args.workload == "batched-uneven":
         run_batched(args)
+        return
+    if args.workload == "gradients":
+        run_gradients(args)
         return
     import torch
     import torch.distributed as dist
