@@ -57,6 +57,7 @@ typedef struct nca_tree nca_tree;
 typedef struct nca_partition nca_partition;
 typedef struct nca_core nca_core;
 typedef struct nca_workspace nca_workspace;
+typedef struct nca_dirplan nca_dirplan;
 
 int32_t nca_version(void);
 /* Copies the last error message of this thread into buf (always NUL-terminated). */
@@ -81,11 +82,34 @@ int32_t nca_tree_export(const nca_tree *tree, int32_t *perm, int32_t *begin, int
  *      src/admissibility/farinteractions.jl:66-92) ---- */
 int32_t nca_interactions(const nca_tree *test, const nca_tree *trial, double eta,
                          nca_partition **out);
+/* isnearwideband(k; eta_lf, eta_hf, gamma) (src/admissibility/nearinteractions.jl:62-95, bounding
+ * balls): low frequency when k min(d) <= gamma, then near iff max(d) > eta_lf sep; high
+ * frequency near iff 4 k max(r)^2 > eta_hf sep. A core built on this partition is directional. */
+int32_t nca_interactions_wideband(const nca_tree *test, const nca_tree *trial, double k, double etalf,
+                                  double etahf, double gamma, nca_partition **out);
 void nca_partition_destroy(nca_partition *part);
 int32_t nca_partition_sizes(const nca_partition *part, int64_t *nnear, int64_t *nfar);
 int32_t nca_partition_export(const nca_partition *part, int32_t *nearptr, int32_t *nearnodes,
                              int32_t *farptr, int32_t *farnodes, int32_t *trialfarptr,
                              int32_t *trialfarnodes);
+
+/* ---- directional far data of one side (directionalfardata(fardata, tree, fartree, isnear),
+ *      src/admissibility/directionalsubdivision/boundingballdirections.jl:44-152 and
+ *      abstractdirections.jl:57-116) and its basis items, one per (cluster, direction): the
+ *      plan the directional core is built on, exposed for inspection. side 0: test tree
+ *      (far nodes in the trial tree), 1: trial tree. ---- */
+int32_t nca_directional_plan(const nca_tree *tree, const nca_tree *fartree, const nca_partition *part,
+                             int32_t side, nca_dirplan **out);
+void nca_dirplan_destroy(nca_dirplan *plan);
+int32_t nca_dirplan_sizes(const nca_dirplan *plan, int32_t *nitems, int64_t *nfar, int64_t *nchildren);
+/* farnodes[nfar] (grouped by direction), dirptr[nnodes+1], dirs[nitems] (0: low frequency, else the
+ * 1-based candidate direction), dirvec[3 nitems], dirfarptr[nitems+1], item_basis[nitems],
+ * item_chptr[nitems+1], item_chidx[nchildren] (the children's items of nested items). */
+int32_t nca_dirplan_export(const nca_dirplan *plan, int32_t *farnodes, int32_t *dirptr, int32_t *dirs, double *dirvec,
+                           int32_t *dirfarptr, int32_t *item_basis, int32_t *item_chptr, int32_t *item_chidx);
+/* dirfarfield(tree, data, node, dir) of one item (abstractdirections.jl:192-231): its own far
+ * nodes, then those of the ancestors' directions that map onto it. Writes min(n, cap) entries. */
+int32_t nca_dirplan_farfield(const nca_dirplan *plan, int32_t item, int32_t *out, int32_t cap, int32_t *n);
 
 /* ---- phase 1 for one cluster: _selectfarpivots with tree-mimicry pivoting
  *      (src/compressors/batchedbottomup.jl:54-72) ---- */

@@ -28,6 +28,7 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-mfma", "-I", IN
 
 UNITS = [
     ("host_plan.cpp", "cxx", []),
+    ("directional.cpp", "cxx", []),
     ("build_kernels.cu", "nvcc", ["--fmad=false"]),
     ("apply_kernels.cu", "nvcc", []),
     ("capi.cu", "nvcc", []),

@@ -1626,6 +1626,74 @@ int32_t nca_interactions(const nca_tree *test, const nca_tree *trial, double eta
     });
 }
 
+int32_t nca_interactions_wideband(const nca_tree *test, const nca_tree *trial, double k, double etalf,
+                                  double etahf, double gamma, nca_partition **out) {
+    return guarded([&] {
+        if (!test || !trial || !out) return fail(NCA_ERR_ARG, "null argument");
+        if (!(k >= 0.0) || !(etalf > 0.0) || !(etahf > 0.0) || !(gamma > 0.0))
+            return fail(NCA_ERR_ARG, "isnearwideband needs k >= 0 and positive eta_lf, eta_hf, gamma");
+        auto *p = new nca_partition;
+        p->wideband = true;
+        p->w = nca::Wideband{k, etalf, etahf, gamma};
+        p->p = build_partition_wideband(test->t, trial->t, p->w);
+        *out = p;
+        return int(NCA_OK);
+    });
+}
+
+int32_t nca_directional_plan(const nca_tree *tree, const nca_tree *fartree, const nca_partition *part,
+                             int32_t side, nca_dirplan **out) {
+    return guarded([&] {
+        if (!tree || !fartree || !part || !out || side < 0 || side > 1) return fail(NCA_ERR_ARG, "bad argument");
+        if (!part->wideband) return fail(NCA_ERR_ARG, "directional plans need a wideband partition");
+        const nca::Partition &P = part->p;
+        const auto &ptr = side == 0 ? P.farptr : P.tfarptr;
+        const auto &nodes = side == 0 ? P.farnodes : P.tfarnodes;
+        if (int64_t(ptr.size()) != tree->t.nnodes + 1) return fail(NCA_ERR_DIM, "partition does not match the tree");
+        auto *d = new nca_dirplan;
+        d->tree = &tree->t;
+        d->d = directional_plan(tree->t, fartree->t, ptr, nodes, part->w);
+        *out = d;
+        return int(NCA_OK);
+    });
+}
+
+void nca_dirplan_destroy(nca_dirplan *plan) { delete plan; }
+
+int32_t nca_dirplan_sizes(const nca_dirplan *plan, int32_t *nitems, int64_t *nfar, int64_t *nchildren) {
+    if (!plan || !nitems || !nfar || !nchildren) return fail(NCA_ERR_ARG, "null argument");
+    *nitems = int32_t(plan->d.item_node.size());
+    *nfar = int64_t(plan->d.farnodes.size());
+    *nchildren = int64_t(plan->d.item_chidx.size());
+    return NCA_OK;
+}
+
+int32_t nca_dirplan_export(const nca_dirplan *plan, int32_t *farnodes, int32_t *dirptr, int32_t *dirs, double *dirvec,
+                           int32_t *dirfarptr, int32_t *item_basis, int32_t *item_chptr, int32_t *item_chidx) {
+    if (!plan) return fail(NCA_ERR_ARG, "null plan");
+    const nca::DirSide &D = plan->d;
+    std::copy(D.farnodes.begin(), D.farnodes.end(), farnodes);
+    std::copy(D.dirptr.begin(), D.dirptr.end(), dirptr);
+    std::copy(D.dirs.begin(), D.dirs.end(), dirs);
+    std::copy(D.dirvec.begin(), D.dirvec.end(), dirvec);
+    std::copy(D.dirfarptr.begin(), D.dirfarptr.end(), dirfarptr);
+    std::copy(D.item_basis.begin(), D.item_basis.end(), item_basis);
+    std::copy(D.item_chptr.begin(), D.item_chptr.end(), item_chptr);
+    std::copy(D.item_chidx.begin(), D.item_chidx.end(), item_chidx);
+    return NCA_OK;
+}
+
+int32_t nca_dirplan_farfield(const nca_dirplan *plan, int32_t item, int32_t *out, int32_t cap, int32_t *n) {
+    return guarded([&] {
+        if (!plan || !n || item < 0 || item >= int32_t(plan->d.item_node.size())) return fail(NCA_ERR_ARG, "bad argument");
+        std::vector<int32_t> ff;
+        item_farfield(*plan->tree, plan->d, item, ff);
+        *n = int32_t(ff.size());
+        if (out) std::copy(ff.begin(), ff.begin() + std::min<size_t>(ff.size(), size_t(std::max(cap, 0))), out);
+        return int(NCA_OK);
+    });
+}
+
 void nca_partition_destroy(nca_partition *part) { delete part; }
 
 int32_t nca_partition_sizes(const nca_partition *part, int64_t *nnear, int64_t *nfar) {

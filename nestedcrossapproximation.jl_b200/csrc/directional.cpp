@@ -1,0 +1,352 @@
+// Host planning of directional (wideband) H^2 matrices:
+//
+//   build_partition_wideband  near/far pairs with the wideband admissibility
+//                             (src/admissibility/nearinteractions.jl:84-95 for bounding balls):
+//                             low frequency (k min(d) <= gamma): near iff max(d) > eta_lf sep,
+//                             high frequency: near iff 4 k max(r)^2 > eta_hf sep.
+//   directional_plan          per cluster the direction set, the far nodes grouped by their
+//                             nearest direction and the parent-to-child direction map
+//                             (src/admissibility/directionalsubdivision/boundingballdirections.jl:44-152,
+//                             abstractdirections.jl:73-116), then the basis items: one per
+//                             (cluster, direction), a basis item if the cluster is a leaf or a
+//                             high-frequency cluster with low-frequency children
+//                             (abstractdirections.jl:238-243), otherwise nested in the children's
+//                             items of the mapped directions (src/compressors/bottomup.jl:214-320).
+//   item_farfield             the far field of an item: its own far nodes followed by those of
+//                             the ancestors' directions that map onto it (dirfarfield,
+//                             abstractdirections.jl:192-231).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <stdexcept>
+#include <thread>
+
+#include "nca_internal.h"
+
+namespace nca {
+
+namespace {
+
+inline double d2(const double *a, const double *b) {
+    const double x = a[0] - b[0], y = a[1] - b[1], z = a[2] - b[2];
+    return x * x + y * y + z * z;
+}
+
+bool isnear_wideband(const Tree &A, const Tree &B, int a, int b, const Wideband &w) {
+    const double ra = A.radius[a], rb = B.radius[b];
+    const double gap = std::sqrt(d2(&A.center[3 * size_t(a)], &B.center[3 * size_t(b)])) - (ra + rb);
+    const double sep = gap > 0.0 ? gap : 0.0;
+    if (w.k * std::min(2.0 * ra, 2.0 * rb) <= w.gamma) return 2.0 * std::max(ra, rb) > w.etalf * sep;
+    return 4.0 * w.k * std::max(ra * ra, rb * rb) > w.etahf * sep;
+}
+
+struct Pairs {
+    std::vector<int32_t> nt, ns, ft, fs;
+};
+
+void traverse_wideband(const Tree &T, const Tree &S, int t, int s, const Wideband &w, Pairs &out) {
+    if (!isnear_wideband(T, S, t, s, w)) {
+        out.ft.push_back(t);
+        out.fs.push_back(s);
+        return;
+    }
+    const bool lt = T.isleaf(t), ls = S.isleaf(s);
+    if (lt && ls) {
+        out.nt.push_back(t);
+        out.ns.push_back(s);
+    } else if (lt) {
+        for (int c = 0; c < S.nchildren[s]; ++c) traverse_wideband(T, S, t, S.firstchild[s] + c, w, out);
+    } else if (ls) {
+        for (int c = 0; c < T.nchildren[t]; ++c) traverse_wideband(T, S, T.firstchild[t] + c, s, w, out);
+    } else {
+        for (int c = 0; c < T.nchildren[t]; ++c)
+            for (int d = 0; d < S.nchildren[s]; ++d)
+                traverse_wideband(T, S, T.firstchild[t] + c, S.firstchild[s] + d, w, out);
+    }
+}
+
+void csr(const std::vector<int32_t> &key, const std::vector<int32_t> &val, int nrows, std::vector<int32_t> &ptr,
+         std::vector<int32_t> &idx) {
+    ptr.assign(nrows + 1, 0);
+    for (int32_t k : key) ++ptr[k + 1];
+    for (int r = 0; r < nrows; ++r) ptr[r + 1] += ptr[r];
+    idx.resize(key.size());
+    std::vector<int32_t> cursor(ptr.begin(), ptr.end() - 1);
+    for (size_t i = 0; i < key.size(); ++i) idx[cursor[key[i]]++] = val[i];
+    for (int r = 0; r < nrows; ++r) std::sort(idx.begin() + ptr[r], idx.begin() + ptr[r + 1]);
+}
+
+// Generalised radius of a node: the smaller of the parent's and the mean radius of the
+// siblings, so that siblings share one low/high-frequency class
+// (nearinteractions.jl:142-153).
+double genradius(const Tree &T, int node) {
+    const int p = T.parent[node];
+    if (p < 0) return T.radius[node];
+    double sum = 0.0;
+    for (int c = 0; c < T.nchildren[p]; ++c) sum += T.radius[T.firstchild[p] + c];
+    return std::min(genradius(T, p), sum / T.nchildren[p]);
+}
+
+// Candidate directions of a cluster of diameter diam: n = max(6, ceil(6 * 4^log2(
+// acos(1/sqrt 3) / asin(min(1, gamma / (k diam)))))) spherical Fibonacci points
+// (boundingballdirections.jl:12-29).
+void candidate_directions(double diam, double k, double gamma, std::vector<double> &out) {
+    const double kd = std::max(k * diam, 0x1p-52);
+    const double ratio = std::acos(1.0 / std::sqrt(3.0)) / std::asin(std::min(1.0, gamma / kd));
+    int64_t n = int64_t(std::ceil(6.0 * std::pow(4.0, std::log(ratio) / std::log(2.0))));
+    n = std::max<int64_t>(6, n);
+    out.resize(3 * size_t(n));
+    const double ga = M_PI * (3.0 - std::sqrt(5.0));
+    for (int64_t i = 0; i < n; ++i) {
+        const double z = 1.0 - 2.0 * (double(i) + 0.5) / double(n);
+        const double r = std::sqrt(std::max(0.0, 1.0 - z * z));
+        out[3 * i] = r * std::cos(double(i) * ga);
+        out[3 * i + 1] = r * std::sin(double(i) * ga);
+        out[3 * i + 2] = z;
+    }
+}
+
+// 0-based index of the direction with the largest dot product (first on ties).
+int nearest_direction(const std::vector<double> &dirs, const double *v) {
+    const size_t n = dirs.size() / 3;
+    int best = 0;
+    double bd = dirs[0] * v[0] + dirs[1] * v[1] + dirs[2] * v[2];
+    for (size_t i = 1; i < n; ++i) {
+        const double d = dirs[3 * i] * v[0] + dirs[3 * i + 1] * v[1] + dirs[3 * i + 2] * v[2];
+        if (d > bd) {
+            bd = d;
+            best = int(i);
+        }
+    }
+    return best;
+}
+
+}  // namespace
+
+Partition build_partition_wideband(const Tree &test, const Tree &trial, const Wideband &w) {
+    Pairs sink;
+    if (test.nnodes > 0 && trial.nnodes > 0) traverse_wideband(test, trial, 0, 0, w, sink);
+    Partition P;
+    csr(sink.nt, sink.ns, test.nnodes, P.nearptr, P.nearnodes);
+    csr(sink.ft, sink.fs, test.nnodes, P.farptr, P.farnodes);
+    csr(sink.ns, sink.nt, trial.nnodes, P.tnearptr, P.tnearnodes);
+    csr(sink.fs, sink.ft, trial.nnodes, P.tfarptr, P.tfarnodes);
+    return P;
+}
+
+bool is_lowfrequency(const Tree &T, int node, const Wideband &w) { return w.k * (2.0 * genradius(T, node)) <= w.gamma; }
+
+DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t> &farptr,
+                         const std::vector<int32_t> &farnodes_in, const Wideband &w) {
+    const int nn = T.nnodes;
+    DirSide D;
+    D.farptr = farptr;
+    D.farnodes = farnodes_in;
+    std::vector<std::vector<int32_t>> dirs(nn), dircount(nn), pmap(nn);
+    std::vector<std::vector<double>> dirvec(nn);
+    std::vector<char> hasvec(nn, 0);
+    std::vector<int32_t> pcount(nn, 0);
+    std::vector<char> lf(nn);
+    for (int node = 0; node < nn; ++node) lf[node] = is_lowfrequency(T, node, w);
+    std::vector<double> total;
+    for (int level = 0; level < T.nlevels; ++level) {
+        for (int node = T.levelptr[level]; node < T.levelptr[level + 1]; ++node) {
+            const int p = T.parent[node];
+            const bool hasfars = farptr[node + 1] > farptr[node];
+            const bool hasparentvecs = p >= 0 && hasvec[p];
+            const bool hasparentdirs = p >= 0 && !dirs[p].empty();
+            if (lf[node]) {
+                const bool inherit = hasparentdirs && level > 0 && lf[p];
+                if (hasfars || inherit) dirs[node] = {0};
+                if (inherit) pmap[node] = {1};
+                continue;
+            }
+            if (!hasfars && !hasparentvecs) continue;
+            candidate_directions(2.0 * T.radius[node], w.k, w.gamma, total);
+            const int b = farptr[node], nfar = farptr[node + 1] - b;
+            std::vector<int32_t> nd(nfar);
+            const double *c = &T.center[3 * size_t(node)];
+            for (int i = 0; i < nfar; ++i) {
+                const double *cf = &F.center[3 * size_t(D.farnodes[b + i])];
+                const double v[3] = {c[0] - cf[0], c[1] - cf[1], c[2] - cf[2]};
+                nd[i] = nearest_direction(total, v) + 1;
+            }
+            // far nodes grouped by direction (stable)
+            std::vector<int32_t> order(nfar);
+            for (int i = 0; i < nfar; ++i) order[i] = i;
+            std::stable_sort(order.begin(), order.end(), [&](int a, int q) { return nd[a] < nd[q]; });
+            std::vector<int32_t> permuted(nfar), sorted(nfar);
+            for (int i = 0; i < nfar; ++i) {
+                permuted[i] = D.farnodes[b + order[i]];
+                sorted[i] = nd[order[i]];
+            }
+            std::copy(permuted.begin(), permuted.end(), D.farnodes.begin() + b);
+            std::vector<int32_t> uniq(sorted);
+            uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+            const size_t noriginal = uniq.size();
+            // the child's direction of every parent direction, seen from the child's centre
+            std::vector<int32_t> map;
+            if (p >= 0) {
+                map.assign(dirs[p].size(), 0);
+                const double *cp = &T.center[3 * size_t(p)];
+                const double rp2 = 2.0 * T.radius[p];
+                const double mult = w.k * rp2 / w.etahf + rp2;
+                for (size_t di = 0; di < dirs[p].size(); ++di) {
+                    const double *pv = &dirvec[p][3 * di];
+                    const double v[3] = {c[0] - cp[0] + mult * pv[0], c[1] - cp[1] + mult * pv[1],
+                                         c[2] - cp[2] + mult * pv[2]};
+                    map[di] = nearest_direction(total, v) + 1;
+                }
+                for (size_t di = 0; di < map.size(); ++di) {
+                    auto it = std::find(uniq.begin(), uniq.end(), map[di]);
+                    if (it != uniq.end()) {
+                        map[di] = int32_t(it - uniq.begin()) + 1;
+                    } else {
+                        uniq.push_back(map[di]);
+                        map[di] = int32_t(uniq.size());
+                    }
+                }
+            }
+            std::vector<int32_t> count(uniq.size(), 0);
+            for (size_t u = 0, i = 0; u < noriginal; ++u)
+                while (i < size_t(nfar) && sorted[i] == uniq[u]) {
+                    ++count[u];
+                    ++i;
+                }
+            dirvec[node].resize(3 * uniq.size());
+            for (size_t u = 0; u < uniq.size(); ++u)
+                for (int d = 0; d < 3; ++d) dirvec[node][3 * u + d] = total[3 * size_t(uniq[u] - 1) + d];
+            hasvec[node] = 1;
+            pcount[node] = int32_t(std::count_if(map.begin(), map.end(), [](int32_t x) { return x != 0; }));
+            pmap[node] = map;
+            dirs[node] = uniq;
+            dircount[node] = count;
+        }
+    }
+    for (int node = 0; node < nn; ++node)
+        if (!dirs[node].empty() && dircount[node].empty()) {
+            dircount[node] = {std::max(0, farptr[node + 1] - farptr[node])};
+            pcount[node] = int32_t(pmap[node].size());
+        }
+    // CSR: items (node, direction), far ranges per item, parent-to-child maps per node
+    D.dirptr.assign(nn + 1, 0);
+    D.chdirptr.assign(nn + 1, 0);
+    for (int node = 0; node < nn; ++node) {
+        D.dirptr[node + 1] = D.dirptr[node] + int32_t(dirs[node].size());
+        D.chdirptr[node + 1] = D.chdirptr[node] + pcount[node];
+    }
+    const int ni = D.dirptr[nn];
+    D.dirs.resize(ni);
+    D.dirvec.assign(3 * size_t(ni), 0.0);
+    D.dirfarptr.resize(ni + 1);
+    D.chdirmap.resize(D.chdirptr[nn]);
+    D.item_node.resize(ni);
+    for (int node = 0; node < nn; ++node) {
+        int32_t off = farptr[node];
+        for (size_t u = 0; u < dirs[node].size(); ++u) {
+            const int item = D.dirptr[node] + int(u);
+            D.dirs[item] = dirs[node][u];
+            D.item_node[item] = node;
+            if (hasvec[node])
+                for (int d = 0; d < 3; ++d) D.dirvec[3 * size_t(item) + d] = dirvec[node][3 * u + d];
+            D.dirfarptr[item] = off;
+            off += dircount[node][u];
+        }
+        std::copy(pmap[node].begin(), pmap[node].end(), D.chdirmap.begin() + D.chdirptr[node]);
+    }
+    D.dirfarptr[ni] = farptr[nn];
+    // basis items and the children's items of nested ones
+    D.item_basis.resize(ni);
+    D.item_chptr.assign(ni + 1, 0);
+    D.item_chidx.clear();
+    for (int item = 0; item < ni; ++item) {
+        const int node = D.item_node[item];
+        bool basis;
+        if (T.isleaf(node)) {
+            basis = true;
+        } else if (D.dirs[item] == 0) {
+            basis = false;
+        } else {
+            const int fc = T.firstchild[node];
+            basis = D.dirptr[fc + 1] == D.dirptr[fc] ||
+                    (D.dirptr[fc + 1] - D.dirptr[fc] == 1 && D.dirs[D.dirptr[fc]] == 0);
+        }
+        D.item_basis[item] = basis;
+        if (!basis) {
+            const int local = item - D.dirptr[node];  // 0-based local direction of the parent
+            for (int c = 0; c < T.nchildren[node]; ++c) {
+                const int ch = T.firstchild[node] + c;
+                const int cnt = D.chdirptr[ch + 1] - D.chdirptr[ch];
+                const int m = local < cnt ? D.chdirmap[D.chdirptr[ch] + local] : 0;  // 1-based local direction
+                if (m <= 0) throw std::runtime_error("directional plan: a child has no direction for its parent's");
+                D.item_chidx.push_back(D.dirptr[ch] + m - 1);
+            }
+        }
+        D.item_chptr[item + 1] = int32_t(D.item_chidx.size());
+    }
+    return D;
+}
+
+void item_farfield(const Tree &T, const DirSide &D, int item, std::vector<int32_t> &ff) {
+    ff.clear();
+    const int node = D.item_node[item];
+    auto append = [&](int it) {
+        ff.insert(ff.end(), D.farnodes.begin() + D.dirfarptr[it], D.farnodes.begin() + D.dirfarptr[it + 1]);
+    };
+    if (D.dirs[item] == 0) {
+        for (int cur = node; cur >= 0; cur = T.parent[cur]) {
+            int found = -1;
+            for (int it = D.dirptr[cur]; it < D.dirptr[cur + 1]; ++it)
+                if (D.dirs[it] == 0) {
+                    found = it;
+                    break;
+                }
+            if (found < 0) break;
+            append(found);
+        }
+        return;
+    }
+    append(item);
+    std::vector<int32_t> idcs{item - D.dirptr[node] + 1}, next;
+    for (int cur = node; T.parent[cur] >= 0; cur = T.parent[cur]) {
+        const int p = T.parent[cur];
+        next.clear();
+        for (int i = D.chdirptr[cur]; i < D.chdirptr[cur + 1]; ++i)
+            if (std::find(idcs.begin(), idcs.end(), D.chdirmap[i]) != idcs.end()) next.push_back(i - D.chdirptr[cur] + 1);
+        for (int32_t pi : next) append(D.dirptr[p] + pi - 1);
+        idcs.swap(next);
+    }
+}
+
+void all_item_farpivots(const Tree &own, const Tree &far, const DirSide &D, const double *ownpts,
+                        const double *farpts, int maxrank, std::vector<int32_t> &fpptr, std::vector<int32_t> &fpidx) {
+    const int ni = int(D.item_node.size());
+    std::vector<int32_t> count(ni, 0);
+    std::vector<int32_t> buf(size_t(ni) * std::max(maxrank, 1));
+    std::atomic<int> cursor{0};
+    auto work = [&]() {
+        std::vector<int32_t> ff;
+        for (;;) {
+            const int item = cursor.fetch_add(1);
+            if (item >= ni) break;
+            item_farfield(own, D, item, ff);
+            if (ff.empty()) continue;
+            const int t = D.item_node[item];
+            count[item] = select_farpivots(far, ownpts, farpts, own.perm.data() + own.begin[t], own.size(t), ff.data(),
+                                           int(ff.size()), maxrank, buf.data() + size_t(item) * maxrank);
+        }
+    };
+    const int nth = std::max(1, std::min(host_threads(), ni));
+    std::vector<std::thread> pool;
+    for (int i = 1; i < nth; ++i) pool.emplace_back(work);
+    work();
+    for (auto &th : pool) th.join();
+    fpptr.assign(ni + 1, 0);
+    for (int i = 0; i < ni; ++i) fpptr[i + 1] = fpptr[i] + count[i];
+    fpidx.resize(fpptr[ni]);
+    for (int i = 0; i < ni; ++i)
+        std::copy(buf.begin() + size_t(i) * maxrank, buf.begin() + size_t(i) * maxrank + count[i],
+                  fpidx.begin() + fpptr[i]);
+}
+
+}  // namespace nca

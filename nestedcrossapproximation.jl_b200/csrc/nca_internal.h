@@ -49,11 +49,41 @@ void all_farpivots(const Tree &own, const Tree &far, const double *ownpts, const
 // Worker count of the host planner.
 int host_threads();
 
+// ---- directional (wideband) planning, directional.cpp ----
+struct Wideband {
+    double k, etalf, etahf, gamma;
+};
+Partition build_partition_wideband(const Tree &test, const Tree &trial, const Wideband &w);
+bool is_lowfrequency(const Tree &T, int node, const Wideband &w);
+
+// Directional far data of one side and its basis items (one per (cluster, direction)).
+struct DirSide {
+    std::vector<int32_t> farptr, farnodes;  // far nodes of each node, grouped by direction
+    std::vector<int32_t> dirptr;            // node -> its first item (nnodes + 1)
+    std::vector<int32_t> dirs;              // item -> direction (0: low frequency; else 1-based candidate id)
+    std::vector<double> dirvec;             // item -> unit direction (zero for low frequency)
+    std::vector<int32_t> dirfarptr;         // item -> its own far nodes in farnodes (nitems + 1)
+    std::vector<int32_t> chdirptr, chdirmap;  // node -> for each parent direction its own (1-based)
+    std::vector<int32_t> item_node, item_basis;
+    std::vector<int32_t> item_chptr, item_chidx;  // nested items: the children's items in child order
+};
+DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t> &farptr,
+                         const std::vector<int32_t> &farnodes, const Wideband &w);
+void item_farfield(const Tree &T, const DirSide &D, int item, std::vector<int32_t> &ff);
+void all_item_farpivots(const Tree &own, const Tree &far, const DirSide &D, const double *ownpts,
+                        const double *farpts, int maxrank, std::vector<int32_t> &fpptr, std::vector<int32_t> &fpidx);
+
 }  // namespace nca
 
 struct nca_tree {
     nca::Tree t;
 };
+struct nca_dirplan {
+    const nca::Tree *tree;  // borrowed: the plan's own tree
+    nca::DirSide d;
+};
 struct nca_partition {
     nca::Partition p;
+    bool wideband = false;  // built with the wideband admissibility: the core becomes directional
+    nca::Wideband w{};
 };

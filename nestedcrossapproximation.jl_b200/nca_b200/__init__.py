@@ -8,7 +8,8 @@ libnca_b200.so (hand-written sm_100a kernels behind a C ABI, include/nca_b200.h)
 from . import seams
 from ._lib import (ArgumentError, ConcurrentWorkspaceError, CudaError, DimensionMismatch, SingularCrossMatrixError,
                    LIBPATH, lib)
-from .admissibility import FarData, fardata, farfield, farinteractions, farnodes, farptr, interactions, isnear
+from .admissibility import DirectionalData, FarData, IsNearWideband, directionalfardata, fardata, farfield, farinteractions, farnodes, farptr, interactions, isnear, \
+    isnearwideband
 from .compressors import ACA, BatchedBottomUp, FNormEstimator, FullPivoting, TreeMimicryPivoting, _clustersize, \
     _selectfarpivots
 from .kernels import HelmholtzKernel, LaplaceKernel, MatrixKernel

@@ -77,7 +77,13 @@ SIGNATURES = {
     "nca_tree_sizes": (I32, [P, P, P, P]),
     "nca_tree_export": (I32, [P] * 10),
     "nca_interactions": (I32, [P, P, D, P]),
+    "nca_interactions_wideband": (I32, [P, P, D, D, D, D, P]),
     "nca_partition_destroy": (None, [P]),
+    "nca_directional_plan": (I32, [P, P, P, I32, P]),
+    "nca_dirplan_destroy": (None, [P]),
+    "nca_dirplan_sizes": (I32, [P, P, P, P]),
+    "nca_dirplan_export": (I32, [P] * 9),
+    "nca_dirplan_farfield": (I32, [P, I32, P, I32, P]),
     "nca_partition_sizes": (I32, [P, P, P]),
     "nca_partition_export": (I32, [P] * 7),
     "nca_select_farpivots": (I32, [P, P, P, P, I32, P, I32, I32, P, P]),
