@@ -98,6 +98,7 @@ __device__ __forceinline__ int out_rows(const RowArgs<S> &a, int o) {
     if (STAGE == STAGE_UP) return a.rank[o];
     if (STAGE == STAGE_DOWN) return a.nrows[o];
     if (STAGE == STAGE_COUPLE) return a.rank_out[o];
+    if (STAGE == STAGE_GATHER) return a.g_rows[o];
     return a.end[o] - a.begin[o];
 }
 
@@ -109,6 +110,7 @@ __device__ __forceinline__ int own_segment(const RowArgs<S> &a, int o) {
 template <typename S, int STAGE>
 __device__ __forceinline__ int nsegs(const RowArgs<S> &a, int o) {
     if (STAGE == STAGE_UP || STAGE == STAGE_DOWN) return 1;
+    if (STAGE == STAGE_GATHER) return a.g_segptr[o + 1] - a.g_segptr[o];
     const int list = a.ptr ? a.ptr[o + 1] - a.ptr[o] : 0;
     return own_segment<S, STAGE>(a, o) + list;
 }
@@ -124,6 +126,12 @@ __device__ __forceinline__ Seg<S> segment(const RowArgs<S> &a, int o, int k) {
         g.M = a.M + a.moff[o];
         g.w = a.rank[o];
         g.v = a.coef + a.cptr[o] * a.vs;
+    } else if (STAGE == STAGE_GATHER) {
+        const int e = a.g_segptr[o] + k;
+        const int64_t mo = a.g_moff[e];
+        g.M = mo >= 0 ? a.M + mo : a.M2 + (-1 - mo);
+        g.w = a.g_w[e];
+        g.v = a.src + a.g_voff[e] * a.vs;
     } else if (STAGE == STAGE_COUPLE) {
         const int e = a.ptr[o] + k;
         const int other = a.other[e];
@@ -451,10 +459,11 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
         return;
     }
     if (tid == 0 && ctl.err) atomicCAS(a.error, 0, ctl.err);
+    const bool scatter = STAGE == STAGE_LEAVES || (STAGE == STAGE_GATHER && a.y != nullptr);
     for (int e = tid; e < R * bc; e += NT) {
         // coefficients: right-hand sides fastest (contiguous rows); y: rows fastest (the caller's columns)
-        const int i = STAGE == STAGE_LEAVES ? e % R : e / bc;
-        const int qq = STAGE == STAGE_LEAVES ? e / R : e % bc;
+        const int i = scatter ? e % R : e / bc;
+        const int qq = scatter ? e / R : e % bc;
         double2 v = red[i * bc + qq];
         for (int kg = 1; kg < tm.kgroups; ++kg) {
             const double2 p = red[(kg * R + i) * bc + qq];
@@ -462,9 +471,10 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
             v.y += p.y;
         }
         const int col = a.q0 + qq;
-        if (STAGE == STAGE_UP || STAGE == STAGE_COUPLE) {
-            double2 *d = STAGE == STAGE_UP ? (a.coef_out ? a.coef_out : a.coef) + (a.cptr[o] + i) * a.vs + col
-                                           : a.dst + (a.cptr_out[o] + i) * a.vs + col;
+        if (STAGE == STAGE_UP || STAGE == STAGE_COUPLE || (STAGE == STAGE_GATHER && !scatter)) {
+            double2 *d = STAGE == STAGE_UP       ? (a.coef_out ? a.coef_out : a.coef) + (a.cptr[o] + i) * a.vs + col
+                         : STAGE == STAGE_COUPLE ? a.dst + (a.cptr_out[o] + i) * a.vs + col
+                                                 : a.dst + (a.g_out[o] + i) * a.vs + col;
             if (a.accumulate) {
                 const double2 old = *d;
                 v = make_double2(old.x + v.x, old.y + v.y);
@@ -475,7 +485,8 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
             const double2 old = *d;
             *d = make_double2(old.x + v.x, old.y + v.y);
         } else {
-            double2 *yp = a.y + a.perm[a.begin[o] + i] + int64_t(col) * a.ldy;
+            const int64_t pos = STAGE == STAGE_GATHER ? a.g_out[o] + i : int64_t(a.begin[o]) + i;
+            double2 *yp = a.y + a.perm[pos] + int64_t(col) * a.ldy;
             double2 out = make_double2(a.alpha.x * v.x - a.alpha.y * v.y, a.alpha.x * v.y + a.alpha.y * v.x);
             if (a.usebeta) {
                 const double2 yo = *yp;
@@ -498,6 +509,7 @@ NCA_ROWS_KERNEL(k_rows_up, STAGE_UP)
 NCA_ROWS_KERNEL(k_rows_couple, STAGE_COUPLE)
 NCA_ROWS_KERNEL(k_rows_down, STAGE_DOWN)
 NCA_ROWS_KERNEL(k_rows_leaves, STAGE_LEAVES)
+NCA_ROWS_KERNEL(k_rows_gather, STAGE_GATHER)
 #undef NCA_ROWS_KERNEL
 
 size_t rows_smem_bytes() { return size_t(NSTAGE) * STAGE_BYTES; }
@@ -531,6 +543,10 @@ void launch_tiles(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStre
     case STAGE_DOWN:
         cudaFuncSetAttribute(k_rows_down<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
         k_rows_down<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
+        break;
+    case STAGE_GATHER:
+        cudaFuncSetAttribute(k_rows_gather<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        k_rows_gather<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
         break;
     default:
         cudaFuncSetAttribute(k_rows_leaves<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
@@ -566,6 +582,36 @@ void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStrea
 
 template void launch_rows<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
 template void launch_rows<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+
+namespace {
+template <typename S>
+__global__ void k_copy_blocks(const S *src, const int64_t *soff, const int32_t *sld, const int32_t *rows,
+                              const int32_t *cols, const int64_t *doff, int64_t nblocks, S *dst) {
+    for (int64_t blk = blockIdx.x; blk < nblocks; blk += gridDim.x) {
+        const int R = rows[blk], Cc = cols[blk], ld = sld[blk];
+        const S *in = src + soff[blk];
+        S *out = dst + doff[blk];
+        for (int e = threadIdx.x; e < R * Cc; e += blockDim.x) {
+            const int i = e % R, j = e / R;
+            out[e] = in[i + int64_t(j) * ld];
+        }
+    }
+}
+}  // namespace
+
+template <typename S>
+void launch_copy_blocks(const S *src, const int64_t *soff, const int32_t *sld, const int32_t *rows,
+                        const int32_t *cols, const int64_t *doff, int64_t nblocks, S *dst, cudaStream_t s) {
+    if (nblocks <= 0) return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = int(nblocks < int64_t(sms) * 16 ? nblocks : int64_t(sms) * 16);
+    k_copy_blocks<S><<<grid, 256, 0, s>>>(src, soff, sld, rows, cols, doff, nblocks, dst);
+}
+
+template void launch_copy_blocks<double2>(const double2 *, const int64_t *, const int32_t *, const int32_t *,
+                                          const int32_t *, const int64_t *, int64_t, double2 *, cudaStream_t);
 
 namespace {
 template <typename S>

@@ -7,7 +7,7 @@
 
 namespace nca {
 
-enum { STAGE_UP = 0, STAGE_COUPLE = 1, STAGE_DOWN = 2, STAGE_LEAVES = 3 };
+enum { STAGE_UP = 0, STAGE_COUPLE = 1, STAGE_DOWN = 2, STAGE_LEAVES = 3, STAGE_GATHER = 4 };
 
 // out_o = sum over segments op(M_seg) v_seg for every output node o of a launch.
 //   STAGE_UP:     o a node of the input side; one segment XT_o (rank x nrows) times the gathered
@@ -18,6 +18,11 @@ enum { STAGE_UP = 0, STAGE_COUPLE = 1, STAGE_DOWN = 2, STAGE_LEAVES = 3 };
 //                 to the children's yhat.
 //   STAGE_LEAVES: o a leaf of the output side; segments X_o yhat_o (if ranked) and the near
 //                 blocks M + moff[e] times the partner's input slice; scattered into y.
+//   STAGE_GATHER: generic block-sparse gather (directional products): output o has g_rows[o]
+//                 rows at row g_out[o] of dst (or, with y set, scattered through perm from
+//                 position g_out[o]); its segments e in [g_segptr[o], g_segptr[o+1]) are blocks
+//                 at g_moff[e] (>= 0: in M, < 0: at -1 - g_moff[e] in M2) with g_w[e] columns,
+//                 times the vector rows g_voff[e].. of src.
 template <typename S>
 struct RowArgs {
     int stage;
@@ -47,6 +52,9 @@ struct RowArgs {
     // UP and COUPLE add to the existing output with accumulate; UP skips leaves with skip_leaves
     double2 *coef_out;
     int accumulate, skip_leaves;
+    const int32_t *g_rows, *g_segptr, *g_w;
+    const int64_t *g_out, *g_moff, *g_voff;
+    const S *M2;
 };
 
 size_t rows_smem_bytes();
@@ -58,6 +66,12 @@ int vector_stride(int b);  // row stride of the internal vector buffers for b ri
 
 template <typename S>
 void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
+
+// dst[doff[e] + i + j * rows[e]] = src[soff[e] + i + j * sld[e]]: sub-matrix copies into
+// contiguous column-major blocks.
+template <typename S>
+void launch_copy_blocks(const S *src, const int64_t *soff, const int32_t *sld, const int32_t *rows,
+                        const int32_t *cols, const int64_t *doff, int64_t nblocks, S *dst, cudaStream_t s);
 
 // out block e = (in block e)^T for R_e x C_e column-major blocks.
 template <typename S>

@@ -20,6 +20,11 @@ struct LevelArgs {
     const int32_t *fpptr, *fpidx;  // phase-1 far pivots (CSR over nodes)
     int32_t *rank, *nrows, *piv;   // outputs: rank, block rows, pivots (maxrank per node)
     int32_t *cpiv;                 // optional output: column pivots (far-side point ids)
+    // item mode (directional bases): the launch's work items are (cluster, direction) pairs;
+    // every per-node array above is indexed by item, item_node gives the cluster, item_basis
+    // whether its rows are the cluster's points, item_chptr/item_chidx the children's items
+    // whose pivots form the rows otherwise. All null: one item per node (node mode).
+    const int32_t *item_node, *item_basis, *item_chptr, *item_chidx;
     double2 *X;                    // interpolation operators, node slot at xoff[node]
     const int64_t *xoff;
     int maxrank;

@@ -72,6 +72,13 @@ struct DBuf {
     }
 };
 
+template <typename T>
+std::vector<T> download_now(const DBuf<T> &b, size_t n) {
+    std::vector<T> h(n);
+    if (n) CK(cudaMemcpy(h.data(), b.p, sizeof(T) * n, cudaMemcpyDeviceToHost));
+    return h;
+}
+
 int fail(int code, const std::string &msg) {
     g_error = msg;
     return code;
@@ -442,6 +449,59 @@ void fill_bases(nca_core *c, int sd, int mode, const KernelParams &K, const Kern
     CK(cudaGetLastError());
 }
 
+// Near-field stores: one block per near pair (test CSR order) and its transpose (trial CSR
+// order), with the pair lists and transposition plans kept for refills. Returns the entries.
+int64_t build_near(nca_core *c, cudaStream_t s) {
+    const nca::Partition &P = c->part;
+    const nca::Tree &Tt = c->tree[0], &Ts = c->tree[1];
+    const int64_t nnear = P.nearnodes.size();
+    c->h_noff.assign(Tt.nnodes + 1, 0);
+    c->h_ncols.assign(Tt.nnodes, 0);
+    c->h_nfoff.assign(nnear + 1, 0);
+    std::vector<int32_t> near_t(nnear);
+    int64_t near_entries = 0;
+    for (int t = 0; t < Tt.nnodes; ++t) {
+        int col = 0;
+        for (int i = P.nearptr[t]; i < P.nearptr[t + 1]; ++i) {
+            near_t[i] = t;
+            const int ms = Ts.size(P.nearnodes[i]);
+            col += ms;
+            const int64_t e = int64_t(Tt.size(t)) * ms;
+            near_entries += e;
+            c->h_nfoff[i + 1] = c->h_nfoff[i] + pad2(e);
+        }
+        c->h_ncols[t] = col;
+        c->h_noff[t + 1] = c->h_noff[t] + int64_t(Tt.size(t)) * col;
+    }
+    const int64_t ntn = P.tnearnodes.size();
+    std::vector<int32_t> ntr_rows(ntn), ntr_cols(ntn);
+    std::vector<int64_t> ntr_in(ntn), h_ntoff(ntn + 1, 0);
+    for (int sn = 0; sn < Ts.nnodes; ++sn)
+        for (int k = P.tnearptr[sn]; k < P.tnearptr[sn + 1]; ++k) {
+            const int t = P.tnearnodes[k];
+            auto it = std::lower_bound(P.nearnodes.begin() + P.nearptr[t], P.nearnodes.begin() + P.nearptr[t + 1], sn);
+            ntr_in[k] = c->h_nfoff[it - P.nearnodes.begin()];
+            ntr_rows[k] = Tt.size(t);
+            ntr_cols[k] = Ts.size(sn);
+            h_ntoff[k + 1] = h_ntoff[k] + pad2(int64_t(Tt.size(t)) * Ts.size(sn));
+        }
+    c->nearptr.upload(P.nearptr, s);
+    c->nearnodes.upload(P.nearnodes, s);
+    c->tnearptr.upload(P.tnearptr, s);
+    c->tnearnodes.upload(P.tnearnodes, s);
+    c->nfoff.upload(c->h_nfoff, s);
+    c->ntoff.upload(h_ntoff, s);
+    c->N.alloc(size_t(c->h_nfoff.back()));
+    c->NT.alloc(size_t(h_ntoff.back()));
+    c->near_t.upload(near_t, s);
+    c->ntr_in.upload(ntr_in, s);
+    c->ntr_rows.upload(ntr_rows, s);
+    c->ntr_cols.upload(ntr_cols, s);
+    c->n_ntr = ntn;
+    fill_near(c, c->K, c->N.p, c->NT.p, s);
+    return near_entries;
+}
+
 void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int64_t ns,
                 const nca_build_opts *o) {
     const int maxrank = c->maxrank;
@@ -493,7 +553,7 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         DBuf<int32_t> nodes;
         nodes.upload(lv_nodes, s);
         status.zero(s);
-        LevelArgs a;
+        LevelArgs a{};
         a.K = c->K;
         a.side = sd;
         a.own_pts = d.pts.p;
@@ -609,38 +669,6 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
     c->n_couple_rev = int(rev.size());
     c->couple_fwd.upload(fwd, s);
     c->couple_rev.upload(rev, s);
-    // near field: one block per near pair (test CSR order) and its transpose (trial CSR order)
-    const int64_t nnear = P.nearnodes.size();
-    c->h_noff.assign(Tt.nnodes + 1, 0);
-    c->h_ncols.assign(Tt.nnodes, 0);
-    c->h_nfoff.assign(nnear + 1, 0);
-    std::vector<int32_t> near_t(nnear);
-    int64_t near_entries = 0;
-    for (int t = 0; t < Tt.nnodes; ++t) {
-        int col = 0;
-        for (int i = P.nearptr[t]; i < P.nearptr[t + 1]; ++i) {
-            near_t[i] = t;
-            const int ms = Ts.size(P.nearnodes[i]);
-            col += ms;
-            const int64_t e = int64_t(Tt.size(t)) * ms;
-            near_entries += e;
-            c->h_nfoff[i + 1] = c->h_nfoff[i] + pad2(e);
-        }
-        c->h_ncols[t] = col;
-        c->h_noff[t + 1] = c->h_noff[t] + int64_t(Tt.size(t)) * col;
-    }
-    const int64_t ntn = P.tnearnodes.size();
-    std::vector<int32_t> ntr_rows(ntn), ntr_cols(ntn);
-    std::vector<int64_t> ntr_in(ntn), h_ntoff(ntn + 1, 0);
-    for (int sn = 0; sn < Ts.nnodes; ++sn)
-        for (int k = P.tnearptr[sn]; k < P.tnearptr[sn + 1]; ++k) {
-            const int t = P.tnearnodes[k];
-            auto it = std::lower_bound(P.nearnodes.begin() + P.nearptr[t], P.nearnodes.begin() + P.nearptr[t + 1], sn);
-            ntr_in[k] = c->h_nfoff[it - P.nearnodes.begin()];
-            ntr_rows[k] = Tt.size(t);
-            ntr_cols[k] = Ts.size(sn);
-            h_ntoff[k + 1] = h_ntoff[k] + pad2(int64_t(Tt.size(t)) * Ts.size(sn));
-        }
     // leaves of both sides, largest work (near columns + own basis) first
     for (int sd = 0; sd < 2; ++sd) {
         const nca::Tree &T = c->tree[sd];
@@ -659,20 +687,7 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         std::stable_sort(leaves.begin(), leaves.end(), [&](int a, int b) { return work[a] > work[b]; });
         c->side[sd].leaves.upload(leaves, s);
     }
-    c->nearptr.upload(P.nearptr, s);
-    c->nearnodes.upload(P.nearnodes, s);
-    c->tnearptr.upload(P.tnearptr, s);
-    c->tnearnodes.upload(P.tnearnodes, s);
-    c->nfoff.upload(c->h_nfoff, s);
-    c->ntoff.upload(h_ntoff, s);
-    c->N.alloc(size_t(c->h_nfoff.back()));
-    c->NT.alloc(size_t(h_ntoff.back()));
-    c->near_t.upload(near_t, s);
-    c->ntr_in.upload(ntr_in, s);
-    c->ntr_rows.upload(ntr_rows, s);
-    c->ntr_cols.upload(ntr_cols, s);
-    c->n_ntr = ntn;
-    fill_near(c, c->K, c->N.p, c->NT.p, s);
+    const int64_t near_entries = build_near(c, s);
     if (c->f32) make_f32_copies(c, s);
     CK(cudaEventRecord(ev1, s));
     CK(cudaStreamSynchronize(s));
@@ -699,7 +714,7 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         (sd == 0 ? I.transfer_entries_test : I.transfer_entries_trial) = transfer;
     }
     I.nfarpairs = npairs;
-    I.nnearpairs = nnear;
+    I.nnearpairs = int64_t(P.nearnodes.size());
     I.build_seconds = ms * 1e-3;
     I.build_seconds_host = std::chrono::duration<double>(h1 - h0).count() +
                            std::chrono::duration<double>(h2 - h1).count() - ms * 1e-3;
@@ -1131,12 +1146,6 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
 // back, so every product stage (one launch per level of the deepest member, one coupling and one
 // leaf launch) covers all members at once. x and y are the members' vectors stacked in order.
 
-template <typename T>
-std::vector<T> download_now(const DBuf<T> &b, size_t n) {
-    std::vector<T> h(n);
-    if (n) CK(cudaMemcpy(h.data(), b.p, sizeof(T) * n, cudaMemcpyDeviceToHost));
-    return h;
-}
 
 // dst = concatenation of counts[i] elements of parts[i]; with release, each part is freed once
 // its copy has completed (moving the members' stores keeps the peak near one copy)
