@@ -175,6 +175,11 @@ int32_t nca_core_get_info(const nca_core *core, nca_core_info *info);
  * batchedbottomup.jl:344,446): ranks[nnodes], ptr[nnodes+1], idx[ptr[nnodes]]. */
 int32_t nca_core_export_pivots(const nca_core *core, int32_t side, int32_t *ranks, int32_t *nrows,
                                int32_t *ptr, int32_t *idx);
+/* Directional cores: the basis items of one side (the plan's items, in its order) with their
+ * ranks, block rows and row pivots (tpivots/spivots of the directional compressor,
+ * src/compressors/bottomup.jl:214-424). Call with ranks = NULL for the item count. */
+int32_t nca_core_dir_items(const nca_core *core, int32_t side, int32_t *nitems, int32_t *ranks, int32_t *nrows,
+                           int32_t *ptr, int32_t *idx);
 /* Far pivots of phase 1 per node of one side: ptr[nnodes+1], idx. */
 int32_t nca_core_farpivots_total(const nca_core *core, int32_t side, int64_t *total);
 int32_t nca_core_export_farpivots(const nca_core *core, int32_t side, int32_t *ptr, int32_t *idx);

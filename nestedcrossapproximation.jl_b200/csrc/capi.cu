@@ -12,6 +12,7 @@
 #include <mutex>
 #include <new>
 #include <type_traits>
+#include <unordered_map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -137,6 +138,41 @@ struct DevSide {
     int nleaves = 0, leafcap = 0;
 };
 
+// ---- directional cores: basis items (one per (cluster, direction)) and gather plans ----
+struct DirItems {
+    nca::DirSide plan;
+    int nitems = 0;
+    std::vector<int32_t> h_fpptr, h_fpidx, h_rank, h_nrows, h_piv;
+    std::vector<int64_t> h_xoff, h_cptr;
+    DBuf<int32_t> item_node, item_basis, item_chptr, item_chidx, fpptr, fpidx, rank, nrows, piv, cpiv;
+    DBuf<int64_t> xoff;
+    DBuf<double2> X, XT;
+};
+
+// One product stage as block-sparse gathers over the vector arena: outputs (ordered by launch
+// group), their segments, and the stage's block store.
+struct GatherStage {
+    std::vector<int32_t> group_ptr;  // launch groups (levels) over the outputs
+    std::vector<int> group_maxrows;
+    DBuf<int32_t> outputs, rows, segptr, w;
+    DBuf<int64_t> out, moff, voff;
+    DBuf<double2> M;
+    DBuf<float2> M32;
+    int64_t entries = 0;  // algorithmic entries of the store
+};
+
+// Products of one orientation: mode N (test <- trial) or T (trial <- test; C conjugates it).
+// Arena rows: [0, nin) gathered x, [nin, nin + cin) input-side coefficients, then output-side.
+struct DirProduct {
+    int64_t nin = 0, nout = 0, cin = 0, cout = 0;
+    GatherStage up, couple, down, leaves;
+};
+
+struct DirCore {
+    DirItems side[2];
+    DirProduct prod[2];
+};
+
 struct nca_core {
     int device = 0;
     int maxrank = 50;
@@ -172,6 +208,7 @@ struct nca_core {
     DBuf<double2> dC, dCT, dN, dNT;  // dS/dk and dN/dk on the frozen skeleton
     bool has_dk = false;
     bool batch = false;  // block-diagonal batch of several cores (one wavenumber per member)
+    std::unique_ptr<DirCore> dir;  // directional (wideband) core: items and gather plans
     nca_core_info info{};
     bool moved = false;  // stores moved into a batch: the core may only be destroyed
 };
@@ -183,6 +220,7 @@ struct nca_workspace {
     int max_nrhs = 0;
     DBuf<double2> xt, xhat, yhat, xstage, ystage;
     DBuf<double2> dxhat, dyhat;  // tangent products (d/dk)
+    DBuf<double2> arena;         // directional products: [x; input coefficients; output coefficients]
     std::atomic<bool> busy{false};
     DBuf<int32_t> error;
     int32_t *error_host = nullptr;  // pinned
@@ -720,6 +758,480 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
                            std::chrono::duration<double>(h2 - h1).count() - ms * 1e-3;
 }
 
+// ---- directional (wideband) build ------------------------------------------------------
+// Bases are built per item (cluster, direction) with the level kernel in item mode: the rows of a
+// basis item are its cluster's points, those of a nested item the pivots of its children's items
+// in the mapped directions; the column pivots come from tree mimicry over the item's directional
+// far field. The product stages then become block-sparse gathers over one vector arena, each
+// block stored contiguously: up (item <- its children's items or its cluster's x slice), coupling
+// (item <- far items), down (child item <- its parents' items: several parent directions can map
+// onto one child direction, so the children gather), leaves (leaf <- every basis item whose
+// cluster contains it, and the near blocks).
+
+struct StageBuilder {
+    std::vector<int32_t> group_ptr{0};
+    std::vector<int> group_maxrows;
+    std::vector<int32_t> rows, segptr{0}, w;
+    std::vector<int64_t> out, moff, voff, work;
+    // sub-matrix copies from the source store into the stage store
+    std::vector<int64_t> soff, doff;
+    std::vector<int32_t> sld, crows, ccols;
+    int64_t store = 0;
+    int cur_max = 0;
+    void begin_output(int32_t R, int64_t o) {
+        rows.push_back(R);
+        out.push_back(o);
+        work.push_back(0);
+        cur_max = std::max(cur_max, R);
+    }
+    void segment(int64_t mo, int32_t width, int64_t vo) {
+        moff.push_back(mo);
+        w.push_back(width);
+        voff.push_back(vo);
+        work.back() += int64_t(rows.back()) * width;
+    }
+    // a block copied from the source store (R x C at offset so, leading dimension ld) into the
+    // stage store; returns its offset there
+    int64_t copy(int64_t so, int32_t ld, int32_t R, int32_t C) {
+        const int64_t d = store;
+        soff.push_back(so);
+        sld.push_back(ld);
+        crows.push_back(R);
+        ccols.push_back(C);
+        doff.push_back(d);
+        store += pad2(int64_t(R) * C);
+        return d;
+    }
+    void end_output() { segptr.push_back(int32_t(moff.size())); }
+    void end_group() {
+        group_ptr.push_back(int32_t(rows.size()));
+        group_maxrows.push_back(std::max(cur_max, 1));
+        cur_max = 0;
+    }
+    // uploads the plan; with a source, allocates the stage store and copies its blocks
+    void finish(GatherStage &G, const double2 *src, cudaStream_t s) {
+        // outputs of each group largest work first (shorter tail of the last wave)
+        std::vector<int32_t> order(rows.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = int32_t(i);
+        for (size_t g = 0; g + 1 < group_ptr.size(); ++g)
+            std::stable_sort(order.begin() + group_ptr[g], order.begin() + group_ptr[g + 1],
+                             [&](int a, int b) { return work[a] > work[b]; });
+        G.group_ptr = group_ptr;
+        G.group_maxrows = group_maxrows;
+        G.outputs.upload(order, s);
+        G.rows.upload(rows, s);
+        G.out.upload(out, s);
+        G.segptr.upload(segptr, s);
+        G.moff.upload(moff, s);
+        G.w.upload(w, s);
+        G.voff.upload(voff, s);
+        if (!src) return;
+        G.M.alloc(size_t(store));
+        G.entries = 0;
+        for (size_t i = 0; i < crows.size(); ++i) G.entries += int64_t(crows[i]) * ccols[i];
+        if (!crows.empty()) {
+            DBuf<int64_t> dso, ddo;
+            DBuf<int32_t> dld, dr, dc;
+            dso.upload(soff, s);
+            ddo.upload(doff, s);
+            dld.upload(sld, s);
+            dr.upload(crows, s);
+            dc.upload(ccols, s);
+            launch_copy_blocks<double2>(src, dso.p, dld.p, dr.p, dc.p, ddo.p, int64_t(crows.size()), G.M.p, s);
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(s));
+        }
+    }
+};
+
+void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_build_opts *o, const nca::Wideband &wb) {
+    const int maxrank = c->maxrank;
+    auto h0 = std::chrono::steady_clock::now();
+    cudaStream_t s;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } sg{s};
+    upload_tree(c->side[0], c->tree[0], tp, s);
+    upload_tree(c->side[1], c->tree[1], sp, s);
+    const nca::Partition &P = c->part;
+    auto D = std::make_unique<DirCore>();
+    const double *pts[2] = {tp, sp};
+    for (int sd = 0; sd < 2; ++sd) {
+        DirItems &d = D->side[sd];
+        d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
+                                  sd == 0 ? P.farnodes : P.tfarnodes, wb);
+        all_item_farpivots(c->tree[sd], c->tree[1 - sd], d.plan, pts[sd], pts[1 - sd], maxrank, d.h_fpptr, d.h_fpidx);
+    }
+    auto h1 = std::chrono::steady_clock::now();
+    cudaEvent_t ev0, ev1;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } eg{ev0, ev1};
+    DBuf<int32_t> status;
+    status.alloc(4);
+    CK(cudaEventRecord(ev0, s));
+    std::vector<std::vector<int32_t>> bylevel[2];
+    int64_t basis_entries[2] = {0, 0}, transfer_entries[2] = {0, 0};
+    for (int sd = 0; sd < 2; ++sd) {
+        DirItems &d = D->side[sd];
+        const nca::DirSide &pl = d.plan;
+        const nca::Tree &T = c->tree[sd];
+        DevSide &ds = c->side[sd];
+        const int ni = int(pl.item_node.size());
+        d.nitems = ni;
+        bylevel[sd].assign(T.nlevels, {});
+        for (int it = 0; it < ni; ++it) bylevel[sd][T.level[pl.item_node[it]]].push_back(it);
+        std::vector<int64_t> mb(ni, 0), rb(ni, 0);
+        std::vector<int32_t> lv_ptr{0}, lv_nodes;
+        std::vector<int> lv_mcap, lv_ncap;
+        for (int lev = T.nlevels - 1; lev >= 0; --lev) {
+            int mc = 0, nc = 0;
+            for (int it : bylevel[sd][lev]) {
+                const int nfp = d.h_fpptr[it + 1] - d.h_fpptr[it];
+                if (nfp == 0) continue;
+                int64_t m = 0;
+                if (pl.item_basis[it]) {
+                    m = T.size(pl.item_node[it]);
+                } else {
+                    for (int k = pl.item_chptr[it]; k < pl.item_chptr[it + 1]; ++k) m += rb[pl.item_chidx[k]];
+                }
+                mb[it] = m;
+                rb[it] = std::min<int64_t>({int64_t(maxrank), m, int64_t(nfp)});
+                lv_nodes.push_back(it);
+                mc = std::max<int>(mc, int(m));
+                nc = std::max(nc, nfp);
+            }
+            lv_ptr.push_back(int32_t(lv_nodes.size()));
+            lv_mcap.push_back(mc);
+            lv_ncap.push_back(nc);
+        }
+        d.h_xoff.assign(ni + 1, 0);
+        for (int it = 0; it < ni; ++it) d.h_xoff[it + 1] = d.h_xoff[it] + pad2(mb[it] * rb[it]);
+        d.item_node.upload(pl.item_node, s);
+        d.item_basis.upload(pl.item_basis, s);
+        d.item_chptr.upload(pl.item_chptr, s);
+        d.item_chidx.upload(pl.item_chidx, s);
+        d.fpptr.upload(d.h_fpptr, s);
+        d.fpidx.upload(d.h_fpidx, s);
+        d.xoff.upload(d.h_xoff, s);
+        d.X.alloc(size_t(d.h_xoff.back()));
+        d.rank.alloc(std::max(ni, 1));
+        d.rank.zero(s);
+        d.nrows.alloc(std::max(ni, 1));
+        d.nrows.zero(s);
+        d.piv.alloc(size_t(std::max(ni, 1)) * maxrank);
+        d.cpiv.alloc(size_t(std::max(ni, 1)) * maxrank);
+        DBuf<int32_t> nodes;
+        nodes.upload(lv_nodes, s);
+        status.zero(s);
+        LevelArgs a{};
+        a.K = c->K;
+        a.side = sd;
+        a.own_pts = ds.pts.p;
+        a.far_pts = c->side[1 - sd].pts.p;
+        a.perm = ds.perm.p;
+        a.begin = ds.begin.p;
+        a.end = ds.end.p;
+        a.firstchild = ds.firstchild.p;
+        a.nchildren = ds.nchildren.p;
+        a.fpptr = d.fpptr.p;
+        a.fpidx = d.fpidx.p;
+        a.rank = d.rank.p;
+        a.nrows = d.nrows.p;
+        a.piv = d.piv.p;
+        a.cpiv = d.cpiv.p;
+        a.X = d.X.p;
+        a.xoff = d.xoff.p;
+        a.maxrank = maxrank;
+        a.tol = sd == 0 ? o->tol_test : o->tol_trial;
+        a.sampled = o->sampled;
+        a.status = status.p;
+        a.item_node = d.item_node.p;
+        a.item_basis = d.item_basis.p;
+        a.item_chptr = d.item_chptr.p;
+        a.item_chidx = d.item_chidx.p;
+        size_t maxsm = 0;
+        for (size_t l = 0; l + 1 < lv_ptr.size(); ++l)
+            maxsm = std::max(maxsm, level_smem_bytes(lv_mcap[l], lv_ncap[l]));
+        if (maxsm > size_t(kMaxSmem))
+            throw Failure(NCA_ERR_ARG, "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
+        CK(cudaFuncSetAttribute(k_level_compress, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(std::max<size_t>(maxsm, 16))));
+        for (size_t l = 0; l + 1 < lv_ptr.size(); ++l) {
+            const int cnt = lv_ptr[l + 1] - lv_ptr[l];
+            if (cnt == 0) continue;
+            k_level_compress<<<cnt, 256, level_smem_bytes(lv_mcap[l], lv_ncap[l]), s>>>(a, nodes.p + lv_ptr[l],
+                                                                                         lv_mcap[l], lv_ncap[l]);
+            CK(cudaGetLastError());
+        }
+        const std::vector<int32_t> st = status.download(s);
+        if (st[0] == 1) {
+            set_singular(sd, st[1], st[2], st[3]);
+            throw Failure(NCA_ERR_SINGULAR, "SingularCrossMatrixError: the cross matrix of " +
+                                                std::string(sd == 0 ? "test" : "trial") + " item " +
+                                                std::to_string(st[1]) + " is singular - " + std::to_string(st[2]) +
+                                                " pivots were selected but only " + std::to_string(st[3]) +
+                                                " of them are linearly independent");
+        }
+        if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: level block exceeds its planned capacity");
+        d.h_rank = d.rank.download(s);
+        d.h_nrows = d.nrows.download(s);
+        d.h_piv = d.piv.download(s);
+        d.h_rank.resize(ni);
+        d.h_nrows.resize(ni);
+        d.h_cptr.assign(ni + 1, 0);
+        for (int it = 0; it < ni; ++it) {
+            d.h_cptr[it + 1] = d.h_cptr[it] + d.h_rank[it];
+            const int64_t e = int64_t(d.h_rank[it]) * d.h_nrows[it];
+            (pl.item_basis[it] ? basis_entries[sd] : transfer_entries[sd]) += e;
+        }
+        d.XT.alloc(d.X.n);
+        launch_transpose_blocks<double2>(d.X.p, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, ni, d.XT.p, s);
+        CK(cudaGetLastError());
+    }
+    // far pairs (test CSR grouped by test direction) and their items on both sides
+    const nca::DirSide &pt = D->side[0].plan, &ps = D->side[1].plan;
+    const int64_t npairs = int64_t(pt.farnodes.size());
+    std::vector<int32_t> item_of_pos[2];
+    for (int sd = 0; sd < 2; ++sd) {
+        const nca::DirSide &pl = D->side[sd].plan;
+        item_of_pos[sd].assign(pl.farnodes.size(), -1);
+        for (size_t it = 0; it < pl.item_node.size(); ++it)
+            for (int q = pl.dirfarptr[it]; q < pl.dirfarptr[it + 1]; ++q) item_of_pos[sd][q] = int32_t(it);
+    }
+    const int64_t ntn_nodes = c->tree[0].nnodes;
+    std::unordered_map<int64_t, int32_t> trialpos;  // (trial node, test node) -> position in the trial far lists
+    trialpos.reserve(size_t(npairs) * 2 + 1);
+    for (int sn = 0; sn < c->tree[1].nnodes; ++sn)
+        for (int q = ps.farptr[sn]; q < ps.farptr[sn + 1]; ++q) trialpos[int64_t(sn) * ntn_nodes + ps.farnodes[q]] = q;
+    std::vector<int32_t> pair_it(npairs), pair_is(npairs);
+    std::vector<int32_t> pair_of_pos(ps.farnodes.size(), -1);
+    for (int t = 0; t < c->tree[0].nnodes; ++t)
+        for (int e = pt.farptr[t]; e < pt.farptr[t + 1]; ++e) {
+            const int sn = pt.farnodes[e];
+            const int32_t q = trialpos.at(int64_t(sn) * ntn_nodes + t);
+            pair_it[e] = item_of_pos[0][e];
+            pair_is[e] = item_of_pos[1][q];
+            pair_of_pos[q] = e;
+        }
+    const std::vector<int32_t> &rt = D->side[0].h_rank, &rs = D->side[1].h_rank;
+    // coupling blocks S_e = K[tau_(t, dt), tau_(s, ds)] in test pair order, transposes in trial order
+    std::vector<int64_t> cfoff(npairs + 1, 0), ctoff(ps.farnodes.size() + 1, 0);
+    int64_t coupling_entries = 0;
+    for (int64_t e = 0; e < npairs; ++e) {
+        const int64_t n = int64_t(rt[pair_it[e]]) * rs[pair_is[e]];
+        coupling_entries += n;
+        cfoff[e + 1] = cfoff[e] + pad2(n);
+    }
+    std::vector<int64_t> tr_in(ps.farnodes.size());
+    std::vector<int32_t> tr_rows(ps.farnodes.size()), tr_cols(ps.farnodes.size());
+    for (size_t q = 0; q < ps.farnodes.size(); ++q) {
+        const int e = pair_of_pos[q];
+        tr_in[q] = cfoff[e];
+        tr_rows[q] = rt[pair_it[e]];
+        tr_cols[q] = rs[pair_is[e]];
+        ctoff[q + 1] = ctoff[q] + pad2(int64_t(tr_rows[q]) * tr_cols[q]);
+    }
+    GatherStage &CN = D->prod[0].couple, &CTs = D->prod[1].couple;
+    CN.M.alloc(size_t(cfoff.back()));
+    CTs.M.alloc(size_t(ctoff.back()));
+    CN.entries = CTs.entries = coupling_entries;
+    {
+        DBuf<int32_t> dpt, dps, drows, dcols;
+        DBuf<int64_t> dcoff, din, dctoff;
+        dpt.upload(pair_it, s);
+        dps.upload(pair_is, s);
+        dcoff.upload(cfoff, s);
+        CouplingArgs a;
+        a.K = c->K;
+        a.test_pts = c->side[0].pts.p;
+        a.trial_pts = c->side[1].pts.p;
+        a.pair_t = dpt.p;
+        a.pair_s = dps.p;
+        a.rank_t = D->side[0].rank.p;
+        a.rank_s = D->side[1].rank.p;
+        a.piv_t = D->side[0].piv.p;
+        a.piv_s = D->side[1].piv.p;
+        a.maxrank = maxrank;
+        a.coff = dcoff.p;
+        a.npairs = npairs;
+        a.C = CN.M.p;
+        a.C32 = nullptr;
+        if (npairs > 0) {
+            k_couplings<<<launch_grid(npairs, 16), 256, 0, s>>>(a);
+            CK(cudaGetLastError());
+        }
+        din.upload(tr_in, s);
+        drows.upload(tr_rows, s);
+        dcols.upload(tr_cols, s);
+        dctoff.upload(ctoff, s);
+        launch_transpose_blocks<double2>(CN.M.p, din.p, drows.p, dcols.p, dctoff.p, int64_t(ps.farnodes.size()), CTs.M.p,
+                                         s);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s));
+    }
+    const int64_t near_entries = build_near(c, s);
+    const std::vector<int64_t> h_ntoff = download_now(c->ntoff, P.tnearnodes.size() + 1);
+    // gather plans of both orientations
+    for (int m = 0; m < 2; ++m) {
+        const int I = m == 0 ? 1 : 0, O = 1 - I;
+        DirItems &di = D->side[I], &dout = D->side[O];
+        const nca::Tree &TI = c->tree[I], &TO = c->tree[O];
+        DirProduct &pr = D->prod[m];
+        pr.nin = TI.npoints;
+        pr.nout = TO.npoints;
+        pr.cin = di.h_cptr.back();
+        pr.cout = dout.h_cptr.back();
+        const int64_t xin = pr.nin, yo = pr.nin + pr.cin;
+        // up: input-side items, deepest level first
+        {
+            StageBuilder B;
+            for (int lev = TI.nlevels - 1; lev >= 0; --lev) {
+                for (int it : bylevel[I][lev]) {
+                    const int r = di.h_rank[it];
+                    if (r <= 0) continue;
+                    B.begin_output(r, xin + di.h_cptr[it]);
+                    if (di.plan.item_basis[it]) {
+                        const int node = di.plan.item_node[it];
+                        const int nr = di.h_nrows[it];
+                        B.segment(B.copy(di.h_xoff[it], r, r, nr), nr, TI.begin[node]);
+                    } else {
+                        int64_t c0 = 0;
+                        for (int k = di.plan.item_chptr[it]; k < di.plan.item_chptr[it + 1]; ++k) {
+                            const int ch = di.plan.item_chidx[k];
+                            const int rc = di.h_rank[ch];
+                            if (rc > 0) B.segment(B.copy(di.h_xoff[it] + c0 * r, r, r, rc), rc, xin + di.h_cptr[ch]);
+                            c0 += rc;
+                        }
+                    }
+                    B.end_output();
+                }
+                B.end_group();
+            }
+            B.finish(pr.up, di.XT.p, s);
+        }
+        // coupling: output-side items with a rank and their far pairs' blocks (store built above)
+        {
+            StageBuilder B;
+            const nca::DirSide &pl = dout.plan;
+            const std::vector<int64_t> &off = m == 0 ? cfoff : ctoff;
+            for (int it = 0; it < dout.nitems; ++it) {
+                const int r = dout.h_rank[it];
+                if (r <= 0) continue;
+                B.begin_output(r, yo + dout.h_cptr[it]);
+                for (int q = pl.dirfarptr[it]; q < pl.dirfarptr[it + 1]; ++q) {
+                    const int e = m == 0 ? q : pair_of_pos[q];
+                    const int other = m == 0 ? pair_is[e] : pair_it[e];
+                    const int ro = di.h_rank[other];
+                    if (ro > 0) B.segment(off[q], ro, xin + di.h_cptr[other]);
+                }
+                B.end_output();
+            }
+            B.end_group();
+            B.finish(pr.couple, nullptr, s);
+        }
+        // down: output-side items gather from the parent items that map onto them, root level first
+        {
+            std::vector<std::vector<std::pair<int32_t, int64_t>>> parents(dout.nitems);
+            for (int it = 0; it < dout.nitems; ++it) {
+                if (dout.h_rank[it] <= 0 || dout.plan.item_basis[it]) continue;
+                int64_t c0 = 0;
+                for (int k = dout.plan.item_chptr[it]; k < dout.plan.item_chptr[it + 1]; ++k) {
+                    const int ch = dout.plan.item_chidx[k];
+                    if (dout.h_rank[ch] > 0) parents[ch].push_back({it, c0});
+                    c0 += dout.h_rank[ch];
+                }
+            }
+            StageBuilder B;
+            for (int lev = 1; lev < TO.nlevels; ++lev) {
+                for (int it : bylevel[O][lev]) {
+                    const int r = dout.h_rank[it];
+                    if (r <= 0 || parents[it].empty()) continue;
+                    B.begin_output(r, yo + dout.h_cptr[it]);
+                    for (const auto &pc : parents[it]) {
+                        const int p = pc.first;
+                        const int rp = dout.h_rank[p];
+                        B.segment(B.copy(dout.h_xoff[p] + pc.second, dout.h_nrows[p], r, rp), rp, yo + dout.h_cptr[p]);
+                    }
+                    B.end_output();
+                }
+                B.end_group();
+            }
+            B.finish(pr.down, dout.X.p, s);
+        }
+        // leaves: every basis item whose cluster contains the leaf, then the near blocks
+        {
+            StageBuilder B;
+            const nca::DirSide &pl = dout.plan;
+            const std::vector<int32_t> &nptr = m == 0 ? P.nearptr : P.tnearptr;
+            const std::vector<int32_t> &nnodes = m == 0 ? P.nearnodes : P.tnearnodes;
+            for (int leaf = 0; leaf < TO.nnodes; ++leaf) {
+                if (!TO.isleaf(leaf)) continue;
+                const int R = TO.size(leaf);
+                B.begin_output(R, TO.begin[leaf]);
+                for (int a = leaf; a >= 0; a = TO.parent[a])
+                    for (int it = pl.dirptr[a]; it < pl.dirptr[a + 1]; ++it) {
+                        const int r = dout.h_rank[it];
+                        if (r <= 0 || !pl.item_basis[it]) continue;
+                        B.segment(B.copy(dout.h_xoff[it] + (TO.begin[leaf] - TO.begin[a]), dout.h_nrows[it], R, r), r,
+                                  yo + dout.h_cptr[it]);
+                    }
+                for (int i = nptr[leaf]; i < nptr[leaf + 1]; ++i) {
+                    const int other = nnodes[i];
+                    const int64_t noff = m == 0 ? c->h_nfoff[i] : h_ntoff[i];
+                    B.segment(-1 - noff, TI.size(other), TI.begin[other]);
+                }
+                B.end_output();
+            }
+            B.end_group();
+            B.finish(pr.leaves, dout.X.p, s);
+        }
+    }
+    if (c->f32) {
+        auto down = [&](DBuf<double2> &src, DBuf<float2> &dst) {
+            dst.alloc(src.n);
+            if (src.n) k_to_f32<<<launch_grid(int64_t(src.n) / 256 + 1, 8), 256, 0, s>>>(src.p, dst.p, int64_t(src.n));
+            CK(cudaGetLastError());
+        };
+        for (DirProduct &pr : D->prod)
+            for (GatherStage *G : {&pr.up, &pr.couple, &pr.down, &pr.leaves}) down(G->M, G->M32);
+        down(c->N, c->N32);
+        down(c->NT, c->NT32);
+    }
+    CK(cudaEventRecord(ev1, s));
+    CK(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    auto h2 = std::chrono::steady_clock::now();
+    nca_core_info &I = c->info;
+    I.ntest = c->tree[0].npoints;
+    I.ntrial = c->tree[1].npoints;
+    I.nnodes_test = c->tree[0].nnodes;
+    I.nnodes_trial = c->tree[1].nnodes;
+    I.ncoeff_test = D->side[0].h_cptr.back();
+    I.ncoeff_trial = D->side[1].h_cptr.back();
+    I.near_entries = near_entries;
+    I.coupling_entries = coupling_entries;
+    I.basis_entries_test = basis_entries[0];
+    I.basis_entries_trial = basis_entries[1];
+    I.transfer_entries_test = transfer_entries[0];
+    I.transfer_entries_trial = transfer_entries[1];
+    I.nfarpairs = npairs;
+    I.nnearpairs = int64_t(P.nearnodes.size());
+    I.build_seconds = ms * 1e-3;
+    I.build_seconds_host = std::chrono::duration<double>(h1 - h0).count() +
+                           std::chrono::duration<double>(h2 - h1).count() - ms * 1e-3;
+    c->dir = std::move(D);
+}
+
 // Device buffers one product runs on: the gathered input (nin x vs), the input side's
 // coefficients xhat and the output side's yhat (coefficient rows x vs), and the error word the
 // kernels raise (must be zero when the product starts).
@@ -1050,6 +1562,78 @@ int enqueue_tangent(nca_core *c, const double2 *xd, int64_t lx, double2 *yd, int
     return NCA_OK;
 }
 
+// Enqueues y = alpha op(H) x + beta y for a directional core: gather x into the arena, then the
+// up, coupling, down and leaf gathers (mode C = mode T with every block conjugated).
+int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd, int64_t lx, double2 *yd,
+                        int64_t ly, int b, double2 alpha, double2 beta, double2 *arena, int32_t *error,
+                        cudaStream_t s, ProductLaunches &count) {
+    DirProduct &pr = c->dir->prod[mode == 0 ? 0 : 1];
+    const int I = mode == 0 ? 1 : 0, O = 1 - I;
+    const int vs = vector_stride(b);
+    const int cap = rows_capacity(std::min(b, 16));
+    for (const GatherStage *G : {&pr.up, &pr.couple, &pr.down, &pr.leaves})
+        for (int r : G->group_maxrows)
+            if (r > cap) return fail(NCA_ERR_ARG, "a leaf or basis block has more rows than one product CTA holds");
+    k_gather<<<launch_grid(pr.nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, c->side[I].perm.p, pr.nin, b, vs, arena);
+    ++count.total;
+    const bool conj = mode == 2;
+    auto run = [&](auto tag) {
+        using S = decltype(tag);
+        constexpr bool f64 = std::is_same<S, double2>::value;
+        const S *nearM = f64 ? (const S *)(mode == 0 ? c->N.p : c->NT.p) : (const S *)(mode == 0 ? c->N32.p : c->NT32.p);
+        for (int q0 = 0; q0 < b; q0 += 16) {
+            const int bc = std::min(16, b - q0);
+            auto stage = [&](const GatherStage &G, bool accumulate, bool scatter) {
+                const S *M = f64 ? (const S *)G.M.p : (const S *)G.M32.p;
+                for (size_t g = 0; g + 1 < G.group_ptr.size(); ++g) {
+                    const int cnt = G.group_ptr[g + 1] - G.group_ptr[g];
+                    if (!cnt) continue;
+                    RowArgs<S> a{};
+                    a.stage = STAGE_GATHER;
+                    a.M = M;
+                    a.M2 = nearM;
+                    a.g_rows = G.rows.p;
+                    a.g_out = G.out.p;
+                    a.g_segptr = G.segptr.p;
+                    a.g_moff = G.moff.p;
+                    a.g_w = G.w.p;
+                    a.g_voff = G.voff.p;
+                    a.src = arena;
+                    a.dst = arena;
+                    a.accumulate = accumulate;
+                    if (scatter) {
+                        a.y = yd;
+                        a.ldy = ly;
+                        a.perm = c->side[O].perm.p;
+                        a.alpha = alpha;
+                        a.beta = beta;
+                        a.usebeta = beta.x != 0.0 || beta.y != 0.0;
+                    }
+                    a.b = b;
+                    a.bc = bc;
+                    a.q0 = q0;
+                    a.vs = vs;
+                    a.conj = conj;
+                    a.maxrows = G.group_maxrows[g];
+                    a.error = error;
+                    launch_rows<S>(a, G.outputs.p + G.group_ptr[g], cnt, s);
+                    ++count.total;
+                }
+            };
+            stage(pr.up, false, false);
+            stage(pr.couple, false, false);
+            stage(pr.down, true, false);
+            stage(pr.leaves, false, true);
+        }
+    };
+    if (precision == NCA_PREC_F64)
+        run(double2{});
+    else
+        run(float2{});
+    CK(cudaGetLastError());
+    return NCA_OK;
+}
+
 // Argument checks shared by the product entry points.
 int check_product_args(nca_core *c, int mode, int precision, int64_t ldx, int64_t ldy, int64_t nrhs) {
     if (mode < 0 || mode > 2) return fail(NCA_ERR_ARG, "mode must be 0 (N), 1 (T) or 2 (C)");
@@ -1069,6 +1653,7 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     if (int st = check_product_args(c, mode, precision, ldx, ldy, nrhs)) return st;
     if (tangent && (mode != 0 || precision != NCA_PREC_F64))
         return fail(NCA_ERR_ARG, "the d/dk product is forward mode and complex FP64");
+    if (tangent && c->dir) return fail(NCA_ERR_ARG, "d/dk products are not available for directional cores");
     if (tangent && !c->has_dk) return fail(NCA_ERR_ARG, "call nca_core_prepare_dk before the d/dk product");
     const int in = mode == 0 ? 1 : 0, out = 1 - in;
     const int64_t nin = c->side[in].npts, nout = c->side[out].npts;
@@ -1076,7 +1661,7 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     CK(cudaSetDevice(c->device));
     cudaStream_t s = ws->stream;
     const int b = int(nrhs);
-    if (b > ws->max_nrhs) {
+    if (b > ws->max_nrhs && !c->dir) {
         const int vsm = vector_slots(b);
         ws->xt.alloc(size_t(std::max(c->side[0].npts, c->side[1].npts)) * vsm);
         ws->xhat.alloc(size_t(std::max(c->side[0].h_cptr.back(), c->side[1].h_cptr.back())) * vsm);
@@ -1104,13 +1689,25 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
         lx = nin;
         ly = nout;
     }
+    if (c->dir) {
+        const DirProduct &pr = c->dir->prod[mode == 0 ? 0 : 1];
+        const size_t need = size_t(pr.nin + pr.cin + pr.cout) * vector_slots(b);
+        if (ws->arena.n < need) ws->arena.alloc(need);
+    }
     if (tangent && ws->dxhat.n < ws->xhat.n) {
         ws->dxhat.alloc(ws->xhat.n);
         ws->dyhat.alloc(ws->xhat.n);
     }
     const ProductBuffers buf{ws->xt.p, ws->xhat.p, ws->yhat.p, ws->error.p, ws->far, ws->near};
     ProductLaunches count;
-    if (tangent) {
+    if (c->dir) {
+        if (ws->profiling) CK(cudaEventRecord(ws->stage_ev[0], s));
+        if (int st = enqueue_dir_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, ws->arena.p, ws->error.p,
+                                         s, count))
+            return st;
+        if (ws->profiling)
+            for (int k = 1; k < 6; ++k) CK(cudaEventRecord(ws->stage_ev[k], s));
+    } else if (tangent) {
         if (int st = enqueue_tangent(c, xd, lx, yd, ly, b, alpha, beta, buf, ws->dxhat.p, ws->dyhat.p, s, count))
             return st;
     } else if (int st = enqueue_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, buf, s,
@@ -1511,6 +2108,7 @@ int static_scratch_base(int device, unsigned char **base) {
 int apply_static_impl(nca_core *c, int mode, int precision, const void *x, int64_t ldx, void *y, int64_t ldy,
                       int64_t nrhs, double2 alpha, double2 beta, cudaStream_t s) {
     if (c->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
+    if (c->dir) return fail(NCA_ERR_ARG, "nca_apply_static does not take directional cores; use nca_apply");
     if (int st = check_product_args(c, mode, precision, ldx, ldy, nrhs)) return st;
     if (nrhs == 0) return NCA_OK;
     if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15)
@@ -1760,7 +2358,10 @@ int32_t nca_core_build(const double *testpoints, int64_t ntest, const double *tr
         c->tree[1] = trialtree->t;
         c->part = part->p;
         set_kernel_params(c.get(), kernel, ntest, ntrial, nullptr);
-        build_core(c.get(), testpoints, ntest, trialpoints, ntrial, opts);
+        if (part->wideband)
+            build_dir_core(c.get(), testpoints, trialpoints, opts, part->w);
+        else
+            build_core(c.get(), testpoints, ntest, trialpoints, ntrial, opts);
         *out = c.release();
         return int(NCA_OK);
     });
@@ -1777,6 +2378,7 @@ int32_t nca_core_set_wavenumber(nca_core *core, double k) {
         if (!core) return fail(NCA_ERR_ARG, "null core");
         if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
         if (core->batch) return fail(NCA_ERR_ARG, "a batch has one wavenumber per member: refill the members");
+        if (core->dir) return fail(NCA_ERR_ARG, "frozen-skeleton refills are not available for directional cores");
         if (core->K.kind == NCA_KERNEL_MATRIX) return fail(NCA_ERR_ARG, "a matrix kernel has no wavenumber");
         if (!std::isfinite(k)) return fail(NCA_ERR_ARG, "the wavenumber must be finite");
         CK(cudaSetDevice(core->device));
@@ -1821,6 +2423,7 @@ int32_t nca_core_prepare_dk(nca_core *core) {
         if (!core) return fail(NCA_ERR_ARG, "null core");
         if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
         if (core->batch) return fail(NCA_ERR_ARG, "prepare the d/dk stores of the members, not of a batch");
+        if (core->dir) return fail(NCA_ERR_ARG, "d/dk stores are not available for directional cores");
         if (core->K.kind == NCA_KERNEL_MATRIX) return fail(NCA_ERR_ARG, "a matrix kernel has no wavenumber derivative");
         if (core->has_dk) return int(NCA_OK);
         CK(cudaSetDevice(core->device));
@@ -1860,6 +2463,7 @@ int32_t nca_core_batch(nca_core *const *cores, int32_t ncores, int32_t flags, nc
             const nca_core *c = cs[i];
             if (!c) return fail(NCA_ERR_ARG, "null core in the batch");
             if (c->moved) return fail(NCA_ERR_ARG, "a core of the batch was moved into another batch");
+            if (c->dir) return fail(NCA_ERR_ARG, "directional cores cannot be batched");
             for (size_t j = 0; j < i; ++j)
                 if (cs[j] == c) return fail(NCA_ERR_ARG, "a core appears twice in the batch");
             if (c->device != cs[0]->device) return fail(NCA_ERR_ARG, "the cores of a batch must share one device");
@@ -1886,6 +2490,7 @@ int32_t nca_core_get_info(const nca_core *core, nca_core_info *info) {
 int32_t nca_core_export_pivots(const nca_core *core, int32_t side, int32_t *ranks, int32_t *nrows,
                                int32_t *ptr, int32_t *idx) {
     if (!core || side < 0 || side > 1) return fail(NCA_ERR_ARG, "bad argument");
+    if (core->dir) return fail(NCA_ERR_ARG, "node exports are not available for directional cores");
     const DevSide &d = core->side[side];
     int nn = d.nnodes;
     std::copy(d.h_rank.begin(), d.h_rank.end(), ranks);
@@ -1899,14 +2504,34 @@ int32_t nca_core_export_pivots(const nca_core *core, int32_t side, int32_t *rank
     return NCA_OK;
 }
 
+int32_t nca_core_dir_items(const nca_core *core, int32_t side, int32_t *nitems, int32_t *ranks, int32_t *nrows,
+                           int32_t *ptr, int32_t *idx) {
+    if (!core || side < 0 || side > 1 || !nitems) return fail(NCA_ERR_ARG, "bad argument");
+    if (!core->dir) return fail(NCA_ERR_ARG, "not a directional core");
+    const DirItems &d = core->dir->side[side];
+    *nitems = d.nitems;
+    if (!ranks) return NCA_OK;
+    std::copy(d.h_rank.begin(), d.h_rank.end(), ranks);
+    std::copy(d.h_nrows.begin(), d.h_nrows.end(), nrows);
+    ptr[0] = 0;
+    for (int it = 0; it < d.nitems; ++it) {
+        ptr[it + 1] = ptr[it] + d.h_rank[it];
+        std::copy(d.h_piv.begin() + int64_t(it) * core->maxrank,
+                  d.h_piv.begin() + int64_t(it) * core->maxrank + d.h_rank[it], idx + ptr[it]);
+    }
+    return NCA_OK;
+}
+
 int32_t nca_core_farpivots_total(const nca_core *core, int32_t side, int64_t *total) {
     if (!core || side < 0 || side > 1) return fail(NCA_ERR_ARG, "bad argument");
+    if (core->dir) return fail(NCA_ERR_ARG, "node exports are not available for directional cores");
     *total = core->side[side].h_fpptr.back();
     return NCA_OK;
 }
 
 int32_t nca_core_export_farpivots(const nca_core *core, int32_t side, int32_t *ptr, int32_t *idx) {
     if (!core || side < 0 || side > 1) return fail(NCA_ERR_ARG, "bad argument");
+    if (core->dir) return fail(NCA_ERR_ARG, "node exports are not available for directional cores");
     const DevSide &d = core->side[side];
     std::copy(d.h_fpptr.begin(), d.h_fpptr.end(), ptr);
     std::copy(d.h_fpidx.begin(), d.h_fpidx.end(), idx);
@@ -1917,6 +2542,7 @@ int32_t nca_core_export_x(const nca_core *core, int32_t side, int64_t *off, doub
     return guarded([&] {
         if (!core || side < 0 || side > 1) return fail(NCA_ERR_ARG, "bad argument");
         if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
+        if (core->dir) return fail(NCA_ERR_ARG, "node exports are not available for directional cores");
         const DevSide &d = core->side[side];
         CK(cudaSetDevice(core->device));
         std::vector<double2> all(d.X.n);
@@ -1935,6 +2561,7 @@ int32_t nca_core_export_couplings(const nca_core *core, int64_t *off, double *C)
     return guarded([&] {
         if (!core) return fail(NCA_ERR_ARG, "null core");
         if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
+        if (core->dir) return fail(NCA_ERR_ARG, "node exports are not available for directional cores");
         CK(cudaSetDevice(core->device));
         std::vector<double2> all(core->C.n);
         if (core->C.n) CK(cudaMemcpy(all.data(), core->C.p, sizeof(double2) * core->C.n, cudaMemcpyDeviceToHost));
@@ -1983,9 +2610,11 @@ int32_t nca_workspace_create(nca_core *core, int32_t max_nrhs, nca_workspace **o
         CK(cudaEventCreate(&ws->e0));
         CK(cudaEventCreate(&ws->e1));
         int b = std::max(1, max_nrhs);
-        ws->xt.alloc(size_t(std::max(core->side[0].npts, core->side[1].npts)) * vector_slots(b));
-        ws->xhat.alloc(size_t(std::max(core->side[0].h_cptr.back(), core->side[1].h_cptr.back())) * vector_slots(b));
-        ws->yhat.alloc(ws->xhat.n);
+        if (!core->dir) {
+            ws->xt.alloc(size_t(std::max(core->side[0].npts, core->side[1].npts)) * vector_slots(b));
+            ws->xhat.alloc(size_t(std::max(core->side[0].h_cptr.back(), core->side[1].h_cptr.back())) * vector_slots(b));
+            ws->yhat.alloc(ws->xhat.n);
+        }
         ws->max_nrhs = b;
         ws->error.alloc(1);
         CK(cudaMallocHost(&ws->error_host, sizeof(int32_t)));

@@ -92,6 +92,7 @@ SIGNATURES = {
     "nca_core_batch": (I32, [P, I32, I32, P]),
     "nca_core_get_info": (I32, [P, P]),
     "nca_core_export_pivots": (I32, [P, I32, P, P, P, P]),
+    "nca_core_dir_items": (I32, [P, I32, P, P, P, P, P]),
     "nca_core_farpivots_total": (I32, [P, I32, P]),
     "nca_core_export_farpivots": (I32, [P, I32, P, P]),
     "nca_core_export_x": (I32, [P, I32, P, P]),

@@ -266,3 +266,160 @@ class DirectionalData:
                 ff.extend(self.dirfarnodes(par, pardirs[i - 1]))
             cur = par
         return np.array(ff, np.int32)
+
+
+class DirectionalH2:
+    """Oracle directional H^2 matrix: the bottom-up compressor per (cluster, direction) item
+    (src/compressors/bottomup.jl:214-424) with the project's pivoting rules (tree mimicry over
+    the item's directional far field, the sampled fully pivoted ACA on K[rows, far pivots],
+    X = K[rows, sigma] K[tau, sigma]^{-1}), couplings per directional far pair
+    (src/couplingmatrices.jl:55-111), the near field, and the directional product
+    (src/nca/{aggregate,couple,disaggregate}.jl, directional methods)."""
+
+    def __init__(self, testpts, trialpts, kernel, k, minvalues=32, tol=1e-4, maxrank=50, etalf=1.0, etahf=5.0,
+                 gamma=1.0):
+        from . import oracle as O
+        self.O = O
+        self.testpts = np.ascontiguousarray(testpts, dtype=np.float64)
+        self.trialpts = np.ascontiguousarray(trialpts, dtype=np.float64)
+        self.kernel = kernel
+        self.trees = [O.OwnedTree(self.testpts, minvalues), O.OwnedTree(self.trialpts, minvalues)]
+        T, S = self.trees
+        (self.nearptr, self.nearnodes, fptr, fnodes, tptr, tnodes) = interactions_wideband(T, S, k, etalf, etahf, gamma)
+        self.tnearptr, self.tnearnodes = self._transpose(self.nearptr, self.nearnodes, S.nnodes)
+        self.dirs = [DirectionalData(T, S, fptr, fnodes, k, etahf, gamma),
+                     DirectionalData(S, T, tptr, tnodes, k, etahf, gamma)]
+        self.maxrank, self.tol = maxrank, tol
+        self.piv = [None, None]
+        self.X = [None, None]
+        for side in (0, 1):
+            self._build_side(side)
+        self._couplings()
+
+    @staticmethod
+    def _transpose(ptr, nodes, n):
+        lists = [[] for _ in range(n)]
+        for t in range(len(ptr) - 1):
+            for s in nodes[ptr[t]:ptr[t + 1]]:
+                lists[s].append(t)
+        tp = np.zeros(n + 1, np.int32)
+        for i in range(n):
+            tp[i + 1] = tp[i] + len(lists[i])
+        return tp, np.array([v for lst in lists for v in lst], np.int32)
+
+    def _block(self, side, rows, cols):
+        """K[rows, cols]; side 0: rows are test points, side 1: rows are trial points."""
+        O = self.O
+        rows = np.asarray(rows, np.int64)
+        cols = np.asarray(cols, np.int64)
+        if side == 0:
+            ii, jj = np.repeat(rows, len(cols)), np.tile(cols, len(rows))
+        else:
+            ii, jj = np.tile(cols, len(rows)), np.repeat(rows, len(cols))
+        v = O.entries(self.kernel, self.testpts, self.trialpts, ii, jj)
+        return v.reshape(len(rows), len(cols))
+
+    def _build_side(self, side):
+        O = self.O
+        D = self.dirs[side]
+        T, F = self.trees[side], self.trees[1 - side]
+        own = self.testpts if side == 0 else self.trialpts
+        far = self.trialpts if side == 0 else self.testpts
+        piv = [np.zeros(0, np.int32)] * D.nitems
+        X = [None] * D.nitems
+        for level in range(T.nlevels - 1, -1, -1):
+            for item in range(D.nitems):
+                node = int(D.item_node[item])
+                if T.level[node] != level:
+                    continue
+                ff = D.farfield(item)
+                if len(ff) == 0:
+                    continue
+                if D.item_basis[item]:
+                    rows = T.values(node)
+                else:
+                    rows = np.concatenate([piv[ch] for ch in D.item_chidx[D.item_chptr[item]:D.item_chptr[item + 1]]]
+                                          + [np.zeros(0, np.int32)]).astype(np.int32)
+                fp = O.select_farpivots(F, own, far, T.values(node), ff, self.maxrank)
+                if len(fp) == 0 or len(rows) == 0:
+                    continue
+                A = self._block(side, rows, fp)
+                r, rp, cp = O.aca(A, self.maxrank, self.tol, True)
+                if r == 0:
+                    continue
+                piv[item] = rows[rp]
+                X[item] = O.cross_solve(A[:, cp], rp)
+        self.piv[side] = piv
+        self.X[side] = X
+
+    def _couplings(self):
+        Dt, Ds = self.dirs
+        pos = {}
+        for s in range(self.trees[1].nnodes):
+            for q in range(Ds.farptr[s], Ds.farptr[s + 1]):
+                pos[(s, int(Ds.farnodes[q]))] = q
+        item_of = [np.zeros(len(D.farnodes), np.int32) for D in self.dirs]
+        for D, io in zip(self.dirs, item_of):
+            for it in range(D.nitems):
+                io[D.dirfarptr[it]:D.dirfarptr[it + 1]] = it
+        self.C = {}
+        for t in range(self.trees[0].nnodes):
+            for e in range(Dt.farptr[t], Dt.farptr[t + 1]):
+                s = int(Dt.farnodes[e])
+                it, is_ = int(item_of[0][e]), int(item_of[1][pos[(s, t)]])
+                if len(self.piv[0][it]) and len(self.piv[1][is_]):
+                    self.C[(it, is_)] = self._block(0, self.piv[0][it], self.piv[1][is_])
+
+    def apply(self, x, mode=0):
+        """y = op(H) x for a vector or a block of columns; mode 0: H, 1: H^T, 2: H^H."""
+        x = np.asarray(x, dtype=np.complex128)
+        vec = x.ndim == 1
+        X = x.reshape(x.shape[0], -1)
+        I = 1 if mode == 0 else 0
+        O_ = 1 - I
+        conj = (lambda a: a.conj()) if mode == 2 else (lambda a: a)
+        DI, DO = self.dirs[I], self.dirs[O_]
+        TI, TO = self.trees[I], self.trees[O_]
+        XI, XO = self.X[I], self.X[O_]
+        xhat = [None] * DI.nitems
+        for level in range(TI.nlevels - 1, -1, -1):
+            for it in range(DI.nitems):
+                if XI[it] is None or TI.level[DI.item_node[it]] != level:
+                    continue
+                if DI.item_basis[it]:
+                    xhat[it] = conj(XI[it]).T @ X[TI.values(int(DI.item_node[it]))]
+                else:
+                    acc, r0 = np.zeros((XI[it].shape[1], X.shape[1]), complex), 0
+                    for ch in DI.item_chidx[DI.item_chptr[it]:DI.item_chptr[it + 1]]:
+                        rc = 0 if XI[ch] is None else XI[ch].shape[1]
+                        if rc:
+                            acc = acc + conj(XI[it][r0:r0 + rc]).T @ xhat[ch]
+                        r0 += rc
+                    xhat[it] = acc
+        yhat = [None if XO[it] is None else np.zeros((XO[it].shape[1], X.shape[1]), complex) for it in range(DO.nitems)]
+        for (it, is_), Cb in self.C.items():
+            if mode == 0:
+                yhat[it] += Cb @ xhat[is_]
+            else:
+                yhat[is_] += conj(Cb).T @ xhat[it]
+        Y = np.zeros((TO.perm.shape[0], X.shape[1]), complex)
+        for level in range(TO.nlevels):
+            for it in range(DO.nitems):
+                if XO[it] is None or TO.level[DO.item_node[it]] != level:
+                    continue
+                if DO.item_basis[it]:
+                    Y[TO.values(int(DO.item_node[it]))] += conj(XO[it]) @ yhat[it]
+                else:
+                    r0 = 0
+                    for ch in DO.item_chidx[DO.item_chptr[it]:DO.item_chptr[it + 1]]:
+                        rc = 0 if XO[ch] is None else XO[ch].shape[1]
+                        if rc:
+                            yhat[ch] = yhat[ch] + conj(XO[it][r0:r0 + rc]) @ yhat[it]
+                        r0 += rc
+        nptr, nnodes = (self.nearptr, self.nearnodes) if mode == 0 else (self.tnearptr, self.tnearnodes)
+        for t in range(TO.nnodes):
+            for s in nnodes[nptr[t]:nptr[t + 1]]:
+                rows, cols = TO.values(t), TI.values(int(s))
+                Nb = self._block(0, rows, cols) if mode == 0 else self._block(0, cols, rows).T
+                Y[rows] += conj(Nb) @ X[cols]
+        return Y[:, 0] if vec else Y

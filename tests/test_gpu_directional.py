@@ -1,0 +1,105 @@
+"""GPU: directional (wideband) H^2 matrices against the oracle.
+
+Basis items (one per (cluster, direction)), their ranks and pivots must agree exactly with the
+oracle's directional compressor; products in the three modes and with blocks of right-hand
+sides within 1e-12 (relative) of the oracle's directional product; the error against the
+dense matrix below 10 tol (the bar of the reference's IACA compressor tests,
+test/nca/test_petrovgalerkinnca.jl:152); the mixed-precision product within 1e-5 of FP64.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import cgauss, sphere
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+
+
+def _n():
+    import nca_b200
+    return nca_b200
+
+
+def build(test, trial, k, tol, minvalues, store_f32=False):
+    N = _n()
+    tt = N.KMeansTree(test, N.KMeansTreeBuilder(minvalues=minvalues))
+    st = N.KMeansTree(trial, N.KMeansTreeBuilder(minvalues=minvalues))
+    aca = N.ACA(N.FullPivoting(), N.FullPivoting(), N.FNormEstimator(tol))
+    tc = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(test, trial, st), compressor=aca)
+    sc = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(trial, test, tt), compressor=aca)
+    return N.PetrovGalerkinNCA(N.HelmholtzKernel(k, rmin=1e-12), test, trial, N.BlockTree(tt, st),
+                               isnear=N.isnearwideband(k), testcompressor=tc, trialcompressor=sc,
+                               store_f32=store_f32)
+
+
+def items(A, side):
+    N = _n()
+    L = N.lib()
+    n = C.c_int32()
+    N._lib.check(L.nca_core_dir_items(A.core._h, side, C.byref(n), None, None, None, None))
+    ni = n.value
+    ranks = np.zeros(max(ni, 1), np.int32)
+    nrows = np.zeros(max(ni, 1), np.int32)
+    ptr = np.zeros(ni + 1, np.int32)
+    idx = np.zeros(max(ni * A.core.maxrank, 1), np.int32)
+    N._lib.check(L.nca_core_dir_items(A.core._h, side, C.byref(n), N._lib.ptr(ranks), N._lib.ptr(nrows),
+                                      N._lib.ptr(ptr), N._lib.ptr(idx)))
+    return ranks[:ni], [idx[ptr[i]:ptr[i + 1]] for i in range(ni)]
+
+
+def relerr(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+CASES = [
+    ("galerkin sphere k=12", lambda: (sphere(2000, 1), None), 12.0, 1e-4, 32),
+    ("two point sets k=8", lambda: (sphere(1500, 2), sphere(1200, 3) * 0.8 + np.array([2.2, 0.4, 0.1])), 8.0, 1e-5, 24),
+    ("low frequency k=0.5", lambda: (sphere(1200, 4), None), 0.5, 1e-4, 32),
+]
+
+
+@pytest.mark.parametrize("name,make,k,tol,minvalues", CASES, ids=[c[0] for c in CASES])
+def test_directional_against_oracle(name, make, k, tol, minvalues):
+    from oracle import directional as OD
+    from oracle import oracle as O
+    N = _n()
+    test, trial = make()
+    trial = test if trial is None else trial
+    A = build(test, trial, k, tol, minvalues, store_f32=True)
+    H = OD.DirectionalH2(test, trial, O.Kernel(O.KIND_HELMHOLTZ, k=k, rmin=1e-12), k, minvalues=minvalues, tol=tol)
+    for side in (0, 1):
+        ranks, piv = items(A, side)
+        assert len(ranks) == H.dirs[side].nitems
+        for it in range(len(ranks)):
+            assert np.array_equal(piv[it], H.piv[side][it]), (side, it)
+    nt, ns = len(test), len(trial)
+    for b in (1, 5, 17):
+        x = cgauss((ns, b), 10 + b)
+        u = cgauss((nt, b), 20 + b)
+        assert relerr(A @ x, H.apply(x, 0)) < REL
+        assert relerr(A.T @ u, H.apply(u, 1)) < REL
+        assert relerr(A.H @ u, H.apply(u, 2)) < REL
+    x = cgauss(ns, 7)
+    rows = np.arange(0, nt, max(1, nt // 200))
+    ref = O.dense_rows(O.Kernel(O.KIND_HELMHOLTZ, k=k, rmin=1e-12), test, trial, rows, x)
+    assert relerr((A @ x)[rows], ref) < 10 * tol
+    W = N.H2Workspace(N.core(A), np.complex64)
+    X = cgauss((ns, 8), 8)
+    assert relerr(W @ X, A @ X) < 1e-5
+
+
+def test_directional_structure_and_limits():
+    N = _n()
+    pts = sphere(2000, 5)
+    A = build(pts, pts, 20.0, 1e-4, 32)
+    ranks, _ = items(A, 0)
+    assert len(ranks) > N.core(A).info.nnodes_test  # several directions per cluster
+    with pytest.raises(N.ArgumentError):
+        N.core(A).set_wavenumber(21.0)
+    with pytest.raises(N.ArgumentError):
+        N.batch([A])
+    with pytest.raises(N.ArgumentError):
+        N.core(A).pivots(0)
