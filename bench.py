@@ -44,9 +44,11 @@ def parse():
     p.add_argument("--precision", default="f64", choices=["f64", "f32"])
     p.add_argument("--npoints", type=int, default=65536)
     p.add_argument("--nrhs", type=int, default=16)
+    p.add_argument("--wideband-points", type=int, default=0, help="point count of the wideband workload")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-stages", action="store_true", help="print per-stage times to stderr")
-    p.add_argument("--workload", default="galerkin-sphere", choices=["galerkin-sphere", "batched-uneven", "gradients"],
+    p.add_argument("--workload", default="galerkin-sphere",
+                   choices=["galerkin-sphere", "batched-uneven", "gradients", "wideband"],
                    help="batched-uneven: 64 problems of uneven size, one batched product vs 64 calls; "
                         "gradients: dJ/dx and dJ/dk of J = ||H(k) x - b||^2 on a perturbed sphere")
     return p.parse_args()
@@ -511,6 +513,104 @@ def run_gradients(args):
             "clocks": clk}), flush=True)
 
 
+def run_wideband(args):
+    """Directional (wideband) sphere: n points uniform on the unit sphere (default 262,144),
+    k = 2 pi 8 (diameter 16 wavelengths), isnearwideband(k), tol 1e-4, minvalues 64; the work is
+    the build plus 100 matvecs with seeded complex Gaussian x. Plain FP64 form: 100 single-vector
+    FP64 products. Batched mixed-precision form: the 100 vectors as one block of right-hand sides
+    on the complex-FP32 stores (FP64 pivots and skeletons, FP64 accumulation)."""
+    import torch
+    import nca_b200 as N
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    n, k, nvec = args.wideband_points or 262144, 2 * np.pi * 8, 100
+    pts = sphere(n, 888)
+    t0 = time.perf_counter()
+    tree = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=64))
+    aca = N.ACA(N.FullPivoting(), N.FullPivoting(), N.FNormEstimator(1e-4))
+    comp = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(pts, pts, tree), compressor=aca)
+    core = N.PetrovGalerkinNCACore(N.HelmholtzKernel(k, rmin=1e-12), pts, pts, N.BlockTree(tree, tree),
+                                   isnear=N.isnearwideband(k), testcompressor=comp, trialcompressor=comp,
+                                   store_f32=True, device=local)
+    torch.cuda.synchronize()
+    build = time.perf_counter() - t0
+    info = info_dict(core)
+    L = N.lib()
+    X = rhs(n, nvec, seed=31)
+    dev = f"cuda:{local}"
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(dev)
+    Yd = torch.zeros_like(Xd)
+    W64 = N.H2Workspace(core, max_nrhs=16)
+    W32 = N.H2Workspace(core, np.complex64, max_nrhs=16)
+
+    def seq(W, prec):
+        def f():
+            for j in range(nvec):
+                N._lib.check(L.nca_apply(W._h, 0, prec, C.c_void_p(Xd[j].data_ptr()), n, C.c_void_p(Yd[j].data_ptr()),
+                                         n, 1, 1.0, 0.0, 0.0, 0.0, 1))
+        return f
+
+    def block(W, prec):
+        def f():
+            N._lib.check(L.nca_apply(W._h, 0, prec, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Yd.data_ptr()), n, nvec,
+                                     1.0, 0.0, 0.0, 0.0, 1))
+        return f
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3 / reps
+
+    clocks = Clocks(local)
+    clocks.start()
+    reps = max(1, args.steps // 10)
+    t_seq64 = timed(seq(W64, 0), reps)
+    t_seq32 = timed(seq(W32, 1), reps)
+    t_blk64 = timed(block(W64, 0), max(3, args.steps))
+    t_blk32 = timed(block(W32, 1), max(3, args.steps))
+    clk = clocks.stop()
+    launches = C.c_int32()
+    L.nca_workspace_last_launches(W32._h, C.byref(launches))
+    # errors: FP32 block vs FP64 block; FP64 vs dense rows (first vector)
+    Y64 = torch.zeros_like(Xd)
+    N._lib.check(L.nca_apply(W64._h, 0, 0, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Y64.data_ptr()), n, nvec,
+                             1.0, 0.0, 0.0, 0.0, 1))
+    block(W32, 1)()
+    torch.cuda.synchronize()
+    rel32 = float((Yd - Y64).norm() / Y64.norm())
+    err = dense_rows_error_k(N, pts, core, W64, X, k) if rank == 0 else None
+    bytes32 = product_bytes(info, nvec, 8)
+    plain = build + t_seq64
+    mixed = build + t_blk32
+    peak, peak_kind = peaks()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": bytes32 / t_blk32 / 1e9, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": 1e3 * t_blk32, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "complex-f32 stores, f64 accumulation", "data": "synthetic",
+            "config": {"workload": f"wideband-sphere-{n}-k16pi-tol1e-4-100vec", "npoints": n, "k": k,
+                       "admissibility": "isnearwideband(k; eta_lf=1, eta_hf=5, gamma=1)",
+                       "step": "100 matvecs as one block of 100 right-hand sides",
+                       "l2": "inputs larger than L2", "build_s": build, "build_device_s": info["build_seconds"],
+                       "stored_gb_f64": E * store_entries(info) / 1e9, "relerr_vs_dense_rows": err,
+                       "relerr_f32_vs_f64": rel32},
+            "plain_f64_100_single_matvecs_s": t_seq64, "mixed_f32_100_single_matvecs_s": t_seq32,
+            "f64_block_of_100_s": t_blk64, "mixed_block_of_100_s": t_blk32,
+            "build_plus_100_matvecs_s": {"plain_f64": plain, "batched_mixed": mixed, "speedup": plain / mixed},
+            "matvec_speedup_batched_mixed_vs_plain_f64": t_seq64 / t_blk32,
+            "roofline": {"bound": "hbm", "achieved": bytes32 / t_blk32 / 1e9, "peak": peak, "peak_source": peak_kind,
+                         "unit": "GB/s", "frac": bytes32 / t_blk32 / 1e9 / peak, "traffic": None,
+                         "note": "whole block product, algorithmic bytes (stores once per 16-column pass)"},
+            "gpu_launches": launches.value, "clocks": clk}), flush=True)
+
+
 def tangent_bytes(info, b, e=E):
     """Algorithmic bytes of one tangent product: every stored entry and its d/dk twice as many
     stores (X, dX, S, dS, N, dN), x read, y written, four coefficient vectors written and read."""
@@ -539,6 +639,9 @@ def main():
         return
     if args.workload == "gradients":
         run_gradients(args)
+        return
+    if args.workload == "wideband":
+        run_wideband(args)
         return
     import torch
     import torch.distributed as dist

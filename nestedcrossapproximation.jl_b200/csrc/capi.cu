@@ -1195,6 +1195,11 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             B.finish(pr.leaves, dout.X.p, s);
         }
     }
+    // the per-item operators live on in the stage stores (directional cores have no node exports)
+    for (DirItems &d : D->side) {
+        d.X.release();
+        d.XT.release();
+    }
     if (c->f32) {
         auto down = [&](DBuf<double2> &src, DBuf<float2> &dst) {
             dst.alloc(src.n);

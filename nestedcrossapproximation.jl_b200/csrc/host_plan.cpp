@@ -223,17 +223,51 @@ Partition build_partition(const Tree &test, const Tree &trial, double eta) {
 
 namespace {
 
+// Per-thread caches of the tree-mimicry selection, valid for one selection (generation stamp):
+// the running minimum squared distance of a point / node centre to the chosen pivots and how
+// many pivots it already accounts for, the pivots taken inside each node, the taken positions.
+// Minima and counts are exact, so the cached selection equals the direct one bit for bit.
+struct MimicryCache {
+    uint32_t gen = 0;
+    std::vector<uint32_t> pst, nst, tst, kst;
+    std::vector<double> pd, nd;
+    std::vector<int32_t> pc, nc, taken;
+    void prepare(const Tree &F) {
+        if (pst.size() < size_t(F.npoints)) {
+            pst.assign(F.npoints, 0);
+            kst.assign(F.npoints, 0);
+            pd.assign(F.npoints, 0.0);
+            pc.assign(F.npoints, 0);
+        }
+        if (nst.size() < size_t(F.nnodes)) {
+            nst.assign(F.nnodes, 0);
+            tst.assign(F.nnodes, 0);
+            nd.assign(F.nnodes, 0.0);
+            nc.assign(F.nnodes, 0);
+            taken.assign(F.nnodes, 0);
+        }
+        if (++gen == 0) {  // wrapped: clear every stamp
+            std::fill(pst.begin(), pst.end(), 0);
+            std::fill(kst.begin(), kst.end(), 0);
+            std::fill(nst.begin(), nst.end(), 0);
+            std::fill(tst.begin(), tst.end(), 0);
+            gen = 1;
+        }
+    }
+};
+thread_local MimicryCache t_cache;
+
 // Greedy tree-mimicry selection state for one cluster.
 class Mimicry {
   public:
     Mimicry(const Tree &far, const double *farpts, const double *centroid, const int32_t *roots,
             int nroots, int capacity)
-        : F_(far), pts_(farpts), roots_(roots), nroots_(nroots) {
+        : F_(far), pts_(farpts), roots_(roots), nroots_(nroots), C_(t_cache) {
         std::memcpy(c_, centroid, sizeof(c_));
         chosen_xyz_.reserve(3 * size_t(capacity));
-        chosen_pos_.reserve(capacity);
         root_dmin_.assign(nroots, 1.0);
         root_taken_.assign(nroots, 0);
+        C_.prepare(far);
     }
 
     int32_t next() {
@@ -255,7 +289,7 @@ class Mimicry {
                 int ch = F_.firstchild[node] + c;
                 if (F_.size(ch) - taken_inside(ch) <= 0) continue;
                 const double *cc = &F_.center[3 * size_t(ch)];
-                double sc = score(cc, dmin(cc));
+                double sc = score(cc, dmin_cached(C_.nst, C_.nd, C_.nc, ch, cc));
                 if (sc > pbest) {
                     pbest = sc;
                     pick = ch;
@@ -266,9 +300,9 @@ class Mimicry {
         int bestpos = -1;
         best = -1.0;
         for (int pos = F_.begin[node]; pos < F_.end[node]; ++pos) {
-            if (std::find(chosen_pos_.begin(), chosen_pos_.end(), pos) != chosen_pos_.end()) continue;
+            if (C_.kst[pos] == C_.gen) continue;  // already chosen
             const double *y = pts_ + 3 * int64_t(F_.perm[pos]);
-            double sc = score(y, dmin(y));
+            double sc = score(y, dmin_cached(C_.pst, C_.pd, C_.pc, pos, y));
             if (sc > best) {
                 best = sc;
                 bestpos = pos;
@@ -276,9 +310,17 @@ class Mimicry {
         }
         int32_t id = F_.perm[bestpos];
         const double *y = pts_ + 3 * int64_t(id);
-        bool firstpick = chosen_pos_.empty();
-        chosen_pos_.push_back(bestpos);
+        bool firstpick = nchosen_ == 0;
+        C_.kst[bestpos] = C_.gen;
         chosen_xyz_.insert(chosen_xyz_.end(), y, y + 3);
+        ++nchosen_;
+        for (int a = node; a >= 0; a = F_.parent[a]) {
+            if (C_.tst[a] != C_.gen) {
+                C_.tst[a] = C_.gen;
+                C_.taken[a] = 0;
+            }
+            ++C_.taken[a];
+        }
         for (int i = 0; i < nroots_; ++i) {
             int f = roots_[i];
             double d = dist2(&F_.center[3 * size_t(f)], y);
@@ -294,25 +336,32 @@ class Mimicry {
         if (d2 < 1e-300) d2 = 1e-300;
         return dmin2 / d2;
     }
-    double dmin(const double *y) const {
-        if (chosen_pos_.empty()) return 1.0;
-        double m = INFINITY;
-        for (size_t q = 0; q < chosen_pos_.size(); ++q) m = std::min(m, dist2(y, &chosen_xyz_[3 * q]));
+    // min over the chosen pivots of the squared distance to y (1 before the first pick),
+    // caught up from the pivots this entry has not seen yet
+    double dmin_cached(std::vector<uint32_t> &st, std::vector<double> &dv, std::vector<int32_t> &cnt, int idx,
+                       const double *y) {
+        if (nchosen_ == 0) return 1.0;
+        if (st[idx] != C_.gen) {
+            st[idx] = C_.gen;
+            dv[idx] = INFINITY;
+            cnt[idx] = 0;
+        }
+        double m = dv[idx];
+        for (int q = cnt[idx]; q < nchosen_; ++q) m = std::min(m, dist2(y, &chosen_xyz_[3 * size_t(q)]));
+        dv[idx] = m;
+        cnt[idx] = nchosen_;
         return m;
     }
-    int taken_inside(int node) const {
-        int k = 0;
-        for (int pos : chosen_pos_) k += (pos >= F_.begin[node] && pos < F_.end[node]);
-        return k;
-    }
+    int taken_inside(int node) const { return C_.tst[node] == C_.gen ? C_.taken[node] : 0; }
 
     const Tree &F_;
     const double *pts_;
     const int32_t *roots_;
     int nroots_;
+    MimicryCache &C_;
     double c_[3];
     std::vector<double> chosen_xyz_;
-    std::vector<int> chosen_pos_;
+    int nchosen_ = 0;
     std::vector<double> root_dmin_;
     std::vector<int> root_taken_;
 };
