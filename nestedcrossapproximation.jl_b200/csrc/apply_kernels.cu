@@ -584,6 +584,127 @@ template void launch_rows<double2>(const RowArgs<double2> &, const int32_t *, in
 template void launch_rows<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
 
 namespace {
+__device__ __forceinline__ double2 widen(double2 v) { return v; }
+__device__ __forceinline__ double2 widen(float2 v) { return make_double2(v.x, v.y); }
+
+// One warp per output of R <= 64 rows. RG = lanes per row group (a power of two >= min(R, 32));
+// the 32 / RG column groups of the warp take the segment columns round robin and are summed by
+// shuffles at the end; with R > 32 every lane keeps two rows. QB right-hand sides per pass; U
+// columns per step, their loads issued together so that one memory round trip serves U columns.
+template <typename S, int QB, int U>
+__global__ void __launch_bounds__(256) k_gather_small(RowArgs<S> a, const int32_t *nodes, int count) {
+    const int lane = threadIdx.x & 31;
+    const int wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (wid >= count) return;
+    const int o = nodes[wid];
+    const int R = a.g_rows[o];
+    int RG = 32;
+    while (RG > 1 && RG / 2 >= R) RG >>= 1;
+    const int CG = 32 / RG;
+    const int r0 = lane % RG, cg = lane / RG;
+    const bool two = R > 32;
+    const int e0 = a.g_segptr[o], e1 = a.g_segptr[o + 1];
+    const double sg = a.conj ? -1.0 : 1.0;
+    const bool scatter = a.y != nullptr;
+    for (int qb = 0; qb < a.bc; qb += QB) {
+        const int nq = a.bc - qb < QB ? a.bc - qb : QB;
+        double2 acc0[QB], acc1[QB];
+#pragma unroll
+        for (int q = 0; q < QB; ++q) acc0[q] = acc1[q] = make_double2(0.0, 0.0);
+        for (int e = e0; e < e1; ++e) {
+            const int64_t mo = a.g_moff[e];
+            const S *M = mo >= 0 ? a.M + mo : a.M2 + (-1 - mo);
+            const int w = a.g_w[e];
+            const double2 *V = a.src + a.g_voff[e] * a.vs + a.q0 + qb;
+            for (int j0 = cg; j0 < w; j0 += U * CG) {
+                double2 m0[U], m1[U], x[U][QB];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int j = j0 + u * CG;
+                    const bool in = j < w;
+                    m0[u] = in && r0 < R ? widen(M[r0 + int64_t(j) * R]) : make_double2(0.0, 0.0);
+                    m1[u] = in && two && r0 + 32 < R ? widen(M[r0 + 32 + int64_t(j) * R]) : make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int q = 0; q < QB; ++q)
+                        x[u][q] = in && q < nq ? V[int64_t(j) * a.vs + q] : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    m0[u].y *= sg;
+                    m1[u].y *= sg;
+#pragma unroll
+                    for (int q = 0; q < QB; ++q) {
+                        const double2 xv = x[u][q];
+                        acc0[q].x = fma(m0[u].x, xv.x, fma(-m0[u].y, xv.y, acc0[q].x));
+                        acc0[q].y = fma(m0[u].x, xv.y, fma(m0[u].y, xv.x, acc0[q].y));
+                        if (two) {
+                            acc1[q].x = fma(m1[u].x, xv.x, fma(-m1[u].y, xv.y, acc1[q].x));
+                            acc1[q].y = fma(m1[u].x, xv.y, fma(m1[u].y, xv.x, acc1[q].y));
+                        }
+                    }
+                }
+            }
+        }
+        // sum the column groups (lane bits above the row group)
+        for (int off = RG; off < 32; off <<= 1) {
+#pragma unroll
+            for (int q = 0; q < QB; ++q) {
+                acc0[q].x += __shfl_xor_sync(0xffffffffu, acc0[q].x, off);
+                acc0[q].y += __shfl_xor_sync(0xffffffffu, acc0[q].y, off);
+                if (two) {
+                    acc1[q].x += __shfl_xor_sync(0xffffffffu, acc1[q].x, off);
+                    acc1[q].y += __shfl_xor_sync(0xffffffffu, acc1[q].y, off);
+                }
+            }
+        }
+        if (cg != 0) continue;
+        for (int h = 0; h < (two ? 2 : 1); ++h) {
+            const int i = r0 + 32 * h;
+            if (i >= R) continue;
+#pragma unroll
+            for (int q = 0; q < QB; ++q) {
+                if (q >= nq) break;
+                double2 v = h ? acc1[q] : acc0[q];
+                const int col = a.q0 + qb + q;
+                if (scatter) {
+                    double2 *yp = a.y + a.perm[a.g_out[o] + i] + int64_t(col) * a.ldy;
+                    double2 out = make_double2(a.alpha.x * v.x - a.alpha.y * v.y, a.alpha.x * v.y + a.alpha.y * v.x);
+                    if (a.usebeta) {
+                        const double2 yo = *yp;
+                        out.x += a.beta.x * yo.x - a.beta.y * yo.y;
+                        out.y += a.beta.x * yo.y + a.beta.y * yo.x;
+                    }
+                    *yp = out;
+                } else {
+                    double2 *d = a.dst + (a.g_out[o] + i) * a.vs + col;
+                    if (a.accumulate) {
+                        const double2 old = *d;
+                        v = make_double2(old.x + v.x, old.y + v.y);
+                    }
+                    *d = v;
+                }
+            }
+        }
+    }
+}
+}  // namespace
+
+template <typename S>
+void launch_gather_small(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
+    if (count <= 0) return;
+    const int grid = (count + 7) / 8;
+    if (a.bc <= 1)
+        k_gather_small<S, 1, 8><<<grid, 256, 0, s>>>(a, nodes, count);
+    else if (a.bc <= 4)
+        k_gather_small<S, 4, 2><<<grid, 256, 0, s>>>(a, nodes, count);
+    else
+        k_gather_small<S, 8, 1><<<grid, 256, 0, s>>>(a, nodes, count);
+}
+
+template void launch_gather_small<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
+template void launch_gather_small<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+
+namespace {
 template <typename S>
 __global__ void k_copy_blocks(const S *src, const int64_t *soff, const int32_t *sld, const int32_t *rows,
                               const int32_t *cols, const int64_t *doff, int64_t nblocks, S *dst) {

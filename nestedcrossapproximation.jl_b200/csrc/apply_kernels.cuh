@@ -67,6 +67,11 @@ int vector_stride(int b);  // row stride of the internal vector buffers for b ri
 template <typename S>
 void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
 
+// STAGE_GATHER for outputs of at most 64 rows: one warp per output, operands read straight from
+// global memory, complex FP64 FMA (directional products, whose outputs are many small blocks).
+template <typename S>
+void launch_gather_small(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
+
 // dst[doff[e] + i + j * rows[e]] = src[soff[e] + i + j * sld[e]]: sub-matrix copies into
 // contiguous column-major blocks.
 template <typename S>

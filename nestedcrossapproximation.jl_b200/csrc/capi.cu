@@ -154,6 +154,7 @@ struct DirItems {
 struct GatherStage {
     std::vector<int32_t> group_ptr;  // launch groups (levels) over the outputs
     std::vector<int> group_maxrows;
+    std::vector<double> group_work;  // mean block entries per output of each group
     DBuf<int32_t> outputs, rows, segptr, w;
     DBuf<int64_t> out, moff, voff;
     DBuf<double2> M;
@@ -771,6 +772,7 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
 struct StageBuilder {
     std::vector<int32_t> group_ptr{0};
     std::vector<int> group_maxrows;
+    std::vector<double> group_work;
     std::vector<int32_t> rows, segptr{0}, w;
     std::vector<int64_t> out, moff, voff, work;
     // sub-matrix copies from the source store into the stage store
@@ -804,7 +806,11 @@ struct StageBuilder {
     }
     void end_output() { segptr.push_back(int32_t(moff.size())); }
     void end_group() {
-        group_ptr.push_back(int32_t(rows.size()));
+        const int32_t b = group_ptr.back(), e = int32_t(rows.size());
+        double sum = 0.0;
+        for (int32_t i = b; i < e; ++i) sum += double(work[i]);
+        group_work.push_back(e > b ? sum / double(e - b) : 0.0);
+        group_ptr.push_back(e);
         group_maxrows.push_back(std::max(cur_max, 1));
         cur_max = 0;
     }
@@ -818,6 +824,7 @@ struct StageBuilder {
                              [&](int a, int b) { return work[a] > work[b]; });
         G.group_ptr = group_ptr;
         G.group_maxrows = group_maxrows;
+        G.group_work = group_work;
         G.outputs.upload(order, s);
         G.rows.upload(rows, s);
         G.out.upload(out, s);
@@ -1621,7 +1628,11 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
                     a.conj = conj;
                     a.maxrows = G.group_maxrows[g];
                     a.error = error;
-                    launch_rows<S>(a, G.outputs.p + G.group_ptr[g], cnt, s);
+                    // many small outputs: one warp each; few large ones: the streaming MMA kernel
+                    if (a.maxrows <= 64 && G.group_work[g] < 8192.0)
+                        launch_gather_small<S>(a, G.outputs.p + G.group_ptr[g], cnt, s);
+                    else
+                        launch_rows<S>(a, G.outputs.p + G.group_ptr[g], cnt, s);
                     ++count.total;
                 }
             };
