@@ -896,49 +896,18 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         d.nitems = ni;
         bylevel[sd].assign(T.nlevels, {});
         for (int it = 0; it < ni; ++it) bylevel[sd][T.level[pl.item_node[it]]].push_back(it);
-        std::vector<int64_t> mb(ni, 0), rb(ni, 0);
-        std::vector<int32_t> lv_ptr{0}, lv_nodes;
-        std::vector<int> lv_mcap, lv_ncap;
-        for (int lev = T.nlevels - 1; lev >= 0; --lev) {
-            int mc = 0, nc = 0;
-            for (int it : bylevel[sd][lev]) {
-                const int nfp = d.h_fpptr[it + 1] - d.h_fpptr[it];
-                if (nfp == 0) continue;
-                int64_t m = 0;
-                if (pl.item_basis[it]) {
-                    m = T.size(pl.item_node[it]);
-                } else {
-                    for (int k = pl.item_chptr[it]; k < pl.item_chptr[it + 1]; ++k) m += rb[pl.item_chidx[k]];
-                }
-                mb[it] = m;
-                rb[it] = std::min<int64_t>({int64_t(maxrank), m, int64_t(nfp)});
-                lv_nodes.push_back(it);
-                mc = std::max<int>(mc, int(m));
-                nc = std::max(nc, nfp);
-            }
-            lv_ptr.push_back(int32_t(lv_nodes.size()));
-            lv_mcap.push_back(mc);
-            lv_ncap.push_back(nc);
-        }
-        d.h_xoff.assign(ni + 1, 0);
-        for (int it = 0; it < ni; ++it) d.h_xoff[it + 1] = d.h_xoff[it] + pad2(mb[it] * rb[it]);
         d.item_node.upload(pl.item_node, s);
         d.item_basis.upload(pl.item_basis, s);
         d.item_chptr.upload(pl.item_chptr, s);
         d.item_chidx.upload(pl.item_chidx, s);
         d.fpptr.upload(d.h_fpptr, s);
         d.fpidx.upload(d.h_fpidx, s);
-        d.xoff.upload(d.h_xoff, s);
-        d.X.alloc(size_t(d.h_xoff.back()));
         d.rank.alloc(std::max(ni, 1));
         d.rank.zero(s);
         d.nrows.alloc(std::max(ni, 1));
         d.nrows.zero(s);
         d.piv.alloc(size_t(std::max(ni, 1)) * maxrank);
         d.cpiv.alloc(size_t(std::max(ni, 1)) * maxrank);
-        DBuf<int32_t> nodes;
-        nodes.upload(lv_nodes, s);
-        status.zero(s);
         LevelArgs a{};
         a.K = c->K;
         a.side = sd;
@@ -955,8 +924,6 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         a.nrows = d.nrows.p;
         a.piv = d.piv.p;
         a.cpiv = d.cpiv.p;
-        a.X = d.X.p;
-        a.xoff = d.xoff.p;
         a.maxrank = maxrank;
         a.tol = sd == 0 ? o->tol_test : o->tol_trial;
         a.sampled = o->sampled;
@@ -965,35 +932,116 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         a.item_basis = d.item_basis.p;
         a.item_chptr = d.item_chptr.p;
         a.item_chidx = d.item_chidx.p;
-        size_t maxsm = 0;
-        for (size_t l = 0; l + 1 < lv_ptr.size(); ++l)
-            maxsm = std::max(maxsm, level_smem_bytes(lv_mcap[l], lv_ncap[l]));
-        if (maxsm > size_t(kMaxSmem))
-            throw Failure(NCA_ERR_ARG, "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
-        CK(cudaFuncSetAttribute(k_level_compress, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                int(std::max<size_t>(maxsm, 16))));
-        for (size_t l = 0; l + 1 < lv_ptr.size(); ++l) {
-            const int cnt = lv_ptr[l + 1] - lv_ptr[l];
-            if (cnt == 0) continue;
-            k_level_compress<<<cnt, 256, level_smem_bytes(lv_mcap[l], lv_ncap[l]), s>>>(a, nodes.p + lv_ptr[l],
-                                                                                         lv_mcap[l], lv_ncap[l]);
+        // Level by level, deepest first: the rows of a nested item are its children's actual
+        // ranks, so each level's X is allocated for min(maxrank, rows, far pivots) columns, then
+        // compacted to the ranks found before the next level runs.
+        d.h_rank.assign(ni, 0);
+        d.h_nrows.assign(ni, 0);
+        std::vector<int64_t> lvoff(std::max(ni, 1), 0), cpos(ni, -1);
+        std::vector<std::unique_ptr<DBuf<double2>>> levelX;
+        std::vector<std::vector<int32_t>> levelItems;
+        DBuf<int64_t> dlvoff;
+        int64_t total = 0;
+        for (int lev = T.nlevels - 1; lev >= 0; --lev) {
+            std::vector<int32_t> items;
+            int mc = 0, nc = 0;
+            int64_t bound = 0;
+            for (int it : bylevel[sd][lev]) {
+                const int nfp = d.h_fpptr[it + 1] - d.h_fpptr[it];
+                if (nfp == 0) continue;
+                int64_t m = 0;
+                if (pl.item_basis[it]) {
+                    m = T.size(pl.item_node[it]);
+                } else {
+                    for (int k = pl.item_chptr[it]; k < pl.item_chptr[it + 1]; ++k) m += d.h_rank[pl.item_chidx[k]];
+                }
+                const int64_t rb = std::min<int64_t>(std::min<int64_t>(maxrank, m), int64_t(nfp));
+                lvoff[it] = bound;
+                bound += pad2(m * rb);
+                items.push_back(it);
+                mc = std::max<int>(mc, int(m));
+                nc = std::max(nc, nfp);
+            }
+            if (items.empty()) continue;
+            const size_t sm = level_smem_bytes(mc, nc);
+            if (sm > size_t(kMaxSmem))
+                throw Failure(NCA_ERR_ARG, "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
+            CK(cudaFuncSetAttribute(k_level_compress, cudaFuncAttributeMaxDynamicSharedMemorySize, int(std::max<size_t>(sm, 16))));
+            DBuf<double2> chunk;
+            chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
+            dlvoff.upload(lvoff, s);
+            DBuf<int32_t> nodes;
+            nodes.upload(items, s);
+            status.zero(s);
+            a.X = chunk.p;
+            a.xoff = dlvoff.p;
+            k_level_compress<<<int(items.size()), 256, sm, s>>>(a, nodes.p, mc, nc);
             CK(cudaGetLastError());
+            const std::vector<int32_t> st = status.download(s);
+            if (st[0] == 1) {
+                set_singular(sd, st[1], st[2], st[3]);
+                throw Failure(NCA_ERR_SINGULAR, "SingularCrossMatrixError: the cross matrix of " +
+                                                    std::string(sd == 0 ? "test" : "trial") + " item " +
+                                                    std::to_string(st[1]) + " is singular - " + std::to_string(st[2]) +
+                                                    " pivots were selected but only " + std::to_string(st[3]) +
+                                                    " of them are linearly independent");
+            }
+            if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: level block exceeds its planned capacity");
+            const std::vector<int32_t> rk = download_now(d.rank, size_t(ni)), nr = download_now(d.nrows, size_t(ni));
+            // compact this level: exact m x r blocks, back to back
+            std::vector<int64_t> soff, doff;
+            std::vector<int32_t> sld, crows, ccols;
+            int64_t lt = 0;
+            for (int it : items) {
+                d.h_rank[it] = rk[it];
+                d.h_nrows[it] = nr[it];
+                cpos[it] = lt;
+                if (rk[it] > 0 && nr[it] > 0) {
+                    soff.push_back(lvoff[it]);
+                    sld.push_back(nr[it]);
+                    crows.push_back(nr[it]);
+                    ccols.push_back(rk[it]);
+                    doff.push_back(lt);
+                }
+                lt += pad2(int64_t(nr[it]) * rk[it]);
+            }
+            levelX.emplace_back(new DBuf<double2>());
+            levelX.back()->alloc(size_t(std::max<int64_t>(lt, 1)));
+            if (!soff.empty()) {
+                DBuf<int64_t> dso, ddo;
+                DBuf<int32_t> dld, dr, dc;
+                dso.upload(soff, s);
+                ddo.upload(doff, s);
+                dld.upload(sld, s);
+                dr.upload(crows, s);
+                dc.upload(ccols, s);
+                launch_copy_blocks<double2>(chunk.p, dso.p, dld.p, dr.p, dc.p, ddo.p, int64_t(soff.size()),
+                                            levelX.back()->p, s);
+                CK(cudaGetLastError());
+                CK(cudaStreamSynchronize(s));
+            }
+            levelItems.push_back(items);
+            for (int it : items) cpos[it] += total;
+            total += lt;
         }
-        const std::vector<int32_t> st = status.download(s);
-        if (st[0] == 1) {
-            set_singular(sd, st[1], st[2], st[3]);
-            throw Failure(NCA_ERR_SINGULAR, "SingularCrossMatrixError: the cross matrix of " +
-                                                std::string(sd == 0 ? "test" : "trial") + " item " +
-                                                std::to_string(st[1]) + " is singular - " + std::to_string(st[2]) +
-                                                " pivots were selected but only " + std::to_string(st[3]) +
-                                                " of them are linearly independent");
+        // one X for the side: the compacted levels back to back
+        d.h_xoff.assign(ni + 1, 0);
+        for (int it = 0; it < ni; ++it) d.h_xoff[it] = cpos[it] >= 0 ? cpos[it] : 0;
+        d.h_xoff[ni] = total;
+        d.X.alloc(size_t(std::max<int64_t>(total, 1)));
+        {
+            int64_t off = 0;
+            for (size_t l = 0; l < levelX.size(); ++l) {
+                int64_t lt = 0;
+                for (int it : levelItems[l]) lt += pad2(int64_t(d.h_nrows[it]) * d.h_rank[it]);
+                if (lt) CK(cudaMemcpyAsync(d.X.p + off, levelX[l]->p, sizeof(double2) * lt, cudaMemcpyDeviceToDevice, s));
+                off += lt;
+            }
+            CK(cudaStreamSynchronize(s));
+            levelX.clear();
         }
-        if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: level block exceeds its planned capacity");
-        d.h_rank = d.rank.download(s);
-        d.h_nrows = d.nrows.download(s);
+        d.xoff.upload(d.h_xoff, s);
         d.h_piv = d.piv.download(s);
-        d.h_rank.resize(ni);
-        d.h_nrows.resize(ni);
         d.h_cptr.assign(ni + 1, 0);
         for (int it = 0; it < ni; ++it) {
             d.h_cptr[it + 1] = d.h_cptr[it] + d.h_rank[it];
