@@ -13,7 +13,7 @@
 //   leaves   y_t = X_t yhat_t + sum_s N_ts x_s (reverse: from the transposed near blocks NT),
 //            scattered straight into the caller's layout.
 //
-// CTA = 8 consumer warps + 1 producer warp. The producer streams tiles through a 3-stage
+// CTA = 8 consumer warps + 1 producer warp. The producer streams tiles through a 2-stage
 // shared-memory ring with cp.async.bulk (bulk copies completing on a "full" mbarrier), filling
 // each stage with columns of successive segments; the consumers release stages on an "empty"
 // mbarrier. Tiles go through the FP64 tensor-core MMA (mma.m8n8k4.f64) with three real
@@ -37,8 +37,8 @@ namespace {
 
 constexpr int NCONS = 8;              // consumer warps
 constexpr int NT = (NCONS + 1) * 32;  // + one producer warp
-constexpr int NSTAGE = 3;
-constexpr int STAGE_BYTES = 23552;  // one ring stage: w matrix columns, then w vector rows
+constexpr int NSTAGE = 2;
+constexpr int STAGE_BYTES = 35328;  // one ring stage: w matrix columns, then w vector rows
 
 // Shared-memory strides (in 16-byte elements) that are 2 mod 4: the four lanes of an MMA
 // fragment row then hit four different bank groups.
@@ -309,10 +309,13 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
     const bool vwhole = bc == a.b;
     const int ldv = vwhole ? a.vs : conflict_free(bc);
     // columns per stage: matrix columns first, the vector rows at voff (16-byte aligned). Chunks
-    // are whole groups of 8 columns (two k-steps of 4, one per accumulator set), so interior
-    // FP32 chunks stay 16-byte multiples.
+    // are whole groups of k-steps of 4, one per accumulator set, so interior FP32 chunks stay
+    // 16-byte multiples.
     int wmax = STAGE_BYTES / (ldm * elem + ldv * 16);
-    wmax &= wmax >= 8 ? ~7 : ~3;
+    {
+        constexpr int kq = 4 * Acc<NRT, NTL>::NSET;
+        wmax = wmax >= kq ? wmax - wmax % kq : (wmax & ~3);
+    }
     if (wmax < 4) wmax = 4;
     int voff = (wmax * ldm * elem + 15) & ~15;
     while (wmax > 4 && voff + wmax * ldv * 16 > STAGE_BYTES) {
