@@ -193,7 +193,9 @@ int32_t nca_core_export_couplings(const nca_core *core, int64_t *off, double *C)
 int32_t nca_core_export_near(const nca_core *core, int64_t *off, int32_t *ncols, double *N);
 
 /* ---- the H^2 product: H2Workspace + _unsafe_mul!/_mul! (petrovgalerkinnca.jl:253-271,
- *      :415-589). A workspace owns the coefficient buffers and a CUDA stream. ---- */
+ *      :415-589). A workspace owns the coefficient buffers and two CUDA streams (the product
+ *      stream and, for non-directional cores, a higher-priority stream for the far-field
+ *      sweeps, joined back before the leaf bases). ---- */
 int32_t nca_workspace_create(nca_core *core, int32_t max_nrhs, nca_workspace **out);
 void nca_workspace_destroy(nca_workspace *ws);
 /* y = alpha * op(H) x + beta * y for nrhs columns. memspace 0: x and y are host pointers
@@ -229,9 +231,12 @@ int32_t nca_workspace_last_launches(const nca_workspace *ws, int32_t *launches);
 /* Which parts the workspace applies: the far field (nested bases, transfers, couplings) and/or
  * the near field. farmatrix / nearmatrix of the reference (petrovgalerkinnca.jl:344-371). */
 int32_t nca_workspace_set_parts(nca_workspace *ws, int32_t far, int32_t near);
-/* Stage timers (CUDA events around each stage on the workspace stream). With profiling on,
- * nca_workspace_stage_times returns the device seconds and launches of the last nca_apply per
- * stage: 0 gather of x, 1 upward sweep, 2 coupling, 3 downward sweep, 4 leaves + near field. */
+/* Stage timers (CUDA events around each stage). With profiling on, nca_workspace_stage_times
+ * returns the device seconds and launches of the last nca_apply per stage: 0 gather of x,
+ * 1 upward sweep, 2 coupling, 3 downward sweep, 4 near field, 5 leaves. A workspace runs the
+ * three sweeps on a second stream of its own beside the near field (stage 4) and then adds the
+ * leaf bases (stage 5); with only one part present, stage 5 is the whole leaf launch and
+ * stage 4 is empty. Stages 1-3 and 4 overlap in time. */
 int32_t nca_workspace_set_profiling(nca_workspace *ws, int32_t on);
 int32_t nca_workspace_stage_times(const nca_workspace *ws, double *seconds, int32_t *launches,
                                   int32_t nstages);

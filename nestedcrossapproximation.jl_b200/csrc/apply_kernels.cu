@@ -532,8 +532,7 @@ int vector_stride(int b) { return conflict_free(b); }
 
 namespace {
 template <typename S, int NRT, int NTL>
-void launch_tiles(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
-    const size_t sm = rows_smem_bytes();
+void launch_tiles(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t sm) {
     switch (a.stage) {
     case STAGE_UP:
         cudaFuncSetAttribute(k_rows_up<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
@@ -560,31 +559,33 @@ void launch_tiles(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStre
 // Row tiles per warp for the largest block of the launch: 1, 2, 4 or (one column tile only) 8;
 // rows_capacity keeps R * ceil(bc / 8) <= 512, so the tiles of a warp never exceed 8.
 template <typename S, int NTL>
-void launch_ntl(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
+void launch_ntl(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t sm) {
     const int MT = (a.maxrows + 7) / 8;
     const int nrt = (MT + NCONS - 1) / NCONS;
     if (nrt <= 1)
-        launch_tiles<S, 1, NTL>(a, nodes, count, s);
+        launch_tiles<S, 1, NTL>(a, nodes, count, s, sm);
     else if (nrt <= 2)
-        launch_tiles<S, 2, NTL>(a, nodes, count, s);
+        launch_tiles<S, 2, NTL>(a, nodes, count, s, sm);
     else if (nrt <= 4 || NTL == 2)
-        launch_tiles<S, 4, NTL>(a, nodes, count, s);
+        launch_tiles<S, 4, NTL>(a, nodes, count, s, sm);
     else
-        launch_tiles<S, (NTL == 1 ? 8 : 4), NTL>(a, nodes, count, s);
+        launch_tiles<S, (NTL == 1 ? 8 : 4), NTL>(a, nodes, count, s, sm);
 }
 }  // namespace
 
 template <typename S>
-void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
+void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t smem_bytes) {
     if (count <= 0) return;
+    const size_t sm = smem_bytes ? smem_bytes : rows_smem_bytes();
     if (a.bc > 8)
-        launch_ntl<S, 2>(a, nodes, count, s);
+        launch_ntl<S, 2>(a, nodes, count, s, sm);
     else
-        launch_ntl<S, 1>(a, nodes, count, s);
+        launch_ntl<S, 1>(a, nodes, count, s, sm);
 }
 
-template void launch_rows<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
-template void launch_rows<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+template void launch_rows<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t, size_t);
+template void launch_rows<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t, size_t);
+
 
 namespace {
 __device__ __forceinline__ double2 widen(double2 v) { return v; }

@@ -229,9 +229,13 @@ struct nca_workspace {
     int last_launches = 0;
     bool far = true, near = true;
     bool profiling = false;
-    cudaEvent_t stage_ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    double stage_seconds[5] = {0, 0, 0, 0, 0};
-    int stage_launches[5] = {0, 0, 0, 0, 0};
+    cudaEvent_t stage_ev[9] = {};  // StageEvent order
+    double stage_seconds[6] = {0, 0, 0, 0, 0, 0};
+    int stage_launches[6] = {0, 0, 0, 0, 0, 0};
+    // far-field sweeps beside the near field: a second stream (higher priority, so the sweeps'
+    // small launches take SM slots as the near-field CTAs retire) and its fork / join events
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 namespace {
@@ -1301,18 +1305,40 @@ struct ProductBuffers {
     bool far, near;
 };
 
-// Launch counts of one product: total and per stage (gather, up, couple, down, leaves).
+// Launch counts of one product: total and per stage (gather, up, couple, down, near field,
+// leaves).
+constexpr int kStages = 6;
 struct ProductLaunches {
     int total = 0;
-    int stage[5] = {0, 0, 0, 0, 0};
+    int stage[kStages] = {0, 0, 0, 0, 0, 0};
 };
 
-// Enqueues the gather and the four product stages of y = alpha op(A) x + beta y on stream s.
-// x, y are device arrays (ldx, ldy leading dimensions); stage_ev (nullable) receives six events
-// that bracket the stages.
+// Stage events of one product (profiling): the gather, the three far-field sweeps on the sweep
+// stream, the near field and the leaf stage on the product stream.
+enum StageEvent { EV_START, EV_GATHER, EV_UP, EV_COUPLE, EV_DOWN, EV_NEAR0, EV_NEAR1, EV_LEAVES0, EV_END, EV_COUNT };
+
+// Second stream of a product: with aux set, the far-field sweeps (upward, coupling, downward)
+// run on aux while the near field streams on the product stream; fork and join order them.
+struct ProductStreams {
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+// Enqueues the gather and the product stages of y = alpha op(A) x + beta y on stream s. x, y are
+// device arrays (ldx, ldy leading dimensions); stage_ev (nullable) receives EV_COUNT events.
+//
+// Serial form (no aux stream): per 16-column pass, upward sweep, coupling, downward sweep and one
+// leaf launch y_t = alpha (X_t yhat_t + sum_s N_ts x_s) + beta y_t.
+// Overlapped form (aux stream, far and near parts): the near field depends on the gathered x
+// alone, so it runs beside the sweeps: y_t = alpha sum_s N_ts x_s + beta y_t on s while aux runs
+// the sweeps; after the join a leaf-basis launch adds alpha X_t yhat_t. The near field is the
+// bandwidth-bound bulk of the product and the sweeps are chains of small launches per tree
+// level, so the sweeps' latency hides under the near field's streaming. Results differ from the
+// serial form only in the rounding of the final sum.
 int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int64_t lx, double2 *yd,
                     int64_t ly, int b, double2 alpha, double2 beta, const ProductBuffers &buf,
-                    cudaStream_t s, cudaEvent_t *stage_ev, ProductLaunches &count) {
+                    cudaStream_t s, cudaEvent_t *stage_ev, ProductLaunches &count,
+                    const ProductStreams &ps = ProductStreams{}) {
     const int in = mode == 0 ? 1 : 0, out = 1 - in;
     const int64_t nin = c->side[in].npts;
     DevSide &I = c->side[in], &O = c->side[out];
@@ -1321,14 +1347,19 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
     const int cap = rows_capacity(std::min(b, 16));
     if (O.leafcap > cap || I.leafcap > cap || 2 * c->maxrank > cap)
         return fail(NCA_ERR_ARG, "a leaf or transfer block has more rows than one product CTA holds");
-    auto mark = [&](int k) {
-        if (stage_ev) CK(cudaEventRecord(stage_ev[k], s));
+    const bool overlap = ps.aux != nullptr && buf.far && buf.near;
+    auto mark = [&](int k, cudaStream_t st) {
+        if (stage_ev) CK(cudaEventRecord(stage_ev[k], st));
     };
-    mark(0);
+    mark(EV_START, s);
     k_gather<<<launch_grid(nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, I.perm.p, nin, b, vs, buf.xt);
     ++count.total;
     ++count.stage[0];
-    mark(1);
+    mark(EV_GATHER, s);
+    if (overlap) {
+        CK(cudaEventRecord(ps.fork, s));
+        CK(cudaStreamWaitEvent(ps.aux, ps.fork, 0));
+    }
     const bool conj = mode == 2;
     auto run = [&](auto tag) {
         using S = decltype(tag);
@@ -1343,40 +1374,38 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
             Cm = f64 ? (const S *)c->CT.p : (const S *)c->CT32.p;
             Nm = f64 ? (const S *)c->NT.p : (const S *)c->NT32.p;
         }
-        for (int q0 = 0; q0 < b; q0 += 16) {
-            const int bc = std::min(16, b - q0);
-            if (buf.far) {
-                // upward sweep: xhat_p = XT_p [leaf x slice | children's xhat], deepest level first
-                for (size_t l = 0; l + 1 < I.up.ptr.size(); ++l) {
-                    const int cnt = I.up.ptr[l + 1] - I.up.ptr[l];
-                    if (!cnt) continue;
-                    RowArgs<S> a{};
-                    a.stage = STAGE_UP;
-                    a.begin = I.begin.p;
-                    a.firstchild = I.firstchild.p;
-                    a.nchildren = I.nchildren.p;
-                    a.rank = I.rank.p;
-                    a.nrows = I.nrows.p;
-                    a.cptr = I.cptr.p;
-                    a.M = XTi;
-                    a.moff = I.xoff.p;
-                    a.src = buf.xt;
-                    a.coef = buf.xhat;
-                    a.b = b;
-                    a.bc = bc;
-                    a.q0 = q0;
-                    a.vs = vs;
-                    a.conj = conj && in == 0;
-                    a.maxrows = I.up.mcap[l];
-                    a.error = buf.error;
-                    launch_rows<S>(a, I.up.d_nodes.p + I.up.ptr[l], cnt, s);
-                    ++count.total;
-                    ++count.stage[1];
-                }
+        // far-field sweeps of one 16-column pass on stream st
+        auto sweeps = [&](int q0, int bc, cudaStream_t st, bool first) {
+            // upward sweep: xhat_p = XT_p [leaf x slice | children's xhat], deepest level first
+            for (size_t l = 0; l + 1 < I.up.ptr.size(); ++l) {
+                const int cnt = I.up.ptr[l + 1] - I.up.ptr[l];
+                if (!cnt) continue;
+                RowArgs<S> a{};
+                a.stage = STAGE_UP;
+                a.begin = I.begin.p;
+                a.firstchild = I.firstchild.p;
+                a.nchildren = I.nchildren.p;
+                a.rank = I.rank.p;
+                a.nrows = I.nrows.p;
+                a.cptr = I.cptr.p;
+                a.M = XTi;
+                a.moff = I.xoff.p;
+                a.src = buf.xt;
+                a.coef = buf.xhat;
+                a.b = b;
+                a.bc = bc;
+                a.q0 = q0;
+                a.vs = vs;
+                a.conj = conj && in == 0;
+                a.maxrows = I.up.mcap[l];
+                a.error = buf.error;
+                launch_rows<S>(a, I.up.d_nodes.p + I.up.ptr[l], cnt, st);
+                ++count.total;
+                ++count.stage[1];
             }
-            if (q0 == 0) mark(2);
+            if (first) mark(EV_UP, st);
             const int ncp = mode == 0 ? c->n_couple_fwd : c->n_couple_rev;
-            if (buf.far && ncp > 0) {
+            if (ncp > 0) {
                 RowArgs<S> a{};
                 a.stage = STAGE_COUPLE;
                 a.M = Cm;
@@ -1402,39 +1431,40 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
                 a.conj = conj;
                 a.maxrows = c->maxrank;
                 a.error = buf.error;
-                launch_rows<S>(a, mode == 0 ? c->couple_fwd.p : c->couple_rev.p, ncp, s);
+                launch_rows<S>(a, mode == 0 ? c->couple_fwd.p : c->couple_rev.p, ncp, st);
                 ++count.total;
                 ++count.stage[2];
             }
-            if (q0 == 0) mark(3);
-            if (buf.far) {
-                // downward sweep: [yhat_children] += X_p yhat_p, root level first
-                for (size_t l = 0; l + 1 < O.down.ptr.size(); ++l) {
-                    const int cnt = O.down.ptr[l + 1] - O.down.ptr[l];
-                    if (!cnt) continue;
-                    RowArgs<S> a{};
-                    a.stage = STAGE_DOWN;
-                    a.firstchild = O.firstchild.p;
-                    a.rank = O.rank.p;
-                    a.nrows = O.nrows.p;
-                    a.cptr = O.cptr.p;
-                    a.M = Xo;
-                    a.moff = O.xoff.p;
-                    a.coef = buf.yhat;
-                    a.b = b;
-                    a.bc = bc;
-                    a.q0 = q0;
-                    a.vs = vs;
-                    a.conj = conj && out == 1;
-                    a.maxrows = O.down.mcap[l];
-                    a.error = buf.error;
-                    launch_rows<S>(a, O.down.d_nodes.p + O.down.ptr[l], cnt, s);
-                    ++count.total;
-                    ++count.stage[3];
-                }
+            if (first) mark(EV_COUPLE, st);
+            // downward sweep: [yhat_children] += X_p yhat_p, root level first
+            for (size_t l = 0; l + 1 < O.down.ptr.size(); ++l) {
+                const int cnt = O.down.ptr[l + 1] - O.down.ptr[l];
+                if (!cnt) continue;
+                RowArgs<S> a{};
+                a.stage = STAGE_DOWN;
+                a.firstchild = O.firstchild.p;
+                a.rank = O.rank.p;
+                a.nrows = O.nrows.p;
+                a.cptr = O.cptr.p;
+                a.M = Xo;
+                a.moff = O.xoff.p;
+                a.coef = buf.yhat;
+                a.b = b;
+                a.bc = bc;
+                a.q0 = q0;
+                a.vs = vs;
+                a.conj = conj && out == 1;
+                a.maxrows = O.down.mcap[l];
+                a.error = buf.error;
+                launch_rows<S>(a, O.down.d_nodes.p + O.down.ptr[l], cnt, st);
+                ++count.total;
+                ++count.stage[3];
             }
-            if (q0 == 0) mark(4);
-            // leaves: y_t = X_t yhat_t + sum_s N_ts x_s, scattered into y
+            if (first) mark(EV_DOWN, st);
+        };
+        // leaf stage of one pass: y_t = al (X_t yhat_t [with_basis] + sum_s N_ts x_s [with_near]) + be y_t
+        auto leaves = [&](int q0, int bc, bool with_basis, bool with_near, double2 al, double2 be, bool ube,
+                          int stage) {
             RowArgs<S> a{};
             a.stage = STAGE_LEAVES;
             a.begin = O.begin.p;
@@ -1442,10 +1472,10 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
             a.perm = O.perm.p;
             a.rank = O.rank.p;
             a.cptr = O.cptr.p;
-            a.X = buf.far ? Xo : nullptr;
+            a.X = with_basis ? Xo : nullptr;
             a.xoff = O.xoff.p;
             a.coef = buf.yhat;
-            if (buf.near) {
+            if (with_near) {
                 a.M = Nm;
                 a.moff = mode == 0 ? c->nfoff.p : c->ntoff.p;
                 a.ptr = mode == 0 ? c->nearptr.p : c->tnearptr.p;
@@ -1456,9 +1486,9 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
             a.src = buf.xt;
             a.y = yd;
             a.ldy = ly;
-            a.alpha = alpha;
-            a.beta = beta;
-            a.usebeta = usebeta;
+            a.alpha = al;
+            a.beta = be;
+            a.usebeta = ube;
             a.b = b;
             a.bc = bc;
             a.q0 = q0;
@@ -1468,9 +1498,37 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
             a.error = buf.error;
             launch_rows<S>(a, O.leaves.p, O.nleaves, s);
             ++count.total;
-            ++count.stage[4];
+            ++count.stage[stage];
+        };
+        if (overlap) {
+            for (int q0 = 0; q0 < b; q0 += 16) sweeps(q0, std::min(16, b - q0), ps.aux, q0 == 0);
+            CK(cudaEventRecord(ps.join, ps.aux));
+            mark(EV_NEAR0, s);
+            for (int q0 = 0; q0 < b; q0 += 16) leaves(q0, std::min(16, b - q0), false, true, alpha, beta, usebeta, 4);
+            mark(EV_NEAR1, s);
+            CK(cudaStreamWaitEvent(s, ps.join, 0));
+            mark(EV_LEAVES0, s);
+            // y_t += alpha X_t yhat_t
+            for (int q0 = 0; q0 < b; q0 += 16)
+                leaves(q0, std::min(16, b - q0), true, false, alpha, make_double2(1.0, 0.0), true, 5);
+        } else {
+            for (int q0 = 0; q0 < b; q0 += 16) {
+                const int bc = std::min(16, b - q0);
+                if (buf.far) sweeps(q0, bc, s, q0 == 0);
+                if (q0 == 0) {
+                    if (!buf.far) {
+                        mark(EV_UP, s);
+                        mark(EV_COUPLE, s);
+                        mark(EV_DOWN, s);
+                    }
+                    mark(EV_NEAR0, s);
+                    mark(EV_NEAR1, s);
+                    mark(EV_LEAVES0, s);
+                }
+                leaves(q0, bc, buf.far, buf.near, alpha, beta, usebeta, 5);
+            }
         }
-        mark(5);
+        mark(EV_END, s);
     };
     if (precision == NCA_PREC_F64)
         run(double2{});
@@ -1770,13 +1828,18 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
                                          s, count))
             return st;
         if (ws->profiling)
-            for (int k = 1; k < 6; ++k) CK(cudaEventRecord(ws->stage_ev[k], s));
+            for (int k = 1; k < EV_COUNT; ++k) CK(cudaEventRecord(ws->stage_ev[k], s));
     } else if (tangent) {
         if (int st = enqueue_tangent(c, xd, lx, yd, ly, b, alpha, beta, buf, ws->dxhat.p, ws->dyhat.p, s, count))
             return st;
-    } else if (int st = enqueue_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, buf, s,
-                                        ws->profiling ? ws->stage_ev : nullptr, count)) {
-        return st;
+    } else {
+        ProductStreams ps;
+        ps.aux = ws->aux;
+        ps.fork = ws->fork;
+        ps.join = ws->join;
+        if (int st = enqueue_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, buf, s,
+                                     ws->profiling ? ws->stage_ev : nullptr, count, ps))
+            return st;
     }
     CK(cudaMemcpyAsync(ws->error_host, ws->error.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     if (memspace == 0)
@@ -1789,9 +1852,13 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     ws->last_seconds = ms * 1e-3;
     ws->last_launches = count.total;
     if (ws->profiling && !tangent) {
-        for (int k = 0; k < 5; ++k) {
+        // gather, up, couple, down, near field, leaves (the sweeps and the near field overlap
+        // when the workspace has its sweep stream)
+        static const int from[kStages] = {EV_START, EV_GATHER, EV_UP, EV_COUPLE, EV_NEAR0, EV_LEAVES0};
+        static const int to[kStages] = {EV_GATHER, EV_UP, EV_COUPLE, EV_DOWN, EV_NEAR1, EV_END};
+        for (int k = 0; k < kStages; ++k) {
             float t = 0.f;
-            CK(cudaEventElapsedTime(&t, ws->stage_ev[k], ws->stage_ev[k + 1]));
+            CK(cudaEventElapsedTime(&t, ws->stage_ev[from[k]], ws->stage_ev[to[k]]));
             ws->stage_seconds[k] = t * 1e-3;
             ws->stage_launches[k] = count.stage[k];
         }
@@ -2673,6 +2740,13 @@ int32_t nca_workspace_create(nca_core *core, int32_t max_nrhs, nca_workspace **o
         CK(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
         CK(cudaEventCreate(&ws->e0));
         CK(cudaEventCreate(&ws->e1));
+        if (!core->dir) {
+            int least = 0, greatest = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+            CK(cudaStreamCreateWithPriority(&ws->aux, cudaStreamNonBlocking, greatest));
+            CK(cudaEventCreateWithFlags(&ws->fork, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ws->join, cudaEventDisableTiming));
+        }
         int b = std::max(1, max_nrhs);
         if (!core->dir) {
             ws->xt.alloc(size_t(std::max(core->side[0].npts, core->side[1].npts)) * vector_slots(b));
@@ -2691,6 +2765,9 @@ void nca_workspace_destroy(nca_workspace *ws) {
     if (!ws) return;
     cudaSetDevice(ws->core->device);
     if (ws->stream) cudaStreamDestroy(ws->stream);
+    if (ws->aux) cudaStreamDestroy(ws->aux);
+    if (ws->fork) cudaEventDestroy(ws->fork);
+    if (ws->join) cudaEventDestroy(ws->join);
     if (ws->e0) cudaEventDestroy(ws->e0);
     if (ws->e1) cudaEventDestroy(ws->e1);
     for (cudaEvent_t &e : ws->stage_ev)
@@ -2770,7 +2847,7 @@ int32_t nca_workspace_set_profiling(nca_workspace *ws, int32_t on) {
 
 int32_t nca_workspace_stage_times(const nca_workspace *ws, double *seconds, int32_t *launches, int32_t nstages) {
     if (!ws || nstages < 0) return fail(NCA_ERR_ARG, "bad argument");
-    for (int k = 0; k < std::min(nstages, 5); ++k) {
+    for (int k = 0; k < std::min(nstages, kStages); ++k) {
         if (seconds) seconds[k] = ws->stage_seconds[k];
         if (launches) launches[k] = ws->stage_launches[k];
     }

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <functional>
 #include <stdexcept>
 #include <thread>
 
@@ -323,7 +324,17 @@ void all_item_farpivots(const Tree &own, const Tree &far, const DirSide &D, cons
     const int ni = int(D.item_node.size());
     std::vector<int32_t> count(ni, 0);
     std::vector<int32_t> buf(size_t(ni) * std::max(maxrank, 1));
+    // every direction of a cluster shares its centroid: computed once per cluster
+    std::vector<double> centroid(3 * size_t(own.nnodes));
     std::atomic<int> cursor{0};
+    auto cwork = [&]() {
+        for (;;) {
+            const int t = cursor.fetch_add(1);
+            if (t >= own.nnodes) break;
+            if (own.size(t) > 0)
+                cluster_centroid(ownpts, own.perm.data() + own.begin[t], own.size(t), &centroid[3 * size_t(t)]);
+        }
+    };
     auto work = [&]() {
         std::vector<int32_t> ff;
         for (;;) {
@@ -332,15 +343,20 @@ void all_item_farpivots(const Tree &own, const Tree &far, const DirSide &D, cons
             item_farfield(own, D, item, ff);
             if (ff.empty()) continue;
             const int t = D.item_node[item];
-            count[item] = select_farpivots(far, ownpts, farpts, own.perm.data() + own.begin[t], own.size(t), ff.data(),
-                                           int(ff.size()), maxrank, buf.data() + size_t(item) * maxrank);
+            count[item] = select_farpivots_at(far, farpts, &centroid[3 * size_t(t)], own.size(t), ff.data(),
+                                              int(ff.size()), maxrank, buf.data() + size_t(item) * maxrank);
         }
     };
     const int nth = std::max(1, std::min(host_threads(), ni));
-    std::vector<std::thread> pool;
-    for (int i = 1; i < nth; ++i) pool.emplace_back(work);
-    work();
-    for (auto &th : pool) th.join();
+    auto run = [&](const std::function<void()> &job) {
+        cursor = 0;
+        std::vector<std::thread> pool;
+        for (int i = 1; i < nth; ++i) pool.emplace_back(job);
+        job();
+        for (auto &th : pool) th.join();
+    };
+    run(cwork);
+    run(work);
     fpptr.assign(ni + 1, 0);
     for (int i = 0; i < ni; ++i) fpptr[i + 1] = fpptr[i] + count[i];
     fpidx.resize(fpptr[ni]);

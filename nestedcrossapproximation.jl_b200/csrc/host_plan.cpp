@@ -368,23 +368,32 @@ class Mimicry {
 
 }  // namespace
 
-int select_farpivots(const Tree &far, const double *ownpts, const double *farpts,
-                     const int32_t *refidcs, int nref, const int32_t *farnodes, int nfar,
-                     int maxrank, int32_t *out) {
+void cluster_centroid(const double *ownpts, const int32_t *refidcs, int nref, double *c) {
+    double s[3] = {0, 0, 0};
+    for (int i = 0; i < nref; ++i)
+        for (int d = 0; d < 3; ++d) s[d] += ownpts[3 * int64_t(refidcs[i]) + d];
+    for (int d = 0; d < 3; ++d) c[d] = s[d] / nref;
+}
+
+int select_farpivots_at(const Tree &far, const double *farpts, const double *centroid, int nref,
+                        const int32_t *farnodes, int nfar, int maxrank, int32_t *out) {
     int limit = std::min(maxrank, nref);
     int n = 0;
     for (int i = 0; i < nfar && limit - n > 0; ++i) {
         n += std::min(limit - n, far.size(farnodes[i]));
     }
     if (n <= 0) return 0;
-    double s[3] = {0, 0, 0};
-    for (int i = 0; i < nref; ++i)
-        for (int d = 0; d < 3; ++d) s[d] += ownpts[3 * int64_t(refidcs[i]) + d];
-    double c[3];
-    for (int d = 0; d < 3; ++d) c[d] = s[d] / nref;
-    Mimicry M(far, farpts, c, farnodes, nfar, n);
+    Mimicry M(far, farpts, centroid, farnodes, nfar, n);
     for (int p = 0; p < n; ++p) out[p] = M.next();
     return n;
+}
+
+int select_farpivots(const Tree &far, const double *ownpts, const double *farpts,
+                     const int32_t *refidcs, int nref, const int32_t *farnodes, int nfar,
+                     int maxrank, int32_t *out) {
+    double c[3];
+    cluster_centroid(ownpts, refidcs, nref, c);
+    return select_farpivots_at(far, farpts, c, nref, farnodes, nfar, maxrank, out);
 }
 
 int host_threads() {

@@ -37,6 +37,11 @@ struct Partition {
 Partition build_partition(const Tree &test, const Tree &trial, double eta);
 
 // Phase 1 of the batched compressor for one cluster (tree mimicry on the far tree).
+// centroid of the reference points (sequential sums in index order, then one division each)
+void cluster_centroid(const double *ownpts, const int32_t *refidcs, int nref, double *c);
+// select_farpivots with the centroid of the nref reference points given
+int select_farpivots_at(const Tree &far, const double *farpts, const double *centroid, int nref,
+                        const int32_t *farnodes, int nfar, int maxrank, int32_t *out);
 int select_farpivots(const Tree &far, const double *ownpts, const double *farpts,
                      const int32_t *refidcs, int nref, const int32_t *farnodes, int nfar,
                      int maxrank, int32_t *out);

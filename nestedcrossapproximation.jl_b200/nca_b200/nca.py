@@ -365,11 +365,13 @@ class H2Workspace(LinearMap):
 
     def stage_times(self):
         """Device seconds and launches of the last product per stage: gather, upward sweep,
-        coupling, downward sweep, leaves + near field."""
-        t = (C.c_double * 5)()
-        n = (C.c_int32 * 5)()
-        check(lib().nca_workspace_stage_times(self._h, t, n, 5))
-        names = ("gather", "upward", "coupling", "downward", "leaves")
+        coupling, downward sweep, near field, leaves. The workspace runs the sweeps on a second
+        stream beside the near field (both parts present), then adds the leaf bases ("leaves");
+        otherwise the near field is part of the leaf launches and "near" is empty."""
+        t = (C.c_double * 6)()
+        n = (C.c_int32 * 6)()
+        check(lib().nca_workspace_stage_times(self._h, t, n, 6))
+        names = ("gather", "upward", "coupling", "downward", "near", "leaves")
         return {k: (t[i], n[i]) for i, k in enumerate(names)}
 
     def launches(self):

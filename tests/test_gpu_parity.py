@@ -252,3 +252,32 @@ def test_f32_product(c1):
     ref = H.apply(X, 0)
     assert relerr(W @ X, ref) < 1e-5
     assert relerr(W.H @ X, H.apply(X, 2)) < 1e-5
+
+
+def test_parts_and_overlapped_stages(c1):
+    """The workspace runs the far-field sweeps on its second stream beside the near field and adds
+    the leaf bases after the join; far-only and near-only workspaces run the serial leaf launch.
+    far + near = whole product, and each part against the oracle's own split."""
+    test, trial, A, H = c1
+    N = _n()
+    X = cgauss((1024, 37), 70)  # three 16-column passes
+    whole = A @ X
+    far, near = N.farmatrix(A), N.nearmatrix(A)
+    assert relerr(far @ X + near @ X, whole) < REL
+    assert relerr(whole, H.apply(X, 0)) < REL
+    y0 = cgauss((1024, 37), 71)
+    y = y0.copy()
+    N.mul(y, N.adjoint(A), X, 0.5 - 0.25j, 2.0)
+    assert relerr(y, (0.5 - 0.25j) * H.apply(X, 2) + 2.0 * y0) < REL
+    A.set_profiling(True)
+    try:
+        A @ X[:, :16]
+        st = A.stage_times()
+        assert st["near"][1] == 1 and st["leaves"][1] == 1 and st["coupling"][1] == 1
+        assert all(t >= 0 for t, _ in st.values())
+        far.set_profiling(True)
+        far @ X[:, :16]
+        sf = far.stage_times()
+        assert sf["near"][1] == 0 and sf["leaves"][1] == 1
+    finally:
+        A.set_profiling(False)
