@@ -4,7 +4,7 @@
 
 nvcc cross-compiles for sm_100a without a GPU. The host planner is compiled with
 -ffp-contract=off (its arithmetic is reproduced bit for bit elsewhere); build_kernels.cu with
---fmad=false (the pivot search spells out every fused multiply-add).
+--fmad=false (the pivot search and the tree mimicry spell out every fused multiply-add).
 """
 from __future__ import annotations
 
@@ -30,6 +30,7 @@ UNITS = [
     ("host_plan.cpp", "cxx", []),
     ("directional.cpp", "cxx", []),
     ("build_kernels.cu", "nvcc", ["--fmad=false"]),
+    ("mimicry.cu", "nvcc", ["--fmad=false"]),
     ("apply_kernels.cu", "nvcc", []),
     ("capi.cu", "nvcc", []),
 ]

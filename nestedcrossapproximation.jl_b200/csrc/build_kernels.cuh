@@ -89,4 +89,25 @@ __global__ void k_entries(KernelParams K, const double *tp, const double *sp, co
                           const int64_t *jj, int64_t n, double2 *out);
 __global__ void k_to_f32(const double2 *in, float2 *out, int64_t n);
 
+// Phase-1 far pivots (tree mimicry) of many items, one warp each (mimicry.cu). Item i belongs to
+// own-side cluster item_node[i] (null: cluster i), whose centroid and point count are given; its
+// far field is ffnodes[ffptr[i] .. ffptr[i + 1]) (far-tree node ids, in the reference's farfield
+// order). Writes count[i] pivots (far point ids) to piv[i * maxrank ..].
+struct MimicryArgs {
+    const int32_t *begin, *end, *firstchild, *nchildren, *perm;  // far tree
+    const double *center;                                         // far node centres, 3 each
+    const double *pts;                                            // far points by id, 3 each
+    int nitems;
+    const int64_t *ffptr;
+    const int32_t *ffnodes;
+    const int32_t *item_node;
+    const double *centroid;   // own clusters, 3 each
+    const int32_t *own_size;  // own clusters' point counts
+    int maxrank;
+    int32_t *count, *piv;
+    int32_t *error;  // 1: an item ran out of candidates before its pivot count
+};
+size_t mimicry_smem_bytes(int maxrank);
+void launch_mimicry(const MimicryArgs &a, cudaStream_t s);
+
 }  // namespace nca

@@ -15,6 +15,7 @@
 #include <unordered_map>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "apply_kernels.cuh"
@@ -277,6 +278,110 @@ void upload_tree(DevSide &d, const nca::Tree &T, const double *pts, cudaStream_t
     d.end.upload(T.end, s);
     d.firstchild.upload(T.firstchild, s);
     d.nchildren.upload(T.nchildren, s);
+}
+
+// CSR of n lists filled by fill(i, list) on the host's worker threads (contiguous item ranges
+// per thread, concatenated in item order).
+template <typename F>
+void parallel_csr(int n, F fill, std::vector<int64_t> &ptr, std::vector<int32_t> &idx) {
+    const int nth = std::max(1, std::min(nca::host_threads(), std::max(n, 1)));
+    std::vector<std::vector<int64_t>> lptr(nth);
+    std::vector<std::vector<int32_t>> lidx(nth);
+    auto work = [&](int w) {
+        const int i0 = int(int64_t(n) * w / nth), i1 = int(int64_t(n) * (w + 1) / nth);
+        std::vector<int32_t> one;
+        lptr[w].assign(1, 0);
+        for (int i = i0; i < i1; ++i) {
+            fill(i, one);
+            lidx[w].insert(lidx[w].end(), one.begin(), one.end());
+            lptr[w].push_back(int64_t(lidx[w].size()));
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < nth; ++w) pool.emplace_back(work, w);
+    work(0);
+    for (auto &th : pool) th.join();
+    ptr.assign(1, 0);
+    idx.clear();
+    for (int w = 0; w < nth; ++w) {
+        const int64_t off = int64_t(idx.size());
+        for (size_t k = 1; k < lptr[w].size(); ++k) ptr.push_back(lptr[w][k] + off);
+        idx.insert(idx.end(), lidx[w].begin(), lidx[w].end());
+    }
+}
+
+// Phase 1 on the device: tree-mimicry far pivots of every item of one side (item i is own
+// cluster item_node[i], or cluster i when item_node is null), with far field ffnodes[ffptr[i]..)
+// in the reference's farfield order. Returns the CSR of pivots (far point ids).
+void device_farpivots(const nca::Tree &own, const double *ownpts, const nca::Tree &far, const DevSide &fd,
+                      int nitems, const std::vector<int64_t> &ffptr, const std::vector<int32_t> &ffnodes,
+                      const std::vector<int32_t> *item_node, int maxrank, cudaStream_t s,
+                      std::vector<int32_t> &fpptr, std::vector<int32_t> &fpidx) {
+    fpptr.assign(nitems + 1, 0);
+    fpidx.clear();
+    if (nitems == 0) return;
+    // centroids of the own clusters (the host planner's sums, in its order)
+    std::vector<double> centroid(3 * size_t(own.nnodes), 0.0);
+    std::vector<int32_t> own_size(own.nnodes);
+    for (int t = 0; t < own.nnodes; ++t) own_size[t] = own.size(t);
+    {
+        std::atomic<int> cursor{0};
+        auto work = [&]() {
+            for (;;) {
+                const int t = cursor.fetch_add(1);
+                if (t >= own.nnodes) break;
+                if (own.size(t) > 0)
+                    nca::cluster_centroid(ownpts, own.perm.data() + own.begin[t], own.size(t), &centroid[3 * size_t(t)]);
+            }
+        };
+        const int nth = std::max(1, std::min(nca::host_threads(), own.nnodes));
+        std::vector<std::thread> pool;
+        for (int i = 1; i < nth; ++i) pool.emplace_back(work);
+        work();
+        for (auto &th : pool) th.join();
+    }
+    DBuf<int64_t> dptr;
+    DBuf<int32_t> dnodes, ditem, dsize, dcount, dpiv, derr;
+    DBuf<double> dcent, dcenter;
+    dptr.upload(ffptr, s);
+    dnodes.upload(ffnodes, s);
+    if (item_node) ditem.upload(*item_node, s);
+    dsize.upload(own_size, s);
+    dcent.upload(centroid, s);
+    dcenter.upload(far.center, s);
+    dcount.alloc(nitems);
+    dpiv.alloc(size_t(nitems) * maxrank);
+    derr.alloc(1);
+    derr.zero(s);
+    MimicryArgs a{};
+    a.begin = fd.begin.p;
+    a.end = fd.end.p;
+    a.firstchild = fd.firstchild.p;
+    a.nchildren = fd.nchildren.p;
+    a.perm = fd.perm.p;
+    a.center = dcenter.p;
+    a.pts = fd.pts.p;
+    a.nitems = nitems;
+    a.ffptr = dptr.p;
+    a.ffnodes = dnodes.p;
+    a.item_node = item_node ? ditem.p : nullptr;
+    a.centroid = dcent.p;
+    a.own_size = dsize.p;
+    a.maxrank = maxrank;
+    a.count = dcount.p;
+    a.piv = dpiv.p;
+    a.error = derr.p;
+    launch_mimicry(a, s);
+    CK(cudaGetLastError());
+    const std::vector<int32_t> count = dcount.download(s);
+    const std::vector<int32_t> piv = dpiv.download(s);
+    const std::vector<int32_t> err = derr.download(s);
+    if (err[0] != 0) throw Failure(NCA_ERR_CUDA, "internal: tree mimicry ran out of far points");
+    for (int i = 0; i < nitems; ++i) fpptr[i + 1] = fpptr[i] + count[i];
+    fpidx.resize(fpptr[nitems]);
+    for (int i = 0; i < nitems; ++i)
+        std::copy(piv.begin() + size_t(i) * maxrank, piv.begin() + size_t(i) * maxrank + count[i],
+                  fpidx.begin() + fpptr[i]);
 }
 
 // Rows/rank bounds per node (bottom-up), X slot offsets and per-level active node lists.
@@ -558,11 +663,24 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
     upload_tree(c->side[0], c->tree[0], tp, s);
     upload_tree(c->side[1], c->tree[1], sp, s);
     const nca::Partition &P = c->part;
-    // phase 1 on the host (tree mimicry); far field = own far nodes + ancestors'
-    all_farpivots(c->tree[0], c->tree[1], tp, sp, P.farptr, P.farnodes, maxrank, c->side[0].h_fpptr,
-                  c->side[0].h_fpidx);
-    all_farpivots(c->tree[1], c->tree[0], sp, tp, P.tfarptr, P.tfarnodes, maxrank, c->side[1].h_fpptr,
-                  c->side[1].h_fpidx);
+    // phase 1 on the device (tree mimicry); far field = own far nodes + ancestors'
+    for (int sd = 0; sd < 2; ++sd) {
+        const nca::Tree &T = c->tree[sd];
+        const std::vector<int32_t> &ptr = sd == 0 ? P.farptr : P.tfarptr;
+        const std::vector<int32_t> &nodes = sd == 0 ? P.farnodes : P.tfarnodes;
+        std::vector<int64_t> ffptr;
+        std::vector<int32_t> ffnodes;
+        parallel_csr(
+            T.nnodes,
+            [&](int t, std::vector<int32_t> &ff) {
+                ff.clear();
+                for (int a = t; a >= 0; a = T.parent[a])
+                    ff.insert(ff.end(), nodes.begin() + ptr[a], nodes.begin() + ptr[a + 1]);
+            },
+            ffptr, ffnodes);
+        device_farpivots(T, sd == 0 ? tp : sp, c->tree[1 - sd], c->side[1 - sd], T.nnodes, ffptr, ffnodes, nullptr,
+                         maxrank, s, c->side[sd].h_fpptr, c->side[sd].h_fpidx);
+    }
     auto h1 = std::chrono::steady_clock::now();
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
@@ -873,7 +991,15 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         DirItems &d = D->side[sd];
         d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
                                   sd == 0 ? P.farnodes : P.tfarnodes, wb);
-        all_item_farpivots(c->tree[sd], c->tree[1 - sd], d.plan, pts[sd], pts[1 - sd], maxrank, d.h_fpptr, d.h_fpidx);
+        // phase 1 on the device: tree mimicry per item over the item's directional far field
+        std::vector<int64_t> ffptr;
+        std::vector<int32_t> ffnodes;
+        const int ni = int(d.plan.item_node.size());
+        parallel_csr(
+            ni, [&](int it, std::vector<int32_t> &ff) { nca::item_farfield(c->tree[sd], d.plan, it, ff); }, ffptr,
+            ffnodes);
+        device_farpivots(c->tree[sd], pts[sd], c->tree[1 - sd], c->side[1 - sd], ni, ffptr, ffnodes,
+                         &d.plan.item_node, maxrank, s, d.h_fpptr, d.h_fpidx);
     }
     auto h1 = std::chrono::steady_clock::now();
     cudaEvent_t ev0, ev1;
