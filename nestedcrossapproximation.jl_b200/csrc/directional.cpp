@@ -149,9 +149,9 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
     std::vector<int32_t> pcount(nn, 0);
     std::vector<char> lf(nn);
     for (int node = 0; node < nn; ++node) lf[node] = is_lowfrequency(T, node, w);
-    std::vector<double> total;
-    for (int level = 0; level < T.nlevels; ++level) {
-        for (int node = T.levelptr[level]; node < T.levelptr[level + 1]; ++node) {
+    // the nodes of one level depend on their parents only: a level's nodes run on the host
+    // threads, each writing its own entries (and its own range of the far-node list)
+    auto plan_node = [&](int level, int node, std::vector<double> &total) {
             const int p = T.parent[node];
             const bool hasfars = farptr[node + 1] > farptr[node];
             const bool hasparentvecs = p >= 0 && hasvec[p];
@@ -160,9 +160,9 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
                 const bool inherit = hasparentdirs && level > 0 && lf[p];
                 if (hasfars || inherit) dirs[node] = {0};
                 if (inherit) pmap[node] = {1};
-                continue;
+                return;
             }
-            if (!hasfars && !hasparentvecs) continue;
+            if (!hasfars && !hasparentvecs) return;
             candidate_directions(2.0 * T.radius[node], w.k, w.gamma, total);
             const int b = farptr[node], nfar = farptr[node + 1] - b;
             std::vector<int32_t> nd(nfar);
@@ -222,7 +222,24 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
             pmap[node] = map;
             dirs[node] = uniq;
             dircount[node] = count;
-        }
+    };
+    const int nth = host_threads();
+    for (int level = 0; level < T.nlevels; ++level) {
+        const int n0 = T.levelptr[level], n1 = T.levelptr[level + 1];
+        std::atomic<int> cursor{n0};
+        auto work = [&]() {
+            std::vector<double> total;
+            for (;;) {
+                const int node = cursor.fetch_add(1);
+                if (node >= n1) break;
+                plan_node(level, node, total);
+            }
+        };
+        const int use = std::max(1, std::min(nth, n1 - n0));
+        std::vector<std::thread> pool;
+        for (int i = 1; i < use; ++i) pool.emplace_back(work);
+        work();
+        for (auto &th : pool) th.join();
     }
     for (int node = 0; node < nn; ++node)
         if (!dirs[node].empty() && dircount[node].empty()) {
