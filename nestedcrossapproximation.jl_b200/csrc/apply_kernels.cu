@@ -205,6 +205,15 @@ __device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.
 // groups are summed at the end.
 struct TileMap {
     int kgroups, mykg, rt0, nrt;
+    int step = NCONS;  // row tiles between a warp's successive tiles
+    // one warp holding every tile of an R-row output (row tiles 0, 1, ...)
+    __device__ void init_single(int R) {
+        kgroups = 1;
+        mykg = 0;
+        rt0 = 0;
+        nrt = (R + 7) >> 3;
+        step = 1;
+    }
     __device__ void init(int R, int warp) {
         const int MT = (R + 7) >> 3;
         const int mt1 = MT > 0 ? MT : 1;
@@ -214,7 +223,7 @@ struct TileMap {
         const bool busy = MT > 0 && (kgroups > 1 ? warp < MT * kgroups : warp < MT);
         nrt = !busy ? 0 : kgroups > 1 ? 1 : (MT - rt0 + NCONS - 1) / NCONS;
     }
-    __device__ int row(int j, int g) const { return (rt0 + j * NCONS) * 8 + g; }
+    __device__ int row(int j, int g) const { return (rt0 + j * step) * 8 + g; }
 };
 
 // One chunk (w columns, tile at smem offset 0, vectors at voff) of the consumer warp's tiles,
@@ -707,6 +716,252 @@ void launch_gather_small(const RowArgs<S> &a, const int32_t *nodes, int count, c
 
 template void launch_gather_small<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
 template void launch_gather_small<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+
+namespace {
+constexpr int TINY_WARPS = 4;       // warps (independent output streams) per CTA
+constexpr int TINY_STAGE = 9216;    // bytes of one chunk buffer; two per warp
+
+__device__ __forceinline__ void cp_async(void *dst, const double2 *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async(void *dst, const float2 *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ int pow2_at_least(int n) {
+    int p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+// Descriptors of one output of a warp's sequence: uniform fields, plus the first 32 segments'
+// block offsets, widths and vector rows spread over the lanes (lane l: segment e0 + l).
+struct TinyOut {
+    int o = -1, R = 0, e0 = 0, e1 = 0;
+    int64_t moff = 0, voff = 0;
+    int w = 0;
+};
+
+// STAGE_GATHER for many small outputs (at most 8 NRT rows, bc <= 8 NTL right-hand sides): one
+// warp per output, a warp streaming the outputs o = nodes[i] of every TINY_WARPS * gridDim.x-th i.
+// The warp's column stream (output by output, segment by segment) is cut into chunks of at most
+// wcap columns of one output; every lane issues asynchronous copies (cp.async) of its share of a
+// chunk's block columns and vector rows into one of two buffers, so that the next chunk is in
+// flight while the current one goes through the FP64 tensor-core MMA (the product kernel's
+// consume). The descriptors of the next two outputs are loaded ahead into registers, so that
+// issuing a chunk waits on no global load. Outputs are written from the accumulators when their
+// last chunk is done (no atomics, fixed order).
+template <typename S, int NRT, int NTL>
+__global__ void __launch_bounds__(TINY_WARPS * 32) k_gather_tiny(RowArgs<S> a, const int32_t *nodes, int count) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tq = lane & 3;
+    unsigned char *const wbuf = smem + 2 * warp * TINY_STAGE;  // this warp's two chunk buffers
+    const int bc = a.bc, ldv = conflict_free(bc), bcp = pow2_at_least(bc);
+    int bs = 0;
+    while (bcp >> (bs + 1)) ++bs;  // log2 of bcp
+    const int stride = gridDim.x * TINY_WARPS;
+    const double sgn = a.conj ? -1.0 : 1.0;
+    const bool scatter = a.y != nullptr;
+    constexpr int elem = int(sizeof(S));
+    // the output sequence of this warp: positions first + j * stride
+    const int first = blockIdx.x * TINY_WARPS + warp;
+    auto head = [&](int j, TinyOut &d) {  // uniform fields of output j
+        const int oi = first + j * stride;
+        d.o = -1;
+        if (oi < count) {
+            d.o = nodes[oi];
+            d.R = a.g_rows[d.o];
+            d.e0 = a.g_segptr[d.o];
+            d.e1 = a.g_segptr[d.o + 1];
+        }
+    };
+    auto segs = [&](TinyOut &d) {  // lane-spread segment fields of output d
+        if (d.o >= 0 && lane < d.e1 - d.e0) {
+            d.moff = a.g_moff[d.e0 + lane];
+            d.w = a.g_w[d.e0 + lane];
+            d.voff = a.g_voff[d.e0 + lane];
+        }
+    };
+    // layout of a chunk of an R-row output: block columns (leading dimension ldm) from offset 0,
+    // vector rows (stride ldv) from voff; wcap columns, a multiple of 4 when more than 4 fit
+    auto layout = [&](int rows, int &ldm, int &wcap, int &voff) {
+        ldm = conflict_free(rows);
+        wcap = TINY_STAGE / (ldm * elem + ldv * 16);
+        if (wcap > 4) wcap &= ~3;
+        voff = (wcap * ldm * elem + 15) & ~15;
+        while (wcap > 1 && voff + wcap * ldv * 16 > TINY_STAGE) {  // the 16-byte rounding of voff
+            --wcap;
+            voff = (wcap * ldm * elem + 15) & ~15;
+        }
+    };
+    // issuing side: output j (cur, with its segments), j + 1 (nxt, segments in flight) and j + 2
+    // (far, uniform fields in flight); position e (absolute segment), column c0 in the segment
+    int j = 0;
+    TinyOut cur, nxt, far;
+    head(0, cur);
+    segs(cur);
+    head(1, nxt);
+    segs(nxt);
+    head(2, far);
+    int e = cur.e0, c0 = 0;
+    // issues the next chunk into b; returns its output (-1: none left), rows, width, last flag
+    auto issue = [&](unsigned char *b, int &co, int &cR, int &cW, bool &clast) {
+        co = cur.o;
+        cR = cur.R;
+        cW = 0;
+        clast = false;
+        if (cur.o < 0) return;
+        const int R = cur.R;
+        int ldm, wcap, voff;
+        layout(R, ldm, wcap, voff);
+        S *Ms = reinterpret_cast<S *>(b);
+        double2 *Vs = reinterpret_cast<double2 *>(b + voff);
+        const int rp = pow2_at_least(R);
+        int rs = 0;
+        while (rp >> (rs + 1)) ++rs;  // log2 of rp
+        while (e < cur.e1 && cW < wcap) {
+            const int l = e - cur.e0;
+            int64_t mo, vo;
+            int wseg;
+            if (l < 32) {
+                mo = __shfl_sync(0xffffffffu, cur.moff, l);
+                vo = __shfl_sync(0xffffffffu, cur.voff, l);
+                wseg = __shfl_sync(0xffffffffu, cur.w, l);
+            } else {
+                mo = a.g_moff[e];
+                vo = a.g_voff[e];
+                wseg = a.g_w[e];
+            }
+            const S *M = mo >= 0 ? a.M + mo : a.M2 + (-1 - mo);
+            const int w = wseg - c0 < wcap - cW ? wseg - c0 : wcap - cW;
+            const S *msrc = M + int64_t(c0) * R;
+            for (int k = lane; k < (w << rs); k += 32) {
+                const int r = k & (rp - 1), cc = k >> rs;
+                if (r < R) cp_async(Ms + (cW + cc) * ldm + r, msrc + int64_t(cc) * R + r);
+            }
+            const double2 *vsrc = a.src + (vo + c0) * a.vs + a.q0;
+            for (int k = lane; k < (w << bs); k += 32) {
+                const int q = k & (bcp - 1), rr = k >> bs;
+                if (q < bc) cp_async(Vs + (cW + rr) * ldv + q, vsrc + int64_t(rr) * a.vs + q);
+            }
+            cW += w;
+            c0 += w;
+            if (c0 >= wseg) {
+                ++e;
+                c0 = 0;
+            }
+        }
+        if (e >= cur.e1) {
+            clast = true;
+            ++j;
+            cur = nxt;
+            nxt = far;
+            segs(nxt);
+            head(j + 2, far);
+            e = cur.e0;
+            c0 = 0;
+        }
+    };
+    Acc<NRT, NTL> acc;
+    acc.zero();
+    int co, cR, cW;
+    bool clast;
+    issue(wbuf, co, cR, cW, clast);
+    cp_async_commit();
+    for (int k = 0; co >= 0; ++k) {
+        int no, nR, nW;
+        bool nlast;
+        issue(wbuf + ((k + 1) & 1) * TINY_STAGE, no, nR, nW, nlast);
+        cp_async_commit();
+        cp_async_wait<1>();  // this lane's copies of chunk k have landed
+        __syncwarp();        // and every lane's
+        TileMap tm;
+        tm.init_single(cR);
+        int ldm, wcap, voff;
+        layout(cR, ldm, wcap, voff);
+        consume<S, NRT, NTL>(acc, tm, wbuf + (k & 1) * TINY_STAGE, cW, voff, cR, ldm, bc, ldv, g, tq, sgn);
+        if (clast) {
+            const int64_t gout = a.g_out[co];
+#pragma unroll
+            for (int jj = 0; jj < NRT; ++jj) {
+                if (jj >= tm.nrt) break;
+                const int i = tm.row(jj, g);
+                if (i >= cR) continue;
+#pragma unroll
+                for (int t = 0; t < NTL; ++t)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int qq = t * 8 + 2 * tq + h;
+                        if (qq >= bc) continue;
+                        double2 v = acc.value(jj * NTL + t, h, sgn);
+                        const int col = a.q0 + qq;
+                        if (scatter) {
+                            double2 *yp = a.y + a.perm[gout + i] + int64_t(col) * a.ldy;
+                            double2 out = make_double2(a.alpha.x * v.x - a.alpha.y * v.y,
+                                                       a.alpha.x * v.y + a.alpha.y * v.x);
+                            if (a.usebeta) {
+                                const double2 yo = *yp;
+                                out.x += a.beta.x * yo.x - a.beta.y * yo.y;
+                                out.y += a.beta.x * yo.y + a.beta.y * yo.x;
+                            }
+                            *yp = out;
+                        } else {
+                            double2 *d = a.dst + (gout + i) * a.vs + col;
+                            if (a.accumulate) {
+                                const double2 old = *d;
+                                v = make_double2(old.x + v.x, old.y + v.y);
+                            }
+                            *d = v;
+                        }
+                    }
+            }
+            acc.zero();
+        }
+        __syncwarp();  // buffer k & 1 is free for chunk k + 2
+        co = no;
+        cR = nR;
+        cW = nW;
+        clast = nlast;
+    }
+    cp_async_wait<0>();
+}
+}  // namespace
+
+// a single right-hand side keeps the lane-per-row FMA kernel: the tensor-core tiles would be
+// 7/8 idle and its single column per memory round trip is then no handicap
+bool gather_tiny_fits(int maxrows, int bc) { return maxrows <= 32 && bc >= 2 && bc <= 16; }
+
+template <typename S>
+void launch_gather_tiny(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
+    if (count <= 0) return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t sm = size_t(2 * TINY_WARPS) * TINY_STAGE;
+    const int need = (count + TINY_WARPS - 1) / TINY_WARPS;
+    const int grid = need < 3 * sms ? need : 3 * sms;  // one resident wave of persistent warps
+    const int nrt = (a.maxrows + 7) / 8;
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+        kern<<<grid, TINY_WARPS * 32, sm, s>>>(a, nodes, count);
+    };
+    if (a.bc > 8) {
+        if (nrt <= 1) go(k_gather_tiny<S, 1, 2>);
+        else if (nrt <= 2) go(k_gather_tiny<S, 2, 2>);
+        else go(k_gather_tiny<S, 4, 2>);
+    } else {
+        if (nrt <= 1) go(k_gather_tiny<S, 1, 1>);
+        else if (nrt <= 2) go(k_gather_tiny<S, 2, 1>);
+        else go(k_gather_tiny<S, 4, 1>);
+    }
+}
+
+template void launch_gather_tiny<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
+template void launch_gather_tiny<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
 
 namespace {
 template <typename S>

@@ -74,6 +74,13 @@ void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStrea
 template <typename S>
 void launch_gather_small(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
 
+// STAGE_GATHER for many outputs of at most 32 rows with 2..16 right-hand sides per pass: one
+// warp streams a sequence of outputs, double-buffering their block columns and vector rows in
+// shared memory with asynchronous copies, and multiplies on the FP64 tensor cores.
+bool gather_tiny_fits(int maxrows, int bc);
+template <typename S>
+void launch_gather_tiny(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
+
 // dst[doff[e] + i + j * rows[e]] = src[soff[e] + i + j * sld[e]]: sub-matrix copies into
 // contiguous column-major blocks.
 template <typename S>

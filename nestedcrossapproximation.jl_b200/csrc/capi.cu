@@ -1860,8 +1860,11 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
                     a.conj = conj;
                     a.maxrows = G.group_maxrows[g];
                     a.error = error;
-                    // many small outputs: one warp each; few large ones: the streaming MMA kernel
-                    if (a.maxrows <= 64 && G.group_work[g] < 8192.0)
+                    // many small outputs: one warp streams a sequence of them (up to 32 rows) or
+                    // takes one (up to 64 rows); few large ones: the streaming MMA kernel
+                    if (G.group_work[g] < 8192.0 && gather_tiny_fits(a.maxrows, bc))
+                        launch_gather_tiny<S>(a, G.outputs.p + G.group_ptr[g], cnt, s);
+                    else if (a.maxrows <= 64 && G.group_work[g] < 8192.0)
                         launch_gather_small<S>(a, G.outputs.p + G.group_ptr[g], cnt, s);
                     else
                         launch_rows<S>(a, G.outputs.p + G.group_ptr[g], cnt, s);
