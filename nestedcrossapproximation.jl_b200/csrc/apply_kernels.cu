@@ -206,6 +206,8 @@ __device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.
 struct TileMap {
     int kgroups, mykg, rt0, nrt;
     int step = NCONS;  // row tiles between a warp's successive tiles
+    // partial sums per output row: rows 0-31 and rows from 32 on (the same for every warp)
+    int parts_lo = 1, parts_hi = 1;
     // one warp holding every tile of an R-row output (row tiles 0, 1, ...)
     __device__ void init_single(int R) {
         kgroups = 1;
@@ -216,12 +218,33 @@ struct TileMap {
     }
     __device__ void init(int R, int warp) {
         const int MT = (R + 7) >> 3;
+        if (MT == 5 || MT == 6) {
+            // Four whole row tiles on warps 0-3 (one per SM sub-partition, warp w runs on
+            // sub-partition w mod 4) and the other MT - 4 row tiles split by k-steps over warps
+            // 4-7, so that every sub-partition's tensor pipe gets the same share (whole tiles on
+            // warps 0-4 would give one sub-partition two tiles while the others have one).
+            const int split = 4 / (MT - 4);
+            if (warp < 4) {
+                kgroups = 1;
+                mykg = 0;
+                rt0 = warp;
+            } else {
+                kgroups = split;
+                mykg = (warp - 4) % split;
+                rt0 = 4 + (warp - 4) / split;
+            }
+            nrt = 1;
+            parts_lo = 1;
+            parts_hi = split;
+            return;
+        }
         const int mt1 = MT > 0 ? MT : 1;
         kgroups = MT >= NCONS ? 1 : NCONS / mt1;
         mykg = kgroups > 1 ? warp / mt1 : 0;
         rt0 = kgroups > 1 ? warp % mt1 : warp;
         const bool busy = MT > 0 && (kgroups > 1 ? warp < MT * kgroups : warp < MT);
         nrt = !busy ? 0 : kgroups > 1 ? 1 : (MT - rt0 + NCONS - 1) / NCONS;
+        parts_lo = parts_hi = kgroups;
     }
     __device__ int row(int j, int g) const { return (rt0 + j * step) * 8 + g; }
 };
@@ -477,7 +500,8 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
         const int i = scatter ? e % R : e / bc;
         const int qq = scatter ? e / R : e % bc;
         double2 v = red[i * bc + qq];
-        for (int kg = 1; kg < tm.kgroups; ++kg) {
+        const int parts = i < 32 ? tm.parts_lo : tm.parts_hi;
+        for (int kg = 1; kg < parts; ++kg) {
             const double2 p = red[(kg * R + i) * bc + qq];
             v.x += p.x;
             v.y += p.y;
