@@ -109,5 +109,8 @@ struct MimicryArgs {
 };
 size_t mimicry_smem_bytes(int maxrank);
 void launch_mimicry(const MimicryArgs &a, cudaStream_t s);
+// packs count[i] pivots of every item from its maxrank-wide slot into the CSR list fpidx
+void launch_compact_pivots(const int32_t *piv, int maxrank, const int32_t *count, const int32_t *fpptr,
+                           int nitems, int32_t *fpidx, cudaStream_t s);
 
 }  // namespace nca

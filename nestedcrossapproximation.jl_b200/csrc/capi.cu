@@ -143,7 +143,7 @@ struct DevSide {
 struct DirItems {
     nca::DirSide plan;
     int nitems = 0;
-    std::vector<int32_t> h_fpptr, h_fpidx, h_rank, h_nrows, h_piv;
+    std::vector<int32_t> h_fpptr, h_rank, h_nrows, h_piv;  // far pivots stay on the device (fpidx)
     std::vector<int64_t> h_xoff, h_cptr;
     DBuf<int32_t> item_node, item_basis, item_chptr, item_chidx, fpptr, fpidx, rank, nrows, piv, cpiv;
     DBuf<int64_t> xoff;
@@ -312,14 +312,20 @@ void parallel_csr(int n, F fill, std::vector<int64_t> &ptr, std::vector<int32_t>
 
 // Phase 1 on the device: tree-mimicry far pivots of every item of one side (item i is own
 // cluster item_node[i], or cluster i when item_node is null), with far field ffnodes[ffptr[i]..)
-// in the reference's farfield order. Returns the CSR of pivots (far point ids).
+// in the reference's farfield order. Returns the CSR of pivots (far point ids) on the device
+// (dptr, didx) and its pointer array on the host; the host copy of the list only when asked for.
 void device_farpivots(const nca::Tree &own, const double *ownpts, const nca::Tree &far, const DevSide &fd,
                       int nitems, const std::vector<int64_t> &ffptr, const std::vector<int32_t> &ffnodes,
                       const std::vector<int32_t> *item_node, int maxrank, cudaStream_t s,
-                      std::vector<int32_t> &fpptr, std::vector<int32_t> &fpidx) {
+                      std::vector<int32_t> &fpptr, DBuf<int32_t> &dfpptr, DBuf<int32_t> &dfpidx,
+                      std::vector<int32_t> *fpidx) {
     fpptr.assign(nitems + 1, 0);
-    fpidx.clear();
-    if (nitems == 0) return;
+    if (fpidx) fpidx->clear();
+    if (nitems == 0) {
+        dfpptr.upload(fpptr, s);
+        dfpidx.alloc(1);
+        return;
+    }
     // centroids of the own clusters (the host planner's sums, in its order)
     std::vector<double> centroid(3 * size_t(own.nnodes), 0.0);
     std::vector<int32_t> own_size(own.nnodes);
@@ -374,14 +380,19 @@ void device_farpivots(const nca::Tree &own, const double *ownpts, const nca::Tre
     launch_mimicry(a, s);
     CK(cudaGetLastError());
     const std::vector<int32_t> count = dcount.download(s);
-    const std::vector<int32_t> piv = dpiv.download(s);
     const std::vector<int32_t> err = derr.download(s);
     if (err[0] != 0) throw Failure(NCA_ERR_CUDA, "internal: tree mimicry ran out of far points");
     for (int i = 0; i < nitems; ++i) fpptr[i + 1] = fpptr[i] + count[i];
-    fpidx.resize(fpptr[nitems]);
-    for (int i = 0; i < nitems; ++i)
-        std::copy(piv.begin() + size_t(i) * maxrank, piv.begin() + size_t(i) * maxrank + count[i],
-                  fpidx.begin() + fpptr[i]);
+    dfpptr.upload(fpptr, s);
+    dfpidx.alloc(size_t(std::max(fpptr[nitems], 1)));
+    launch_compact_pivots(dpiv.p, maxrank, dcount.p, dfpptr.p, nitems, dfpidx.p, s);
+    CK(cudaGetLastError());
+    if (fpidx) {
+        fpidx->resize(fpptr[nitems]);
+        if (fpptr[nitems])
+            CK(cudaMemcpyAsync(fpidx->data(), dfpidx.p, sizeof(int32_t) * fpptr[nitems], cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
 }
 
 // Rows/rank bounds per node (bottom-up), X slot offsets and per-level active node lists.
@@ -679,7 +690,8 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
             },
             ffptr, ffnodes);
         device_farpivots(T, sd == 0 ? tp : sp, c->tree[1 - sd], c->side[1 - sd], T.nnodes, ffptr, ffnodes, nullptr,
-                         maxrank, s, c->side[sd].h_fpptr, c->side[sd].h_fpidx);
+                         maxrank, s, c->side[sd].h_fpptr, c->side[sd].fpptr, c->side[sd].fpidx,
+                         &c->side[sd].h_fpidx);
     }
     auto h1 = std::chrono::steady_clock::now();
     cudaEvent_t ev0, ev1;
@@ -698,8 +710,6 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
     for (int sd = 0; sd < 2; ++sd) {
         DevSide &d = c->side[sd];
         const nca::Tree &T = c->tree[sd];
-        d.fpptr.upload(d.h_fpptr, s);
-        d.fpidx.upload(d.h_fpidx, s);
         std::vector<int32_t> lv_ptr, lv_nodes;
         std::vector<int> lv_mcap, lv_ncap;
         plan_side(d, T, maxrank, lv_ptr, lv_nodes, lv_mcap, lv_ncap);
@@ -938,12 +948,20 @@ struct StageBuilder {
     }
     // uploads the plan; with a source, allocates the stage store and copies its blocks
     void finish(GatherStage &G, const double2 *src, cudaStream_t s) {
-        // outputs of each group largest work first (shorter tail of the last wave)
+        // outputs of each group largest work first (shorter tail of the last wave): a stable
+        // counting sort on the work, linear in the outputs
         std::vector<int32_t> order(rows.size());
-        for (size_t i = 0; i < order.size(); ++i) order[i] = int32_t(i);
-        for (size_t g = 0; g + 1 < group_ptr.size(); ++g)
-            std::stable_sort(order.begin() + group_ptr[g], order.begin() + group_ptr[g + 1],
-                             [&](int a, int b) { return work[a] > work[b]; });
+        std::vector<int64_t> cnt;
+        for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
+            const int32_t b = group_ptr[g], e = group_ptr[g + 1];
+            if (e <= b) continue;
+            int64_t wmax = 0;
+            for (int32_t i = b; i < e; ++i) wmax = std::max(wmax, work[i]);
+            cnt.assign(size_t(wmax) + 2, 0);
+            for (int32_t i = b; i < e; ++i) ++cnt[size_t(wmax - work[i]) + 1];
+            for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
+            for (int32_t i = b; i < e; ++i) order[size_t(b + cnt[size_t(wmax - work[i])]++)] = i;
+        }
         G.group_ptr = group_ptr;
         G.group_maxrows = group_maxrows;
         G.group_work = group_work;
@@ -999,7 +1017,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             ni, [&](int it, std::vector<int32_t> &ff) { nca::item_farfield(c->tree[sd], d.plan, it, ff); }, ffptr,
             ffnodes);
         device_farpivots(c->tree[sd], pts[sd], c->tree[1 - sd], c->side[1 - sd], ni, ffptr, ffnodes,
-                         &d.plan.item_node, maxrank, s, d.h_fpptr, d.h_fpidx);
+                         &d.plan.item_node, maxrank, s, d.h_fpptr, d.fpptr, d.fpidx, nullptr);
     }
     auto h1 = std::chrono::steady_clock::now();
     cudaEvent_t ev0, ev1;
@@ -1030,8 +1048,6 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         d.item_basis.upload(pl.item_basis, s);
         d.item_chptr.upload(pl.item_chptr, s);
         d.item_chidx.upload(pl.item_chidx, s);
-        d.fpptr.upload(d.h_fpptr, s);
-        d.fpidx.upload(d.h_fpidx, s);
         d.rank.alloc(std::max(ni, 1));
         d.rank.zero(s);
         d.nrows.alloc(std::max(ni, 1));
@@ -1325,26 +1341,40 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         }
         // down: output-side items gather from the parent items that map onto them, root level first
         {
-            std::vector<std::vector<std::pair<int32_t, int64_t>>> parents(dout.nitems);
-            for (int it = 0; it < dout.nitems; ++it) {
-                if (dout.h_rank[it] <= 0 || dout.plan.item_basis[it]) continue;
-                int64_t c0 = 0;
-                for (int k = dout.plan.item_chptr[it]; k < dout.plan.item_chptr[it + 1]; ++k) {
-                    const int ch = dout.plan.item_chidx[k];
-                    if (dout.h_rank[ch] > 0) parents[ch].push_back({it, c0});
-                    c0 += dout.h_rank[ch];
+            // parents of every child item (CSR in parent order), with the child's row offset in
+            // the parent's X
+            std::vector<int32_t> pptr(size_t(dout.nitems) + 1, 0), ppar;
+            std::vector<int64_t> prow;
+            auto each_child = [&](auto fn) {
+                for (int it = 0; it < dout.nitems; ++it) {
+                    if (dout.h_rank[it] <= 0 || dout.plan.item_basis[it]) continue;
+                    int64_t c0 = 0;
+                    for (int k = dout.plan.item_chptr[it]; k < dout.plan.item_chptr[it + 1]; ++k) {
+                        const int ch = dout.plan.item_chidx[k];
+                        if (dout.h_rank[ch] > 0) fn(ch, it, c0);
+                        c0 += dout.h_rank[ch];
+                    }
                 }
-            }
+            };
+            each_child([&](int ch, int, int64_t) { ++pptr[size_t(ch) + 1]; });
+            for (int it = 0; it < dout.nitems; ++it) pptr[size_t(it) + 1] += pptr[it];
+            ppar.resize(pptr.back());
+            prow.resize(pptr.back());
+            std::vector<int32_t> fill(pptr.begin(), pptr.end() - 1);
+            each_child([&](int ch, int it, int64_t c0) {
+                ppar[fill[ch]] = it;
+                prow[fill[ch]++] = c0;
+            });
             StageBuilder B;
             for (int lev = 1; lev < TO.nlevels; ++lev) {
                 for (int it : bylevel[O][lev]) {
                     const int r = dout.h_rank[it];
-                    if (r <= 0 || parents[it].empty()) continue;
+                    if (r <= 0 || pptr[it + 1] == pptr[it]) continue;
                     B.begin_output(r, yo + dout.h_cptr[it]);
-                    for (const auto &pc : parents[it]) {
-                        const int p = pc.first;
+                    for (int q = pptr[it]; q < pptr[it + 1]; ++q) {
+                        const int p = ppar[q];
                         const int rp = dout.h_rank[p];
-                        B.segment(B.copy(dout.h_xoff[p] + pc.second, dout.h_nrows[p], r, rp), rp, yo + dout.h_cptr[p]);
+                        B.segment(B.copy(dout.h_xoff[p] + prow[q], dout.h_nrows[p], r, rp), rp, yo + dout.h_cptr[p]);
                     }
                     B.end_output();
                 }

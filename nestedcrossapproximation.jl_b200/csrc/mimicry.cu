@@ -201,7 +201,30 @@ __global__ void __launch_bounds__(kWarps * 32) k_mimicry(MimicryArgs a) {
     }
 }
 
+// fpidx[fpptr[i] + r] = piv[i * maxrank + r] for r < count[i]: the padded pivot slots of every
+// item packed into one CSR list
+__global__ void k_compact_pivots(const int32_t *piv, int maxrank, const int32_t *count, const int32_t *fpptr,
+                                 int64_t nslots, int32_t *fpidx) {
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < nslots; e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = e / maxrank;
+        const int r = int(e - i * maxrank);
+        if (r < count[i]) fpidx[fpptr[i] + r] = piv[e];
+    }
+}
+
 }  // namespace
+
+void launch_compact_pivots(const int32_t *piv, int maxrank, const int32_t *count, const int32_t *fpptr,
+                           int nitems, int32_t *fpidx, cudaStream_t s) {
+    const int64_t nslots = int64_t(nitems) * maxrank;
+    if (nslots <= 0) return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t need = (nslots + 255) / 256;
+    k_compact_pivots<<<int(need < int64_t(sms) * 16 ? need : int64_t(sms) * 16), 256, 0, s>>>(piv, maxrank, count, fpptr,
+                                                                                              nslots, fpidx);
+}
 
 size_t mimicry_smem_bytes(int maxrank) { return size_t(kWarps) * maxrank * (3 * sizeof(double) + sizeof(int32_t)); }
 
