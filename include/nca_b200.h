@@ -238,6 +238,14 @@ int32_t nca_workspace_set_parts(nca_workspace *ws, int32_t far, int32_t near);
  * leaf bases (stage 5); with only one part present, stage 5 is the whole leaf launch and
  * stage 4 is empty. Stages 1-3 and 4 overlap in time. */
 int32_t nca_workspace_set_profiling(nca_workspace *ws, int32_t on);
+/* CUDA-graph replay (off by default): an nca_apply on device arrays (memspace 1) whose arguments
+ * (mode, precision, pointers, leading dimensions, nrhs, alpha, beta, parts, profiling) equal one
+ * of the workspace's last few calls is captured once into a CUDA graph, and later identical calls
+ * launch that graph instead of enqueueing every stage. Results are bitwise those of the enqueued
+ * product. It pays off for launch-bound products (small problems); for large ones it is slower,
+ * because the graph loses the overlap of the far-field sweeps with the near field (measured on the
+ * 65,536-point sphere: 1.53 ms per step with graphs, 1.46 ms without). */
+int32_t nca_workspace_set_graphs(nca_workspace *ws, int32_t on);
 int32_t nca_workspace_stage_times(const nca_workspace *ws, double *seconds, int32_t *launches,
                                   int32_t nstages);
 

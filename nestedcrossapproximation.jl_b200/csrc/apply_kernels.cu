@@ -564,60 +564,78 @@ __global__ void k_gather(const double2 *x, int64_t ldx, const int32_t *perm, int
 int vector_stride(int b) { return conflict_free(b); }
 
 namespace {
+// One product launch; with a nonzero priority as a per-launch attribute, which a stream capture
+// keeps in the graph (a graph does not carry its streams' priorities).
+template <typename S, typename K>
+void launch_one(K kern, const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t sm, int priority) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+    if (priority == 0) {
+        kern<<<count, NT, sm, s>>>(a, nodes);
+        return;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(count);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributePriority;
+    at[0].val.priority = priority;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, a, nodes);
+}
+
 template <typename S, int NRT, int NTL>
-void launch_tiles(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t sm) {
+void launch_tiles(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t sm, int priority) {
     switch (a.stage) {
     case STAGE_UP:
-        cudaFuncSetAttribute(k_rows_up<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        k_rows_up<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
+        launch_one<S>(k_rows_up<S, NRT, NTL>, a, nodes, count, s, sm, priority);
         break;
     case STAGE_COUPLE:
-        cudaFuncSetAttribute(k_rows_couple<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        k_rows_couple<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
+        launch_one<S>(k_rows_couple<S, NRT, NTL>, a, nodes, count, s, sm, priority);
         break;
     case STAGE_DOWN:
-        cudaFuncSetAttribute(k_rows_down<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        k_rows_down<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
+        launch_one<S>(k_rows_down<S, NRT, NTL>, a, nodes, count, s, sm, priority);
         break;
     case STAGE_GATHER:
-        cudaFuncSetAttribute(k_rows_gather<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        k_rows_gather<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
+        launch_one<S>(k_rows_gather<S, NRT, NTL>, a, nodes, count, s, sm, priority);
         break;
     default:
-        cudaFuncSetAttribute(k_rows_leaves<S, NRT, NTL>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
-        k_rows_leaves<S, NRT, NTL><<<count, NT, sm, s>>>(a, nodes);
+        launch_one<S>(k_rows_leaves<S, NRT, NTL>, a, nodes, count, s, sm, priority);
     }
 }
 
 // Row tiles per warp for the largest block of the launch: 1, 2, 4 or (one column tile only) 8;
 // rows_capacity keeps R * ceil(bc / 8) <= 512, so the tiles of a warp never exceed 8.
 template <typename S, int NTL>
-void launch_ntl(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t sm) {
+void launch_ntl(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t sm, int priority) {
     const int MT = (a.maxrows + 7) / 8;
     const int nrt = (MT + NCONS - 1) / NCONS;
     if (nrt <= 1)
-        launch_tiles<S, 1, NTL>(a, nodes, count, s, sm);
+        launch_tiles<S, 1, NTL>(a, nodes, count, s, sm, priority);
     else if (nrt <= 2)
-        launch_tiles<S, 2, NTL>(a, nodes, count, s, sm);
+        launch_tiles<S, 2, NTL>(a, nodes, count, s, sm, priority);
     else if (nrt <= 4 || NTL == 2)
-        launch_tiles<S, 4, NTL>(a, nodes, count, s, sm);
+        launch_tiles<S, 4, NTL>(a, nodes, count, s, sm, priority);
     else
-        launch_tiles<S, (NTL == 1 ? 8 : 4), NTL>(a, nodes, count, s, sm);
+        launch_tiles<S, (NTL == 1 ? 8 : 4), NTL>(a, nodes, count, s, sm, priority);
 }
 }  // namespace
 
 template <typename S>
-void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t smem_bytes) {
+void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t smem_bytes,
+                 int priority) {
     if (count <= 0) return;
     const size_t sm = smem_bytes ? smem_bytes : rows_smem_bytes();
     if (a.bc > 8)
-        launch_ntl<S, 2>(a, nodes, count, s, sm);
+        launch_ntl<S, 2>(a, nodes, count, s, sm, priority);
     else
-        launch_ntl<S, 1>(a, nodes, count, s, sm);
+        launch_ntl<S, 1>(a, nodes, count, s, sm, priority);
 }
 
-template void launch_rows<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t, size_t);
-template void launch_rows<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t, size_t);
+template void launch_rows<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t, size_t, int);
+template void launch_rows<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t, size_t, int);
 
 
 namespace {

@@ -65,9 +65,11 @@ __global__ void k_gather(const double2 *x, int64_t ldx, const int32_t *perm, int
 int vector_stride(int b);  // row stride of the internal vector buffers for b right-hand sides
 
 // smem_bytes: dynamic shared memory of each CTA (0: rows_smem_bytes()); a larger request only
-// lowers how many CTAs of the launch share an SM.
+// lowers how many CTAs of the launch share an SM. priority: 0 for the stream's, else the launch's
+// own scheduling priority (a CUDA stream priority value).
 template <typename S>
-void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t smem_bytes = 0);
+void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s, size_t smem_bytes = 0,
+                 int priority = 0);
 
 // STAGE_GATHER for outputs of at most 64 rows: one warp per output, operands read straight from
 // global memory, complex FP64 FMA (directional products, whose outputs are many small blocks).

@@ -237,9 +237,37 @@ struct nca_workspace {
     // small launches take SM slots as the near-field CTAs retire) and its fork / join events
     cudaStream_t aux = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
+    int aux_priority = 0;
+    // Products repeated with identical arguments on device arrays replay a CUDA graph of their
+    // launches: a call whose arguments were seen in one of the last few calls is captured once,
+    // later identical calls launch the graph. Buffer reallocation (gen) invalidates every graph.
+    struct GraphKey {
+        int mode, precision, b, far, near, profiling;
+        const void *x, *y;
+        int64_t ldx, ldy;
+        double ar, ai, br, bi;
+        uint64_t gen;
+        bool operator==(const GraphKey &o) const {
+            return mode == o.mode && precision == o.precision && b == o.b && far == o.far && near == o.near &&
+                   profiling == o.profiling && x == o.x && y == o.y && ldx == o.ldx && ldy == o.ldy && ar == o.ar &&
+                   ai == o.ai && br == o.br && bi == o.bi && gen == o.gen;
+        }
+    };
+    struct Graph {
+        GraphKey key;
+        cudaGraphExec_t exec = nullptr;
+        int launches = 0;
+        int stage[6] = {0, 0, 0, 0, 0, 0};
+    };
+    std::vector<Graph> graphs;     // at most kGraphs, oldest first
+    std::vector<GraphKey> seen;    // the last few eager calls' arguments
+    uint64_t gen = 0;
+    bool use_graphs = false;
 };
 
 namespace {
+
+constexpr size_t kGraphs = 4;
 
 constexpr int kMaxSmem = 227 * 1024;
 
@@ -1461,6 +1489,15 @@ struct ProductBuffers {
     bool far, near;
 };
 
+// Records a timing event; inside a stream capture as an external event node, so that the event
+// is recorded each time the graph runs.
+cudaError_t record_stage_event(cudaEvent_t ev, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) return e;
+    return cudaEventRecordWithFlags(ev, st, cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0);
+}
+
 // Launch counts of one product: total and per stage (gather, up, couple, down, near field,
 // leaves).
 constexpr int kStages = 6;
@@ -1478,6 +1515,7 @@ enum StageEvent { EV_START, EV_GATHER, EV_UP, EV_COUPLE, EV_DOWN, EV_NEAR0, EV_N
 struct ProductStreams {
     cudaStream_t aux = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
+    int priority = 0;  // the sweeps' launch priority (that of aux)
 };
 
 // Enqueues the gather and the product stages of y = alpha op(A) x + beta y on stream s. x, y are
@@ -1505,7 +1543,7 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
         return fail(NCA_ERR_ARG, "a leaf or transfer block has more rows than one product CTA holds");
     const bool overlap = ps.aux != nullptr && buf.far && buf.near;
     auto mark = [&](int k, cudaStream_t st) {
-        if (stage_ev) CK(cudaEventRecord(stage_ev[k], st));
+        if (stage_ev) CK(record_stage_event(stage_ev[k], st));
     };
     mark(EV_START, s);
     k_gather<<<launch_grid(nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, I.perm.p, nin, b, vs, buf.xt);
@@ -1552,7 +1590,7 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
                 a.conj = conj && in == 0;
                 a.maxrows = I.up.mcap[l];
                 a.error = buf.error;
-                launch_rows<S>(a, I.up.d_nodes.p + I.up.ptr[l], cnt, st);
+                launch_rows<S>(a, I.up.d_nodes.p + I.up.ptr[l], cnt, st, 0, st == ps.aux ? ps.priority : 0);
                 ++count.total;
                 ++count.stage[1];
             }
@@ -1585,7 +1623,8 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
                 a.conj = conj;
                 a.maxrows = c->maxrank;
                 a.error = buf.error;
-                launch_rows<S>(a, mode == 0 ? c->couple_fwd.p : c->couple_rev.p, ncp, st);
+                launch_rows<S>(a, mode == 0 ? c->couple_fwd.p : c->couple_rev.p, ncp, st, 0,
+                               st == ps.aux ? ps.priority : 0);
                 ++count.total;
                 ++count.stage[2];
             }
@@ -1610,7 +1649,7 @@ int enqueue_product(nca_core *c, int mode, int precision, const double2 *xd, int
                 a.conj = conj && out == 1;
                 a.maxrows = O.down.mcap[l];
                 a.error = buf.error;
-                launch_rows<S>(a, O.down.d_nodes.p + O.down.ptr[l], cnt, st);
+                launch_rows<S>(a, O.down.d_nodes.p + O.down.ptr[l], cnt, st, 0, st == ps.aux ? ps.priority : 0);
                 ++count.total;
                 ++count.stage[3];
             }
@@ -1929,6 +1968,15 @@ int check_product_args(nca_core *c, int mode, int precision, int64_t ldx, int64_
     return NCA_OK;
 }
 
+// Destroys the workspace's graphs and forgets the arguments seen (buffers are about to move).
+void drop_graphs(nca_workspace *ws) {
+    for (auto &g : ws->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    ws->graphs.clear();
+    ws->seen.clear();
+    ++ws->gen;
+}
+
 int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_t ldx, void *y,
                int64_t ldy, int64_t nrhs, double2 alpha, double2 beta, int memspace, bool tangent = false) {
     nca_core *c = ws->core;
@@ -1946,6 +1994,7 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     const int b = int(nrhs);
     if (b > ws->max_nrhs && !c->dir) {
         const int vsm = vector_slots(b);
+        drop_graphs(ws);
         ws->xt.alloc(size_t(std::max(c->side[0].npts, c->side[1].npts)) * vsm);
         ws->xhat.alloc(size_t(std::max(c->side[0].h_cptr.back(), c->side[1].h_cptr.back())) * vsm);
         ws->yhat.alloc(ws->xhat.n);
@@ -1975,7 +2024,10 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     if (c->dir) {
         const DirProduct &pr = c->dir->prod[mode == 0 ? 0 : 1];
         const size_t need = size_t(pr.nin + pr.cin + pr.cout) * vector_slots(b);
-        if (ws->arena.n < need) ws->arena.alloc(need);
+        if (ws->arena.n < need) {
+            drop_graphs(ws);
+            ws->arena.alloc(need);
+        }
     }
     if (tangent && ws->dxhat.n < ws->xhat.n) {
         ws->dxhat.alloc(ws->xhat.n);
@@ -1983,24 +2035,85 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     }
     const ProductBuffers buf{ws->xt.p, ws->xhat.p, ws->yhat.p, ws->error.p, ws->far, ws->near};
     ProductLaunches count;
-    if (c->dir) {
-        if (ws->profiling) CK(cudaEventRecord(ws->stage_ev[0], s));
-        if (int st = enqueue_dir_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, ws->arena.p, ws->error.p,
-                                         s, count))
-            return st;
-        if (ws->profiling)
-            for (int k = 1; k < EV_COUNT; ++k) CK(cudaEventRecord(ws->stage_ev[k], s));
-    } else if (tangent) {
-        if (int st = enqueue_tangent(c, xd, lx, yd, ly, b, alpha, beta, buf, ws->dxhat.p, ws->dyhat.p, s, count))
-            return st;
+    // graph replay of repeated products on device arrays
+    const bool graphable = ws->use_graphs && memspace == 1 && !tangent;
+    const nca_workspace::GraphKey key{mode,     precision, b,       int(ws->far), int(ws->near), int(ws->profiling),
+                                      x,        y,         ldx,     ldy,          alpha.x,       alpha.y,
+                                      beta.x,   beta.y,    ws->gen};
+    nca_workspace::Graph *graph = nullptr;
+    bool capture = false;
+    if (graphable) {
+        for (auto &gr : ws->graphs)
+            if (gr.key == key) graph = &gr;
+        if (!graph)
+            for (const auto &k : ws->seen)
+                if (k == key) capture = true;
+    }
+    auto enqueue = [&]() -> int {
+        if (c->dir) {
+            if (ws->profiling) CK(record_stage_event(ws->stage_ev[0], s));
+            if (int st = enqueue_dir_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, ws->arena.p,
+                                             ws->error.p, s, count))
+                return st;
+            if (ws->profiling)
+                for (int k = 1; k < EV_COUNT; ++k) CK(record_stage_event(ws->stage_ev[k], s));
+        } else if (tangent) {
+            if (int st = enqueue_tangent(c, xd, lx, yd, ly, b, alpha, beta, buf, ws->dxhat.p, ws->dyhat.p, s, count))
+                return st;
+        } else {
+            ProductStreams ps;
+            ps.aux = ws->aux;
+            ps.fork = ws->fork;
+            ps.join = ws->join;
+            ps.priority = ws->aux_priority;
+            if (int st = enqueue_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, buf, s,
+                                         ws->profiling ? ws->stage_ev : nullptr, count, ps))
+                return st;
+        }
+        return NCA_OK;
+    };
+    if (graph) {
+        CK(cudaGraphLaunch(graph->exec, s));
+        count.total = graph->launches;
+        std::copy(graph->stage, graph->stage + kStages, count.stage);
+    } else if (capture) {
+        // a failed capture (an error return or a thrown CUDA error) is ended and discarded
+        struct CaptureGuard {
+            cudaStream_t s;
+            bool active = true;
+            ~CaptureGuard() {
+                if (!active) return;
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(s, &g);
+                if (g) cudaGraphDestroy(g);
+            }
+        } guard{s};
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        if (int st = enqueue()) return st;
+        cudaGraph_t g = nullptr;
+        guard.active = false;
+        CK(cudaStreamEndCapture(s, &g));
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        CK(ie);
+        if (ws->graphs.size() >= kGraphs) {
+            cudaGraphExecDestroy(ws->graphs.front().exec);
+            ws->graphs.erase(ws->graphs.begin());
+        }
+        nca_workspace::Graph gr;
+        gr.key = key;
+        gr.exec = exec;
+        gr.launches = count.total;
+        std::copy(count.stage, count.stage + kStages, gr.stage);
+        ws->graphs.push_back(gr);
+        CK(cudaGraphLaunch(exec, s));
     } else {
-        ProductStreams ps;
-        ps.aux = ws->aux;
-        ps.fork = ws->fork;
-        ps.join = ws->join;
-        if (int st = enqueue_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, buf, s,
-                                     ws->profiling ? ws->stage_ev : nullptr, count, ps))
-            return st;
+        if (int st = enqueue()) return st;
+        if (graphable) {
+            if (ws->seen.size() >= kGraphs) ws->seen.erase(ws->seen.begin());
+            ws->seen.push_back(key);
+        }
     }
     CK(cudaMemcpyAsync(ws->error_host, ws->error.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     if (memspace == 0)
@@ -2905,6 +3018,7 @@ int32_t nca_workspace_create(nca_core *core, int32_t max_nrhs, nca_workspace **o
             int least = 0, greatest = 0;
             CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
             CK(cudaStreamCreateWithPriority(&ws->aux, cudaStreamNonBlocking, greatest));
+            ws->aux_priority = greatest;
             CK(cudaEventCreateWithFlags(&ws->fork, cudaEventDisableTiming));
             CK(cudaEventCreateWithFlags(&ws->join, cudaEventDisableTiming));
         }
@@ -2925,6 +3039,7 @@ int32_t nca_workspace_create(nca_core *core, int32_t max_nrhs, nca_workspace **o
 void nca_workspace_destroy(nca_workspace *ws) {
     if (!ws) return;
     cudaSetDevice(ws->core->device);
+    drop_graphs(ws);
     if (ws->stream) cudaStreamDestroy(ws->stream);
     if (ws->aux) cudaStreamDestroy(ws->aux);
     if (ws->fork) cudaEventDestroy(ws->fork);
@@ -2993,6 +3108,16 @@ int32_t nca_workspace_set_parts(nca_workspace *ws, int32_t far, int32_t near) {
     ws->far = far != 0;
     ws->near = near != 0;
     return NCA_OK;
+}
+
+int32_t nca_workspace_set_graphs(nca_workspace *ws, int32_t on) {
+    return guarded([&] {
+        if (!ws) return fail(NCA_ERR_ARG, "null workspace");
+        CK(cudaSetDevice(ws->core->device));
+        if (!on) drop_graphs(ws);
+        ws->use_graphs = on != 0;
+        return int(NCA_OK);
+    });
 }
 
 int32_t nca_workspace_set_profiling(nca_workspace *ws, int32_t on) {

@@ -359,6 +359,11 @@ class H2Workspace(LinearMap):
         return mul(None, self if mode == MODE_N else _Transposed(self, mode), x)
 
 
+    def set_graphs(self, on: bool = True):
+        """Replay repeated products on device arrays from CUDA graphs (off by default; pays off for
+        launch-bound small problems)."""
+        check(lib().nca_workspace_set_graphs(self._h, int(on)))
+
     def set_profiling(self, on: bool = True):
         """Record CUDA events around each stage of every product (see stage_times)."""
         check(lib().nca_workspace_set_profiling(self._h, int(on)))

@@ -281,3 +281,43 @@ def test_parts_and_overlapped_stages(c1):
         assert sf["near"][1] == 0 and sf["leaves"][1] == 1
     finally:
         A.set_profiling(False)
+
+
+def test_graph_replay_matches_enqueued_products(c1):
+    """Repeated products on device arrays replay a CUDA graph from the third identical call on;
+    every replay is bitwise the enqueued product, for both orientations alternating, with stage
+    timers on, after alpha / beta change and after the workspace's buffers grow."""
+    import ctypes as C
+    import torch
+    test, trial, A, H = c1
+    N = _n()
+    L = N._lib.lib()
+    W = N.H2Workspace(N.core(A), max_nrhs=4)
+    W.set_graphs(True)
+    E = N.H2Workspace(N.core(A), max_nrhs=4)  # graphs off by default
+
+    def run(ws, mode, X, Y, b, al, be):
+        N._lib.check(L.nca_apply(ws._h, mode, 0, C.c_void_p(X.data_ptr()), 1024, C.c_void_p(Y.data_ptr()), 1024, b,
+                                 al.real, al.imag, be.real, be.imag, 1))
+        torch.cuda.synchronize()
+
+    X = torch.from_numpy(np.ascontiguousarray(cgauss((1024, 20), 80).T)).cuda()
+    Y0 = torch.from_numpy(np.ascontiguousarray(cgauss((1024, 20), 81).T)).cuda()
+    for b, al, be in ((4, 1 + 0j, 0j), (4, 0.5 - 1j, 2 + 0.5j), (20, 1 + 0j, 0j)):
+        for rep in range(4):
+            for mode in (0, 2):
+                Yg, Ye = Y0.clone(), Y0.clone()
+                run(W, mode, X, Yg, b, al, be)
+                run(E, mode, X, Ye, b, al, be)
+                assert torch.equal(Yg, Ye), (b, rep, mode)
+        ref = H.apply(X[:b].cpu().numpy().T, 0)
+        Yg = Y0.clone()
+        run(W, 0, X, Yg, b, al, be)
+        assert relerr(Yg[:b].cpu().numpy().T, al * ref + be * Y0[:b].cpu().numpy().T) < REL
+    W.set_profiling(True)
+    for rep in range(3):
+        Yg = Y0.clone()
+        run(W, 0, X, Yg, 4, 1 + 0j, 0j)
+        st = W.stage_times()
+        assert st["near"][1] == 1 and st["near"][0] > 0 and st["leaves"][0] > 0
+    W.set_profiling(False)
