@@ -86,12 +86,26 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-template <typename S>
+// V: the vector element type (complex FP64; complex FP32 for the gathers of a complex-FP32
+// coefficient arena)
+template <typename S, typename V = double2>
 struct Seg {
     const S *M;
-    const double2 *v;
+    const V *v;
     int w;
 };
+
+// the gathers' input vectors and output rows in the arena's element type
+template <typename V, typename S>
+__device__ __forceinline__ const V *vec_src(const RowArgs<S> &a) {
+    if constexpr (std::is_same<V, float2>::value) return a.src32;
+    else return a.src;
+}
+template <typename V, typename S>
+__device__ __forceinline__ V *vec_dst(const RowArgs<S> &a) {
+    if constexpr (std::is_same<V, float2>::value) return a.dst32;
+    else return a.dst;
+}
 
 template <typename S, int STAGE>
 __device__ __forceinline__ int out_rows(const RowArgs<S> &a, int o) {
@@ -115,10 +129,18 @@ __device__ __forceinline__ int nsegs(const RowArgs<S> &a, int o) {
     return own_segment<S, STAGE>(a, o) + list;
 }
 
-template <typename S, int STAGE>
-__device__ __forceinline__ Seg<S> segment(const RowArgs<S> &a, int o, int k) {
-    Seg<S> g;
-    if (STAGE == STAGE_UP) {
+template <typename S, int STAGE, typename V = double2>
+__device__ __forceinline__ Seg<S, V> segment(const RowArgs<S> &a, int o, int k) {
+    Seg<S, V> g;
+    if constexpr (!std::is_same<V, double2>::value) {
+        // complex-FP32 vectors: the block-sparse gathers only
+        const int e = a.g_segptr[o] + k;
+        const int64_t mo = a.g_moff[e];
+        g.M = mo >= 0 ? a.M + mo : a.M2 + (-1 - mo);
+        g.w = a.g_w[e];
+        g.v = vec_src<V>(a) + a.g_voff[e] * a.vs;
+        return g;
+    } else if (STAGE == STAGE_UP) {
         g.M = a.M + a.moff[o];
         g.w = a.nrows[o];
         g.v = a.nchildren[o] == 0 ? a.src + int64_t(a.begin[o]) * a.vs : a.coef + a.cptr[a.firstchild[o]] * a.vs;
@@ -255,11 +277,11 @@ struct TileMap {
 // past R and B columns past bc only reach outputs that are never stored (each C row / column
 // depends on its own A row / B column alone), so their addresses are clamped into the block.
 // Only k-steps that cross the chunk end need zeros (a k past w would reach every output).
-template <typename S, int NRT, int NTL>
+template <typename S, int NRT, int NTL, typename V = double2>
 __device__ __forceinline__ void consume(Acc<NRT, NTL> &acc, const TileMap &tm, const unsigned char *tile, int w,
                                         int voff, int R, int ldm, int bc, int ldv, int g, int tq, double sgn) {
     const S *Ms = reinterpret_cast<const S *>(tile);
-    const double2 *Vs = reinterpret_cast<const double2 *>(tile + voff);
+    const V *Vs = reinterpret_cast<const V *>(tile + voff);
     constexpr int NSET = Acc<NRT, NTL>::NSET;
     const int step = 4 * tm.kgroups;
     int ar[NRT], bcl[NTL];
@@ -275,7 +297,7 @@ __device__ __forceinline__ void consume(Acc<NRT, NTL> &acc, const TileMap &tm, c
         double bs[NTL];
 #pragma unroll
         for (int t = 0; t < NTL; ++t) {
-            bv[t] = (full || kk < w) ? Vs[kk * ldv + bcl[t]] : make_double2(0.0, 0.0);
+            bv[t] = (full || kk < w) ? to_d2(Vs[kk * ldv + bcl[t]]) : make_double2(0.0, 0.0);
             bs[t] = bv[t].x + bv[t].y;
         }
 #pragma unroll
@@ -321,7 +343,7 @@ int rows_capacity(int bc) {
     return cap < by_ring ? cap : by_ring;
 }
 
-template <typename S, int STAGE, int NRT, int NTL>
+template <typename S, int STAGE, int NRT, int NTL, typename V = double2>
 __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *nodes) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ Ctl ctl;
@@ -339,18 +361,19 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
     const bool percol = f64 && R >= 32;
     const int ldm = percol ? conflict_free(R) : R;
     const bool vwhole = bc == a.b;
-    const int ldv = vwhole ? a.vs : conflict_free(bc);
+    const int ldv = vwhole ? a.vs : conflict_free(bc);  // >= bc + 1 for odd bc
+    constexpr int vel = int(sizeof(V));
     // columns per stage: matrix columns first, the vector rows at voff (16-byte aligned). Chunks
     // are whole groups of k-steps of 4, one per accumulator set, so interior FP32 chunks stay
     // 16-byte multiples.
-    int wmax = STAGE_BYTES / (ldm * elem + ldv * 16);
+    int wmax = STAGE_BYTES / (ldm * elem + ldv * vel);
     {
         constexpr int kq = 4 * Acc<NRT, NTL>::NSET;
         wmax = wmax >= kq ? wmax - wmax % kq : (wmax & ~3);
     }
     if (wmax < 4) wmax = 4;
     int voff = (wmax * ldm * elem + 15) & ~15;
-    while (wmax > 4 && voff + wmax * ldv * 16 > STAGE_BYTES) {
+    while (wmax > 4 && voff + wmax * ldv * vel > STAGE_BYTES) {
         wmax -= 4;
         voff = (wmax * ldm * elem + 15) & ~15;
     }
@@ -381,11 +404,11 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
             int k = 0, c0 = 0;
             // the next segment's descriptor is loaded one segment ahead, so the dependent index
             // loads (CSR entry -> partner node -> its range) overlap the current segment's copies
-            Seg<S> gs, gnext;
+            Seg<S, V> gs, gnext;
             gs.w = 0;
             gnext.w = 0;
-            if (nseg > 0) gs = segment<S, STAGE>(a, o, 0);
-            if (nseg > 1) gnext = segment<S, STAGE>(a, o, 1);
+            if (nseg > 0) gs = segment<S, STAGE, V>(a, o, 0);
+            if (nseg > 1) gnext = segment<S, STAGE, V>(a, o, 1);
             for (int chunk = 0;; ++chunk) {
                 const int s = chunk % NSTAGE;
                 if (chunk >= NSTAGE && !mbar_wait_bounded(&ctl.empty[s], ((chunk / NSTAGE) - 1) & 1)) {
@@ -403,22 +426,24 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
                         ++k;
                         c0 = 0;
                         gs = gnext;
-                        if (k + 1 < nseg) gnext = segment<S, STAGE>(a, o, k + 1);
+                        if (k + 1 < nseg) gnext = segment<S, STAGE, V>(a, o, k + 1);
                     }
                     if (k >= nseg) break;
                     int w = gs.w - c0;
                     if (w > wmax - filled) w = wmax - filled;
                     const S *msrc = gs.M + int64_t(c0) * R;
-                    const double2 *vsrc = gs.v + int64_t(c0) * a.vs + a.q0;
+                    const V *vsrc = gs.v + int64_t(c0) * a.vs + a.q0;
                     c0 += w;
                     if (((reinterpret_cast<uintptr_t>(msrc) | reinterpret_cast<uintptr_t>(vsrc)) & 15u) != 0) {
                         ctl.err = 1;  // never issue an unaligned bulk copy: skip this piece
                         continue;
                     }
-                    const uint32_t vrow = uint32_t(bc) * 16u;
-                    const uint32_t vbytes = vwhole ? uint32_t(w) * uint32_t(a.vs) * 16u : vrow * uint32_t(w);
+                    // a row of bc complex-FP32 values is rounded up to 16 bytes (an odd bc only
+                    // occurs in the last pass of an odd b, whose rows have a padding slot)
+                    const uint32_t vrow = (uint32_t(bc) * uint32_t(vel) + 15u) & ~15u;
+                    const uint32_t vbytes = vwhole ? uint32_t(w) * uint32_t(a.vs) * uint32_t(vel) : vrow * uint32_t(w);
                     unsigned char *mdst = tile + filled * ldm * elem;
-                    unsigned char *vdst = tile + voff + filled * ldv * 16;
+                    unsigned char *vdst = tile + voff + filled * ldv * vel;
                     if (percol) {
                         const uint32_t col = uint32_t(R) * 16u;
                         mbar_expect_tx_only(&ctl.full[s], col * uint32_t(w) + vbytes);
@@ -433,7 +458,7 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
                         bulk_g2s(vdst, vsrc, vbytes, &ctl.full[s]);
                     } else {
                         for (int j = 0; j < w; ++j)
-                            bulk_g2s(vdst + j * ldv * 16, vsrc + int64_t(j) * a.vs, vrow, &ctl.full[s]);
+                            bulk_g2s(vdst + j * ldv * vel, vsrc + int64_t(j) * a.vs, vrow, &ctl.full[s]);
                     }
                     filled += w;
                     if (!f64 && (R & 1)) break;  // odd-row FP32 pieces may end off a 16-byte boundary
@@ -458,7 +483,8 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
             }
             const int w = ctl.w[s];
             if (w < 0 || *abort_flag) break;
-            if (tm.nrt > 0) consume<S, NRT, NTL>(acc, tm, smem + s * STAGE_BYTES, w, voff, R, ldm, bc, ldv, g, tq, sgn);
+            if (tm.nrt > 0)
+                consume<S, NRT, NTL, V>(acc, tm, smem + s * STAGE_BYTES, w, voff, R, ldm, bc, ldv, g, tq, sgn);
             __syncwarp();
             if (lane == 0) mbar_arrive(&ctl.empty[s]);
         }
@@ -507,6 +533,17 @@ __device__ __forceinline__ void rows_body(const RowArgs<S> &a, const int32_t *no
             v.y += p.y;
         }
         const int col = a.q0 + qq;
+        if constexpr (!std::is_same<V, double2>::value) {
+            if (!scatter) {  // complex-FP32 arena rows
+                V *d = vec_dst<V>(a) + (a.g_out[o] + i) * a.vs + col;
+                if (a.accumulate) {
+                    const V old = *d;
+                    v = make_double2(double(old.x) + v.x, double(old.y) + v.y);
+                }
+                *d = V{float(v.x), float(v.y)};
+                continue;
+            }
+        }
         if (STAGE == STAGE_UP || STAGE == STAGE_COUPLE || (STAGE == STAGE_GATHER && !scatter)) {
             double2 *d = STAGE == STAGE_UP       ? (a.coef_out ? a.coef_out : a.coef) + (a.cptr[o] + i) * a.vs + col
                          : STAGE == STAGE_COUPLE ? a.dst + (a.cptr_out[o] + i) * a.vs + col
@@ -545,8 +582,11 @@ NCA_ROWS_KERNEL(k_rows_up, STAGE_UP)
 NCA_ROWS_KERNEL(k_rows_couple, STAGE_COUPLE)
 NCA_ROWS_KERNEL(k_rows_down, STAGE_DOWN)
 NCA_ROWS_KERNEL(k_rows_leaves, STAGE_LEAVES)
-NCA_ROWS_KERNEL(k_rows_gather, STAGE_GATHER)
 #undef NCA_ROWS_KERNEL
+template <typename S, int NRT, int NTL, typename V>
+__global__ void __launch_bounds__(NT, NRT * NTL <= 2 ? 3 : 1) k_rows_gather(RowArgs<S> a, const int32_t *nodes) {
+    rows_body<S, STAGE_GATHER, NRT, NTL, V>(a, nodes);
+}
 
 size_t rows_smem_bytes() { return size_t(NSTAGE) * STAGE_BYTES; }
 
@@ -558,6 +598,18 @@ __global__ void k_gather(const double2 *x, int64_t ldx, const int32_t *perm, int
         const int64_t i = e / b;
         const int q = int(e % b);
         xt[i * vs + q] = x[perm[i] + q * ldx];
+    }
+}
+
+__global__ void k_gather_to_f32(const double2 *x, int64_t ldx, const int32_t *perm, int64_t n, int b, int vs,
+                                float2 *xt) {
+    const int64_t total = n * b;
+    for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+         e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = e / b;
+        const int q = int(e % b);
+        const double2 v = x[perm[i] + q * ldx];
+        xt[i * vs + q] = make_float2(float(v.x), float(v.y));
     }
 }
 
@@ -599,7 +651,7 @@ void launch_tiles(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStre
         launch_one<S>(k_rows_down<S, NRT, NTL>, a, nodes, count, s, sm, priority);
         break;
     case STAGE_GATHER:
-        launch_one<S>(k_rows_gather<S, NRT, NTL>, a, nodes, count, s, sm, priority);
+        launch_one<S>(k_rows_gather<S, NRT, NTL, double2>, a, nodes, count, s, sm, priority);
         break;
     default:
         launch_one<S>(k_rows_leaves<S, NRT, NTL>, a, nodes, count, s, sm, priority);
@@ -641,12 +693,17 @@ template void launch_rows<float2>(const RowArgs<float2> &, const int32_t *, int,
 namespace {
 __device__ __forceinline__ double2 widen(double2 v) { return v; }
 __device__ __forceinline__ double2 widen(float2 v) { return make_double2(v.x, v.y); }
+template <typename T>
+__device__ __forceinline__ T narrow(double2 v) {
+    if constexpr (std::is_same<T, float2>::value) return make_float2(float(v.x), float(v.y));
+    else return v;
+}
 
 // One warp per output of R <= 64 rows. RG = lanes per row group (a power of two >= min(R, 32));
 // the 32 / RG column groups of the warp take the segment columns round robin and are summed by
 // shuffles at the end; with R > 32 every lane keeps two rows. QB right-hand sides per pass; U
 // columns per step, their loads issued together so that one memory round trip serves U columns.
-template <typename S, int QB, int U>
+template <typename S, int QB, int U, typename VT>
 __global__ void __launch_bounds__(256) k_gather_small(RowArgs<S> a, const int32_t *nodes, int count) {
     const int lane = threadIdx.x & 31;
     const int wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -670,7 +727,7 @@ __global__ void __launch_bounds__(256) k_gather_small(RowArgs<S> a, const int32_
             const int64_t mo = a.g_moff[e];
             const S *M = mo >= 0 ? a.M + mo : a.M2 + (-1 - mo);
             const int w = a.g_w[e];
-            const double2 *V = a.src + a.g_voff[e] * a.vs + a.q0 + qb;
+            const VT *V = vec_src<VT>(a) + a.g_voff[e] * a.vs + a.q0 + qb;
             for (int j0 = cg; j0 < w; j0 += U * CG) {
                 double2 m0[U], m1[U], x[U][QB];
 #pragma unroll
@@ -681,7 +738,7 @@ __global__ void __launch_bounds__(256) k_gather_small(RowArgs<S> a, const int32_
                     m1[u] = in && two && r0 + 32 < R ? widen(M[r0 + 32 + int64_t(j) * R]) : make_double2(0.0, 0.0);
 #pragma unroll
                     for (int q = 0; q < QB; ++q)
-                        x[u][q] = in && q < nq ? V[int64_t(j) * a.vs + q] : make_double2(0.0, 0.0);
+                        x[u][q] = in && q < nq ? widen(V[int64_t(j) * a.vs + q]) : make_double2(0.0, 0.0);
                 }
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
@@ -731,12 +788,12 @@ __global__ void __launch_bounds__(256) k_gather_small(RowArgs<S> a, const int32_
                     }
                     *yp = out;
                 } else {
-                    double2 *d = a.dst + (a.g_out[o] + i) * a.vs + col;
+                    VT *d = vec_dst<VT>(a) + (a.g_out[o] + i) * a.vs + col;
                     if (a.accumulate) {
-                        const double2 old = *d;
+                        const double2 old = widen(*d);
                         v = make_double2(old.x + v.x, old.y + v.y);
                     }
-                    *d = v;
+                    *d = narrow<VT>(v);
                 }
             }
         }
@@ -744,20 +801,21 @@ __global__ void __launch_bounds__(256) k_gather_small(RowArgs<S> a, const int32_
 }
 }  // namespace
 
-template <typename S>
+template <typename S, typename VT>
 void launch_gather_small(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
     if (count <= 0) return;
     const int grid = (count + 7) / 8;
     if (a.bc <= 1)
-        k_gather_small<S, 1, 8><<<grid, 256, 0, s>>>(a, nodes, count);
+        k_gather_small<S, 1, 8, VT><<<grid, 256, 0, s>>>(a, nodes, count);
     else if (a.bc <= 4)
-        k_gather_small<S, 4, 2><<<grid, 256, 0, s>>>(a, nodes, count);
+        k_gather_small<S, 4, 2, VT><<<grid, 256, 0, s>>>(a, nodes, count);
     else
-        k_gather_small<S, 8, 1><<<grid, 256, 0, s>>>(a, nodes, count);
+        k_gather_small<S, 8, 1, VT><<<grid, 256, 0, s>>>(a, nodes, count);
 }
 
-template void launch_gather_small<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
-template void launch_gather_small<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+template void launch_gather_small<double2, double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
+template void launch_gather_small<float2, double2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+template void launch_gather_small<float2, float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
 
 namespace {
 constexpr int TINY_WARPS = 4;       // warps (independent output streams) per CTA
@@ -796,7 +854,7 @@ struct TinyOut {
 // consume). The descriptors of the next two outputs are loaded ahead into registers, so that
 // issuing a chunk waits on no global load. Outputs are written from the accumulators when their
 // last chunk is done (no atomics, fixed order).
-template <typename S, int NRT, int NTL>
+template <typename S, int NRT, int NTL, typename VT>
 __global__ void __launch_bounds__(TINY_WARPS * 32) k_gather_tiny(RowArgs<S> a, const int32_t *nodes, int count) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -808,7 +866,7 @@ __global__ void __launch_bounds__(TINY_WARPS * 32) k_gather_tiny(RowArgs<S> a, c
     const int stride = gridDim.x * TINY_WARPS;
     const double sgn = a.conj ? -1.0 : 1.0;
     const bool scatter = a.y != nullptr;
-    constexpr int elem = int(sizeof(S));
+    constexpr int elem = int(sizeof(S)), vel = int(sizeof(VT));
     // the output sequence of this warp: positions first + j * stride
     const int first = blockIdx.x * TINY_WARPS + warp;
     auto head = [&](int j, TinyOut &d) {  // uniform fields of output j
@@ -832,10 +890,10 @@ __global__ void __launch_bounds__(TINY_WARPS * 32) k_gather_tiny(RowArgs<S> a, c
     // vector rows (stride ldv) from voff; wcap columns, a multiple of 4 when more than 4 fit
     auto layout = [&](int rows, int &ldm, int &wcap, int &voff) {
         ldm = conflict_free(rows);
-        wcap = TINY_STAGE / (ldm * elem + ldv * 16);
+        wcap = TINY_STAGE / (ldm * elem + ldv * vel);
         if (wcap > 4) wcap &= ~3;
         voff = (wcap * ldm * elem + 15) & ~15;
-        while (wcap > 1 && voff + wcap * ldv * 16 > TINY_STAGE) {  // the 16-byte rounding of voff
+        while (wcap > 1 && voff + wcap * ldv * vel > TINY_STAGE) {  // the 16-byte rounding of voff
             --wcap;
             voff = (wcap * ldm * elem + 15) & ~15;
         }
@@ -861,7 +919,7 @@ __global__ void __launch_bounds__(TINY_WARPS * 32) k_gather_tiny(RowArgs<S> a, c
         int ldm, wcap, voff;
         layout(R, ldm, wcap, voff);
         S *Ms = reinterpret_cast<S *>(b);
-        double2 *Vs = reinterpret_cast<double2 *>(b + voff);
+        VT *Vs = reinterpret_cast<VT *>(b + voff);
         const int rp = pow2_at_least(R);
         int rs = 0;
         while (rp >> (rs + 1)) ++rs;  // log2 of rp
@@ -885,7 +943,7 @@ __global__ void __launch_bounds__(TINY_WARPS * 32) k_gather_tiny(RowArgs<S> a, c
                 const int r = k & (rp - 1), cc = k >> rs;
                 if (r < R) cp_async(Ms + (cW + cc) * ldm + r, msrc + int64_t(cc) * R + r);
             }
-            const double2 *vsrc = a.src + (vo + c0) * a.vs + a.q0;
+            const VT *vsrc = vec_src<VT>(a) + (vo + c0) * a.vs + a.q0;
             for (int k = lane; k < (w << bs); k += 32) {
                 const int q = k & (bcp - 1), rr = k >> bs;
                 if (q < bc) cp_async(Vs + (cW + rr) * ldv + q, vsrc + int64_t(rr) * a.vs + q);
@@ -925,7 +983,7 @@ __global__ void __launch_bounds__(TINY_WARPS * 32) k_gather_tiny(RowArgs<S> a, c
         tm.init_single(cR);
         int ldm, wcap, voff;
         layout(cR, ldm, wcap, voff);
-        consume<S, NRT, NTL>(acc, tm, wbuf + (k & 1) * TINY_STAGE, cW, voff, cR, ldm, bc, ldv, g, tq, sgn);
+        consume<S, NRT, NTL, VT>(acc, tm, wbuf + (k & 1) * TINY_STAGE, cW, voff, cR, ldm, bc, ldv, g, tq, sgn);
         if (clast) {
             const int64_t gout = a.g_out[co];
 #pragma unroll
@@ -952,12 +1010,12 @@ __global__ void __launch_bounds__(TINY_WARPS * 32) k_gather_tiny(RowArgs<S> a, c
                             }
                             *yp = out;
                         } else {
-                            double2 *d = a.dst + (gout + i) * a.vs + col;
+                            VT *d = vec_dst<VT>(a) + (gout + i) * a.vs + col;
                             if (a.accumulate) {
-                                const double2 old = *d;
+                                const double2 old = widen(*d);
                                 v = make_double2(old.x + v.x, old.y + v.y);
                             }
-                            *d = v;
+                            *d = narrow<VT>(v);
                         }
                     }
             }
@@ -977,7 +1035,7 @@ __global__ void __launch_bounds__(TINY_WARPS * 32) k_gather_tiny(RowArgs<S> a, c
 // 7/8 idle and its single column per memory round trip is then no handicap
 bool gather_tiny_fits(int maxrows, int bc) { return maxrows <= 32 && bc >= 2 && bc <= 16; }
 
-template <typename S>
+template <typename S, typename VT>
 void launch_gather_tiny(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
     if (count <= 0) return;
     int dev = 0, sms = 148;
@@ -992,18 +1050,43 @@ void launch_gather_tiny(const RowArgs<S> &a, const int32_t *nodes, int count, cu
         kern<<<grid, TINY_WARPS * 32, sm, s>>>(a, nodes, count);
     };
     if (a.bc > 8) {
-        if (nrt <= 1) go(k_gather_tiny<S, 1, 2>);
-        else if (nrt <= 2) go(k_gather_tiny<S, 2, 2>);
-        else go(k_gather_tiny<S, 4, 2>);
+        if (nrt <= 1) go(k_gather_tiny<S, 1, 2, VT>);
+        else if (nrt <= 2) go(k_gather_tiny<S, 2, 2, VT>);
+        else go(k_gather_tiny<S, 4, 2, VT>);
     } else {
-        if (nrt <= 1) go(k_gather_tiny<S, 1, 1>);
-        else if (nrt <= 2) go(k_gather_tiny<S, 2, 1>);
-        else go(k_gather_tiny<S, 4, 1>);
+        if (nrt <= 1) go(k_gather_tiny<S, 1, 1, VT>);
+        else if (nrt <= 2) go(k_gather_tiny<S, 2, 1, VT>);
+        else go(k_gather_tiny<S, 4, 1, VT>);
     }
 }
 
-template void launch_gather_tiny<double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
-template void launch_gather_tiny<float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+template void launch_gather_tiny<double2, double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
+template void launch_gather_tiny<float2, double2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+template void launch_gather_tiny<float2, float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+
+// STAGE_GATHER through the streaming kernel with vectors of type VT
+template <typename S, typename VT>
+void launch_gather_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s) {
+    if (count <= 0) return;
+    const size_t sm = rows_smem_bytes();
+    const int MT = (a.maxrows + 7) / 8;
+    const int nrt = (MT + NCONS - 1) / NCONS;
+    auto go = [&](auto kern) { launch_one<S>(kern, a, nodes, count, s, sm, 0); };
+    if (a.bc > 8) {
+        if (nrt <= 1) go(k_rows_gather<S, 1, 2, VT>);
+        else if (nrt <= 2) go(k_rows_gather<S, 2, 2, VT>);
+        else go(k_rows_gather<S, 4, 2, VT>);
+    } else {
+        if (nrt <= 1) go(k_rows_gather<S, 1, 1, VT>);
+        else if (nrt <= 2) go(k_rows_gather<S, 2, 1, VT>);
+        else if (nrt <= 4) go(k_rows_gather<S, 4, 1, VT>);
+        else go(k_rows_gather<S, 8, 1, VT>);
+    }
+}
+
+template void launch_gather_rows<double2, double2>(const RowArgs<double2> &, const int32_t *, int, cudaStream_t);
+template void launch_gather_rows<float2, double2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
+template void launch_gather_rows<float2, float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
 
 namespace {
 template <typename S>

@@ -39,6 +39,10 @@ struct RowArgs {
     const double2 *src;
     double2 *coef;
     double2 *dst;
+    // STAGE_GATHER over a complex-FP32 vector arena (the kernels' VT = float2): src32 / dst32 in
+    // place of src / dst; accumulation stays FP64
+    const float2 *src32;
+    float2 *dst32;
     double2 *y;
     int64_t ldy;
     double2 alpha, beta;
@@ -62,6 +66,9 @@ int rows_capacity(int bc);  // largest output block one CTA computes for bc righ
 
 __global__ void k_gather(const double2 *x, int64_t ldx, const int32_t *perm, int64_t n, int b, int vs,
                          double2 *xt);
+// k_gather into a complex-FP32 vector buffer (x rounded to FP32)
+__global__ void k_gather_to_f32(const double2 *x, int64_t ldx, const int32_t *perm, int64_t n, int b, int vs,
+                                float2 *xt);
 int vector_stride(int b);  // row stride of the internal vector buffers for b right-hand sides
 
 // smem_bytes: dynamic shared memory of each CTA (0: rows_smem_bytes()); a larger request only
@@ -73,14 +80,17 @@ void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStrea
 
 // STAGE_GATHER for outputs of at most 64 rows: one warp per output, operands read straight from
 // global memory, complex FP64 FMA (directional products, whose outputs are many small blocks).
-template <typename S>
+template <typename S, typename VT = double2>
 void launch_gather_small(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
+// STAGE_GATHER through the streaming kernel with vectors of type VT (launch_rows: VT = double2)
+template <typename S, typename VT>
+void launch_gather_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
 
 // STAGE_GATHER for many outputs of at most 32 rows with 2..16 right-hand sides per pass: one
 // warp streams a sequence of outputs, double-buffering their block columns and vector rows in
 // shared memory with asynchronous copies, and multiplies on the FP64 tensor cores.
 bool gather_tiny_fits(int maxrows, int bc);
-template <typename S>
+template <typename S, typename VT = double2>
 void launch_gather_tiny(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
 
 // dst[doff[e] + i + j * rows[e]] = src[soff[e] + i + j * sld[e]]: sub-matrix copies into

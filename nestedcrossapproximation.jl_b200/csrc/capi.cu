@@ -1889,12 +1889,21 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
     for (const GatherStage *G : {&pr.up, &pr.couple, &pr.down, &pr.leaves})
         for (int r : G->group_maxrows)
             if (r > cap) return fail(NCA_ERR_ARG, "a leaf or basis block has more rows than one product CTA holds");
-    k_gather<<<launch_grid(pr.nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, c->side[I].perm.p, pr.nin, b, vs, arena);
+    // Complex-FP32 products keep the arena [x; coefficients] in complex FP32 too: the stages
+    // accumulate in FP64 and round each output row once, and the vector rows, which outweigh
+    // the FP32 blocks of these tiny gathers, move half the bytes.
+    float2 *arena32 = reinterpret_cast<float2 *>(arena);
+    if (precision == NCA_PREC_F64)
+        k_gather<<<launch_grid(pr.nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, c->side[I].perm.p, pr.nin, b, vs, arena);
+    else
+        k_gather_to_f32<<<launch_grid(pr.nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, c->side[I].perm.p, pr.nin, b, vs,
+                                                                             arena32);
     ++count.total;
     const bool conj = mode == 2;
     auto run = [&](auto tag) {
         using S = decltype(tag);
         constexpr bool f64 = std::is_same<S, double2>::value;
+        using VT = S;  // FP64 stores with FP64 vectors, FP32 stores with FP32 vectors
         const S *nearM = f64 ? (const S *)(mode == 0 ? c->N.p : c->NT.p) : (const S *)(mode == 0 ? c->N32.p : c->NT32.p);
         for (int q0 = 0; q0 < b; q0 += 16) {
             const int bc = std::min(16, b - q0);
@@ -1913,8 +1922,13 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
                     a.g_moff = G.moff.p;
                     a.g_w = G.w.p;
                     a.g_voff = G.voff.p;
-                    a.src = arena;
-                    a.dst = arena;
+                    if (f64) {
+                        a.src = arena;
+                        a.dst = arena;
+                    } else {
+                        a.src32 = arena32;
+                        a.dst32 = arena32;
+                    }
                     a.accumulate = accumulate;
                     if (scatter) {
                         a.y = yd;
@@ -1934,11 +1948,11 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
                     // many small outputs: one warp streams a sequence of them (up to 32 rows) or
                     // takes one (up to 64 rows); few large ones: the streaming MMA kernel
                     if (G.group_work[g] < 8192.0 && gather_tiny_fits(a.maxrows, bc))
-                        launch_gather_tiny<S>(a, G.outputs.p + G.group_ptr[g], cnt, s);
+                        launch_gather_tiny<S, VT>(a, G.outputs.p + G.group_ptr[g], cnt, s);
                     else if (a.maxrows <= 64 && G.group_work[g] < 8192.0)
-                        launch_gather_small<S>(a, G.outputs.p + G.group_ptr[g], cnt, s);
+                        launch_gather_small<S, VT>(a, G.outputs.p + G.group_ptr[g], cnt, s);
                     else
-                        launch_rows<S>(a, G.outputs.p + G.group_ptr[g], cnt, s);
+                        launch_gather_rows<S, VT>(a, G.outputs.p + G.group_ptr[g], cnt, s);
                     ++count.total;
                 }
             };
