@@ -86,9 +86,13 @@ def test_directional_against_oracle(name, make, k, tol, minvalues):
     rows = np.arange(0, nt, max(1, nt // 200))
     ref = O.dense_rows(O.Kernel(O.KIND_HELMHOLTZ, k=k, rmin=1e-12), test, trial, rows, x)
     assert relerr((A @ x)[rows], ref) < 10 * tol
+    # complex-FP32 stores and coefficient arena: one column, an odd block, and an odd last pass
     W = N.H2Workspace(N.core(A), np.complex64)
-    X = cgauss((ns, 8), 8)
-    assert relerr(W @ X, A @ X) < 1e-5
+    for b in (1, 5, 8, 17):
+        X = cgauss((ns, b), 30 + b)
+        assert relerr(W @ X, A @ X) < 1e-5, b
+        U = cgauss((nt, b), 40 + b)
+        assert relerr(W.H @ U, A.H @ U) < 1e-5, b
 
 
 def test_directional_structure_and_limits():
