@@ -120,30 +120,55 @@ Tree build_kmeans_tree(const double *pts, int64_t n, int minvalues) {
     T.end.push_back(int32_t(n));
     T.parent.push_back(-1);
     T.level.push_back(0);
-    Splitter sp{pts, {}, {}};
-    for (size_t node = 0; node < T.begin.size(); ++node) {
-        int b = T.begin[node], e = T.end[node];
-        int cnt = e - b;
-        if (cnt > minvalues && cnt >= 2) {
-            int first = sp.split(T.perm.data() + b, cnt);
-            T.firstchild.push_back(int32_t(T.begin.size()));
-            T.nchildren.push_back(2);
-            int bounds[3] = {b, b + first, e};
-            for (int c = 0; c < 2; ++c) {
-                T.begin.push_back(bounds[c]);
-                T.end.push_back(bounds[c + 1]);
-                T.parent.push_back(int32_t(node));
-                T.level.push_back(T.level[node] + 1);
+    // Breadth-first, one level at a time: the nodes of a level split their own ranges of perm
+    // independently on the host threads, then their children are numbered in node order.
+    const int nth = n >= 32768 ? host_threads() : 1;  // small trees: no thread start-up
+    auto parallel_for = [&](int n0, int n1, auto &&fn) {
+        std::atomic<int> cursor{n0};
+        auto work = [&]() {
+            for (;;) {
+                const int i = cursor.fetch_add(1);
+                if (i >= n1) break;
+                fn(i);
             }
-        } else {
-            T.firstchild.push_back(-1);
-            T.nchildren.push_back(0);
+        };
+        const int use = std::max(1, std::min(nth, n1 - n0));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < use; ++t) pool.emplace_back(work);
+        work();
+        for (auto &th : pool) th.join();
+    };
+    std::vector<int32_t> first;
+    for (size_t lev0 = 0, lev1 = T.begin.size(); lev0 < lev1; lev0 = lev1, lev1 = T.begin.size()) {
+        first.assign(lev1 - lev0, -1);
+        parallel_for(int(lev0), int(lev1), [&](int node) {
+            thread_local Splitter sp{nullptr, {}, {}};
+            sp.pts = pts;
+            const int b = T.begin[node], cnt = T.end[node] - b;
+            if (cnt > minvalues && cnt >= 2) first[node - lev0] = sp.split(T.perm.data() + b, cnt);
+        });
+        for (size_t node = lev0; node < lev1; ++node) {
+            const int b = T.begin[node], e = T.end[node];
+            if (first[node - lev0] >= 0) {
+                T.firstchild.push_back(int32_t(T.begin.size()));
+                T.nchildren.push_back(2);
+                const int bounds[3] = {b, b + first[node - lev0], e};
+                for (int c = 0; c < 2; ++c) {
+                    T.begin.push_back(bounds[c]);
+                    T.end.push_back(bounds[c + 1]);
+                    T.parent.push_back(int32_t(node));
+                    T.level.push_back(T.level[node] + 1);
+                }
+            } else {
+                T.firstchild.push_back(-1);
+                T.nchildren.push_back(0);
+            }
         }
     }
     T.nnodes = int(T.begin.size());
     T.center.resize(3 * size_t(T.nnodes));
     T.radius.resize(T.nnodes);
-    for (int node = 0; node < T.nnodes; ++node) {
+    parallel_for(0, T.nnodes, [&](int node) {
         double s[3] = {0, 0, 0};
         for (int i = T.begin[node]; i < T.end[node]; ++i)
             for (int d = 0; d < 3; ++d) s[d] += pts[3 * int64_t(T.perm[i]) + d];
@@ -154,7 +179,7 @@ Tree build_kmeans_tree(const double *pts, int64_t n, int minvalues) {
         for (int i = T.begin[node]; i < T.end[node]; ++i)
             m = std::max(m, dist2(pts + 3 * int64_t(T.perm[i]), c));
         T.radius[node] = std::sqrt(m);
-    }
+    });
     T.nlevels = T.level.back() + 1;
     T.levelptr.assign(T.nlevels + 1, T.nnodes);
     for (int node = T.nnodes - 1; node >= 0; --node) T.levelptr[T.level[node]] = node;
