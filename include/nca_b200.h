@@ -246,6 +246,12 @@ int32_t nca_workspace_set_profiling(nca_workspace *ws, int32_t on);
  * because the graph loses the overlap of the far-field sweeps with the near field (measured on the
  * 65,536-point sphere: 1.53 ms per step with graphs, 1.46 ms without). */
 int32_t nca_workspace_set_graphs(nca_workspace *ws, int32_t on);
+/* Schedule autotuner: times the product (mode, precision, nrhs columns, on zero device arrays of
+ * the workspace's own) under each schedule — near field beside the far-field sweeps or after
+ * them, with or without CUDA-graph replay — and keeps the fastest for the workspace. choice
+ * (nullable) receives bit 0 = overlap, bit 1 = graphs. Results do not depend on the schedule
+ * beyond the rounding of the final sum (overlap) and are bitwise equal with and without graphs. */
+int32_t nca_workspace_autotune(nca_workspace *ws, int32_t mode, int32_t precision, int64_t nrhs, int32_t *choice);
 int32_t nca_workspace_stage_times(const nca_workspace *ws, double *seconds, int32_t *launches,
                                   int32_t nstages);
 

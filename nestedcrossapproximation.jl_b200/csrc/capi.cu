@@ -242,14 +242,15 @@ struct nca_workspace {
     // launches: a call whose arguments were seen in one of the last few calls is captured once,
     // later identical calls launch the graph. Buffer reallocation (gen) invalidates every graph.
     struct GraphKey {
-        int mode, precision, b, far, near, profiling;
+        int mode, precision, b, far, near, profiling, overlap;
         const void *x, *y;
         int64_t ldx, ldy;
         double ar, ai, br, bi;
         uint64_t gen;
         bool operator==(const GraphKey &o) const {
             return mode == o.mode && precision == o.precision && b == o.b && far == o.far && near == o.near &&
-                   profiling == o.profiling && x == o.x && y == o.y && ldx == o.ldx && ldy == o.ldy && ar == o.ar &&
+                   profiling == o.profiling && overlap == o.overlap && x == o.x && y == o.y && ldx == o.ldx &&
+                   ldy == o.ldy && ar == o.ar &&
                    ai == o.ai && br == o.br && bi == o.bi && gen == o.gen;
         }
     };
@@ -263,6 +264,7 @@ struct nca_workspace {
     std::vector<GraphKey> seen;    // the last few eager calls' arguments
     uint64_t gen = 0;
     bool use_graphs = false;
+    bool use_overlap = true;  // near field beside the sweeps (second stream)
 };
 
 namespace {
@@ -2051,9 +2053,9 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     ProductLaunches count;
     // graph replay of repeated products on device arrays
     const bool graphable = ws->use_graphs && memspace == 1 && !tangent;
-    const nca_workspace::GraphKey key{mode,     precision, b,       int(ws->far), int(ws->near), int(ws->profiling),
-                                      x,        y,         ldx,     ldy,          alpha.x,       alpha.y,
-                                      beta.x,   beta.y,    ws->gen};
+    const nca_workspace::GraphKey key{mode,    precision, b,   int(ws->far), int(ws->near), int(ws->profiling),
+                                      int(ws->use_overlap),         x,   y,            ldx,           ldy,
+                                      alpha.x, alpha.y,   beta.x, beta.y,     ws->gen};
     nca_workspace::Graph *graph = nullptr;
     bool capture = false;
     if (graphable) {
@@ -2076,7 +2078,7 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
                 return st;
         } else {
             ProductStreams ps;
-            ps.aux = ws->aux;
+            ps.aux = ws->use_overlap ? ws->aux : nullptr;
             ps.fork = ws->fork;
             ps.join = ws->join;
             ps.priority = ws->aux_priority;
@@ -3064,6 +3066,57 @@ void nca_workspace_destroy(nca_workspace *ws) {
         if (e) cudaEventDestroy(e);
     if (ws->error_host) cudaFreeHost(ws->error_host);
     delete ws;
+}
+
+int32_t nca_workspace_autotune(nca_workspace *ws, int32_t mode, int32_t precision, int64_t nrhs, int32_t *choice) {
+    if (!ws) return fail(NCA_ERR_ARG, "null workspace");
+    bool expected = false;
+    if (!ws->busy.compare_exchange_strong(expected, true))
+        return fail(NCA_ERR_BUSY, "ConcurrentWorkspaceError: the workspace is in use by another matrix-vector product");
+    int st = guarded([&] {
+        nca_core *c = ws->core;
+        if (nrhs < 1) return fail(NCA_ERR_ARG, "nrhs must be positive");
+        if (mode < 0 || mode > 2) return fail(NCA_ERR_ARG, "mode must be 0 (N), 1 (T) or 2 (C)");
+        CK(cudaSetDevice(c->device));
+        const int in = mode == 0 ? 1 : 0, out = 1 - in;
+        const int64_t nin = c->side[in].npts, nout = c->side[out].npts;
+        DBuf<double2> xd, yd;
+        xd.alloc(size_t(nin) * nrhs);
+        yd.alloc(size_t(nout) * nrhs);
+        xd.zero(ws->stream);
+        yd.zero(ws->stream);
+        const bool profiling = ws->profiling;
+        ws->profiling = false;
+        // schedules: (overlap of the near field with the sweeps, CUDA-graph replay); directional
+        // cores have no second stream
+        const int nconf = c->dir ? 2 : 4;
+        double best = 1e30;
+        int arg = 0;
+        for (int k = 0; k < nconf; ++k) {
+            ws->use_overlap = c->dir ? false : (k & 1) == 0;
+            ws->use_graphs = (k & 2) != 0 || (c->dir && k == 1);
+            drop_graphs(ws);
+            double tsum = 0.0;
+            for (int rep = 0; rep < 8; ++rep) {
+                if (int e = apply_impl(ws, mode, precision, xd.p, nin, yd.p, nout, nrhs, make_double2(1.0, 0.0),
+                                       make_double2(0.0, 0.0), 1))
+                    return e;
+                if (rep >= 3) tsum += ws->last_seconds;  // three calls warm up (and capture a graph)
+            }
+            if (tsum < best) {
+                best = tsum;
+                arg = k;
+            }
+        }
+        ws->use_overlap = c->dir ? false : (arg & 1) == 0;
+        ws->use_graphs = (arg & 2) != 0 || (c->dir && arg == 1);
+        drop_graphs(ws);
+        ws->profiling = profiling;
+        if (choice) *choice = (ws->use_overlap ? 1 : 0) | (ws->use_graphs ? 2 : 0);
+        return int(NCA_OK);
+    });
+    ws->busy.store(false);
+    return st;
 }
 
 int32_t nca_apply(nca_workspace *ws, int32_t mode, int32_t precision, const void *x, int64_t ldx, void *y,

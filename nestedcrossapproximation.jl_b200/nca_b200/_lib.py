@@ -108,6 +108,7 @@ SIGNATURES = {
     "nca_workspace_set_profiling": (I32, [P, I32]),
     "nca_workspace_stage_times": (I32, [P, P, P, I32]),
     "nca_workspace_set_graphs": (I32, [P, I32]),
+    "nca_workspace_autotune": (I32, [P, I32, I32, I64, P]),
     "nca_blocks_aca": (I32, [P, I64, I32, P, P, I32, I32, D, I32, I32, P, P, P]),
     "nca_blocks_factors": (I32, [P, I64, I32, P, I32, P, P, P, I32, I32, P, P]),
     "nca_entries": (I32, [P, P, I64, P, I64, P, P, I64, I32, P]),

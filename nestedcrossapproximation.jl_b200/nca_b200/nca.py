@@ -364,6 +364,13 @@ class H2Workspace(LinearMap):
         launch-bound small problems)."""
         check(lib().nca_workspace_set_graphs(self._h, int(on)))
 
+    def autotune(self, mode: int = MODE_N, nrhs: int = 1):
+        """Time the product under each schedule (near field beside or after the sweeps, with or
+        without CUDA graphs) and keep the fastest; returns {"overlap": bool, "graphs": bool}."""
+        ch = C.c_int32()
+        check(lib().nca_workspace_autotune(self._h, int(mode), self.precision, int(nrhs), C.byref(ch)))
+        return {"overlap": bool(ch.value & 1), "graphs": bool(ch.value & 2)}
+
     def set_profiling(self, on: bool = True):
         """Record CUDA events around each stage of every product (see stage_times)."""
         check(lib().nca_workspace_set_profiling(self._h, int(on)))

@@ -321,3 +321,17 @@ def test_graph_replay_matches_enqueued_products(c1):
         st = W.stage_times()
         assert st["near"][1] == 1 and st["near"][0] > 0 and st["leaves"][0] > 0
     W.set_profiling(False)
+
+
+def test_autotune_keeps_results(c1):
+    """The schedule autotuner picks one of four schedules; products afterwards still match the
+    oracle (and each other bitwise across repeated calls)."""
+    test, trial, A, H = c1
+    N = _n()
+    W = N.H2Workspace(N.core(A), max_nrhs=8)
+    choice = W.autotune(0, 8)
+    assert set(choice) == {"overlap", "graphs"}
+    X = cgauss((1024, 8), 90)
+    assert relerr(W @ X, H.apply(X, 0)) < REL
+    assert np.array_equal(W @ X, W @ X)
+    assert relerr(W.H @ X, H.apply(X, 2)) < REL
