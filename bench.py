@@ -65,6 +65,18 @@ def rhs(n, b, seed=99):
     return rng.standard_normal((n, b)) + 1j * rng.standard_normal((n, b))
 
 
+def max_over_ranks(x, device):
+    """The largest x over the ranks of the job (replicas time their own work; the job's time is the
+    slowest rank's). x itself when no process group is running or it has one rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def store_entries(info):
     return (info["near_entries"] + info["coupling_entries"] + info["transfer_entries_test"] +
             info["transfer_entries_trial"] + info["basis_entries_test"] + info["basis_entries_trial"])
@@ -203,11 +215,7 @@ def measure_chosen(N, L, core, ws64, X, Xd, Yd, n, b, args, world, local, info, 
         step()
     e1.record()
     torch.cuda.synchronize()
-    el = e0.elapsed_time(e1) * 1e-3
-    if world > 1:
-        t = torch.tensor([el], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el = float(t.item())
+    el = max_over_ranks(e0.elapsed_time(e1) * 1e-3, f"cuda:{local}")
     # error of the forward product against the FP64 product and against dense rows
     Y64 = torch.zeros_like(Yd)
     for W, Y in ((ws64, Y64), (ws, Y32)):
@@ -708,11 +716,7 @@ def main():
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    elapsed = e0.elapsed_time(e1) * 1e-3
-    if world > 1:
-        t = torch.tensor([elapsed], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(e0.elapsed_time(e1) * 1e-3, f"cuda:{local}")
     step_bytes = 2 * product_bytes(info, b, 8 if f32 else E)
     value = world * step_bytes * args.steps / elapsed / 1e9
     # end to end: the same products through the C ABI with pinned host buffers
@@ -729,11 +733,7 @@ def main():
         for mode in (0, 2):
             N._lib.check(L.nca_apply(ws._h, mode, prec, C.c_void_p(Xh.data_ptr()), n, C.c_void_p(Yh.data_ptr()), n,
                                      b, 1.0, 0.0, 0.0, 0.0, 0))
-    e2e_el = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_el], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_el = float(t.item())
+    e2e_el = max_over_ranks(time.perf_counter() - t0, f"cuda:{local}")
     e2e = {"value": world * step_bytes * args.steps / e2e_el / 1e9, "unit": "GB/s",
            "h2d_bytes_per_step": 2 * n * b * E, "d2h_bytes_per_step": 2 * n * b * E}
     err = dense_rows_error(N, pts, core, ws, X) if rank == 0 else None
