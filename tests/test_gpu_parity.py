@@ -335,3 +335,33 @@ def test_autotune_keeps_results(c1):
     assert relerr(W @ X, H.apply(X, 0)) < REL
     assert np.array_equal(W @ X, W @ X)
     assert relerr(W.H @ X, H.apply(X, 2)) < REL
+
+
+def test_two_workspaces_on_two_threads(c1):
+    """Workspaces of one core run products at the same time from two host threads (each its own
+    streams and buffers, the core read-only): every result equals the one computed alone."""
+    import threading
+    test, trial, A, H = c1
+    N = _n()
+    X = [cgauss((1024, 5), 100 + i) for i in range(2)]
+    ref = [H.apply(x, 0) for x in X]
+    W = [N.H2Workspace(N.core(A), max_nrhs=5) for _ in range(2)]
+    out = [None, None]
+    err = []
+
+    def work(i):
+        try:
+            for _ in range(20):
+                out[i] = W[i] @ X[i]
+        except Exception as e:  # reported below
+            err.append(e)
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not err
+    for i in range(2):
+        assert relerr(out[i], ref[i]) < REL
+        assert np.array_equal(out[i], W[i] @ X[i])
