@@ -238,7 +238,8 @@ int32_t nca_workspace_set_parts(nca_workspace *ws, int32_t far, int32_t near);
  * leaf bases (stage 5); with only one part present, stage 5 is the whole leaf launch and
  * stage 4 is empty. Stages 1-3 and 4 overlap in time. */
 int32_t nca_workspace_set_profiling(nca_workspace *ws, int32_t on);
-/* CUDA-graph replay (off by default): an nca_apply on device arrays (memspace 1) whose arguments
+/* CUDA-graph replay (no counterpart in the reference, whose products run on the CPU; off by
+ * default): an nca_apply on device arrays (memspace 1) whose arguments
  * (mode, precision, pointers, leading dimensions, nrhs, alpha, beta, parts, profiling) equal one
  * of the workspace's last few calls is captured once into a CUDA graph, and later identical calls
  * launch that graph instead of enqueueing every stage. Results are bitwise those of the enqueued
@@ -246,7 +247,8 @@ int32_t nca_workspace_set_profiling(nca_workspace *ws, int32_t on);
  * because the graph loses the overlap of the far-field sweeps with the near field (measured on the
  * 65,536-point sphere: 1.53 ms per step with graphs, 1.46 ms without). */
 int32_t nca_workspace_set_graphs(nca_workspace *ws, int32_t on);
-/* Schedule autotuner: times the product (mode, precision, nrhs columns, on zero device arrays of
+/* Schedule autotuner (no counterpart in the reference): times the product (mode, precision, nrhs
+ * columns, on zero device arrays of
  * the workspace's own) under each schedule — near field beside the far-field sweeps or after
  * them, with or without CUDA-graph replay — and keeps the fastest for the workspace. choice
  * (nullable) receives bit 0 = overlap, bit 1 = graphs. Results do not depend on the schedule
