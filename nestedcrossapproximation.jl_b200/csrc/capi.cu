@@ -8,6 +8,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -691,6 +692,17 @@ int64_t build_near(nca_core *c, cudaStream_t s) {
     return near_entries;
 }
 
+// Raises k_level_compress's dynamic shared-memory limit on the current device to at least sm and
+// never lowers it, so that a build on another host thread keeps the limit its launches rely on.
+void level_smem_at_least(size_t sm) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, k_level_compress));
+    if (sm > size_t(fa.maxDynamicSharedSizeBytes))
+        CK(cudaFuncSetAttribute(k_level_compress, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+}
+
 void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int64_t ns,
                 const nca_build_opts *o) {
     const int maxrank = c->maxrank;
@@ -781,7 +793,7 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
             maxsm = std::max(maxsm, level_smem_bytes(lv_mcap[l], lv_ncap[l]));
         if (maxsm > size_t(kMaxSmem))
             throw Failure(NCA_ERR_ARG, "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
-        CK(cudaFuncSetAttribute(k_level_compress, cudaFuncAttributeMaxDynamicSharedMemorySize, int(maxsm)));
+        level_smem_at_least(maxsm);
         for (size_t l = 0; l + 1 < lv_ptr.size(); ++l) {
             int cnt = lv_ptr[l + 1] - lv_ptr[l];
             if (cnt == 0) continue;
@@ -1021,6 +1033,31 @@ struct StageBuilder {
     }
 };
 
+// fn(0) and fn(1) on two host threads (the caller and one more, both on the core's device); the
+// first failure, with its singular-matrix record, is rethrown on the caller once both are done
+template <typename F>
+void both_sides(int device, F fn) {
+    std::exception_ptr err[2];
+    int sing[2][4] = {};
+    auto run = [&](int sd) {
+        try {
+            if (sd) CK(cudaSetDevice(device));
+            fn(sd);
+        } catch (...) {
+            err[sd] = std::current_exception();
+            std::copy(g_singular, g_singular + 4, sing[sd]);
+        }
+    };
+    std::thread other(run, 1);
+    run(0);
+    other.join();
+    for (int sd = 0; sd < 2; ++sd)
+        if (err[sd]) {
+            set_singular(sing[sd][0], sing[sd][1], sing[sd][2], sing[sd][3]);
+            std::rethrow_exception(err[sd]);
+        }
+}
+
 void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_build_opts *o, const nca::Wideband &wb) {
     const int maxrank = c->maxrank;
     auto h0 = std::chrono::steady_clock::now();
@@ -1035,7 +1072,15 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     const nca::Partition &P = c->part;
     auto D = std::make_unique<DirCore>();
     const double *pts[2] = {tp, sp};
-    for (int sd = 0; sd < 2; ++sd) {
+    // the two sides (and later the two orientations of the gather plans) are independent: each
+    // runs on its own host thread and stream
+    cudaStream_t s1;
+    CK(cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking));
+    StreamGuard sg1{s1};
+    const cudaStream_t ss[2] = {s, s1};
+    CK(cudaStreamSynchronize(s));
+    both_sides(c->device, [&](int sd) {
+        const cudaStream_t s = ss[sd];
         DirItems &d = D->side[sd];
         d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
                                   sd == 0 ? P.farnodes : P.tfarnodes, wb);
@@ -1048,7 +1093,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             ffnodes);
         device_farpivots(c->tree[sd], pts[sd], c->tree[1 - sd], c->side[1 - sd], ni, ffptr, ffnodes,
                          &d.plan.item_node, maxrank, s, d.h_fpptr, d.fpptr, d.fpidx, nullptr);
-    }
+    });
     auto h1 = std::chrono::steady_clock::now();
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
@@ -1060,12 +1105,13 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             cudaEventDestroy(b);
         }
     } eg{ev0, ev1};
-    DBuf<int32_t> status;
-    status.alloc(4);
     CK(cudaEventRecord(ev0, s));
     std::vector<std::vector<int32_t>> bylevel[2];
     int64_t basis_entries[2] = {0, 0}, transfer_entries[2] = {0, 0};
-    for (int sd = 0; sd < 2; ++sd) {
+    both_sides(c->device, [&](int sd) {
+        const cudaStream_t s = ss[sd];
+        DBuf<int32_t> status;
+        status.alloc(4);
         DirItems &d = D->side[sd];
         const nca::DirSide &pl = d.plan;
         const nca::Tree &T = c->tree[sd];
@@ -1142,7 +1188,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             const size_t sm = level_smem_bytes(mc, nc);
             if (sm > size_t(kMaxSmem))
                 throw Failure(NCA_ERR_ARG, "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
-            CK(cudaFuncSetAttribute(k_level_compress, cudaFuncAttributeMaxDynamicSharedMemorySize, int(std::max<size_t>(sm, 16))));
+            level_smem_at_least(sm);
             DBuf<double2> chunk;
             chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
             dlvoff.upload(lvoff, s);
@@ -1227,7 +1273,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         d.XT.alloc(d.X.n);
         launch_transpose_blocks<double2>(d.X.p, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, ni, d.XT.p, s);
         CK(cudaGetLastError());
-    }
+        CK(cudaStreamSynchronize(s));
+    });
     // far pairs (test CSR grouped by test direction) and their items on both sides
     const nca::DirSide &pt = D->side[0].plan, &ps = D->side[1].plan;
     const int64_t npairs = int64_t(pt.farnodes.size());
@@ -1310,9 +1357,11 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         CK(cudaStreamSynchronize(s));
     }
     const int64_t near_entries = build_near(c, s);
+    CK(cudaStreamSynchronize(s));
     const std::vector<int64_t> h_ntoff = download_now(c->ntoff, P.tnearnodes.size() + 1);
     // gather plans of both orientations
-    for (int m = 0; m < 2; ++m) {
+    both_sides(c->device, [&](int m) {
+        const cudaStream_t s = ss[m];
         const int I = m == 0 ? 1 : 0, O = 1 - I;
         DirItems &di = D->side[I], &dout = D->side[O];
         const nca::Tree &TI = c->tree[I], &TO = c->tree[O];
@@ -1439,7 +1488,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             B.end_group();
             B.finish(pr.leaves, dout.X.p, s);
         }
-    }
+        CK(cudaStreamSynchronize(s));
+    });
     // the per-item operators live on in the stage stores (directional cores have no node exports)
     for (DirItems &d : D->side) {
         d.X.release();

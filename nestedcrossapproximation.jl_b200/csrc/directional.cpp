@@ -273,6 +273,24 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
         std::copy(pmap[node].begin(), pmap[node].end(), D.chdirmap.begin() + D.chdirptr[node]);
     }
     D.dirfarptr[ni] = farptr[nn];
+    // the inverse of the parent-to-child maps: for every item the parent directions mapped onto it
+    D.invptr.assign(ni + 1, 0);
+    for (int node = 0; node < nn; ++node) {
+        const int nown = D.dirptr[node + 1] - D.dirptr[node];
+        for (int i = D.chdirptr[node]; i < D.chdirptr[node + 1]; ++i)
+            if (D.chdirmap[i] >= 1 && D.chdirmap[i] <= nown) ++D.invptr[D.dirptr[node] + D.chdirmap[i]];
+    }
+    for (int item = 0; item < ni; ++item) D.invptr[item + 1] += D.invptr[item];
+    D.invidx.resize(D.invptr[ni]);
+    {
+        std::vector<int32_t> fill(D.invptr.begin(), D.invptr.end() - 1);
+        for (int node = 0; node < nn; ++node) {
+            const int nown = D.dirptr[node + 1] - D.dirptr[node];
+            for (int i = D.chdirptr[node]; i < D.chdirptr[node + 1]; ++i)
+                if (D.chdirmap[i] >= 1 && D.chdirmap[i] <= nown)
+                    D.invidx[fill[D.dirptr[node] + D.chdirmap[i] - 1]++] = i - D.chdirptr[node] + 1;
+        }
+    }
     // basis items and the children's items of nested ones
     D.item_basis.resize(ni);
     D.item_chptr.assign(ni + 1, 0);
@@ -325,13 +343,20 @@ void item_farfield(const Tree &T, const DirSide &D, int item, std::vector<int32_
         return;
     }
     append(item);
+    // idcs: the 1-based local directions of cur on the chain; next: the parent directions that map
+    // onto any of them, ascending (each parent direction maps onto one child direction, so the
+    // inverse lists are disjoint and their sorted union is the reference's scan in order)
     std::vector<int32_t> idcs{item - D.dirptr[node] + 1}, next;
     for (int cur = node; T.parent[cur] >= 0; cur = T.parent[cur]) {
         const int p = T.parent[cur];
         next.clear();
-        for (int i = D.chdirptr[cur]; i < D.chdirptr[cur + 1]; ++i)
-            if (std::find(idcs.begin(), idcs.end(), D.chdirmap[i]) != idcs.end()) next.push_back(i - D.chdirptr[cur] + 1);
+        for (int32_t c : idcs) {
+            const int it = D.dirptr[cur] + c - 1;
+            next.insert(next.end(), D.invidx.begin() + D.invptr[it], D.invidx.begin() + D.invptr[it + 1]);
+        }
+        std::sort(next.begin(), next.end());
         for (int32_t pi : next) append(D.dirptr[p] + pi - 1);
+        if (next.empty()) break;  // no ancestor direction maps onto the chain any more
         idcs.swap(next);
     }
 }

@@ -69,6 +69,7 @@ struct DirSide {
     std::vector<double> dirvec;             // item -> unit direction (zero for low frequency)
     std::vector<int32_t> dirfarptr;         // item -> its own far nodes in farnodes (nitems + 1)
     std::vector<int32_t> chdirptr, chdirmap;  // node -> for each parent direction its own (1-based)
+    std::vector<int32_t> invptr, invidx;      // item -> the parent directions (1-based, ascending) mapped onto it
     std::vector<int32_t> item_node, item_basis;
     std::vector<int32_t> item_chptr, item_chidx;  // nested items: the children's items in child order
 };
