@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <atomic>
 #include <chrono>
@@ -72,6 +73,25 @@ struct DBuf {
         if (n) CK(cudaMemcpyAsync(h.data(), p, sizeof(T) * n, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         return h;
+    }
+};
+
+// uploads v into the scratch buffer b, reallocating only when b is too small
+template <typename T>
+void upload_reuse(DBuf<T> &b, const std::vector<T> &v, cudaStream_t s) {
+    if (!b.p || v.size() > b.n) b.alloc(v.size());
+    if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+}
+
+// page-locked host array (downloads that need no staging copy)
+template <typename T>
+struct PinnedBuf {
+    T *p = nullptr;
+    explicit PinnedBuf(size_t n) { CK(cudaMallocHost(&p, sizeof(T) * std::max<size_t>(n, 1))); }
+    PinnedBuf(const PinnedBuf &) = delete;
+    PinnedBuf &operator=(const PinnedBuf &) = delete;
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
     }
 };
 
@@ -144,7 +164,7 @@ struct DevSide {
 struct DirItems {
     nca::DirSide plan;
     int nitems = 0;
-    std::vector<int32_t> h_fpptr, h_rank, h_nrows, h_piv;  // far pivots stay on the device (fpidx)
+    std::vector<int32_t> h_fpptr, h_rank, h_nrows;  // far pivots and item pivots stay on the device
     std::vector<int64_t> h_xoff, h_cptr;
     DBuf<int32_t> item_node, item_basis, item_chptr, item_chidx, fpptr, fpidx, rank, nrows, piv, cpiv;
     DBuf<int64_t> xoff;
@@ -1033,28 +1053,30 @@ struct StageBuilder {
     }
 };
 
-// fn(0) and fn(1) on two host threads (the caller and one more, both on the core's device); the
-// first failure, with its singular-matrix record, is rethrown on the caller once both are done
+// fn(0) .. fn(n - 1) on n host threads (the caller and n - 1 more, all on the core's device); the
+// first failure in task order, with its singular-matrix record, is rethrown on the caller once
+// all are done
 template <typename F>
-void both_sides(int device, F fn) {
-    std::exception_ptr err[2];
-    int sing[2][4] = {};
-    auto run = [&](int sd) {
+void on_threads(int device, int n, F fn) {
+    std::vector<std::exception_ptr> err(n);
+    std::vector<std::array<int, 4>> sing(n);
+    auto run = [&](int i) {
         try {
-            if (sd) CK(cudaSetDevice(device));
-            fn(sd);
+            if (i) CK(cudaSetDevice(device));
+            fn(i);
         } catch (...) {
-            err[sd] = std::current_exception();
-            std::copy(g_singular, g_singular + 4, sing[sd]);
+            err[i] = std::current_exception();
+            std::copy(g_singular, g_singular + 4, sing[i].begin());
         }
     };
-    std::thread other(run, 1);
+    std::vector<std::thread> pool;
+    for (int i = 1; i < n; ++i) pool.emplace_back(run, i);
     run(0);
-    other.join();
-    for (int sd = 0; sd < 2; ++sd)
-        if (err[sd]) {
-            set_singular(sing[sd][0], sing[sd][1], sing[sd][2], sing[sd][3]);
-            std::rethrow_exception(err[sd]);
+    for (auto &th : pool) th.join();
+    for (int i = 0; i < n; ++i)
+        if (err[i]) {
+            set_singular(sing[i][0], sing[i][1], sing[i][2], sing[i][3]);
+            std::rethrow_exception(err[i]);
         }
 }
 
@@ -1079,22 +1101,6 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     StreamGuard sg1{s1};
     const cudaStream_t ss[2] = {s, s1};
     CK(cudaStreamSynchronize(s));
-    both_sides(c->device, [&](int sd) {
-        const cudaStream_t s = ss[sd];
-        DirItems &d = D->side[sd];
-        d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
-                                  sd == 0 ? P.farnodes : P.tfarnodes, wb);
-        // phase 1 on the device: tree mimicry per item over the item's directional far field
-        std::vector<int64_t> ffptr;
-        std::vector<int32_t> ffnodes;
-        const int ni = int(d.plan.item_node.size());
-        parallel_csr(
-            ni, [&](int it, std::vector<int32_t> &ff) { nca::item_farfield(c->tree[sd], d.plan, it, ff); }, ffptr,
-            ffnodes);
-        device_farpivots(c->tree[sd], pts[sd], c->tree[1 - sd], c->side[1 - sd], ni, ffptr, ffnodes,
-                         &d.plan.item_node, maxrank, s, d.h_fpptr, d.fpptr, d.fpidx, nullptr);
-    });
-    auto h1 = std::chrono::steady_clock::now();
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
@@ -1106,13 +1112,27 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         }
     } eg{ev0, ev1};
     CK(cudaEventRecord(ev0, s));
-    std::vector<std::vector<int32_t>> bylevel[2];
+    std::vector<std::vector<int32_t>> bylevel[2];  // items per level, filled by each side's task
     int64_t basis_entries[2] = {0, 0}, transfer_entries[2] = {0, 0};
-    both_sides(c->device, [&](int sd) {
+    on_threads(c->device, 2, [&](int sd) {
         const cudaStream_t s = ss[sd];
+        DirItems &d = D->side[sd];
+        d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
+                                  sd == 0 ? P.farnodes : P.tfarnodes, wb);
+        {
+            // phase 1 on the device: tree mimicry per item over the item's directional far field
+            std::vector<int64_t> ffptr;
+            std::vector<int32_t> ffnodes;
+            const int ni = int(d.plan.item_node.size());
+            parallel_csr(
+                ni, [&](int it, std::vector<int32_t> &ff) { nca::item_farfield(c->tree[sd], d.plan, it, ff); },
+                ffptr, ffnodes);
+            device_farpivots(c->tree[sd], pts[sd], c->tree[1 - sd], c->side[1 - sd], ni, ffptr, ffnodes,
+                             &d.plan.item_node, maxrank, s, d.h_fpptr, d.fpptr, d.fpidx, nullptr);
+        }
+        // phase 2: the side's items, level by level
         DBuf<int32_t> status;
         status.alloc(4);
-        DirItems &d = D->side[sd];
         const nca::DirSide &pl = d.plan;
         const nca::Tree &T = c->tree[sd];
         DevSide &ds = c->side[sd];
@@ -1162,7 +1182,11 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         std::vector<int64_t> lvoff(std::max(ni, 1), 0), cpos(ni, -1);
         std::vector<std::unique_ptr<DBuf<double2>>> levelX;
         std::vector<std::vector<int32_t>> levelItems;
-        DBuf<int64_t> dlvoff;
+        // scratch reused by every level (grown, never shrunk: no device-wide frees between levels)
+        DBuf<int64_t> dlvoff, dso, ddo;
+        DBuf<int32_t> nodes, dld, dr, dc;
+        DBuf<double2> chunk;
+        PinnedBuf<int32_t> hrank(2 * size_t(std::max(ni, 1)));
         int64_t total = 0;
         for (int lev = T.nlevels - 1; lev >= 0; --lev) {
             std::vector<int32_t> items;
@@ -1189,11 +1213,9 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             if (sm > size_t(kMaxSmem))
                 throw Failure(NCA_ERR_ARG, "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
             level_smem_at_least(sm);
-            DBuf<double2> chunk;
-            chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
-            dlvoff.upload(lvoff, s);
-            DBuf<int32_t> nodes;
-            nodes.upload(items, s);
+            if (!chunk.p || size_t(bound) > chunk.n) chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
+            upload_reuse(dlvoff, lvoff, s);
+            upload_reuse(nodes, items, s);
             status.zero(s);
             a.X = chunk.p;
             a.xoff = dlvoff.p;
@@ -1209,7 +1231,10 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                                                     " of them are linearly independent");
             }
             if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: level block exceeds its planned capacity");
-            const std::vector<int32_t> rk = download_now(d.rank, size_t(ni)), nr = download_now(d.nrows, size_t(ni));
+            CK(cudaMemcpyAsync(hrank.p, d.rank.p, sizeof(int32_t) * ni, cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(hrank.p + ni, d.nrows.p, sizeof(int32_t) * ni, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            const int32_t *rk = hrank.p, *nr = hrank.p + ni;
             // compact this level: exact m x r blocks, back to back
             std::vector<int64_t> soff, doff;
             std::vector<int32_t> sld, crows, ccols;
@@ -1230,13 +1255,11 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             levelX.emplace_back(new DBuf<double2>());
             levelX.back()->alloc(size_t(std::max<int64_t>(lt, 1)));
             if (!soff.empty()) {
-                DBuf<int64_t> dso, ddo;
-                DBuf<int32_t> dld, dr, dc;
-                dso.upload(soff, s);
-                ddo.upload(doff, s);
-                dld.upload(sld, s);
-                dr.upload(crows, s);
-                dc.upload(ccols, s);
+                upload_reuse(dso, soff, s);
+                upload_reuse(ddo, doff, s);
+                upload_reuse(dld, sld, s);
+                upload_reuse(dr, crows, s);
+                upload_reuse(dc, ccols, s);
                 launch_copy_blocks<double2>(chunk.p, dso.p, dld.p, dr.p, dc.p, ddo.p, int64_t(soff.size()),
                                             levelX.back()->p, s);
                 CK(cudaGetLastError());
@@ -1263,7 +1286,6 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             levelX.clear();
         }
         d.xoff.upload(d.h_xoff, s);
-        d.h_piv = d.piv.download(s);
         d.h_cptr.assign(ni + 1, 0);
         for (int it = 0; it < ni; ++it) {
             d.h_cptr[it + 1] = d.h_cptr[it] + d.h_rank[it];
@@ -1275,6 +1297,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s));
     });
+    auto h1 = std::chrono::steady_clock::now();
     // far pairs (test CSR grouped by test direction) and their items on both sides
     const nca::DirSide &pt = D->side[0].plan, &ps = D->side[1].plan;
     const int64_t npairs = int64_t(pt.farnodes.size());
@@ -1285,17 +1308,25 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         for (size_t it = 0; it < pl.item_node.size(); ++it)
             for (int q = pl.dirfarptr[it]; q < pl.dirfarptr[it + 1]; ++q) item_of_pos[sd][q] = int32_t(it);
     }
-    const int64_t ntn_nodes = c->tree[0].nnodes;
-    std::unordered_map<int64_t, int32_t> trialpos;  // (trial node, test node) -> position in the trial far lists
-    trialpos.reserve(size_t(npairs) * 2 + 1);
-    for (int sn = 0; sn < c->tree[1].nnodes; ++sn)
-        for (int q = ps.farptr[sn]; q < ps.farptr[sn + 1]; ++q) trialpos[int64_t(sn) * ntn_nodes + ps.farnodes[q]] = q;
+    // (trial node, test node) -> position in the trial far lists: each trial node's list sorted by
+    // test node and searched by bisection
+    std::vector<std::pair<int32_t, int32_t>> bytest(ps.farnodes.size());
+    for (int sn = 0; sn < c->tree[1].nnodes; ++sn) {
+        for (int q = ps.farptr[sn]; q < ps.farptr[sn + 1]; ++q) bytest[q] = {ps.farnodes[q], q};
+        std::sort(bytest.begin() + ps.farptr[sn], bytest.begin() + ps.farptr[sn + 1]);
+    }
+    auto trialpos = [&](int sn, int t) {
+        const auto b = bytest.begin() + ps.farptr[sn], e = bytest.begin() + ps.farptr[sn + 1];
+        const auto it = std::lower_bound(b, e, std::make_pair(int32_t(t), INT32_MIN));
+        if (it == e || it->first != t) throw Failure(NCA_ERR_ARG, "internal: a far pair has no transpose");
+        return it->second;
+    };
     std::vector<int32_t> pair_it(npairs), pair_is(npairs);
     std::vector<int32_t> pair_of_pos(ps.farnodes.size(), -1);
     for (int t = 0; t < c->tree[0].nnodes; ++t)
         for (int e = pt.farptr[t]; e < pt.farptr[t + 1]; ++e) {
             const int sn = pt.farnodes[e];
-            const int32_t q = trialpos.at(int64_t(sn) * ntn_nodes + t);
+            const int32_t q = trialpos(sn, t);
             pair_it[e] = item_of_pos[0][e];
             pair_is[e] = item_of_pos[1][q];
             pair_of_pos[q] = e;
@@ -1359,20 +1390,33 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     const int64_t near_entries = build_near(c, s);
     CK(cudaStreamSynchronize(s));
     const std::vector<int64_t> h_ntoff = download_now(c->ntoff, P.tnearnodes.size() + 1);
-    // gather plans of both orientations
-    both_sides(c->device, [&](int m) {
-        const cudaStream_t s = ss[m];
+    // gather plans: the four stages of both orientations, each task on its own thread and stream
+    for (int m = 0; m < 2; ++m) {
         const int I = m == 0 ? 1 : 0, O = 1 - I;
-        DirItems &di = D->side[I], &dout = D->side[O];
+        DirProduct &pr = D->prod[m];
+        pr.nin = c->tree[I].npoints;
+        pr.nout = c->tree[O].npoints;
+        pr.cin = D->side[I].h_cptr.back();
+        pr.cout = D->side[O].h_cptr.back();
+    }
+    cudaStream_t ts[8];
+    for (cudaStream_t &t : ts) CK(cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
+    struct StreamsGuard {
+        cudaStream_t *t;
+        ~StreamsGuard() {
+            for (int i = 0; i < 8; ++i) cudaStreamDestroy(t[i]);
+        }
+    } tsg{ts};
+    on_threads(c->device, 8, [&](int task) {
+        const cudaStream_t s = ts[task];
+        const int m = task / 4, stage = task % 4;
+        const int I = m == 0 ? 1 : 0, O = 1 - I;
+        const DirItems &di = D->side[I], &dout = D->side[O];
         const nca::Tree &TI = c->tree[I], &TO = c->tree[O];
         DirProduct &pr = D->prod[m];
-        pr.nin = TI.npoints;
-        pr.nout = TO.npoints;
-        pr.cin = di.h_cptr.back();
-        pr.cout = dout.h_cptr.back();
         const int64_t xin = pr.nin, yo = pr.nin + pr.cin;
         // up: input-side items, deepest level first
-        {
+        if (stage == 0) {
             StageBuilder B;
             for (int lev = TI.nlevels - 1; lev >= 0; --lev) {
                 for (int it : bylevel[I][lev]) {
@@ -1399,7 +1443,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             B.finish(pr.up, di.XT.p, s);
         }
         // coupling: output-side items with a rank and their far pairs' blocks (store built above)
-        {
+        if (stage == 1) {
             StageBuilder B;
             const nca::DirSide &pl = dout.plan;
             const std::vector<int64_t> &off = m == 0 ? cfoff : ctoff;
@@ -1419,7 +1463,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             B.finish(pr.couple, nullptr, s);
         }
         // down: output-side items gather from the parent items that map onto them, root level first
-        {
+        if (stage == 2) {
             // parents of every child item (CSR in parent order), with the child's row offset in
             // the parent's X
             std::vector<int32_t> pptr(size_t(dout.nitems) + 1, 0), ppar;
@@ -1462,7 +1506,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             B.finish(pr.down, dout.X.p, s);
         }
         // leaves: every basis item whose cluster contains the leaf, then the near blocks
-        {
+        if (stage == 3) {
             StageBuilder B;
             const nca::DirSide &pl = dout.plan;
             const std::vector<int32_t> &nptr = m == 0 ? P.nearptr : P.tnearptr;
@@ -2982,15 +3026,19 @@ int32_t nca_core_dir_items(const nca_core *core, int32_t side, int32_t *nitems, 
     const DirItems &d = core->dir->side[side];
     *nitems = d.nitems;
     if (!ranks) return NCA_OK;
-    std::copy(d.h_rank.begin(), d.h_rank.end(), ranks);
-    std::copy(d.h_nrows.begin(), d.h_nrows.end(), nrows);
-    ptr[0] = 0;
-    for (int it = 0; it < d.nitems; ++it) {
-        ptr[it + 1] = ptr[it] + d.h_rank[it];
-        std::copy(d.h_piv.begin() + int64_t(it) * core->maxrank,
-                  d.h_piv.begin() + int64_t(it) * core->maxrank + d.h_rank[it], idx + ptr[it]);
-    }
-    return NCA_OK;
+    return guarded([&] {
+        CK(cudaSetDevice(core->device));
+        const std::vector<int32_t> piv = download_now(d.piv, size_t(d.nitems) * core->maxrank);
+        std::copy(d.h_rank.begin(), d.h_rank.end(), ranks);
+        std::copy(d.h_nrows.begin(), d.h_nrows.end(), nrows);
+        ptr[0] = 0;
+        for (int it = 0; it < d.nitems; ++it) {
+            ptr[it + 1] = ptr[it] + d.h_rank[it];
+            std::copy(piv.begin() + int64_t(it) * core->maxrank, piv.begin() + int64_t(it) * core->maxrank + d.h_rank[it],
+                      idx + ptr[it]);
+        }
+        return int(NCA_OK);
+    });
 }
 
 int32_t nca_core_farpivots_total(const nca_core *core, int32_t side, int64_t *total) {
