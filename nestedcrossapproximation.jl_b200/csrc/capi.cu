@@ -661,7 +661,7 @@ void fill_bases(nca_core *c, int sd, int mode, const KernelParams &K, const Kern
 
 // Near-field stores: one block per near pair (test CSR order) and its transpose (trial CSR
 // order), with the pair lists and transposition plans kept for refills. Returns the entries.
-int64_t build_near(nca_core *c, cudaStream_t s) {
+int64_t build_near(nca_core *c, cudaStream_t s, std::vector<int64_t> *ntoff_out = nullptr) {
     const nca::Partition &P = c->part;
     const nca::Tree &Tt = c->tree[0], &Ts = c->tree[1];
     const int64_t nnear = P.nearnodes.size();
@@ -709,6 +709,7 @@ int64_t build_near(nca_core *c, cudaStream_t s) {
     c->ntr_cols.upload(ntr_cols, s);
     c->n_ntr = ntn;
     fill_near(c, c->K, c->N.p, c->NT.p, s);
+    if (ntoff_out) *ntoff_out = std::move(h_ntoff);
     return near_entries;
 }
 
@@ -1353,9 +1354,11 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     CN.M.alloc(size_t(cfoff.back()));
     CTs.M.alloc(size_t(ctoff.back()));
     CN.entries = CTs.entries = coupling_entries;
+    // the couplings and the near field are computed on stream s while the host builds the gather
+    // plans (which only need their offsets); their inputs stay alive until s is synchronised
+    DBuf<int32_t> dpt, dps, drows, dcols;
+    DBuf<int64_t> dcoff, din, dctoff;
     {
-        DBuf<int32_t> dpt, dps, drows, dcols;
-        DBuf<int64_t> dcoff, din, dctoff;
         dpt.upload(pair_it, s);
         dps.upload(pair_is, s);
         dcoff.upload(cfoff, s);
@@ -1385,11 +1388,9 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         launch_transpose_blocks<double2>(CN.M.p, din.p, drows.p, dcols.p, dctoff.p, int64_t(ps.farnodes.size()), CTs.M.p,
                                          s);
         CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(s));
     }
-    const int64_t near_entries = build_near(c, s);
-    CK(cudaStreamSynchronize(s));
-    const std::vector<int64_t> h_ntoff = download_now(c->ntoff, P.tnearnodes.size() + 1);
+    std::vector<int64_t> h_ntoff;
+    const int64_t near_entries = build_near(c, s, &h_ntoff);
     // gather plans: the four stages of both orientations, each task on its own thread and stream
     for (int m = 0; m < 2; ++m) {
         const int I = m == 0 ? 1 : 0, O = 1 - I;
@@ -1534,6 +1535,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         }
         CK(cudaStreamSynchronize(s));
     });
+    CK(cudaStreamSynchronize(s));
     // the per-item operators live on in the stage stores (directional cores have no node exports)
     for (DirItems &d : D->side) {
         d.X.release();
