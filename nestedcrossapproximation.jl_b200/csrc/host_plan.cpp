@@ -21,8 +21,12 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
+
+#include <sched.h>
 
 #include "nca_internal.h"
 
@@ -421,9 +425,28 @@ int select_farpivots(const Tree &far, const double *ownpts, const double *farpts
     return select_farpivots_at(far, farpts, c, nref, farnodes, nfar, maxrank, out);
 }
 
+// The cores this process may run on: its CPU affinity mask, capped by a cgroup CPU quota
+// (cpu.max) when there is one, at most 64. The machine's processor count alone overstates it in a
+// container that is given a share of a larger host.
 int host_threads() {
-    unsigned hc = std::thread::hardware_concurrency();
-    return hc == 0 ? 1 : int(std::min(hc, 64u));
+    static const int n = [] {
+        int c = 0;
+        cpu_set_t set;
+        CPU_ZERO(&set);
+        if (sched_getaffinity(0, sizeof(set), &set) == 0) c = CPU_COUNT(&set);
+        if (c <= 0) c = int(std::thread::hardware_concurrency());
+        if (FILE *f = std::fopen("/sys/fs/cgroup/cpu.max", "r")) {
+            char quota[32] = {0};
+            long long period = 0;
+            if (std::fscanf(f, "%31s %lld", quota, &period) == 2 && std::strcmp(quota, "max") != 0 && period > 0) {
+                const long long q = std::atoll(quota);
+                if (q > 0) c = std::min<long long>(c, std::max<long long>(1, (q + period - 1) / period));
+            }
+            std::fclose(f);
+        }
+        return std::max(1, std::min(c, 64));
+    }();
+    return n;
 }
 
 void all_farpivots(const Tree &own, const Tree &far, const double *ownpts, const double *farpts,
