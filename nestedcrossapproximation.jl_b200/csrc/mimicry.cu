@@ -11,10 +11,11 @@
 //   far); descend by the same score through the children with untaken points to a leaf; take
 //   the leaf's untaken point of the largest score. Ties go to the first candidate (root list
 //   order, child order, point position).
-// The host keeps running minima between picks; here every minimum is taken afresh over the
-// chosen pivots. A minimum does not depend on the order it is taken in and every squared
-// distance uses the host's operation order (fma(dx, dx, fma(dy, dy, dz * dz)); compiled with
-// --fmad=false), so the pivots agree with the host's bit for bit.
+// The host keeps running minima between picks; here the far nodes' minima (and their counts of
+// taken points) are kept running per lane for items with at most 128 far nodes, and every other
+// minimum is taken afresh over the chosen pivots. A minimum does not depend on the order it is
+// taken in and every squared distance uses the host's operation order (fma(dx, dx, fma(dy, dy,
+// dz * dz)); compiled with --fmad=false), so the pivots agree with the host's bit for bit.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -26,6 +27,7 @@ namespace nca {
 namespace {
 
 constexpr int kWarps = 8;  // items per CTA
+constexpr int kRootSlots = 4;  // roots a lane keeps running minima for (items with <= 128 far nodes)
 
 __device__ __forceinline__ double dist2(double ax, double ay, double az, double bx, double by, double bz) {
     const double dx = ax - bx, dy = ay - by, dz = az - bz;
@@ -84,7 +86,7 @@ __device__ __forceinline__ void warp_argmax(double &sc, int &idx) {
     }
 }
 
-__global__ void __launch_bounds__(kWarps * 32) k_mimicry(MimicryArgs a) {
+__global__ void __launch_bounds__(kWarps * 32, 4) k_mimicry(MimicryArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m = a.maxrank;
@@ -108,27 +110,56 @@ __global__ void __launch_bounds__(kWarps * 32) k_mimicry(MimicryArgs a) {
                              a.centroid[3 * size_t(own) + 2]};
         int32_t *out = a.piv + size_t(item) * m;
         int nch = 0;
+        // Items with at most 32 * kRootSlots far nodes: lane l keeps, for its roots l + 32 r, the
+        // running minimum of the squared distances to the chosen pivots and the count of chosen
+        // positions inside the root (updated once per pick; a minimum is exact in any order).
+        const bool running = nroots <= 32 * kRootSlots;
+        double rdm[kRootSlots];
+        int rtk[kRootSlots];
+#pragma unroll
+        for (int r = 0; r < kRootSlots; ++r) {
+            rdm[r] = INFINITY;
+            rtk[r] = 0;
+        }
         for (int p = 0; p < n; ++p) {
             // root: the far node of the best centre score among those with untaken points
             double best = -1.0;
             int bi = 0x7fffffff;
-            for (int i = lane; i < nroots; i += 32) {
-                const int f = roots[i];
-                const int lo = a.begin[f], hi = a.end[f];
-                int taken = 0;
-                double dm = nch == 0 ? 1.0 : INFINITY;
-                const double yx = a.center[3 * size_t(f)], yy = a.center[3 * size_t(f) + 1],
-                             yz = a.center[3 * size_t(f) + 2];
-                for (int q = 0; q < nch; ++q) {
-                    taken += ch.pos[q] >= lo && ch.pos[q] < hi;
-                    const double d = dist2(yx, yy, yz, ch.x[q], ch.y[q], ch.z[q]);
-                    dm = d < dm ? d : dm;
+            if (running) {
+#pragma unroll
+                for (int r = 0; r < kRootSlots; ++r) {
+                    const int i = lane + 32 * r;
+                    if (i < nroots) {
+                        const int f = roots[i];
+                        if (a.end[f] - a.begin[f] - rtk[r] > 0) {
+                            const double sc = score(a.center[3 * size_t(f)], a.center[3 * size_t(f) + 1],
+                                                    a.center[3 * size_t(f) + 2], c, nch == 0 ? 1.0 : rdm[r]);
+                            if (sc > best) {
+                                best = sc;
+                                bi = i;
+                            }
+                        }
+                    }
                 }
-                if (hi - lo - taken <= 0) continue;
-                const double sc = score(yx, yy, yz, c, dm);
-                if (sc > best) {
-                    best = sc;
-                    bi = i;
+            } else {
+                for (int i = lane; i < nroots; i += 32) {
+                    const int f = roots[i];
+                    const int lo = a.begin[f], hi = a.end[f];
+                    int taken = 0;
+                    double dm = nch == 0 ? 1.0 : INFINITY;
+                    const double yx = a.center[3 * size_t(f)], yy = a.center[3 * size_t(f) + 1],
+                                 yz = a.center[3 * size_t(f) + 2];
+                    for (int q = 0; q < nch; ++q) {
+                        taken += ch.pos[q] >= lo && ch.pos[q] < hi;
+                        const double d = dist2(yx, yy, yz, ch.x[q], ch.y[q], ch.z[q]);
+                        dm = d < dm ? d : dm;
+                    }
+                    if (hi - lo - taken <= 0) continue;
+                    const double sc = score(yx, yy, yz, c, dm);
+                    if (sc > best) {
+                        best = sc;
+                        bi = i;
+                    }
                 }
             }
             warp_argmax(best, bi);
@@ -160,13 +191,20 @@ __global__ void __launch_bounds__(kWarps * 32) k_mimicry(MimicryArgs a) {
                 if (lane == 0) atomicCAS(a.error, 0, 1);
                 break;
             }
-            // leaf: the untaken point of the best score
+            // leaf: the untaken point of the best score; the taken positions of each 32-point
+            // window come from one OR-reduction per 32 chosen pivots
             double pb = -1.0;
             int bp = 0x7fffffff;
-            for (int pos = a.begin[node] + lane; pos < a.end[node]; pos += 32) {
-                bool taken = false;
-                for (int q = 0; q < nch; ++q) taken |= ch.pos[q] == pos;
-                if (taken) continue;
+            const int lend = a.end[node];
+            for (int base = a.begin[node]; base < lend; base += 32) {
+                unsigned tmask = 0;
+                for (int q0 = 0; q0 < nch; q0 += 32) {
+                    const int q = q0 + lane;
+                    const int off = q < nch ? ch.pos[q] - base : -1;
+                    tmask |= __reduce_or_sync(0xffffffffu, off >= 0 && off < 32 ? 1u << off : 0u);
+                }
+                const int pos = base + lane;
+                if (pos >= lend || ((tmask >> lane) & 1u)) continue;
                 const int id = a.perm[pos];
                 const double yx = a.pts[3 * size_t(id)], yy = a.pts[3 * size_t(id) + 1], yz = a.pts[3 * size_t(id) + 2];
                 double dm = nch == 0 ? 1.0 : INFINITY;
@@ -193,8 +231,22 @@ __global__ void __launch_bounds__(kWarps * 32) k_mimicry(MimicryArgs a) {
                 ch.pos[nch] = bp;
                 out[p] = id;
             }
-            ++nch;
             __syncwarp();
+            if (running) {
+                const double px = ch.x[nch], py = ch.y[nch], pz = ch.z[nch];
+#pragma unroll
+                for (int r = 0; r < kRootSlots; ++r) {
+                    const int i = lane + 32 * r;
+                    if (i < nroots) {
+                        const int f = roots[i];
+                        rtk[r] += bp >= a.begin[f] && bp < a.end[f];
+                        const double d = dist2(a.center[3 * size_t(f)], a.center[3 * size_t(f) + 1],
+                                               a.center[3 * size_t(f) + 2], px, py, pz);
+                        rdm[r] = d < rdm[r] ? d : rdm[r];
+                    }
+                }
+            }
+            ++nch;
         }
         if (lane == 0) a.count[item] = nch;
         __syncwarp();
