@@ -346,7 +346,8 @@ void item_farfield(const Tree &T, const DirSide &D, int item, std::vector<int32_
     // idcs: the 1-based local directions of cur on the chain; next: the parent directions that map
     // onto any of them, ascending (each parent direction maps onto one child direction, so the
     // inverse lists are disjoint and their sorted union is the reference's scan in order)
-    std::vector<int32_t> idcs{item - D.dirptr[node] + 1}, next;
+    thread_local std::vector<int32_t> idcs, next;  // reused by every call on this thread
+    idcs.assign(1, item - D.dirptr[node] + 1);
     for (int cur = node; T.parent[cur] >= 0; cur = T.parent[cur]) {
         const int p = T.parent[cur];
         next.clear();
