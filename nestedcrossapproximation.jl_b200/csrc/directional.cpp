@@ -122,6 +122,35 @@ int nearest_direction(const std::vector<double> &dirs, const double *v) {
     return best;
 }
 
+// nearest_direction over the spherical Fibonacci candidates of candidate_directions (z_i =
+// 1 - 2 (i + 1/2) / n, descending): only the indices whose z lies within an angle of
+// 4 sqrt(4 pi / n) of v's polar angle are searched. That band holds every candidate within twice
+// the lattice's covering radius of v, so the largest dot product lies inside it, ahead of every
+// candidate outside by about 75 / n of |v|, far above the rounding of a three-term dot product.
+// Inside the band the dots are formed and compared as in the full search (ascending index, first
+// on ties), so the result is the full search's.
+int nearest_candidate(const std::vector<double> &dirs, const double *v) {
+    const int64_t n = int64_t(dirs.size() / 3);
+    const double r = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const double band = 4.0 * std::sqrt(4.0 * M_PI / double(n));
+    if (!(r > 0.0) || !std::isfinite(r) || band >= 0.5 * M_PI) return nearest_direction(dirs, v);
+    const double theta = std::acos(std::max(-1.0, std::min(1.0, v[2] / r)));
+    const double zhi = std::cos(std::max(0.0, theta - band)), zlo = std::cos(std::min(M_PI, theta + band));
+    // z_i <= zhi  <=>  i >= (1 - zhi) n / 2 - 1/2;  z_i >= zlo  <=>  i <= (1 - zlo) n / 2 - 1/2
+    const int64_t i0 = std::max<int64_t>(0, int64_t(std::floor((1.0 - zhi) * double(n) / 2.0 - 0.5)) - 1);
+    const int64_t i1 = std::min<int64_t>(n - 1, int64_t(std::ceil((1.0 - zlo) * double(n) / 2.0 - 0.5)) + 1);
+    int64_t best = i0;
+    double bd = dirs[3 * i0] * v[0] + dirs[3 * i0 + 1] * v[1] + dirs[3 * i0 + 2] * v[2];
+    for (int64_t i = i0 + 1; i <= i1; ++i) {
+        const double d = dirs[3 * i] * v[0] + dirs[3 * i + 1] * v[1] + dirs[3 * i + 2] * v[2];
+        if (d > bd) {
+            bd = d;
+            best = i;
+        }
+    }
+    return int(best);
+}
+
 }  // namespace
 
 Partition build_partition_wideband(const Tree &test, const Tree &trial, const Wideband &w) {
@@ -170,7 +199,7 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
             for (int i = 0; i < nfar; ++i) {
                 const double *cf = &F.center[3 * size_t(D.farnodes[b + i])];
                 const double v[3] = {c[0] - cf[0], c[1] - cf[1], c[2] - cf[2]};
-                nd[i] = nearest_direction(total, v) + 1;
+                nd[i] = nearest_candidate(total, v) + 1;
             }
             // far nodes grouped by direction (stable)
             std::vector<int32_t> order(nfar);
@@ -196,7 +225,7 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
                     const double *pv = &dirvec[p][3 * di];
                     const double v[3] = {c[0] - cp[0] + mult * pv[0], c[1] - cp[1] + mult * pv[1],
                                          c[2] - cp[2] + mult * pv[2]};
-                    map[di] = nearest_direction(total, v) + 1;
+                    map[di] = nearest_candidate(total, v) + 1;
                 }
                 for (size_t di = 0; di < map.size(); ++di) {
                     auto it = std::find(uniq.begin(), uniq.end(), map[di]);

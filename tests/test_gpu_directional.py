@@ -107,3 +107,19 @@ def test_directional_structure_and_limits():
         N.batch([A])
     with pytest.raises(N.ArgumentError):
         N.core(A).pivots(0)
+
+
+def test_directional_build_errors_reach_the_caller():
+    """The two sides of a directional build run on their own host threads: a side that fails (here
+    a level block beyond one CTA's shared memory: ~600-point leaves with far pivots) raises on the
+    caller with its message, and the next build in the process is unaffected."""
+    N = _n()
+    pts = sphere(1200, 11)
+    far = pts + np.array([10.0, 0.0, 0.0])
+    with pytest.raises(N.ArgumentError, match="shared memory|more rows"):
+        build(pts, far, 0.5, 1e-12, 600)
+    test = sphere(900, 12)
+    A = build(test, test, 12.0, 1e-4, 32)
+    x = cgauss((900, 2), 13)
+    y = A @ x
+    assert y.shape == (900, 2) and np.all(np.isfinite(y))
