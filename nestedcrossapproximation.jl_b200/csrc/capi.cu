@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cstring>
 #include <exception>
+#include <future>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -1299,98 +1300,108 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         CK(cudaStreamSynchronize(s));
     });
     auto h1 = std::chrono::steady_clock::now();
-    // far pairs (test CSR grouped by test direction) and their items on both sides
-    const nca::DirSide &pt = D->side[0].plan, &ps = D->side[1].plan;
-    const int64_t npairs = int64_t(pt.farnodes.size());
-    std::vector<int32_t> item_of_pos[2];
-    for (int sd = 0; sd < 2; ++sd) {
-        const nca::DirSide &pl = D->side[sd].plan;
-        item_of_pos[sd].assign(pl.farnodes.size(), -1);
-        for (size_t it = 0; it < pl.item_node.size(); ++it)
-            for (int q = pl.dirfarptr[it]; q < pl.dirfarptr[it + 1]; ++q) item_of_pos[sd][q] = int32_t(it);
-    }
-    // (trial node, test node) -> position in the trial far lists: each trial node's list sorted by
-    // test node and searched by bisection
-    std::vector<std::pair<int32_t, int32_t>> bytest(ps.farnodes.size());
-    for (int sn = 0; sn < c->tree[1].nnodes; ++sn) {
-        for (int q = ps.farptr[sn]; q < ps.farptr[sn + 1]; ++q) bytest[q] = {ps.farnodes[q], q};
-        std::sort(bytest.begin() + ps.farptr[sn], bytest.begin() + ps.farptr[sn + 1]);
-    }
-    auto trialpos = [&](int sn, int t) {
-        const auto b = bytest.begin() + ps.farptr[sn], e = bytest.begin() + ps.farptr[sn + 1];
-        const auto it = std::lower_bound(b, e, std::make_pair(int32_t(t), INT32_MIN));
-        if (it == e || it->first != t) throw Failure(NCA_ERR_ARG, "internal: a far pair has no transpose");
-        return it->second;
-    };
-    std::vector<int32_t> pair_it(npairs), pair_is(npairs);
-    std::vector<int32_t> pair_of_pos(ps.farnodes.size(), -1);
-    for (int t = 0; t < c->tree[0].nnodes; ++t)
-        for (int e = pt.farptr[t]; e < pt.farptr[t + 1]; ++e) {
-            const int sn = pt.farnodes[e];
-            const int32_t q = trialpos(sn, t);
-            pair_it[e] = item_of_pos[0][e];
-            pair_is[e] = item_of_pos[1][q];
-            pair_of_pos[q] = e;
-        }
-    const std::vector<int32_t> &rt = D->side[0].h_rank, &rs = D->side[1].h_rank;
-    // coupling blocks S_e = K[tau_(t, dt), tau_(s, ds)] in test pair order, transposes in trial order
-    std::vector<int64_t> cfoff(npairs + 1, 0), ctoff(ps.farnodes.size() + 1, 0);
-    int64_t coupling_entries = 0;
-    for (int64_t e = 0; e < npairs; ++e) {
-        const int64_t n = int64_t(rt[pair_it[e]]) * rs[pair_is[e]];
-        coupling_entries += n;
-        cfoff[e + 1] = cfoff[e] + pad2(n);
-    }
-    std::vector<int64_t> tr_in(ps.farnodes.size());
-    std::vector<int32_t> tr_rows(ps.farnodes.size()), tr_cols(ps.farnodes.size());
-    for (size_t q = 0; q < ps.farnodes.size(); ++q) {
-        const int e = pair_of_pos[q];
-        tr_in[q] = cfoff[e];
-        tr_rows[q] = rt[pair_it[e]];
-        tr_cols[q] = rs[pair_is[e]];
-        ctoff[q + 1] = ctoff[q] + pad2(int64_t(tr_rows[q]) * tr_cols[q]);
-    }
-    GatherStage &CN = D->prod[0].couple, &CTs = D->prod[1].couple;
-    CN.M.alloc(size_t(cfoff.back()));
-    CTs.M.alloc(size_t(ctoff.back()));
-    CN.entries = CTs.entries = coupling_entries;
-    // the couplings and the near field are computed on stream s while the host builds the gather
-    // plans (which only need their offsets); their inputs stay alive until s is synchronised
-    DBuf<int32_t> dpt, dps, drows, dcols;
-    DBuf<int64_t> dcoff, din, dctoff;
-    {
-        dpt.upload(pair_it, s);
-        dps.upload(pair_is, s);
-        dcoff.upload(cfoff, s);
-        CouplingArgs a;
-        a.K = c->K;
-        a.test_pts = c->side[0].pts.p;
-        a.trial_pts = c->side[1].pts.p;
-        a.pair_t = dpt.p;
-        a.pair_s = dps.p;
-        a.rank_t = D->side[0].rank.p;
-        a.rank_s = D->side[1].rank.p;
-        a.piv_t = D->side[0].piv.p;
-        a.piv_s = D->side[1].piv.p;
-        a.maxrank = maxrank;
-        a.coff = dcoff.p;
-        a.npairs = npairs;
-        a.C = CN.M.p;
-        a.C32 = nullptr;
-        if (npairs > 0) {
-            k_couplings<<<launch_grid(npairs, 16), 256, 0, s>>>(a);
-            CK(cudaGetLastError());
-        }
-        din.upload(tr_in, s);
-        drows.upload(tr_rows, s);
-        dcols.upload(tr_cols, s);
-        dctoff.upload(ctoff, s);
-        launch_transpose_blocks<double2>(CN.M.p, din.p, drows.p, dcols.p, dctoff.p, int64_t(ps.farnodes.size()), CTs.M.p,
-                                         s);
-        CK(cudaGetLastError());
-    }
+    // near field first (its offsets feed the leaf plans); its kernels run on stream s
     std::vector<int64_t> h_ntoff;
     const int64_t near_entries = build_near(c, s, &h_ntoff);
+    // couplings: prepared on the host by the thread of the forward coupling plan (the transposed
+    // coupling plan waits for it) and computed on stream s while the other plans are built; their
+    // device inputs stay alive until s is synchronised
+    const nca::DirSide &pt = D->side[0].plan, &ps = D->side[1].plan;
+    const int64_t npairs = int64_t(pt.farnodes.size());
+    std::vector<int32_t> pair_it, pair_is, pair_of_pos;
+    std::vector<int64_t> cfoff, ctoff;
+    int64_t coupling_entries = 0;
+    DBuf<int32_t> dpt, dps, drows, dcols;
+    DBuf<int64_t> dcoff, din, dctoff;
+    auto couplings = [&]() {
+        // far pairs (test CSR grouped by test direction) and their items on both sides
+        std::vector<int32_t> item_of_pos[2];
+        for (int sd = 0; sd < 2; ++sd) {
+            const nca::DirSide &pl = D->side[sd].plan;
+            item_of_pos[sd].assign(pl.farnodes.size(), -1);
+            for (size_t it = 0; it < pl.item_node.size(); ++it)
+                for (int q = pl.dirfarptr[it]; q < pl.dirfarptr[it + 1]; ++q) item_of_pos[sd][q] = int32_t(it);
+        }
+        // (trial node, test node) -> position in the trial far lists: each trial node's list sorted by
+        // test node and searched by bisection
+        std::vector<std::pair<int32_t, int32_t>> bytest(ps.farnodes.size());
+        for (int sn = 0; sn < c->tree[1].nnodes; ++sn) {
+            for (int q = ps.farptr[sn]; q < ps.farptr[sn + 1]; ++q) bytest[q] = {ps.farnodes[q], q};
+            std::sort(bytest.begin() + ps.farptr[sn], bytest.begin() + ps.farptr[sn + 1]);
+        }
+        auto trialpos = [&](int sn, int t) {
+            const auto b = bytest.begin() + ps.farptr[sn], e = bytest.begin() + ps.farptr[sn + 1];
+            const auto it = std::lower_bound(b, e, std::make_pair(int32_t(t), INT32_MIN));
+            if (it == e || it->first != t) throw Failure(NCA_ERR_ARG, "internal: a far pair has no transpose");
+            return it->second;
+        };
+        pair_it.assign(npairs, 0);
+        pair_is.assign(npairs, 0);
+        pair_of_pos.assign(ps.farnodes.size(), -1);
+        for (int t = 0; t < c->tree[0].nnodes; ++t)
+            for (int e = pt.farptr[t]; e < pt.farptr[t + 1]; ++e) {
+                const int sn = pt.farnodes[e];
+                const int32_t q = trialpos(sn, t);
+                pair_it[e] = item_of_pos[0][e];
+                pair_is[e] = item_of_pos[1][q];
+                pair_of_pos[q] = e;
+            }
+        const std::vector<int32_t> &rt = D->side[0].h_rank, &rs = D->side[1].h_rank;
+        // coupling blocks S_e = K[tau_(t, dt), tau_(s, ds)] in test pair order, transposes in trial order
+        cfoff.assign(npairs + 1, 0);
+        ctoff.assign(ps.farnodes.size() + 1, 0);
+        for (int64_t e = 0; e < npairs; ++e) {
+            const int64_t n = int64_t(rt[pair_it[e]]) * rs[pair_is[e]];
+            coupling_entries += n;
+            cfoff[e + 1] = cfoff[e] + pad2(n);
+        }
+        std::vector<int64_t> tr_in(ps.farnodes.size());
+        std::vector<int32_t> tr_rows(ps.farnodes.size()), tr_cols(ps.farnodes.size());
+        for (size_t q = 0; q < ps.farnodes.size(); ++q) {
+            const int e = pair_of_pos[q];
+            tr_in[q] = cfoff[e];
+            tr_rows[q] = rt[pair_it[e]];
+            tr_cols[q] = rs[pair_is[e]];
+            ctoff[q + 1] = ctoff[q] + pad2(int64_t(tr_rows[q]) * tr_cols[q]);
+        }
+        GatherStage &CN = D->prod[0].couple, &CTs = D->prod[1].couple;
+        CN.M.alloc(size_t(cfoff.back()));
+        CTs.M.alloc(size_t(ctoff.back()));
+        CN.entries = CTs.entries = coupling_entries;
+        {
+            dpt.upload(pair_it, s);
+            dps.upload(pair_is, s);
+            dcoff.upload(cfoff, s);
+            CouplingArgs a;
+            a.K = c->K;
+            a.test_pts = c->side[0].pts.p;
+            a.trial_pts = c->side[1].pts.p;
+            a.pair_t = dpt.p;
+            a.pair_s = dps.p;
+            a.rank_t = D->side[0].rank.p;
+            a.rank_s = D->side[1].rank.p;
+            a.piv_t = D->side[0].piv.p;
+            a.piv_s = D->side[1].piv.p;
+            a.maxrank = maxrank;
+            a.coff = dcoff.p;
+            a.npairs = npairs;
+            a.C = CN.M.p;
+            a.C32 = nullptr;
+            if (npairs > 0) {
+                k_couplings<<<launch_grid(npairs, 16), 256, 0, s>>>(a);
+                CK(cudaGetLastError());
+            }
+            din.upload(tr_in, s);
+            drows.upload(tr_rows, s);
+            dcols.upload(tr_cols, s);
+            dctoff.upload(ctoff, s);
+            launch_transpose_blocks<double2>(CN.M.p, din.p, drows.p, dcols.p, dctoff.p, int64_t(ps.farnodes.size()), CTs.M.p,
+                                             s);
+            CK(cudaGetLastError());
+        }
+    };
+    std::promise<void> coupled;
+    std::shared_future<void> coupled_done = coupled.get_future().share();
     // gather plans: the four stages of both orientations, each task on its own thread and stream
     for (int m = 0; m < 2; ++m) {
         const int I = m == 0 ? 1 : 0, O = 1 - I;
@@ -1445,6 +1456,17 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         }
         // coupling: output-side items with a rank and their far pairs' blocks (store built above)
         if (stage == 1) {
+            if (m == 0) {
+                try {
+                    couplings();
+                    coupled.set_value();
+                } catch (...) {
+                    coupled.set_exception(std::current_exception());
+                    throw;
+                }
+            } else {
+                coupled_done.get();
+            }
             StageBuilder B;
             const nca::DirSide &pl = dout.plan;
             const std::vector<int64_t> &off = m == 0 ? cfoff : ctoff;
