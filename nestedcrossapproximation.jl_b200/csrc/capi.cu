@@ -167,7 +167,7 @@ struct DirItems {
     int nitems = 0;
     std::vector<int32_t> h_fpptr, h_rank, h_nrows;  // far pivots and item pivots stay on the device
     std::vector<int64_t> h_xoff, h_cptr;
-    DBuf<int32_t> item_node, item_basis, item_chptr, item_chidx, fpptr, fpidx, rank, nrows, piv, cpiv;
+    DBuf<int32_t> item_node, item_basis, item_chptr, item_chidx, fpptr, fpidx, rank, nrows, piv;
     DBuf<int64_t> xoff;
     DBuf<double2> X, XT;
 };
@@ -1151,7 +1151,6 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         d.nrows.alloc(std::max(ni, 1));
         d.nrows.zero(s);
         d.piv.alloc(size_t(std::max(ni, 1)) * maxrank);
-        d.cpiv.alloc(size_t(std::max(ni, 1)) * maxrank);
         LevelArgs a{};
         a.K = c->K;
         a.side = sd;
@@ -1167,7 +1166,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         a.rank = d.rank.p;
         a.nrows = d.nrows.p;
         a.piv = d.piv.p;
-        a.cpiv = d.cpiv.p;
+        a.cpiv = nullptr;  // column pivots serve frozen-skeleton refills, which directional cores do not offer
         a.maxrank = maxrank;
         a.tol = sd == 0 ? o->tol_test : o->tol_trial;
         a.sampled = o->sampled;
