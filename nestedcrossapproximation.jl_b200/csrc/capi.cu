@@ -45,61 +45,23 @@ void check(cudaError_t e, const char *what, int line) {
 }
 #define CK(call) check((call), #call, __LINE__)
 
-// Device memory of the library comes from each device's default stream-ordered pool, which keeps
-// up to a quarter of the device's memory reserved after frees: repeated builds and growing
-// workspaces reuse it instead of mapping fresh memory from the driver each time. Allocations and
-// frees are ordered on one non-blocking stream per device, and a free first waits for the device
-// to be idle (as cudaFree does), so no buffer is handed out again while a kernel may still use it.
-constexpr int kPoolDevices = 64;
-
-cudaStream_t pool_stream(int dev) {
-    static std::mutex mu;
-    static cudaStream_t streams[kPoolDevices] = {};
-    if (dev < 0 || dev >= kPoolDevices) throw Failure(NCA_ERR_ARG, "device index beyond the supported range");
-    std::lock_guard<std::mutex> lock(mu);
-    if (!streams[dev]) {
-        cudaMemPool_t pool;
-        CK(cudaDeviceGetDefaultMemPool(&pool, dev));
-        size_t freeb = 0, total = 0;
-        CK(cudaMemGetInfo(&freeb, &total));
-        uint64_t keep = total / 4;
-        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-        CK(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking));
-    }
-    return streams[dev];
-}
-
 template <typename T>
 struct DBuf {
     T *p = nullptr;
     size_t n = 0;
-    int dev = 0;  // the device the buffer lives on
     DBuf() = default;
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
     ~DBuf() { release(); }
-    void release() noexcept {
-        if (p) {
-            int cur = dev;
-            cudaGetDevice(&cur);
-            if (cur != dev) cudaSetDevice(dev);
-            cudaDeviceSynchronize();
-            try {
-                cudaFreeAsync(p, pool_stream(dev));  // the stream exists: the allocation made it
-            } catch (...) {
-            }
-            if (cur != dev) cudaSetDevice(cur);
-        }
+    void release() {
+        if (p) cudaFree(p);
         p = nullptr;
         n = 0;
     }
     void alloc(size_t count) {
         release();
         n = count;
-        CK(cudaGetDevice(&dev));
-        const cudaStream_t ps = pool_stream(dev);
-        CK(cudaMallocAsync(reinterpret_cast<void **>(&p), sizeof(T) * std::max<size_t>(count, 1), ps));
-        CK(cudaStreamSynchronize(ps));
+        CK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)));
     }
     void upload(const T *h, size_t count, cudaStream_t s) {
         alloc(count);
