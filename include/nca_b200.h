@@ -131,6 +131,9 @@ typedef struct {
     int32_t store_f32;          /* 1: also keep complex FP32 copies of all stores */
 } nca_build_opts;
 
+/* The host planning runs on the process's cores (its CPU affinity mask, capped by a cgroup CPU
+ * quota); a directional build also runs its two sides, and then its eight gather plans, on host
+ * threads and streams of their own. The call returns once the core is complete. */
 int32_t nca_core_build(const double *testpoints, int64_t ntest, const double *trialpoints,
                        int64_t ntrial, const nca_tree *testtree, const nca_tree *trialtree,
                        const nca_partition *part, const nca_kernel_desc *kernel,
@@ -145,8 +148,8 @@ typedef struct {
     int64_t near_entries, coupling_entries, basis_entries_test, basis_entries_trial,
         transfer_entries_test, transfer_entries_trial;
     int64_t nfarpairs, nnearpairs;
-    double build_seconds;             /* device build time (events) */
-    double build_seconds_host;        /* host planning time (tree mimicry, plans) */
+    double build_seconds;             /* span of the build's device work (events) */
+    double build_seconds_host;        /* host time outside that span */
 } nca_core_info;
 /* ---- differentiation on frozen skeletons (no counterpart in the reference, which has no
  *      gradients): the tree, partition, ranks and row/column pivots of a build stay fixed. ---- */
