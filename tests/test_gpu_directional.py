@@ -123,3 +123,41 @@ def test_directional_build_errors_reach_the_caller():
     x = cgauss((900, 2), 13)
     y = A @ x
     assert y.shape == (900, 2) and np.all(np.isfinite(y))
+
+
+def test_concurrent_directional_builds_match():
+    """Two directional builds at once from two host threads (each with its own side threads and
+    streams, and a plain build beside them raising the level kernel's shared-memory limit) give
+    the pivots of a build made alone, bit for bit."""
+    import threading
+    N = _n()
+    pts = sphere(2500, 21)
+    alone = build(pts, pts, 16.0, 1e-4, 32)
+    want = [items(alone, sd) for sd in (0, 1)]
+    out, errors = {}, []
+
+    def run(key, fn):
+        try:
+            out[key] = fn()
+        except Exception as e:  # noqa: BLE001 - reported below
+            errors.append(e)
+
+    def plain():
+        tt = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=128))
+        aca = N.ACA(N.FullPivoting(), N.FullPivoting(), N.FNormEstimator(1e-6))
+        comp = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(pts, pts, tt), compressor=aca)
+        return N.PetrovGalerkinNCA(N.HelmholtzKernel(1.0), pts, pts, N.BlockTree(tt, tt), testcompressor=comp,
+                                   trialcompressor=comp)
+
+    threads = [threading.Thread(target=run, args=(i, lambda: build(pts, pts, 16.0, 1e-4, 32))) for i in range(2)]
+    threads.append(threading.Thread(target=run, args=("plain", plain)))
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for i in range(2):
+        for sd in (0, 1):
+            ranks, piv = items(out[i], sd)
+            assert np.array_equal(ranks, want[sd][0])
+            assert all(np.array_equal(a, b) for a, b in zip(piv, want[sd][1]))
