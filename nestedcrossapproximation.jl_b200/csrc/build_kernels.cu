@@ -95,8 +95,7 @@ __device__ __forceinline__ double2 block_entry(const LevelArgs &a, const double 
 
 size_t level_smem_bytes(int mcap, int ncap) {
     size_t b = 0;
-    b += sizeof(double2) * size_t(mcap) * ncap;  // R
-    b += sizeof(double2) * size_t(ncap) * ncap;  // P
+    b += sizeof(double2) * size_t(mcap) * ncap;  // R (the cross matrix P lives in the node's X slot)
     b += sizeof(double2) * (mcap + ncap);        // u, v
     b += sizeof(double) * 3 * (mcap + ncap);     // coordinates
     b += sizeof(int32_t) * (mcap + 3 * ncap);    // row ids, col ids, rp, cp, ipiv
@@ -172,9 +171,10 @@ __device__ int aca_smem(double2 *R, int m, int n, int maxrank, double tol, int s
     return r;
 }
 
-// LU with partial pivoting of the r x r cross matrix P (shared memory, in place) and the
-// singular check of _crossfactorization: |U_ii|^2 <= (10 eps)^2 max|U_jj|^2 for some i, or an
-// exactly zero pivot. Returns 1 if singular (*rank_out: numerical rank). All threads call it.
+// LU with partial pivoting of the r x r cross matrix P (the CTA's shared or global memory, in
+// place, ordered by the block barriers) and the singular check of _crossfactorization:
+// |U_ii|^2 <= (10 eps)^2 max|U_jj|^2 for some i, or an exactly zero pivot. Returns 1 if singular
+// (*rank_out: numerical rank). All threads call it.
 __device__ int cross_factor_smem(double2 *P, int r, int32_t *ipiv, int *s_flag, int *rank_out) {
     const int tid = threadIdx.x;
     if (tid == 0) *s_flag = 0;
@@ -284,8 +284,7 @@ __global__ void __launch_bounds__(NT) k_level_compress(LevelArgs a, const int32_
                                                        int ncap) {
     extern __shared__ __align__(16) unsigned char smem[];
     double2 *R = reinterpret_cast<double2 *>(smem);
-    double2 *P = R + size_t(mcap) * ncap;
-    double2 *u = P + size_t(ncap) * ncap;
+    double2 *u = R + size_t(mcap) * ncap;
     double2 *v = u + mcap;
     double *rowxyz = reinterpret_cast<double *>(v + ncap);
     double *colxyz = rowxyz + 3 * mcap;
@@ -363,7 +362,11 @@ __global__ void __launch_bounds__(NT) k_level_compress(LevelArgs a, const int32_
     }
     if (r == 0) return;
 
-    // phase 3b: L = A[:, cp] regenerated into R, P = L[rp, :], X = L P^{-1}
+    // phase 3b: L = A[:, cp] regenerated into R, P = L[rp, :], X = L P^{-1}. The r x r cross
+    // matrix is factorised in the node's own X slot (m x rank bound >= r x r entries, in L2),
+    // which keeps shared memory to the block and lets more CTAs share an SM; X overwrites it
+    // once every row is solved.
+    double2 *P = a.X + a.xoff[node];
     for (int e = tid; e < m * r; e += NT)
         R[e] = block_entry(a, rowxyz, rowid, colxyz, colid, e % m, cp[e / m]);
     __syncthreads();

@@ -721,8 +721,11 @@ void level_smem_at_least(size_t sm) {
     std::lock_guard<std::mutex> lock(mu);
     cudaFuncAttributes fa{};
     CK(cudaFuncGetAttributes(&fa, k_level_compress));
-    if (sm > size_t(fa.maxDynamicSharedSizeBytes))
+    if (sm > size_t(fa.maxDynamicSharedSizeBytes)) {
         CK(cudaFuncSetAttribute(k_level_compress, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+        // all of the SM's unified L1/shared memory as shared: the CTAs per SM are bounded by it
+        CK(cudaFuncSetAttribute(k_level_compress, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    }
 }
 
 void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int64_t ns,
