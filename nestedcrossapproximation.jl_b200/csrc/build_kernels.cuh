@@ -105,7 +105,8 @@ struct MimicryArgs {
     const int32_t *own_size;  // own clusters' point counts
     int maxrank;
     int32_t *count, *piv;
-    int32_t *error;  // 1: an item ran out of candidates before its pivot count
+    int32_t *error;   // 1: an item ran out of candidates before its pivot count
+    int32_t *cursor;  // next item to take (zero at launch): warps take items one at a time
 };
 size_t mimicry_smem_bytes(int maxrank);
 void launch_mimicry(const MimicryArgs &a, cudaStream_t s);

@@ -409,7 +409,7 @@ void device_farpivots(const nca::Tree &own, const double *ownpts, const nca::Tre
     dcenter.upload(far.center, s);
     dcount.alloc(nitems);
     dpiv.alloc(size_t(nitems) * maxrank);
-    derr.alloc(1);
+    derr.alloc(2);  // error word, item cursor
     derr.zero(s);
     MimicryArgs a{};
     a.begin = fd.begin.p;
@@ -429,6 +429,7 @@ void device_farpivots(const nca::Tree &own, const double *ownpts, const nca::Tre
     a.count = dcount.p;
     a.piv = dpiv.p;
     a.error = derr.p;
+    a.cursor = derr.p + 1;
     launch_mimicry(a, s);
     CK(cudaGetLastError());
     const std::vector<int32_t> count = dcount.download(s);

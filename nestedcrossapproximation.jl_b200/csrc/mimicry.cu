@@ -93,7 +93,12 @@ __global__ void __launch_bounds__(kWarps * 32, 4) k_mimicry(MimicryArgs a) {
     double *base = reinterpret_cast<double *>(smem) + size_t(warp) * 3 * m;
     Chosen ch{base, base + m, base + 2 * m,
               reinterpret_cast<int32_t *>(reinterpret_cast<double *>(smem) + size_t(kWarps) * 3 * m) + warp * m};
-    for (int item = blockIdx.x * kWarps + warp; item < a.nitems; item += gridDim.x * kWarps) {
+    for (;;) {
+        // items differ widely in cost: each warp takes the next untaken one
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.cursor, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= a.nitems) break;
         const int64_t f0 = a.ffptr[item], f1 = a.ffptr[item + 1];
         const int nroots = int(f1 - f0);
         const int32_t *roots = a.ffnodes + f0;
