@@ -26,7 +26,7 @@ namespace nca {
 
 namespace {
 
-constexpr int kWarps = 8;  // items per CTA
+constexpr int kWarps = 8;  // warps per CTA, each on one item at a time
 constexpr int kRootSlots = 4;  // roots a lane keeps running minima for (items with <= 128 far nodes)
 
 __device__ __forceinline__ double dist2(double ax, double ay, double az, double bx, double by, double bz) {
