@@ -180,7 +180,7 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
     for (int node = 0; node < nn; ++node) lf[node] = is_lowfrequency(T, node, w);
     // the nodes of one level depend on their parents only: a level's nodes run on the host
     // threads, each writing its own entries (and its own range of the far-node list)
-    auto plan_node = [&](int level, int node, std::vector<double> &total) {
+    auto plan_node = [&](int level, int node, std::vector<double> &total, std::vector<int32_t> &slot) {
             const int p = T.parent[node];
             const bool hasfars = farptr[node + 1] > farptr[node];
             const bool hasparentvecs = p >= 0 && hasvec[p];
@@ -227,14 +227,17 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
                                          c[2] - cp[2] + mult * pv[2]};
                     map[di] = nearest_candidate(total, v) + 1;
                 }
+                // candidate -> 1-based position in uniq (0: not yet listed), instead of a search
+                // of uniq per parent direction
+                slot.assign(total.size() / 3 + 1, 0);
+                for (size_t u = 0; u < uniq.size(); ++u) slot[uniq[u]] = int32_t(u) + 1;
                 for (size_t di = 0; di < map.size(); ++di) {
-                    auto it = std::find(uniq.begin(), uniq.end(), map[di]);
-                    if (it != uniq.end()) {
-                        map[di] = int32_t(it - uniq.begin()) + 1;
-                    } else {
+                    int32_t &at = slot[map[di]];
+                    if (at == 0) {
                         uniq.push_back(map[di]);
-                        map[di] = int32_t(uniq.size());
+                        at = int32_t(uniq.size());
                     }
+                    map[di] = at;
                 }
             }
             std::vector<int32_t> count(uniq.size(), 0);
@@ -258,10 +261,11 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
         std::atomic<int> cursor{n0};
         auto work = [&]() {
             std::vector<double> total;
+            std::vector<int32_t> slot;
             for (;;) {
                 const int node = cursor.fetch_add(1);
                 if (node >= n1) break;
-                plan_node(level, node, total);
+                plan_node(level, node, total, slot);
             }
         };
         const int use = std::max(1, std::min(nth, n1 - n0));
