@@ -353,13 +353,21 @@ void parallel_csr(int n, F fill, std::vector<int64_t> &ptr, std::vector<int32_t>
     for (int w = 1; w < nth; ++w) pool.emplace_back(work, w);
     work(0);
     for (auto &th : pool) th.join();
-    ptr.assign(1, 0);
-    idx.clear();
-    for (int w = 0; w < nth; ++w) {
-        const int64_t off = int64_t(idx.size());
-        for (size_t k = 1; k < lptr[w].size(); ++k) ptr.push_back(lptr[w][k] + off);
-        idx.insert(idx.end(), lidx[w].begin(), lidx[w].end());
-    }
+    // the threads' pieces back to back, each copied by its own thread
+    std::vector<int64_t> off(nth + 1, 0);
+    for (int w = 0; w < nth; ++w) off[w + 1] = off[w] + int64_t(lidx[w].size());
+    ptr.assign(size_t(n) + 1, 0);
+    idx.resize(size_t(off[nth]));
+    auto place = [&](int w) {
+        const int i0 = int(int64_t(n) * w / nth);
+        for (size_t k = 1; k < lptr[w].size(); ++k) ptr[size_t(i0) + k] = lptr[w][k] + off[w];
+        std::copy(lidx[w].begin(), lidx[w].end(), idx.begin() + off[w]);
+        std::vector<int32_t>().swap(lidx[w]);
+    };
+    pool.clear();
+    for (int w = 1; w < nth; ++w) pool.emplace_back(place, w);
+    place(0);
+    for (auto &th : pool) th.join();
 }
 
 // Phase 1 on the device: tree-mimicry far pivots of every item of one side (item i is own
@@ -980,6 +988,21 @@ struct StageBuilder {
     std::vector<int32_t> sld, crows, ccols;
     int64_t store = 0;
     int cur_max = 0;
+    // room for the outputs, segments and copies a stage is known to have at most
+    void reserve(size_t outputs, size_t segments, size_t copies) {
+        rows.reserve(outputs);
+        out.reserve(outputs);
+        work.reserve(outputs);
+        segptr.reserve(outputs + 1);
+        moff.reserve(segments);
+        w.reserve(segments);
+        voff.reserve(segments);
+        soff.reserve(copies);
+        doff.reserve(copies);
+        sld.reserve(copies);
+        crows.reserve(copies);
+        ccols.reserve(copies);
+    }
     void begin_output(int32_t R, int64_t o) {
         rows.push_back(R);
         out.push_back(o);
@@ -1433,6 +1456,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         // up: input-side items, deepest level first
         if (stage == 0) {
             StageBuilder B;
+            const size_t seg = size_t(di.nitems) + di.plan.item_chidx.size();
+            B.reserve(size_t(di.nitems), seg, seg);
             for (int lev = TI.nlevels - 1; lev >= 0; --lev) {
                 for (int it : bylevel[I][lev]) {
                     const int r = di.h_rank[it];
@@ -1473,6 +1498,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             StageBuilder B;
             const nca::DirSide &pl = dout.plan;
             const std::vector<int64_t> &off = m == 0 ? cfoff : ctoff;
+            B.reserve(size_t(dout.nitems), pl.farnodes.size(), 0);
             for (int it = 0; it < dout.nitems; ++it) {
                 const int r = dout.h_rank[it];
                 if (r <= 0) continue;
@@ -1515,6 +1541,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 prow[fill[ch]++] = c0;
             });
             StageBuilder B;
+            B.reserve(size_t(dout.nitems), ppar.size(), ppar.size());
             for (int lev = 1; lev < TO.nlevels; ++lev) {
                 for (int it : bylevel[O][lev]) {
                     const int r = dout.h_rank[it];
