@@ -18,6 +18,7 @@
 #include <unordered_map>
 #include <stdexcept>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -1099,7 +1100,13 @@ void on_threads(int device, int n, F fn) {
         }
     };
     std::vector<std::thread> pool;
-    for (int i = 1; i < n; ++i) pool.emplace_back(run, i);
+    for (int i = 1; i < n; ++i) {
+        try {
+            pool.emplace_back(run, i);
+        } catch (const std::system_error &) {
+            run(i);  // no thread to be had: the task runs here, in order
+        }
+    }
     run(0);
     for (auto &th : pool) th.join();
     for (int i = 0; i < n; ++i)
