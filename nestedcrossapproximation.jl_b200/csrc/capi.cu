@@ -1246,7 +1246,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             if (items.empty()) continue;
             const size_t sm = level_smem_bytes(mc, nc);
             if (sm > size_t(kMaxSmem))
-                throw Failure(NCA_ERR_ARG, "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
+                throw Failure(NCA_ERR_ARG,
+                              "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
             level_smem_at_least(sm);
             if (!chunk.p || size_t(bound) > chunk.n) chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
             upload_reuse(dlvoff, lvoff, s);
@@ -1314,7 +1315,9 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             for (size_t l = 0; l < levelX.size(); ++l) {
                 int64_t lt = 0;
                 for (int it : levelItems[l]) lt += pad2(int64_t(d.h_nrows[it]) * d.h_rank[it]);
-                if (lt) CK(cudaMemcpyAsync(d.X.p + off, levelX[l]->p, sizeof(double2) * lt, cudaMemcpyDeviceToDevice, s));
+                if (lt)
+                    CK(cudaMemcpyAsync(d.X.p + off, levelX[l]->p, sizeof(double2) * lt, cudaMemcpyDeviceToDevice,
+                                       s));
                 off += lt;
             }
             CK(cudaStreamSynchronize(s));
@@ -1428,8 +1431,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             drows.upload(tr_rows, s);
             dcols.upload(tr_cols, s);
             dctoff.upload(ctoff, s);
-            launch_transpose_blocks<double2>(CN.M.p, din.p, drows.p, dcols.p, dctoff.p, int64_t(ps.farnodes.size()), CTs.M.p,
-                                             s);
+            launch_transpose_blocks<double2>(CN.M.p, din.p, drows.p, dcols.p, dctoff.p, int64_t(ps.farnodes.size()),
+                                             CTs.M.p, s);
             CK(cudaGetLastError());
         }
     };
