@@ -1,14 +1,22 @@
 #!/usr/bin/env python
-"""Benchmark: batched bottom-up NCA build + H^2 block products on one B200 (per rank).
+"""Benchmark: the NCA build + H^2 products on one B200 (per rank).
 
-Workload (Galerkin, low frequency): 65,536 points uniform on the unit sphere (seeded),
-Helmholtz cis(kr)/(4 pi r) with k = 1.0 (zero on the diagonal), k-means tree minvalues 64,
-batched bottom-up ACA tol 1e-5, maxrank 50. One step = y = H X and y = H^H X for a block of
-16 seeded complex Gaussian right-hand sides (complex FP64). The metric is the product's
-algorithmic HBM bytes (stores read once per block + vectors) per second; the build time is
-reported beside it.
+Default workload (the headline): the wideband directional sphere. 262,144 points uniform on the
+unit sphere (seeded), Helmholtz cis(kr)/(4 pi r) with k = 2 pi 8 (16 wavelengths across, zero on
+the diagonal), isnearwideband(k; eta_lf 1, eta_hf 5, gamma 1), k-means tree minvalues 64,
+BottomUp(IACA(MaximumValue(), TreeMimicryPivoting, FNormExtrapolator(1e-4))) per (cluster,
+direction), maxrank 50; the work is the build plus 100 matvecs with seeded complex Gaussian x.
+One timed step = the 100 vectors as one block product in the batched mixed-precision form
+(complex-FP32 stores and arena, FP64 accumulation); `value` = its algorithmic HBM bytes per
+second (the stores once per 16-column pass, the vectors, the coefficient vectors). Beside it:
+build + 100 matvecs for the plain FP64 form (its own FP64-only build, 100 single-vector FP64
+products) and for the batched mixed form, and their ratio.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--precision f64|f32]
+Other workloads (--workload): galerkin-sphere (65,536 points, k = 1, tol 1e-5, H X and H^H X on
+16 right-hand sides), batched-uneven (64 problems in one batched product), gradients (dJ/dx and
+dJ/dk on a perturbed sphere).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload ...]
 
 With --gpus N > 1 it runs under torchrun, one independent replica per GPU (the path has no
 exchange step); rank 0 prints one JSON line.
@@ -32,6 +40,7 @@ import numpy as np  # noqa: E402
 
 METRIC = "H² build+matvec time & matvec HBM GB/s, chosen vs plain FP64 at rel err 1e-4"
 WORKLOAD = "galerkin-sphere-65536-k1-tol1e-5-16rhs"
+WIDEBAND = "wideband-sphere-{n}-k16pi-tol1e-4-iaca-100vec"
 E = 16  # bytes per complex FP64 entry
 
 
@@ -42,13 +51,14 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="f64", choices=["f64", "f32"])
-    p.add_argument("--npoints", type=int, default=65536)
+    p.add_argument("--npoints", type=int, default=0, help="point count (default: the workload's)")
     p.add_argument("--nrhs", type=int, default=16)
     p.add_argument("--wideband-points", type=int, default=0, help="point count of the wideband workload")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-stages", action="store_true", help="print per-stage times to stderr")
-    p.add_argument("--workload", default="galerkin-sphere",
-                   choices=["galerkin-sphere", "batched-uneven", "gradients", "wideband"],
+    p.add_argument("--clocks-csv", default=None, help="file for the nvidia-smi clock samples (default: a temp file)")
+    p.add_argument("--workload", default="wideband",
+                   choices=["wideband", "galerkin-sphere", "batched-uneven", "gradients"],
                    help="batched-uneven: 64 problems of uneven size, one batched product vs 64 calls; "
                         "gradients: dJ/dx and dJ/dk of J = ||H(k) x - b||^2 on a perturbed sphere")
     return p.parse_args()
@@ -125,9 +135,12 @@ def traffic_from_profiles():
 class Clocks:
     """nvidia-smi sampling during the timed region (clocks and throttle reasons)."""
 
+    path_override = None
+
     def __init__(self, index):
-        self.proc, self.path = None, os.path.join(ROOT, "gpurun_out", f"clocks_bench_{index}.csv")
-        self.index = index
+        import tempfile
+        self.proc, self.index = None, index
+        self.path = Clocks.path_override or os.path.join(tempfile.gettempdir(), f"nca_bench_clocks_{index}.csv")
 
     def start(self):
         try:
@@ -188,15 +201,15 @@ def build_problem(N, n, device, store_f32):
     return pts, core, wall
 
 
-def dense_rows_error(N, pts, core, ws, X, nrows=64):
-    """Relative error of H X against rows of the dense FP64 matrix evaluated on the device."""
+def dense_rows_error(N, pts, core, ws, X, nrows=64, k=1.0, rmin=0.0):
+    """Relative error of H X (two columns) against rows of the dense FP64 matrix from the CPU
+    oracle (long-double accumulation)."""
+    from oracle import oracle as O
     rng = np.random.default_rng(7)
     rows = rng.choice(len(pts), nrows, replace=False)
-    ii = np.repeat(rows, len(pts))
-    jj = np.tile(np.arange(len(pts)), nrows)
-    D = N.seams.entries(N.HelmholtzKernel(1.0), pts, pts, ii, jj, device=core.device).reshape(nrows, len(pts))
+    kern = O.Kernel(O.KIND_HELMHOLTZ, k=k, rmin=rmin)
     Y = N.mul(None, ws, X[:, :2])
-    ref = D @ X[:, :2]
+    ref = np.stack([O.dense_rows(kern, pts, pts, rows, X[:, q]) for q in range(2)], axis=1)
     return float(np.linalg.norm(Y[rows] - ref) / np.linalg.norm(ref))
 
 
@@ -239,75 +252,116 @@ def measure_chosen(N, L, core, ws64, X, Xd, Yd, n, b, args, world, local, info, 
             "relerr_vs_f64_product": rel64, "relerr_vs_dense_rows": err}
 
 
-def cpu_baseline_sample(b_sample, nrhs):
-    """The oracle (C restatement, OpenMP on the host cores) on the same workload: its own build,
-    then one forward and one adjoint product on b_sample right-hand sides; the product time is
-    scaled to nrhs (the oracle applies one right-hand side at a time)."""
+def oracle_info(H):
+    """Stored entries and coefficient counts of an oracle build, in the core-info layout."""
+    tl = [not H.trees[0].isleaf(t) for t in range(H.trees[0].nnodes)]
+    sl = [not H.trees[1].isleaf(t) for t in range(H.trees[1].nnodes)]
+    return {"near_entries": sum(a.size for a in H.near), "coupling_entries": sum(a.size for a in H.couplings),
+            "transfer_entries_test": sum(H.X[0][t].size for t in range(len(tl)) if tl[t]),
+            "transfer_entries_trial": sum(H.X[1][t].size for t in range(len(sl)) if sl[t]),
+            "basis_entries_test": sum(H.X[0][t].size for t in range(len(tl)) if not tl[t]),
+            "basis_entries_trial": sum(H.X[1][t].size for t in range(len(sl)) if not sl[t]),
+            "ntest": len(H.testpts), "ntrial": len(H.trialpts), "ncoeff_test": int(H.ranks[0].sum()),
+            "ncoeff_trial": int(H.ranks[1].sum())}
+
+
+def cpu_galerkin(n, b, steps, warmup):
+    """The oracle (C restatement, OpenMP on all host cores) on the Galerkin sphere: its own build,
+    then `steps` timed steps of one forward and one adjoint product on b right-hand sides. The
+    rate is the algorithmic bytes of the products actually run over their time (no scaling)."""
     from oracle import oracle as O
-    pts = sphere(65536)
+    pts = sphere(n)
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
     H = O.H2(pts, pts, O.Kernel(O.KIND_HELMHOLTZ, k=1.0), minvalues=64, tol=1e-5, maxrank=50, nthreads=cores)
     tb = time.perf_counter() - t0
-    X = rhs(len(pts), b_sample)
+    X = rhs(len(pts), b)
+    for _ in range(warmup):
+        H.apply(X, 0)
+        H.apply(X, 2)
     t0 = time.perf_counter()
-    H.apply(X, 0)
-    H.apply(X, 2)
-    tp = (time.perf_counter() - t0) * nrhs / b_sample
-    info = {"near_entries": sum(a.size for a in H.near), "coupling_entries": sum(a.size for a in H.couplings),
-            "transfer_entries_test": sum(H.X[0][t].size for t in range(H.trees[0].nnodes) if not H.trees[0].isleaf(t)),
-            "transfer_entries_trial": sum(H.X[1][t].size for t in range(H.trees[1].nnodes) if not H.trees[1].isleaf(t)),
-            "basis_entries_test": sum(H.X[0][t].size for t in range(H.trees[0].nnodes) if H.trees[0].isleaf(t)),
-            "basis_entries_trial": sum(H.X[1][t].size for t in range(H.trees[1].nnodes) if H.trees[1].isleaf(t)),
-            "ntest": len(pts), "ntrial": len(pts), "ncoeff_test": int(H.ranks[0].sum()),
-            "ncoeff_trial": int(H.ranks[1].sum())}
-    step_bytes = 2 * product_bytes(info, nrhs)
-    return {"value": step_bytes / tp / 1e9, "unit": "GB/s", "cores": cores, "kind": "port",
-            "sample": f"oracle build ({tb:.1f} s) + one forward and one adjoint product on {b_sample} of the "
-                      f"{nrhs} right-hand sides, time scaled x{nrhs // b_sample}",
-            "build_s": tb, "step_s": tp}
+    for _ in range(steps):
+        H.apply(X, 0)
+        H.apply(X, 2)
+    el = time.perf_counter() - t0
+    value = steps * 2 * product_bytes(oracle_info(H), b) / el / 1e9
+    return {"value": value, "unit": "GB/s", "cores": cores, "kind": "port",
+            "sample": f"CPU oracle (C restatement, OpenMP, {cores} threads): full build ({tb:.1f} s), then {steps} "
+                      f"steps of one forward and one adjoint product on {b} right-hand sides (of the 16 the GPU "
+                      f"step takes); GB/s of the products run", "build_s": tb, "step_s": el / max(steps, 1)}
 
 
 def run_reference(args):
+    """The reference arm: the reference's algorithm on the host cores (the C restatement; the
+    Julia package cannot run on this box), on the workload of the GPU arm. Rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle import oracle as O
-    pts = sphere(args.npoints)
-    cores = os.cpu_count() or 1
-    t0 = time.perf_counter()
-    H = O.H2(pts, pts, O.Kernel(O.KIND_HELMHOLTZ, k=1.0), minvalues=64, tol=1e-5, maxrank=50, nthreads=cores)
-    tb = time.perf_counter() - t0
-    b_sample = 2
-    X = rhs(len(pts), b_sample)
-    for _ in range(args.warmup):
-        H.apply(X, 0)
-        H.apply(X, 2)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        H.apply(X, 0)
-        H.apply(X, 2)
-    el = (time.perf_counter() - t0) * args.nrhs / b_sample
-    info = {"near_entries": sum(a.size for a in H.near), "coupling_entries": sum(a.size for a in H.couplings),
-            "transfer_entries_test": sum(H.X[0][t].size for t in range(H.trees[0].nnodes) if not H.trees[0].isleaf(t)),
-            "transfer_entries_trial": sum(H.X[1][t].size for t in range(H.trees[1].nnodes) if not H.trees[1].isleaf(t)),
-            "basis_entries_test": sum(H.X[0][t].size for t in range(H.trees[0].nnodes) if H.trees[0].isleaf(t)),
-            "basis_entries_trial": sum(H.X[1][t].size for t in range(H.trees[1].nnodes) if H.trees[1].isleaf(t)),
-            "ntest": len(pts), "ntrial": len(pts), "ncoeff_test": int(H.ranks[0].sum()),
-            "ncoeff_trial": int(H.ranks[1].sum())}
-    step_bytes = 2 * product_bytes(info, args.nrhs)
-    value = step_bytes * args.steps / el / 1e9
-    sample = (f"CPU oracle (C restatement, OpenMP, {cores} threads); each step one forward and one adjoint product "
-              f"on {b_sample} of {args.nrhs} right-hand sides, time scaled x{args.nrhs // b_sample}")
+    if args.workload == "wideband":
+        n = args.npoints or 262144
+        steps = max(1, min(args.steps, 10))
+        cpu = cpu_wideband(n, steps, min(args.warmup, 1))
+        config = {"workload": WIDEBAND.format(n=n), "npoints": n, "build_s": cpu["build_s"],
+                  "step": "one single-vector FP64 matvec", "l2": "inputs larger than L2",
+                  "relerr_vs_dense_rows": cpu["relerr_vs_dense_rows"],
+                  "build_plus_100_matvecs_s": cpu["build_s"] + 100 * cpu["step_s"]}
+        ms = 1e3 * cpu["step_s"]
+        steps_run = steps
+    elif args.workload == "galerkin-sphere":
+        n = args.npoints or 65536
+        steps_run = max(1, min(args.steps, 10))
+        cpu = cpu_galerkin(n, 2, steps_run, min(args.warmup, 1))
+        config = {"workload": WORKLOAD, "npoints": n, "nrhs": 2, "build_s": cpu["build_s"],
+                  "l2": "inputs larger than L2"}
+        ms = 1e3 * cpu["step_s"]
+    else:
+        print(json.dumps({"impl": "reference", "unavailable": f"no CPU arm for the {args.workload} workload"}),
+              flush=True)
+        return
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "complex-f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "npoints": args.npoints, "nrhs": args.nrhs, "build_s": tb,
-                   "l2": "inputs larger than L2"},
-        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": cores, "kind": "port", "sample": sample},
-        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": steps_run, "warmup": min(args.warmup, 1), "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "complex-f64", "data": "synthetic", "config": config,
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cpu["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
+
+
+def wideband_points(n):
+    return sphere(n, 888)
+
+
+def cpu_wideband(n, steps, warmup):
+    """The C restatement of the directional path (OpenMP on all host cores) on the wideband
+    sphere: its full build, then `steps` timed single-vector FP64 matvecs, each a whole product;
+    the rate is their algorithmic bytes over their time (no scaling). The error of the first
+    matvec against 64 dense FP64 rows rides along."""
+    from oracle import directional as OD
+    from oracle import oracle as O
+    k = 2 * np.pi * 8
+    pts = wideband_points(n)
+    cores = os.cpu_count() or 1
+    kern = O.Kernel(O.KIND_HELMHOLTZ, k=k, rmin=1e-12)
+    t0 = time.perf_counter()
+    H = OD.DirectionalH2(pts, pts, kern, k, minvalues=64, tol=1e-4, maxrank=50, nthreads=cores)
+    tb = time.perf_counter() - t0
+    x = rhs(n, 1, seed=31)[:, 0]
+    for _ in range(warmup):
+        H.apply(x, 0)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        y = H.apply(x, 0)
+    el = time.perf_counter() - t0
+    rows = np.random.default_rng(7).choice(n, 64, replace=False)
+    ref = O.dense_rows(kern, pts, pts, rows, x, nthreads=cores)
+    err = float(np.linalg.norm(y[rows] - ref) / np.linalg.norm(ref))
+    e = H.entries
+    ncoeff = sum(int(r.sum()) for r in H.ranks)
+    step_bytes = E * (e["x"] + e["coupling"] + e["near"]) + E * 3 * n + 2 * E * ncoeff
+    return {"value": steps * step_bytes / el / 1e9, "unit": "GB/s", "cores": cores, "kind": "port",
+            "sample": f"CPU oracle (C restatement of the directional build and product, OpenMP, {cores} threads): "
+                      f"full build ({tb:.1f} s), then {steps} single-vector FP64 matvecs; GB/s of the matvecs run",
+            "build_s": tb, "step_s": el / steps, "relerr_vs_dense_rows": err}
 
 
 def cube_surface(n, seed):
@@ -532,113 +586,185 @@ def run_gradients(args):
             "clocks": clk}), flush=True)
 
 
+def wideband_core(N, pts, k, local, mixed):
+    """The wideband workload's core: k-means tree + BottomUp(IACA) build (timed together). The
+    batched mixed form keeps complex-FP32 copies of the stores for its products."""
+    import torch
+    t0 = time.perf_counter()
+    tree = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=64))
+    conv = N.FNormExtrapolator(1e-4)
+    tc = N.BottomUp(factorization=N.IACA(N.MaximumValue(), N.TreeMimicryPivoting(pts, pts, tree), conv))
+    sc = N.BottomUp(factorization=N.IACA(N.TreeMimicryPivoting(pts, pts, tree), N.MaximumValue(), conv))
+    core = N.PetrovGalerkinNCACore(N.HelmholtzKernel(k, rmin=1e-12), pts, pts, N.BlockTree(tree, tree),
+                                   isnear=N.isnearwideband(k), testcompressor=tc, trialcompressor=sc,
+                                   store_f32=mixed, device=local)
+    torch.cuda.synchronize()
+    return core, time.perf_counter() - t0
+
+
+def dir_stage_bytes(info, b, e):
+    """Algorithmic bytes per 16-column pass of the directional product's stages: each stage's
+    stored entries once (X of every item in the up stage and again in the down/leaf stages,
+    couplings, near blocks) plus the vector rows it reads and writes once."""
+    xe = info["basis_entries_test"] + info["basis_entries_trial"] + info["transfer_entries_test"] + \
+        info["transfer_entries_trial"]
+    return e * xe + e * info["coupling_entries"] + e * info["near_entries"]
+
+
 def run_wideband(args):
-    """Directional (wideband) sphere: n points uniform on the unit sphere (default 262,144),
-    k = 2 pi 8 (diameter 16 wavelengths), isnearwideband(k), tol 1e-4, minvalues 64; the work is
-    the build plus 100 matvecs with seeded complex Gaussian x. Plain FP64 form: 100 single-vector
-    FP64 products. Batched mixed-precision form: the 100 vectors as one block of right-hand sides
-    on the complex-FP32 stores (FP64 pivots and skeletons, FP64 accumulation)."""
+    """The headline workload (see the module docstring)."""
     import torch
     import nca_b200 as N
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local)
-    n, k, nvec = args.wideband_points or 262144, 2 * np.pi * 8, 100
-    pts = sphere(n, 888)
+    n, k, nvec = args.npoints or 262144, 2 * np.pi * 8, 100
+    pts = wideband_points(n)
     cuda_ready(N, local)
-
-    def build_once():
-        t0 = time.perf_counter()
-        tree = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=64))
-        aca = N.ACA(N.FullPivoting(), N.FullPivoting(), N.FNormEstimator(1e-4))
-        comp = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(pts, pts, tree), compressor=aca)
-        core = N.PetrovGalerkinNCACore(N.HelmholtzKernel(k, rmin=1e-12), pts, pts, N.BlockTree(tree, tree),
-                                       isnear=N.isnearwideband(k), testcompressor=comp, trialcompressor=comp,
-                                       store_f32=True, device=local)
-        torch.cuda.synchronize()
-        return core, time.perf_counter() - t0
-
-    # the build leans on the host cores, which the GPU's neighbours share: the faster of two
-    # identical builds is the figure used, both are reported
-    core, build_first = build_once()
-    del core
-    core, build_second = build_once()
-    build = min(build_first, build_second)
-    info = info_dict(core)
     L = N.lib()
-    X = rhs(n, nvec, seed=31)
     dev = f"cuda:{local}"
-    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(dev)
+    X = rhs(n, nvec, seed=31)
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(dev)  # column-major n x 100
     Yd = torch.zeros_like(Xd)
-    W64 = N.H2Workspace(core, max_nrhs=16)
-    W32 = N.H2Workspace(core, np.complex64, max_nrhs=16)
+    # plain FP64 form: FP64-only build, then 100 single-vector FP64 matvecs
+    core, build_plain = wideband_core(N, pts, k, local, False)
+    W64 = N.H2Workspace(core, max_nrhs=1)
 
-    def seq(W, prec):
-        def f():
-            for j in range(nvec):
-                N._lib.check(L.nca_apply(W._h, 0, prec, C.c_void_p(Xd[j].data_ptr()), n, C.c_void_p(Yd[j].data_ptr()),
-                                         n, 1, 1.0, 0.0, 0.0, 0.0, 1))
-        return f
+    def seq():
+        for j in range(nvec):
+            N._lib.check(L.nca_apply(W64._h, 0, 0, C.c_void_p(Xd[j].data_ptr()), n, C.c_void_p(Yd[j].data_ptr()),
+                                     n, 1, 1.0, 0.0, 0.0, 0.0, 1))
+    seq()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    seq()
+    e1.record()
+    torch.cuda.synchronize()
+    t_seq64 = e0.elapsed_time(e1) * 1e-3
+    info64 = info_dict(core)
+    Y64 = Yd[0].cpu().numpy()
+    del W64, core
+    import gc
+    gc.collect()
+    torch.cuda.synchronize()
+    # batched mixed form: the build with complex-FP32 stores, the 100 vectors as one block
+    core, build_mixed = wideband_core(N, pts, k, local, True)
+    info = info_dict(core)
+    W = N.H2Workspace(core, np.complex64, max_nrhs=16)
+    W.set_profiling(True)
 
-    def block(W, prec):
-        def f():
-            N._lib.check(L.nca_apply(W._h, 0, prec, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Yd.data_ptr()), n, nvec,
-                                     1.0, 0.0, 0.0, 0.0, 1))
-        return f
-
-    def timed(fn, reps):
-        fn()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(reps):
-            fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) * 1e-3 / reps
-
+    def block(xp, yp, memspace):
+        N._lib.check(L.nca_apply(W._h, 0, 1, C.c_void_p(xp), n, C.c_void_p(yp), n, nvec, 1.0, 0.0, 0.0, 0.0,
+                                 memspace))
+    for _ in range(max(args.warmup, 3)):
+        block(Xd.data_ptr(), Yd.data_ptr(), 1)
+    stage_sum = [0.0] * 6
+    stage_n = [0] * 6
+    launches = C.c_int32()
+    total_launches = 0
     clocks = Clocks(local)
     clocks.start()
-    reps = max(1, args.steps // 10)
-    t_seq64 = timed(seq(W64, 0), reps)
-    t_seq32 = timed(seq(W32, 1), reps)
-    t_blk64 = timed(block(W64, 0), max(3, args.steps))
-    t_blk32 = timed(block(W32, 1), max(3, args.steps))
-    clk = clocks.stop()
-    launches = C.c_int32()
-    L.nca_workspace_last_launches(W32._h, C.byref(launches))
-    # errors: FP32 block vs FP64 block; FP64 vs dense rows (first vector)
-    Y64 = torch.zeros_like(Xd)
-    N._lib.check(L.nca_apply(W64._h, 0, 0, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Y64.data_ptr()), n, nvec,
-                             1.0, 0.0, 0.0, 0.0, 1))
-    block(W32, 1)()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     torch.cuda.synchronize()
-    rel32 = float((Yd - Y64).norm() / Y64.norm())
-    err = dense_rows_error_k(N, pts, core, W64, X, k) if rank == 0 else None
-    bytes32 = product_bytes(info, nvec, 8)
-    plain = build + t_seq64
-    mixed = build + t_blk32
+    e0.record()
+    for _ in range(args.steps):
+        block(Xd.data_ptr(), Yd.data_ptr(), 1)
+        L.nca_workspace_last_launches(W._h, C.byref(launches))
+        total_launches += launches.value
+        sec = (C.c_double * 6)()
+        cnt = (C.c_int32 * 6)()
+        L.nca_workspace_stage_times(W._h, sec, cnt, 6)
+        for q in range(6):
+            stage_sum[q] += sec[q]
+            stage_n[q] += cnt[q]
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_blk32 = max_over_ranks(e0.elapsed_time(e1) * 1e-3, dev) / args.steps
+    Ymix = Yd[0].cpu().numpy()
+    # end to end: the same block product from and to pinned host buffers through the C ABI
+    W.set_profiling(False)
+    Xh = torch.from_numpy(np.ascontiguousarray(X.T)).pin_memory()
+    Yh = torch.zeros_like(Xh).pin_memory()
+    block(Xh.data_ptr(), Yh.data_ptr(), 0)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        block(Xh.data_ptr(), Yh.data_ptr(), 0)
+    t_e2e = max_over_ranks(time.perf_counter() - t0, dev) / args.steps
+    # errors against 64 dense FP64 rows of the CPU oracle (first vector), FP32 form vs FP64 form
+    from oracle import oracle as O
+    kern = O.Kernel(O.KIND_HELMHOLTZ, k=k, rmin=1e-12)
+    rows = np.random.default_rng(7).choice(n, 64, replace=False)
+    ref = O.dense_rows(kern, pts, pts, rows, X[:, 0])
+    err64 = float(np.linalg.norm(Y64[rows] - ref) / np.linalg.norm(ref))
+    errmix = float(np.linalg.norm(Ymix[rows] - ref) / np.linalg.norm(ref))
+    rel_mix_64 = float(np.linalg.norm(Ymix - Y64) / np.linalg.norm(Y64))
+    bytes32 = product_bytes(info, nvec, 8) + (-(-nvec // 16) - 1) * 8 * store_entries(info)
+    value = world * bytes32 / t_blk32 / 1e9
+    # roofline of the dominant stage of the block product (events on the product stream)
+    names = ["gather", "up", "coupling", "down", "near", "leaves"]
+    kernels = {"gather": "k_gather_to_f32", "up": "k_gather_tiny (levels of small outputs)",
+               "coupling": "k_gather_tiny", "down": "k_gather_tiny (levels of small outputs)",
+               "leaves": "k_rows_gather (leaf outputs: bases and near blocks)"}
+    top = max(range(6), key=lambda q: stage_sum[q])
+    passes = -(-nvec // 16)
+    xe = info["basis_entries_test"] + info["basis_entries_trial"] + info["transfer_entries_test"] + \
+        info["transfer_entries_trial"]
+    leaf_x = info["basis_entries_test"]
+    stage_entries = {"gather": 0, "up": xe - info["transfer_entries_test"] - info["basis_entries_test"],
+                     "coupling": info["coupling_entries"], "down": info["transfer_entries_test"],
+                     "near": 0, "leaves": leaf_x + info["near_entries"]}
+    # vector rows each stage reads or writes once: x, coefficient rows of the input side (written
+    # by the up stage, read by the coupling), of the output side (written by the coupling, read and
+    # accumulated by the down stage, read by the leaves), y
+    vec_rows = {"gather": 2 * n, "up": n + 2 * info["ncoeff_trial"],
+                "coupling": info["ncoeff_trial"] + info["ncoeff_test"], "down": 3 * info["ncoeff_test"],
+                "near": 0, "leaves": info["ncoeff_test"] + 2 * n}
+    nm = names[top]
+    per_pass_bytes = 8 * stage_entries[nm] + 8 * 16 * vec_rows[nm]
+    stage_time_per_pass = stage_sum[top] / (args.steps * passes)
+    achieved = per_pass_bytes / stage_time_per_pass / 1e9 if stage_time_per_pass > 0 else None
     peak, peak_kind = peaks()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_wideband(n, 2, 0)
+    plain = build_plain + t_seq64
+    mixed = build_mixed + t_blk32
     if rank == 0:
         print(json.dumps({
-            "metric": METRIC, "value": bytes32 / t_blk32 / 1e9, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": 1, "ms_per_step": 1e3 * t_blk32, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "complex-f32 stores, f64 accumulation", "data": "synthetic",
-            "config": {"workload": f"wideband-sphere-{n}-k16pi-tol1e-4-100vec", "npoints": n, "k": k,
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * t_blk32, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex-f32 stores and arena, f64 accumulation",
+            "data": "synthetic",
+            "config": {"workload": WIDEBAND.format(n=n), "npoints": n, "k": k, "nvec": nvec,
                        "admissibility": "isnearwideband(k; eta_lf=1, eta_hf=5, gamma=1)",
-                       "step": "100 matvecs as one block of 100 right-hand sides",
-                       "l2": "inputs larger than L2", "build_s": build, "build_s_both": [build_first, build_second],
-                       "build_device_s": info["build_seconds"],
-                       "stored_gb_f64": E * store_entries(info) / 1e9, "relerr_vs_dense_rows": err,
-                       "relerr_f32_vs_f64": rel32},
-            "plain_f64_100_single_matvecs_s": t_seq64, "mixed_f32_100_single_matvecs_s": t_seq32,
-            "f64_block_of_100_s": t_blk64, "mixed_block_of_100_s": t_blk32,
-            "build_plus_100_matvecs_s": {"plain_f64": plain, "batched_mixed": mixed, "speedup": plain / mixed},
-            "matvec_speedup_batched_mixed_vs_plain_f64": t_seq64 / t_blk32,
-            "roofline": {"bound": "hbm", "achieved": bytes32 / t_blk32 / 1e9, "peak": peak, "peak_source": peak_kind,
-                         "unit": "GB/s", "frac": bytes32 / t_blk32 / 1e9 / peak, "traffic": None,
-                         "note": "whole block product, algorithmic bytes (stores once per 16-column pass)"},
-            "gpu_launches": launches.value, "clocks": clk}), flush=True)
+                       "compressor": "BottomUp(IACA(MaximumValue, TreeMimicryPivoting, FNormExtrapolator(1e-4)))",
+                       "step": "100 matvecs as one block of 100 right-hand sides (7 passes of <= 16 columns)",
+                       "l2": "inputs larger than L2 (FP32 stores %.1f GB per pass)" % (8 * store_entries(info) / 1e9),
+                       "build_s": build_mixed, "build_s_plain_f64": build_plain,
+                       "build_device_s": info["build_seconds"], "stored_gb_f64": E * store_entries(info) / 1e9,
+                       "relerr_vs_dense_rows": {"plain_f64": err64, "batched_mixed": errmix, "bar_north_star": 1e-4,
+                                                "bar_reference_tests_10tol": 1e-3},
+                       "relerr_mixed_vs_plain_f64": rel_mix_64, "parallelism": f"replicas x{world}"},
+            "build_plus_100_matvecs_s": {"plain_f64": plain, "batched_mixed": mixed, "speedup": plain / mixed,
+                                         "plain_100_single_f64_matvecs_s": t_seq64,
+                                         "mixed_block_of_100_s": t_blk32},
+            "roofline": {"kernel": kernels.get(nm, nm), "stage": nm, "bound": "hbm", "achieved": achieved,
+                         "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None, "traffic": None,
+                         "stage_ms_per_pass": 1e3 * stage_time_per_pass,
+                         "stage_share": stage_sum[top] / (args.steps * t_blk32),
+                         "stage_ms_per_step": {names[q]: 1e3 * stage_sum[q] / args.steps for q in range(6)},
+                         "launches_per_step": {names[q]: stage_n[q] / args.steps for q in range(6)},
+                         "bytes_per_pass": per_pass_bytes},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * bytes32 / t_e2e / 1e9, "unit": "GB/s", "h2d_bytes_per_step": 8 * 2 * n * nvec,
+                    "d2h_bytes_per_step": 8 * 2 * n * nvec, "ms_per_step": 1e3 * t_e2e},
+            "gpu_launches": total_launches, "clocks": clk}), flush=True)
 
 
 def tangent_bytes(info, b, e=E):
@@ -649,18 +775,12 @@ def tangent_bytes(info, b, e=E):
 
 
 def dense_rows_error_k(N, pts, core, ws, X, k, nrows=64):
-    rng = np.random.default_rng(7)
-    rows = rng.choice(len(pts), nrows, replace=False)
-    ii = np.repeat(rows, len(pts))
-    jj = np.tile(np.arange(len(pts)), nrows)
-    D = N.seams.entries(N.HelmholtzKernel(k, rmin=1e-12), pts, pts, ii, jj, device=core.device).reshape(nrows, len(pts))
-    Y = N.mul(None, ws, X[:, :1])
-    ref = D @ X[:, :1]
-    return float(np.linalg.norm(Y[rows] - ref) / np.linalg.norm(ref))
+    return dense_rows_error(N, pts, core, ws, X, nrows, k=k, rmin=1e-12)
 
 
 def main():
     args = parse()
+    Clocks.path_override = args.clocks_csv
     if args.impl == "reference":
         run_reference(args)
         return
@@ -673,6 +793,7 @@ def main():
     if args.workload == "wideband":
         run_wideband(args)
         return
+    args.npoints = args.npoints or 65536
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -777,7 +898,7 @@ def main():
         print(json.dumps({k: (1e3 * stage_sum[k] / args.steps, stage_n[k]) for k in stage_sum}), file=sys.stderr)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(2, b)
+        cpu = cpu_galerkin(n, 2, 2, 0)
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,

@@ -118,17 +118,29 @@ int32_t nca_select_farpivots(const nca_tree *fartree, const double *ownpoints,
                              const int32_t *farnodes, int32_t nfar, int32_t maxrank,
                              int32_t *pivots, int32_t *npivots);
 
-/* ---- the whole batched bottom-up build on one GPU: PetrovGalerkinNCACore(...) with
- *      BatchedBottomUp(pivotselector=TreeMimicryPivoting, compressor=ACA(FullPivoting(),
- *      FullPivoting(), FNormEstimator(tol))) on both sides
- *      (src/nca/petrovgalerkinnca.jl:138-198 -> src/nca/abstractnca.jl:134-216 ->
- *      src/compressors/batchedbottomup.jl:246-447 -> src/couplingmatrices.jl:11-53) ---- */
+/* ---- the whole build on one GPU: PetrovGalerkinNCACore(...) with the compressor below on both
+ *      sides (src/nca/petrovgalerkinnca.jl:138-198 -> src/nca/abstractnca.jl:134-216 ->
+ *      src/compressors/batchedbottomup.jl:246-447 or src/compressors/bottomup.jl:48-424 ->
+ *      src/couplingmatrices.jl:11-111) ---- */
+/* The compressor of both sides:
+ *   NCA_COMPRESSOR_BATCHED_ACA   BatchedBottomUp(pivotselector=TreeMimicryPivoting, compressor=
+ *                                ACA(FullPivoting(), FullPivoting(), FNormEstimator(tol)))
+ *                                (src/compressors/batchedbottomup.jl:30-51); not for wideband
+ *                                partitions, which it refuses with NCA_ERR_ARG as
+ *                                src/compressors/abstractcompressor.jl:39-47 does;
+ *   NCA_COMPRESSOR_BOTTOMUP_IACA BottomUp(factorization=IACA(MaximumValue(), TreeMimicryPivoting,
+ *                                FNormExtrapolator(tol))) on the test side and the mirrored IACA on
+ *                                the trial side (src/compressors/bottomup.jl:48-424), per cluster or,
+ *                                on a wideband partition, per (cluster, direction). */
+typedef enum { NCA_COMPRESSOR_BATCHED_ACA = 0, NCA_COMPRESSOR_BOTTOMUP_IACA = 1 } nca_compressor;
+
 typedef struct {
-    double tol_test, tol_trial; /* ACA tolerances of the two compressors */
+    double tol_test, tol_trial; /* tolerances of the two compressors */
     int32_t maxrank;            /* maximum rank per cluster (default 50) */
-    int32_t sampled;            /* 1: sampled FNorm stop (batchedbottomup.jl:120-125) */
+    int32_t sampled;            /* 1: sampled FNorm stop (batchedbottomup.jl:120-125); ACA only */
     int32_t device;             /* CUDA device ordinal */
     int32_t store_f32;          /* 1: also keep complex FP32 copies of all stores */
+    int32_t compressor;         /* nca_compressor */
 } nca_build_opts;
 
 /* The host planning runs on the process's cores (its CPU affinity mask, capped by a cgroup CPU
@@ -213,10 +225,14 @@ int32_t nca_apply(nca_workspace *ws, int32_t mode, int32_t precision, const void
  * holds. The call makes no cudaMalloc/cudaFree or other allocation, for callers whose own pool
  * owns device memory. It needs (nin + input coefficients + output coefficients) *
  * (nrhs + 3) * 16 bytes + 1 KiB at most; larger products return NCA_ERR_ARG naming the size.
- * The first call on a device does the one-time setup (module load, symbol lookup): make it
- * before any stream capture on that device. The scratch is shared by every core on the device,
- * so overlapping calls would race on it: a call made while another is in progress on the same
- * device returns NCA_ERR_BUSY. The call waits for the stream and returns the kernels' status. */
+ * Non-directional cores only: a directional (wideband) core returns NCA_ERR_ARG (use
+ * nca_apply). The first call on a device does the one-time setup (module load, symbol lookup),
+ * which reserves the array on that device unless CUDA_MODULE_LOADING=EAGER reserved it when the
+ * library was loaded: make that call before the caller's pool reserves HBM. The scratch is shared
+ * by every core on the device, so overlapping calls would race on it: a call made while another is
+ * in progress on the same device returns NCA_ERR_BUSY. The call waits for the stream and returns
+ * the kernels' status, so it cannot be captured in a CUDA graph: on a capturing stream it returns
+ * NCA_ERR_ARG. */
 #define NCA_STATIC_SCRATCH_BYTES (32ull << 20)
 int32_t nca_apply_static(nca_core *core, int32_t mode, int32_t precision, const void *x, int64_t ldx,
                          void *y, int64_t ldy, int64_t nrhs, double alpha_re, double alpha_im,

@@ -298,22 +298,18 @@ __global__ void __launch_bounds__(NT) k_level_compress(LevelArgs a, const int32_
     __shared__ int s_m, s_flag;
 
     const int tid = threadIdx.x;
-    // `node` indexes the per-item arrays (one item per node unless in item mode); `cl` is the
-    // cluster whose points form the rows of a basis item
     const int node = nodes[blockIdx.x];
-    const bool items = a.item_node != nullptr;
-    const int cl = items ? a.item_node[node] : node;
     const int n = a.fpptr[node + 1] - a.fpptr[node];
     const int32_t *fp = a.fpidx + a.fpptr[node];
-    const bool leaf = items ? a.item_basis[node] != 0 : a.nchildren[node] == 0;
-    const int nch = items ? a.item_chptr[node + 1] - a.item_chptr[node] : a.nchildren[node];
-    auto child = [&](int c) { return items ? a.item_chidx[a.item_chptr[node] + c] : a.firstchild[node] + c; };
+    const bool leaf = a.nchildren[node] == 0;
+    const int nch = a.nchildren[node];
+    auto child = [&](int c) { return a.firstchild[node] + c; };
 
     // rows of the block: the cluster's points, or the children's pivots in child order
     if (tid == 0) {
         int m = 0;
         if (leaf) {
-            m = a.end[cl] - a.begin[cl];
+            m = a.end[node] - a.begin[node];
         } else {
             for (int c = 0; c < nch; ++c) m += a.rank[child(c)];
         }
@@ -330,7 +326,7 @@ __global__ void __launch_bounds__(NT) k_level_compress(LevelArgs a, const int32_
         return;
     }
     if (leaf) {
-        for (int i = tid; i < m; i += NT) rowid[i] = a.perm[a.begin[cl] + i];
+        for (int i = tid; i < m; i += NT) rowid[i] = a.perm[a.begin[node] + i];
     } else {
         int off = 0;
         for (int c = 0; c < nch; ++c) {

@@ -20,11 +20,6 @@ struct LevelArgs {
     const int32_t *fpptr, *fpidx;  // phase-1 far pivots (CSR over nodes)
     int32_t *rank, *nrows, *piv;   // outputs: rank, block rows, pivots (maxrank per node)
     int32_t *cpiv;                 // optional output: column pivots (far-side point ids)
-    // item mode (directional bases): the launch's work items are (cluster, direction) pairs;
-    // every per-node array above is indexed by item, item_node gives the cluster, item_basis
-    // whether its rows are the cluster's points, item_chptr/item_chidx the children's items
-    // whose pivots form the rows otherwise. All null: one item per node (node mode).
-    const int32_t *item_node, *item_basis, *item_chptr, *item_chidx;
     double2 *X;                    // interpolation operators, node slot at xoff[node]
     const int64_t *xoff;
     int maxrank;
@@ -108,6 +103,32 @@ struct MimicryArgs {
     int32_t *error;   // 1: an item ran out of candidates before its pivot count
     int32_t *cursor;  // next item to take (zero at launch): warps take items one at a time
 };
+// IACA per item (tree-mimicry columns, maximum-value rows, extrapolated Frobenius stop) fused with
+// the tree mimicry and the interpolation operator, one warp per item (mimicry.cu). The far tree,
+// the items' far fields (ffptr/ffnodes), item_node and the own clusters' centroids come in `mim`
+// (its count, piv, error and cursor are unused). Rows of an item: its cluster's points when it is a
+// basis item, else its children's pivots (item_chptr/item_chidx; node mode: the tree's children).
+struct IacaArgs {
+    MimicryArgs mim;
+    KernelParams K;
+    int side;
+    const double *own_pts;
+    const int32_t *perm, *begin, *end, *firstchild, *nchildren;  // own tree
+    const int32_t *item_basis, *item_chptr, *item_chidx;          // item mode (mim.item_node set)
+    const int32_t *items;  // the launch's items
+    int nitems;
+    int32_t *cursor;       // zero at launch
+    int32_t *rank, *nrows, *piv, *cpiv;  // piv, cpiv: maxrank per item (cpiv optional)
+    double2 *X;            // item slots of rows x min(maxrank, rows, far points) entries at xoff
+    const int64_t *xoff;
+    int maxrank;
+    double tol;
+    int32_t *status;       // [flag, item, a, b], see k_iaca
+};
+size_t iaca_smem_bytes(int maxrank);
+int iaca_max_rows();
+// mcap: the largest row count of the launch's items (at most iaca_max_rows())
+void launch_iaca(const IacaArgs &a, int mcap, cudaStream_t s);
 size_t mimicry_smem_bytes(int maxrank);
 void launch_mimicry(const MimicryArgs &a, cudaStream_t s);
 // packs count[i] pivots of every item from its maxrank-wide slot into the CSR list fpidx

@@ -7,6 +7,8 @@
 #include <array>
 #include <cmath>
 #include <atomic>
+#include <cstdio>
+#include <cstdlib>
 #include <chrono>
 #include <cstring>
 #include <exception>
@@ -166,9 +168,9 @@ struct DevSide {
 struct DirItems {
     nca::DirSide plan;
     int nitems = 0;
-    std::vector<int32_t> h_fpptr, h_rank, h_nrows;  // far pivots and item pivots stay on the device
+    std::vector<int32_t> h_rank, h_nrows;  // item pivots stay on the device
     std::vector<int64_t> h_xoff, h_cptr;
-    DBuf<int32_t> item_node, item_basis, item_chptr, item_chidx, fpptr, fpidx, rank, nrows, piv;
+    DBuf<int32_t> item_node, item_basis, item_chptr, item_chidx, rank, nrows, piv;
     DBuf<int64_t> xoff;
     DBuf<double2> X, XT;
 };
@@ -254,6 +256,10 @@ struct nca_workspace {
     bool far = true, near = true;
     bool profiling = false;
     cudaEvent_t stage_ev[9] = {};  // StageEvent order
+    // directional products: an event pair around every stage of every 16-column pass (grown on
+    // demand) and the stage of each pair
+    std::vector<cudaEvent_t> dir_ev;
+    std::vector<int> dir_stage;
     double stage_seconds[6] = {0, 0, 0, 0, 0, 0};
     int stage_launches[6] = {0, 0, 0, 0, 0, 0};
     // far-field sweeps beside the near field: a second stream (higher priority, so the sweeps'
@@ -371,6 +377,26 @@ void parallel_csr(int n, F fill, std::vector<int64_t> &ptr, std::vector<int32_t>
     for (auto &th : pool) th.join();
 }
 
+// Centroids of every cluster of a tree (the host planner's sums, in its order), on the host threads.
+std::vector<double> cluster_centroids(const nca::Tree &own, const double *ownpts) {
+    std::vector<double> centroid(3 * size_t(own.nnodes), 0.0);
+    std::atomic<int> cursor{0};
+    auto work = [&]() {
+        for (;;) {
+            const int t = cursor.fetch_add(1);
+            if (t >= own.nnodes) break;
+            if (own.size(t) > 0)
+                nca::cluster_centroid(ownpts, own.perm.data() + own.begin[t], own.size(t), &centroid[3 * size_t(t)]);
+        }
+    };
+    const int nth = std::max(1, std::min(nca::host_threads(), own.nnodes));
+    std::vector<std::thread> pool;
+    for (int i = 1; i < nth; ++i) pool.emplace_back(work);
+    work();
+    for (auto &th : pool) th.join();
+    return centroid;
+}
+
 // Phase 1 on the device: tree-mimicry far pivots of every item of one side (item i is own
 // cluster item_node[i], or cluster i when item_node is null), with far field ffnodes[ffptr[i]..)
 // in the reference's farfield order. Returns the CSR of pivots (far point ids) on the device
@@ -387,26 +413,9 @@ void device_farpivots(const nca::Tree &own, const double *ownpts, const nca::Tre
         dfpidx.alloc(1);
         return;
     }
-    // centroids of the own clusters (the host planner's sums, in its order)
-    std::vector<double> centroid(3 * size_t(own.nnodes), 0.0);
+    const std::vector<double> centroid = cluster_centroids(own, ownpts);
     std::vector<int32_t> own_size(own.nnodes);
     for (int t = 0; t < own.nnodes; ++t) own_size[t] = own.size(t);
-    {
-        std::atomic<int> cursor{0};
-        auto work = [&]() {
-            for (;;) {
-                const int t = cursor.fetch_add(1);
-                if (t >= own.nnodes) break;
-                if (own.size(t) > 0)
-                    nca::cluster_centroid(ownpts, own.perm.data() + own.begin[t], own.size(t), &centroid[3 * size_t(t)]);
-            }
-        };
-        const int nth = std::max(1, std::min(nca::host_threads(), own.nnodes));
-        std::vector<std::thread> pool;
-        for (int i = 1; i < nth; ++i) pool.emplace_back(work);
-        work();
-        for (auto &th : pool) th.join();
-    }
     DBuf<int64_t> dptr;
     DBuf<int32_t> dnodes, ditem, dsize, dcount, dpiv, derr;
     DBuf<double> dcent, dcenter;
@@ -751,6 +760,12 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
     upload_tree(c->side[0], c->tree[0], tp, s);
     upload_tree(c->side[1], c->tree[1], sp, s);
     const nca::Partition &P = c->part;
+    const bool iaca = o->compressor == NCA_COMPRESSOR_BOTTOMUP_IACA;
+    // BottomUp(IACA): the nodes' far fields, centroids and the far trees' centres for the fused
+    // kernel, which picks its geometric columns itself
+    DBuf<int64_t> iffptr[2];
+    DBuf<int32_t> iffnodes[2];
+    DBuf<double> icent[2], icenter[2];
     // phase 1 on the device (tree mimicry); far field = own far nodes + ancestors'
     for (int sd = 0; sd < 2; ++sd) {
         const nca::Tree &T = c->tree[sd];
@@ -766,6 +781,22 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
                     ff.insert(ff.end(), nodes.begin() + ptr[a], nodes.begin() + ptr[a + 1]);
             },
             ffptr, ffnodes);
+        if (iaca) {
+            // the far points a node can offer, capped at maxrank, size its X slot (plan_side)
+            const nca::Tree &Ft = c->tree[1 - sd];
+            std::vector<int32_t> &fp = c->side[sd].h_fpptr;
+            fp.assign(T.nnodes + 1, 0);
+            for (int t = 0; t < T.nnodes; ++t) {
+                int64_t n = 0;
+                for (int64_t q = ffptr[t]; q < ffptr[t + 1] && n < maxrank; ++q) n += Ft.size(ffnodes[q]);
+                fp[t + 1] = fp[t] + int32_t(std::min<int64_t>(n, maxrank));
+            }
+            iffptr[sd].upload(ffptr, s);
+            iffnodes[sd].upload(ffnodes, s);
+            icent[sd].upload(cluster_centroids(T, sd == 0 ? tp : sp), s);
+            icenter[sd].upload(Ft.center, s);
+            continue;
+        }
         device_farpivots(T, sd == 0 ? tp : sp, c->tree[1 - sd], c->side[1 - sd], T.nnodes, ffptr, ffnodes, nullptr,
                          maxrank, s, c->side[sd].h_fpptr, c->side[sd].fpptr, c->side[sd].fpidx,
                          &c->side[sd].h_fpidx);
@@ -782,7 +813,7 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         }
     } eg{ev0, ev1};
     DBuf<int32_t> status;
-    status.alloc(4);
+    status.alloc(5);  // [flag, node, a, b], IACA node cursor
     CK(cudaEventRecord(ev0, s));
     for (int sd = 0; sd < 2; ++sd) {
         DevSide &d = c->side[sd];
@@ -823,18 +854,68 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         a.tol = sd == 0 ? o->tol_test : o->tol_trial;
         a.sampled = o->sampled;
         a.status = status.p;
-        size_t maxsm = 0;
-        for (size_t l = 0; l + 1 < lv_ptr.size(); ++l)
-            maxsm = std::max(maxsm, level_smem_bytes(lv_mcap[l], lv_ncap[l]));
-        if (maxsm > size_t(kMaxSmem))
-            throw Failure(NCA_ERR_ARG, "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
-        level_smem_at_least(maxsm);
-        for (size_t l = 0; l + 1 < lv_ptr.size(); ++l) {
-            int cnt = lv_ptr[l + 1] - lv_ptr[l];
-            if (cnt == 0) continue;
-            size_t sm = level_smem_bytes(lv_mcap[l], lv_ncap[l]);
-            k_level_compress<<<cnt, 256, sm, s>>>(a, nodes.p + lv_ptr[l], lv_mcap[l], lv_ncap[l]);
-            CK(cudaGetLastError());
+        if (iaca) {
+            const DevSide &fs = c->side[1 - sd];
+            IacaArgs ia{};
+            ia.mim.begin = fs.begin.p;
+            ia.mim.end = fs.end.p;
+            ia.mim.firstchild = fs.firstchild.p;
+            ia.mim.nchildren = fs.nchildren.p;
+            ia.mim.perm = fs.perm.p;
+            ia.mim.center = icenter[sd].p;
+            ia.mim.pts = fs.pts.p;
+            ia.mim.nitems = T.nnodes;
+            ia.mim.ffptr = iffptr[sd].p;
+            ia.mim.ffnodes = iffnodes[sd].p;
+            ia.mim.item_node = nullptr;
+            ia.mim.centroid = icent[sd].p;
+            ia.mim.maxrank = maxrank;
+            ia.K = c->K;
+            ia.side = sd;
+            ia.own_pts = d.pts.p;
+            ia.perm = d.perm.p;
+            ia.begin = d.begin.p;
+            ia.end = d.end.p;
+            ia.firstchild = d.firstchild.p;
+            ia.nchildren = d.nchildren.p;
+            ia.rank = d.rank.p;
+            ia.nrows = d.nrows.p;
+            ia.piv = d.piv.p;
+            ia.cpiv = d.cpiv.p;
+            ia.X = d.X.p;
+            ia.xoff = d.xoff.p;
+            ia.maxrank = maxrank;
+            ia.tol = a.tol;
+            ia.status = status.p;
+            ia.cursor = status.p + 4;
+            for (size_t l = 0; l + 1 < lv_ptr.size(); ++l) {
+                const int cnt = lv_ptr[l + 1] - lv_ptr[l];
+                if (cnt == 0) continue;
+                if (lv_mcap[l] > nca::iaca_max_rows())
+                    throw Failure(NCA_ERR_ARG, "a cluster block has up to " + std::to_string(lv_mcap[l]) +
+                                                   " rows; the IACA kernel holds at most " +
+                                                   std::to_string(nca::iaca_max_rows()) + " (reduce the leaf size)");
+                CK(cudaMemsetAsync(status.p + 4, 0, sizeof(int32_t), s));
+                ia.items = nodes.p + lv_ptr[l];
+                ia.nitems = cnt;
+                launch_iaca(ia, lv_mcap[l], s);
+                CK(cudaGetLastError());
+            }
+        } else {
+            size_t maxsm = 0;
+            for (size_t l = 0; l + 1 < lv_ptr.size(); ++l)
+                maxsm = std::max(maxsm, level_smem_bytes(lv_mcap[l], lv_ncap[l]));
+            if (maxsm > size_t(kMaxSmem))
+                throw Failure(NCA_ERR_ARG,
+                              "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
+            level_smem_at_least(maxsm);
+            for (size_t l = 0; l + 1 < lv_ptr.size(); ++l) {
+                int cnt = lv_ptr[l + 1] - lv_ptr[l];
+                if (cnt == 0) continue;
+                size_t sm = level_smem_bytes(lv_mcap[l], lv_ncap[l]);
+                k_level_compress<<<cnt, 256, sm, s>>>(a, nodes.p + lv_ptr[l], lv_mcap[l], lv_ncap[l]);
+                CK(cudaGetLastError());
+            }
         }
         std::vector<int32_t> st = status.download(s);
         if (st[0] == 1) {
@@ -846,9 +927,21 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
                               " of them are linearly independent (coincident points?)");
         }
         if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: level block exceeds its planned capacity");
+        if (st[0] == 3) throw Failure(NCA_ERR_CUDA, "internal: tree mimicry ran out of far points");
         d.h_rank = d.rank.download(s);
         d.h_nrows = d.nrows.download(s);
         d.h_piv = d.piv.download(s);
+        if (iaca) {
+            // the far pivots of a BottomUp(IACA) core are its column pivots sigma
+            const std::vector<int32_t> cp = d.cpiv.download(s);
+            d.h_fpptr.assign(T.nnodes + 1, 0);
+            d.h_fpidx.clear();
+            for (int t = 0; t < T.nnodes; ++t) {
+                d.h_fpidx.insert(d.h_fpidx.end(), cp.begin() + int64_t(t) * maxrank,
+                                 cp.begin() + int64_t(t) * maxrank + d.h_rank[t]);
+                d.h_fpptr[t + 1] = int32_t(d.h_fpidx.size());
+            }
+        }
         plan_apply(d, T, s);
         d.XT.alloc(d.X.n);
         launch_transpose_blocks<double2>(d.X.p, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, T.nnodes, d.XT.p, s);
@@ -969,10 +1062,10 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
 }
 
 // ---- directional (wideband) build ------------------------------------------------------
-// Bases are built per item (cluster, direction) with the level kernel in item mode: the rows of a
-// basis item are its cluster's points, those of a nested item the pivots of its children's items
-// in the mapped directions; the column pivots come from tree mimicry over the item's directional
-// far field. The product stages then become block-sparse gathers over one vector arena, each
+// Bases are built per item (cluster, direction) by BottomUp(IACA) (k_iaca, one warp per item, level
+// by level): the rows of a basis item are its cluster's points, those of a nested item the pivots
+// of its children's items in the mapped directions; the geometric columns come from tree mimicry
+// over the item's directional far field. The product stages then become block-sparse gathers over one vector arena, each
 // block stored contiguously: up (item <- its children's items or its cluster's x slice), coupling
 // (item <- far items), down (child item <- its parents' items: several parent directions can map
 // onto one child direction, so the children gather), leaves (leaf <- every basis item whose
@@ -1116,8 +1209,30 @@ void on_threads(int device, int n, F fn) {
         }
 }
 
+// Wall-clock marks of the build's phases; with NCA_BUILD_TIMING set they are printed to stderr
+// when the build ends (the reference prints its batched compressor's phases under
+// NCA_BATCHED_TIMING, src/compressors/batchedbottomup.jl:74-78).
+struct PhaseTimer {
+    bool on = std::getenv("NCA_BUILD_TIMING") != nullptr;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    std::mutex mu;
+    std::vector<std::pair<double, std::string>> marks;
+    void mark(const std::string &what) {
+        if (!on) return;
+        const double t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::lock_guard<std::mutex> g(mu);
+        marks.emplace_back(t, what);
+    }
+    ~PhaseTimer() {
+        if (!on) return;
+        std::sort(marks.begin(), marks.end());
+        for (const auto &m : marks) std::fprintf(stderr, "nca build %9.4f s  %s\n", m.first, m.second.c_str());
+    }
+};
+
 void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_build_opts *o, const nca::Wideband &wb) {
     const int maxrank = c->maxrank;
+    PhaseTimer timer;
     auto h0 = std::chrono::steady_clock::now();
     cudaStream_t s;
     CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -1153,27 +1268,40 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     on_threads(c->device, 2, [&](int sd) {
         const cudaStream_t s = ss[sd];
         DirItems &d = D->side[sd];
+        const std::string side = sd == 0 ? "test: " : "trial: ";
         d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
                                   sd == 0 ? P.farnodes : P.tfarnodes, wb);
-        {
-            // phase 1 on the device: tree mimicry per item over the item's directional far field
-            std::vector<int64_t> ffptr;
-            std::vector<int32_t> ffnodes;
-            const int ni = int(d.plan.item_node.size());
-            parallel_csr(
-                ni, [&](int it, std::vector<int32_t> &ff) { nca::item_farfield(c->tree[sd], d.plan, it, ff); },
-                ffptr, ffnodes);
-            device_farpivots(c->tree[sd], pts[sd], c->tree[1 - sd], c->side[1 - sd], ni, ffptr, ffnodes,
-                             &d.plan.item_node, maxrank, s, d.h_fpptr, d.fpptr, d.fpidx, nullptr);
-        }
-        // phase 2: the side's items, level by level
-        DBuf<int32_t> status;
-        status.alloc(4);
+        timer.mark(side + "directional plan (" + std::to_string(d.plan.item_node.size()) + " items)");
         const nca::DirSide &pl = d.plan;
-        const nca::Tree &T = c->tree[sd];
+        const nca::Tree &T = c->tree[sd], &Ft = c->tree[1 - sd];
         DevSide &ds = c->side[sd];
+        const DevSide &fs = c->side[1 - sd];
         const int ni = int(pl.item_node.size());
         d.nitems = ni;
+        // the items' directional far fields (dirfarfield), in the reference's order, and the far
+        // points each can offer (capped at maxrank)
+        std::vector<int64_t> ffptr;
+        std::vector<int32_t> ffnodes;
+        parallel_csr(
+            ni, [&](int it, std::vector<int32_t> &ff) { nca::item_farfield(T, pl, it, ff); }, ffptr, ffnodes);
+        std::vector<int32_t> farpts(ni, 0);
+        for (int it = 0; it < ni; ++it) {
+            int64_t n = 0;
+            for (int64_t q = ffptr[it]; q < ffptr[it + 1] && n < maxrank; ++q) n += Ft.size(ffnodes[q]);
+            farpts[it] = int32_t(std::min<int64_t>(n, maxrank));
+        }
+        const std::vector<double> centroid = cluster_centroids(T, pts[sd]);
+        DBuf<int64_t> dffptr;
+        DBuf<int32_t> dffnodes;
+        DBuf<double> dcent, dcenter;
+        dffptr.upload(ffptr, s);
+        dffnodes.upload(ffnodes, s);
+        dcent.upload(centroid, s);
+        dcenter.upload(Ft.center, s);
+        timer.mark(side + "item far fields and centroids uploaded");
+        // the side's items, level by level
+        DBuf<int32_t> status;
+        status.alloc(5);  // [flag, item, a, b], item cursor
         bylevel[sd].assign(T.nlevels, {});
         for (int it = 0; it < ni; ++it) bylevel[sd][T.level[pl.item_node[it]]].push_back(it);
         d.item_node.upload(pl.item_node, s);
@@ -1185,32 +1313,41 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         d.nrows.alloc(std::max(ni, 1));
         d.nrows.zero(s);
         d.piv.alloc(size_t(std::max(ni, 1)) * maxrank);
-        LevelArgs a{};
+        IacaArgs a{};
+        a.mim.begin = fs.begin.p;
+        a.mim.end = fs.end.p;
+        a.mim.firstchild = fs.firstchild.p;
+        a.mim.nchildren = fs.nchildren.p;
+        a.mim.perm = fs.perm.p;
+        a.mim.center = dcenter.p;
+        a.mim.pts = fs.pts.p;
+        a.mim.nitems = ni;
+        a.mim.ffptr = dffptr.p;
+        a.mim.ffnodes = dffnodes.p;
+        a.mim.item_node = d.item_node.p;
+        a.mim.centroid = dcent.p;
+        a.mim.maxrank = maxrank;
         a.K = c->K;
         a.side = sd;
         a.own_pts = ds.pts.p;
-        a.far_pts = c->side[1 - sd].pts.p;
         a.perm = ds.perm.p;
         a.begin = ds.begin.p;
         a.end = ds.end.p;
         a.firstchild = ds.firstchild.p;
         a.nchildren = ds.nchildren.p;
-        a.fpptr = d.fpptr.p;
-        a.fpidx = d.fpidx.p;
+        a.item_basis = d.item_basis.p;
+        a.item_chptr = d.item_chptr.p;
+        a.item_chidx = d.item_chidx.p;
         a.rank = d.rank.p;
         a.nrows = d.nrows.p;
         a.piv = d.piv.p;
         a.cpiv = nullptr;  // column pivots serve frozen-skeleton refills, which directional cores do not offer
         a.maxrank = maxrank;
         a.tol = sd == 0 ? o->tol_test : o->tol_trial;
-        a.sampled = o->sampled;
         a.status = status.p;
-        a.item_node = d.item_node.p;
-        a.item_basis = d.item_basis.p;
-        a.item_chptr = d.item_chptr.p;
-        a.item_chidx = d.item_chidx.p;
+        a.cursor = status.p + 4;
         // Level by level, deepest first: the rows of a nested item are its children's actual
-        // ranks, so each level's X is allocated for min(maxrank, rows, far pivots) columns, then
+        // ranks, so each level's X is allocated for min(maxrank, rows, far points) columns, then
         // compacted to the ranks found before the next level runs.
         d.h_rank.assign(ni, 0);
         d.h_nrows.assign(ni, 0);
@@ -1225,37 +1362,36 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         int64_t total = 0;
         for (int lev = T.nlevels - 1; lev >= 0; --lev) {
             std::vector<int32_t> items;
-            int mc = 0, nc = 0;
+            int mc = 0;
             int64_t bound = 0;
             for (int it : bylevel[sd][lev]) {
-                const int nfp = d.h_fpptr[it + 1] - d.h_fpptr[it];
-                if (nfp == 0) continue;
+                if (farpts[it] == 0) continue;
                 int64_t m = 0;
                 if (pl.item_basis[it]) {
                     m = T.size(pl.item_node[it]);
                 } else {
                     for (int k = pl.item_chptr[it]; k < pl.item_chptr[it + 1]; ++k) m += d.h_rank[pl.item_chidx[k]];
                 }
-                const int64_t rb = std::min<int64_t>(std::min<int64_t>(maxrank, m), int64_t(nfp));
+                const int64_t rb = std::min<int64_t>(std::min<int64_t>(maxrank, m), int64_t(farpts[it]));
                 lvoff[it] = bound;
                 bound += pad2(m * rb);
                 items.push_back(it);
-                mc = std::max<int>(mc, int(m));
-                nc = std::max(nc, nfp);
+                mc = int(std::max<int64_t>(mc, m));
             }
             if (items.empty()) continue;
-            const size_t sm = level_smem_bytes(mc, nc);
-            if (sm > size_t(kMaxSmem))
-                throw Failure(NCA_ERR_ARG,
-                              "a level block does not fit in shared memory (reduce the leaf size or maxrank)");
-            level_smem_at_least(sm);
+            if (mc > nca::iaca_max_rows())
+                throw Failure(NCA_ERR_ARG, "a basis item has " + std::to_string(mc) +
+                                               " rows; the IACA kernel holds at most " +
+                                               std::to_string(nca::iaca_max_rows()) + " (reduce the leaf size)");
             if (!chunk.p || size_t(bound) > chunk.n) chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
             upload_reuse(dlvoff, lvoff, s);
             upload_reuse(nodes, items, s);
             status.zero(s);
             a.X = chunk.p;
             a.xoff = dlvoff.p;
-            k_level_compress<<<int(items.size()), 256, sm, s>>>(a, nodes.p, mc, nc);
+            a.items = nodes.p;
+            a.nitems = int(items.size());
+            launch_iaca(a, mc, s);
             CK(cudaGetLastError());
             const std::vector<int32_t> st = status.download(s);
             if (st[0] == 1) {
@@ -1266,7 +1402,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                                                     " pivots were selected but only " + std::to_string(st[3]) +
                                                     " of them are linearly independent");
             }
-            if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: level block exceeds its planned capacity");
+            if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: an item exceeds the IACA kernel's row capacity");
+            if (st[0] == 3) throw Failure(NCA_ERR_CUDA, "internal: tree mimicry ran out of far points");
             CK(cudaMemcpyAsync(hrank.p, d.rank.p, sizeof(int32_t) * ni, cudaMemcpyDeviceToHost, s));
             CK(cudaMemcpyAsync(hrank.p + ni, d.nrows.p, sizeof(int32_t) * ni, cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
@@ -1304,6 +1441,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             levelItems.push_back(items);
             for (int it : items) cpos[it] += total;
             total += lt;
+            timer.mark(side + "level " + std::to_string(lev) + " (" + std::to_string(items.size()) +
+                       " items, up to " + std::to_string(mc) + " rows) compressed and compacted");
         }
         // one X for the side: the compacted levels back to back
         d.h_xoff.assign(ni + 1, 0);
@@ -1334,11 +1473,13 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         launch_transpose_blocks<double2>(d.X.p, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, ni, d.XT.p, s);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s));
+        timer.mark(side + "bases joined and transposed");
     });
     auto h1 = std::chrono::steady_clock::now();
     // near field first (its offsets feed the leaf plans); its kernels run on stream s
     std::vector<int64_t> h_ntoff;
     const int64_t near_entries = build_near(c, s, &h_ntoff);
+    timer.mark("near field launched");
     // couplings: prepared on the host by the thread of the forward coupling plan (the transposed
     // coupling plan waits for it) and computed on stream s while the other plans are built; their
     // device inputs stay alive until s is synchronised
@@ -1491,6 +1632,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 B.end_group();
             }
             B.finish(pr.up, di.XT.p, s);
+            timer.mark("gather plan " + std::to_string(task) + ": up");
         }
         // coupling: output-side items with a rank and their far pairs' blocks (store built above)
         if (stage == 1) {
@@ -1523,6 +1665,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             }
             B.end_group();
             B.finish(pr.couple, nullptr, s);
+            timer.mark("gather plan " + std::to_string(task) + ": coupling");
         }
         // down: output-side items gather from the parent items that map onto them, root level first
         if (stage == 2) {
@@ -1567,6 +1710,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 B.end_group();
             }
             B.finish(pr.down, dout.X.p, s);
+            timer.mark("gather plan " + std::to_string(task) + ": down");
         }
         // leaves: every basis item whose cluster contains the leaf, then the near blocks
         if (stage == 3) {
@@ -1594,6 +1738,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             }
             B.end_group();
             B.finish(pr.leaves, dout.X.p, s);
+            timer.mark("gather plan " + std::to_string(task) + ": leaves");
         }
         CK(cudaStreamSynchronize(s));
     });
@@ -1616,6 +1761,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     }
     CK(cudaEventRecord(ev1, s));
     CK(cudaStreamSynchronize(s));
+    timer.mark("complex-FP32 copies done, build complete");
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
     auto h2 = std::chrono::steady_clock::now();
@@ -2039,9 +2185,27 @@ int enqueue_tangent(nca_core *c, const double2 *xd, int64_t lx, double2 *yd, int
 
 // Enqueues y = alpha op(H) x + beta y for a directional core: gather x into the arena, then the
 // up, coupling, down and leaf gathers (mode C = mode T with every block conjugated).
+// Stage timing of a directional product: an event pair around each stage launch sequence (the
+// gather is stage 0, then up 1, coupling 2, down 3 and leaves 5, the near field being part of the
+// leaf outputs); events are created as needed.
+struct DirTimer {
+    std::vector<cudaEvent_t> *ev;
+    std::vector<int> *stage;
+    void mark(int k, bool end, cudaStream_t s) {
+        const size_t i = stage->size() * 2 + (end ? 1 : 0);
+        while (ev->size() <= i) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            ev->push_back(e);
+        }
+        CK(cudaEventRecord((*ev)[i], s));
+        if (end) stage->push_back(k);
+    }
+};
+
 int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd, int64_t lx, double2 *yd,
                         int64_t ly, int b, double2 alpha, double2 beta, double2 *arena, int32_t *error,
-                        cudaStream_t s, ProductLaunches &count) {
+                        cudaStream_t s, ProductLaunches &count, DirTimer *timer = nullptr) {
     DirProduct &pr = c->dir->prod[mode == 0 ? 0 : 1];
     const int I = mode == 0 ? 1 : 0, O = 1 - I;
     const int vs = vector_stride(b);
@@ -2053,12 +2217,15 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
     // accumulate in FP64 and round each output row once, and the vector rows, which outweigh
     // the FP32 blocks of these tiny gathers, move half the bytes.
     float2 *arena32 = reinterpret_cast<float2 *>(arena);
+    if (timer) timer->mark(0, false, s);
     if (precision == NCA_PREC_F64)
         k_gather<<<launch_grid(pr.nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, c->side[I].perm.p, pr.nin, b, vs, arena);
     else
         k_gather_to_f32<<<launch_grid(pr.nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, c->side[I].perm.p, pr.nin, b, vs,
                                                                              arena32);
     ++count.total;
+    ++count.stage[0];
+    if (timer) timer->mark(0, true, s);
     const bool conj = mode == 2;
     auto run = [&](auto tag) {
         using S = decltype(tag);
@@ -2067,8 +2234,9 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
         const S *nearM = f64 ? (const S *)(mode == 0 ? c->N.p : c->NT.p) : (const S *)(mode == 0 ? c->N32.p : c->NT32.p);
         for (int q0 = 0; q0 < b; q0 += 16) {
             const int bc = std::min(16, b - q0);
-            auto stage = [&](const GatherStage &G, bool accumulate, bool scatter) {
+            auto stage = [&](const GatherStage &G, bool accumulate, bool scatter, int sk) {
                 const S *M = f64 ? (const S *)G.M.p : (const S *)G.M32.p;
+                if (timer) timer->mark(sk, false, s);
                 for (size_t g = 0; g + 1 < G.group_ptr.size(); ++g) {
                     const int cnt = G.group_ptr[g + 1] - G.group_ptr[g];
                     if (!cnt) continue;
@@ -2114,12 +2282,14 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
                     else
                         launch_gather_rows<S, VT>(a, G.outputs.p + G.group_ptr[g], cnt, s);
                     ++count.total;
+                    ++count.stage[sk];
                 }
+                if (timer) timer->mark(sk, true, s);
             };
-            stage(pr.up, false, false);
-            stage(pr.couple, false, false);
-            stage(pr.down, true, false);
-            stage(pr.leaves, false, true);
+            stage(pr.up, false, false, 1);
+            stage(pr.couple, false, false, 2);
+            stage(pr.down, true, false, 3);
+            stage(pr.leaves, false, true, 5);
         }
     };
     if (precision == NCA_PREC_F64)
@@ -2225,12 +2395,11 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     }
     auto enqueue = [&]() -> int {
         if (c->dir) {
-            if (ws->profiling) CK(record_stage_event(ws->stage_ev[0], s));
+            ws->dir_stage.clear();
+            DirTimer timer{&ws->dir_ev, &ws->dir_stage};
             if (int st = enqueue_dir_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, ws->arena.p,
-                                             ws->error.p, s, count))
+                                             ws->error.p, s, count, ws->profiling ? &timer : nullptr))
                 return st;
-            if (ws->profiling)
-                for (int k = 1; k < EV_COUNT; ++k) CK(record_stage_event(ws->stage_ev[k], s));
         } else if (tangent) {
             if (int st = enqueue_tangent(c, xd, lx, yd, ly, b, alpha, beta, buf, ws->dxhat.p, ws->dyhat.p, s, count))
                 return st;
@@ -2299,7 +2468,18 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     CK(cudaEventElapsedTime(&ms, ws->e0, ws->e1));
     ws->last_seconds = ms * 1e-3;
     ws->last_launches = count.total;
-    if (ws->profiling && !tangent) {
+    if (ws->profiling && c->dir) {
+        // directional: the stages' event pairs summed per stage (no near-field stage of its own)
+        for (int k = 0; k < kStages; ++k) {
+            ws->stage_seconds[k] = 0.0;
+            ws->stage_launches[k] = count.stage[k];
+        }
+        for (size_t i = 0; i < ws->dir_stage.size(); ++i) {
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, ws->dir_ev[2 * i], ws->dir_ev[2 * i + 1]));
+            ws->stage_seconds[ws->dir_stage[i]] += t * 1e-3;
+        }
+    } else if (ws->profiling && !tangent) {
         // gather, up, couple, down, near field, leaves (the sweeps and the near field overlap
         // when the workspace has its sweep stream)
         static const int from[kStages] = {EV_START, EV_GATHER, EV_UP, EV_COUPLE, EV_NEAR0, EV_LEAVES0};
@@ -2657,8 +2837,11 @@ void merge_core(const std::vector<nca_core *> &cs, nca_core *m, bool move, cudaS
 // caching allocator) has reserved nearly all of HBM, so a cudaMalloc inside the library fails or
 // fragments the pool, and callers on a path that must not synchronise on cudaMalloc/cudaFree.
 // nca_apply_static keeps every intermediate buffer of the product (gathered input, xhat, yhat,
-// error word) in this file-scope array instead: NCA_STATIC_SCRATCH_BYTES per device, allocated
-// once when the module is loaded, never by the call.
+// error word) in this file-scope array instead: NCA_STATIC_SCRATCH_BYTES per device, reserved by
+// the CUDA runtime when it loads the library's module on that device (at the library load under
+// CUDA_MODULE_LOADING=EAGER, else at the first use on the device, which for a caller of this entry
+// point alone is its first call there) and held until the process exits; the call itself never
+// allocates.
 static __device__ __align__(256) unsigned char g_static_scratch[NCA_STATIC_SCRATCH_BYTES];
 
 constexpr int kMaxStaticDevices = 64;
@@ -2708,20 +2891,33 @@ int apply_static_impl(nca_core *c, int mode, int precision, const void *x, int64
     if (c->device < 0 || c->device >= kMaxStaticDevices)
         return fail(NCA_ERR_ARG, "nca_apply_static supports devices 0..63");
     CK(cudaSetDevice(c->device));
+    // the call reads its status back and waits for its stream, which a stream capture forbids
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(s, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(NCA_ERR_ARG, "nca_apply_static cannot be captured in a CUDA graph (it waits for its stream)");
     unsigned char *base = nullptr;
     if (int st = static_scratch_base(c->device, &base)) return st;
     bool expected = false;
     if (!g_static_busy[c->device].compare_exchange_strong(expected, true))
         return fail(NCA_ERR_BUSY, "nca_apply_static: another call on this device is using the static scratch");
+    // the flag is released only once no kernel of this call can touch the scratch any more: after
+    // a failure past the first launch the stream is drained first (its status ignored)
     struct Release {
         std::atomic<bool> &flag;
-        ~Release() { flag.store(false); }
-    } release{g_static_busy[c->device]};
+        cudaStream_t s;
+        bool launched = false;
+        ~Release() {
+            if (launched) cudaStreamSynchronize(s);
+            flag.store(false);
+        }
+    } release{g_static_busy[c->device], s};
     const ProductBuffers buf{reinterpret_cast<double2 *>(base + o_xt), reinterpret_cast<double2 *>(base + o_xhat),
                              reinterpret_cast<double2 *>(base + o_yhat), reinterpret_cast<int32_t *>(base), true,
                              true};
     // Only the error word must start at zero: every xt row is gathered, every xhat / yhat block
     // is written (up sweep, coupling) before it is read.
+    release.launched = true;
     CK(cudaMemsetAsync(buf.error, 0, sizeof(int32_t), s));
     ProductLaunches count;
     if (int st = enqueue_product(c, mode, precision, reinterpret_cast<const double2 *>(x), ldx,
@@ -2743,7 +2939,7 @@ int entries_impl(const nca_kernel_desc *kernel, const double *testpoints, int64_
 
 extern "C" {
 
-int32_t nca_version(void) { return 1; }
+int32_t nca_version(void) { return 2; }
 
 int32_t nca_last_error(char *buf, size_t len) {
     if (!buf || len == 0) return NCA_ERR_ARG;
@@ -2925,6 +3121,11 @@ int32_t nca_core_build(const double *testpoints, int64_t ntest, const double *tr
             return fail(NCA_ERR_DIM, "DimensionMismatch: tree and point counts differ");
         if (opts->maxrank < 1 || opts->maxrank > 128) return fail(NCA_ERR_ARG, "maxrank must be in 1..128");
         if (!(opts->tol_test >= 0.0) || !(opts->tol_trial >= 0.0)) return fail(NCA_ERR_ARG, "tolerances must be non-negative");
+        if (opts->compressor != NCA_COMPRESSOR_BATCHED_ACA && opts->compressor != NCA_COMPRESSOR_BOTTOMUP_IACA)
+            return fail(NCA_ERR_ARG, "unknown compressor");
+        if (part->wideband && opts->compressor != NCA_COMPRESSOR_BOTTOMUP_IACA)
+            return fail(NCA_ERR_ARG, "Wideband (directional) NCA is only supported with BottomUp; got BatchedBottomUp "
+                                     "as test compressor.");
         if (int64_t(part->p.nearptr.size()) != testtree->t.nnodes + 1 ||
             int64_t(part->p.tfarptr.size()) != trialtree->t.nnodes + 1)
             return fail(NCA_ERR_DIM, "partition does not match the trees");
@@ -3226,6 +3427,7 @@ void nca_workspace_destroy(nca_workspace *ws) {
     if (ws->e1) cudaEventDestroy(ws->e1);
     for (cudaEvent_t &e : ws->stage_ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ws->dir_ev) cudaEventDestroy(e);
     if (ws->error_host) cudaFreeHost(ws->error_host);
     delete ws;
 }

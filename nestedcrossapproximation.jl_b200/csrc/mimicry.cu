@@ -86,174 +86,434 @@ __device__ __forceinline__ void warp_argmax(double &sc, int &idx) {
     }
 }
 
-__global__ void __launch_bounds__(kWarps * 32, 4) k_mimicry(MimicryArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m = a.maxrank;
-    double *base = reinterpret_cast<double *>(smem) + size_t(warp) * 3 * m;
-    Chosen ch{base, base + m, base + 2 * m,
-              reinterpret_cast<int32_t *>(reinterpret_cast<double *>(smem) + size_t(kWarps) * 3 * m) + warp * m};
-    for (;;) {
-        // items differ widely in cost: each warp takes the next untaken one
-        int item = 0;
-        if (lane == 0) item = atomicAdd(a.cursor, 1);
-        item = __shfl_sync(0xffffffffu, item, 0);
-        if (item >= a.nitems) break;
-        const int64_t f0 = a.ffptr[item], f1 = a.ffptr[item + 1];
-        const int nroots = int(f1 - f0);
-        const int32_t *roots = a.ffnodes + f0;
-        const int own = a.item_node ? a.item_node[item] : item;
-        const int nref = a.own_size[own];
-        const int limit = nref < m ? nref : m;
-        int n = 0;
-        for (int i = 0; i < nroots && limit - n > 0; ++i) {
-            const int f = roots[i];
-            const int sz = a.end[f] - a.begin[f];
-            n += limit - n < sz ? limit - n : sz;
-        }
-        const double c[3] = {a.centroid[3 * size_t(own)], a.centroid[3 * size_t(own) + 1],
-                             a.centroid[3 * size_t(own) + 2]};
-        int32_t *out = a.piv + size_t(item) * m;
-        int nch = 0;
-        // Items with at most 32 * kRootSlots far nodes: lane l keeps, for its roots l + 32 r, the
-        // running minimum of the squared distances to the chosen pivots and the count of chosen
-        // positions inside the root (updated once per pick; a minimum is exact in any order).
-        const bool running = nroots <= 32 * kRootSlots;
-        double rdm[kRootSlots];
-        int rtk[kRootSlots];
+// One warp's tree-mimicry state for one item: its far nodes (roots), the cluster centroid, the
+// pivots chosen so far (shared memory) and, for items with at most 32 * kRootSlots far nodes,
+// lane-held running minima and taken counts of the roots.
+struct MimWarp {
+    const int32_t *roots;
+    int nroots;
+    double c[3];
+    bool running;
+    double rdm[kRootSlots];
+    int rtk[kRootSlots];
+    Chosen ch;
+    int nch;
+};
+
+__device__ __forceinline__ void mim_start(const MimicryArgs &a, MimWarp &w, int item, int own) {
+    const int64_t f0 = a.ffptr[item], f1 = a.ffptr[item + 1];
+    w.nroots = int(f1 - f0);
+    w.roots = a.ffnodes + f0;
+    w.c[0] = a.centroid[3 * size_t(own)];
+    w.c[1] = a.centroid[3 * size_t(own) + 1];
+    w.c[2] = a.centroid[3 * size_t(own) + 2];
+    w.running = w.nroots <= 32 * kRootSlots;
+#pragma unroll
+    for (int r = 0; r < kRootSlots; ++r) {
+        w.rdm[r] = INFINITY;
+        w.rtk[r] = 0;
+    }
+    w.nch = 0;
+}
+
+// The next pivot: returns its position in the far tree's permutation (the same on all lanes) and
+// stores its point id in *id, or returns -1 when no far point is left (cannot happen for disjoint
+// far nodes with points to spare). Lane 0 appends the pivot to the chosen list.
+__device__ __forceinline__ int mim_pick(const MimicryArgs &a, MimWarp &w, int lane, int32_t *id) {
+    const Chosen &ch = w.ch;
+    const int nch = w.nch;
+    const int32_t *roots = w.roots;
+    const int nroots = w.nroots;
+    const double *c = w.c;
+    // root: the far node of the best centre score among those with untaken points
+    double best = -1.0;
+    int bi = 0x7fffffff;
+    if (w.running) {
 #pragma unroll
         for (int r = 0; r < kRootSlots; ++r) {
-            rdm[r] = INFINITY;
-            rtk[r] = 0;
-        }
-        for (int p = 0; p < n; ++p) {
-            // root: the far node of the best centre score among those with untaken points
-            double best = -1.0;
-            int bi = 0x7fffffff;
-            if (running) {
-#pragma unroll
-                for (int r = 0; r < kRootSlots; ++r) {
-                    const int i = lane + 32 * r;
-                    if (i < nroots) {
-                        const int f = roots[i];
-                        if (a.end[f] - a.begin[f] - rtk[r] > 0) {
-                            const double sc = score(a.center[3 * size_t(f)], a.center[3 * size_t(f) + 1],
-                                                    a.center[3 * size_t(f) + 2], c, nch == 0 ? 1.0 : rdm[r]);
-                            if (sc > best) {
-                                best = sc;
-                                bi = i;
-                            }
-                        }
-                    }
-                }
-            } else {
-                for (int i = lane; i < nroots; i += 32) {
-                    const int f = roots[i];
-                    const int lo = a.begin[f], hi = a.end[f];
-                    int taken = 0;
-                    double dm = nch == 0 ? 1.0 : INFINITY;
-                    const double yx = a.center[3 * size_t(f)], yy = a.center[3 * size_t(f) + 1],
-                                 yz = a.center[3 * size_t(f) + 2];
-                    for (int q = 0; q < nch; ++q) {
-                        taken += ch.pos[q] >= lo && ch.pos[q] < hi;
-                        const double d = dist2(yx, yy, yz, ch.x[q], ch.y[q], ch.z[q]);
-                        dm = d < dm ? d : dm;
-                    }
-                    if (hi - lo - taken <= 0) continue;
-                    const double sc = score(yx, yy, yz, c, dm);
+            const int i = lane + 32 * r;
+            if (i < nroots) {
+                const int f = roots[i];
+                if (a.end[f] - a.begin[f] - w.rtk[r] > 0) {
+                    const double sc = score(a.center[3 * size_t(f)], a.center[3 * size_t(f) + 1],
+                                            a.center[3 * size_t(f) + 2], c, nch == 0 ? 1.0 : w.rdm[r]);
                     if (sc > best) {
                         best = sc;
                         bi = i;
                     }
                 }
             }
-            warp_argmax(best, bi);
-            if (bi == 0x7fffffff) {  // no far point left (cannot happen for disjoint far nodes)
+        }
+    } else {
+        for (int i = lane; i < nroots; i += 32) {
+            const int f = roots[i];
+            const int lo = a.begin[f], hi = a.end[f];
+            int taken = 0;
+            double dm = nch == 0 ? 1.0 : INFINITY;
+            const double yx = a.center[3 * size_t(f)], yy = a.center[3 * size_t(f) + 1],
+                         yz = a.center[3 * size_t(f) + 2];
+            for (int q = 0; q < nch; ++q) {
+                taken += ch.pos[q] >= lo && ch.pos[q] < hi;
+                const double d = dist2(yx, yy, yz, ch.x[q], ch.y[q], ch.z[q]);
+                dm = d < dm ? d : dm;
+            }
+            if (hi - lo - taken <= 0) continue;
+            const double sc = score(yx, yy, yz, c, dm);
+            if (sc > best) {
+                best = sc;
+                bi = i;
+            }
+        }
+    }
+    warp_argmax(best, bi);
+    if (bi == 0x7fffffff) return -1;
+    int node = roots[bi];
+    // descent through the children with untaken points, best centre score first
+    while (a.nchildren[node] > 0) {
+        int pick = -1;
+        double pbest = -1.0;
+        for (int k = 0; k < a.nchildren[node]; ++k) {
+            const int cnode = a.firstchild[node] + k;
+            const int lo = a.begin[cnode], hi = a.end[cnode];
+            if (hi - lo - warp_taken(ch, nch, lo, hi, lane) <= 0) continue;
+            const double yx = a.center[3 * size_t(cnode)], yy = a.center[3 * size_t(cnode) + 1],
+                         yz = a.center[3 * size_t(cnode) + 2];
+            const double sc = score(yx, yy, yz, c, warp_dmin(ch, nch, yx, yy, yz, lane));
+            if (sc > pbest) {
+                pbest = sc;
+                pick = cnode;
+            }
+        }
+        node = pick;
+        if (node < 0) return -1;
+    }
+    // leaf: the untaken point of the best score; the taken positions of each 32-point window come
+    // from one OR-reduction per 32 chosen pivots
+    double pb = -1.0;
+    int bp = 0x7fffffff;
+    const int lend = a.end[node];
+    for (int base = a.begin[node]; base < lend; base += 32) {
+        unsigned tmask = 0;
+        for (int q0 = 0; q0 < nch; q0 += 32) {
+            const int q = q0 + lane;
+            const int off = q < nch ? ch.pos[q] - base : -1;
+            tmask |= __reduce_or_sync(0xffffffffu, off >= 0 && off < 32 ? 1u << off : 0u);
+        }
+        const int pos = base + lane;
+        if (pos >= lend || ((tmask >> lane) & 1u)) continue;
+        const int pid = a.perm[pos];
+        const double yx = a.pts[3 * size_t(pid)], yy = a.pts[3 * size_t(pid) + 1], yz = a.pts[3 * size_t(pid) + 2];
+        double dm = nch == 0 ? 1.0 : INFINITY;
+        for (int q = 0; q < nch; ++q) {
+            const double d = dist2(yx, yy, yz, ch.x[q], ch.y[q], ch.z[q]);
+            dm = d < dm ? d : dm;
+        }
+        const double sc = score(yx, yy, yz, c, dm);
+        if (sc > pb) {
+            pb = sc;
+            bp = pos;
+        }
+    }
+    warp_argmax(pb, bp);
+    if (bp == 0x7fffffff) return -1;
+    const int pid = a.perm[bp];
+    if (lane == 0) {
+        ch.x[nch] = a.pts[3 * size_t(pid)];
+        ch.y[nch] = a.pts[3 * size_t(pid) + 1];
+        ch.z[nch] = a.pts[3 * size_t(pid) + 2];
+        ch.pos[nch] = bp;
+    }
+    __syncwarp();
+    if (w.running) {
+        const double px = ch.x[nch], py = ch.y[nch], pz = ch.z[nch];
+#pragma unroll
+        for (int r = 0; r < kRootSlots; ++r) {
+            const int i = lane + 32 * r;
+            if (i < nroots) {
+                const int f = roots[i];
+                w.rtk[r] += bp >= a.begin[f] && bp < a.end[f];
+                const double d = dist2(a.center[3 * size_t(f)], a.center[3 * size_t(f) + 1],
+                                       a.center[3 * size_t(f) + 2], px, py, pz);
+                w.rdm[r] = d < w.rdm[r] ? d : w.rdm[r];
+            }
+        }
+    }
+    w.nch = nch + 1;
+    *id = pid;
+    return bp;
+}
+
+__global__ void __launch_bounds__(kWarps * 32, 4) k_mimicry(MimicryArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m = a.maxrank;
+    double *base = reinterpret_cast<double *>(smem) + size_t(warp) * 3 * m;
+    MimWarp w;
+    w.ch = Chosen{base, base + m, base + 2 * m,
+                  reinterpret_cast<int32_t *>(reinterpret_cast<double *>(smem) + size_t(kWarps) * 3 * m) + warp * m};
+    for (;;) {
+        // items differ widely in cost: each warp takes the next untaken one
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.cursor, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= a.nitems) break;
+        const int own = a.item_node ? a.item_node[item] : item;
+        mim_start(a, w, item, own);
+        const int nref = a.own_size[own];
+        const int limit = nref < m ? nref : m;
+        int n = 0;
+        for (int i = 0; i < w.nroots && limit - n > 0; ++i) {
+            const int f = w.roots[i];
+            const int sz = a.end[f] - a.begin[f];
+            n += limit - n < sz ? limit - n : sz;
+        }
+        int32_t *out = a.piv + size_t(item) * m;
+        for (int p = 0; p < n; ++p) {
+            int32_t id = 0;
+            if (mim_pick(a, w, lane, &id) < 0) {
                 if (lane == 0) atomicCAS(a.error, 0, 1);
                 break;
             }
-            int node = roots[bi];
-            // descent through the children with untaken points, best centre score first
-            while (a.nchildren[node] > 0) {
-                int pick = -1;
-                double pbest = -1.0;
-                for (int k = 0; k < a.nchildren[node]; ++k) {
-                    const int cnode = a.firstchild[node] + k;
-                    const int lo = a.begin[cnode], hi = a.end[cnode];
-                    if (hi - lo - warp_taken(ch, nch, lo, hi, lane) <= 0) continue;
-                    const double yx = a.center[3 * size_t(cnode)], yy = a.center[3 * size_t(cnode) + 1],
-                                 yz = a.center[3 * size_t(cnode) + 2];
-                    const double sc = score(yx, yy, yz, c, warp_dmin(ch, nch, yx, yy, yz, lane));
-                    if (sc > pbest) {
-                        pbest = sc;
-                        pick = cnode;
+            if (lane == 0) out[p] = id;
+        }
+        if (lane == 0) a.count[item] = w.nch;
+        __syncwarp();
+    }
+}
+
+constexpr int kIacaWarps = 4;  // warps per CTA of the IACA kernel, each on one item at a time
+constexpr unsigned kFull = 0xffffffffu;
+
+// sum over the warp in the xor butterfly order (offsets 16, 8, 4, 2, 1): every lane gets the value
+// of the oracle's restatement
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = __dadd_rn(v, __shfl_xor_sync(kFull, v, off));
+    return v;
+}
+
+// value of slot q (a warp-uniform index) of a lane's register array
+template <int RPL, typename T>
+__device__ __forceinline__ T slot(const T (&v)[RPL], int q) {
+    T out = v[0];
+#pragma unroll
+    for (int k = 1; k < RPL; ++k)
+        if (q == k) out = v[k];
+    return out;
+}
+
+// IACA of every item of one level, one warp per item (items taken from an atomic cursor): tree
+// mimicry picks the geometric columns one at a time, the column is evaluated on the item's rows
+// (lane l holds rows l + 32 q), eliminated against the accepted crosses, tested by the
+// extrapolated Frobenius stop (||r||^2 k <= tol^2 ||sampled block||_F^2; the build stops, rejecting
+// the column, when two consecutive columns pass or r is exactly zero) and, if kept, pivoted at its
+// largest entry (lowest row on ties); the cross matrix is
+// unit lower triangular in the eliminated columns, so X = U L^{-1} is solved in place in the
+// item's X slot. Status: [1, item, npivots, rank] singular cross matrix, [2, item, rows, limit]
+// more rows than the warp holds, [3, item, 0, 0] tree mimicry out of far points.
+template <int RPL>
+__global__ void __launch_bounds__(kIacaWarps * 32) k_iaca(IacaArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mr = a.maxrank;
+    double *dbase = reinterpret_cast<double *>(smem) + size_t(warp) * 4 * mr;
+    int32_t *ibase = reinterpret_cast<int32_t *>(reinterpret_cast<double *>(smem) + size_t(kIacaWarps) * 4 * mr) +
+                     size_t(warp) * 2 * mr;
+    MimWarp w;
+    w.ch = Chosen{dbase, dbase + mr, dbase + 2 * mr, ibase};
+    double *pivabs = dbase + 3 * mr;  // |pivot|^2 of every accepted cross
+    int32_t *rp = ibase + mr;         // local pivot row of every accepted cross
+    const MimicryArgs &F = a.mim;
+    const bool items = F.item_node != nullptr;
+    for (;;) {
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(a.cursor, 1);
+        idx = __shfl_sync(kFull, idx, 0);
+        if (idx >= a.nitems) break;
+        const int item = a.items[idx];
+        const int cl = items ? F.item_node[item] : item;
+        const bool basis = items ? a.item_basis[item] != 0 : a.nchildren[cl] == 0;
+        const int nchd = basis ? 0 : items ? a.item_chptr[item + 1] - a.item_chptr[item] : a.nchildren[cl];
+        auto child = [&](int c) { return items ? a.item_chidx[a.item_chptr[item] + c] : a.firstchild[cl] + c; };
+        int m = 0;
+        if (basis) {
+            m = a.end[cl] - a.begin[cl];
+        } else {
+            for (int c = 0; c < nchd; ++c) m += a.rank[child(c)];
+        }
+        const int limit = mr < m ? mr : m;
+        if (m > 32 * RPL) {
+            if (lane == 0 && atomicCAS(a.status, 0, 2) == 0) {
+                a.status[1] = item;
+                a.status[2] = m;
+                a.status[3] = 32 * RPL;
+            }
+            continue;
+        }
+        // the lane's rows: the cluster's points or the children's pivots, in order
+        int32_t rid[RPL];
+        double rx[RPL], ry[RPL], rz[RPL];
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            const int i = lane + 32 * q;
+            rid[q] = -1;
+            if (i < m) {
+                if (basis) {
+                    rid[q] = a.perm[a.begin[cl] + i];
+                } else {
+                    int off = 0;
+                    for (int c = 0; c < nchd; ++c) {
+                        const int ch = child(c), kc = a.rank[ch];
+                        if (i < off + kc) {
+                            rid[q] = a.piv[int64_t(ch) * mr + (i - off)];
+                            break;
+                        }
+                        off += kc;
                     }
                 }
-                node = pick;
-                if (node < 0) break;
+                rx[q] = a.own_pts[3 * int64_t(rid[q])];
+                ry[q] = a.own_pts[3 * int64_t(rid[q]) + 1];
+                rz[q] = a.own_pts[3 * int64_t(rid[q]) + 2];
+            } else {
+                rx[q] = ry[q] = rz[q] = 0.0;
             }
-            if (node < 0) {  // no child with untaken points (cannot happen: the node had some)
-                if (lane == 0) atomicCAS(a.error, 0, 1);
+        }
+        mim_start(F, w, item, cl);
+        // rank limit: min(maxrank, rows, far points)
+        int n = 0;
+        for (int i = 0; i < w.nroots && limit - n > 0; ++i) {
+            const int f = w.roots[i];
+            const int sz = F.end[f] - F.begin[f];
+            n += limit - n < sz ? limit - n : sz;
+        }
+        double2 *U = a.X + a.xoff[item];
+        const double tol2 = __dmul_rn(a.tol, a.tol);
+        double S = 0.0;
+        int k = 0;
+        bool lost = false, passed = false;
+        for (; k < n; ++k) {
+            int32_t jid = 0;
+            if (mim_pick(F, w, lane, &jid) < 0) {
+                lost = true;
                 break;
             }
-            // leaf: the untaken point of the best score; the taken positions of each 32-point
-            // window come from one OR-reduction per 32 chosen pivots
-            double pb = -1.0;
-            int bp = 0x7fffffff;
-            const int lend = a.end[node];
-            for (int base = a.begin[node]; base < lend; base += 32) {
-                unsigned tmask = 0;
-                for (int q0 = 0; q0 < nch; q0 += 32) {
-                    const int q = q0 + lane;
-                    const int off = q < nch ? ch.pos[q] - base : -1;
-                    tmask |= __reduce_or_sync(0xffffffffu, off >= 0 && off < 32 ? 1u << off : 0u);
-                }
-                const int pos = base + lane;
-                if (pos >= lend || ((tmask >> lane) & 1u)) continue;
-                const int id = a.perm[pos];
-                const double yx = a.pts[3 * size_t(id)], yy = a.pts[3 * size_t(id) + 1], yz = a.pts[3 * size_t(id) + 2];
-                double dm = nch == 0 ? 1.0 : INFINITY;
-                for (int q = 0; q < nch; ++q) {
-                    const double d = dist2(yx, yy, yz, ch.x[q], ch.y[q], ch.z[q]);
-                    dm = d < dm ? d : dm;
-                }
-                const double sc = score(yx, yy, yz, c, dm);
-                if (sc > pb) {
-                    pb = sc;
-                    bp = pos;
+            const double qx = w.ch.x[k], qy = w.ch.y[k], qz = w.ch.z[k];
+            double2 r[RPL];
+            double cs = 0.0;
+#pragma unroll
+            for (int q = 0; q < RPL; ++q) {
+                r[q] = make_double2(0.0, 0.0);
+                if (rid[q] >= 0) {
+                    r[q] = a.side == 0 ? kernel_entry(a.K, rx[q], ry[q], rz[q], qx, qy, qz, rid[q], jid)
+                                       : kernel_entry(a.K, qx, qy, qz, rx[q], ry[q], rz[q], jid, rid[q]);
+                    cs = __dadd_rn(cs, cabs2_rn(r[q]));
                 }
             }
-            warp_argmax(pb, bp);
-            if (bp == 0x7fffffff) {  // every point of the leaf taken (cannot happen, as above)
-                if (lane == 0) atomicCAS(a.error, 0, 1);
-                break;
+            S = __dadd_rn(S, warp_sum(cs));
+            // elimination against the accepted crosses, in order
+            for (int l = 0; l < k; ++l) {
+                const int il = rp[l];
+                const double2 v = slot<RPL>(r, il >> 5);
+                const double2 p = make_double2(__shfl_sync(kFull, v.x, il & 31), __shfl_sync(kFull, v.y, il & 31));
+                const double2 *ul = U + int64_t(l) * m;
+#pragma unroll
+                for (int q = 0; q < RPL; ++q)
+                    if (rid[q] >= 0) {
+                        const double2 t = cmul_rn(ul[lane + 32 * q], p);
+                        r[q] = make_double2(__dsub_rn(r[q].x, t.x), __dsub_rn(r[q].y, t.y));
+                    }
             }
+            double e2 = 0.0, best = -1.0;
+            int bi = 0x7fffffff;
+#pragma unroll
+            for (int q = 0; q < RPL; ++q)
+                if (rid[q] >= 0) {
+                    const double s2 = cabs2_rn(r[q]);
+                    e2 = __dadd_rn(e2, s2);
+                    if (s2 > best) {
+                        best = s2;
+                        bi = lane + 32 * q;
+                    }
+                }
+            e2 = warp_sum(e2);
+            // extrapolated Frobenius stop, confirmed on two consecutive columns
+            const bool pass = !(__dmul_rn(e2, double(k + 1)) > __dmul_rn(tol2, S));
+            if (pass && (passed || e2 == 0.0)) break;
+            passed = pass;
+            warp_argmax(best, bi);
+            if (bi >= m) break;  // no finite residual entry (non-finite kernel values): stop here
+            const double2 v = slot<RPL>(r, bi >> 5);
+            const double px = __shfl_sync(kFull, v.x, bi & 31), py = __shfl_sync(kFull, v.y, bi & 31);
+            const int32_t pid = __shfl_sync(kFull, slot<RPL>(rid, bi >> 5), bi & 31);
+            const double d = cabs2_rn(make_double2(px, py));
+            const double2 wv = make_double2(__ddiv_rn(px, d), -__ddiv_rn(py, d));
+            double2 *uk = U + int64_t(k) * m;
+#pragma unroll
+            for (int q = 0; q < RPL; ++q)
+                if (rid[q] >= 0) {
+                    const int i = lane + 32 * q;
+                    uk[i] = i == bi ? make_double2(1.0, 0.0) : cmul_rn(r[q], wv);
+                }
             if (lane == 0) {
-                const int id = a.perm[bp];
-                ch.x[nch] = a.pts[3 * size_t(id)];
-                ch.y[nch] = a.pts[3 * size_t(id) + 1];
-                ch.z[nch] = a.pts[3 * size_t(id) + 2];
-                ch.pos[nch] = bp;
-                out[p] = id;
+                rp[k] = bi;
+                pivabs[k] = d;
+                a.piv[int64_t(item) * mr + k] = pid;
+                if (a.cpiv) a.cpiv[int64_t(item) * mr + k] = jid;
             }
             __syncwarp();
-            if (running) {
-                const double px = ch.x[nch], py = ch.y[nch], pz = ch.z[nch];
+        }
+        if (lost) {
+            if (lane == 0 && atomicCAS(a.status, 0, 3) == 0) a.status[1] = item;
+            continue;
+        }
+        const int rank = k;
+        if (rank > 0) {
+            // singular check of _crossfactorization on the pivots
+            double d2max = 0.0, d2min = INFINITY;
+            for (int l = 0; l < rank; ++l) {
+                const double d = pivabs[l];
+                d2max = d > d2max ? d : d2max;
+                d2min = d < d2min ? d : d2min;
+            }
+            const double eps = 0x1p-52;
+            const double thr = (10.0 * eps) * (10.0 * eps) * d2max;
+            if (!(d2min > thr)) {
+                if (lane == 0 && atomicCAS(a.status, 0, 1) == 0) {
+                    int nr = 0;
+                    for (int l = 0; l < rank; ++l) nr += pivabs[l] > thr;
+                    a.status[1] = item;
+                    a.status[2] = limit;
+                    a.status[3] = nr;
+                }
+                continue;
+            }
+        }
+        // X L = U with L[l][kk] = U[i_l, kk]: columns from the last, each row summed over l ascending
+        for (int kk = rank - 1; kk >= 0; --kk) {
+            double2 val[RPL];
 #pragma unroll
-                for (int r = 0; r < kRootSlots; ++r) {
-                    const int i = lane + 32 * r;
-                    if (i < nroots) {
-                        const int f = roots[i];
-                        rtk[r] += bp >= a.begin[f] && bp < a.end[f];
-                        const double d = dist2(a.center[3 * size_t(f)], a.center[3 * size_t(f) + 1],
-                                               a.center[3 * size_t(f) + 2], px, py, pz);
-                        rdm[r] = d < rdm[r] ? d : rdm[r];
+            for (int q = 0; q < RPL; ++q) {
+                val[q] = make_double2(0.0, 0.0);
+                if (rid[q] >= 0) {
+                    const int i = lane + 32 * q;
+                    double2 acc = U[i + int64_t(kk) * m];
+                    for (int l = kk + 1; l < rank; ++l) {
+                        const double2 t = cmul_rn(U[i + int64_t(l) * m], U[rp[l] + int64_t(kk) * m]);
+                        acc = make_double2(__dsub_rn(acc.x, t.x), __dsub_rn(acc.y, t.y));
                     }
+                    val[q] = acc;
                 }
             }
-            ++nch;
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < RPL; ++q)
+                if (rid[q] >= 0) U[lane + 32 * q + int64_t(kk) * m] = val[q];
+            __syncwarp();
         }
-        if (lane == 0) a.count[item] = nch;
+        if (lane == 0) {
+            a.rank[item] = rank;
+            a.nrows[item] = m;
+        }
         __syncwarp();
     }
 }
@@ -281,6 +541,31 @@ void launch_compact_pivots(const int32_t *piv, int maxrank, const int32_t *count
     const int64_t need = (nslots + 255) / 256;
     k_compact_pivots<<<int(need < int64_t(sms) * 16 ? need : int64_t(sms) * 16), 256, 0, s>>>(piv, maxrank, count, fpptr,
                                                                                               nslots, fpidx);
+}
+
+size_t iaca_smem_bytes(int maxrank) {
+    return size_t(kIacaWarps) * maxrank * (4 * sizeof(double) + 2 * sizeof(int32_t));
+}
+
+int iaca_max_rows() { return 256; }
+
+void launch_iaca(const IacaArgs &a, int mcap, cudaStream_t s) {
+    if (a.nitems <= 0) return;
+    const size_t sm = iaca_smem_bytes(a.maxrank);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int need = (a.nitems + kIacaWarps - 1) / kIacaWarps;
+    const int grid = need < sms * 16 ? need : sms * 16;
+    if (mcap <= 32) {
+        k_iaca<1><<<grid, kIacaWarps * 32, sm, s>>>(a);
+    } else if (mcap <= 64) {
+        k_iaca<2><<<grid, kIacaWarps * 32, sm, s>>>(a);
+    } else if (mcap <= 128) {
+        k_iaca<4><<<grid, kIacaWarps * 32, sm, s>>>(a);
+    } else {
+        k_iaca<8><<<grid, kIacaWarps * 32, sm, s>>>(a);
+    }
 }
 
 size_t mimicry_smem_bytes(int maxrank) { return size_t(kWarps) * maxrank * (3 * sizeof(double) + sizeof(int32_t)); }

@@ -53,7 +53,8 @@ class KernelDesc(C.Structure):
 
 class BuildOpts(C.Structure):
     _fields_ = [("tol_test", C.c_double), ("tol_trial", C.c_double), ("maxrank", C.c_int32),
-                ("sampled", C.c_int32), ("device", C.c_int32), ("store_f32", C.c_int32)]
+                ("sampled", C.c_int32), ("device", C.c_int32), ("store_f32", C.c_int32),
+                ("compressor", C.c_int32)]
 
 
 class CoreInfo(C.Structure):

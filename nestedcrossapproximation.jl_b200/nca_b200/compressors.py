@@ -1,8 +1,12 @@
-"""The batched bottom-up compressor and its configuration objects.
+"""The compressors and their configuration objects.
 
-Mirrors src/compressors/batchedbottomup.jl: `BatchedBottomUp(pivotselector, compressor)`
-with a geometric pivot selector (tree mimicry) and a dense fully pivoted ACA with the
-sampled Frobenius-norm stop. The work itself runs in libnca_b200.so.
+Mirrors src/compressors/batchedbottomup.jl: `BatchedBottomUp(pivotselector, compressor)` with a
+geometric pivot selector (tree mimicry) and a dense fully pivoted ACA with the sampled
+Frobenius-norm stop; and src/compressors/bottomup.jl: `BottomUp(factorization=IACA(...))`, the
+only compressor of directional (wideband) H^2 matrices, with IACA(MaximumValue(),
+TreeMimicryPivoting(...), FNormExtrapolator(tol)) on the test side and the mirrored
+IACA(TreeMimicryPivoting(...), MaximumValue(), ...) on the trial side
+(test/nca/test_petrovgalerkinnca.jl:131-139). The work itself runs in libnca_b200.so.
 """
 from __future__ import annotations
 
@@ -62,6 +66,58 @@ class TreeMimicryPivoting:
         self.ownpoints = np.ascontiguousarray(ownpoints, dtype=np.float64).reshape(-1, 3)
         self.farpoints = np.ascontiguousarray(farpoints, dtype=np.float64).reshape(-1, 3)
         self.fartree = fartree
+
+
+class MaximumValue:
+    """Value pivoting of IACA: the row of the largest residual entry (ties: lowest row)."""
+
+
+class FNormExtrapolator:
+    """IACA stop: the candidate column's residual r passes when ||r||^2 k <= tol^2 S (S: squared
+    Frobenius norm of the k sampled columns). This is FNormEstimator's test ||u_k|| ||v_k|| <= tol
+    ||A_k||_F with the norms over the whole far field extrapolated uniformly from the sampled
+    columns. The factorization stops, rejecting the candidate, once two consecutive candidates
+    pass (or a residual is exactly zero). Accepts a tolerance or an FNormEstimator
+    (FNormExtrapolator(FNormEstimator(tol)), test/pivoting/test_pivots.jl:34-38)."""
+
+    def __init__(self, tol=1e-4):
+        self.tol = float(tol.tol if isinstance(tol, FNormEstimator) else tol)
+
+
+class IACA:
+    """IACA(rowpivoting, columnpivoting, convergence): one side geometric (TreeMimicryPivoting),
+    the other by value (MaximumValue); test side IACA(MaximumValue(), TreeMimicryPivoting, conv),
+    trial side IACA(TreeMimicryPivoting, MaximumValue(), conv)."""
+
+    def __init__(self, rowpivoting=None, columnpivoting=None, convergence=None):
+        self.rowpivoting, self.columnpivoting = rowpivoting, columnpivoting
+        self.convergence = convergence if convergence is not None else FNormExtrapolator(1e-4)
+        kinds = (type(rowpivoting), type(columnpivoting))
+        if kinds not in ((MaximumValue, TreeMimicryPivoting), (TreeMimicryPivoting, MaximumValue)):
+            raise ArgumentError("IACA needs one TreeMimicryPivoting side and one MaximumValue side")
+        if not isinstance(self.convergence, FNormExtrapolator):
+            raise ArgumentError("IACA needs an FNormExtrapolator convergence criterion")
+
+    @property
+    def tol(self):
+        return self.convergence.tol
+
+    def geometric_side(self):
+        """0 when the columns are geometric (a test-side IACA), 1 when the rows are."""
+        return 0 if isinstance(self.columnpivoting, TreeMimicryPivoting) else 1
+
+
+class BottomUp:
+    """BottomUp(factorization=IACA(...), representor=None) (src/compressors/bottomup.jl:1-96).
+    The factorization must be an IACA with tree-mimicry pivoting; representors are not offered."""
+
+    def __init__(self, factorization=None, representor=None):
+        if not isinstance(factorization, IACA):
+            raise ArgumentError("BottomUp needs factorization=IACA(MaximumValue(), TreeMimicryPivoting(...), "
+                                "FNormExtrapolator(tol)) (trial side: the pivotings swapped)")
+        if representor is not None:
+            raise ArgumentError("BottomUp representors are not offered")
+        self.factorization, self.representor = factorization, representor
 
 
 class BatchedBottomUp:

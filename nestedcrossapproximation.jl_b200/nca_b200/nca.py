@@ -14,8 +14,8 @@ import numpy as np
 
 from ._lib import (ArgumentError, BuildOpts, ConcurrentWorkspaceError, CoreInfo, DimensionMismatch, check, lib,
                    ptr)
-from .admissibility import IsNear, Partition, isnear as _isnear
-from .compressors import ACA, BatchedBottomUp
+from .admissibility import IsNear, IsNearWideband, Partition, isnear as _isnear
+from .compressors import ACA, BatchedBottomUp, BottomUp
 from .trees import BlockTree
 from .utils import CoefficientPlan
 
@@ -48,27 +48,49 @@ class CouplingStore:
 class PetrovGalerkinNCACore:
     """Read-only H^2 matrix built by the batched bottom-up NCA on one GPU."""
 
-    def __init__(self, operator, testspace, trialspace, tree: BlockTree, *, testcompressor: BatchedBottomUp,
-                 trialcompressor: BatchedBottomUp, isnear: IsNear | None = None, maxrank: int = 50,
-                 ntasks: int | None = None, store_f32: bool = False, device: int = 0, sampled: bool = True,
-                 partition: Partition | None = None, verbose: bool = False):
+    def __init__(self, operator, testspace, trialspace, tree: BlockTree, *, testcompressor, trialcompressor,
+                 isnear: IsNear | None = None, maxrank: int = 50, ntasks: int | None = None, store_f32: bool = False,
+                 device: int = 0, sampled: bool = True, partition: Partition | None = None, verbose: bool = False):
         if ntasks is not None and ntasks < 1:
             raise ArgumentError(f"ntasks must be positive, got {ntasks}")
-        for comp in (testcompressor, trialcompressor):
-            if not isinstance(comp, BatchedBottomUp) or not isinstance(comp.compressor, ACA):
+        self.isnear = isnear or _isnear()
+        wideband = isinstance(self.isnear, IsNearWideband) or (partition is not None and partition.wideband)
+        for side, comp in (("test", testcompressor), ("trial", trialcompressor)):
+            if wideband and not isinstance(comp, BottomUp):
+                # src/compressors/abstractcompressor.jl:39-47
+                raise ArgumentError("Wideband (directional) NCA is only supported with BottomUp; got "
+                                    f"{type(comp).__name__} as {side} compressor.")
+            if isinstance(comp, BatchedBottomUp):
+                if not isinstance(comp.compressor, ACA):
+                    raise ArgumentError("BatchedBottomUp needs compressor=ACA(FullPivoting(), FullPivoting(), "
+                                        "FNormEstimator(tol))")
+            elif isinstance(comp, BottomUp):
+                if comp.factorization.geometric_side() != (0 if side == "test" else 1):
+                    raise ArgumentError(f"the {side} side's IACA has its pivotings swapped: test side "
+                                        "IACA(MaximumValue(), TreeMimicryPivoting, conv), trial side "
+                                        "IACA(TreeMimicryPivoting, MaximumValue(), conv)")
+            else:
                 raise ArgumentError("compressors must be BatchedBottomUp(pivotselector=TreeMimicryPivoting, "
-                                    "compressor=ACA(FullPivoting(), FullPivoting(), FNormEstimator(tol)))")
+                                    "compressor=ACA(...)) or BottomUp(factorization=IACA(...))")
+        if type(testcompressor) is not type(trialcompressor):
+            raise ArgumentError("the test and trial compressors must be of one kind (both BatchedBottomUp or both "
+                                "BottomUp)")
+        iaca = isinstance(testcompressor, BottomUp)
         self.operator = operator
         self.testpoints = np.ascontiguousarray(testspace, dtype=np.float64).reshape(-1, 3)
         self.trialpoints = np.ascontiguousarray(trialspace, dtype=np.float64).reshape(-1, 3)
         self.tree = tree
-        self.isnear = isnear or _isnear()
         self.partition = partition or Partition(tree, self.isnear)
         self.maxrank = int(maxrank)
         self.device = int(device)
         self.f32 = bool(store_f32)
         opts = BuildOpts()
-        opts.tol_test, opts.tol_trial = testcompressor.compressor.tol, trialcompressor.compressor.tol
+        if iaca:
+            opts.tol_test = testcompressor.factorization.tol
+            opts.tol_trial = trialcompressor.factorization.tol
+        else:
+            opts.tol_test, opts.tol_trial = testcompressor.compressor.tol, trialcompressor.compressor.tol
+        opts.compressor = 1 if iaca else 0
         opts.maxrank, opts.sampled, opts.device, opts.store_f32 = self.maxrank, int(sampled), self.device, int(self.f32)
         desc = operator.desc()
         h = C.c_void_p()

@@ -12,8 +12,10 @@ Follows NestedCrossApproximation.jl line by line, in Python on 0-based ids:
   - dirfarfield: abstractdirections.jl:192-231; isbasisnode: abstractdirections.jl:238-243;
   - the basis items of the bottom-up compressor and their children's items:
     src/compressors/bottomup.jl:214-320.
-Only the tests import this module. Dot products and sums are written out element by element in
-the same order as the library's host code, so ties resolve identically.
+Dot products and sums are written out element by element in the same order as the library's
+host code, so ties resolve identically. DirectionalH2 wraps the C restatement of the same plan,
+the directional build (IACA per item) and the directional product (nca_oracle.c). Only the tests
+and the CPU legs of the benchmark import this module.
 """
 from __future__ import annotations
 
@@ -269,157 +271,92 @@ class DirectionalData:
 
 
 class DirectionalH2:
-    """Oracle directional H^2 matrix: the bottom-up compressor per (cluster, direction) item
-    (src/compressors/bottomup.jl:214-424) with the project's pivoting rules (tree mimicry over
-    the item's directional far field, the sampled fully pivoted ACA on K[rows, far pivots],
-    X = K[rows, sigma] K[tau, sigma]^{-1}), couplings per directional far pair
+    """Oracle directional H^2 matrix, built and applied by the C restatement (nca_oracle.c,
+    OpenMP): the directional plan (as DirectionalData above), the bottom-up compressor per
+    (cluster, direction) item with IACA (tree-mimicry columns over the item's directional far
+    field, maximum-value rows, extrapolated Frobenius stop; src/compressors/bottomup.jl:214-424,
+    src/pivoting/pivots.jl:329-364), couplings per directional far pair
     (src/couplingmatrices.jl:55-111), the near field, and the directional product
     (src/nca/{aggregate,couple,disaggregate}.jl, directional methods)."""
 
     def __init__(self, testpts, trialpts, kernel, k, minvalues=32, tol=1e-4, maxrank=50, etalf=1.0, etahf=5.0,
-                 gamma=1.0):
+                 gamma=1.0, nthreads=None):
+        import ctypes as C
+        import os
         from . import oracle as O
         self.O = O
+        L = O.lib()
         self.testpts = np.ascontiguousarray(testpts, dtype=np.float64)
         self.trialpts = np.ascontiguousarray(trialpts, dtype=np.float64)
-        self.kernel = kernel
-        self.trees = [O.OwnedTree(self.testpts, minvalues), O.OwnedTree(self.trialpts, minvalues)]
-        T, S = self.trees
-        (self.nearptr, self.nearnodes, fptr, fnodes, tptr, tnodes) = interactions_wideband(T, S, k, etalf, etahf, gamma)
-        self.tnearptr, self.tnearnodes = self._transpose(self.nearptr, self.nearnodes, S.nnodes)
-        self.dirs = [DirectionalData(T, S, fptr, fnodes, k, etahf, gamma),
-                     DirectionalData(S, T, tptr, tnodes, k, etahf, gamma)]
-        self.maxrank, self.tol = maxrank, tol
-        self.piv = [None, None]
-        self.X = [None, None]
-        for side in (0, 1):
-            self._build_side(side)
-        self._couplings()
+        self.kernel, self.maxrank, self.tol = kernel, maxrank, tol
+        if maxrank > 256:
+            raise ValueError("the oracle supports maxrank <= 256")
+        self._h = L.oracle_dir_build(O._p(self.testpts), len(self.testpts), O._p(self.trialpts),
+                                     len(self.trialpts), int(minvalues), float(k), float(etalf), float(etahf),
+                                     float(gamma), *kernel.args(), float(tol), float(tol), int(maxrank),
+                                     int(nthreads or os.cpu_count() or 1))
+        side, item, npiv, rank = (C.c_int() for _ in range(4))
+        st = L.oracle_dir_status(self._h, C.byref(side), C.byref(item), C.byref(npiv), C.byref(rank))
+        self.trees = [O.Tree(L.oracle_dir_tree(self._h, s), len(p), self) for s, p in
+                      ((0, self.testpts), (1, self.trialpts))]
+        if st:
+            raise O.SingularBuild(f"singular cross matrix (side {side.value}, item {item.value}, "
+                                  f"{npiv.value} pivots, rank {rank.value})")
+        self.nitems, self.ranks, self.nrows, self.piv, self.plan = [], [], [], [], []
+        for sd in (0, 1):
+            ni = L.oracle_dir_nitems(self._h, sd)
+            nn = self.trees[sd].nnodes
+            nf = L.oracle_dir_nfar(self._h, sd)
+            nc = L.oracle_dir_nchildren(self._h, sd)
+            plan = {"farnodes": np.zeros(nf, np.int32), "dirptr": np.zeros(nn + 1, np.int32),
+                    "dirs": np.zeros(ni, np.int32), "dirvec": np.zeros((ni, 3)),
+                    "dirfarptr": np.zeros(ni + 1, np.int32), "item_basis": np.zeros(ni, np.int32),
+                    "item_chptr": np.zeros(ni + 1, np.int32), "item_chidx": np.zeros(nc, np.int32)}
+            L.oracle_dir_plan(self._h, sd, *[O._p(plan[f]) for f in ("farnodes", "dirptr", "dirs", "dirvec",
+                                                                        "dirfarptr", "item_basis", "item_chptr",
+                                                                        "item_chidx")])
+            rank = np.zeros(max(ni, 1), np.int32)
+            nrows = np.zeros(max(ni, 1), np.int32)
+            ptr = np.zeros(ni + 1, np.int32)
+            idx = np.zeros(max(ni * maxrank, 1), np.int32)
+            L.oracle_dir_pivots(self._h, sd, O._p(rank), O._p(nrows), O._p(ptr), O._p(idx))
+            self.nitems.append(ni)
+            self.ranks.append(rank[:ni])
+            self.nrows.append(nrows[:ni])
+            self.piv.append([idx[ptr[i]:ptr[i + 1]].copy() for i in range(ni)])
+            self.plan.append(plan)
+        xe, ce, ne, npairs = (C.c_long() for _ in range(4))
+        L.oracle_dir_sizes(self._h, C.byref(xe), C.byref(ce), C.byref(ne), C.byref(npairs))
+        self.entries = {"x": xe.value, "coupling": ce.value, "near": ne.value, "pairs": npairs.value}
 
-    @staticmethod
-    def _transpose(ptr, nodes, n):
-        lists = [[] for _ in range(n)]
-        for t in range(len(ptr) - 1):
-            for s in nodes[ptr[t]:ptr[t + 1]]:
-                lists[s].append(t)
-        tp = np.zeros(n + 1, np.int32)
-        for i in range(n):
-            tp[i + 1] = tp[i] + len(lists[i])
-        return tp, np.array([v for lst in lists for v in lst], np.int32)
+    def interpolation(self, side):
+        """X of every item of one side (nrows x rank)."""
+        L = self.O.lib()
+        tot = L.oracle_dir_x_total(self._h, side)
+        ni = self.nitems[side]
+        off = np.zeros(ni + 1, np.int64)
+        X = np.zeros(max(tot, 1), np.complex128)
+        L.oracle_dir_x(self._h, side, self.O._p(off), self.O._p(X))
+        return [X[off[i]:off[i + 1]].reshape((self.nrows[side][i], self.ranks[side][i]), order="F")
+                for i in range(ni)]
 
-    def _block(self, side, rows, cols):
-        """K[rows, cols]; side 0: rows are test points, side 1: rows are trial points."""
-        O = self.O
-        rows = np.asarray(rows, np.int64)
-        cols = np.asarray(cols, np.int64)
-        if side == 0:
-            ii, jj = np.repeat(rows, len(cols)), np.tile(cols, len(rows))
-        else:
-            ii, jj = np.tile(cols, len(rows)), np.repeat(rows, len(cols))
-        v = O.entries(self.kernel, self.testpts, self.trialpts, ii, jj)
-        return v.reshape(len(rows), len(cols))
-
-    def _build_side(self, side):
-        O = self.O
-        D = self.dirs[side]
-        T, F = self.trees[side], self.trees[1 - side]
-        own = self.testpts if side == 0 else self.trialpts
-        far = self.trialpts if side == 0 else self.testpts
-        piv = [np.zeros(0, np.int32)] * D.nitems
-        X = [None] * D.nitems
-        for level in range(T.nlevels - 1, -1, -1):
-            for item in range(D.nitems):
-                node = int(D.item_node[item])
-                if T.level[node] != level:
-                    continue
-                ff = D.farfield(item)
-                if len(ff) == 0:
-                    continue
-                if D.item_basis[item]:
-                    rows = T.values(node)
-                else:
-                    rows = np.concatenate([piv[ch] for ch in D.item_chidx[D.item_chptr[item]:D.item_chptr[item + 1]]]
-                                          + [np.zeros(0, np.int32)]).astype(np.int32)
-                fp = O.select_farpivots(F, own, far, T.values(node), ff, self.maxrank)
-                if len(fp) == 0 or len(rows) == 0:
-                    continue
-                A = self._block(side, rows, fp)
-                r, rp, cp = O.aca(A, self.maxrank, self.tol, True)
-                if r == 0:
-                    continue
-                piv[item] = rows[rp]
-                X[item] = O.cross_solve(A[:, cp], rp)
-        self.piv[side] = piv
-        self.X[side] = X
-
-    def _couplings(self):
-        Dt, Ds = self.dirs
-        pos = {}
-        for s in range(self.trees[1].nnodes):
-            for q in range(Ds.farptr[s], Ds.farptr[s + 1]):
-                pos[(s, int(Ds.farnodes[q]))] = q
-        item_of = [np.zeros(len(D.farnodes), np.int32) for D in self.dirs]
-        for D, io in zip(self.dirs, item_of):
-            for it in range(D.nitems):
-                io[D.dirfarptr[it]:D.dirfarptr[it + 1]] = it
-        self.C = {}
-        for t in range(self.trees[0].nnodes):
-            for e in range(Dt.farptr[t], Dt.farptr[t + 1]):
-                s = int(Dt.farnodes[e])
-                it, is_ = int(item_of[0][e]), int(item_of[1][pos[(s, t)]])
-                if len(self.piv[0][it]) and len(self.piv[1][is_]):
-                    self.C[(it, is_)] = self._block(0, self.piv[0][it], self.piv[1][is_])
+    @property
+    def shape(self):
+        return (len(self.testpts), len(self.trialpts))
 
     def apply(self, x, mode=0):
         """y = op(H) x for a vector or a block of columns; mode 0: H, 1: H^T, 2: H^H."""
         x = np.asarray(x, dtype=np.complex128)
         vec = x.ndim == 1
-        X = x.reshape(x.shape[0], -1)
-        I = 1 if mode == 0 else 0
-        O_ = 1 - I
-        conj = (lambda a: a.conj()) if mode == 2 else (lambda a: a)
-        DI, DO = self.dirs[I], self.dirs[O_]
-        TI, TO = self.trees[I], self.trees[O_]
-        XI, XO = self.X[I], self.X[O_]
-        xhat = [None] * DI.nitems
-        for level in range(TI.nlevels - 1, -1, -1):
-            for it in range(DI.nitems):
-                if XI[it] is None or TI.level[DI.item_node[it]] != level:
-                    continue
-                if DI.item_basis[it]:
-                    xhat[it] = conj(XI[it]).T @ X[TI.values(int(DI.item_node[it]))]
-                else:
-                    acc, r0 = np.zeros((XI[it].shape[1], X.shape[1]), complex), 0
-                    for ch in DI.item_chidx[DI.item_chptr[it]:DI.item_chptr[it + 1]]:
-                        rc = 0 if XI[ch] is None else XI[ch].shape[1]
-                        if rc:
-                            acc = acc + conj(XI[it][r0:r0 + rc]).T @ xhat[ch]
-                        r0 += rc
-                    xhat[it] = acc
-        yhat = [None if XO[it] is None else np.zeros((XO[it].shape[1], X.shape[1]), complex) for it in range(DO.nitems)]
-        for (it, is_), Cb in self.C.items():
-            if mode == 0:
-                yhat[it] += Cb @ xhat[is_]
-            else:
-                yhat[is_] += conj(Cb).T @ xhat[it]
-        Y = np.zeros((TO.perm.shape[0], X.shape[1]), complex)
-        for level in range(TO.nlevels):
-            for it in range(DO.nitems):
-                if XO[it] is None or TO.level[DO.item_node[it]] != level:
-                    continue
-                if DO.item_basis[it]:
-                    Y[TO.values(int(DO.item_node[it]))] += conj(XO[it]) @ yhat[it]
-                else:
-                    r0 = 0
-                    for ch in DO.item_chidx[DO.item_chptr[it]:DO.item_chptr[it + 1]]:
-                        rc = 0 if XO[ch] is None else XO[ch].shape[1]
-                        if rc:
-                            yhat[ch] = yhat[ch] + conj(XO[it][r0:r0 + rc]) @ yhat[it]
-                        r0 += rc
-        nptr, nnodes = (self.nearptr, self.nearnodes) if mode == 0 else (self.tnearptr, self.tnearnodes)
-        for t in range(TO.nnodes):
-            for s in nnodes[nptr[t]:nptr[t + 1]]:
-                rows, cols = TO.values(t), TI.values(int(s))
-                Nb = self._block(0, rows, cols) if mode == 0 else self._block(0, cols, rows).T
-                Y[rows] += conj(Nb) @ X[cols]
+        X = np.asfortranarray(x.reshape(x.shape[0], -1))
+        nin, nout = (self.shape[1], self.shape[0]) if mode == 0 else self.shape
+        if X.shape[0] != nin:
+            raise ValueError("dimension mismatch")
+        Y = np.zeros((nout, X.shape[1]), dtype=np.complex128, order="F")
+        self.O.lib().oracle_dir_apply(self._h, int(mode), self.O._p(X), nin, self.O._p(Y), nout, X.shape[1])
         return Y[:, 0] if vec else Y
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self.O.lib().oracle_dir_free(self._h)
+            self._h = None

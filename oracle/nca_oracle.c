@@ -878,6 +878,7 @@ typedef struct {
     int *tnear_coloff;
     int status, bad_side, bad_node, bad_npiv, bad_rank;
     int nthreads;
+    int iaca; /* BottomUp(IACA) instead of the batched ACA (node mode) */
 } ohandle;
 
 static const double *side_pt(const ohandle *H, int side, long idx) {
@@ -889,6 +890,78 @@ static inline oc level_entry(const ohandle *H, int side, long own, long far) {
     if (side == 0)
         return okern_entry(&H->K, side_pt(H, 0, own), side_pt(H, 1, far), own, far);
     return okern_entry(&H->K, side_pt(H, 0, far), side_pt(H, 1, own), far, own);
+}
+
+static int iaca_block(const okern *K, int side, const double *ownpts, const double *farpts,
+                      const otree *F, const double *c, const int *farnodes, int nfar,
+                      const int *rows, int m, int maxrank, double tol, int *rowpiv,
+                      int *colpiv, oc *U, int *nrank);
+static void centroid_of(const double *pts, const int *refidcs, int n, double *c);
+
+/* BottomUp(IACA) for cluster t (src/compressors/bottomup.jl:96-208): rows = the cluster's points
+ * (leaf) or its children's pivots, far field = its own and its ancestors' far nodes. */
+static void build_node_iaca(ohandle *H, int side, int t, int *tmpcp, oc **Xn, int *failed) {
+    const otree *T = H->tree[side], *F = H->tree[1 - side];
+    const int maxrank = H->maxrank;
+    const int *ptr = side == 0 ? H->farptr : H->tfarptr;
+    const int *nodes = side == 0 ? H->farnodes : H->tfarnodes;
+    int total = 0;
+    for (int a = t; a >= 0; a = T->parent[a])
+        total += ptr[a + 1] - ptr[a];
+    if (total == 0)
+        return;
+    int *ff = malloc(sizeof(int) * total);
+    int k = 0;
+    for (int a = t; a >= 0; a = T->parent[a])
+        for (int i = ptr[a]; i < ptr[a + 1]; ++i)
+            ff[k++] = nodes[i];
+    int m = 0;
+    int *rows;
+    if (isleaf(T, t)) {
+        m = T->end[t] - T->begin[t];
+        rows = malloc(sizeof(int) * (m > 0 ? m : 1));
+        memcpy(rows, T->perm + T->begin[t], sizeof(int) * m);
+    } else {
+        for (int c = 0; c < T->nchildren[t]; ++c)
+            m += H->rank[side][T->firstchild[t] + c];
+        rows = malloc(sizeof(int) * (m > 0 ? m : 1));
+        int o = 0;
+        for (int c = 0; c < T->nchildren[t]; ++c) {
+            int ch = T->firstchild[t] + c;
+            memcpy(rows + o, H->pivtmp[side] + (size_t)ch * maxrank, sizeof(int) * H->rank[side][ch]);
+            o += H->rank[side][ch];
+        }
+    }
+    H->nrows[side][t] = m;
+    double c[3];
+    centroid_of(H->pts[side], T->perm + T->begin[t], T->end[t] - T->begin[t], c);
+    int limit = maxrank < m ? maxrank : m;
+    oc *U = malloc(sizeof(oc) * ((size_t)m * (limit > 0 ? limit : 1) + 1));
+    int rp[256], cp[256], nr = 0;
+    int r = m > 0 ? iaca_block(&H->K, side, H->pts[side], H->pts[1 - side], F, c, ff, total, rows, m,
+                               maxrank, H->tol[side], rp, cp, U, &nr)
+                  : 0;
+    if (r < 0) {
+#pragma omp critical
+        {
+            if (!*failed || t < H->bad_node) {
+                *failed = 1;
+                H->bad_side = side;
+                H->bad_node = t;
+                H->bad_npiv = limit;
+                H->bad_rank = nr;
+            }
+        }
+        r = 0;
+    }
+    H->rank[side][t] = r;
+    for (int l = 0; l < r; ++l) {
+        H->pivtmp[side][(size_t)t * maxrank + l] = rows[rp[l]];
+        tmpcp[(size_t)t * maxrank + l] = cp[l];
+    }
+    Xn[t] = U;
+    free(rows);
+    free(ff);
 }
 
 static void build_side(ohandle *H, int side) {
@@ -903,6 +976,8 @@ static void build_side(ohandle *H, int side) {
     int *tmpfp = malloc(sizeof(int) * (size_t)nn * (maxrank > 0 ? maxrank : 1));
 #pragma omp parallel for schedule(dynamic, 4) num_threads(H->nthreads)
     for (int t = 0; t < nn; ++t) {
+        if (H->iaca)
+            continue; /* IACA picks its geometric columns itself */
         int total = 0;
         for (int a = t; a >= 0; a = T->parent[a])
             total += ptr[a + 1] - ptr[a];
@@ -934,12 +1009,17 @@ static void build_side(ohandle *H, int side) {
     H->nrows[side] = calloc(nn, sizeof(int));
     H->pivtmp[side] = malloc(sizeof(int) * (size_t)nn * (maxrank > 0 ? maxrank : 1));
     oc **Xn = calloc(nn, sizeof(oc *));
+    int *tmpcp = malloc(sizeof(int) * (size_t)nn * (maxrank > 0 ? maxrank : 1));
     double tol = H->tol[side];
     int failed = 0;
     for (int lev = T->nlevels - 1; lev >= 0 && !failed; --lev) {
         int lb = T->levelptr[lev], le = T->levelptr[lev + 1];
 #pragma omp parallel for schedule(dynamic, 1) num_threads(H->nthreads)
         for (int t = lb; t < le; ++t) {
+            if (H->iaca) {
+                build_node_iaca(H, side, t, tmpcp, Xn, &failed);
+                continue;
+            }
             int n = H->fpptr[side][t + 1] - H->fpptr[side][t];
             if (n == 0)
                 continue;
@@ -1006,6 +1086,17 @@ static void build_side(ohandle *H, int side) {
     }
     if (failed)
         H->status = 1;
+    if (H->iaca) {
+        /* the far pivots of an IACA build are its column pivots */
+        for (int t = 0; t < nn; ++t)
+            H->fpptr[side][t + 1] = H->fpptr[side][t] + H->rank[side][t];
+        free(H->fpidx[side]);
+        H->fpidx[side] = malloc(sizeof(int) * (H->fpptr[side][nn] > 0 ? H->fpptr[side][nn] : 1));
+        for (int t = 0; t < nn; ++t)
+            memcpy(H->fpidx[side] + H->fpptr[side][t], tmpcp + (size_t)t * maxrank,
+                   sizeof(int) * H->rank[side][t]);
+    }
+    free(tmpcp);
     /* flatten pivots and X */
     H->pivptr[side] = malloc(sizeof(int) * (nn + 1));
     H->pivptr[side][0] = 0;
@@ -1124,9 +1215,10 @@ static void build_near(ohandle *H) {
 ohandle *oracle_build(const double *tp, long nt, const double *sp, long ns, int minvalues,
                       double eta, int kind, int sign, double k, double rmin, const double *mat,
                       long ldmat, double tol_test, double tol_trial, int maxrank, int sampled,
-                      int nthreads) {
+                      int nthreads, int iaca) {
     ohandle *H = calloc(1, sizeof(ohandle));
     H->nthreads = nthreads > 0 ? nthreads : 1;
+    H->iaca = iaca;
     H->npts[0] = nt;
     H->npts[1] = ns;
     H->pts[0] = malloc(sizeof(double) * 3 * (nt > 0 ? nt : 1));
@@ -1164,9 +1256,7 @@ ohandle *oracle_build(const double *tp, long nt, const double *sp, long ns, int 
     return H;
 }
 
-void oracle_free(ohandle *H) {
-    if (!H)
-        return;
+static void oracle_free_fields(ohandle *H) {
     for (int s = 0; s < 2; ++s) {
         free(H->pts[s]); oracle_tree_free(H->tree[s]);
         free(H->fpptr[s]); free(H->fpidx[s]); free(H->rank[s]); free(H->nrows[s]);
@@ -1178,6 +1268,12 @@ void oracle_free(ohandle *H) {
     free(H->tnearptr); free(H->tnearnodes); free(H->tfarptr); free(H->tfarnodes);
     free(H->coff); free(H->C); free(H->noff); free(H->ncols); free(H->N);
     free(H->tnear_coloff);
+}
+
+void oracle_free(ohandle *H) {
+    if (!H)
+        return;
+    oracle_free_fields(H);
     free(H);
 }
 
@@ -1271,6 +1367,64 @@ static void small_gemv(const oc *B, int nrow, int ncol, long ld, int trans, int 
                 acc.im += t.im;
             }
             y[j] = acc;
+        }
+    }
+}
+
+/* y += op(N) x for the stored near field (petrovgalerkinnca.jl:474, :531, :587): mode 0 by the
+ * test near lists, modes 1 and 2 by the trial near lists through the transposed column offsets. */
+static void near_apply(const ohandle *H, int mode, const oc *x, oc *y) {
+    int conj = mode == 2;
+    const otree *Tt = H->tree[0], *Ts = H->tree[1];
+    if (mode == 0) {
+#pragma omp parallel for schedule(dynamic, 4) num_threads(H->nthreads)
+        for (int t = 0; t < Tt->nnodes; ++t) {
+            int mt = Tt->end[t] - Tt->begin[t];
+            int nc = H->ncols[t];
+            if (nc == 0)
+                continue;
+            const oc *B = H->N + H->noff[t];
+            oc *acc = calloc(mt, sizeof(oc));
+            int col = 0;
+            for (int i = H->nearptr[t]; i < H->nearptr[t + 1]; ++i) {
+                int s = H->nearnodes[i];
+                for (int pos = Ts->begin[s]; pos < Ts->end[s]; ++pos, ++col) {
+                    oc xj = x[Ts->perm[pos]];
+                    for (int a = 0; a < mt; ++a) {
+                        oc t2 = oc_mul(B[a + (long)col * mt], xj);
+                        acc[a].re += t2.re;
+                        acc[a].im += t2.im;
+                    }
+                }
+            }
+            for (int a = 0; a < mt; ++a) {
+                long gi = Tt->perm[Tt->begin[t] + a];
+                y[gi].re += acc[a].re;
+                y[gi].im += acc[a].im;
+            }
+            free(acc);
+        }
+    } else {
+#pragma omp parallel for schedule(dynamic, 4) num_threads(H->nthreads)
+        for (int s = 0; s < Ts->nnodes; ++s) {
+            int ms = Ts->end[s] - Ts->begin[s];
+            for (int k = H->tnearptr[s]; k < H->tnearptr[s + 1]; ++k) {
+                int t = H->tnearnodes[k];
+                int mt = Tt->end[t] - Tt->begin[t];
+                const oc *B = H->N + H->noff[t] + (long)H->tnear_coloff[k] * mt;
+                for (int j = 0; j < ms; ++j) {
+                    oc acc = oc_make(0.0, 0.0);
+                    for (int a = 0; a < mt; ++a) {
+                        oc t2 = oc_mul(opentry(B[a + (long)j * mt], conj),
+                                       x[Tt->perm[Tt->begin[t] + a]]);
+                        acc.re += t2.re;
+                        acc.im += t2.im;
+                    }
+                    long gj = Ts->perm[Ts->begin[s] + j];
+                    y[gj].re += acc.re;
+                    y[gj].im += acc.im;
+                }
+            }
         }
     }
 }
@@ -1391,58 +1545,7 @@ static void apply_one(const ohandle *H, int mode, const oc *x, oc *y) {
         }
     }
     /* 6. near field (petrovgalerkinnca.jl:474, :531, :587) */
-    const otree *Tt = H->tree[0], *Ts = H->tree[1];
-    if (mode == 0) {
-#pragma omp parallel for schedule(dynamic, 4) num_threads(H->nthreads)
-        for (int t = 0; t < Tt->nnodes; ++t) {
-            int mt = Tt->end[t] - Tt->begin[t];
-            int nc = H->ncols[t];
-            if (nc == 0)
-                continue;
-            const oc *B = H->N + H->noff[t];
-            oc *acc = calloc(mt, sizeof(oc));
-            int col = 0;
-            for (int i = H->nearptr[t]; i < H->nearptr[t + 1]; ++i) {
-                int s = H->nearnodes[i];
-                for (int pos = Ts->begin[s]; pos < Ts->end[s]; ++pos, ++col) {
-                    oc xj = x[Ts->perm[pos]];
-                    for (int a = 0; a < mt; ++a) {
-                        oc t2 = oc_mul(B[a + (long)col * mt], xj);
-                        acc[a].re += t2.re;
-                        acc[a].im += t2.im;
-                    }
-                }
-            }
-            for (int a = 0; a < mt; ++a) {
-                long gi = Tt->perm[Tt->begin[t] + a];
-                y[gi].re += acc[a].re;
-                y[gi].im += acc[a].im;
-            }
-            free(acc);
-        }
-    } else {
-#pragma omp parallel for schedule(dynamic, 4) num_threads(H->nthreads)
-        for (int s = 0; s < Ts->nnodes; ++s) {
-            int ms = Ts->end[s] - Ts->begin[s];
-            for (int k = H->tnearptr[s]; k < H->tnearptr[s + 1]; ++k) {
-                int t = H->tnearnodes[k];
-                int mt = Tt->end[t] - Tt->begin[t];
-                const oc *B = H->N + H->noff[t] + (long)H->tnear_coloff[k] * mt;
-                for (int j = 0; j < ms; ++j) {
-                    oc acc = oc_make(0.0, 0.0);
-                    for (int a = 0; a < mt; ++a) {
-                        oc t2 = oc_mul(opentry(B[a + (long)j * mt], conj),
-                                       x[Tt->perm[Tt->begin[t] + a]]);
-                        acc.re += t2.re;
-                        acc.im += t2.im;
-                    }
-                    long gj = Ts->perm[Ts->begin[s] + j];
-                    y[gj].re += acc.re;
-                    y[gj].im += acc.im;
-                }
-            }
-        }
-    }
+    near_apply(H, mode, x, y);
     free(xhat);
     free(yhat);
 }
@@ -1474,4 +1577,1031 @@ void oracle_dense_rows(int kind, int sign, double k, double rmin, const double *
         y[2 * r] = (double)re;
         y[2 * r + 1] = (double)im;
     }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* IACA: tree-mimicry columns, maximum-value rows, extrapolated Frobenius stop            */
+/* ------------------------------------------------------------------------------------ */
+/*
+ * The reference builds directional bases with BottomUp(factorization=IACA(MaximumValue(),
+ * TreeMimicryPivoting(...), FNormExtrapolator(tol))) on the test side and the mirrored
+ * IACA(TreeMimicryPivoting(...), MaximumValue(), ...) on the trial side
+ * (test/nca/test_petrovgalerkinnca.jl:131-139; call sites src/pivoting/pivots.jl:215-300,
+ * :329-364, :450-513). IACA, MaximumValue and FNormExtrapolator live in
+ * AdaptiveCrossApproximation.jl 0.4, which is not in the reference tree, so the project fixes
+ * this rule (what the call sites fix is kept: only the own side is sampled by value, the
+ * geometric side by tree mimicry over the far nodes, the rank limit is
+ * min(maxrank, candidates, far points), and one evaluated column past the rank is rejected):
+ *
+ *   for k = 1, 2, ... up to the rank limit n:
+ *     j_k   = the next tree-mimicry far point (the pick sequence of _selectfarpivots);
+ *     c     = K[rows, j_k]                      (a column of the block, rows = candidates);
+ *     S    += ||c||^2                           (squared norm of the sampled columns);
+ *     r     = c; for l < k: r -= u_l * r[i_l]   (elimination against the accepted crosses);
+ *     pass  = ||r||^2 * k <= tol^2 * S
+ *           (FNormEstimator's test ||u_k|| ||v_k|| <= tol ||A_k||_F with the norms over the
+ *            whole far field extrapolated uniformly from the k sampled columns: the new
+ *            column's residual stands for every column's);
+ *     stop, rejecting column k, when it passes and column k - 1 passed too (the extrapolation
+ *           confirmed by two samples), or when r is exactly zero;
+ *     i_k   = argmax_i |r_i|^2                  (maximum value, lowest row on ties);
+ *     u_k   = r / r[i_k], u_k[i_k] = 1.
+ *   Singular check as _crossfactorization (src/utils/utils.jl:57-80) on the pivots |r[i_k]|^2.
+ *   X = U L^{-1} with L = U[tau, :] (unit lower triangular): X = K[rows, sigma] K[tau, sigma]^{-1},
+ *   solved in place column by column from the last, row by row.
+ *
+ * The squared norms are summed in the order of a 32-lane warp whose lane l owns the rows
+ * l + 32 q (each lane in q order, then an xor butterfly over offsets 16, 8, 4, 2, 1); the
+ * device kernel uses the same order, so both take the same decisions bit for bit.
+ */
+static double warp_norm2(const oc *v, int m) {
+    double part[32], nxt[32];
+    for (int l = 0; l < 32; ++l) {
+        double a = 0.0;
+        for (int i = l; i < m; i += 32)
+            a = a + oc_abs2(v[i]);
+        part[l] = a;
+    }
+    for (int off = 16; off >= 1; off >>= 1) {
+        for (int l = 0; l < 32; ++l)
+            nxt[l] = part[l] + part[l ^ off];
+        memcpy(part, nxt, sizeof part);
+    }
+    return part[0];
+}
+
+/* Sum of the capped sizes of the far nodes in list order, up to `limit` (the far points
+ * available to the rank limit, pivots.jl:15-25 and :66-68). */
+static int farcount_capped(const otree *F, const int *farnodes, int nfar, int limit) {
+    int n = 0;
+    for (int i = 0; i < nfar && n < limit; ++i)
+        n += clustersize_capped(F, farnodes[i], limit - n);
+    return n;
+}
+
+/* IACA of the block K[rows, far field] of one cluster (or item) with the centroid c of its
+ * points. side 0: rows are test points, columns trial points; side 1 the transposed block.
+ * Writes the local row pivots, the far point ids of the column pivots and X (m x rank, in the
+ * m x n buffer U). Returns the rank, or -1 for a singular cross matrix (*nrank: numerical rank). */
+static int iaca_block(const okern *K, int side, const double *ownpts, const double *farpts,
+                      const otree *F, const double *c, const int *farnodes, int nfar,
+                      const int *rows, int m, int maxrank, double tol, int *rowpiv,
+                      int *colpiv, oc *U, int *nrank) {
+    int limit = maxrank < m ? maxrank : m;
+    int n = farcount_capped(F, farnodes, nfar, limit);
+    if (n <= 0)
+        return 0;
+    mimicry M;
+    M.F = F;
+    M.fpts = farpts;
+    memcpy(M.c, c, sizeof M.c);
+    M.nodes = farnodes;
+    M.nnodes = nfar;
+    int *chosen = malloc(sizeof(int) * n);
+    M.chosen = chosen;
+    M.chosenxyz = malloc(sizeof(double) * 3 * n);
+    M.chosenpos = malloc(sizeof(int) * n);
+    M.nchosen = 0;
+    M.rootdmin = malloc(sizeof(double) * nfar);
+    M.rootcnt = calloc(nfar, sizeof(int));
+    for (int i = 0; i < nfar; ++i)
+        M.rootdmin[i] = 1.0;
+    oc *r = malloc(sizeof(oc) * m);
+    double *piv2 = malloc(sizeof(double) * n);
+    const double tol2 = tol * tol;
+    double S = 0.0;
+    int k = 0, passed = 0;
+    for (; k < n; ++k) {
+        int j = mim_next(&M);
+        const double *q = farpts + 3 * (long)j;
+        for (int i = 0; i < m; ++i) {
+            const double *p = ownpts + 3 * (long)rows[i];
+            r[i] = side == 0 ? okern_entry(K, p, q, rows[i], j) : okern_entry(K, q, p, j, rows[i]);
+        }
+        S = S + warp_norm2(r, m);
+        for (int l = 0; l < k; ++l) {
+            oc pv = r[rowpiv[l]];
+            const oc *ul = U + (long)l * m;
+            for (int i = 0; i < m; ++i) {
+                oc t = oc_mul(ul[i], pv);
+                r[i].re = r[i].re - t.re;
+                r[i].im = r[i].im - t.im;
+            }
+        }
+        double e2 = warp_norm2(r, m);
+        const int pass = !(e2 * (double)(k + 1) > tol2 * S);
+        if (pass && (passed || e2 == 0.0))
+            break;
+        passed = pass;
+        int ib = -1;
+        double vb = -1.0;
+        for (int i = 0; i < m; ++i) {
+            double a = oc_abs2(r[i]);
+            if (a > vb) {
+                vb = a;
+                ib = i;
+            }
+        }
+        if (ib < 0)
+            break; /* no finite residual entry (non-finite kernel values): stop here */
+        oc p = r[ib];
+        double d = oc_abs2(p);
+        oc w = oc_make(p.re / d, -(p.im / d));
+        oc *uk = U + (long)k * m;
+        for (int i = 0; i < m; ++i)
+            uk[i] = i == ib ? oc_make(1.0, 0.0) : oc_mul(r[i], w);
+        rowpiv[k] = ib;
+        colpiv[k] = j;
+        piv2[k] = d;
+    }
+    const int rank = k;
+    free(r);
+    free(M.chosenxyz);
+    free(M.chosenpos);
+    free(M.rootdmin);
+    free(M.rootcnt);
+    free(chosen);
+    if (rank > 0) {
+        double d2max = 0.0, d2min = INFINITY;
+        for (int l = 0; l < rank; ++l) {
+            if (piv2[l] > d2max)
+                d2max = piv2[l];
+            if (piv2[l] < d2min)
+                d2min = piv2[l];
+        }
+        const double eps = 0x1p-52;
+        const double thr = (10.0 * eps) * (10.0 * eps) * d2max;
+        if (!(d2min > thr)) {
+            int nr = 0;
+            for (int l = 0; l < rank; ++l)
+                nr += piv2[l] > thr;
+            *nrank = nr;
+            free(piv2);
+            return -1;
+        }
+    }
+    free(piv2);
+    /* X L = U, L[l][k] = U[i_l, k]: columns from the last, each row summed over l ascending */
+    oc *Lk = malloc(sizeof(oc) * (rank > 0 ? rank : 1));
+    oc *col = malloc(sizeof(oc) * (m > 0 ? m : 1));
+    for (int kk = rank - 1; kk >= 0; --kk) {
+        for (int l = kk + 1; l < rank; ++l)
+            Lk[l] = U[rowpiv[l] + (long)kk * m];
+        for (int i = 0; i < m; ++i) {
+            oc acc = U[i + (long)kk * m];
+            for (int l = kk + 1; l < rank; ++l) {
+                oc t = oc_mul(U[i + (long)l * m], Lk[l]);
+                acc.re = acc.re - t.re;
+                acc.im = acc.im - t.im;
+            }
+            col[i] = acc;
+        }
+        memcpy(U + (long)kk * m, col, sizeof(oc) * m);
+    }
+    free(Lk);
+    free(col);
+    return rank;
+}
+
+/* Centroid of the points refidcs[0:n) (sequential sums in index order, one division each). */
+static void centroid_of(const double *pts, const int *refidcs, int n, double *c) {
+    double s[3] = {0, 0, 0};
+    for (int i = 0; i < n; ++i) {
+        const double *p = pts + 3 * (long)refidcs[i];
+        s[0] += p[0];
+        s[1] += p[1];
+        s[2] += p[2];
+    }
+    for (int d = 0; d < 3; ++d)
+        c[d] = s[d] / n;
+}
+
+/* One IACA block for the tests (rows and far nodes given; the centroid of refidcs). Returns the
+ * rank or -1 (singular, *nrank set); X is m x n_limit column-major, its first rank columns set. */
+int oracle_iaca(const otree *F, const double *ownpts, const double *farpts, int kind, int sign,
+                double k, double rmin, const double *mat, long ldmat, int side,
+                const int *refidcs, int nref, const int *rows, int m, const int *farnodes,
+                int nfar, int maxrank, double tol, int *rowpiv, int *colpiv, double *X,
+                int *nrank) {
+    okern K = {kind, sign, k, rmin, mat, ldmat};
+    double c[3];
+    centroid_of(ownpts, refidcs, nref, c);
+    return iaca_block(&K, side, ownpts, farpts, F, c, farnodes, nfar, rows, m, maxrank, tol,
+                      rowpiv, colpiv, (oc *)X, nrank);
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Directional (wideband) H^2 matrices                                                   */
+/* ------------------------------------------------------------------------------------ */
+/*
+ * Restates, on 0-based ids:
+ *   isnearwideband for bounding balls          src/admissibility/nearinteractions.jl:62-95
+ *   generalised radius, low-frequency class     nearinteractions.jl:138-158
+ *   candidate directions (spherical Fibonacci)  src/admissibility/directionalsubdivision/boundingballdirections.jl:12-29
+ *   directionalfardata                          boundingballdirections.jl:44-152, abstractdirections.jl:57-116
+ *   dirfarfield, isbasisnode                    abstractdirections.jl:192-231, :238-243
+ *   directional BottomUp per (cluster, direction) src/compressors/bottomup.jl:214-424 with the IACA above
+ *   directional couplings                        src/couplingmatrices.jl:55-111
+ *   directional product stages                   src/nca/aggregate.jl:21-67, couple.jl:26-50 and :77-100,
+ *                                                disaggregate.jl:27-60 and :82-103
+ * The product loops over items with OpenMP; every output is summed by one thread in the
+ * sequential order (children gather from their parents in ascending parent order, leaves
+ * collect their clusters' basis items level by level), so the result does not depend on the
+ * thread count.
+ */
+static int isnear_wideband(const otree *A, const otree *B, int a, int b, double k, double etalf,
+                           double etahf, double gamma) {
+    double ra = A->radius[a], rb = B->radius[b];
+    const double *ca = A->center + 3 * a, *cb = B->center + 3 * b;
+    double x = ca[0] - cb[0], y = ca[1] - cb[1], z = ca[2] - cb[2];
+    double dist = sqrt(x * x + y * y + z * z) - (ra + rb);
+    double sep = dist > 0.0 ? dist : 0.0;
+    double dmin = 2.0 * ra < 2.0 * rb ? 2.0 * ra : 2.0 * rb;
+    if (k * dmin <= gamma)
+        return 2.0 * (ra > rb ? ra : rb) > etalf * sep;
+    double r2 = ra * ra > rb * rb ? ra * ra : rb * rb;
+    return 4.0 * k * r2 > etahf * sep;
+}
+
+static void dual_visit_wb(const otree *T, const otree *S, int t, int s, const double *w,
+                          pairlist *nearp, pairlist *farp) {
+    if (!isnear_wideband(T, S, t, s, w[0], w[1], w[2], w[3])) {
+        pl_push(farp, t, s);
+    } else if (isleaf(T, t) && isleaf(S, s)) {
+        pl_push(nearp, t, s);
+    } else if (isleaf(T, t)) {
+        for (int c = 0; c < S->nchildren[s]; ++c)
+            dual_visit_wb(T, S, t, S->firstchild[s] + c, w, nearp, farp);
+    } else if (isleaf(S, s)) {
+        for (int c = 0; c < T->nchildren[t]; ++c)
+            dual_visit_wb(T, S, T->firstchild[t] + c, s, w, nearp, farp);
+    } else {
+        for (int c = 0; c < T->nchildren[t]; ++c)
+            for (int d = 0; d < S->nchildren[s]; ++d)
+                dual_visit_wb(T, S, T->firstchild[t] + c, S->firstchild[s] + d, w, nearp, farp);
+    }
+}
+
+static double genradius(const otree *T, int node) {
+    int p = T->parent[node];
+    if (p < 0)
+        return T->radius[node];
+    double total = 0.0;
+    for (int c = 0; c < T->nchildren[p]; ++c)
+        total += T->radius[T->firstchild[p] + c];
+    double g = genradius(T, p), a = total / T->nchildren[p];
+    return g < a ? g : a;
+}
+
+static int islf(const otree *T, int node, double k, double gamma) {
+    return k * (2.0 * genradius(T, node)) <= gamma;
+}
+
+/* n spherical Fibonacci directions for a cluster of diameter diam; returns n. */
+static long candidate_dirs(double diam, double k, double gamma, double **out) {
+    double kd = k * diam > 0x1p-52 ? k * diam : 0x1p-52;
+    double g = gamma / kd < 1.0 ? gamma / kd : 1.0;
+    double ratio = acos(1.0 / sqrt(3.0)) / asin(g);
+    long n = (long)ceil(6.0 * pow(4.0, log(ratio) / log(2.0)));
+    if (n < 6)
+        n = 6;
+    double *D = malloc(sizeof(double) * 3 * n);
+    double ga = M_PI * (3.0 - sqrt(5.0));
+    for (long i = 0; i < n; ++i) {
+        double z = 1.0 - 2.0 * ((double)i + 0.5) / (double)n;
+        double t = 1.0 - z * z;
+        double r = sqrt(t > 0.0 ? t : 0.0);
+        D[3 * i] = r * cos((double)i * ga);
+        D[3 * i + 1] = r * sin((double)i * ga);
+        D[3 * i + 2] = z;
+    }
+    *out = D;
+    return n;
+}
+
+/* 1-based index of the candidate with the largest dot product, first on ties. */
+static int nearest_dir(const double *D, long n, const double *v) {
+    long best = 0;
+    double bd = D[0] * v[0] + D[1] * v[1] + D[2] * v[2];
+    for (long i = 1; i < n; ++i) {
+        double d = D[3 * i] * v[0] + D[3 * i + 1] * v[1] + D[3 * i + 2] * v[2];
+        if (d > bd) {
+            bd = d;
+            best = i;
+        }
+    }
+    return (int)best + 1;
+}
+
+typedef struct {
+    int *v;
+    int n, cap;
+} ivec;
+static void iv_push(ivec *a, int x) {
+    if (a->n == a->cap) {
+        a->cap = a->cap ? 2 * a->cap : 8;
+        a->v = realloc(a->v, sizeof(int) * a->cap);
+    }
+    a->v[a->n++] = x;
+}
+
+typedef struct {
+    int nitems;
+    int *farptr, *farnodes; /* far nodes grouped by direction (stable) */
+    int *dirptr, *dirs, *dirfarptr, *chdirptr, *chdirmap;
+    double *dirvec;
+    int *item_node, *item_basis, *item_chptr, *item_chidx;
+    /* build */
+    int *rank, *nrows, *piv; /* piv: nitems x maxrank */
+    long *xoff;
+    oc *X;
+    long *cptr;
+    /* product plans: the items of each level, the parents of each nested child item */
+    int *lvptr, *lvitems;
+    int *upar_ptr, *upar_item, *upar_row; /* child item -> (parent item, row offset) */
+} odirside;
+
+typedef struct {
+    ohandle base; /* points, kernel, trees, near/far lists, near blocks */
+    double wb[4]; /* k, eta_lf, eta_hf, gamma */
+    odirside sd[2];
+    long npairs;
+    int *pair_it, *pair_is; /* coupling pairs in test far-entry order */
+    long *coff;
+    oc *C;
+    int *rev_ptr, *rev_pair; /* pairs grouped by trial item (ascending pair order) */
+} odh;
+
+static int dir_local(const odirside *D, int node, int d) {
+    for (int i = D->dirptr[node]; i < D->dirptr[node + 1]; ++i)
+        if (D->dirs[i] == d)
+            return i - D->dirptr[node];
+    return -1;
+}
+
+/* directionalfardata plus the basis items (mirrors the library's host plan step for step). */
+static void dir_plan(odirside *D, const otree *T, const otree *F, const int *farptr,
+                     const int *farnodes_in, double k, double etahf, double gamma) {
+    int nn = T->nnodes;
+    D->farptr = malloc(sizeof(int) * (nn + 1));
+    memcpy(D->farptr, farptr, sizeof(int) * (nn + 1));
+    D->farnodes = malloc(sizeof(int) * (farptr[nn] > 0 ? farptr[nn] : 1));
+    memcpy(D->farnodes, farnodes_in, sizeof(int) * farptr[nn]);
+    ivec *dirs = calloc(nn, sizeof(ivec)), *cnt = calloc(nn, sizeof(ivec)), *pmap = calloc(nn, sizeof(ivec));
+    double **vec = calloc(nn, sizeof(double *));
+    int *pcount = calloc(nn, sizeof(int));
+    for (int level = 0; level < T->nlevels; ++level)
+        for (int node = T->levelptr[level]; node < T->levelptr[level + 1]; ++node) {
+            int p = T->parent[node];
+            int hasfars = farptr[node + 1] > farptr[node];
+            int hasparentvecs = p >= 0 && vec[p] != NULL;
+            int hasparentdirs = p >= 0 && dirs[p].n > 0;
+            if (islf(T, node, k, gamma)) {
+                int inherit = hasparentdirs && level > 0 && islf(T, p, k, gamma);
+                if (hasfars || inherit)
+                    iv_push(&dirs[node], 0);
+                if (inherit)
+                    iv_push(&pmap[node], 1);
+                continue;
+            }
+            if (!hasfars && !hasparentvecs)
+                continue;
+            double *total;
+            long nd = candidate_dirs(2.0 * T->radius[node], k, gamma, &total);
+            int b = farptr[node], nf = farptr[node + 1] - b;
+            int *ndir = malloc(sizeof(int) * (nf > 0 ? nf : 1));
+            const double *c = T->center + 3 * node;
+            for (int i = 0; i < nf; ++i) {
+                const double *cf = F->center + 3 * D->farnodes[b + i];
+                double v[3] = {c[0] - cf[0], c[1] - cf[1], c[2] - cf[2]};
+                ndir[i] = nearest_dir(total, nd, v);
+            }
+            /* stable grouping by direction (insertion sort keeps equal keys in order) */
+            int *ord = malloc(sizeof(int) * (nf > 0 ? nf : 1));
+            for (int i = 0; i < nf; ++i) {
+                int j = i;
+                while (j > 0 && ndir[ord[j - 1]] > ndir[i]) {
+                    ord[j] = ord[j - 1];
+                    --j;
+                }
+                ord[j] = i;
+            }
+            int *perm_nodes = malloc(sizeof(int) * (nf > 0 ? nf : 1));
+            int *sorted = malloc(sizeof(int) * (nf > 0 ? nf : 1));
+            for (int i = 0; i < nf; ++i) {
+                perm_nodes[i] = D->farnodes[b + ord[i]];
+                sorted[i] = ndir[ord[i]];
+            }
+            memcpy(D->farnodes + b, perm_nodes, sizeof(int) * nf);
+            ivec uniq = {0};
+            for (int i = 0; i < nf; ++i)
+                if (i == 0 || sorted[i] != sorted[i - 1])
+                    iv_push(&uniq, sorted[i]);
+            int noriginal = uniq.n;
+            if (p >= 0) {
+                const double *cp = T->center + 3 * p;
+                double rp2 = 2.0 * T->radius[p];
+                double mult = k * rp2 / etahf + rp2;
+                for (int di = 0; di < dirs[p].n; ++di) {
+                    const double *pv = vec[p] + 3 * di;
+                    double v[3] = {c[0] - cp[0] + mult * pv[0], c[1] - cp[1] + mult * pv[1],
+                                   c[2] - cp[2] + mult * pv[2]};
+                    int cd = nearest_dir(total, nd, v);
+                    int at = 0;
+                    for (int u = 0; u < uniq.n; ++u)
+                        if (uniq.v[u] == cd) {
+                            at = u + 1;
+                            break;
+                        }
+                    if (at == 0) {
+                        iv_push(&uniq, cd);
+                        at = uniq.n;
+                    }
+                    iv_push(&pmap[node], at);
+                }
+            }
+            for (int u = 0; u < uniq.n; ++u)
+                iv_push(&cnt[node], 0);
+            for (int u = 0, i = 0; u < noriginal; ++u)
+                while (i < nf && sorted[i] == uniq.v[u]) {
+                    cnt[node].v[u]++;
+                    ++i;
+                }
+            vec[node] = malloc(sizeof(double) * 3 * (uniq.n > 0 ? uniq.n : 1));
+            for (int u = 0; u < uniq.n; ++u)
+                memcpy(vec[node] + 3 * u, total + 3 * (long)(uniq.v[u] - 1), 3 * sizeof(double));
+            for (int i = 0; i < pmap[node].n; ++i)
+                pcount[node] += pmap[node].v[i] != 0;
+            dirs[node] = uniq;
+            free(total);
+            free(ndir);
+            free(ord);
+            free(perm_nodes);
+            free(sorted);
+        }
+    for (int node = 0; node < nn; ++node)
+        if (dirs[node].n > 0 && cnt[node].n == 0) {
+            int f = farptr[node + 1] - farptr[node];
+            iv_push(&cnt[node], f > 0 ? f : 0);
+            pcount[node] = pmap[node].n;
+        }
+    D->dirptr = malloc(sizeof(int) * (nn + 1));
+    D->chdirptr = malloc(sizeof(int) * (nn + 1));
+    D->dirptr[0] = D->chdirptr[0] = 0;
+    for (int node = 0; node < nn; ++node) {
+        D->dirptr[node + 1] = D->dirptr[node] + dirs[node].n;
+        D->chdirptr[node + 1] = D->chdirptr[node] + pcount[node];
+    }
+    int ni = D->dirptr[nn];
+    D->nitems = ni;
+    D->dirs = malloc(sizeof(int) * (ni > 0 ? ni : 1));
+    D->dirvec = calloc(3 * (size_t)(ni > 0 ? ni : 1), sizeof(double));
+    D->dirfarptr = malloc(sizeof(int) * (ni + 1));
+    D->chdirmap = malloc(sizeof(int) * (D->chdirptr[nn] > 0 ? D->chdirptr[nn] : 1));
+    D->item_node = malloc(sizeof(int) * (ni > 0 ? ni : 1));
+    for (int node = 0; node < nn; ++node) {
+        int off = farptr[node];
+        for (int u = 0; u < dirs[node].n; ++u) {
+            int item = D->dirptr[node] + u;
+            D->dirs[item] = dirs[node].v[u];
+            D->item_node[item] = node;
+            if (vec[node])
+                memcpy(D->dirvec + 3 * item, vec[node] + 3 * u, 3 * sizeof(double));
+            D->dirfarptr[item] = off;
+            off += cnt[node].v[u];
+        }
+        for (int i = 0; i < pcount[node]; ++i)
+            D->chdirmap[D->chdirptr[node] + i] = pmap[node].v[i];
+    }
+    D->dirfarptr[ni] = farptr[nn];
+    /* basis items and the children's items of nested ones */
+    D->item_basis = malloc(sizeof(int) * (ni > 0 ? ni : 1));
+    D->item_chptr = malloc(sizeof(int) * (ni + 1));
+    ivec ch = {0};
+    D->item_chptr[0] = 0;
+    for (int item = 0; item < ni; ++item) {
+        int node = D->item_node[item];
+        int basis;
+        if (isleaf(T, node)) {
+            basis = 1;
+        } else if (D->dirs[item] == 0) {
+            basis = 0;
+        } else {
+            int fc = T->firstchild[node];
+            int nfc = D->dirptr[fc + 1] - D->dirptr[fc];
+            basis = nfc == 0 || (nfc == 1 && D->dirs[D->dirptr[fc]] == 0);
+        }
+        D->item_basis[item] = basis;
+        if (!basis) {
+            int local = item - D->dirptr[node];
+            for (int c = 0; c < T->nchildren[node]; ++c) {
+                int chn = T->firstchild[node] + c;
+                int ncm = D->chdirptr[chn + 1] - D->chdirptr[chn];
+                int m = local < ncm ? D->chdirmap[D->chdirptr[chn] + local] : 0;
+                iv_push(&ch, m > 0 ? D->dirptr[chn] + m - 1 : -1);
+            }
+        }
+        D->item_chptr[item + 1] = ch.n;
+    }
+    D->item_chidx = ch.v ? ch.v : malloc(sizeof(int));
+    for (int node = 0; node < nn; ++node) {
+        free(dirs[node].v);
+        free(cnt[node].v);
+        free(pmap[node].v);
+        free(vec[node]);
+    }
+    free(dirs);
+    free(cnt);
+    free(pmap);
+    free(vec);
+    free(pcount);
+}
+
+/* dirfarfield of an item (abstractdirections.jl:192-231): its own far nodes, then those of the
+ * ancestors' directions that map onto it, nearest ancestor first. */
+static void dir_farfield(const odirside *D, const otree *T, int item, ivec *ff) {
+    ff->n = 0;
+    int node = D->item_node[item];
+    if (D->dirs[item] == 0) {
+        for (int cur = node; cur >= 0; cur = T->parent[cur]) {
+            int loc = dir_local(D, cur, 0);
+            if (loc < 0)
+                break;
+            int it = D->dirptr[cur] + loc;
+            for (int i = D->dirfarptr[it]; i < D->dirfarptr[it + 1]; ++i)
+                iv_push(ff, D->farnodes[i]);
+        }
+        return;
+    }
+    for (int i = D->dirfarptr[item]; i < D->dirfarptr[item + 1]; ++i)
+        iv_push(ff, D->farnodes[i]);
+    ivec idcs = {0}, next = {0};
+    iv_push(&idcs, item - D->dirptr[node] + 1);
+    for (int cur = node; T->parent[cur] >= 0; cur = T->parent[cur]) {
+        next.n = 0;
+        int b = D->chdirptr[cur], e = D->chdirptr[cur + 1];
+        for (int i = b; i < e; ++i) {
+            int x = D->chdirmap[i], in = 0;
+            for (int q = 0; q < idcs.n; ++q)
+                in |= idcs.v[q] == x;
+            if (in)
+                iv_push(&next, i - b + 1);
+        }
+        int par = T->parent[cur];
+        for (int q = 0; q < next.n; ++q) {
+            int it = D->dirptr[par] + next.v[q] - 1;
+            for (int i = D->dirfarptr[it]; i < D->dirfarptr[it + 1]; ++i)
+                iv_push(ff, D->farnodes[i]);
+        }
+        ivec t = idcs;
+        idcs = next;
+        next = t;
+    }
+    free(idcs.v);
+    free(next.v);
+}
+
+static void dir_build_side(odh *H, int side) {
+    ohandle *B = &H->base;
+    odirside *D = &H->sd[side];
+    const otree *T = B->tree[side], *F = B->tree[1 - side];
+    const int maxrank = B->maxrank, ni = D->nitems;
+    const double tol = B->tol[side];
+    const double *own = B->pts[side], *far = B->pts[1 - side];
+    D->rank = calloc(ni > 0 ? ni : 1, sizeof(int));
+    D->nrows = calloc(ni > 0 ? ni : 1, sizeof(int));
+    D->piv = malloc(sizeof(int) * (size_t)(ni > 0 ? ni : 1) * (maxrank > 0 ? maxrank : 1));
+    oc **Xi = calloc(ni > 0 ? ni : 1, sizeof(oc *));
+    double *cent = malloc(sizeof(double) * 3 * T->nnodes);
+    for (int t = 0; t < T->nnodes; ++t)
+        if (T->end[t] > T->begin[t])
+            centroid_of(own, T->perm + T->begin[t], T->end[t] - T->begin[t], cent + 3 * t);
+    /* items per level */
+    D->lvptr = calloc(T->nlevels + 1, sizeof(int));
+    D->lvitems = malloc(sizeof(int) * (ni > 0 ? ni : 1));
+    for (int it = 0; it < ni; ++it)
+        D->lvptr[T->level[D->item_node[it]] + 1]++;
+    for (int l = 0; l < T->nlevels; ++l)
+        D->lvptr[l + 1] += D->lvptr[l];
+    {
+        int *fill = malloc(sizeof(int) * (T->nlevels + 1));
+        memcpy(fill, D->lvptr, sizeof(int) * (T->nlevels + 1));
+        for (int it = 0; it < ni; ++it)
+            D->lvitems[fill[T->level[D->item_node[it]]]++] = it;
+        free(fill);
+    }
+    int failed = 0;
+    for (int lev = T->nlevels - 1; lev >= 0 && !failed; --lev) {
+#pragma omp parallel for schedule(dynamic, 16) num_threads(B->nthreads)
+        for (int q = D->lvptr[lev]; q < D->lvptr[lev + 1]; ++q) {
+            int it = D->lvitems[q];
+            int node = D->item_node[it];
+            ivec ff = {0};
+            dir_farfield(D, T, it, &ff);
+            if (ff.n == 0) {
+                free(ff.v);
+                continue;
+            }
+            int m = 0;
+            int *rows;
+            if (D->item_basis[it]) {
+                m = T->end[node] - T->begin[node];
+                rows = malloc(sizeof(int) * (m > 0 ? m : 1));
+                memcpy(rows, T->perm + T->begin[node], sizeof(int) * m);
+            } else {
+                for (int c = D->item_chptr[it]; c < D->item_chptr[it + 1]; ++c)
+                    m += D->item_chidx[c] >= 0 ? D->rank[D->item_chidx[c]] : 0;
+                rows = malloc(sizeof(int) * (m > 0 ? m : 1));
+                int o = 0;
+                for (int c = D->item_chptr[it]; c < D->item_chptr[it + 1]; ++c) {
+                    int chi = D->item_chidx[c];
+                    if (chi < 0)
+                        continue;
+                    memcpy(rows + o, D->piv + (size_t)chi * maxrank, sizeof(int) * D->rank[chi]);
+                    o += D->rank[chi];
+                }
+            }
+            D->nrows[it] = m;
+            int limit = maxrank < m ? maxrank : m;
+            oc *U = malloc(sizeof(oc) * ((size_t)m * (limit > 0 ? limit : 1) + 1));
+            int rp[256], cp[256], nr = 0;
+            int r = m > 0 ? iaca_block(&B->K, side, own, far, F, cent + 3 * node, ff.v, ff.n, rows, m,
+                                       maxrank, tol, rp, cp, U, &nr)
+                          : 0;
+            if (r < 0) {
+#pragma omp critical
+                {
+                    if (!failed || it < B->bad_node) {
+                        failed = 1;
+                        B->bad_side = side;
+                        B->bad_node = it;
+                        B->bad_npiv = limit;
+                        B->bad_rank = nr;
+                    }
+                }
+                r = 0;
+            }
+            D->rank[it] = r;
+            for (int l = 0; l < r; ++l)
+                D->piv[(size_t)it * maxrank + l] = rows[rp[l]];
+            Xi[it] = U;
+            free(rows);
+            free(ff.v);
+        }
+    }
+    if (failed)
+        B->status = 1;
+    D->xoff = malloc(sizeof(long) * (ni + 1));
+    D->cptr = malloc(sizeof(long) * (ni + 1));
+    D->xoff[0] = D->cptr[0] = 0;
+    for (int it = 0; it < ni; ++it) {
+        D->xoff[it + 1] = D->xoff[it] + (long)D->nrows[it] * D->rank[it];
+        D->cptr[it + 1] = D->cptr[it] + D->rank[it];
+    }
+    D->X = malloc(sizeof(oc) * (D->xoff[ni] > 0 ? D->xoff[ni] : 1));
+    for (int it = 0; it < ni; ++it) {
+        if (Xi[it])
+            memcpy(D->X + D->xoff[it], Xi[it], sizeof(oc) * (D->xoff[it + 1] - D->xoff[it]));
+        free(Xi[it]);
+    }
+    free(Xi);
+    free(cent);
+    /* parents of each nested child item, ascending parent order, with the child's row offset */
+    D->upar_ptr = calloc(ni + 1, sizeof(int));
+    for (int it = 0; it < ni; ++it)
+        if (!D->item_basis[it])
+            for (int c = D->item_chptr[it]; c < D->item_chptr[it + 1]; ++c)
+                if (D->item_chidx[c] >= 0)
+                    D->upar_ptr[D->item_chidx[c] + 1]++;
+    for (int it = 0; it < ni; ++it)
+        D->upar_ptr[it + 1] += D->upar_ptr[it];
+    int tot = D->upar_ptr[ni];
+    D->upar_item = malloc(sizeof(int) * (tot > 0 ? tot : 1));
+    D->upar_row = malloc(sizeof(int) * (tot > 0 ? tot : 1));
+    int *fill = malloc(sizeof(int) * (ni > 0 ? ni : 1));
+    memcpy(fill, D->upar_ptr, sizeof(int) * ni);
+    for (int it = 0; it < ni; ++it) {
+        if (D->item_basis[it])
+            continue;
+        int row = 0;
+        for (int c = D->item_chptr[it]; c < D->item_chptr[it + 1]; ++c) {
+            int chi = D->item_chidx[c];
+            if (chi < 0)
+                continue;
+            D->upar_item[fill[chi]] = it;
+            D->upar_row[fill[chi]++] = row;
+            row += D->rank[chi];
+        }
+    }
+    free(fill);
+}
+
+static void dir_couplings(odh *H) {
+    ohandle *B = &H->base;
+    odirside *Dt = &H->sd[0], *Ds = &H->sd[1];
+    const otree *T = B->tree[0], *S = B->tree[1];
+    long nf = Dt->farptr[T->nnodes];
+    int *item_t = malloc(sizeof(int) * (nf > 0 ? nf : 1));
+    int *item_s = malloc(sizeof(int) * (Ds->farptr[S->nnodes] > 0 ? Ds->farptr[S->nnodes] : 1));
+    for (int it = 0; it < Dt->nitems; ++it)
+        for (int e = Dt->dirfarptr[it]; e < Dt->dirfarptr[it + 1]; ++e)
+            item_t[e] = it;
+    for (int it = 0; it < Ds->nitems; ++it)
+        for (int e = Ds->dirfarptr[it]; e < Ds->dirfarptr[it + 1]; ++e)
+            item_s[e] = it;
+    H->pair_it = malloc(sizeof(int) * (nf > 0 ? nf : 1));
+    H->pair_is = malloc(sizeof(int) * (nf > 0 ? nf : 1));
+    long np = 0;
+    for (int t = 0; t < T->nnodes; ++t)
+        for (int e = Dt->farptr[t]; e < Dt->farptr[t + 1]; ++e) {
+            int s = Dt->farnodes[e];
+            int q = -1;
+            for (int f = Ds->farptr[s]; f < Ds->farptr[s + 1]; ++f)
+                if (Ds->farnodes[f] == t) {
+                    q = f;
+                    break;
+                }
+            int it = item_t[e], is = item_s[q];
+            if (Dt->rank[it] > 0 && Ds->rank[is] > 0) {
+                H->pair_it[np] = it;
+                H->pair_is[np] = is;
+                ++np;
+            }
+        }
+    H->npairs = np;
+    H->coff = malloc(sizeof(long) * (np + 1));
+    H->coff[0] = 0;
+    for (long p = 0; p < np; ++p)
+        H->coff[p + 1] = H->coff[p] + (long)Dt->rank[H->pair_it[p]] * Ds->rank[H->pair_is[p]];
+    H->C = malloc(sizeof(oc) * (H->coff[np] > 0 ? H->coff[np] : 1));
+    const int maxrank = B->maxrank;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(B->nthreads)
+    for (long p = 0; p < np; ++p) {
+        int it = H->pair_it[p], is = H->pair_is[p];
+        int kt = Dt->rank[it], ks = Ds->rank[is];
+        const int *tp = Dt->piv + (size_t)it * maxrank, *sp = Ds->piv + (size_t)is * maxrank;
+        oc *Cb = H->C + H->coff[p];
+        for (int j = 0; j < ks; ++j)
+            for (int a = 0; a < kt; ++a)
+                Cb[a + (long)j * kt] = okern_entry(&B->K, side_pt(B, 0, tp[a]), side_pt(B, 1, sp[j]),
+                                                   tp[a], sp[j]);
+    }
+    /* pairs grouped by trial item, in ascending pair order inside each group */
+    int nis = Ds->nitems;
+    H->rev_ptr = calloc(nis + 1, sizeof(int));
+    for (long p = 0; p < np; ++p)
+        H->rev_ptr[H->pair_is[p] + 1]++;
+    for (int i = 0; i < nis; ++i)
+        H->rev_ptr[i + 1] += H->rev_ptr[i];
+    H->rev_pair = malloc(sizeof(int) * (np > 0 ? np : 1));
+    int *fill = malloc(sizeof(int) * (nis > 0 ? nis : 1));
+    memcpy(fill, H->rev_ptr, sizeof(int) * nis);
+    for (long p = 0; p < np; ++p)
+        H->rev_pair[fill[H->pair_is[p]]++] = (int)p;
+    free(fill);
+    free(item_t);
+    free(item_s);
+}
+
+odh *oracle_dir_build(const double *tp, long nt, const double *sp, long ns, int minvalues, double k,
+                      double etalf, double etahf, double gamma, int kind, int sign, double kk,
+                      double rmin, const double *mat, long ldmat, double tol_test, double tol_trial,
+                      int maxrank, int nthreads) {
+    odh *H = calloc(1, sizeof(odh));
+    ohandle *B = &H->base;
+    B->nthreads = nthreads > 0 ? nthreads : 1;
+    B->npts[0] = nt;
+    B->npts[1] = ns;
+    B->pts[0] = malloc(sizeof(double) * 3 * (nt > 0 ? nt : 1));
+    B->pts[1] = malloc(sizeof(double) * 3 * (ns > 0 ? ns : 1));
+    memcpy(B->pts[0], tp, sizeof(double) * 3 * nt);
+    memcpy(B->pts[1], sp, sizeof(double) * 3 * ns);
+    if (kind == OK_MATRIX) {
+        B->mat_copy = malloc(sizeof(double) * 2 * ldmat * ns);
+        memcpy(B->mat_copy, mat, sizeof(double) * 2 * ldmat * ns);
+    }
+    okern K = {kind, sign, kk, rmin, B->mat_copy, ldmat};
+    B->K = K;
+    B->maxrank = maxrank;
+    B->tol[0] = tol_test;
+    B->tol[1] = tol_trial;
+    H->wb[0] = k;
+    H->wb[1] = etalf;
+    H->wb[2] = etahf;
+    H->wb[3] = gamma;
+    B->tree[0] = oracle_tree_build(tp, nt, minvalues);
+    B->tree[1] = oracle_tree_build(sp, ns, minvalues);
+    pairlist nearp = {0}, farp = {0};
+    dual_visit_wb(B->tree[0], B->tree[1], 0, 0, H->wb, &nearp, &farp);
+    int nnt = B->tree[0]->nnodes, nns = B->tree[1]->nnodes;
+    pairs_to_csr(nearp.t, nearp.s, nearp.n, nnt, &B->nearptr, &B->nearnodes);
+    pairs_to_csr(farp.t, farp.s, farp.n, nnt, &B->farptr, &B->farnodes);
+    pairs_to_csr(nearp.s, nearp.t, nearp.n, nns, &B->tnearptr, &B->tnearnodes);
+    pairs_to_csr(farp.s, farp.t, farp.n, nns, &B->tfarptr, &B->tfarnodes);
+    free(nearp.t); free(nearp.s); free(farp.t); free(farp.s);
+    dir_plan(&H->sd[0], B->tree[0], B->tree[1], B->farptr, B->farnodes, k, etahf, gamma);
+    dir_plan(&H->sd[1], B->tree[1], B->tree[0], B->tfarptr, B->tfarnodes, k, etahf, gamma);
+    dir_build_side(H, 0);
+    if (B->status == 0)
+        dir_build_side(H, 1);
+    if (B->status == 0) {
+        dir_couplings(H);
+        build_near(B);
+    }
+    return H;
+}
+
+void oracle_dir_free(odh *H) {
+    if (!H)
+        return;
+    for (int s = 0; s < 2; ++s) {
+        odirside *D = &H->sd[s];
+        free(D->farptr); free(D->farnodes); free(D->dirptr); free(D->dirs); free(D->dirfarptr);
+        free(D->chdirptr); free(D->chdirmap); free(D->dirvec); free(D->item_node);
+        free(D->item_basis); free(D->item_chptr); free(D->item_chidx); free(D->rank);
+        free(D->nrows); free(D->piv); free(D->xoff); free(D->X); free(D->cptr); free(D->lvptr);
+        free(D->lvitems); free(D->upar_ptr); free(D->upar_item); free(D->upar_row);
+    }
+    free(H->pair_it); free(H->pair_is); free(H->coff); free(H->C); free(H->rev_ptr);
+    free(H->rev_pair);
+    oracle_free_fields(&H->base);
+    free(H);
+}
+
+/* ---- getters (ctypes) ---- */
+int oracle_dir_status(const odh *H, int *side, int *item, int *npiv, int *rank) {
+    return oracle_status(&H->base, side, item, npiv, rank);
+}
+const otree *oracle_dir_tree(const odh *H, int side) { return H->base.tree[side]; }
+int oracle_dir_nitems(const odh *H, int side) { return H->sd[side].nitems; }
+long oracle_dir_nfar(const odh *H, int side) {
+    return H->sd[side].farptr[H->base.tree[side]->nnodes];
+}
+int oracle_dir_nchildren(const odh *H, int side) {
+    return H->sd[side].item_chptr[H->sd[side].nitems];
+}
+void oracle_dir_plan(const odh *H, int side, int *farnodes, int *dirptr, int *dirs, double *dirvec,
+                     int *dirfarptr, int *item_basis, int *item_chptr, int *item_chidx) {
+    const odirside *D = &H->sd[side];
+    int nn = H->base.tree[side]->nnodes, ni = D->nitems;
+    memcpy(farnodes, D->farnodes, sizeof(int) * D->farptr[nn]);
+    memcpy(dirptr, D->dirptr, sizeof(int) * (nn + 1));
+    memcpy(dirs, D->dirs, sizeof(int) * ni);
+    memcpy(dirvec, D->dirvec, sizeof(double) * 3 * ni);
+    memcpy(dirfarptr, D->dirfarptr, sizeof(int) * (ni + 1));
+    memcpy(item_basis, D->item_basis, sizeof(int) * ni);
+    memcpy(item_chptr, D->item_chptr, sizeof(int) * (ni + 1));
+    memcpy(item_chidx, D->item_chidx, sizeof(int) * D->item_chptr[ni]);
+}
+/* ranks, rows and pivots (CSR over items) of one side */
+void oracle_dir_pivots(const odh *H, int side, int *rank, int *nrows, int *ptr, int *idx) {
+    const odirside *D = &H->sd[side];
+    int ni = D->nitems;
+    memcpy(rank, D->rank, sizeof(int) * ni);
+    memcpy(nrows, D->nrows, sizeof(int) * ni);
+    ptr[0] = 0;
+    for (int it = 0; it < ni; ++it) {
+        memcpy(idx + ptr[it], D->piv + (size_t)it * H->base.maxrank, sizeof(int) * D->rank[it]);
+        ptr[it + 1] = ptr[it] + D->rank[it];
+    }
+}
+long oracle_dir_x_total(const odh *H, int side) { return H->sd[side].xoff[H->sd[side].nitems]; }
+void oracle_dir_x(const odh *H, int side, long *off, double *X) {
+    const odirside *D = &H->sd[side];
+    memcpy(off, D->xoff, sizeof(long) * (D->nitems + 1));
+    memcpy(X, D->X, sizeof(oc) * D->xoff[D->nitems]);
+}
+/* entries the product reads once: bases/transfers (X), couplings and the near field */
+void oracle_dir_sizes(const odh *H, long *xentries, long *centries, long *nentries, long *npairs) {
+    *xentries = H->sd[0].xoff[H->sd[0].nitems] + H->sd[1].xoff[H->sd[1].nitems];
+    *centries = H->coff[H->npairs];
+    *nentries = H->base.noff[H->base.tree[0]->nnodes];
+    *npairs = H->npairs;
+}
+
+/* One right-hand side of the directional product: mode 0 = A, 1 = transpose, 2 = adjoint. */
+static void dir_apply_one(const odh *H, int mode, const oc *x, oc *y) {
+    const ohandle *B = &H->base;
+    int conj = mode == 2;
+    int in = mode == 0 ? 1 : 0, out = 1 - in;
+    const odirside *DI = &H->sd[in], *DO = &H->sd[out];
+    const otree *TI = B->tree[in], *TO = B->tree[out];
+    oc *xhat = calloc(DI->cptr[DI->nitems] > 0 ? DI->cptr[DI->nitems] : 1, sizeof(oc));
+    oc *yhat = calloc(DO->cptr[DO->nitems] > 0 ? DO->cptr[DO->nitems] : 1, sizeof(oc));
+    for (long i = 0; i < B->npts[out]; ++i)
+        y[i] = oc_make(0.0, 0.0);
+    int cin = in == 1 ? 0 : conj, cout = out == 0 ? 0 : conj;
+    /* up: xhat_item = op(X)^T [x of its cluster | xhat of its children's items] */
+    for (int lev = TI->nlevels - 1; lev >= 0; --lev) {
+#pragma omp parallel for schedule(dynamic, 32) num_threads(B->nthreads)
+        for (int q = DI->lvptr[lev]; q < DI->lvptr[lev + 1]; ++q) {
+            int it = DI->lvitems[q];
+            int r = DI->rank[it], m = DI->nrows[it];
+            if (r == 0)
+                continue;
+            const oc *X = DI->X + DI->xoff[it];
+            oc *xh = xhat + DI->cptr[it];
+            if (DI->item_basis[it]) {
+                int node = DI->item_node[it];
+                oc *xs = malloc(sizeof(oc) * m);
+                for (int a = 0; a < m; ++a)
+                    xs[a] = x[TI->perm[TI->begin[node] + a]];
+                small_gemv(X, m, r, m, 1, cin, xs, xh);
+                free(xs);
+            } else {
+                int row = 0;
+                for (int c = DI->item_chptr[it]; c < DI->item_chptr[it + 1]; ++c) {
+                    int chi = DI->item_chidx[c];
+                    if (chi < 0)
+                        continue;
+                    int rc = DI->rank[chi];
+                    if (rc)
+                        small_gemv(X + row, rc, r, m, 1, cin, xhat + DI->cptr[chi], xh);
+                    row += rc;
+                }
+            }
+        }
+    }
+    /* coupling */
+    if (mode == 0) {
+        /* the pairs of one test item are consecutive (test far-entry order): the thread that
+         * meets the first of them sums them all */
+#pragma omp parallel for schedule(dynamic, 64) num_threads(B->nthreads)
+        for (long q = 0; q < H->npairs; ++q) {
+            if (q > 0 && H->pair_it[q - 1] == H->pair_it[q])
+                continue;
+            int it = H->pair_it[q];
+            for (long e = q; e < H->npairs && H->pair_it[e] == it; ++e) {
+                int is = H->pair_is[e];
+                small_gemv(H->C + H->coff[e], H->sd[0].rank[it], H->sd[1].rank[is], H->sd[0].rank[it],
+                           0, 0, xhat + H->sd[1].cptr[is], yhat + H->sd[0].cptr[it]);
+            }
+        }
+    } else {
+#pragma omp parallel for schedule(dynamic, 64) num_threads(B->nthreads)
+        for (int is = 0; is < H->sd[1].nitems; ++is)
+            for (int k = H->rev_ptr[is]; k < H->rev_ptr[is + 1]; ++k) {
+                long e = H->rev_pair[k];
+                int it = H->pair_it[e];
+                small_gemv(H->C + H->coff[e], H->sd[0].rank[it], H->sd[1].rank[is], H->sd[0].rank[it],
+                           1, conj, xhat + H->sd[0].cptr[it], yhat + H->sd[1].cptr[is]);
+            }
+    }
+    /* down: each nested child item gathers op(X_parent)[its rows] yhat_parent, parents ascending */
+    for (int lev = 1; lev < TO->nlevels; ++lev) {
+#pragma omp parallel for schedule(dynamic, 32) num_threads(B->nthreads)
+        for (int q = DO->lvptr[lev]; q < DO->lvptr[lev + 1]; ++q) {
+            int ch = DO->lvitems[q];
+            int rc = DO->rank[ch];
+            if (rc == 0)
+                continue;
+            oc *yc = yhat + DO->cptr[ch];
+            for (int k = DO->upar_ptr[ch]; k < DO->upar_ptr[ch + 1]; ++k) {
+                int par = DO->upar_item[k], row = DO->upar_row[k];
+                int r = DO->rank[par], m = DO->nrows[par];
+                const oc *X = DO->X + DO->xoff[par];
+                const oc *yp = yhat + DO->cptr[par];
+                for (int j = 0; j < r; ++j) {
+                    oc xj = yp[j];
+                    for (int a = 0; a < rc; ++a) {
+                        oc t = oc_mul(opentry(X[row + a + (long)j * m], cout), xj);
+                        yc[a].re += t.re;
+                        yc[a].im += t.im;
+                    }
+                }
+            }
+        }
+    }
+    /* leaves: y[points of the cluster] += op(X) yhat for every basis item, level by level */
+    for (int lev = 0; lev < TO->nlevels; ++lev) {
+#pragma omp parallel for schedule(dynamic, 16) num_threads(B->nthreads)
+        for (int node = TO->levelptr[lev]; node < TO->levelptr[lev + 1]; ++node)
+            for (int it = DO->dirptr[node]; it < DO->dirptr[node + 1]; ++it) {
+                int r = DO->rank[it], m = DO->nrows[it];
+                if (!DO->item_basis[it] || r == 0)
+                    continue;
+                const oc *X = DO->X + DO->xoff[it];
+                const oc *yh = yhat + DO->cptr[it];
+                for (int a = 0; a < m; ++a) {
+                    oc acc = oc_make(0.0, 0.0);
+                    for (int j = 0; j < r; ++j) {
+                        oc t = oc_mul(opentry(X[a + (long)j * m], cout), yh[j]);
+                        acc.re += t.re;
+                        acc.im += t.im;
+                    }
+                    long gi = TO->perm[TO->begin[node] + a];
+                    y[gi].re += acc.re;
+                    y[gi].im += acc.im;
+                }
+            }
+    }
+    near_apply(B, mode, x, y);
+    free(xhat);
+    free(yhat);
+}
+
+void oracle_dir_apply(const odh *H, int mode, const double *x, long ldx, double *y, long ldy,
+                      long nrhs) {
+    for (long q = 0; q < nrhs; ++q)
+        dir_apply_one(H, mode, (const oc *)(x + 2 * q * ldx), (oc *)(y + 2 * q * ldy));
 }

@@ -38,7 +38,7 @@ def lib():
         L = C.CDLL(LIBPATH)
         P, I, D, LG = C.c_void_p, C.c_int, C.c_double, C.c_long
         L.oracle_build.restype = P
-        L.oracle_build.argtypes = [P, LG, P, LG, I, D, I, I, D, D, P, LG, D, D, I, I, I]
+        L.oracle_build.argtypes = [P, LG, P, LG, I, D, I, I, D, D, P, LG, D, D, I, I, I, I]
         L.oracle_free.argtypes = [P]
         L.oracle_status.argtypes = [P, P, P, P, P]
         L.oracle_tree.restype = P
@@ -71,6 +71,24 @@ def lib():
         L.oracle_aca.argtypes = [P, I, I, I, D, I, P, P]
         L.oracle_cross_solve.argtypes = [P, I, I, P, P, P]
         L.oracle_select_farpivots.argtypes = [P, P, P, P, I, P, I, I, P]
+        L.oracle_iaca.argtypes = [P, P, P, I, I, D, D, P, LG, I, P, I, P, I, P, I, I, D, P, P, P, P]
+        L.oracle_dir_build.restype = P
+        L.oracle_dir_build.argtypes = [P, LG, P, LG, I, D, D, D, D, I, I, D, D, P, LG, D, D, I, I]
+        L.oracle_dir_free.argtypes = [P]
+        L.oracle_dir_status.argtypes = [P, P, P, P, P]
+        L.oracle_dir_tree.restype = P
+        L.oracle_dir_tree.argtypes = [P, I]
+        L.oracle_dir_nitems.argtypes = [P, I]
+        L.oracle_dir_nfar.restype = LG
+        L.oracle_dir_nfar.argtypes = [P, I]
+        L.oracle_dir_nchildren.argtypes = [P, I]
+        L.oracle_dir_plan.argtypes = [P, I] + [P] * 8
+        L.oracle_dir_pivots.argtypes = [P, I, P, P, P, P]
+        L.oracle_dir_x_total.restype = LG
+        L.oracle_dir_x_total.argtypes = [P, I]
+        L.oracle_dir_x.argtypes = [P, I, P, P]
+        L.oracle_dir_sizes.argtypes = [P, P, P, P, P]
+        L.oracle_dir_apply.argtypes = [P, I, P, LG, P, LG, LG]
         _lib = L
     return _lib
 
@@ -191,15 +209,38 @@ def select_farpivots(fartree: OwnedTree, ownpts, farpts, refidcs, farnodes, maxr
     return out[:n].copy()
 
 
+def iaca(fartree: OwnedTree, kernel: Kernel, ownpts, farpts, refidcs, rows, farnodes, maxrank, tol, side=0):
+    """IACA of K[rows, far field] with tree-mimicry columns over `farnodes` (centroid of the
+    points `refidcs`): (rank, local row pivots, far column pivots, X = K[rows, sigma] K[tau, sigma]^-1)."""
+    ownpts = np.ascontiguousarray(ownpts, dtype=np.float64)
+    farpts = np.ascontiguousarray(farpts, dtype=np.float64)
+    ref = np.ascontiguousarray(refidcs, dtype=np.int32)
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    fn = np.ascontiguousarray(farnodes, dtype=np.int32)
+    m = len(rows)
+    lim = max(min(maxrank, m), 1)
+    rp = np.zeros(lim, np.int32)
+    cp = np.zeros(lim, np.int32)
+    X = np.zeros(m * lim + 1, np.complex128)
+    nr = C.c_int()
+    r = lib().oracle_iaca(fartree._ptr, _p(ownpts), _p(farpts), *kernel.args(), int(side), _p(ref), len(ref),
+                          _p(rows), m, _p(fn), len(fn), int(maxrank), float(tol), _p(rp), _p(cp), _p(X),
+                          C.byref(nr))
+    if r < 0:
+        raise SingularCross(lim, nr.value)
+    return r, rp[:r].copy(), cp[:r].copy(), X[:m * r].reshape((m, r), order="F").copy()
+
+
 class SingularBuild(Exception):
     pass
 
 
 class H2:
-    """Oracle H^2 build (batched bottom-up NCA) and its product."""
+    """Oracle H^2 build and its product: the batched bottom-up NCA, or with iaca=True the plain
+    BottomUp compressor with IACA per cluster (src/compressors/bottomup.jl:96-208)."""
 
     def __init__(self, testpts, trialpts, kernel: Kernel, minvalues=32, eta=1.0, tol=1e-4,
-                 tol_trial=None, maxrank=50, sampled=True, nthreads=None):
+                 tol_trial=None, maxrank=50, sampled=True, nthreads=None, iaca=False):
         self.testpts = np.ascontiguousarray(testpts, dtype=np.float64)
         self.trialpts = np.ascontiguousarray(trialpts, dtype=np.float64)
         self.kernel = kernel
@@ -211,6 +252,7 @@ class H2:
             _p(self.testpts), len(self.testpts), _p(self.trialpts), len(self.trialpts),
             int(minvalues), float(eta), *kernel.args(), float(tol),
             float(tol if tol_trial is None else tol_trial), int(maxrank), int(sampled), int(nthreads),
+            int(bool(iaca)),
         )
         side, node, npiv, rank = (C.c_int() for _ in range(4))
         st = L.oracle_status(self._h, C.byref(side), C.byref(node), C.byref(npiv), C.byref(rank))

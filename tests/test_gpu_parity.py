@@ -26,19 +26,26 @@ def _o():
     return oracle
 
 
-def build_pair(test, trial, k, tol, minvalues, maxrank=50, sign=1, rmin=0.0, store_f32=False):
+def build_pair(test, trial, k, tol, minvalues, maxrank=50, sign=1, rmin=0.0, store_f32=False, iaca=False):
+    """The GPU core and the oracle on the same inputs: BatchedBottomUp(ACA), or with iaca=True
+    BottomUp(IACA) on both sides (test/nca/test_petrovgalerkinnca.jl:73-80)."""
     N, O = _n(), _o()
     kern = N.HelmholtzKernel(k, sign=sign, rmin=rmin)
     tt = N.KMeansTree(test, N.KMeansTreeBuilder(minvalues=minvalues))
     st = N.KMeansTree(trial, N.KMeansTreeBuilder(minvalues=minvalues))
     tree = N.BlockTree(tt, st)
-    aca = N.ACA(N.FullPivoting(), N.FullPivoting(), N.FNormEstimator(tol))
-    tc = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(test, trial, st), compressor=aca)
-    sc = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(trial, test, tt), compressor=aca)
+    if iaca:
+        conv = N.FNormExtrapolator(tol)
+        tc = N.BottomUp(factorization=N.IACA(N.MaximumValue(), N.TreeMimicryPivoting(test, trial, st), conv))
+        sc = N.BottomUp(factorization=N.IACA(N.TreeMimicryPivoting(trial, test, tt), N.MaximumValue(), conv))
+    else:
+        aca = N.ACA(N.FullPivoting(), N.FullPivoting(), N.FNormEstimator(tol))
+        tc = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(test, trial, st), compressor=aca)
+        sc = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(trial, test, tt), compressor=aca)
     A = N.PetrovGalerkinNCA(kern, test, trial, tree, testcompressor=tc, trialcompressor=sc, maxrank=maxrank,
                             store_f32=store_f32)
     H = O.H2(test, trial, O.Kernel(O.KIND_HELMHOLTZ, k=k, sign=sign, rmin=rmin), minvalues=minvalues, tol=tol,
-             maxrank=maxrank)
+             maxrank=maxrank, iaca=iaca)
     return A, H
 
 
@@ -232,6 +239,40 @@ def test_galerkin_sphere_against_oracle():
     rows = np.random.default_rng(3).choice(8192, 256, replace=False)
     yd = O.dense_rows(O.Kernel(O.KIND_HELMHOLTZ, k=1.0), pts, pts, rows, X[:, 0])
     assert relerr(Y[rows, 0], yd) < 5e-5
+
+
+def test_galerkin_sphere_full_size():
+    """The 65,536-point low-frequency Galerkin sphere (k = 1, tol 1e-5, 64-point leaves) at full
+    size: tree, far pivots, ranks and pivots bit-exact, operators within 1e-12, and a 16-column
+    block within 1e-12 of the oracle in the forward and adjoint modes."""
+    pts = sphere(65536, 2024)
+    A, H = build_pair(pts, pts, 1.0, 1e-5, 64, rmin=1e-12)
+    compare_build(A, H)
+    X = cgauss((65536, 16), 5)
+    assert relerr(A @ X, H.apply(X, 0)) < REL
+    assert relerr(A.H @ X, H.apply(X, 2)) < REL
+
+
+@pytest.mark.parametrize("case", ["c1", "sphere"])
+def test_bottomup_iaca_against_oracle(case):
+    """BottomUp(IACA) on the plain admissibility: pivots bit-exact, operators and products within
+    1e-12 of the oracle's IACA build, dense error below 5 tol (test/nca/test_petrovgalerkinnca.jl:102)."""
+    O = _o()
+    if case == "c1":
+        test, trial = grid_c1()
+        k, tol, mv = 2 * np.pi / 10, 1e-4, 32
+    else:
+        test = trial = sphere(8192, 41)
+        k, tol, mv = 2.0, 1e-5, 64
+    A, H = build_pair(test, trial, k, tol, mv, rmin=1e-12, iaca=True)
+    compare_build(A, H)
+    X = cgauss((len(trial), 3), 42)
+    for mode, op in ((0, lambda v: A @ v), (1, lambda v: A.T @ v), (2, lambda v: A.H @ v)):
+        V = X if mode == 0 else cgauss((len(test), 3), 43)
+        assert relerr(op(V), H.apply(V, mode)) < REL
+    rows = np.arange(0, len(test), max(1, len(test) // 512))
+    yd = O.dense_rows(O.Kernel(O.KIND_HELMHOLTZ, k=k, rmin=1e-12), test, trial, rows, X[:, 0])
+    assert relerr((A @ X[:, 0])[rows], yd) < 5 * tol
 
 
 def test_exp_minus_ikr_and_rmin():

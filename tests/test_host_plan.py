@@ -21,7 +21,7 @@ def test_library_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(N._lib.SIGNATURES) == declared
-    assert lib.nca_version() == 1
+    assert lib.nca_version() == 2
 
 
 @pytest.mark.parametrize("n,mv,seed", [(1024, 32, 1), (5000, 20, 2), (30000, 64, 3)])

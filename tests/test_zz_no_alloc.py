@@ -169,3 +169,97 @@ def test_static_rejections(cores):
     st = lib.nca_apply_static(core._h, 5, 0, C.c_void_p(X.data_ptr()), nin, C.c_void_p(Y.data_ptr()), nout, 1,
                               1.0, 0.0, 0.0, 0.0, None)
     assert st == N._lib.NCA_ERR_ARG
+
+
+def _cudart():
+    """The CUDA runtime that torch has loaded (by soname), for stream creation and host functions."""
+    return C.CDLL("libcudart.so.12")
+
+
+def test_static_refuses_directional_cores():
+    """Directional (wideband) cores go through nca_apply only."""
+    import torch
+    N = _n()
+    pts = sphere(1500, 61)
+    t = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=32))
+    conv = N.FNormExtrapolator(1e-4)
+    A = N.PetrovGalerkinNCA(
+        N.HelmholtzKernel(12.0, rmin=1e-12), pts, pts, N.BlockTree(t, t), isnear=N.isnearwideband(12.0),
+        testcompressor=N.BottomUp(factorization=N.IACA(N.MaximumValue(), N.TreeMimicryPivoting(pts, pts, t), conv)),
+        trialcompressor=N.BottomUp(factorization=N.IACA(N.TreeMimicryPivoting(pts, pts, t), N.MaximumValue(), conv)))
+    X = device_cols(cgauss((1500, 1), 62))
+    Y = torch.zeros_like(X)
+    assert call_static(N.core(A), 0, X, Y, 1 + 0j, 0j) == N._lib.NCA_ERR_ARG
+    assert "directional" in N._lib.last_error()
+
+
+def test_static_refuses_stream_capture(cores):
+    """The call waits for its stream, so on a capturing stream it is refused before any work and
+    the capture stays valid."""
+    import torch
+    N = _n()
+    core = cores[0]
+    nin, nout = dims(core, 0)
+    X = device_cols(cgauss((nin, 2), 71))
+    Y = torch.zeros((2, nout), dtype=torch.complex128, device="cuda")
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        st = call_static(core, 0, X, Y, 1 + 0j, 0j, torch.cuda.current_stream().cuda_stream)
+        Y.add_(1.0)
+    assert st == N._lib.NCA_ERR_ARG
+    assert "captured" in N._lib.last_error()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.all(Y == 1.0)
+
+
+def test_static_overlapping_calls_are_refused(cores):
+    """A call that holds the scratch (its stream held up by a host function that waits, with a
+    timeout, on a host event) makes a second call from another thread return NCA_ERR_BUSY; once
+    the event is set, the first call completes with the product of nca_apply. Only the host
+    waits: no kernel spins."""
+    import threading
+    import time
+    import torch
+    N = _n()
+    rt = _cudart()
+    core = cores[0]
+    nin, nout = dims(core, 0)
+    X = device_cols(cgauss((nin, 3), 81))
+    ref = torch.zeros((3, nout), dtype=torch.complex128, device="cuda")
+    call_workspace(N.H2Workspace(core, max_nrhs=3), 0, X, ref, 1 + 0j, 0j)
+    torch.cuda.synchronize()
+    streams = []
+    for _ in range(2):
+        h = C.c_void_p()
+        assert rt.cudaStreamCreateWithFlags(C.byref(h), 1) == 0  # cudaStreamNonBlocking
+        streams.append(h)
+    release = threading.Event()
+    HOSTFN = C.CFUNCTYPE(None, C.c_void_p)
+    hold = HOSTFN(lambda _: release.wait(10.0))
+    Ya = torch.zeros_like(ref)
+    Yb = torch.zeros_like(ref)
+    out = {}
+    try:
+        assert rt.cudaLaunchHostFunc(streams[0], hold, None) == 0
+        thread_a = threading.Thread(target=lambda: out.setdefault("a", call_static(core, 0, X, Ya, 1 + 0j, 0j,
+                                                                                   streams[0].value)))
+        thread_a.start()
+        busy = False
+        t_end = time.time() + 5.0
+        while time.time() < t_end and not busy:
+            st = call_static(core, 0, X, Yb, 1 + 0j, 0j, streams[1].value)
+            busy = st == N._lib.NCA_ERR_BUSY
+            if not busy:
+                assert st == N._lib.NCA_OK
+                time.sleep(0.001)
+        assert busy, "the second call was never refused"
+        assert "another call" in N._lib.last_error()
+    finally:
+        release.set()
+        thread_a.join(30.0)
+        for h in streams:
+            rt.cudaStreamSynchronize(h)
+            rt.cudaStreamDestroy(h)
+    assert out.get("a") == N._lib.NCA_OK
+    assert relerr(Ya, ref) < REL
