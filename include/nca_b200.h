@@ -165,6 +165,17 @@ typedef struct {
 } nca_core_info;
 /* ---- differentiation on frozen skeletons (no counterpart in the reference, which has no
  *      gradients): the tree, partition, ranks and row/column pivots of a build stay fixed. ---- */
+/* ---- serialised cores (the reference saves a built matrix's stores and plans with JLD2 for reuse
+ *      across runs, scripts/create_test_matrix.jl:50-68) ----
+ * nca_core_save writes the core's inputs and skeleton to a file: points, trees, partition, kernel,
+ * options and per side (cluster, or directional item) the ranks, block rows, pivots and
+ * interpolation operators, plus the directional plan. nca_core_load reads it and rebuilds the
+ * couplings, the near field and the product plans on the given device: the loaded core's products
+ * equal the saved core's bit for bit. Batches are not saved (save their members); a file that is
+ * not a saved core, or is truncated, gives NCA_ERR_ARG. */
+int32_t nca_core_save(const nca_core *core, const char *path);
+int32_t nca_core_load(const char *path, int32_t device, nca_core **out);
+
 /* Refills every store at wavenumber k with the frozen skeleton: X = K[rows, sigma] K[tau, sigma]^{-1},
  * couplings, near field (and FP32 copies); bit-identical to the build at the build's own k. A
  * singular frozen cross matrix returns NCA_ERR_SINGULAR and leaves the core unchanged. Drops

@@ -236,6 +236,7 @@ struct nca_core {
     bool has_dk = false;
     bool batch = false;  // block-diagonal batch of several cores (one wavenumber per member)
     std::unique_ptr<DirCore> dir;  // directional (wideband) core: items and gather plans
+    nca::Wideband wb{};            // the wideband admissibility of a directional core
     nca_core_info info{};
     bool moved = false;  // stores moved into a batch: the core may only be destroyed
 };
@@ -747,8 +748,23 @@ void level_smem_at_least(size_t sm) {
     }
 }
 
+// The skeleton of a built core as nca_core_save writes it: per side (node or item) the ranks, block
+// rows, row pivots tau and column pivots sigma (maxrank per node), the interpolation operators X
+// at their padded offsets and, for directional cores, the directional plan. Everything else
+// (couplings, near field, product plans) is a function of the skeleton and is rebuilt by the
+// build functions when they are given one.
+struct SavedSide {
+    std::vector<int32_t> rank, nrows, piv, cpiv, fpptr, fpidx;
+    std::vector<int64_t> xoff;
+    std::vector<double2> X;
+    nca::DirSide plan;
+};
+struct SavedCore {
+    SavedSide side[2];
+};
+
 void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int64_t ns,
-                const nca_build_opts *o) {
+                const nca_build_opts *o, const SavedCore *sv = nullptr) {
     const int maxrank = c->maxrank;
     auto h0 = std::chrono::steady_clock::now();
     cudaStream_t s;
@@ -767,7 +783,7 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
     DBuf<int32_t> iffnodes[2];
     DBuf<double> icent[2], icenter[2];
     // phase 1 on the device (tree mimicry); far field = own far nodes + ancestors'
-    for (int sd = 0; sd < 2; ++sd) {
+    for (int sd = 0; sd < 2 && !sv; ++sd) {
         const nca::Tree &T = c->tree[sd];
         const std::vector<int32_t> &ptr = sd == 0 ? P.farptr : P.tfarptr;
         const std::vector<int32_t> &nodes = sd == 0 ? P.farnodes : P.tfarnodes;
@@ -818,6 +834,27 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
     for (int sd = 0; sd < 2; ++sd) {
         DevSide &d = c->side[sd];
         const nca::Tree &T = c->tree[sd];
+        if (sv) {
+            // a saved skeleton: the operators and pivots as the build left them
+            const SavedSide &v = sv->side[sd];
+            d.h_xoff = v.xoff;
+            d.xoff.upload(d.h_xoff, s);
+            d.X.upload(v.X, s);
+            d.rank.upload(v.rank, s);
+            d.nrows.upload(v.nrows, s);
+            d.piv.upload(v.piv, s);
+            d.cpiv.upload(v.cpiv, s);
+            d.h_rank = v.rank;
+            d.h_nrows = v.nrows;
+            d.h_piv = v.piv;
+            d.h_fpptr = v.fpptr;
+            d.h_fpidx = v.fpidx;
+            plan_apply(d, T, s);
+            d.XT.alloc(d.X.n);
+            launch_transpose_blocks<double2>(d.X.p, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, T.nnodes, d.XT.p, s);
+            CK(cudaGetLastError());
+            continue;
+        }
         std::vector<int32_t> lv_ptr, lv_nodes;
         std::vector<int> lv_mcap, lv_ncap;
         plan_side(d, T, maxrank, lv_ptr, lv_nodes, lv_mcap, lv_ncap);
@@ -1230,7 +1267,204 @@ struct PhaseTimer {
     }
 };
 
-void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_build_opts *o, const nca::Wideband &wb) {
+// BottomUp(IACA) of one side of a directional core: the items' far fields, then one k_iaca launch
+// per level (deepest first), each level's operators compacted to the ranks found; leaves the
+// side's X, h_xoff, ranks and rows in d.
+void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
+                       const std::vector<std::vector<int32_t>> &bylevel, cudaStream_t s, const nca_build_opts *o,
+                       PhaseTimer &timer, const std::string &side) {
+    const int maxrank = c->maxrank;
+    const nca::DirSide &pl = d.plan;
+    const nca::Tree &T = c->tree[sd], &Ft = c->tree[1 - sd];
+    DevSide &ds = c->side[sd];
+    const DevSide &fs = c->side[1 - sd];
+    const int ni = d.nitems;
+    // the items' directional far fields (dirfarfield), in the reference's order, and the far
+    // points each can offer (capped at maxrank)
+    std::vector<int64_t> ffptr;
+    std::vector<int32_t> ffnodes;
+    parallel_csr(
+        ni, [&](int it, std::vector<int32_t> &ff) { nca::item_farfield(T, pl, it, ff); }, ffptr, ffnodes);
+    std::vector<int32_t> farpts(ni, 0);
+    for (int it = 0; it < ni; ++it) {
+        int64_t n = 0;
+        for (int64_t q = ffptr[it]; q < ffptr[it + 1] && n < maxrank; ++q) n += Ft.size(ffnodes[q]);
+        farpts[it] = int32_t(std::min<int64_t>(n, maxrank));
+    }
+    const std::vector<double> centroid = cluster_centroids(T, ownpts);
+    DBuf<int64_t> dffptr;
+    DBuf<int32_t> dffnodes;
+    DBuf<double> dcent, dcenter;
+    dffptr.upload(ffptr, s);
+    dffnodes.upload(ffnodes, s);
+    dcent.upload(centroid, s);
+    dcenter.upload(Ft.center, s);
+    timer.mark(side + "item far fields and centroids uploaded");
+    // the side's items, level by level
+    DBuf<int32_t> status;
+    status.alloc(5);  // [flag, item, a, b], item cursor
+    d.item_node.upload(pl.item_node, s);
+    d.item_basis.upload(pl.item_basis, s);
+    d.item_chptr.upload(pl.item_chptr, s);
+    d.item_chidx.upload(pl.item_chidx, s);
+    d.rank.alloc(std::max(ni, 1));
+    d.rank.zero(s);
+    d.nrows.alloc(std::max(ni, 1));
+    d.nrows.zero(s);
+    d.piv.alloc(size_t(std::max(ni, 1)) * maxrank);
+    IacaArgs a{};
+    a.mim.begin = fs.begin.p;
+    a.mim.end = fs.end.p;
+    a.mim.firstchild = fs.firstchild.p;
+    a.mim.nchildren = fs.nchildren.p;
+    a.mim.perm = fs.perm.p;
+    a.mim.center = dcenter.p;
+    a.mim.pts = fs.pts.p;
+    a.mim.nitems = ni;
+    a.mim.ffptr = dffptr.p;
+    a.mim.ffnodes = dffnodes.p;
+    a.mim.item_node = d.item_node.p;
+    a.mim.centroid = dcent.p;
+    a.mim.maxrank = maxrank;
+    a.K = c->K;
+    a.side = sd;
+    a.own_pts = ds.pts.p;
+    a.perm = ds.perm.p;
+    a.begin = ds.begin.p;
+    a.end = ds.end.p;
+    a.firstchild = ds.firstchild.p;
+    a.nchildren = ds.nchildren.p;
+    a.item_basis = d.item_basis.p;
+    a.item_chptr = d.item_chptr.p;
+    a.item_chidx = d.item_chidx.p;
+    a.rank = d.rank.p;
+    a.nrows = d.nrows.p;
+    a.piv = d.piv.p;
+    a.cpiv = nullptr;  // column pivots serve frozen-skeleton refills, which directional cores do not offer
+    a.maxrank = maxrank;
+    a.tol = sd == 0 ? o->tol_test : o->tol_trial;
+    a.status = status.p;
+    a.cursor = status.p + 4;
+    // Level by level, deepest first: the rows of a nested item are its children's actual
+    // ranks, so each level's X is allocated for min(maxrank, rows, far points) columns, then
+    // compacted to the ranks found before the next level runs.
+    d.h_rank.assign(ni, 0);
+    d.h_nrows.assign(ni, 0);
+    std::vector<int64_t> lvoff(std::max(ni, 1), 0), cpos(ni, -1);
+    std::vector<std::unique_ptr<DBuf<double2>>> levelX;
+    std::vector<std::vector<int32_t>> levelItems;
+    // scratch reused by every level (grown, never shrunk: no device-wide frees between levels)
+    DBuf<int64_t> dlvoff, dso, ddo;
+    DBuf<int32_t> nodes, dld, dr, dc;
+    DBuf<double2> chunk;
+    PinnedBuf<int32_t> hrank(2 * size_t(std::max(ni, 1)));
+    int64_t total = 0;
+    for (int lev = T.nlevels - 1; lev >= 0; --lev) {
+        std::vector<int32_t> items;
+        int mc = 0;
+        int64_t bound = 0;
+        for (int it : bylevel[lev]) {
+            if (farpts[it] == 0) continue;
+            int64_t m = 0;
+            if (pl.item_basis[it]) {
+                m = T.size(pl.item_node[it]);
+            } else {
+                for (int k = pl.item_chptr[it]; k < pl.item_chptr[it + 1]; ++k) m += d.h_rank[pl.item_chidx[k]];
+            }
+            const int64_t rb = std::min<int64_t>(std::min<int64_t>(maxrank, m), int64_t(farpts[it]));
+            lvoff[it] = bound;
+            bound += pad2(m * rb);
+            items.push_back(it);
+            mc = int(std::max<int64_t>(mc, m));
+        }
+        if (items.empty()) continue;
+        if (mc > nca::iaca_max_rows())
+            throw Failure(NCA_ERR_ARG, "a basis item has " + std::to_string(mc) +
+                                           " rows; the IACA kernel holds at most " +
+                                           std::to_string(nca::iaca_max_rows()) + " (reduce the leaf size)");
+        if (!chunk.p || size_t(bound) > chunk.n) chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
+        upload_reuse(dlvoff, lvoff, s);
+        upload_reuse(nodes, items, s);
+        status.zero(s);
+        a.X = chunk.p;
+        a.xoff = dlvoff.p;
+        a.items = nodes.p;
+        a.nitems = int(items.size());
+        launch_iaca(a, mc, s);
+        CK(cudaGetLastError());
+        const std::vector<int32_t> st = status.download(s);
+        if (st[0] == 1) {
+            set_singular(sd, st[1], st[2], st[3]);
+            throw Failure(NCA_ERR_SINGULAR, "SingularCrossMatrixError: the cross matrix of " +
+                                                std::string(sd == 0 ? "test" : "trial") + " item " +
+                                                std::to_string(st[1]) + " is singular - " + std::to_string(st[2]) +
+                                                " pivots were selected but only " + std::to_string(st[3]) +
+                                                " of them are linearly independent");
+        }
+        if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: an item exceeds the IACA kernel's row capacity");
+        if (st[0] == 3) throw Failure(NCA_ERR_CUDA, "internal: tree mimicry ran out of far points");
+        CK(cudaMemcpyAsync(hrank.p, d.rank.p, sizeof(int32_t) * ni, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hrank.p + ni, d.nrows.p, sizeof(int32_t) * ni, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        const int32_t *rk = hrank.p, *nr = hrank.p + ni;
+        // compact this level: exact m x r blocks, back to back
+        std::vector<int64_t> soff, doff;
+        std::vector<int32_t> sld, crows, ccols;
+        int64_t lt = 0;
+        for (int it : items) {
+            d.h_rank[it] = rk[it];
+            d.h_nrows[it] = nr[it];
+            cpos[it] = lt;
+            if (rk[it] > 0 && nr[it] > 0) {
+                soff.push_back(lvoff[it]);
+                sld.push_back(nr[it]);
+                crows.push_back(nr[it]);
+                ccols.push_back(rk[it]);
+                doff.push_back(lt);
+            }
+            lt += pad2(int64_t(nr[it]) * rk[it]);
+        }
+        levelX.emplace_back(new DBuf<double2>());
+        levelX.back()->alloc(size_t(std::max<int64_t>(lt, 1)));
+        if (!soff.empty()) {
+            upload_reuse(dso, soff, s);
+            upload_reuse(ddo, doff, s);
+            upload_reuse(dld, sld, s);
+            upload_reuse(dr, crows, s);
+            upload_reuse(dc, ccols, s);
+            launch_copy_blocks<double2>(chunk.p, dso.p, dld.p, dr.p, dc.p, ddo.p, int64_t(soff.size()),
+                                        levelX.back()->p, s);
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(s));
+        }
+        levelItems.push_back(items);
+        for (int it : items) cpos[it] += total;
+        total += lt;
+        timer.mark(side + "level " + std::to_string(lev) + " (" + std::to_string(items.size()) +
+                   " items, up to " + std::to_string(mc) + " rows) compressed and compacted");
+    }
+    // one X for the side: the compacted levels back to back
+    d.h_xoff.assign(ni + 1, 0);
+    for (int it = 0; it < ni; ++it) d.h_xoff[it] = cpos[it] >= 0 ? cpos[it] : 0;
+    d.h_xoff[ni] = total;
+    d.X.alloc(size_t(std::max<int64_t>(total, 1)));
+    {
+        int64_t off = 0;
+        for (size_t l = 0; l < levelX.size(); ++l) {
+            int64_t lt = 0;
+            for (int it : levelItems[l]) lt += pad2(int64_t(d.h_nrows[it]) * d.h_rank[it]);
+            if (lt)
+                CK(cudaMemcpyAsync(d.X.p + off, levelX[l]->p, sizeof(double2) * lt, cudaMemcpyDeviceToDevice,
+                                   s));
+            off += lt;
+        }
+        CK(cudaStreamSynchronize(s));
+        levelX.clear();
+    }
+}
+
+void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_build_opts *o, const nca::Wideband &wb,
+                    const SavedCore *sv = nullptr) {
     const int maxrank = c->maxrank;
     PhaseTimer timer;
     auto h0 = std::chrono::steady_clock::now();
@@ -1269,198 +1503,34 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         const cudaStream_t s = ss[sd];
         DirItems &d = D->side[sd];
         const std::string side = sd == 0 ? "test: " : "trial: ";
-        d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
-                                  sd == 0 ? P.farnodes : P.tfarnodes, wb);
+        if (sv)
+            d.plan = sv->side[sd].plan;
+        else
+            d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
+                                      sd == 0 ? P.farnodes : P.tfarnodes, wb);
         timer.mark(side + "directional plan (" + std::to_string(d.plan.item_node.size()) + " items)");
         const nca::DirSide &pl = d.plan;
-        const nca::Tree &T = c->tree[sd], &Ft = c->tree[1 - sd];
-        DevSide &ds = c->side[sd];
-        const DevSide &fs = c->side[1 - sd];
+        const nca::Tree &T = c->tree[sd];
         const int ni = int(pl.item_node.size());
         d.nitems = ni;
-        // the items' directional far fields (dirfarfield), in the reference's order, and the far
-        // points each can offer (capped at maxrank)
-        std::vector<int64_t> ffptr;
-        std::vector<int32_t> ffnodes;
-        parallel_csr(
-            ni, [&](int it, std::vector<int32_t> &ff) { nca::item_farfield(T, pl, it, ff); }, ffptr, ffnodes);
-        std::vector<int32_t> farpts(ni, 0);
-        for (int it = 0; it < ni; ++it) {
-            int64_t n = 0;
-            for (int64_t q = ffptr[it]; q < ffptr[it + 1] && n < maxrank; ++q) n += Ft.size(ffnodes[q]);
-            farpts[it] = int32_t(std::min<int64_t>(n, maxrank));
-        }
-        const std::vector<double> centroid = cluster_centroids(T, pts[sd]);
-        DBuf<int64_t> dffptr;
-        DBuf<int32_t> dffnodes;
-        DBuf<double> dcent, dcenter;
-        dffptr.upload(ffptr, s);
-        dffnodes.upload(ffnodes, s);
-        dcent.upload(centroid, s);
-        dcenter.upload(Ft.center, s);
-        timer.mark(side + "item far fields and centroids uploaded");
-        // the side's items, level by level
-        DBuf<int32_t> status;
-        status.alloc(5);  // [flag, item, a, b], item cursor
         bylevel[sd].assign(T.nlevels, {});
         for (int it = 0; it < ni; ++it) bylevel[sd][T.level[pl.item_node[it]]].push_back(it);
-        d.item_node.upload(pl.item_node, s);
-        d.item_basis.upload(pl.item_basis, s);
-        d.item_chptr.upload(pl.item_chptr, s);
-        d.item_chidx.upload(pl.item_chidx, s);
-        d.rank.alloc(std::max(ni, 1));
-        d.rank.zero(s);
-        d.nrows.alloc(std::max(ni, 1));
-        d.nrows.zero(s);
-        d.piv.alloc(size_t(std::max(ni, 1)) * maxrank);
-        IacaArgs a{};
-        a.mim.begin = fs.begin.p;
-        a.mim.end = fs.end.p;
-        a.mim.firstchild = fs.firstchild.p;
-        a.mim.nchildren = fs.nchildren.p;
-        a.mim.perm = fs.perm.p;
-        a.mim.center = dcenter.p;
-        a.mim.pts = fs.pts.p;
-        a.mim.nitems = ni;
-        a.mim.ffptr = dffptr.p;
-        a.mim.ffnodes = dffnodes.p;
-        a.mim.item_node = d.item_node.p;
-        a.mim.centroid = dcent.p;
-        a.mim.maxrank = maxrank;
-        a.K = c->K;
-        a.side = sd;
-        a.own_pts = ds.pts.p;
-        a.perm = ds.perm.p;
-        a.begin = ds.begin.p;
-        a.end = ds.end.p;
-        a.firstchild = ds.firstchild.p;
-        a.nchildren = ds.nchildren.p;
-        a.item_basis = d.item_basis.p;
-        a.item_chptr = d.item_chptr.p;
-        a.item_chidx = d.item_chidx.p;
-        a.rank = d.rank.p;
-        a.nrows = d.nrows.p;
-        a.piv = d.piv.p;
-        a.cpiv = nullptr;  // column pivots serve frozen-skeleton refills, which directional cores do not offer
-        a.maxrank = maxrank;
-        a.tol = sd == 0 ? o->tol_test : o->tol_trial;
-        a.status = status.p;
-        a.cursor = status.p + 4;
-        // Level by level, deepest first: the rows of a nested item are its children's actual
-        // ranks, so each level's X is allocated for min(maxrank, rows, far points) columns, then
-        // compacted to the ranks found before the next level runs.
-        d.h_rank.assign(ni, 0);
-        d.h_nrows.assign(ni, 0);
-        std::vector<int64_t> lvoff(std::max(ni, 1), 0), cpos(ni, -1);
-        std::vector<std::unique_ptr<DBuf<double2>>> levelX;
-        std::vector<std::vector<int32_t>> levelItems;
-        // scratch reused by every level (grown, never shrunk: no device-wide frees between levels)
-        DBuf<int64_t> dlvoff, dso, ddo;
-        DBuf<int32_t> nodes, dld, dr, dc;
-        DBuf<double2> chunk;
-        PinnedBuf<int32_t> hrank(2 * size_t(std::max(ni, 1)));
-        int64_t total = 0;
-        for (int lev = T.nlevels - 1; lev >= 0; --lev) {
-            std::vector<int32_t> items;
-            int mc = 0;
-            int64_t bound = 0;
-            for (int it : bylevel[sd][lev]) {
-                if (farpts[it] == 0) continue;
-                int64_t m = 0;
-                if (pl.item_basis[it]) {
-                    m = T.size(pl.item_node[it]);
-                } else {
-                    for (int k = pl.item_chptr[it]; k < pl.item_chptr[it + 1]; ++k) m += d.h_rank[pl.item_chidx[k]];
-                }
-                const int64_t rb = std::min<int64_t>(std::min<int64_t>(maxrank, m), int64_t(farpts[it]));
-                lvoff[it] = bound;
-                bound += pad2(m * rb);
-                items.push_back(it);
-                mc = int(std::max<int64_t>(mc, m));
-            }
-            if (items.empty()) continue;
-            if (mc > nca::iaca_max_rows())
-                throw Failure(NCA_ERR_ARG, "a basis item has " + std::to_string(mc) +
-                                               " rows; the IACA kernel holds at most " +
-                                               std::to_string(nca::iaca_max_rows()) + " (reduce the leaf size)");
-            if (!chunk.p || size_t(bound) > chunk.n) chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
-            upload_reuse(dlvoff, lvoff, s);
-            upload_reuse(nodes, items, s);
-            status.zero(s);
-            a.X = chunk.p;
-            a.xoff = dlvoff.p;
-            a.items = nodes.p;
-            a.nitems = int(items.size());
-            launch_iaca(a, mc, s);
-            CK(cudaGetLastError());
-            const std::vector<int32_t> st = status.download(s);
-            if (st[0] == 1) {
-                set_singular(sd, st[1], st[2], st[3]);
-                throw Failure(NCA_ERR_SINGULAR, "SingularCrossMatrixError: the cross matrix of " +
-                                                    std::string(sd == 0 ? "test" : "trial") + " item " +
-                                                    std::to_string(st[1]) + " is singular - " + std::to_string(st[2]) +
-                                                    " pivots were selected but only " + std::to_string(st[3]) +
-                                                    " of them are linearly independent");
-            }
-            if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: an item exceeds the IACA kernel's row capacity");
-            if (st[0] == 3) throw Failure(NCA_ERR_CUDA, "internal: tree mimicry ran out of far points");
-            CK(cudaMemcpyAsync(hrank.p, d.rank.p, sizeof(int32_t) * ni, cudaMemcpyDeviceToHost, s));
-            CK(cudaMemcpyAsync(hrank.p + ni, d.nrows.p, sizeof(int32_t) * ni, cudaMemcpyDeviceToHost, s));
-            CK(cudaStreamSynchronize(s));
-            const int32_t *rk = hrank.p, *nr = hrank.p + ni;
-            // compact this level: exact m x r blocks, back to back
-            std::vector<int64_t> soff, doff;
-            std::vector<int32_t> sld, crows, ccols;
-            int64_t lt = 0;
-            for (int it : items) {
-                d.h_rank[it] = rk[it];
-                d.h_nrows[it] = nr[it];
-                cpos[it] = lt;
-                if (rk[it] > 0 && nr[it] > 0) {
-                    soff.push_back(lvoff[it]);
-                    sld.push_back(nr[it]);
-                    crows.push_back(nr[it]);
-                    ccols.push_back(rk[it]);
-                    doff.push_back(lt);
-                }
-                lt += pad2(int64_t(nr[it]) * rk[it]);
-            }
-            levelX.emplace_back(new DBuf<double2>());
-            levelX.back()->alloc(size_t(std::max<int64_t>(lt, 1)));
-            if (!soff.empty()) {
-                upload_reuse(dso, soff, s);
-                upload_reuse(ddo, doff, s);
-                upload_reuse(dld, sld, s);
-                upload_reuse(dr, crows, s);
-                upload_reuse(dc, ccols, s);
-                launch_copy_blocks<double2>(chunk.p, dso.p, dld.p, dr.p, dc.p, ddo.p, int64_t(soff.size()),
-                                            levelX.back()->p, s);
-                CK(cudaGetLastError());
-                CK(cudaStreamSynchronize(s));
-            }
-            levelItems.push_back(items);
-            for (int it : items) cpos[it] += total;
-            total += lt;
-            timer.mark(side + "level " + std::to_string(lev) + " (" + std::to_string(items.size()) +
-                       " items, up to " + std::to_string(mc) + " rows) compressed and compacted");
-        }
-        // one X for the side: the compacted levels back to back
-        d.h_xoff.assign(ni + 1, 0);
-        for (int it = 0; it < ni; ++it) d.h_xoff[it] = cpos[it] >= 0 ? cpos[it] : 0;
-        d.h_xoff[ni] = total;
-        d.X.alloc(size_t(std::max<int64_t>(total, 1)));
-        {
-            int64_t off = 0;
-            for (size_t l = 0; l < levelX.size(); ++l) {
-                int64_t lt = 0;
-                for (int it : levelItems[l]) lt += pad2(int64_t(d.h_nrows[it]) * d.h_rank[it]);
-                if (lt)
-                    CK(cudaMemcpyAsync(d.X.p + off, levelX[l]->p, sizeof(double2) * lt, cudaMemcpyDeviceToDevice,
-                                       s));
-                off += lt;
-            }
-            CK(cudaStreamSynchronize(s));
-            levelX.clear();
+        if (sv) {
+            // a saved skeleton: the items' operators and pivots as the build left them
+            const SavedSide &v = sv->side[sd];
+            d.item_node.upload(pl.item_node, s);
+            d.item_basis.upload(pl.item_basis, s);
+            d.item_chptr.upload(pl.item_chptr, s);
+            d.item_chidx.upload(pl.item_chidx, s);
+            d.rank.upload(v.rank, s);
+            d.nrows.upload(v.nrows, s);
+            d.piv.upload(v.piv, s);
+            d.h_rank = v.rank;
+            d.h_nrows = v.nrows;
+            d.h_xoff = v.xoff;
+            d.X.upload(v.X, s);
+        } else {
+            compress_dir_side(c, d, sd, pts[sd], bylevel[sd], s, o, timer, side);
         }
         d.xoff.upload(d.h_xoff, s);
         d.h_cptr.assign(ni + 1, 0);
@@ -1743,11 +1813,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         CK(cudaStreamSynchronize(s));
     });
     CK(cudaStreamSynchronize(s));
-    // the per-item operators live on in the stage stores (directional cores have no node exports)
-    for (DirItems &d : D->side) {
-        d.X.release();
-        d.XT.release();
-    }
+    // the stage stores hold the products' copies of the operators; X stays for nca_core_save
+    for (DirItems &d : D->side) d.XT.release();
     if (c->f32) {
         auto down = [&](DBuf<double2> &src, DBuf<float2> &dst) {
             dst.alloc(src.n);
@@ -2937,6 +3004,258 @@ int entries_impl(const nca_kernel_desc *kernel, const double *testpoints, int64_
 
 }  // namespace
 
+// ---- serialised cores ---------------------------------------------------------------------
+// File layout (little-endian, native sizes): an 8-byte tag, the format number, the core's options
+// and kernel, the points, both trees, the partition, then per side the skeleton (SavedSide); every
+// array is its element count (int64) followed by its elements.
+constexpr char kCoreTag[8] = {'N', 'C', 'A', 'B', '2', '0', '0', 'C'};
+constexpr uint32_t kCoreFormat = 1;
+
+struct FileOut {
+    FILE *f = nullptr;
+    ~FileOut() {
+        if (f) std::fclose(f);
+    }
+    void raw(const void *p, size_t n) {
+        if (n && std::fwrite(p, 1, n, f) != n) throw Failure(NCA_ERR_ARG, "nca_core_save: write failed");
+    }
+    template <typename T>
+    void pod(const T &v) {
+        raw(&v, sizeof(T));
+    }
+    template <typename T>
+    void vec(const std::vector<T> &v) {
+        pod<int64_t>(int64_t(v.size()));
+        raw(v.data(), sizeof(T) * v.size());
+    }
+};
+
+struct FileIn {
+    FILE *f = nullptr;
+    int64_t left = 0;  // bytes not yet read: bounds every array count
+    ~FileIn() {
+        if (f) std::fclose(f);
+    }
+    void raw(void *p, size_t n) {
+        if (int64_t(n) > left || (n && std::fread(p, 1, n, f) != n))
+            throw Failure(NCA_ERR_ARG, "nca_core_load: the file is truncated or not a saved core");
+        left -= int64_t(n);
+    }
+    template <typename T>
+    T pod() {
+        T v{};
+        raw(&v, sizeof(T));
+        return v;
+    }
+    template <typename T>
+    void vec(std::vector<T> &v) {
+        const int64_t n = pod<int64_t>();
+        if (n < 0 || n > left / int64_t(sizeof(T)))
+            throw Failure(NCA_ERR_ARG, "nca_core_load: the file is truncated or not a saved core");
+        v.resize(size_t(n));
+        raw(v.data(), sizeof(T) * size_t(n));
+    }
+};
+
+template <typename IO, typename TreeT>
+void tree_io(IO &io, TreeT &T) {
+    io.vec(T.perm);
+    io.vec(T.iperm);
+    io.vec(T.begin);
+    io.vec(T.end);
+    io.vec(T.parent);
+    io.vec(T.firstchild);
+    io.vec(T.nchildren);
+    io.vec(T.level);
+    io.vec(T.center);
+    io.vec(T.radius);
+    io.vec(T.levelptr);
+}
+
+template <typename IO, typename PartT>
+void partition_io(IO &io, PartT &P) {
+    io.vec(P.nearptr);
+    io.vec(P.nearnodes);
+    io.vec(P.farptr);
+    io.vec(P.farnodes);
+    io.vec(P.tnearptr);
+    io.vec(P.tnearnodes);
+    io.vec(P.tfarptr);
+    io.vec(P.tfarnodes);
+}
+
+template <typename IO, typename PlanT>
+void plan_io(IO &io, PlanT &D) {
+    io.vec(D.farptr);
+    io.vec(D.farnodes);
+    io.vec(D.dirptr);
+    io.vec(D.dirs);
+    io.vec(D.dirvec);
+    io.vec(D.dirfarptr);
+    io.vec(D.chdirptr);
+    io.vec(D.chdirmap);
+    io.vec(D.invptr);
+    io.vec(D.invidx);
+    io.vec(D.item_node);
+    io.vec(D.item_basis);
+    io.vec(D.item_chptr);
+    io.vec(D.item_chidx);
+}
+
+template <typename IO, typename SideT>
+void saved_side_io(IO &io, SideT &v, bool dir) {
+    io.vec(v.rank);
+    io.vec(v.nrows);
+    io.vec(v.piv);
+    io.vec(v.cpiv);
+    io.vec(v.fpptr);
+    io.vec(v.fpidx);
+    io.vec(v.xoff);
+    io.vec(v.X);
+    if (dir) plan_io(io, v.plan);
+}
+
+// every array of a read tree / partition / skeleton has the size its counts imply
+void check_loaded(const nca::Tree &T, const char *what) {
+    const size_t n = size_t(T.nnodes);
+    const bool ok = T.nnodes > 0 && T.nlevels > 0 && T.perm.size() == size_t(T.npoints) &&
+                    T.iperm.size() == size_t(T.npoints) && T.begin.size() == n && T.end.size() == n &&
+                    T.parent.size() == n && T.firstchild.size() == n && T.nchildren.size() == n &&
+                    T.level.size() == n && T.center.size() == 3 * n && T.radius.size() == n &&
+                    T.levelptr.size() == size_t(T.nlevels) + 1;
+    if (!ok) throw Failure(NCA_ERR_ARG, std::string("nca_core_load: inconsistent ") + what);
+}
+
+void save_core(const nca_core *c, const char *path) {
+    if (c->batch) throw Failure(NCA_ERR_ARG, "nca_core_save: a batch is not saved (save its members)");
+    if (c->moved) throw Failure(NCA_ERR_ARG, "the core's stores were moved into a batch");
+    CK(cudaSetDevice(c->device));
+    cudaStream_t s = nullptr;
+    FileOut out;
+    out.f = std::fopen(path, "wb");
+    if (!out.f) throw Failure(NCA_ERR_ARG, std::string("nca_core_save: cannot open ") + path);
+    out.raw(kCoreTag, sizeof(kCoreTag));
+    out.pod<uint32_t>(kCoreFormat);
+    const bool dir = c->dir != nullptr;
+    out.pod<int32_t>(dir);
+    out.pod<int32_t>(c->f32);
+    out.pod<int32_t>(c->maxrank);
+    out.pod<int32_t>(c->K.kind);
+    out.pod<int32_t>(c->K.sign);
+    out.pod<double>(c->K.k);
+    out.pod<double>(c->K.rmin);
+    out.pod<int64_t>(c->K.ldmat);
+    out.pod<double>(c->wb.k);
+    out.pod<double>(c->wb.etalf);
+    out.pod<double>(c->wb.etahf);
+    out.pod<double>(c->wb.gamma);
+    for (int sd = 0; sd < 2; ++sd) {
+        out.pod<int64_t>(c->tree[sd].npoints);
+        out.pod<int32_t>(c->tree[sd].nnodes);
+        out.pod<int32_t>(c->tree[sd].nlevels);
+    }
+    for (int sd = 0; sd < 2; ++sd) out.vec(c->side[sd].pts.download(s));
+    out.vec(c->K.kind == NCA_KERNEL_MATRIX ? c->kmat.download(s) : std::vector<double2>());
+    for (int sd = 0; sd < 2; ++sd) tree_io(out, const_cast<nca::Tree &>(c->tree[sd]));
+    partition_io(out, const_cast<nca::Partition &>(c->part));
+    for (int sd = 0; sd < 2; ++sd) {
+        SavedSide v;
+        if (dir) {
+            const DirItems &d = c->dir->side[sd];
+            v.rank = d.h_rank;
+            v.nrows = d.h_nrows;
+            v.piv = d.piv.download(s);
+            v.xoff = d.h_xoff;
+            v.X = d.X.download(s);
+            v.plan = d.plan;
+        } else {
+            const DevSide &d = c->side[sd];
+            v.rank = d.h_rank;
+            v.nrows = d.h_nrows;
+            v.piv = d.h_piv;
+            v.cpiv = d.cpiv.download(s);
+            v.fpptr = d.h_fpptr;
+            v.fpidx = d.h_fpidx;
+            v.xoff = d.h_xoff;
+            v.X = d.X.download(s);
+        }
+        saved_side_io(out, v, dir);
+    }
+    if (std::fflush(out.f) != 0) throw Failure(NCA_ERR_ARG, "nca_core_save: write failed");
+}
+
+nca_core *load_core(const char *path, int device) {
+    FileIn in;
+    in.f = std::fopen(path, "rb");
+    if (!in.f) throw Failure(NCA_ERR_ARG, std::string("nca_core_load: cannot open ") + path);
+    std::fseek(in.f, 0, SEEK_END);
+    in.left = std::ftell(in.f);
+    std::fseek(in.f, 0, SEEK_SET);
+    char tag[8];
+    in.raw(tag, sizeof(tag));
+    if (std::memcmp(tag, kCoreTag, sizeof(tag)) != 0) throw Failure(NCA_ERR_ARG, "nca_core_load: not a saved core");
+    if (in.pod<uint32_t>() != kCoreFormat) throw Failure(NCA_ERR_ARG, "nca_core_load: unknown format version");
+    auto c = std::make_unique<nca_core>();
+    const bool dir = in.pod<int32_t>() != 0;
+    c->device = device;
+    c->f32 = in.pod<int32_t>() != 0;
+    c->maxrank = in.pod<int32_t>();
+    nca_kernel_desc kd{};
+    kd.kind = in.pod<int32_t>();
+    kd.sign = in.pod<int32_t>();
+    kd.k = in.pod<double>();
+    kd.rmin = in.pod<double>();
+    kd.ldmatrix = in.pod<int64_t>();
+    c->wb.k = in.pod<double>();
+    c->wb.etalf = in.pod<double>();
+    c->wb.etahf = in.pod<double>();
+    c->wb.gamma = in.pod<double>();
+    for (int sd = 0; sd < 2; ++sd) {
+        c->tree[sd].npoints = in.pod<int64_t>();
+        c->tree[sd].nnodes = in.pod<int32_t>();
+        c->tree[sd].nlevels = in.pod<int32_t>();
+    }
+    if (c->maxrank < 1 || c->maxrank > 128) throw Failure(NCA_ERR_ARG, "nca_core_load: bad maxrank");
+    std::vector<double> pts[2];
+    for (int sd = 0; sd < 2; ++sd) {
+        in.vec(pts[sd]);
+        if (pts[sd].size() != 3 * size_t(c->tree[sd].npoints))
+            throw Failure(NCA_ERR_ARG, "nca_core_load: point count differs from the tree's");
+    }
+    std::vector<double2> mat;
+    in.vec(mat);
+    kd.matrix = reinterpret_cast<const double *>(mat.data());
+    for (int sd = 0; sd < 2; ++sd) {
+        tree_io(in, c->tree[sd]);
+        check_loaded(c->tree[sd], sd == 0 ? "test tree" : "trial tree");
+    }
+    partition_io(in, c->part);
+    if (c->part.nearptr.size() != size_t(c->tree[0].nnodes) + 1 ||
+        c->part.tfarptr.size() != size_t(c->tree[1].nnodes) + 1)
+        throw Failure(NCA_ERR_ARG, "nca_core_load: inconsistent partition");
+    SavedCore sv;
+    for (int sd = 0; sd < 2; ++sd) {
+        saved_side_io(in, sv.side[sd], dir);
+        const SavedSide &v = sv.side[sd];
+        const size_t n = dir ? v.plan.item_node.size() : size_t(c->tree[sd].nnodes);
+        if (v.rank.size() != n || v.nrows.size() != n || v.piv.size() != n * size_t(c->maxrank) ||
+            v.xoff.size() != n + 1 || v.xoff.back() != int64_t(v.X.size()))
+            throw Failure(NCA_ERR_ARG, "nca_core_load: inconsistent skeleton");
+    }
+    CK(cudaSetDevice(device));
+    set_kernel_params(c.get(), &kd, c->tree[0].npoints, c->tree[1].npoints, nullptr);
+    nca_build_opts o{};
+    o.maxrank = c->maxrank;
+    o.device = device;
+    o.store_f32 = c->f32;
+    o.compressor = dir ? NCA_COMPRESSOR_BOTTOMUP_IACA : NCA_COMPRESSOR_BATCHED_ACA;
+    if (dir)
+        build_dir_core(c.get(), pts[0].data(), pts[1].data(), &o, c->wb, &sv);
+    else
+        build_core(c.get(), pts[0].data(), c->tree[0].npoints, pts[1].data(), c->tree[1].npoints, &o, &sv);
+    return c.release();
+}
+
 extern "C" {
 
 int32_t nca_version(void) { return 2; }
@@ -3138,8 +3457,10 @@ int32_t nca_core_build(const double *testpoints, int64_t ntest, const double *tr
         c->tree[1] = trialtree->t;
         c->part = part->p;
         set_kernel_params(c.get(), kernel, ntest, ntrial, nullptr);
-        if (part->wideband)
+        if (part->wideband) {
+            c->wb = part->w;
             build_dir_core(c.get(), testpoints, trialpoints, opts, part->w);
+        }
         else
             build_core(c.get(), testpoints, ntest, trialpoints, ntrial, opts);
         *out = c.release();
@@ -3151,6 +3472,22 @@ void nca_core_destroy(nca_core *core) {
     if (!core) return;
     cudaSetDevice(core->device);
     delete core;
+}
+
+int32_t nca_core_save(const nca_core *core, const char *path) {
+    if (!core || !path) return fail(NCA_ERR_ARG, "null argument");
+    return guarded([&] {
+        save_core(core, path);
+        return int(NCA_OK);
+    });
+}
+
+int32_t nca_core_load(const char *path, int32_t device, nca_core **out) {
+    if (!path || !out) return fail(NCA_ERR_ARG, "null argument");
+    return guarded([&] {
+        *out = load_core(path, device);
+        return int(NCA_OK);
+    });
 }
 
 int32_t nca_core_set_wavenumber(nca_core *core, double k) {

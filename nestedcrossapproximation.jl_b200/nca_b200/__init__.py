@@ -13,7 +13,7 @@ from .admissibility import DirectionalData, FarData, IsNearWideband, directional
 from .compressors import ACA, IACA, BatchedBottomUp, BottomUp, FNormEstimator, FNormExtrapolator, FullPivoting, \
     MaximumValue, TreeMimicryPivoting, _clustersize, _selectfarpivots
 from .kernels import HelmholtzKernel, LaplaceKernel, MatrixKernel
-from .nca import (BatchCore, H2Workspace, dHdk, rrule_mul, PetrovGalerkinNCA, PetrovGalerkinNCACore, adjoint, batch, core, farmatrix, mul, nearmatrix,
+from .nca import (BatchCore, H2Workspace, LoadedCore, load_core, dHdk, rrule_mul, PetrovGalerkinNCA, PetrovGalerkinNCACore, adjoint, batch, core, farmatrix, mul, nearmatrix,
                   storage, transpose, withworkspace)
 from .trees import BlockTree, KMeansTree, KMeansTreeBuilder, testtree, trialtree
 from .utils import collect_assigned, plan_from_pivots, ptrfromcounts

@@ -90,6 +90,8 @@ SIGNATURES = {
     "nca_select_farpivots": (I32, [P, P, P, P, I32, P, I32, I32, P, P]),
     "nca_core_build": (I32, [P, I64, P, I64, P, P, P, P, P, P]),
     "nca_core_destroy": (None, [P]),
+    "nca_core_save": (I32, [P, C.c_char_p]),
+    "nca_core_load": (I32, [C.c_char_p, I32, P]),
     "nca_core_batch": (I32, [P, I32, I32, P]),
     "nca_core_get_info": (I32, [P, P]),
     "nca_core_export_pivots": (I32, [P, I32, P, P, P, P]),

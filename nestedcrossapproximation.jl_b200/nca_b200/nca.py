@@ -8,6 +8,7 @@ vectors or blocks of right-hand sides, host (numpy) or device (torch.cuda) array
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 
 import numpy as np
@@ -113,6 +114,13 @@ class PetrovGalerkinNCACore:
     @property
     def shape(self):
         return self.dim
+
+    # ---- serialised cores ----
+    def save(self, path):
+        """Write the core's inputs and skeleton (points, trees, partition, kernel, pivots and
+        interpolation operators) to `path`; `load_core(path)` rebuilds the rest (the reference dumps
+        a built matrix's stores and plans, scripts/create_test_matrix.jl:50-68)."""
+        check(lib().nca_core_save(self._h, os.fsencode(path)))
 
     # ---- frozen-skeleton refills and derivatives ----
     @property
@@ -593,6 +601,46 @@ class BatchCore(PetrovGalerkinNCACore):
         raise ArgumentError("export the member cores of a batch")
 
     pivots = farpivots = interpolation = _member_export
+
+
+class _TreeSizes:
+    def __init__(self, nnodes):
+        self.nnodes = nnodes
+
+
+class _LoadedTree:
+    def __init__(self, info):
+        self.test, self.trial = _TreeSizes(info.nnodes_test), _TreeSizes(info.nnodes_trial)
+
+
+class LoadedCore(PetrovGalerkinNCACore):
+    """A core read back by load_core: products, workspaces and exports as the saved core's (its
+    products equal the saved core's bit for bit); the Python-side trees and points stay with the
+    file."""
+
+    def __init__(self, path, device: int = 0):
+        h = C.c_void_p()
+        check(lib().nca_core_load(os.fsencode(path), int(device), C.byref(h)))
+        self._h = h
+        info = CoreInfo()
+        check(lib().nca_core_get_info(h, C.byref(info)))
+        self.info = info
+        self.dim = (int(info.ntest), int(info.ntrial))
+        self.device = int(device)
+        self.tree = _LoadedTree(info)
+        self.operator = None
+        self._cache = {}
+        # a complex-FP32 product needs the FP32 copies, which the saved core either had or not
+        self.f32 = True
+        self.maxrank = 128
+
+    def set_wavenumber(self, k: float):
+        raise ArgumentError("a loaded core keeps no operator object: refill the core it was saved from")
+
+
+def load_core(path, device: int = 0) -> LoadedCore:
+    """Read a core written by PetrovGalerkinNCACore.save onto `device`."""
+    return LoadedCore(path, device)
 
 
 def batch(cores, move: bool = False) -> BatchCore:

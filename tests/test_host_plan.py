@@ -169,3 +169,17 @@ def test_batchedbottomup_constructor():
     for kwargs in ({}, {"pivotselector": sel}, {"compressor": aca}):
         with pytest.raises(TypeError):
             N.BatchedBottomUp(**kwargs)
+
+
+def test_load_refuses_files_that_are_not_saved_cores(tmp_path):
+    """nca_core_load checks the tag, the format number and every array count against the file
+    before any device work: a foreign or truncated file is an ArgumentError."""
+    p = tmp_path / "junk.nca"
+    p.write_bytes(b"not a core at all" * 10)
+    with pytest.raises(N.ArgumentError, match="not a saved core"):
+        N.load_core(str(p))
+    p.write_bytes(b"NCAB200C" + (1).to_bytes(4, "little") + b"\x00" * 6)
+    with pytest.raises(N.ArgumentError, match="truncated"):
+        N.load_core(str(p))
+    with pytest.raises(N.ArgumentError, match="cannot open"):
+        N.load_core(str(tmp_path / "missing.nca"))
