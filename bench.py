@@ -493,8 +493,9 @@ def perturbed_sphere(n, seed):
 
 
 def run_gradients(args):
-    """131,072 points on a perturbed sphere, Helmholtz k = 20, tol 1e-5 (standard admissibility,
-    maxrank 50), skeleton frozen after the build; J = ||H(k) x - b||^2 with 4 right-hand sides.
+    """131,072 points on a perturbed sphere, Helmholtz k = 20, tol 1e-5, isnearwideband(20) (kd is
+    about 44 at the root, so the upper levels are high frequency) with BottomUp(IACA) per (cluster,
+    direction), maxrank 50, skeleton frozen after the build; J = ||H(k) x - b||^2 with 4 right-hand sides.
     One step = one gradient: y = H x, x_bar = H^H (2 (y - b)), k_bar = Re(y_bar^H dH/dk x)
     (forward, adjoint and tangent products). The d/dk stores are prepared once per skeleton and
     timed separately. k_bar is checked against central differences (h = 1e-6 k) of frozen refills."""
@@ -506,12 +507,13 @@ def run_gradients(args):
     cuda_ready(N, local)
     n, b, k = 131072, 4, 20.0
     pts = perturbed_sphere(n, 4242)
-    tree = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=64))
-    aca = N.ACA(N.FullPivoting(), N.FullPivoting(), N.FNormEstimator(1e-5))
-    comp = N.BatchedBottomUp(pivotselector=N.TreeMimicryPivoting(pts, pts, tree), compressor=aca)
     t0 = time.perf_counter()
+    tree = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=64))
+    conv = N.FNormExtrapolator(1e-5)
+    tc = N.BottomUp(factorization=N.IACA(N.MaximumValue(), N.TreeMimicryPivoting(pts, pts, tree), conv))
+    sc = N.BottomUp(factorization=N.IACA(N.TreeMimicryPivoting(pts, pts, tree), N.MaximumValue(), conv))
     core = N.PetrovGalerkinNCACore(N.HelmholtzKernel(k, rmin=1e-12), pts, pts, N.BlockTree(tree, tree),
-                                   testcompressor=comp, trialcompressor=comp, device=local)
+                                   isnear=N.isnearwideband(k), testcompressor=tc, trialcompressor=sc, device=local)
     build_wall = time.perf_counter() - t0
     info = info_dict(core)
     ws = N.H2Workspace(core, max_nrhs=b)
@@ -574,7 +576,8 @@ def run_gradients(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * el, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "complex-f64", "data": "synthetic",
             "config": {"workload": "gradients-perturbed-sphere-131072-k20-tol1e-5-4rhs", "npoints": n, "nrhs": b,
-                       "k": k, "admissibility": "standard isnear (eta 1), maxrank 50",
+                       "k": k, "admissibility": "isnearwideband(k; eta_lf=1, eta_hf=5, gamma=1), maxrank 50",
+                       "compressor": "BottomUp(IACA(MaximumValue, TreeMimicryPivoting, FNormExtrapolator(1e-5)))",
                        "step": "one gradient: H x, H^H (2 (Hx - b)), dH/dk x",
                        "l2": "inputs larger than L2", "build_s": build_wall, "prepare_dk_s": prep,
                        "stored_gb": E * store_entries(info) / 1e9, "relerr_vs_dense_rows": err},

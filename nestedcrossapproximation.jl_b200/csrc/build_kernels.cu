@@ -416,16 +416,20 @@ __global__ void __launch_bounds__(NT) k_level_values(ValueArgs a, const int32_t 
     int32_t *ipiv = tauid + rcap;
     __shared__ int s_m, s_flag;
     const int tid = threadIdx.x;
-    const int node = nodes[blockIdx.x];
+    const int node = nodes[blockIdx.x];  // the node, or the directional item
     const int r = a.rank[node];
     if (r <= 0) return;
-    const bool leaf = a.nchildren[node] == 0;
+    const bool items = a.item_node != nullptr;
+    const int cl = items ? a.item_node[node] : node;
+    const bool leaf = items ? a.item_basis[node] != 0 : a.nchildren[node] == 0;
+    const int nch = leaf ? 0 : items ? a.item_chptr[node + 1] - a.item_chptr[node] : a.nchildren[node];
+    auto child = [&](int c) { return items ? a.item_chidx[a.item_chptr[node] + c] : a.firstchild[node] + c; };
     if (tid == 0) {
         int m = 0;
         if (leaf) {
-            m = a.end[node] - a.begin[node];
+            m = a.end[cl] - a.begin[cl];
         } else {
-            for (int c = 0; c < a.nchildren[node]; ++c) m += a.rank[a.firstchild[node] + c];
+            for (int c = 0; c < nch; ++c) m += a.rank[child(c)];
         }
         s_m = m;
     }
@@ -440,11 +444,11 @@ __global__ void __launch_bounds__(NT) k_level_values(ValueArgs a, const int32_t 
         return;
     }
     if (leaf) {
-        for (int i = tid; i < m; i += NT) rowid[i] = a.perm[a.begin[node] + i];
+        for (int i = tid; i < m; i += NT) rowid[i] = a.perm[a.begin[cl] + i];
     } else {
         int off = 0;
-        for (int c = 0; c < a.nchildren[node]; ++c) {
-            const int ch = a.firstchild[node] + c;
+        for (int c = 0; c < nch; ++c) {
+            const int ch = child(c);
             const int kc = a.rank[ch];
             for (int k = tid; k < kc; k += NT) rowid[off + k] = a.piv[int64_t(ch) * a.maxrank + k];
             off += kc;

@@ -40,6 +40,9 @@ struct ValueArgs {
     int side, mode;
     const double *own_pts, *far_pts;
     const int32_t *perm, *begin, *end, *firstchild, *nchildren, *rank, *piv, *cpiv;
+    // directional items (null: one item per node): the item's cluster, whether its rows are the
+    // cluster's points, and otherwise its children's items (whose pivots form the rows)
+    const int32_t *item_node, *item_basis, *item_chptr, *item_chidx;
     int maxrank;
     const double2 *Xin;  // mode 1: X at the wavenumber of K
     double2 *Xout;

@@ -171,6 +171,7 @@ struct DirItems {
     std::vector<int32_t> h_rank, h_nrows;  // item pivots stay on the device
     std::vector<int64_t> h_xoff, h_cptr;
     DBuf<int32_t> item_node, item_basis, item_chptr, item_chidx, rank, nrows, piv;
+    DBuf<int32_t> cpiv;  // column pivots sigma of every item (maxrank per item): frozen-skeleton refills
     DBuf<int64_t> xoff;
     DBuf<double2> X, XT;
 };
@@ -185,7 +186,12 @@ struct GatherStage {
     DBuf<int64_t> out, moff, voff;
     DBuf<double2> M;
     DBuf<float2> M32;
+    DBuf<double2> dM;     // d/dk of the store (frozen skeleton), prepared on demand
     int64_t entries = 0;  // algorithmic entries of the store
+    // the copies that fill M from the side's operators (kept for refills at another wavenumber)
+    DBuf<int64_t> c_soff, c_doff;
+    DBuf<int32_t> c_ld, c_rows, c_cols;
+    int64_t ncopies = 0;
 };
 
 // Products of one orientation: mode N (test <- trial) or T (trial <- test; C conjugates it).
@@ -198,6 +204,10 @@ struct DirProduct {
 struct DirCore {
     DirItems side[2];
     DirProduct prod[2];
+    // coupling blocks S_e = K[tau_t, tau_s] per far pair (test order) and their transposition plan
+    DBuf<int32_t> cpair_it, cpair_is, ctr_rows, ctr_cols;
+    DBuf<int64_t> ccoff, ctr_in, ctr_off;
+    int64_t npairs = 0, ntr = 0;
 };
 
 struct nca_core {
@@ -645,7 +655,7 @@ void fill_bases(nca_core *c, int sd, int mode, const KernelParams &K, const Kern
     DBuf<int32_t> status;
     status.alloc(4);
     status.zero(s);
-    ValueArgs a;
+    ValueArgs a{};
     a.K = K;
     a.dK = dK;
     a.side = sd;
@@ -1198,15 +1208,15 @@ struct StageBuilder {
         G.M.alloc(size_t(store));
         G.entries = 0;
         for (size_t i = 0; i < crows.size(); ++i) G.entries += int64_t(crows[i]) * ccols[i];
+        G.ncopies = int64_t(crows.size());
         if (!crows.empty()) {
-            DBuf<int64_t> dso, ddo;
-            DBuf<int32_t> dld, dr, dc;
-            dso.upload(soff, s);
-            ddo.upload(doff, s);
-            dld.upload(sld, s);
-            dr.upload(crows, s);
-            dc.upload(ccols, s);
-            launch_copy_blocks<double2>(src, dso.p, dld.p, dr.p, dc.p, ddo.p, int64_t(crows.size()), G.M.p, s);
+            G.c_soff.upload(soff, s);
+            G.c_doff.upload(doff, s);
+            G.c_ld.upload(sld, s);
+            G.c_rows.upload(crows, s);
+            G.c_cols.upload(ccols, s);
+            launch_copy_blocks<double2>(src, G.c_soff.p, G.c_ld.p, G.c_rows.p, G.c_cols.p, G.c_doff.p, G.ncopies,
+                                        G.M.p, s);
             CK(cudaGetLastError());
             CK(cudaStreamSynchronize(s));
         }
@@ -1340,7 +1350,8 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     a.rank = d.rank.p;
     a.nrows = d.nrows.p;
     a.piv = d.piv.p;
-    a.cpiv = nullptr;  // column pivots serve frozen-skeleton refills, which directional cores do not offer
+    d.cpiv.alloc(size_t(std::max(ni, 1)) * maxrank);
+    a.cpiv = d.cpiv.p;
     a.maxrank = maxrank;
     a.tol = sd == 0 ? o->tol_test : o->tol_trial;
     a.status = status.p;
@@ -1525,6 +1536,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             d.rank.upload(v.rank, s);
             d.nrows.upload(v.nrows, s);
             d.piv.upload(v.piv, s);
+            d.cpiv.upload(v.cpiv, s);
             d.h_rank = v.rank;
             d.h_nrows = v.nrows;
             d.h_xoff = v.xoff;
@@ -1558,8 +1570,6 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     std::vector<int32_t> pair_it, pair_is, pair_of_pos;
     std::vector<int64_t> cfoff, ctoff;
     int64_t coupling_entries = 0;
-    DBuf<int32_t> dpt, dps, drows, dcols;
-    DBuf<int64_t> dcoff, din, dctoff;
     auto couplings = [&]() {
         // far pairs (test CSR grouped by test direction) and their items on both sides
         std::vector<int32_t> item_of_pos[2];
@@ -1616,21 +1626,22 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         CTs.M.alloc(size_t(ctoff.back()));
         CN.entries = CTs.entries = coupling_entries;
         {
-            dpt.upload(pair_it, s);
-            dps.upload(pair_is, s);
-            dcoff.upload(cfoff, s);
+            D->cpair_it.upload(pair_it, s);
+            D->cpair_is.upload(pair_is, s);
+            D->ccoff.upload(cfoff, s);
+            D->npairs = npairs;
             CouplingArgs a;
             a.K = c->K;
             a.test_pts = c->side[0].pts.p;
             a.trial_pts = c->side[1].pts.p;
-            a.pair_t = dpt.p;
-            a.pair_s = dps.p;
+            a.pair_t = D->cpair_it.p;
+            a.pair_s = D->cpair_is.p;
             a.rank_t = D->side[0].rank.p;
             a.rank_s = D->side[1].rank.p;
             a.piv_t = D->side[0].piv.p;
             a.piv_s = D->side[1].piv.p;
             a.maxrank = maxrank;
-            a.coff = dcoff.p;
+            a.coff = D->ccoff.p;
             a.npairs = npairs;
             a.C = CN.M.p;
             a.C32 = nullptr;
@@ -1638,11 +1649,12 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 k_couplings<<<launch_grid(npairs, 16), 256, 0, s>>>(a);
                 CK(cudaGetLastError());
             }
-            din.upload(tr_in, s);
-            drows.upload(tr_rows, s);
-            dcols.upload(tr_cols, s);
-            dctoff.upload(ctoff, s);
-            launch_transpose_blocks<double2>(CN.M.p, din.p, drows.p, dcols.p, dctoff.p, int64_t(ps.farnodes.size()),
+            D->ctr_in.upload(tr_in, s);
+            D->ctr_rows.upload(tr_rows, s);
+            D->ctr_cols.upload(tr_cols, s);
+            D->ctr_off.upload(ctoff, s);
+            D->ntr = int64_t(ps.farnodes.size());
+            launch_transpose_blocks<double2>(CN.M.p, D->ctr_in.p, D->ctr_rows.p, D->ctr_cols.p, D->ctr_off.p, D->ntr,
                                              CTs.M.p, s);
             CK(cudaGetLastError());
         }
@@ -2367,6 +2379,90 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
     return NCA_OK;
 }
 
+// Tangent product of a directional core, dy = alpha (dH/dk) x + beta y on the frozen skeleton
+// (forward mode, complex FP64): the four gather stages run on dual numbers. The arena holds two
+// halves of R = nin + cin + cout rows: [x; x^; y^] and [0; dx^; dy^]; every stage computes its
+// values in the first half and its derivative in the second as dM v + M dv (the second term reads
+// the second half, whose x rows are zero, so the near blocks and the leaf bases' x slices drop out
+// of it); the leaf stage writes dy = dL y^ + L dy^ (with dN x among dL y^).
+int enqueue_dir_tangent(nca_core *c, const double2 *xd, int64_t lx, double2 *yd, int64_t ly, int b, double2 alpha,
+                        double2 beta, double2 *arena, int32_t *error, cudaStream_t s, ProductLaunches &count) {
+    DirProduct &pr = c->dir->prod[0];
+    const int I = 1, O = 0;
+    const int vs = vector_stride(b);
+    const int cap = rows_capacity(std::min(b, 16));
+    for (const GatherStage *G : {&pr.up, &pr.couple, &pr.down, &pr.leaves})
+        for (int r : G->group_maxrows)
+            if (r > cap) return fail(NCA_ERR_ARG, "a leaf or basis block has more rows than one product CTA holds");
+    const int64_t R = pr.nin + pr.cin + pr.cout;
+    double2 *A = arena, *B = arena + R * vs;
+    k_gather<<<launch_grid(pr.nin * b / 256 + 1, 8), 256, 0, s>>>(xd, lx, c->side[I].perm.p, pr.nin, b, vs, A);
+    CK(cudaMemsetAsync(B, 0, sizeof(double2) * size_t(pr.nin) * vs, s));
+    ++count.total;
+    const double2 *N = c->N.p, *dN = c->dN.p;
+    for (int q0 = 0; q0 < b; q0 += 16) {
+        const int bc = std::min(16, b - q0);
+        auto group = [&](const GatherStage &G, size_t g, const double2 *M, const double2 *M2, double2 *src,
+                         double2 *dst, bool accumulate, bool scatter, double2 bt) {
+            const int cnt = G.group_ptr[g + 1] - G.group_ptr[g];
+            if (!cnt) return;
+            RowArgs<double2> a{};
+            a.stage = STAGE_GATHER;
+            a.M = M;
+            a.M2 = M2;
+            a.g_rows = G.rows.p;
+            a.g_out = G.out.p;
+            a.g_segptr = G.segptr.p;
+            a.g_moff = G.moff.p;
+            a.g_w = G.w.p;
+            a.g_voff = G.voff.p;
+            a.src = src;
+            a.dst = dst;
+            a.accumulate = accumulate;
+            if (scatter) {
+                a.y = yd;
+                a.ldy = ly;
+                a.perm = c->side[O].perm.p;
+                a.alpha = alpha;
+                a.beta = bt;
+                a.usebeta = bt.x != 0.0 || bt.y != 0.0;
+            }
+            a.b = b;
+            a.bc = bc;
+            a.q0 = q0;
+            a.vs = vs;
+            a.conj = false;
+            a.maxrows = G.group_maxrows[g];
+            a.error = error;
+            if (G.group_work[g] < 8192.0 && gather_tiny_fits(a.maxrows, bc))
+                launch_gather_tiny<double2, double2>(a, G.outputs.p + G.group_ptr[g], cnt, s);
+            else if (a.maxrows <= 64 && G.group_work[g] < 8192.0)
+                launch_gather_small<double2, double2>(a, G.outputs.p + G.group_ptr[g], cnt, s);
+            else
+                launch_gather_rows<double2, double2>(a, G.outputs.p + G.group_ptr[g], cnt, s);
+            ++count.total;
+        };
+        // value, derivative of the store, store times derivative: level by level where levels depend
+        auto dual = [&](const GatherStage &G, bool accumulate) {
+            for (size_t g = 0; g + 1 < G.group_ptr.size(); ++g) {
+                group(G, g, G.M.p, N, A, A, accumulate, false, beta);
+                group(G, g, G.dM.p, dN, A, B, accumulate, false, beta);
+                group(G, g, G.M.p, N, B, B, true, false, beta);
+            }
+        };
+        dual(pr.up, false);
+        dual(pr.couple, false);
+        dual(pr.down, true);
+        const double2 one = make_double2(1.0, 0.0);
+        for (size_t g = 0; g + 1 < pr.leaves.group_ptr.size(); ++g) {
+            group(pr.leaves, g, pr.leaves.dM.p, dN, A, nullptr, false, true, beta);
+            group(pr.leaves, g, pr.leaves.M.p, N, B, nullptr, false, true, one);
+        }
+    }
+    CK(cudaGetLastError());
+    return NCA_OK;
+}
+
 // Argument checks shared by the product entry points.
 int check_product_args(nca_core *c, int mode, int precision, int64_t ldx, int64_t ldy, int64_t nrhs) {
     if (mode < 0 || mode > 2) return fail(NCA_ERR_ARG, "mode must be 0 (N), 1 (T) or 2 (C)");
@@ -2395,7 +2491,6 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     if (int st = check_product_args(c, mode, precision, ldx, ldy, nrhs)) return st;
     if (tangent && (mode != 0 || precision != NCA_PREC_F64))
         return fail(NCA_ERR_ARG, "the d/dk product is forward mode and complex FP64");
-    if (tangent && c->dir) return fail(NCA_ERR_ARG, "d/dk products are not available for directional cores");
     if (tangent && !c->has_dk) return fail(NCA_ERR_ARG, "call nca_core_prepare_dk before the d/dk product");
     const int in = mode == 0 ? 1 : 0, out = 1 - in;
     const int64_t nin = c->side[in].npts, nout = c->side[out].npts;
@@ -2434,7 +2529,7 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     }
     if (c->dir) {
         const DirProduct &pr = c->dir->prod[mode == 0 ? 0 : 1];
-        const size_t need = size_t(pr.nin + pr.cin + pr.cout) * vector_slots(b);
+        const size_t need = size_t(pr.nin + pr.cin + pr.cout) * vector_slots(b) * (tangent ? 2 : 1);
         if (ws->arena.n < need) {
             drop_graphs(ws);
             ws->arena.alloc(need);
@@ -2461,7 +2556,10 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
                 if (k == key) capture = true;
     }
     auto enqueue = [&]() -> int {
-        if (c->dir) {
+        if (c->dir && tangent) {
+            if (int st = enqueue_dir_tangent(c, xd, lx, yd, ly, b, alpha, beta, ws->arena.p, ws->error.p, s, count))
+                return st;
+        } else if (c->dir) {
             ws->dir_stage.clear();
             DirTimer timer{&ws->dir_ev, &ws->dir_stage};
             if (int st = enqueue_dir_product(c, mode, precision, xd, lx, yd, ly, b, alpha, beta, ws->arena.p,
@@ -2535,7 +2633,7 @@ int apply_impl(nca_workspace *ws, int mode, int precision, const void *x, int64_
     CK(cudaEventElapsedTime(&ms, ws->e0, ws->e1));
     ws->last_seconds = ms * 1e-3;
     ws->last_launches = count.total;
-    if (ws->profiling && c->dir) {
+    if (ws->profiling && c->dir && !tangent) {
         // directional: the stages' event pairs summed per stage (no near-field stage of its own)
         for (int k = 0; k < kStages; ++k) {
             ws->stage_seconds[k] = 0.0;
@@ -3004,6 +3102,182 @@ int entries_impl(const nca_kernel_desc *kernel, const double *testpoints, int64_
 
 }  // namespace
 
+// ---- directional cores on a frozen skeleton: refills and d/dk stores -------------------------
+// X of every item of one side at kernel K (mode 0: K[rows, sigma] K[tau, sigma]^-1) or its
+// wavenumber derivative (mode 1, from Xin = X at K), at the build's offsets.
+void fill_dir_bases(nca_core *c, int sd, int mode, const KernelParams &K, const KernelParams &dK, const double2 *Xin,
+                    double2 *Xout, cudaStream_t s) {
+    DirItems &d = c->dir->side[sd];
+    std::vector<int32_t> items;
+    int mcap = 1, rcap = 1;
+    for (int it = 0; it < d.nitems; ++it)
+        if (d.h_rank[it] > 0) {
+            items.push_back(it);
+            mcap = std::max(mcap, d.h_nrows[it]);
+            rcap = std::max(rcap, d.h_rank[it]);
+        }
+    if (items.empty()) return;
+    const size_t sm = values_smem_bytes(mcap, rcap, mode);
+    if (sm > size_t(kMaxSmem))
+        throw Failure(NCA_ERR_ARG, "a cross block of the frozen skeleton does not fit in shared memory");
+    CK(cudaFuncSetAttribute(k_level_values, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    DBuf<int32_t> status, ditems;
+    status.alloc(4);
+    status.zero(s);
+    ditems.upload(items, s);
+    const DevSide &ds = c->side[sd];
+    ValueArgs a{};
+    a.K = K;
+    a.dK = dK;
+    a.side = sd;
+    a.mode = mode;
+    a.own_pts = ds.pts.p;
+    a.far_pts = c->side[1 - sd].pts.p;
+    a.perm = ds.perm.p;
+    a.begin = ds.begin.p;
+    a.end = ds.end.p;
+    a.firstchild = ds.firstchild.p;
+    a.nchildren = ds.nchildren.p;
+    a.rank = d.rank.p;
+    a.piv = d.piv.p;
+    a.cpiv = d.cpiv.p;
+    a.item_node = d.item_node.p;
+    a.item_basis = d.item_basis.p;
+    a.item_chptr = d.item_chptr.p;
+    a.item_chidx = d.item_chidx.p;
+    a.maxrank = c->maxrank;
+    a.Xin = Xin;
+    a.Xout = Xout;
+    a.xoff = d.xoff.p;
+    a.status = status.p;
+    k_level_values<<<int(items.size()), 256, sm, s>>>(a, ditems.p, mcap, rcap);
+    CK(cudaGetLastError());
+    const std::vector<int32_t> st = status.download(s);
+    if (st[0] == 1) {
+        set_singular(sd, st[1], st[2], st[3]);
+        throw Failure(NCA_ERR_SINGULAR, "SingularCrossMatrixError: the frozen cross matrix of " +
+                                            std::string(sd == 0 ? "test" : "trial") + " item " +
+                                            std::to_string(st[1]) + " is singular at this wavenumber");
+    }
+    if (st[0] == 2) throw Failure(NCA_ERR_CUDA, "internal: a frozen cross block exceeds its planned capacity");
+}
+
+// Every stage store of both orientations from the sides' operators X (and their transposes XT),
+// the couplings and the near field at K: the value stores (deriv = false) or the d/dk stores.
+void fill_dir_stores(nca_core *c, const KernelParams &K, double2 *const X[2], double2 *const XT[2], bool deriv,
+                     cudaStream_t s) {
+    DirCore &D = *c->dir;
+    for (int m = 0; m < 2; ++m) {
+        const int I = m == 0 ? 1 : 0, O = 1 - I;
+        DirProduct &pr = D.prod[m];
+        auto copy = [&](GatherStage &G, const double2 *src) {
+            DBuf<double2> &dst = deriv ? G.dM : G.M;
+            if (deriv && dst.n != G.M.n) dst.alloc(G.M.n);
+            if (G.ncopies)
+                launch_copy_blocks<double2>(src, G.c_soff.p, G.c_ld.p, G.c_rows.p, G.c_cols.p, G.c_doff.p, G.ncopies,
+                                            dst.p, s);
+            CK(cudaGetLastError());
+        };
+        copy(pr.up, XT[I]);
+        copy(pr.down, X[O]);
+        copy(pr.leaves, X[O]);
+    }
+    GatherStage &CN = D.prod[0].couple, &CTs = D.prod[1].couple;
+    DBuf<double2> &C = deriv ? CN.dM : CN.M, &CT = deriv ? CTs.dM : CTs.M;
+    if (deriv) {
+        C.alloc(CN.M.n);
+        CT.alloc(CTs.M.n);
+    }
+    CouplingArgs a{};
+    a.K = K;
+    a.test_pts = c->side[0].pts.p;
+    a.trial_pts = c->side[1].pts.p;
+    a.pair_t = D.cpair_it.p;
+    a.pair_s = D.cpair_is.p;
+    a.rank_t = D.side[0].rank.p;
+    a.rank_s = D.side[1].rank.p;
+    a.piv_t = D.side[0].piv.p;
+    a.piv_s = D.side[1].piv.p;
+    a.maxrank = c->maxrank;
+    a.coff = D.ccoff.p;
+    a.npairs = D.npairs;
+    a.C = C.p;
+    if (D.npairs > 0) {
+        k_couplings<<<launch_grid(D.npairs, 16), 256, 0, s>>>(a);
+        CK(cudaGetLastError());
+    }
+    launch_transpose_blocks<double2>(C.p, D.ctr_in.p, D.ctr_rows.p, D.ctr_cols.p, D.ctr_off.p, D.ntr, CT.p, s);
+    CK(cudaGetLastError());
+    if (deriv) {
+        c->dN.alloc(c->N.n);
+        c->dNT.alloc(c->NT.n);
+    }
+    fill_near(c, K, deriv ? c->dN.p : c->N.p, deriv ? c->dNT.p : c->NT.p, s);
+}
+
+// complex-FP32 copies of a directional core's stage stores and near field
+void make_dir_f32(nca_core *c, cudaStream_t s) {
+    auto down = [&](DBuf<double2> &src, DBuf<float2> &dst) {
+        if (dst.n != src.n) dst.alloc(src.n);
+        if (src.n) k_to_f32<<<launch_grid(int64_t(src.n) / 256 + 1, 8), 256, 0, s>>>(src.p, dst.p, int64_t(src.n));
+        CK(cudaGetLastError());
+    };
+    for (DirProduct &pr : c->dir->prod)
+        for (GatherStage *G : {&pr.up, &pr.couple, &pr.down, &pr.leaves}) down(G->M, G->M32);
+    down(c->N, c->N32);
+    down(c->NT, c->NT32);
+}
+
+// drops the d/dk stores of a directional core (they belong to the wavenumber they were prepared at)
+void drop_dir_dk(nca_core *c) {
+    c->dN.release();
+    c->dNT.release();
+    for (DirProduct &pr : c->dir->prod)
+        for (GatherStage *G : {&pr.up, &pr.couple, &pr.down, &pr.leaves}) G->dM.release();
+    c->has_dk = false;
+}
+
+void set_dir_wavenumber(nca_core *c, double k, cudaStream_t s) {
+    KernelParams K = c->K;
+    K.k = k;
+    K.deriv = 0;
+    // new operators first (a singular frozen cross matrix leaves the core unchanged)
+    DBuf<double2> X[2], XT[2];
+    for (int sd = 0; sd < 2; ++sd) {
+        DirItems &d = c->dir->side[sd];
+        X[sd].alloc(d.X.n);
+        XT[sd].alloc(d.X.n);
+        fill_dir_bases(c, sd, 0, K, K, nullptr, X[sd].p, s);
+        launch_transpose_blocks<double2>(X[sd].p, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, d.nitems, XT[sd].p, s);
+        CK(cudaGetLastError());
+    }
+    double2 *const xs[2] = {X[0].p, X[1].p}, *const xts[2] = {XT[0].p, XT[1].p};
+    fill_dir_stores(c, K, xs, xts, false, s);
+    for (int sd = 0; sd < 2; ++sd) std::swap(c->dir->side[sd].X.p, X[sd].p);
+    c->K.k = k;
+    if (c->f32) make_dir_f32(c, s);
+    drop_dir_dk(c);
+    CK(cudaStreamSynchronize(s));
+}
+
+void prepare_dir_dk(nca_core *c, cudaStream_t s) {
+    KernelParams dK = c->K;
+    dK.deriv = 1;
+    DBuf<double2> dX[2], dXT[2];
+    for (int sd = 0; sd < 2; ++sd) {
+        DirItems &d = c->dir->side[sd];
+        dX[sd].alloc(d.X.n);
+        dXT[sd].alloc(d.X.n);
+        fill_dir_bases(c, sd, 1, c->K, dK, d.X.p, dX[sd].p, s);
+        launch_transpose_blocks<double2>(dX[sd].p, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, d.nitems, dXT[sd].p, s);
+        CK(cudaGetLastError());
+    }
+    double2 *const xs[2] = {dX[0].p, dX[1].p}, *const xts[2] = {dXT[0].p, dXT[1].p};
+    fill_dir_stores(c, dK, xs, xts, true, s);
+    CK(cudaStreamSynchronize(s));
+    c->has_dk = true;
+}
+
 // ---- serialised cores ---------------------------------------------------------------------
 // File layout (little-endian, native sizes): an 8-byte tag, the format number, the core's options
 // and kernel, the points, both trees, the partition, then per side the skeleton (SavedSide); every
@@ -3165,6 +3439,7 @@ void save_core(const nca_core *c, const char *path) {
             v.rank = d.h_rank;
             v.nrows = d.h_nrows;
             v.piv = d.piv.download(s);
+            v.cpiv = d.cpiv.download(s);
             v.xoff = d.h_xoff;
             v.X = d.X.download(s);
             v.plan = d.plan;
@@ -3495,7 +3770,6 @@ int32_t nca_core_set_wavenumber(nca_core *core, double k) {
         if (!core) return fail(NCA_ERR_ARG, "null core");
         if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
         if (core->batch) return fail(NCA_ERR_ARG, "a batch has one wavenumber per member: refill the members");
-        if (core->dir) return fail(NCA_ERR_ARG, "frozen-skeleton refills are not available for directional cores");
         if (core->K.kind == NCA_KERNEL_MATRIX) return fail(NCA_ERR_ARG, "a matrix kernel has no wavenumber");
         if (!std::isfinite(k)) return fail(NCA_ERR_ARG, "the wavenumber must be finite");
         CK(cudaSetDevice(core->device));
@@ -3505,6 +3779,10 @@ int32_t nca_core_set_wavenumber(nca_core *core, double k) {
             cudaStream_t s;
             ~StreamGuard() { cudaStreamDestroy(s); }
         } sg{s};
+        if (core->dir) {
+            set_dir_wavenumber(core, k, s);
+            return int(NCA_OK);
+        }
         KernelParams K = core->K;
         K.k = k;
         K.deriv = 0;
@@ -3540,7 +3818,6 @@ int32_t nca_core_prepare_dk(nca_core *core) {
         if (!core) return fail(NCA_ERR_ARG, "null core");
         if (core->moved) return fail(NCA_ERR_ARG, "the core's stores were moved into a batch");
         if (core->batch) return fail(NCA_ERR_ARG, "prepare the d/dk stores of the members, not of a batch");
-        if (core->dir) return fail(NCA_ERR_ARG, "d/dk stores are not available for directional cores");
         if (core->K.kind == NCA_KERNEL_MATRIX) return fail(NCA_ERR_ARG, "a matrix kernel has no wavenumber derivative");
         if (core->has_dk) return int(NCA_OK);
         CK(cudaSetDevice(core->device));
@@ -3550,6 +3827,10 @@ int32_t nca_core_prepare_dk(nca_core *core) {
             cudaStream_t s;
             ~StreamGuard() { cudaStreamDestroy(s); }
         } sg{s};
+        if (core->dir) {
+            prepare_dir_dk(core, s);
+            return int(NCA_OK);
+        }
         KernelParams dK = core->K;
         dK.deriv = 1;
         for (int sd = 0; sd < 2; ++sd) {

@@ -112,8 +112,6 @@ def test_directional_structure_and_limits():
     ranks, _ = items(A, 0)
     assert len(ranks) > N.core(A).info.nnodes_test  # several directions per cluster
     with pytest.raises(N.ArgumentError):
-        N.core(A).set_wavenumber(21.0)
-    with pytest.raises(N.ArgumentError):
         N.batch([A])
     with pytest.raises(N.ArgumentError):
         N.core(A).pivots(0)

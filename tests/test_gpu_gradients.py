@@ -145,3 +145,59 @@ def test_gradient_errors():
         N.dHdk(A).T @ cgauss(1024, 1)
     with pytest.raises(N.ArgumentError):
         N.dHdk(A.H) @ cgauss(1024, 1)
+
+
+def build_wideband(pts, k, tol, minvalues):
+    """A directional core: BottomUp(IACA) on isnearwideband(k) (test/nca/test_petrovgalerkinnca.jl:131-149)."""
+    N = _n()
+    t = N.KMeansTree(pts, N.KMeansTreeBuilder(minvalues=minvalues))
+    conv = N.FNormExtrapolator(tol)
+    tc = N.BottomUp(factorization=N.IACA(N.MaximumValue(), N.TreeMimicryPivoting(pts, pts, t), conv))
+    sc = N.BottomUp(factorization=N.IACA(N.TreeMimicryPivoting(pts, pts, t), N.MaximumValue(), conv))
+    return N.PetrovGalerkinNCA(N.HelmholtzKernel(k, rmin=1e-12), pts, pts, N.BlockTree(t, t),
+                               isnear=N.isnearwideband(k), testcompressor=tc, trialcompressor=sc, store_f32=True)
+
+
+def test_directional_frozen_skeleton_gradients():
+    """Directional (wideband) cores on their frozen skeleton: the refill at the build's own
+    wavenumber reproduces the product (X recomputed as K[rows, sigma] K[tau, sigma]^-1, equal to
+    IACA's U L^-1 up to rounding); dH/dk x matches central differences of refills; the rrule's
+    k_bar matches central differences of J = ||H(k) x - b||^2 and its x_bar is the adjoint
+    product, which agrees with the oracle's."""
+    from oracle import directional as OD
+    from oracle import oracle as O
+    N = _n()
+    n, k, tol = 3000, 16.0, 1e-5
+    pts = sphere(n, 51)
+    A = build_wideband(pts, k, tol, 32)
+    x = cgauss((n, 2), 52)
+    b = cgauss((n, 2), 53)
+    ybar = cgauss((n, 2), 54)
+    H = OD.DirectionalH2(pts, pts, O.Kernel(O.KIND_HELMHOLTZ, k=k, rmin=1e-12), k, minvalues=32, tol=tol)
+    assert relerr(A.H @ ybar, H.apply(ybar, 2)) < 1e-12
+    y0 = A @ x
+    A.core.set_wavenumber(k)
+    assert relerr(A @ x, y0) < 1e-9
+    h = 1e-6 * k
+    dy = N.dHdk(A) @ x
+    A.core.set_wavenumber(k + h)
+    yp = A @ x
+    A.core.set_wavenumber(k - h)
+    ym = A @ x
+    A.core.set_wavenumber(k)
+    assert relerr(dy, (yp - ym) / (2 * h)) < 1e-6
+
+    def J():
+        return float(np.sum(np.abs(A @ x - b) ** 2))
+    y, pullback = N.rrule_mul(A, x)
+    kbar, xbar = pullback(2 * (y - b))
+    A.core.set_wavenumber(k + h)
+    jp = J()
+    A.core.set_wavenumber(k - h)
+    jm = J()
+    A.core.set_wavenumber(k)
+    assert abs(kbar - (jp - jm) / (2 * h)) < 1e-6 * abs(kbar)
+    assert relerr(xbar, A.H @ (2 * (y - b))) < 1e-13
+    # the mixed-precision stores follow the refill
+    W = N.H2Workspace(N.core(A), np.complex64)
+    assert relerr(W @ x, A @ x) < 1e-5
