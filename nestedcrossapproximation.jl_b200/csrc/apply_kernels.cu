@@ -818,6 +818,121 @@ template void launch_gather_small<float2, double2>(const RowArgs<float2> &, cons
 template void launch_gather_small<float2, float2>(const RowArgs<float2> &, const int32_t *, int, cudaStream_t);
 
 namespace {
+// STAGE_GATHER over complex-FP32 stores and a complex-FP32 arena, every right-hand side of the
+// product in one launch, for outputs of at most NR rows: one warp per output (a grid-stride
+// sequence of outputs), lane l holding columns c0 + 2 l and c0 + 2 l + 1 of every output row in
+// FP32 registers (c0 = 0, 64, ...). A block entry is read at the same address by every lane (one
+// broadcast request), a vector row as one 16-byte load per lane (the row's columns are contiguous);
+// complex FP32 FMA with FP32 accumulation, U block columns per step with their loads issued
+// together. The block is read once per 64 columns instead of once per 16-column pass.
+template <int NR, int U>
+__global__ void __launch_bounds__(256) k_gather_wide(RowArgs<float2> a, const int32_t *nodes, int count) {
+    const int lane = threadIdx.x & 31;
+    const int nw = int((int64_t(gridDim.x) * blockDim.x) >> 5);
+    const float sg = a.conj ? -1.f : 1.f;
+    const bool scatter = a.y != nullptr;
+    for (int wi = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5); wi < count; wi += nw) {
+        const int o = nodes[wi];
+        const int R = a.g_rows[o];
+        const int e0 = a.g_segptr[o], e1 = a.g_segptr[o + 1];
+        const int64_t gout = a.g_out[o];
+        for (int c0 = 0; c0 < a.b; c0 += 64) {
+            const int col = c0 + 2 * lane;
+            const bool ok0 = col < a.b, ok1 = col + 1 < a.b;
+            float2 acc0[NR], acc1[NR];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc0[r] = acc1[r] = make_float2(0.f, 0.f);
+            for (int e = e0; e < e1; ++e) {
+                const int64_t mo = a.g_moff[e];
+                const float2 *M = mo >= 0 ? a.M + mo : a.M2 + (-1 - mo);
+                const int w = a.g_w[e];
+                const float2 *V = a.src32 + a.g_voff[e] * a.vs + col;
+                for (int j0 = 0; j0 < w; j0 += U) {
+                    float4 x[U];
+                    float2 m[U][NR];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int j = j0 + u;
+                        const bool in = j < w;
+                        x[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (in && ok0) x[u] = __ldg(reinterpret_cast<const float4 *>(V + int64_t(j) * a.vs));
+                        if (!ok1) x[u].z = x[u].w = 0.f;
+#pragma unroll
+                        for (int r = 0; r < NR; ++r)
+                            m[u][r] = in && r < R ? __ldg(M + r + int64_t(j) * R) : make_float2(0.f, 0.f);
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+#pragma unroll
+                        for (int r = 0; r < NR; ++r) {
+                            const float mx = m[u][r].x, my = sg * m[u][r].y;
+                            acc0[r].x = fmaf(mx, x[u].x, fmaf(-my, x[u].y, acc0[r].x));
+                            acc0[r].y = fmaf(mx, x[u].y, fmaf(my, x[u].x, acc0[r].y));
+                            acc1[r].x = fmaf(mx, x[u].z, fmaf(-my, x[u].w, acc1[r].x));
+                            acc1[r].y = fmaf(mx, x[u].w, fmaf(my, x[u].z, acc1[r].y));
+                        }
+                }
+            }
+            if (!ok0) continue;
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                if (r >= R) break;
+                if (scatter) {
+                    for (int h = 0; h < (ok1 ? 2 : 1); ++h) {
+                        const float2 v = h ? acc1[r] : acc0[r];
+                        double2 *yp = a.y + a.perm[gout + r] + int64_t(col + h) * a.ldy;
+                        double2 out = make_double2(a.alpha.x * v.x - a.alpha.y * v.y, a.alpha.x * v.y + a.alpha.y * v.x);
+                        if (a.usebeta) {
+                            const double2 yo = *yp;
+                            out.x += a.beta.x * yo.x - a.beta.y * yo.y;
+                            out.y += a.beta.x * yo.y + a.beta.y * yo.x;
+                        }
+                        *yp = out;
+                    }
+                } else {
+                    float2 *d = a.dst32 + (gout + r) * a.vs + col;
+                    float2 v0 = acc0[r], v1 = acc1[r];
+                    if (a.accumulate) {
+                        v0.x += d[0].x;
+                        v0.y += d[0].y;
+                        if (ok1) {
+                            v1.x += d[1].x;
+                            v1.y += d[1].y;
+                        }
+                    }
+                    d[0] = v0;
+                    if (ok1) d[1] = v1;
+                }
+            }
+        }
+    }
+}
+}  // namespace
+
+bool gather_wide_fits(int maxrows) { return maxrows <= 32; }
+
+void launch_gather_wide(const RowArgs<float2> &a, const int32_t *nodes, int count, cudaStream_t s) {
+    if (count <= 0) return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int need = (count + 7) / 8;
+    const int grid = need < sms * 8 ? need : sms * 8;
+    if (a.maxrows <= 4)
+        k_gather_wide<4, 4><<<grid, 256, 0, s>>>(a, nodes, count);
+    else if (a.maxrows <= 8)
+        k_gather_wide<8, 2><<<grid, 256, 0, s>>>(a, nodes, count);
+    else if (a.maxrows <= 12)
+        k_gather_wide<12, 2><<<grid, 256, 0, s>>>(a, nodes, count);
+    else if (a.maxrows <= 16)
+        k_gather_wide<16, 1><<<grid, 256, 0, s>>>(a, nodes, count);
+    else if (a.maxrows <= 24)
+        k_gather_wide<24, 1><<<grid, 256, 0, s>>>(a, nodes, count);
+    else
+        k_gather_wide<32, 1><<<grid, 256, 0, s>>>(a, nodes, count);
+}
+
+namespace {
 constexpr int TINY_WARPS = 4;       // warps (independent output streams) per CTA
 constexpr int TINY_STAGE = 9216;    // bytes of one chunk buffer; two per warp
 

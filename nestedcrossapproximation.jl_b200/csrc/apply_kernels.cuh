@@ -82,6 +82,11 @@ void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStrea
 // global memory, complex FP64 FMA (directional products, whose outputs are many small blocks).
 template <typename S, typename VT = double2>
 void launch_gather_small(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
+// STAGE_GATHER over complex-FP32 stores and arena for outputs of at most 32 rows, all a.b
+// right-hand sides in one launch (a.q0, a.bc unused): one warp per output, two columns per lane,
+// FP32 accumulation.
+bool gather_wide_fits(int maxrows);
+void launch_gather_wide(const RowArgs<float2> &a, const int32_t *nodes, int count, cudaStream_t s);
 // STAGE_GATHER through the streaming kernel with vectors of type VT (launch_rows: VT = double2)
 template <typename S, typename VT>
 void launch_gather_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);

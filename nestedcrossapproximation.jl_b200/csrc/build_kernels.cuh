@@ -123,7 +123,9 @@ struct IacaArgs {
     int32_t *cursor;       // zero at launch
     int32_t *rank, *nrows, *piv, *cpiv;  // piv, cpiv: maxrank per item (cpiv optional)
     double2 *X;            // item slots of rows x min(maxrank, rows, far points) entries at xoff
-    const int64_t *xoff;
+    const int64_t *xoff;   // indexed by item, or by position in `items` with xoff_by_position
+    int xoff_by_position;
+    int32_t *rank_pos;     // optional: rank_pos[i] = rank, rank_pos[nitems + i] = rows of items[i]
     int maxrank;
     double tol;
     int32_t *status;       // [flag, item, a, b], see k_iaca

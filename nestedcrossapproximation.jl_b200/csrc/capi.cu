@@ -1361,17 +1361,20 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     // compacted to the ranks found before the next level runs.
     d.h_rank.assign(ni, 0);
     d.h_nrows.assign(ni, 0);
-    std::vector<int64_t> lvoff(std::max(ni, 1), 0), cpos(ni, -1);
+    std::vector<int64_t> cpos(ni, -1);
     std::vector<std::unique_ptr<DBuf<double2>>> levelX;
     std::vector<std::vector<int32_t>> levelItems;
-    // scratch reused by every level (grown, never shrunk: no device-wide frees between levels)
-    DBuf<int64_t> dlvoff, dso, ddo;
-    DBuf<int32_t> nodes, dld, dr, dc;
+    // scratch reused by every level (grown, never shrunk: no device-wide frees between levels);
+    // the level's slot offsets, ranks and rows are indexed by position in the level's item list
+    DBuf<int64_t> dlvoff, ddo;
+    DBuf<int32_t> nodes, drk;
     DBuf<double2> chunk;
     PinnedBuf<int32_t> hrank(2 * size_t(std::max(ni, 1)));
+    a.xoff_by_position = 1;
     int64_t total = 0;
     for (int lev = T.nlevels - 1; lev >= 0; --lev) {
         std::vector<int32_t> items;
+        std::vector<int64_t> lvoff;
         int mc = 0;
         int64_t bound = 0;
         for (int it : bylevel[lev]) {
@@ -1383,7 +1386,7 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
                 for (int k = pl.item_chptr[it]; k < pl.item_chptr[it + 1]; ++k) m += d.h_rank[pl.item_chidx[k]];
             }
             const int64_t rb = std::min<int64_t>(std::min<int64_t>(maxrank, m), int64_t(farpts[it]));
-            lvoff[it] = bound;
+            lvoff.push_back(bound);
             bound += pad2(m * rb);
             items.push_back(it);
             mc = int(std::max<int64_t>(mc, m));
@@ -1396,11 +1399,14 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
         if (!chunk.p || size_t(bound) > chunk.n) chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
         upload_reuse(dlvoff, lvoff, s);
         upload_reuse(nodes, items, s);
+        const int nl = int(items.size());
+        if (drk.n < 2 * size_t(nl)) drk.alloc(2 * size_t(nl));
         status.zero(s);
         a.X = chunk.p;
         a.xoff = dlvoff.p;
         a.items = nodes.p;
-        a.nitems = int(items.size());
+        a.nitems = nl;
+        a.rank_pos = drk.p;
         launch_iaca(a, mc, s);
         CK(cudaGetLastError());
         const std::vector<int32_t> st = status.download(s);
@@ -1414,36 +1420,26 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
         }
         if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: an item exceeds the IACA kernel's row capacity");
         if (st[0] == 3) throw Failure(NCA_ERR_CUDA, "internal: tree mimicry ran out of far points");
-        CK(cudaMemcpyAsync(hrank.p, d.rank.p, sizeof(int32_t) * ni, cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(hrank.p + ni, d.nrows.p, sizeof(int32_t) * ni, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hrank.p, drk.p, sizeof(int32_t) * 2 * nl, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
-        const int32_t *rk = hrank.p, *nr = hrank.p + ni;
-        // compact this level: exact m x r blocks, back to back
-        std::vector<int64_t> soff, doff;
-        std::vector<int32_t> sld, crows, ccols;
+        const int32_t *rk = hrank.p, *nr = hrank.p + nl;
+        // compact this level: exact m x r blocks, back to back (one copy per item, rank-0 items
+        // copy nothing; sources, rows and columns straight from the positional arrays)
+        std::vector<int64_t> doff(nl);
         int64_t lt = 0;
-        for (int it : items) {
-            d.h_rank[it] = rk[it];
-            d.h_nrows[it] = nr[it];
+        for (int i = 0; i < nl; ++i) {
+            const int it = items[i];
+            d.h_rank[it] = rk[i];
+            d.h_nrows[it] = nr[i];
             cpos[it] = lt;
-            if (rk[it] > 0 && nr[it] > 0) {
-                soff.push_back(lvoff[it]);
-                sld.push_back(nr[it]);
-                crows.push_back(nr[it]);
-                ccols.push_back(rk[it]);
-                doff.push_back(lt);
-            }
-            lt += pad2(int64_t(nr[it]) * rk[it]);
+            doff[i] = lt;
+            lt += pad2(int64_t(nr[i]) * rk[i]);
         }
         levelX.emplace_back(new DBuf<double2>());
         levelX.back()->alloc(size_t(std::max<int64_t>(lt, 1)));
-        if (!soff.empty()) {
-            upload_reuse(dso, soff, s);
+        if (lt > 0) {
             upload_reuse(ddo, doff, s);
-            upload_reuse(dld, sld, s);
-            upload_reuse(dr, crows, s);
-            upload_reuse(dc, ccols, s);
-            launch_copy_blocks<double2>(chunk.p, dso.p, dld.p, dr.p, dc.p, ddo.p, int64_t(soff.size()),
+            launch_copy_blocks<double2>(chunk.p, dlvoff.p, drk.p + nl, drk.p + nl, drk.p, ddo.p, int64_t(nl),
                                         levelX.back()->p, s);
             CK(cudaGetLastError());
             CK(cudaStreamSynchronize(s));
@@ -2306,70 +2302,82 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
     ++count.stage[0];
     if (timer) timer->mark(0, true, s);
     const bool conj = mode == 2;
+    // Stage by stage (each stage's levels in order): a launch group of small outputs over complex
+    // FP32 stores takes every right-hand side in one k_gather_wide launch; any other group runs
+    // once per 16-column pass. A group depends only on earlier groups' outputs for the same
+    // columns, so this order computes what the pass-major order computes.
     auto run = [&](auto tag) {
         using S = decltype(tag);
         constexpr bool f64 = std::is_same<S, double2>::value;
         using VT = S;  // FP64 stores with FP64 vectors, FP32 stores with FP32 vectors
         const S *nearM = f64 ? (const S *)(mode == 0 ? c->N.p : c->NT.p) : (const S *)(mode == 0 ? c->N32.p : c->NT32.p);
-        for (int q0 = 0; q0 < b; q0 += 16) {
-            const int bc = std::min(16, b - q0);
-            auto stage = [&](const GatherStage &G, bool accumulate, bool scatter, int sk) {
-                const S *M = f64 ? (const S *)G.M.p : (const S *)G.M32.p;
-                if (timer) timer->mark(sk, false, s);
-                for (size_t g = 0; g + 1 < G.group_ptr.size(); ++g) {
-                    const int cnt = G.group_ptr[g + 1] - G.group_ptr[g];
-                    if (!cnt) continue;
-                    RowArgs<S> a{};
-                    a.stage = STAGE_GATHER;
-                    a.M = M;
-                    a.M2 = nearM;
-                    a.g_rows = G.rows.p;
-                    a.g_out = G.out.p;
-                    a.g_segptr = G.segptr.p;
-                    a.g_moff = G.moff.p;
-                    a.g_w = G.w.p;
-                    a.g_voff = G.voff.p;
-                    if (f64) {
-                        a.src = arena;
-                        a.dst = arena;
-                    } else {
-                        a.src32 = arena32;
-                        a.dst32 = arena32;
+        auto stage = [&](const GatherStage &G, bool accumulate, bool scatter, int sk) {
+            const S *M = f64 ? (const S *)G.M.p : (const S *)G.M32.p;
+            if (timer) timer->mark(sk, false, s);
+            for (size_t g = 0; g + 1 < G.group_ptr.size(); ++g) {
+                const int cnt = G.group_ptr[g + 1] - G.group_ptr[g];
+                if (!cnt) continue;
+                RowArgs<S> a{};
+                a.stage = STAGE_GATHER;
+                a.M = M;
+                a.M2 = nearM;
+                a.g_rows = G.rows.p;
+                a.g_out = G.out.p;
+                a.g_segptr = G.segptr.p;
+                a.g_moff = G.moff.p;
+                a.g_w = G.w.p;
+                a.g_voff = G.voff.p;
+                if (f64) {
+                    a.src = arena;
+                    a.dst = arena;
+                } else {
+                    a.src32 = arena32;
+                    a.dst32 = arena32;
+                }
+                a.accumulate = accumulate;
+                if (scatter) {
+                    a.y = yd;
+                    a.ldy = ly;
+                    a.perm = c->side[O].perm.p;
+                    a.alpha = alpha;
+                    a.beta = beta;
+                    a.usebeta = beta.x != 0.0 || beta.y != 0.0;
+                }
+                a.b = b;
+                a.vs = vs;
+                a.conj = conj;
+                a.maxrows = G.group_maxrows[g];
+                a.error = error;
+                const bool small = G.group_work[g] < 8192.0;
+                if constexpr (!f64) {
+                    if (b >= 2 && small && gather_wide_fits(a.maxrows)) {
+                        launch_gather_wide(a, G.outputs.p + G.group_ptr[g], cnt, s);
+                        ++count.total;
+                        ++count.stage[sk];
+                        continue;
                     }
-                    a.accumulate = accumulate;
-                    if (scatter) {
-                        a.y = yd;
-                        a.ldy = ly;
-                        a.perm = c->side[O].perm.p;
-                        a.alpha = alpha;
-                        a.beta = beta;
-                        a.usebeta = beta.x != 0.0 || beta.y != 0.0;
-                    }
-                    a.b = b;
-                    a.bc = bc;
+                }
+                for (int q0 = 0; q0 < b; q0 += 16) {
+                    a.bc = std::min(16, b - q0);
                     a.q0 = q0;
-                    a.vs = vs;
-                    a.conj = conj;
-                    a.maxrows = G.group_maxrows[g];
-                    a.error = error;
                     // many small outputs: one warp streams a sequence of them (up to 32 rows) or
                     // takes one (up to 64 rows); few large ones: the streaming MMA kernel
-                    if (G.group_work[g] < 8192.0 && gather_tiny_fits(a.maxrows, bc))
+                    if (small && gather_tiny_fits(a.maxrows, a.bc))
                         launch_gather_tiny<S, VT>(a, G.outputs.p + G.group_ptr[g], cnt, s);
-                    else if (a.maxrows <= 64 && G.group_work[g] < 8192.0)
+                    else if (a.maxrows <= 64 && small)
                         launch_gather_small<S, VT>(a, G.outputs.p + G.group_ptr[g], cnt, s);
                     else
                         launch_gather_rows<S, VT>(a, G.outputs.p + G.group_ptr[g], cnt, s);
                     ++count.total;
                     ++count.stage[sk];
                 }
-                if (timer) timer->mark(sk, true, s);
-            };
-            stage(pr.up, false, false, 1);
-            stage(pr.couple, false, false, 2);
-            stage(pr.down, true, false, 3);
-            stage(pr.leaves, false, true, 5);
-        }
+            }
+            if (timer) timer->mark(sk, true, s);
+        };
+        stage(pr.up, false, false, 1);
+        stage(pr.couple, false, false, 2);
+        stage(pr.down, true, false, 3);
+        stage(pr.leaves, false, true, 5);
     };
     if (precision == NCA_PREC_F64)
         run(double2{});

@@ -302,6 +302,16 @@ __device__ __forceinline__ T slot(const T (&v)[RPL], int q) {
     return out;
 }
 
+// K(own point, far point) in the side's orientation (side 0: own points are test points). Kept
+// out of line: the k_iaca loop calls it once per held row, and one copy of the entry code keeps
+// the kernel's instruction footprint small (an inlined copy per row and orientation made
+// instruction fetch the kernel's top stall).
+__device__ __noinline__ double2 oriented_entry(KernelParams K, bool own_is_test, double rx, double ry, double rz,
+                                              int32_t rid, double qx, double qy, double qz, int32_t qid) {
+    if (own_is_test) return kernel_entry(K, rx, ry, rz, qx, qy, qz, rid, qid);
+    return kernel_entry(K, qx, qy, qz, rx, ry, rz, qid, rid);
+}
+
 // IACA of every item of one level, one warp per item (items taken from an atomic cursor): tree
 // mimicry picks the geometric columns one at a time, the column is evaluated on the item's rows
 // (lane l holds rows l + 32 q), eliminated against the accepted crosses, tested by the
@@ -386,7 +396,7 @@ __global__ void __launch_bounds__(kIacaWarps * 32) k_iaca(IacaArgs a) {
             const int sz = F.end[f] - F.begin[f];
             n += limit - n < sz ? limit - n : sz;
         }
-        double2 *U = a.X + a.xoff[item];
+        double2 *U = a.X + a.xoff[a.xoff_by_position ? idx : item];
         const double tol2 = __dmul_rn(a.tol, a.tol);
         double S = 0.0;
         int k = 0;
@@ -404,8 +414,7 @@ __global__ void __launch_bounds__(kIacaWarps * 32) k_iaca(IacaArgs a) {
             for (int q = 0; q < RPL; ++q) {
                 r[q] = make_double2(0.0, 0.0);
                 if (rid[q] >= 0) {
-                    r[q] = a.side == 0 ? kernel_entry(a.K, rx[q], ry[q], rz[q], qx, qy, qz, rid[q], jid)
-                                       : kernel_entry(a.K, qx, qy, qz, rx[q], ry[q], rz[q], jid, rid[q]);
+                    r[q] = oriented_entry(a.K, a.side == 0, rx[q], ry[q], rz[q], rid[q], qx, qy, qz, jid);
                     cs = __dadd_rn(cs, cabs2_rn(r[q]));
                 }
             }
@@ -513,6 +522,10 @@ __global__ void __launch_bounds__(kIacaWarps * 32) k_iaca(IacaArgs a) {
         if (lane == 0) {
             a.rank[item] = rank;
             a.nrows[item] = m;
+            if (a.rank_pos) {
+                a.rank_pos[idx] = rank;
+                a.rank_pos[a.nitems + idx] = m;
+            }
         }
         __syncwarp();
     }
