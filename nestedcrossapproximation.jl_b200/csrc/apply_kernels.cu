@@ -819,68 +819,207 @@ template void launch_gather_small<float2, float2>(const RowArgs<float2> &, const
 
 namespace {
 // STAGE_GATHER over complex-FP32 stores and a complex-FP32 arena, every right-hand side of the
-// product in one launch, for outputs of at most NR rows: one warp per output (a grid-stride
-// sequence of outputs), lane l holding columns c0 + 2 l and c0 + 2 l + 1 of every output row in
-// FP32 registers (c0 = 0, 64, ...). A block entry is read at the same address by every lane (one
-// broadcast request), a vector row as one 16-byte load per lane (the row's columns are contiguous);
-// complex FP32 FMA with FP32 accumulation, U block columns per step with their loads issued
-// together. The block is read once per 64 columns instead of once per 16-column pass.
-template <int NR, int U>
-__global__ void __launch_bounds__(256) k_gather_wide(RowArgs<float2> a, const int32_t *nodes, int count) {
-    const int lane = threadIdx.x & 31;
+// product in one launch, for outputs of at most NR rows.
+//
+// One warp takes a grid-stride sequence of outputs; lane l holds columns c0 + 2 l and c0 + 2 l + 1
+// of every output row in FP32 registers (passes c0 = 0, 64, ...). An output's segments are one
+// sequence of W = sum w_e (block column, vector row) pairs, cut into chunks of WIDE_J pairs; the
+// warp streams the chunks of all its (output, pass) steps through a WIDE_SLOTS-slot shared-memory
+// ring filled by asynchronous copies, WIDE_SLOTS - 1 chunks ahead of the one being multiplied (a
+// chunk of the next output is in flight while the current one finishes). A chunk holds the R
+// entries of each block column (leading dimension NR, so one 16-byte shared load broadcasts two
+// rows' entries to every lane) and each lane's two columns of each vector row. The multiply skips
+// the row pairs at and beyond R. Complex FP32 FMA with FP32 accumulation.
+constexpr int WIDE_WARPS = 4;  // warps (independent output sequences) per CTA
+constexpr int WIDE_J = 8;      // (block column, vector row) pairs per chunk
+constexpr int WIDE_SLOTS = 3;  // chunks per warp's ring
+
+template <int NR>
+struct WideShape {
+    static constexpr int mslot = NR * WIDE_J;        // float2 entries of a chunk's block columns
+    static constexpr int vslot = WIDE_J * 32 * 2;    // float2 entries of a chunk's vector rows
+    static constexpr int slot = mslot + vslot;
+    static constexpr size_t smem = size_t(WIDE_WARPS) * WIDE_SLOTS * slot * sizeof(float2);
+};
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ WideOut wide_record(const WideOut *outs, int i, int count) {
+    WideOut o{0, 0, 0, 0, 0, 0};
+    if (i < count) {
+        const int4 *q = reinterpret_cast<const int4 *>(outs + i);
+        const int4 u = __ldg(q), v = __ldg(q + 1);
+        o.R = u.x;
+        o.W = u.y;
+        o.e0 = u.z;
+        o.e1 = u.w;
+        o.out = int64_t((uint64_t(uint32_t(v.y)) << 32) | uint32_t(v.x));
+    }
+    return o;
+}
+
+// lane l's share of a window of 32 segments starting at base: segment base + l
+struct WideSeg {
+    int w;
+    int64_t moff, voff;
+};
+__device__ __forceinline__ WideSeg wide_segs(const RowArgs<float2> &a, int base, int e1, int lane) {
+    WideSeg g{0, 0, 0};
+    const int e = base + lane;
+    if (e < e1) {
+        g.w = __ldg(a.g_w + e);
+        g.moff = __ldg(reinterpret_cast<const long long *>(a.g_moff) + e);
+        g.voff = __ldg(reinterpret_cast<const long long *>(a.g_voff) + e);
+    }
+    return g;
+}
+
+template <int NR, bool CONJ>
+__global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 2)
+    k_gather_wide(RowArgs<float2> a, const WideOut *outs, int count) {
+    using Shape = WideShape<NR>;
+    extern __shared__ __align__(16) float2 wsm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    float2 *ring = wsm + size_t(wib) * WIDE_SLOTS * Shape::slot;
     const int nw = int((int64_t(gridDim.x) * blockDim.x) >> 5);
-    const float sg = a.conj ? -1.f : 1.f;
+    const int first = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     const bool scatter = a.y != nullptr;
-    for (int wi = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5); wi < count; wi += nw) {
-        const int o = nodes[wi];
-        const int R = a.g_rows[o];
-        const int e0 = a.g_segptr[o], e1 = a.g_segptr[o + 1];
-        const int64_t gout = a.g_out[o];
+    // ---- producer: walks the warp's outputs (records prefetched two ahead, segment windows one
+    // ahead), their passes and their (block column, vector row) pairs, WIDE_J pairs per chunk
+    int pwi = first;
+    WideOut pc = wide_record(outs, first, count), pn = wide_record(outs, first + nw, count),
+            p2 = wide_record(outs, first + 2 * nw, count);
+    WideSeg gc = wide_segs(a, pc.e0, pc.e1, lane), gn = wide_segs(a, pn.e0, pn.e1, lane);
+    int sb = pc.e0;           // first segment of the window in gc
+    int pc0 = 0, pe = pc.e0, pj = 0, pt = 0;
+    // the current segment's width, block and vector row (uniform)
+    auto seg_at = [&](int e, int &w, const float2 *&M, int64_t &vb) {
+        if (e < sb || e - sb >= 32) {
+            sb = e;
+            gc = wide_segs(a, sb, pc.e1, lane);
+        }
+        const int l = e - sb;
+        w = __shfl_sync(0xffffffffu, gc.w, l);
+        const long long mo = __shfl_sync(0xffffffffu, (long long)gc.moff, l);
+        vb = __shfl_sync(0xffffffffu, (long long)gc.voff, l);
+        M = mo >= 0 ? a.M + mo : a.M2 + (-1 - mo);
+    };
+    int pw = 0;
+    const float2 *pM = nullptr;
+    int64_t pvb = 0;
+    if (pwi < count && pc.W > 0) seg_at(pe, pw, pM, pvb);
+    auto issue = [&](int q) {
+        // skip the (output, pass) steps whose pairs are all issued
+        while (pwi < count && pt >= pc.W) {
+            pc0 += 64;
+            pt = 0;
+            pj = 0;
+            pe = pc.e0;
+            if (pc0 >= a.b || pc.W == 0) {
+                pwi += nw;
+                pc = pn;
+                gc = gn;
+                sb = pc.e0;
+                pn = p2;
+                gn = wide_segs(a, pn.e0, pn.e1, lane);
+                p2 = wide_record(outs, pwi + 2 * nw, count);
+                pc0 = 0;
+                pe = pc.e0;
+            }
+            if (pwi < count && pc.W > 0) seg_at(pe, pw, pM, pvb);
+        }
+        if (pwi < count) {
+            const int jn = min(WIDE_J, pc.W - pt);
+            float2 *Ms = ring + q * Shape::slot;
+            float2 *Vs = Ms + Shape::mslot;
+            const int col = pc0 + 2 * lane;
+            const int ncol = col < a.b ? min(2, a.b - col) : 0;
+            const int R = pc.R;
+            for (int jj = 0; jj < jn; ++jj) {
+                while (pj >= pw) {
+                    ++pe;
+                    pj = 0;
+                    seg_at(pe, pw, pM, pvb);
+                }
+                if (lane < R) cp_async8(Ms + jj * NR + lane, pM + int64_t(pj) * R + lane);
+                const float2 *v = a.src32 + (pvb + pj) * a.vs + col;
+                if (ncol == 2)
+                    cp_async16(Vs + (jj * 32 + lane) * 2, v);
+                else if (ncol == 1)
+                    cp_async8(Vs + (jj * 32 + lane) * 2, v);
+                ++pj;
+            }
+            pt += jn;
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int k = 0; k + 1 < WIDE_SLOTS; ++k) issue(k);
+    // ---- consumer: the same walk, one chunk at a time out of the ring
+    int qc = 0, qp = WIDE_SLOTS - 1;
+    WideOut cc = wide_record(outs, first, count), cn = wide_record(outs, first + nw, count);
+    for (int wi = first; wi < count; wi += nw) {
+        const int R = cc.R, W = cc.W;
+        const int64_t gout = cc.out;
+        cc = cn;
+        cn = wide_record(outs, wi + 2 * nw, count);
         for (int c0 = 0; c0 < a.b; c0 += 64) {
             const int col = c0 + 2 * lane;
-            const bool ok0 = col < a.b, ok1 = col + 1 < a.b;
-            float2 acc0[NR], acc1[NR];
+            const int ncol = col < a.b ? min(2, a.b - col) : 0;
+            float2 acc[NR][2];
 #pragma unroll
-            for (int r = 0; r < NR; ++r) acc0[r] = acc1[r] = make_float2(0.f, 0.f);
-            for (int e = e0; e < e1; ++e) {
-                const int64_t mo = a.g_moff[e];
-                const float2 *M = mo >= 0 ? a.M + mo : a.M2 + (-1 - mo);
-                const int w = a.g_w[e];
-                const float2 *V = a.src32 + a.g_voff[e] * a.vs + col;
-                for (int j0 = 0; j0 < w; j0 += U) {
-                    float4 x[U];
-                    float2 m[U][NR];
+            for (int r = 0; r < NR; ++r) acc[r][0] = acc[r][1] = make_float2(0.f, 0.f);
+            for (int t = 0; t < W; t += WIDE_J) {
+                const int jn = min(WIDE_J, W - t);
+                issue(qp);
+                qp = qp + 1 == WIDE_SLOTS ? 0 : qp + 1;
+                cp_async_wait<WIDE_SLOTS - 1>();
+                __syncwarp();
+                const float2 *Ms = ring + qc * Shape::slot;
+                const float4 *Vs = reinterpret_cast<const float4 *>(Ms + Shape::mslot) + lane;
+                float4 xn = Vs[0];
+#pragma unroll 1
+                for (int jj = 0; jj < jn; ++jj) {
+                    // this pair's vector columns; the next pair's load issued before the FMAs
+                    const float4 x = xn;
+                    xn = Vs[min(jj + 1, WIDE_J - 1) * 32];
+                    const float4 *Mj = reinterpret_cast<const float4 *>(Ms + jj * NR);
 #pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        const int j = j0 + u;
-                        const bool in = j < w;
-                        x[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (in && ok0) x[u] = __ldg(reinterpret_cast<const float4 *>(V + int64_t(j) * a.vs));
-                        if (!ok1) x[u].z = x[u].w = 0.f;
+                    for (int r2 = 0; r2 < NR / 2; ++r2) {
+                        const float4 m2 = Mj[r2];
 #pragma unroll
-                        for (int r = 0; r < NR; ++r)
-                            m[u][r] = in && r < R ? __ldg(M + r + int64_t(j) * R) : make_float2(0.f, 0.f);
-                    }
-#pragma unroll
-                    for (int u = 0; u < U; ++u)
-#pragma unroll
-                        for (int r = 0; r < NR; ++r) {
-                            const float mx = m[u][r].x, my = sg * m[u][r].y;
-                            acc0[r].x = fmaf(mx, x[u].x, fmaf(-my, x[u].y, acc0[r].x));
-                            acc0[r].y = fmaf(mx, x[u].y, fmaf(my, x[u].x, acc0[r].y));
-                            acc1[r].x = fmaf(mx, x[u].z, fmaf(-my, x[u].w, acc1[r].x));
-                            acc1[r].y = fmaf(mx, x[u].w, fmaf(my, x[u].z, acc1[r].y));
+                        for (int h = 0; h < 2; ++h) {
+                            const float mx = h ? m2.z : m2.x, my = CONJ ? -(h ? m2.w : m2.y) : (h ? m2.w : m2.y);
+                            float2 &p0 = acc[2 * r2 + h][0], &p1 = acc[2 * r2 + h][1];
+                            p0.x = fmaf(mx, x.x, fmaf(-my, x.y, p0.x));
+                            p0.y = fmaf(mx, x.y, fmaf(my, x.x, p0.y));
+                            p1.x = fmaf(mx, x.z, fmaf(-my, x.w, p1.x));
+                            p1.y = fmaf(mx, x.w, fmaf(my, x.z, p1.y));
                         }
+                    }
                 }
+                __syncwarp();
+                qc = qc + 1 == WIDE_SLOTS ? 0 : qc + 1;
             }
-            if (!ok0) continue;
+            if (ncol == 0) continue;
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
                 if (r >= R) break;
                 if (scatter) {
-                    for (int h = 0; h < (ok1 ? 2 : 1); ++h) {
-                        const float2 v = h ? acc1[r] : acc0[r];
-                        double2 *yp = a.y + a.perm[gout + r] + int64_t(col + h) * a.ldy;
+                    const int64_t yr = a.perm[gout + r];
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        if (c >= ncol) break;
+                        const float2 v = acc[r][c];
+                        double2 *yp = a.y + yr + int64_t(col + c) * a.ldy;
                         double2 out = make_double2(a.alpha.x * v.x - a.alpha.y * v.y, a.alpha.x * v.y + a.alpha.y * v.x);
                         if (a.usebeta) {
                             const double2 yo = *yp;
@@ -891,45 +1030,71 @@ __global__ void __launch_bounds__(256) k_gather_wide(RowArgs<float2> a, const in
                     }
                 } else {
                     float2 *d = a.dst32 + (gout + r) * a.vs + col;
-                    float2 v0 = acc0[r], v1 = acc1[r];
-                    if (a.accumulate) {
-                        v0.x += d[0].x;
-                        v0.y += d[0].y;
-                        if (ok1) {
-                            v1.x += d[1].x;
-                            v1.y += d[1].y;
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        if (c >= ncol) break;
+                        float2 v = acc[r][c];
+                        if (a.accumulate) {
+                            v.x += d[c].x;
+                            v.y += d[c].y;
                         }
+                        d[c] = v;
                     }
-                    d[0] = v0;
-                    if (ok1) d[1] = v1;
                 }
             }
         }
     }
+    cp_async_wait<0>();
+}
+
+template <int NR, bool CONJ>
+void wide_launch(const RowArgs<float2> &a, const WideOut *outs, int count, cudaStream_t s, int sms) {
+    const size_t sm = WideShape<NR>::smem;
+    cudaFuncSetAttribute(k_gather_wide<NR, CONJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_wide<NR, CONJ>, WIDE_WARPS * 32, sm);
+    const int need = (count + WIDE_WARPS - 1) / WIDE_WARPS;
+    const int cap = sms * (per_sm > 0 ? per_sm : 1);
+    k_gather_wide<NR, CONJ><<<need < cap ? need : cap, WIDE_WARPS * 32, sm, s>>>(a, outs, count);
+}
+
+template <int NR>
+void wide_launch(const RowArgs<float2> &a, const WideOut *outs, int count, cudaStream_t s, int sms) {
+    if (a.conj)
+        wide_launch<NR, true>(a, outs, count, s, sms);
+    else
+        wide_launch<NR, false>(a, outs, count, s, sms);
 }
 }  // namespace
 
 bool gather_wide_fits(int maxrows) { return maxrows <= 32; }
 
-void launch_gather_wide(const RowArgs<float2> &a, const int32_t *nodes, int count, cudaStream_t s) {
+int wide_rows_class(int R) {
+    if (R <= 24) return R <= 2 ? 2 : R + (R & 1);
+    return R <= 28 ? 28 : 32;
+}
+
+void launch_gather_wide(const RowArgs<float2> &a, const WideOut *outs, int count, int nr, cudaStream_t s) {
     if (count <= 0) return;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int need = (count + 7) / 8;
-    const int grid = need < sms * 8 ? need : sms * 8;
-    if (a.maxrows <= 4)
-        k_gather_wide<4, 4><<<grid, 256, 0, s>>>(a, nodes, count);
-    else if (a.maxrows <= 8)
-        k_gather_wide<8, 2><<<grid, 256, 0, s>>>(a, nodes, count);
-    else if (a.maxrows <= 12)
-        k_gather_wide<12, 2><<<grid, 256, 0, s>>>(a, nodes, count);
-    else if (a.maxrows <= 16)
-        k_gather_wide<16, 1><<<grid, 256, 0, s>>>(a, nodes, count);
-    else if (a.maxrows <= 24)
-        k_gather_wide<24, 1><<<grid, 256, 0, s>>>(a, nodes, count);
-    else
-        k_gather_wide<32, 1><<<grid, 256, 0, s>>>(a, nodes, count);
+    switch (nr) {
+        case 2: wide_launch<2>(a, outs, count, s, sms); break;
+        case 4: wide_launch<4>(a, outs, count, s, sms); break;
+        case 6: wide_launch<6>(a, outs, count, s, sms); break;
+        case 8: wide_launch<8>(a, outs, count, s, sms); break;
+        case 10: wide_launch<10>(a, outs, count, s, sms); break;
+        case 12: wide_launch<12>(a, outs, count, s, sms); break;
+        case 14: wide_launch<14>(a, outs, count, s, sms); break;
+        case 16: wide_launch<16>(a, outs, count, s, sms); break;
+        case 18: wide_launch<18>(a, outs, count, s, sms); break;
+        case 20: wide_launch<20>(a, outs, count, s, sms); break;
+        case 22: wide_launch<22>(a, outs, count, s, sms); break;
+        case 24: wide_launch<24>(a, outs, count, s, sms); break;
+        case 28: wide_launch<28>(a, outs, count, s, sms); break;
+        default: wide_launch<32>(a, outs, count, s, sms); break;
+    }
 }
 
 namespace {
@@ -942,9 +1107,6 @@ __device__ __forceinline__ void cp_async(void *dst, const double2 *src) {
 __device__ __forceinline__ void cp_async(void *dst, const float2 *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ int pow2_at_least(int n) {
     int p = 1;

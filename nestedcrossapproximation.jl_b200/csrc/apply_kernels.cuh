@@ -82,11 +82,21 @@ void launch_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStrea
 // global memory, complex FP64 FMA (directional products, whose outputs are many small blocks).
 template <typename S, typename VT = double2>
 void launch_gather_small(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);
+// One output of a launch group, in launch order, as the all-column FP32 gather reads it.
+struct WideOut {
+    int32_t R, W, e0, e1;  // rows, block columns over all its segments, its segments [e0, e1)
+    int64_t out;           // the output's g_out
+    int64_t pad;
+};
 // STAGE_GATHER over complex-FP32 stores and arena for outputs of at most 32 rows, all a.b
-// right-hand sides in one launch (a.q0, a.bc unused): one warp per output, two columns per lane,
-// FP32 accumulation.
+// right-hand sides in one launch (a.q0, a.bc, a.g_rows, a.g_out, a.g_segptr unused; the outputs
+// come as WideOut records): a warp streams a sequence of outputs, two columns per lane, FP32
+// accumulation.
 bool gather_wide_fits(int maxrows);
-void launch_gather_wide(const RowArgs<float2> &a, const int32_t *nodes, int count, cudaStream_t s);
+// the register tile (rows) of the kernel instance that takes an output of R <= 32 rows: R rounded
+// up to even up to 24, then 28 or 32; a launch's outputs all have tile nr
+int wide_rows_class(int R);
+void launch_gather_wide(const RowArgs<float2> &a, const WideOut *outs, int count, int nr, cudaStream_t s);
 // STAGE_GATHER through the streaming kernel with vectors of type VT (launch_rows: VT = double2)
 template <typename S, typename VT>
 void launch_gather_rows(const RowArgs<S> &a, const int32_t *nodes, int count, cudaStream_t s);

@@ -184,6 +184,11 @@ struct GatherStage {
     std::vector<double> group_work;  // mean block entries per output of each group
     DBuf<int32_t> outputs, rows, segptr, w;
     DBuf<int64_t> out, moff, voff;
+    DBuf<WideOut> wout;  // the outputs in launch order as records (all-column FP32 gathers)
+    // launches of the all-column FP32 kernel: group g's are [wide_gptr[g], wide_gptr[g + 1]), each
+    // wide_count outputs from position wide_begin with the register tile wide_nr
+    std::vector<int32_t> wide_gptr, wide_begin, wide_count;
+    std::vector<int> wide_nr;
     DBuf<double2> M;
     DBuf<float2> M32;
     DBuf<double2> dM;     // d/dk of the store (frozen skeleton), prepared on demand
@@ -1178,8 +1183,29 @@ struct StageBuilder {
         group_maxrows.push_back(std::max(cur_max, 1));
         cur_max = 0;
     }
+    // one line per launch group on stderr: outputs, largest and mean output rows, segments and
+    // vector rows per output, block entries
+    void print_stats(const char *tag) const {
+        for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
+            const int32_t b = group_ptr[g], e = group_ptr[g + 1];
+            int64_t R = 0, nseg = 0, vrows = 0, ent = 0;
+            for (int32_t i = b; i < e; ++i) {
+                R += rows[i];
+                nseg += segptr[i + 1] - segptr[i];
+                for (int32_t k = segptr[i]; k < segptr[i + 1]; ++k) vrows += w[k];
+                ent += work[i];
+            }
+            const double n = double(std::max(e - b, 1));
+            fprintf(stderr,
+                    "nca stats %-10s group %2zu: %8d outputs, rows max %3d mean %6.2f, segments %6.2f, "
+                    "vector rows %8.2f, entries %12lld, work %8.1f\n",
+                    tag, g, e - b, group_maxrows[g], double(R) / n, double(nseg) / n, double(vrows) / n,
+                    (long long)ent, group_work[g]);
+        }
+    }
     // uploads the plan; with a source, allocates the stage store and copies its blocks
-    void finish(GatherStage &G, const double2 *src, cudaStream_t s) {
+    void finish(GatherStage &G, const double2 *src, cudaStream_t s, const char *tag = nullptr) {
+        if (tag && getenv("NCA_DIR_STATS")) print_stats(tag);
         // outputs of each group largest work first (shorter tail of the last wave): a stable
         // counting sort on the work, linear in the outputs
         std::vector<int32_t> order(rows.size());
@@ -1194,10 +1220,47 @@ struct StageBuilder {
             for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
             for (int32_t i = b; i < e; ++i) order[size_t(b + cnt[size_t(wmax - work[i])]++)] = i;
         }
+        // within a group whose outputs the all-column FP32 kernel can take, outputs of one row
+        // class (the kernel's register tile) are contiguous, largest work first inside a class:
+        // one launch per class
+        G.wide_gptr.assign(1, 0);
+        G.wide_begin.clear();
+        G.wide_count.clear();
+        G.wide_nr.clear();
+        std::vector<int32_t> tmp;
+        for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
+            const int32_t b = group_ptr[g], e = group_ptr[g + 1];
+            if (e > b && gather_wide_fits(group_maxrows[g])) {
+                std::vector<int32_t> ccount(34, 0);
+                for (int32_t i = b; i < e; ++i) ++ccount[size_t(wide_rows_class(rows[order[i]]))];
+                std::vector<int32_t> start(34, 0);
+                int32_t acc = 0;
+                for (int c = 0; c < 34; ++c) {
+                    start[c] = acc;
+                    if (ccount[c]) {
+                        G.wide_begin.push_back(b + acc);
+                        G.wide_count.push_back(ccount[c]);
+                        G.wide_nr.push_back(c);
+                    }
+                    acc += ccount[c];
+                }
+                tmp.assign(order.begin() + b, order.begin() + e);
+                for (int32_t o : tmp) order[size_t(b + start[size_t(wide_rows_class(rows[o]))]++)] = o;
+            }
+            G.wide_gptr.push_back(int32_t(G.wide_begin.size()));
+        }
         G.group_ptr = group_ptr;
         G.group_maxrows = group_maxrows;
         G.group_work = group_work;
         G.outputs.upload(order, s);
+        std::vector<WideOut> rec(order.size());
+        for (size_t i = 0; i < order.size(); ++i) {
+            const int32_t o = order[i];
+            int32_t W = 0;
+            for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
+            rec[i] = WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], 0};
+        }
+        G.wout.upload(rec, s);
         G.rows.upload(rows, s);
         G.out.upload(out, s);
         G.segptr.upload(segptr, s);
@@ -1302,6 +1365,7 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
         farpts[it] = int32_t(std::min<int64_t>(n, maxrank));
     }
     const std::vector<double> centroid = cluster_centroids(T, ownpts);
+    timer.mark(side + "item far fields listed (" + std::to_string(ffnodes.size()) + " far nodes)");
     DBuf<int64_t> dffptr;
     DBuf<int32_t> dffnodes;
     DBuf<double> dcent, dcenter;
@@ -1422,6 +1486,7 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
         if (st[0] == 3) throw Failure(NCA_ERR_CUDA, "internal: tree mimicry ran out of far points");
         CK(cudaMemcpyAsync(hrank.p, drk.p, sizeof(int32_t) * 2 * nl, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
+        timer.mark(side + "level " + std::to_string(lev) + " IACA done");
         const int32_t *rk = hrank.p, *nr = hrank.p + nl;
         // compact this level: exact m x r blocks, back to back (one copy per item, rank-0 items
         // copy nothing; sources, rows and columns straight from the positional arrays)
@@ -1709,7 +1774,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 }
                 B.end_group();
             }
-            B.finish(pr.up, di.XT.p, s);
+            timer.mark("gather plan " + std::to_string(task) + ": up listed");
+            B.finish(pr.up, di.XT.p, s, m ? "T up" : "N up");
             timer.mark("gather plan " + std::to_string(task) + ": up");
         }
         // coupling: output-side items with a rank and their far pairs' blocks (store built above)
@@ -1742,7 +1808,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 B.end_output();
             }
             B.end_group();
-            B.finish(pr.couple, nullptr, s);
+            timer.mark("gather plan " + std::to_string(task) + ": coupling listed");
+            B.finish(pr.couple, nullptr, s, m ? "T coupling" : "N coupling");
             timer.mark("gather plan " + std::to_string(task) + ": coupling");
         }
         // down: output-side items gather from the parent items that map onto them, root level first
@@ -1787,7 +1854,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 }
                 B.end_group();
             }
-            B.finish(pr.down, dout.X.p, s);
+            timer.mark("gather plan " + std::to_string(task) + ": down listed");
+            B.finish(pr.down, dout.X.p, s, m ? "T down" : "N down");
             timer.mark("gather plan " + std::to_string(task) + ": down");
         }
         // leaves: every basis item whose cluster contains the leaf, then the near blocks
@@ -1815,7 +1883,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 B.end_output();
             }
             B.end_group();
-            B.finish(pr.leaves, dout.X.p, s);
+            timer.mark("gather plan " + std::to_string(task) + ": leaves listed");
+            B.finish(pr.leaves, dout.X.p, s, m ? "T leaves" : "N leaves");
             timer.mark("gather plan " + std::to_string(task) + ": leaves");
         }
         CK(cudaStreamSynchronize(s));
@@ -2351,9 +2420,11 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
                 const bool small = G.group_work[g] < 8192.0;
                 if constexpr (!f64) {
                     if (b >= 2 && small && gather_wide_fits(a.maxrows)) {
-                        launch_gather_wide(a, G.outputs.p + G.group_ptr[g], cnt, s);
-                        ++count.total;
-                        ++count.stage[sk];
+                        for (int32_t k = G.wide_gptr[g]; k < G.wide_gptr[g + 1]; ++k) {
+                            launch_gather_wide(a, G.wout.p + G.wide_begin[k], G.wide_count[k], G.wide_nr[k], s);
+                            ++count.total;
+                            ++count.stage[sk];
+                        }
                         continue;
                     }
                 }

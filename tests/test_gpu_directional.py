@@ -96,9 +96,10 @@ def test_directional_against_oracle(name, make, k, tol, minvalues):
     rows = np.arange(0, nt, max(1, nt // 200))
     ref = O.dense_rows(O.Kernel(O.KIND_HELMHOLTZ, k=k, rmin=1e-12), test, trial, rows, x)
     assert relerr((A @ x)[rows], ref) < 10 * tol
-    # complex-FP32 stores and coefficient arena: one column, an odd block, and an odd last pass
+    # complex-FP32 stores and coefficient arena: one column, an odd block, an odd last pass, and
+    # blocks whose columns leave lanes idle or take a second pass of the all-column kernel
     W = N.H2Workspace(N.core(A), np.complex64)
-    for b in (1, 5, 8, 17):
+    for b in (1, 5, 8, 17, 67, 100, 130):
         X = cgauss((ns, b), 30 + b)
         assert relerr(W @ X, A @ X) < 1e-5, b
         U = cgauss((nt, b), 40 + b)
