@@ -630,6 +630,13 @@ def run_wideband(args):
     X = rhs(n, nvec, seed=31)
     Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(dev)  # column-major n x 100
     Yd = torch.zeros_like(Xd)
+    # an untimed build first: the process's one-time costs (device memory pools, host pages, the
+    # planning threads' first start) fall on neither timed build
+    warm, _ = wideband_core(N, pts, k, local, False)
+    del warm
+    import gc
+    gc.collect()
+    torch.cuda.synchronize()
     # plain FP64 form: FP64-only build, then 100 single-vector FP64 matvecs
     core, build_plain = wideband_core(N, pts, k, local, False)
     W64 = N.H2Workspace(core, max_nrhs=1)

@@ -834,10 +834,10 @@ constexpr int WIDE_WARPS = 4;  // warps (independent output sequences) per CTA
 constexpr int WIDE_J = 8;      // (block column, vector row) pairs per chunk
 constexpr int WIDE_SLOTS = 3;  // chunks per warp's ring
 
-template <int NR>
+template <int NR, int CPL>
 struct WideShape {
     static constexpr int mslot = NR * WIDE_J;        // float2 entries of a chunk's block columns
-    static constexpr int vslot = WIDE_J * 32 * 2;    // float2 entries of a chunk's vector rows
+    static constexpr int vslot = WIDE_J * 32 * CPL;  // float2 entries of a chunk's vector rows
     static constexpr int slot = mslot + vslot;
     static constexpr size_t smem = size_t(WIDE_WARPS) * WIDE_SLOTS * slot * sizeof(float2);
 };
@@ -853,7 +853,7 @@ __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
 }
 
 __device__ __forceinline__ WideOut wide_record(const WideOut *outs, int i, int count) {
-    WideOut o{0, 0, 0, 0, 0, 0};
+    WideOut o{0, 0, 0, 0, 0, 0, 0};
     if (i < count) {
         const int4 *q = reinterpret_cast<const int4 *>(outs + i);
         const int4 u = __ldg(q), v = __ldg(q + 1);
@@ -862,6 +862,8 @@ __device__ __forceinline__ WideOut wide_record(const WideOut *outs, int i, int c
         o.e0 = u.z;
         o.e1 = u.w;
         o.out = int64_t((uint64_t(uint32_t(v.y)) << 32) | uint32_t(v.x));
+        o.ld = v.z;
+        o.r0 = v.w;
     }
     return o;
 }
@@ -882,10 +884,10 @@ __device__ __forceinline__ WideSeg wide_segs(const RowArgs<float2> &a, int base,
     return g;
 }
 
-template <int NR, bool CONJ>
-__global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 2)
+template <int NR, int CPL, bool CONJ>
+__global__ void __launch_bounds__(WIDE_WARPS * 32, CPL == 4 ? 2 : NR <= 8 ? 4 : NR <= 20 ? 3 : 2)
     k_gather_wide(RowArgs<float2> a, const WideOut *outs, int count) {
-    using Shape = WideShape<NR>;
+    using Shape = WideShape<NR, CPL>;
     extern __shared__ __align__(16) float2 wsm[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     float2 *ring = wsm + size_t(wib) * WIDE_SLOTS * Shape::slot;
@@ -919,7 +921,7 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 
     auto issue = [&](int q) {
         // skip the (output, pass) steps whose pairs are all issued
         while (pwi < count && pt >= pc.W) {
-            pc0 += 64;
+            pc0 += 32 * CPL;
             pt = 0;
             pj = 0;
             pe = pc.e0;
@@ -940,8 +942,8 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 
             const int jn = min(WIDE_J, pc.W - pt);
             float2 *Ms = ring + q * Shape::slot;
             float2 *Vs = Ms + Shape::mslot;
-            const int col = pc0 + 2 * lane;
-            const int ncol = col < a.b ? min(2, a.b - col) : 0;
+            const int col = pc0 + CPL * lane;
+            const int ncol = col < a.b ? min(CPL, a.b - col) : 0;
             const int R = pc.R;
             for (int jj = 0; jj < jn; ++jj) {
                 while (pj >= pw) {
@@ -949,12 +951,15 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 
                     pj = 0;
                     seg_at(pe, pw, pM, pvb);
                 }
-                if (lane < R) cp_async8(Ms + jj * NR + lane, pM + int64_t(pj) * R + lane);
+                if (lane < R) cp_async8(Ms + jj * NR + lane, pM + int64_t(pj) * pc.ld + pc.r0 + lane);
                 const float2 *v = a.src32 + (pvb + pj) * a.vs + col;
-                if (ncol == 2)
-                    cp_async16(Vs + (jj * 32 + lane) * 2, v);
-                else if (ncol == 1)
-                    cp_async8(Vs + (jj * 32 + lane) * 2, v);
+                float2 *d = Vs + (jj * 32 + lane) * CPL;
+                if (ncol == CPL) {
+#pragma unroll
+                    for (int c = 0; c < CPL; c += 2) cp_async16(d + c, v + c);
+                } else {
+                    for (int c = 0; c < ncol; ++c) cp_async8(d + c, v + c);
+                }
                 ++pj;
             }
             pt += jn;
@@ -971,12 +976,14 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 
         const int64_t gout = cc.out;
         cc = cn;
         cn = wide_record(outs, wi + 2 * nw, count);
-        for (int c0 = 0; c0 < a.b; c0 += 64) {
-            const int col = c0 + 2 * lane;
-            const int ncol = col < a.b ? min(2, a.b - col) : 0;
-            float2 acc[NR][2];
+        for (int c0 = 0; c0 < a.b; c0 += 32 * CPL) {
+            const int col = c0 + CPL * lane;
+            const int ncol = col < a.b ? min(CPL, a.b - col) : 0;
+            float2 acc[NR][CPL];
 #pragma unroll
-            for (int r = 0; r < NR; ++r) acc[r][0] = acc[r][1] = make_float2(0.f, 0.f);
+            for (int r = 0; r < NR; ++r)
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) acc[r][c] = make_float2(0.f, 0.f);
             for (int t = 0; t < W; t += WIDE_J) {
                 const int jn = min(WIDE_J, W - t);
                 issue(qp);
@@ -984,13 +991,20 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 
                 cp_async_wait<WIDE_SLOTS - 1>();
                 __syncwarp();
                 const float2 *Ms = ring + qc * Shape::slot;
-                const float4 *Vs = reinterpret_cast<const float4 *>(Ms + Shape::mslot) + lane;
-                float4 xn = Vs[0];
+                // lane's CPL columns of pair jj: float4 jj * 16 CPL + lane CPL / 2 + c
+                const float4 *Vs = reinterpret_cast<const float4 *>(Ms + Shape::mslot) + lane * (CPL / 2);
+                float4 xn[CPL / 2];
+#pragma unroll
+                for (int c = 0; c < CPL / 2; ++c) xn[c] = Vs[c];
 #pragma unroll 1
                 for (int jj = 0; jj < jn; ++jj) {
-                    // this pair's vector columns; the next pair's load issued before the FMAs
-                    const float4 x = xn;
-                    xn = Vs[min(jj + 1, WIDE_J - 1) * 32];
+                    // this pair's vector columns; the next pair's loads issued before the FMAs
+                    float4 x[CPL / 2];
+#pragma unroll
+                    for (int c = 0; c < CPL / 2; ++c) {
+                        x[c] = xn[c];
+                        xn[c] = Vs[min(jj + 1, WIDE_J - 1) * 16 * CPL + c];
+                    }
                     const float4 *Mj = reinterpret_cast<const float4 *>(Ms + jj * NR);
 #pragma unroll
                     for (int r2 = 0; r2 < NR / 2; ++r2) {
@@ -998,11 +1012,14 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
                             const float mx = h ? m2.z : m2.x, my = CONJ ? -(h ? m2.w : m2.y) : (h ? m2.w : m2.y);
-                            float2 &p0 = acc[2 * r2 + h][0], &p1 = acc[2 * r2 + h][1];
-                            p0.x = fmaf(mx, x.x, fmaf(-my, x.y, p0.x));
-                            p0.y = fmaf(mx, x.y, fmaf(my, x.x, p0.y));
-                            p1.x = fmaf(mx, x.z, fmaf(-my, x.w, p1.x));
-                            p1.y = fmaf(mx, x.w, fmaf(my, x.z, p1.y));
+#pragma unroll
+                            for (int c = 0; c < CPL / 2; ++c) {
+                                float2 &p0 = acc[2 * r2 + h][2 * c], &p1 = acc[2 * r2 + h][2 * c + 1];
+                                p0.x = fmaf(mx, x[c].x, fmaf(-my, x[c].y, p0.x));
+                                p0.y = fmaf(mx, x[c].y, fmaf(my, x[c].x, p0.y));
+                                p1.x = fmaf(mx, x[c].z, fmaf(-my, x[c].w, p1.x));
+                                p1.y = fmaf(mx, x[c].w, fmaf(my, x[c].z, p1.y));
+                            }
                         }
                     }
                 }
@@ -1016,7 +1033,7 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 
                 if (scatter) {
                     const int64_t yr = a.perm[gout + r];
 #pragma unroll
-                    for (int c = 0; c < 2; ++c) {
+                    for (int c = 0; c < CPL; ++c) {
                         if (c >= ncol) break;
                         const float2 v = acc[r][c];
                         double2 *yp = a.y + yr + int64_t(col + c) * a.ldy;
@@ -1031,7 +1048,7 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 
                 } else {
                     float2 *d = a.dst32 + (gout + r) * a.vs + col;
 #pragma unroll
-                    for (int c = 0; c < 2; ++c) {
+                    for (int c = 0; c < CPL; ++c) {
                         if (c >= ncol) break;
                         float2 v = acc[r][c];
                         if (a.accumulate) {
@@ -1047,23 +1064,35 @@ __global__ void __launch_bounds__(WIDE_WARPS * 32, NR <= 8 ? 4 : NR <= 20 ? 3 : 
     cp_async_wait<0>();
 }
 
-template <int NR, bool CONJ>
+template <int NR, int CPL, bool CONJ>
 void wide_launch(const RowArgs<float2> &a, const WideOut *outs, int count, cudaStream_t s, int sms) {
-    const size_t sm = WideShape<NR>::smem;
-    cudaFuncSetAttribute(k_gather_wide<NR, CONJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+    const size_t sm = WideShape<NR, CPL>::smem;
+    auto kern = k_gather_wide<NR, CPL, CONJ>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather_wide<NR, CONJ>, WIDE_WARPS * 32, sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WIDE_WARPS * 32, sm);
     const int need = (count + WIDE_WARPS - 1) / WIDE_WARPS;
     const int cap = sms * (per_sm > 0 ? per_sm : 1);
-    k_gather_wide<NR, CONJ><<<need < cap ? need : cap, WIDE_WARPS * 32, sm, s>>>(a, outs, count);
+    kern<<<need < cap ? need : cap, WIDE_WARPS * 32, sm, s>>>(a, outs, count);
 }
 
+// four columns per lane (one pass over up to 128 right-hand sides) for tiles of up to 12 rows when
+// the block has more than 64 columns; two otherwise
 template <int NR>
 void wide_launch(const RowArgs<float2> &a, const WideOut *outs, int count, cudaStream_t s, int sms) {
+    if constexpr (NR <= 12) {
+        if (a.b > 64) {
+            if (a.conj)
+                wide_launch<NR, 4, true>(a, outs, count, s, sms);
+            else
+                wide_launch<NR, 4, false>(a, outs, count, s, sms);
+            return;
+        }
+    }
     if (a.conj)
-        wide_launch<NR, true>(a, outs, count, s, sms);
+        wide_launch<NR, 2, true>(a, outs, count, s, sms);
     else
-        wide_launch<NR, false>(a, outs, count, s, sms);
+        wide_launch<NR, 2, false>(a, outs, count, s, sms);
 }
 }  // namespace
 

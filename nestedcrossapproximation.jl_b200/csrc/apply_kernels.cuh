@@ -85,8 +85,9 @@ void launch_gather_small(const RowArgs<S> &a, const int32_t *nodes, int count, c
 // One output of a launch group, in launch order, as the all-column FP32 gather reads it.
 struct WideOut {
     int32_t R, W, e0, e1;  // rows, block columns over all its segments, its segments [e0, e1)
-    int64_t out;           // the output's g_out
-    int64_t pad;
+    int64_t out;           // position of the record's first row (the output's g_out + r0)
+    int32_t ld, r0;        // the output's blocks' leading dimension (its rows) and the record's
+                           // first row in them: an output of many rows is taken as row slices
 };
 // STAGE_GATHER over complex-FP32 stores and arena for outputs of at most 32 rows, all a.b
 // right-hand sides in one launch (a.q0, a.bc, a.g_rows, a.g_out, a.g_segptr unused; the outputs

@@ -12,6 +12,7 @@
 #include <chrono>
 #include <cstring>
 #include <exception>
+#include <functional>
 #include <future>
 #include <memory>
 #include <mutex>
@@ -1123,6 +1124,12 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
 // onto one child direction, so the children gather), leaves (leaf <- every basis item whose
 // cluster contains it, and the near blocks).
 
+// launch groups of small outputs (mean block entries per output below this) run on the gather
+// kernels that keep a warp per output
+constexpr double kSmallGroupWork = 8192.0;
+// a launch group the all-column FP32 kernel takes (complex-FP32 products of two or more columns)
+bool wide_group(int maxrows, double work) { return work < kSmallGroupWork && gather_wide_fits(maxrows); }
+
 struct StageBuilder {
     std::vector<int32_t> group_ptr{0};
     std::vector<int> group_maxrows;
@@ -1204,7 +1211,8 @@ struct StageBuilder {
         }
     }
     // uploads the plan; with a source, allocates the stage store and copies its blocks
-    void finish(GatherStage &G, const double2 *src, cudaStream_t s, const char *tag = nullptr) {
+    void finish(GatherStage &G, const double2 *src, cudaStream_t s, const char *tag = nullptr,
+                const std::function<void(const std::string &)> &mark = {}) {
         if (tag && getenv("NCA_DIR_STATS")) print_stats(tag);
         // outputs of each group largest work first (shorter tail of the last wave): a stable
         // counting sort on the work, linear in the outputs
@@ -1220,46 +1228,53 @@ struct StageBuilder {
             for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
             for (int32_t i = b; i < e; ++i) order[size_t(b + cnt[size_t(wmax - work[i])]++)] = i;
         }
-        // within a group whose outputs the all-column FP32 kernel can take, outputs of one row
-        // class (the kernel's register tile) are contiguous, largest work first inside a class:
-        // one launch per class
+        // Records of the all-column FP32 kernel (groups of small outputs): an output of more than
+        // WIDE_SLICE rows is taken as row slices of at most WIDE_SLICE rows (same segments, the
+        // vector rows read once per slice); inside a group the records of one row class (the
+        // kernel's register tile) are contiguous, largest work first inside a class: one launch
+        // per class
+        constexpr int WIDE_SLICE = 20;
         G.wide_gptr.assign(1, 0);
         G.wide_begin.clear();
         G.wide_count.clear();
         G.wide_nr.clear();
-        std::vector<int32_t> tmp;
+        std::vector<WideOut> rec;
+        rec.reserve(order.size());
+        std::vector<WideOut> grec;
         for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
             const int32_t b = group_ptr[g], e = group_ptr[g + 1];
-            if (e > b && gather_wide_fits(group_maxrows[g])) {
-                std::vector<int32_t> ccount(34, 0);
-                for (int32_t i = b; i < e; ++i) ++ccount[size_t(wide_rows_class(rows[order[i]]))];
-                std::vector<int32_t> start(34, 0);
-                int32_t acc = 0;
-                for (int c = 0; c < 34; ++c) {
-                    start[c] = acc;
-                    if (ccount[c]) {
-                        G.wide_begin.push_back(b + acc);
-                        G.wide_count.push_back(ccount[c]);
-                        G.wide_nr.push_back(c);
-                    }
-                    acc += ccount[c];
-                }
-                tmp.assign(order.begin() + b, order.begin() + e);
-                for (int32_t o : tmp) order[size_t(b + start[size_t(wide_rows_class(rows[o]))]++)] = o;
+            grec.clear();
+            for (int32_t i = wide_group(group_maxrows[g], group_work[g]) ? b : e; i < e; ++i) {
+                const int32_t o = order[i];
+                int32_t W = 0;
+                for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
+                const int32_t R = rows[o];
+                const int32_t ns = (R + WIDE_SLICE - 1) / WIDE_SLICE;
+                const int32_t rs = ns > 1 ? (R + ns - 1) / ns : R;
+                for (int32_t r0 = 0; r0 < std::max(R, 1); r0 += std::max(rs, 1))
+                    grec.push_back(WideOut{std::min(rs, R - r0), W, segptr[o], segptr[o + 1], out[o] + r0, R, r0});
             }
+            std::vector<int32_t> ccount(34, 0), start(34, 0);
+            for (const WideOut &r : grec) ++ccount[size_t(wide_rows_class(r.R))];
+            int32_t at = int32_t(rec.size());
+            for (int c = 0; c < 34; ++c) {
+                start[c] = at;
+                if (ccount[c]) {
+                    G.wide_begin.push_back(at);
+                    G.wide_count.push_back(ccount[c]);
+                    G.wide_nr.push_back(c);
+                }
+                at += ccount[c];
+            }
+            rec.resize(size_t(at));
+            for (const WideOut &r : grec) rec[size_t(start[size_t(wide_rows_class(r.R))]++)] = r;
             G.wide_gptr.push_back(int32_t(G.wide_begin.size()));
         }
         G.group_ptr = group_ptr;
         G.group_maxrows = group_maxrows;
         G.group_work = group_work;
+        if (mark) mark("records");
         G.outputs.upload(order, s);
-        std::vector<WideOut> rec(order.size());
-        for (size_t i = 0; i < order.size(); ++i) {
-            const int32_t o = order[i];
-            int32_t W = 0;
-            for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
-            rec[i] = WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], 0};
-        }
         G.wout.upload(rec, s);
         G.rows.upload(rows, s);
         G.out.upload(out, s);
@@ -1267,8 +1282,10 @@ struct StageBuilder {
         G.moff.upload(moff, s);
         G.w.upload(w, s);
         G.voff.upload(voff, s);
+        if (mark) mark("plan uploaded");
         if (!src) return;
         G.M.alloc(size_t(store));
+        if (mark) mark("store allocated");
         G.entries = 0;
         for (size_t i = 0; i < crows.size(); ++i) G.entries += int64_t(crows[i]) * ccols[i];
         G.ncopies = int64_t(crows.size());
@@ -1460,7 +1477,11 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
             throw Failure(NCA_ERR_ARG, "a basis item has " + std::to_string(mc) +
                                            " rows; the IACA kernel holds at most " +
                                            std::to_string(nca::iaca_max_rows()) + " (reduce the leaf size)");
-        if (!chunk.p || size_t(bound) > chunk.n) chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
+        if (!chunk.p || size_t(bound) > chunk.n) {
+            chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
+            timer.mark(side + "level " + std::to_string(lev) + " scratch of " + std::to_string(bound >> 16) +
+                       " x 1 MiB allocated");
+        }
         upload_reuse(dlvoff, lvoff, s);
         upload_reuse(nodes, items, s);
         const int nl = int(items.size());
@@ -1569,17 +1590,82 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         }
     } eg{ev0, ev1};
     CK(cudaEventRecord(ev0, s));
+    // The near field depends on the trees and the partition only: it is built on a thread and
+    // stream of its own while the sides plan their directions and compress (its offsets feed the
+    // leaf plans).
+    cudaStream_t s2;
+    CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+    StreamGuard sg2{s2};
+    std::vector<int64_t> h_ntoff;
+    int64_t near_entries = 0;
+    std::future<void> near_job = std::async(std::launch::async, [&]() {
+        CK(cudaSetDevice(c->device));
+        near_entries = build_near(c, s2, &h_ntoff);
+        CK(cudaStreamSynchronize(s2));
+        timer.mark("near field built");
+    });
+    // The far pairs matched across the two sides' directional plans (which items a pair couples,
+    // where its transpose sits) need the plans only: matched on a thread of their own while the
+    // sides compress. The couplings then only add the ranks.
+    std::promise<void> planned[2];
+    std::shared_future<void> planned_f[2] = {planned[0].get_future().share(), planned[1].get_future().share()};
+    std::vector<int32_t> pair_it, pair_is, pair_of_pos;
+    std::future<void> pairs_job = std::async(std::launch::async, [&]() {
+        planned_f[0].get();
+        planned_f[1].get();
+        const nca::DirSide &pt = D->side[0].plan, &ps = D->side[1].plan;
+        // far pairs (test CSR grouped by test direction) and their items on both sides
+        std::vector<int32_t> item_of_pos[2];
+        for (int sd = 0; sd < 2; ++sd) {
+            const nca::DirSide &pl = D->side[sd].plan;
+            item_of_pos[sd].assign(pl.farnodes.size(), -1);
+            for (size_t it = 0; it < pl.item_node.size(); ++it)
+                for (int q = pl.dirfarptr[it]; q < pl.dirfarptr[it + 1]; ++q) item_of_pos[sd][q] = int32_t(it);
+        }
+        // (trial node, test node) -> position in the trial far lists: each trial node's list sorted by
+        // test node and searched by bisection
+        std::vector<std::pair<int32_t, int32_t>> bytest(ps.farnodes.size());
+        for (int sn = 0; sn < c->tree[1].nnodes; ++sn) {
+            for (int q = ps.farptr[sn]; q < ps.farptr[sn + 1]; ++q) bytest[q] = {ps.farnodes[q], q};
+            std::sort(bytest.begin() + ps.farptr[sn], bytest.begin() + ps.farptr[sn + 1]);
+        }
+        auto trialpos = [&](int sn, int t) {
+            const auto b = bytest.begin() + ps.farptr[sn], e = bytest.begin() + ps.farptr[sn + 1];
+            const auto it = std::lower_bound(b, e, std::make_pair(int32_t(t), INT32_MIN));
+            if (it == e || it->first != t) throw Failure(NCA_ERR_ARG, "internal: a far pair has no transpose");
+            return it->second;
+        };
+        const int64_t np = int64_t(pt.farnodes.size());
+        pair_it.assign(np, 0);
+        pair_is.assign(np, 0);
+        pair_of_pos.assign(ps.farnodes.size(), -1);
+        for (int t = 0; t < c->tree[0].nnodes; ++t)
+            for (int e = pt.farptr[t]; e < pt.farptr[t + 1]; ++e) {
+                const int sn = pt.farnodes[e];
+                const int32_t q = trialpos(sn, t);
+                pair_it[e] = item_of_pos[0][e];
+                pair_is[e] = item_of_pos[1][q];
+                pair_of_pos[q] = e;
+            }
+        timer.mark("far pairs matched");
+    });
     std::vector<std::vector<int32_t>> bylevel[2];  // items per level, filled by each side's task
     int64_t basis_entries[2] = {0, 0}, transfer_entries[2] = {0, 0};
     on_threads(c->device, 2, [&](int sd) {
         const cudaStream_t s = ss[sd];
         DirItems &d = D->side[sd];
         const std::string side = sd == 0 ? "test: " : "trial: ";
-        if (sv)
-            d.plan = sv->side[sd].plan;
-        else
-            d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
-                                      sd == 0 ? P.farnodes : P.tfarnodes, wb);
+        try {
+            if (sv)
+                d.plan = sv->side[sd].plan;
+            else
+                d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
+                                          sd == 0 ? P.farnodes : P.tfarnodes, wb);
+        } catch (...) {
+            planned[sd].set_exception(std::current_exception());
+            throw;
+        }
+        planned[sd].set_value();
         timer.mark(side + "directional plan (" + std::to_string(d.plan.item_node.size()) + " items)");
         const nca::DirSide &pl = d.plan;
         const nca::Tree &T = c->tree[sd];
@@ -1619,51 +1705,16 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         timer.mark(side + "bases joined and transposed");
     });
     auto h1 = std::chrono::steady_clock::now();
-    // near field first (its offsets feed the leaf plans); its kernels run on stream s
-    std::vector<int64_t> h_ntoff;
-    const int64_t near_entries = build_near(c, s, &h_ntoff);
-    timer.mark("near field launched");
-    // couplings: prepared on the host by the thread of the forward coupling plan (the transposed
-    // coupling plan waits for it) and computed on stream s while the other plans are built; their
-    // device inputs stay alive until s is synchronised
+    near_job.get();
+    pairs_job.get();
+    // couplings: computed by the thread of the forward coupling plan (the transposed coupling plan
+    // waits for it) on stream s while the other plans are built; their device inputs stay alive
+    // until s is synchronised
     const nca::DirSide &pt = D->side[0].plan, &ps = D->side[1].plan;
     const int64_t npairs = int64_t(pt.farnodes.size());
-    std::vector<int32_t> pair_it, pair_is, pair_of_pos;
     std::vector<int64_t> cfoff, ctoff;
     int64_t coupling_entries = 0;
     auto couplings = [&]() {
-        // far pairs (test CSR grouped by test direction) and their items on both sides
-        std::vector<int32_t> item_of_pos[2];
-        for (int sd = 0; sd < 2; ++sd) {
-            const nca::DirSide &pl = D->side[sd].plan;
-            item_of_pos[sd].assign(pl.farnodes.size(), -1);
-            for (size_t it = 0; it < pl.item_node.size(); ++it)
-                for (int q = pl.dirfarptr[it]; q < pl.dirfarptr[it + 1]; ++q) item_of_pos[sd][q] = int32_t(it);
-        }
-        // (trial node, test node) -> position in the trial far lists: each trial node's list sorted by
-        // test node and searched by bisection
-        std::vector<std::pair<int32_t, int32_t>> bytest(ps.farnodes.size());
-        for (int sn = 0; sn < c->tree[1].nnodes; ++sn) {
-            for (int q = ps.farptr[sn]; q < ps.farptr[sn + 1]; ++q) bytest[q] = {ps.farnodes[q], q};
-            std::sort(bytest.begin() + ps.farptr[sn], bytest.begin() + ps.farptr[sn + 1]);
-        }
-        auto trialpos = [&](int sn, int t) {
-            const auto b = bytest.begin() + ps.farptr[sn], e = bytest.begin() + ps.farptr[sn + 1];
-            const auto it = std::lower_bound(b, e, std::make_pair(int32_t(t), INT32_MIN));
-            if (it == e || it->first != t) throw Failure(NCA_ERR_ARG, "internal: a far pair has no transpose");
-            return it->second;
-        };
-        pair_it.assign(npairs, 0);
-        pair_is.assign(npairs, 0);
-        pair_of_pos.assign(ps.farnodes.size(), -1);
-        for (int t = 0; t < c->tree[0].nnodes; ++t)
-            for (int e = pt.farptr[t]; e < pt.farptr[t + 1]; ++e) {
-                const int sn = pt.farnodes[e];
-                const int32_t q = trialpos(sn, t);
-                pair_it[e] = item_of_pos[0][e];
-                pair_is[e] = item_of_pos[1][q];
-                pair_of_pos[q] = e;
-            }
         const std::vector<int32_t> &rt = D->side[0].h_rank, &rs = D->side[1].h_rank;
         // coupling blocks S_e = K[tau_(t, dt), tau_(s, ds)] in test pair order, transposes in trial order
         cfoff.assign(npairs + 1, 0);
@@ -1741,6 +1792,11 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     } tsg{ts};
     on_threads(c->device, 8, [&](int task) {
         const cudaStream_t s = ts[task];
+        auto plan_mark = [&timer, task](const char *stage) {
+            return [&timer, task, stage](const std::string &what) {
+                timer.mark("gather plan " + std::to_string(task) + ": " + stage + " " + what);
+            };
+        };
         const int m = task / 4, stage = task % 4;
         const int I = m == 0 ? 1 : 0, O = 1 - I;
         const DirItems &di = D->side[I], &dout = D->side[O];
@@ -1775,7 +1831,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 B.end_group();
             }
             timer.mark("gather plan " + std::to_string(task) + ": up listed");
-            B.finish(pr.up, di.XT.p, s, m ? "T up" : "N up");
+            B.finish(pr.up, di.XT.p, s, m ? "T up" : "N up", plan_mark("up"));
             timer.mark("gather plan " + std::to_string(task) + ": up");
         }
         // coupling: output-side items with a rank and their far pairs' blocks (store built above)
@@ -1809,7 +1865,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             }
             B.end_group();
             timer.mark("gather plan " + std::to_string(task) + ": coupling listed");
-            B.finish(pr.couple, nullptr, s, m ? "T coupling" : "N coupling");
+            B.finish(pr.couple, nullptr, s, m ? "T coupling" : "N coupling", plan_mark("coupling"));
             timer.mark("gather plan " + std::to_string(task) + ": coupling");
         }
         // down: output-side items gather from the parent items that map onto them, root level first
@@ -1855,7 +1911,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 B.end_group();
             }
             timer.mark("gather plan " + std::to_string(task) + ": down listed");
-            B.finish(pr.down, dout.X.p, s, m ? "T down" : "N down");
+            B.finish(pr.down, dout.X.p, s, m ? "T down" : "N down", plan_mark("down"));
             timer.mark("gather plan " + std::to_string(task) + ": down");
         }
         // leaves: every basis item whose cluster contains the leaf, then the near blocks
@@ -1884,14 +1940,16 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             }
             B.end_group();
             timer.mark("gather plan " + std::to_string(task) + ": leaves listed");
-            B.finish(pr.leaves, dout.X.p, s, m ? "T leaves" : "N leaves");
+            B.finish(pr.leaves, dout.X.p, s, m ? "T leaves" : "N leaves", plan_mark("leaves"));
             timer.mark("gather plan " + std::to_string(task) + ": leaves");
         }
         CK(cudaStreamSynchronize(s));
     });
     CK(cudaStreamSynchronize(s));
+    timer.mark("gather plans done");
     // the stage stores hold the products' copies of the operators; X stays for nca_core_save
     for (DirItems &d : D->side) d.XT.release();
+    timer.mark("transposed bases released");
     if (c->f32) {
         auto down = [&](DBuf<double2> &src, DBuf<float2> &dst) {
             dst.alloc(src.n);
@@ -2417,9 +2475,9 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
                 a.conj = conj;
                 a.maxrows = G.group_maxrows[g];
                 a.error = error;
-                const bool small = G.group_work[g] < 8192.0;
+                const bool small = G.group_work[g] < kSmallGroupWork;
                 if constexpr (!f64) {
-                    if (b >= 2 && small && gather_wide_fits(a.maxrows)) {
+                    if (b >= 2 && wide_group(a.maxrows, G.group_work[g])) {
                         for (int32_t k = G.wide_gptr[g]; k < G.wide_gptr[g + 1]; ++k) {
                             launch_gather_wide(a, G.wout.p + G.wide_begin[k], G.wide_count[k], G.wide_nr[k], s);
                             ++count.total;
@@ -2513,9 +2571,9 @@ int enqueue_dir_tangent(nca_core *c, const double2 *xd, int64_t lx, double2 *yd,
             a.conj = false;
             a.maxrows = G.group_maxrows[g];
             a.error = error;
-            if (G.group_work[g] < 8192.0 && gather_tiny_fits(a.maxrows, bc))
+            if (G.group_work[g] < kSmallGroupWork && gather_tiny_fits(a.maxrows, bc))
                 launch_gather_tiny<double2, double2>(a, G.outputs.p + G.group_ptr[g], cnt, s);
-            else if (a.maxrows <= 64 && G.group_work[g] < 8192.0)
+            else if (a.maxrows <= 64 && G.group_work[g] < kSmallGroupWork)
                 launch_gather_small<double2, double2>(a, G.outputs.p + G.group_ptr[g], cnt, s);
             else
                 launch_gather_rows<double2, double2>(a, G.outputs.p + G.group_ptr[g], cnt, s);
