@@ -56,6 +56,9 @@ def parse():
     p.add_argument("--wideband-points", type=int, default=0, help="point count of the wideband workload")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-stages", action="store_true", help="print per-stage times to stderr")
+    p.add_argument("--profile-run", action="store_true",
+                   help="wideband workload for profiler captures: one mixed-precision build and `steps` block "
+                        "products, no plain arm, no CPU baseline; prints build and stage times")
     p.add_argument("--clocks-csv", default=None, help="file for the nvidia-smi clock samples (default: a temp file)")
     p.add_argument("--workload", default="wideband",
                    choices=["wideband", "galerkin-sphere", "batched-uneven", "gradients"],
@@ -614,6 +617,31 @@ def dir_stage_bytes(info, b, e):
     return e * xe + e * info["coupling_entries"] + e * info["near_entries"]
 
 
+def profile_wideband(args, N, L, pts, k, local, n, nvec, Xd, Yd):
+    """--profile-run: the batched mixed form's build and `steps` block products of 100 columns
+    (after `warmup` untimed ones), with the library's stage events; one JSON line. The command
+    that the committed profiler summaries run."""
+    import torch
+    core, build = wideband_core(N, pts, k, local, True)
+    W = N.H2Workspace(core, np.complex64, max_nrhs=16)
+    W.set_profiling(True)
+    names = ["gather", "up", "coupling", "down", "near", "leaves"]
+    total = [0.0] * 6
+    for i in range(args.warmup + args.steps):
+        N._lib.check(L.nca_apply(W._h, 0, 1, C.c_void_p(Xd.data_ptr()), n, C.c_void_p(Yd.data_ptr()), n, nvec,
+                                 1.0, 0.0, 0.0, 0.0, 1))
+        torch.cuda.synchronize()
+        sec = (C.c_double * 6)()
+        cnt = (C.c_int32 * 6)()
+        L.nca_workspace_stage_times(W._h, sec, cnt, 6)
+        if i >= args.warmup:
+            for q in range(6):
+                total[q] += sec[q]
+    steps = max(args.steps, 1)
+    print(json.dumps({"profile_run": WIDEBAND.format(n=n), "build_s": build,
+                      "stage_ms_per_step": {names[q]: 1e3 * total[q] / steps for q in range(6)}}), flush=True)
+
+
 def run_wideband(args):
     """The headline workload (see the module docstring)."""
     import torch
@@ -630,6 +658,8 @@ def run_wideband(args):
     X = rhs(n, nvec, seed=31)
     Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(dev)  # column-major n x 100
     Yd = torch.zeros_like(Xd)
+    if args.profile_run:
+        return profile_wideband(args, N, L, pts, k, local, n, nvec, Xd, Yd)
     # an untimed build first: the process's one-time costs (device memory pools, host pages, the
     # planning threads' first start) fall on neither timed build
     warm, _ = wideband_core(N, pts, k, local, False)
@@ -719,7 +749,7 @@ def run_wideband(args):
     # stored entries once and the vector rows it reads or writes once, all 100 columns
     names = ["gather", "up", "coupling", "down", "near", "leaves"]
     kernels = {"gather": "k_gather_to_f32", "up": "k_gather_wide", "coupling": "k_gather_wide",
-               "down": "k_gather_wide", "leaves": "k_rows_gather (leaf outputs: bases and near blocks)"}
+               "down": "k_gather_wide", "leaves": "k_gather_tc (tcgen05 kind::tf32, 3xTF32; leaf outputs: bases and near blocks)"}
     top = max(range(6), key=lambda q: stage_sum[q])
     xe = info["basis_entries_test"] + info["basis_entries_trial"] + info["transfer_entries_test"] + \
         info["transfer_entries_trial"]
@@ -759,8 +789,8 @@ def run_wideband(args):
             "config": {"workload": WIDEBAND.format(n=n), "npoints": n, "k": k, "nvec": nvec,
                        "admissibility": "isnearwideband(k; eta_lf=1, eta_hf=5, gamma=1)",
                        "compressor": "BottomUp(IACA(MaximumValue, TreeMimicryPivoting, FNormExtrapolator(1e-4)))",
-                       "step": "100 matvecs as one block of 100 right-hand sides (launch groups of small outputs: "
-                               "all 100 columns per launch; leaf outputs: passes of <= 16 columns)",
+                       "step": "100 matvecs as one block of 100 right-hand sides (all 100 columns per launch: "
+                               "small outputs on the FP32 pipe, leaf outputs on the tcgen05 tensor cores)",
                        "l2": "inputs larger than L2 (FP32 stores %.1f GB per step)" % (8 * store_entries(info) / 1e9),
                        "build_s": build_mixed, "build_s_plain_f64": build_plain,
                        "build_device_s": info["build_seconds"], "stored_gb_f64": E * store_entries(info) / 1e9,

@@ -32,6 +32,7 @@ UNITS = [
     ("build_kernels.cu", "nvcc", ["--fmad=false"]),
     ("mimicry.cu", "nvcc", ["--fmad=false"]),
     ("apply_kernels.cu", "nvcc", []),
+    ("tc_gather.cu", "nvcc", []),
     ("capi.cu", "nvcc", []),
 ]
 HEADERS = ["nca_internal.h", "entry.cuh", "build_kernels.cuh", "apply_kernels.cuh"]

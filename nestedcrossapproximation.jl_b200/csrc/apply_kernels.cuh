@@ -93,6 +93,12 @@ struct WideOut {
 // right-hand sides in one launch (a.q0, a.bc, a.g_rows, a.g_out, a.g_segptr unused; the outputs
 // come as WideOut records): a warp streams a sequence of outputs, two columns per lane, FP32
 // accumulation.
+// STAGE_GATHER over complex-FP32 stores and arena on the tcgen05 tensor cores (3xTF32), for outputs
+// of at most 64 rows, all a.b right-hand sides (passes of 128) in one launch; the outputs come as
+// WideOut records (ld = R, r0 = 0). A CTA per output at a time, two per SM (tc_gather.cu).
+bool gather_tc_fits(int maxrows);
+size_t gather_tc_smem_bytes();
+void launch_gather_tc(const RowArgs<float2> &a, const WideOut *outs, int count, cudaStream_t s);
 bool gather_wide_fits(int maxrows);
 // the register tile (rows) of the kernel instance that takes an output of R <= 32 rows: R rounded
 // up to even up to 24, then 28 or 32; a launch's outputs all have tile nr

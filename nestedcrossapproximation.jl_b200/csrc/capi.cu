@@ -186,6 +186,7 @@ struct GatherStage {
     DBuf<int32_t> outputs, rows, segptr, w;
     DBuf<int64_t> out, moff, voff;
     DBuf<WideOut> wout;  // the outputs in launch order as records (all-column FP32 gathers)
+    DBuf<WideOut> tout;  // every output as a record, in group order (tensor-core gathers)
     // launches of the all-column FP32 kernel: group g's are [wide_gptr[g], wide_gptr[g + 1]), each
     // wide_count outputs from position wide_begin with the register tile wide_nr
     std::vector<int32_t> wide_gptr, wide_begin, wide_count;
@@ -1124,6 +1125,12 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
 // onto one child direction, so the children gather), leaves (leaf <- every basis item whose
 // cluster contains it, and the near blocks).
 
+// complex-FP32 products of at least this many right-hand sides run their gathers on the tensor
+// cores (NCA_TC_COLUMNS overrides it; a large value keeps them on the FP32 pipe)
+const int kTensorCoreColumns = [] {
+    const char *v = std::getenv("NCA_TC_COLUMNS");
+    return v ? std::max(1, std::atoi(v)) : 32;
+}();
 // launch groups of small outputs (mean block entries per output below this) run on the gather
 // kernels that keep a warp per output
 constexpr double kSmallGroupWork = 8192.0;
@@ -1273,9 +1280,17 @@ struct StageBuilder {
         G.group_ptr = group_ptr;
         G.group_maxrows = group_maxrows;
         G.group_work = group_work;
+        std::vector<WideOut> trec(order.size());
+        for (size_t i = 0; i < order.size(); ++i) {
+            const int32_t o = order[i];
+            int32_t W = 0;
+            for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
+            trec[i] = WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], rows[o], 0};
+        }
         if (mark) mark("records");
         G.outputs.upload(order, s);
         G.wout.upload(rec, s);
+        G.tout.upload(trec, s);
         G.rows.upload(rows, s);
         G.out.upload(out, s);
         G.segptr.upload(segptr, s);
@@ -2477,6 +2492,15 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
                 a.error = error;
                 const bool small = G.group_work[g] < kSmallGroupWork;
                 if constexpr (!f64) {
+                    // groups of small outputs on the FP32 pipe (all columns per launch); larger
+                    // outputs of many right-hand sides on the tensor cores
+                    if (b >= kTensorCoreColumns && gather_tc_fits(a.maxrows) &&
+                        !wide_group(a.maxrows, G.group_work[g])) {
+                        launch_gather_tc(a, G.tout.p + G.group_ptr[g], cnt, s);
+                        ++count.total;
+                        ++count.stage[sk];
+                        continue;
+                    }
                     if (b >= 2 && wide_group(a.maxrows, G.group_work[g])) {
                         for (int32_t k = G.wide_gptr[g]; k < G.wide_gptr[g + 1]; ++k) {
                             launch_gather_wide(a, G.wout.p + G.wide_begin[k], G.wide_count[k], G.wide_nr[k], s);
