@@ -98,6 +98,7 @@ struct MimicryArgs {
     int nitems;
     const int64_t *ffptr;
     const int32_t *ffnodes;
+    int ff_by_position;  // 1: ffptr is indexed by the item's position in the launch (IACA levels)
     const int32_t *item_node;
     const double *centroid;   // own clusters, 3 each
     const int32_t *own_size;  // own clusters' point counts

@@ -67,6 +67,13 @@ struct DBuf {
         n = count;
         CK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)));
     }
+    // hands the array to `later` (freed by its owner once no stream needs it) instead of freeing
+    // it now: cudaFree waits for the whole device, including other host threads' work
+    void defer(std::vector<void *> &later) {
+        if (p) later.push_back(p);
+        p = nullptr;
+        n = 0;
+    }
     void upload(const T *h, size_t count, cudaStream_t s) {
         alloc(count);
         if (count) CK(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, s));
@@ -97,6 +104,11 @@ struct PinnedBuf {
     PinnedBuf &operator=(const PinnedBuf &) = delete;
     ~PinnedBuf() {
         if (p) cudaFreeHost(p);
+    }
+    // hands the array to `later` instead of freeing it now (cudaFreeHost waits for the device)
+    void defer(std::vector<void *> &later) {
+        if (p) later.push_back(p);
+        p = nullptr;
     }
 };
 
@@ -175,6 +187,15 @@ struct DirItems {
     DBuf<int32_t> cpiv;  // column pivots sigma of every item (maxrank per item): frozen-skeleton refills
     DBuf<int64_t> xoff;
     DBuf<double2> X, XT;
+    // device and page-locked scratch of the build, freed once the build has synchronised
+    std::vector<void *> later, later_host;
+    void free_later() {
+        for (void *q : later) cudaFree(q);
+        for (void *q : later_host) cudaFreeHost(q);
+        later.clear();
+        later_host.clear();
+    }
+    ~DirItems() { free_later(); }
 };
 
 // One product stage as block-sparse gathers over the vector arena: outputs (ordered by launch
@@ -1217,6 +1238,14 @@ struct StageBuilder {
                     (long long)ent, group_work[g]);
         }
     }
+    // adds dy to the vector rows of the segments that read the store (not the second store's near
+    // blocks) and, with outs, to the outputs' rows: a plan listed before the arena offset was known
+    void shift(int64_t dy, bool outs) {
+        for (size_t k = 0; k < moff.size(); ++k)
+            if (moff[k] >= 0) voff[k] += dy;
+        if (outs)
+            for (int64_t &o : out) o += dy;
+    }
     // uploads the plan; with a source, allocates the stage store and copies its blocks
     void finish(GatherStage &G, const double2 *src, cudaStream_t s, const char *tag = nullptr,
                 const std::function<void(const std::string &)> &mark = {}) {
@@ -1235,57 +1264,55 @@ struct StageBuilder {
             for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
             for (int32_t i = b; i < e; ++i) order[size_t(b + cnt[size_t(wmax - work[i])]++)] = i;
         }
-        // Records of the all-column FP32 kernel (groups of small outputs): an output of more than
-        // WIDE_SLICE rows is taken as row slices of at most WIDE_SLICE rows (same segments, the
-        // vector rows read once per slice); inside a group the records of one row class (the
-        // kernel's register tile) are contiguous, largest work first inside a class: one launch
-        // per class
-        constexpr int WIDE_SLICE = 20;
+        // Records of the all-column FP32 kernel (groups of small outputs): inside a group the
+        // records of one row class (the kernel's register tile) are contiguous, largest work
+        // first inside a class: one launch per class
         G.wide_gptr.assign(1, 0);
         G.wide_begin.clear();
         G.wide_count.clear();
         G.wide_nr.clear();
         std::vector<WideOut> rec;
         rec.reserve(order.size());
-        std::vector<WideOut> grec;
         for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
             const int32_t b = group_ptr[g], e = group_ptr[g + 1];
-            grec.clear();
-            for (int32_t i = wide_group(group_maxrows[g], group_work[g]) ? b : e; i < e; ++i) {
-                const int32_t o = order[i];
-                int32_t W = 0;
-                for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
-                const int32_t R = rows[o];
-                const int32_t ns = (R + WIDE_SLICE - 1) / WIDE_SLICE;
-                const int32_t rs = ns > 1 ? (R + ns - 1) / ns : R;
-                for (int32_t r0 = 0; r0 < std::max(R, 1); r0 += std::max(rs, 1))
-                    grec.push_back(WideOut{std::min(rs, R - r0), W, segptr[o], segptr[o + 1], out[o] + r0, R, r0});
-            }
-            std::vector<int32_t> ccount(34, 0), start(34, 0);
-            for (const WideOut &r : grec) ++ccount[size_t(wide_rows_class(r.R))];
-            int32_t at = int32_t(rec.size());
-            for (int c = 0; c < 34; ++c) {
-                start[c] = at;
-                if (ccount[c]) {
-                    G.wide_begin.push_back(at);
-                    G.wide_count.push_back(ccount[c]);
-                    G.wide_nr.push_back(c);
+            if (e > b && wide_group(group_maxrows[g], group_work[g])) {
+                int32_t ccount[34] = {0}, start[34];
+                for (int32_t i = b; i < e; ++i) ++ccount[wide_rows_class(rows[order[i]])];
+                int32_t at = int32_t(rec.size());
+                for (int c = 0; c < 34; ++c) {
+                    start[c] = at;
+                    if (ccount[c]) {
+                        G.wide_begin.push_back(at);
+                        G.wide_count.push_back(ccount[c]);
+                        G.wide_nr.push_back(c);
+                    }
+                    at += ccount[c];
                 }
-                at += ccount[c];
+                rec.resize(size_t(at));
+                for (int32_t i = b; i < e; ++i) {
+                    const int32_t o = order[i];
+                    int32_t W = 0;
+                    for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
+                    rec[size_t(start[wide_rows_class(rows[o])]++)] =
+                        WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], rows[o], 0};
+                }
             }
-            rec.resize(size_t(at));
-            for (const WideOut &r : grec) rec[size_t(start[size_t(wide_rows_class(r.R))]++)] = r;
             G.wide_gptr.push_back(int32_t(G.wide_begin.size()));
         }
         G.group_ptr = group_ptr;
         G.group_maxrows = group_maxrows;
         G.group_work = group_work;
+        // records of the tensor-core gathers: the groups the all-column FP32 kernel does not take
+        // (left zero elsewhere)
         std::vector<WideOut> trec(order.size());
-        for (size_t i = 0; i < order.size(); ++i) {
-            const int32_t o = order[i];
-            int32_t W = 0;
-            for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
-            trec[i] = WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], rows[o], 0};
+        for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
+            if (wide_group(group_maxrows[g], group_work[g])) continue;
+            for (int32_t i = group_ptr[g]; i < group_ptr[g + 1]; ++i) {
+                const int32_t o = order[i];
+                int32_t W = 0;
+                for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
+                trec[i] = WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], rows[o], 0};
+            }
         }
         if (mark) mark("records");
         G.outputs.upload(order, s);
@@ -1384,28 +1411,42 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     DevSide &ds = c->side[sd];
     const DevSide &fs = c->side[1 - sd];
     const int ni = d.nitems;
-    // the items' directional far fields (dirfarfield), in the reference's order, and the far
-    // points each can offer (capped at maxrank)
-    std::vector<int64_t> ffptr;
-    std::vector<int32_t> ffnodes;
-    parallel_csr(
-        ni, [&](int it, std::vector<int32_t> &ff) { nca::item_farfield(T, pl, it, ff); }, ffptr, ffnodes);
-    std::vector<int32_t> farpts(ni, 0);
-    for (int it = 0; it < ni; ++it) {
-        int64_t n = 0;
-        for (int64_t q = ffptr[it]; q < ffptr[it + 1] && n < maxrank; ++q) n += Ft.size(ffnodes[q]);
-        farpts[it] = int32_t(std::min<int64_t>(n, maxrank));
-    }
+    // The items' directional far fields (dirfarfield, in the reference's order) and the far points
+    // each can offer (capped at maxrank), listed one level at a time on the host threads: a level's
+    // lists are made while the device compresses the level below it. An item without far nodes
+    // is not compressed; its empty range leaves the level's CSR over the remaining items intact.
+    struct LevelFar {
+        std::vector<int32_t> items, farpts;  // the level's items with far points, and their counts
+        std::vector<int64_t> ptr;             // CSR over those items (positional)
+        std::vector<int32_t> nodes;
+    };
+    auto list_level = [&, maxrank](int lev) {
+        LevelFar L;
+        const std::vector<int32_t> &cand = bylevel[lev];
+        std::vector<int64_t> ptr;
+        parallel_csr(
+            int(cand.size()), [&](int i, std::vector<int32_t> &ff) { nca::item_farfield(T, pl, cand[i], ff); }, ptr,
+            L.nodes);
+        L.ptr.push_back(0);
+        for (size_t i = 0; i < cand.size(); ++i) {
+            int64_t n = 0;
+            for (int64_t q = ptr[i]; q < ptr[i + 1] && n < maxrank; ++q) n += Ft.size(L.nodes[q]);
+            if (n == 0) continue;
+            L.items.push_back(cand[i]);
+            L.farpts.push_back(int32_t(std::min<int64_t>(n, maxrank)));
+            L.ptr.push_back(ptr[i + 1]);
+        }
+        return L;
+    };
+    std::future<LevelFar> next_far;
+    if (T.nlevels > 0) next_far = std::async(std::launch::async, list_level, T.nlevels - 1);
     const std::vector<double> centroid = cluster_centroids(T, ownpts);
-    timer.mark(side + "item far fields listed (" + std::to_string(ffnodes.size()) + " far nodes)");
     DBuf<int64_t> dffptr;
     DBuf<int32_t> dffnodes;
     DBuf<double> dcent, dcenter;
-    dffptr.upload(ffptr, s);
-    dffnodes.upload(ffnodes, s);
     dcent.upload(centroid, s);
     dcenter.upload(Ft.center, s);
-    timer.mark(side + "item far fields and centroids uploaded");
+    timer.mark(side + "centroids uploaded");
     // the side's items, level by level
     DBuf<int32_t> status;
     status.alloc(5);  // [flag, item, a, b], item cursor
@@ -1468,31 +1509,38 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     PinnedBuf<int32_t> hrank(2 * size_t(std::max(ni, 1)));
     a.xoff_by_position = 1;
     int64_t total = 0;
+    a.mim.ff_by_position = 1;
     for (int lev = T.nlevels - 1; lev >= 0; --lev) {
-        std::vector<int32_t> items;
+        const LevelFar far = next_far.get();
+        if (lev > 0) next_far = std::async(std::launch::async, list_level, lev - 1);
+        const std::vector<int32_t> &items = far.items;
         std::vector<int64_t> lvoff;
         int mc = 0;
         int64_t bound = 0;
-        for (int it : bylevel[lev]) {
-            if (farpts[it] == 0) continue;
+        for (size_t i = 0; i < items.size(); ++i) {
+            const int it = items[i];
             int64_t m = 0;
             if (pl.item_basis[it]) {
                 m = T.size(pl.item_node[it]);
             } else {
                 for (int k = pl.item_chptr[it]; k < pl.item_chptr[it + 1]; ++k) m += d.h_rank[pl.item_chidx[k]];
             }
-            const int64_t rb = std::min<int64_t>(std::min<int64_t>(maxrank, m), int64_t(farpts[it]));
+            const int64_t rb = std::min<int64_t>(std::min<int64_t>(maxrank, m), int64_t(far.farpts[i]));
             lvoff.push_back(bound);
             bound += pad2(m * rb);
-            items.push_back(it);
             mc = int(std::max<int64_t>(mc, m));
         }
         if (items.empty()) continue;
+        upload_reuse(dffptr, far.ptr, s);
+        upload_reuse(dffnodes, far.nodes, s);
+        a.mim.ffptr = dffptr.p;
+        a.mim.ffnodes = dffnodes.p;
         if (mc > nca::iaca_max_rows())
             throw Failure(NCA_ERR_ARG, "a basis item has " + std::to_string(mc) +
                                            " rows; the IACA kernel holds at most " +
                                            std::to_string(nca::iaca_max_rows()) + " (reduce the leaf size)");
         if (!chunk.p || size_t(bound) > chunk.n) {
+            chunk.defer(d.later);
             chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
             timer.mark(side + "level " + std::to_string(lev) + " scratch of " + std::to_string(bound >> 16) +
                        " x 1 MiB allocated");
@@ -1567,8 +1615,14 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
             off += lt;
         }
         CK(cudaStreamSynchronize(s));
+        for (auto &x : levelX) x->defer(d.later);
         levelX.clear();
     }
+    for (auto *b : {&dffptr, &dlvoff, &ddo}) b->defer(d.later);
+    for (auto *b : {&dffnodes, &status, &nodes, &drk}) b->defer(d.later);
+    for (auto *b : {&dcent, &dcenter}) b->defer(d.later);
+    chunk.defer(d.later);
+    hrank.defer(d.later_host);
 }
 
 void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_build_opts *o, const nca::Wideband &wb,
@@ -1613,19 +1667,19 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     StreamGuard sg2{s2};
     std::vector<int64_t> h_ntoff;
     int64_t near_entries = 0;
-    std::future<void> near_job = std::async(std::launch::async, [&]() {
+    std::shared_future<void> near_f = std::async(std::launch::async, [&]() {
         CK(cudaSetDevice(c->device));
         near_entries = build_near(c, s2, &h_ntoff);
         CK(cudaStreamSynchronize(s2));
         timer.mark("near field built");
-    });
+    }).share();
     // The far pairs matched across the two sides' directional plans (which items a pair couples,
     // where its transpose sits) need the plans only: matched on a thread of their own while the
     // sides compress. The couplings then only add the ranks.
     std::promise<void> planned[2];
     std::shared_future<void> planned_f[2] = {planned[0].get_future().share(), planned[1].get_future().share()};
     std::vector<int32_t> pair_it, pair_is, pair_of_pos;
-    std::future<void> pairs_job = std::async(std::launch::async, [&]() {
+    std::shared_future<void> pairs_f = std::async(std::launch::async, [&]() {
         planned_f[0].get();
         planned_f[1].get();
         const nca::DirSide &pt = D->side[0].plan, &ps = D->side[1].plan;
@@ -1663,10 +1717,12 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 pair_of_pos[q] = e;
             }
         timer.mark("far pairs matched");
-    });
+    }).share();
     std::vector<std::vector<int32_t>> bylevel[2];  // items per level, filled by each side's task
     int64_t basis_entries[2] = {0, 0}, transfer_entries[2] = {0, 0};
-    on_threads(c->device, 2, [&](int sd) {
+    std::promise<void> sided[2];
+    std::shared_future<void> side_done[2] = {sided[0].get_future().share(), sided[1].get_future().share()};
+    auto side_task = [&](int sd) {
         const cudaStream_t s = ss[sd];
         DirItems &d = D->side[sd];
         const std::string side = sd == 0 ? "test: " : "trial: ";
@@ -1718,18 +1774,16 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s));
         timer.mark(side + "bases joined and transposed");
-    });
-    auto h1 = std::chrono::steady_clock::now();
-    near_job.get();
-    pairs_job.get();
+        };
     // couplings: computed by the thread of the forward coupling plan (the transposed coupling plan
     // waits for it) on stream s while the other plans are built; their device inputs stay alive
     // until s is synchronised
     const nca::DirSide &pt = D->side[0].plan, &ps = D->side[1].plan;
-    const int64_t npairs = int64_t(pt.farnodes.size());
+    int64_t npairs = 0;
     std::vector<int64_t> cfoff, ctoff;
     int64_t coupling_entries = 0;
     auto couplings = [&]() {
+        npairs = int64_t(pt.farnodes.size());
         const std::vector<int32_t> &rt = D->side[0].h_rank, &rs = D->side[1].h_rank;
         // coupling blocks S_e = K[tau_(t, dt), tau_(s, ds)] in test pair order, transposes in trial order
         cfoff.assign(npairs + 1, 0);
@@ -1788,15 +1842,6 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     };
     std::promise<void> coupled;
     std::shared_future<void> coupled_done = coupled.get_future().share();
-    // gather plans: the four stages of both orientations, each task on its own thread and stream
-    for (int m = 0; m < 2; ++m) {
-        const int I = m == 0 ? 1 : 0, O = 1 - I;
-        DirProduct &pr = D->prod[m];
-        pr.nin = c->tree[I].npoints;
-        pr.nout = c->tree[O].npoints;
-        pr.cin = D->side[I].h_cptr.back();
-        pr.cout = D->side[O].h_cptr.back();
-    }
     cudaStream_t ts[8];
     for (cudaStream_t &t : ts) CK(cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
     struct StreamsGuard {
@@ -1805,7 +1850,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             for (int i = 0; i < 8; ++i) cudaStreamDestroy(t[i]);
         }
     } tsg{ts};
-    on_threads(c->device, 8, [&](int task) {
+    auto plan_task = [&](int task) {
         const cudaStream_t s = ts[task];
         auto plan_mark = [&timer, task](const char *stage) {
             return [&timer, task, stage](const std::string &what) {
@@ -1817,9 +1862,17 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         const DirItems &di = D->side[I], &dout = D->side[O];
         const nca::Tree &TI = c->tree[I], &TO = c->tree[O];
         DirProduct &pr = D->prod[m];
-        const int64_t xin = pr.nin, yo = pr.nin + pr.cin;
+        // arena rows: [x of the input side; its coefficients; the output side's coefficients]: the
+        // output rows start after the input side's coefficients, known once that side is built
+        const int64_t xin = TI.npoints;
+        int64_t yo = 0;
+        auto input_side_built = [&]() {
+            side_done[I].get();
+            yo = xin + di.h_cptr.back();
+        };
         // up: input-side items, deepest level first
         if (stage == 0) {
+            side_done[I].get();
             StageBuilder B;
             const size_t seg = size_t(di.nitems) + di.plan.item_chidx.size();
             B.reserve(size_t(di.nitems), seg, seg);
@@ -1852,7 +1905,11 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         // coupling: output-side items with a rank and their far pairs' blocks (store built above)
         if (stage == 1) {
             if (m == 0) {
+                // every way out of this block settles `coupled`, which the transposed plan awaits
                 try {
+                    side_done[O].get();
+                    input_side_built();
+                    pairs_f.get();
                     couplings();
                     coupled.set_value();
                 } catch (...) {
@@ -1861,6 +1918,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 }
             } else {
                 coupled_done.get();
+                side_done[O].get();
+                input_side_built();
             }
             StageBuilder B;
             const nca::DirSide &pl = dout.plan;
@@ -1885,6 +1944,9 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         }
         // down: output-side items gather from the parent items that map onto them, root level first
         if (stage == 2) {
+            // listed with output rows relative to yo (the other side may still be compressing),
+            // moved by yo once it is known
+            side_done[O].get();
             // parents of every child item (CSR in parent order), with the child's row offset in
             // the parent's X
             std::vector<int32_t> pptr(size_t(dout.nitems) + 1, 0), ppar;
@@ -1926,11 +1988,15 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 B.end_group();
             }
             timer.mark("gather plan " + std::to_string(task) + ": down listed");
+            input_side_built();
+            B.shift(yo, true);
             B.finish(pr.down, dout.X.p, s, m ? "T down" : "N down", plan_mark("down"));
             timer.mark("gather plan " + std::to_string(task) + ": down");
         }
         // leaves: every basis item whose cluster contains the leaf, then the near blocks
         if (stage == 3) {
+            side_done[O].get();
+            near_f.get();
             StageBuilder B;
             const nca::DirSide &pl = dout.plan;
             const std::vector<int32_t> &nptr = m == 0 ? P.nearptr : P.tnearptr;
@@ -1955,11 +2021,39 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             }
             B.end_group();
             timer.mark("gather plan " + std::to_string(task) + ": leaves listed");
+            input_side_built();
+            B.shift(yo, false);
             B.finish(pr.leaves, dout.X.p, s, m ? "T leaves" : "N leaves", plan_mark("leaves"));
             timer.mark("gather plan " + std::to_string(task) + ": leaves");
         }
         CK(cudaStreamSynchronize(s));
+        };
+    // The two sides (direction plan, far fields, IACA levels) and the eight gather plans (four
+    // stages x two orientations) on ten host threads and streams: a plan starts as soon as the
+    // sides it reads are built (up: the input side; down, leaves: the output side, then the input
+    // side's coefficient count; coupling: both sides and the couplings).
+    on_threads(c->device, 10, [&](int task) {
+        if (task < 2) {
+            try {
+                side_task(task);
+            } catch (...) {
+                sided[task].set_exception(std::current_exception());
+                throw;
+            }
+            sided[task].set_value();
+        } else {
+            plan_task(task - 2);
+        }
     });
+    auto h1 = std::chrono::steady_clock::now();
+    for (int m = 0; m < 2; ++m) {
+        const int I = m == 0 ? 1 : 0, O = 1 - I;
+        DirProduct &pr = D->prod[m];
+        pr.nin = c->tree[I].npoints;
+        pr.nout = c->tree[O].npoints;
+        pr.cin = D->side[I].h_cptr.back();
+        pr.cout = D->side[O].h_cptr.back();
+    }
     CK(cudaStreamSynchronize(s));
     timer.mark("gather plans done");
     // the stage stores hold the products' copies of the operators; X stays for nca_core_save
@@ -1979,6 +2073,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     CK(cudaEventRecord(ev1, s));
     CK(cudaStreamSynchronize(s));
     timer.mark("complex-FP32 copies done, build complete");
+    for (DirItems &d : D->side) d.free_later();
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
     auto h2 = std::chrono::steady_clock::now();

@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(kIacaWarps * 32) k_iaca(IacaArgs a) {
                 rx[q] = ry[q] = rz[q] = 0.0;
             }
         }
-        mim_start(F, w, item, cl);
+        mim_start(F, w, F.ff_by_position ? idx : item, cl);
         // rank limit: min(maxrank, rows, far points)
         int n = 0;
         for (int i = 0; i < w.nroots && limit - n > 0; ++i) {
