@@ -118,10 +118,11 @@ __device__ __forceinline__ uint32_t tf32_round(float x) {
     return r;
 }
 
-// head and tail of x, both as TF32 bit patterns
+// head (rounded to TF32) and tail of x; the tail is passed as FP32 bits, whose low 13 bits the
+// MMA ignores: it loses below 2^-10 of the tail, below 2^-21 of x
 __device__ __forceinline__ void split(float x, uint32_t &hi, uint32_t &lo) {
     hi = tf32_round(x);
-    lo = tf32_round(x - __uint_as_float(hi));
+    lo = __float_as_uint(x - __uint_as_float(hi));
 }
 
 __device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
@@ -152,10 +153,12 @@ struct TcLoad {
     float b[16];
 };
 
-// The CTA's walk over its outputs (grid-stride), their passes of 128 right-hand sides, their
-// segments and the chunks of TC_KC pairs of each segment. Every thread walks it identically.
+// The CTA's walk over its outputs (grid-stride), their passes of 128 right-hand sides and the
+// (block column, vector row) pairs of each pass, TC_KC pairs per chunk across segment boundaries:
+// the chunk starts at pair j0 of segment e, t pairs of the pass are done. Every thread walks it
+// identically.
 struct TcWalk {
-    int wi, c0, e, j0, w;
+    int wi, c0, e, j0, w, t;
     WideOut rec;
 };
 
@@ -173,51 +176,55 @@ __device__ __forceinline__ WideOut tc_record(const WideOut *outs, int i) {
     return o;
 }
 
-// the chunk the walk stands on: jn = 0 for a pass of an output without segments (its outputs are
+// the chunk the walk stands on: jn = 0 for a pass of an output without pairs (its outputs are
 // written from zero); false once the walk is past the last output
-__device__ __forceinline__ bool tc_chunk(const RowArgs<float2> &a, const TcWalk &k, int count, TcChunk &ch) {
+__device__ __forceinline__ bool tc_chunk(const TcWalk &k, int count, TcChunk &ch) {
     if (k.wi >= count) return false;
     ch.wi = k.wi;
     ch.c0 = k.c0;
     ch.e = k.e;
     ch.j0 = k.j0;
-    if (k.rec.e0 >= k.rec.e1) {
-        ch.jn = 0;
-        ch.first = ch.last = true;
-        return true;
-    }
-    ch.jn = min(TC_KC, k.w - k.j0);
-    ch.first = k.e == k.rec.e0 && k.j0 == 0;
-    ch.last = k.j0 + ch.jn >= k.w && k.e + 1 >= k.rec.e1;
+    ch.jn = min(TC_KC, k.rec.W - k.t);
+    ch.first = k.t == 0;
+    ch.last = k.t + ch.jn >= k.rec.W;
     return true;
+}
+
+__device__ __forceinline__ void tc_pass_start(const RowArgs<float2> &a, TcWalk &k) {
+    k.e = k.rec.e0;
+    k.j0 = 0;
+    k.t = 0;
+    k.w = k.e < k.rec.e1 ? a.g_w[k.e] : 0;
 }
 
 __device__ __forceinline__ void tc_start_output(const RowArgs<float2> &a, const WideOut *outs, int count, TcWalk &k) {
     k.c0 = 0;
-    k.j0 = 0;
     if (k.wi >= count) return;
     k.rec = tc_record(outs, k.wi);
-    k.e = k.rec.e0;
-    k.w = k.e < k.rec.e1 ? a.g_w[k.e] : 0;
+    tc_pass_start(a, k);
 }
 
 // moves the walk to the next chunk
 __device__ __forceinline__ void tc_advance(const RowArgs<float2> &a, const WideOut *outs, int count, TcWalk &k) {
-    if (k.rec.e0 < k.rec.e1) {
-        k.j0 += TC_KC;
-        if (k.j0 < k.w) return;
-        k.j0 = 0;
-        if (++k.e < k.rec.e1) {
-            k.w = a.g_w[k.e];
-            return;
+    int rem = min(TC_KC, k.rec.W - k.t);
+    k.t += rem;
+    if (k.t < k.rec.W) {
+        while (rem > 0) {
+            const int take = min(rem, k.w - k.j0);
+            k.j0 += take;
+            rem -= take;
+            if (k.j0 >= k.w) {
+                ++k.e;
+                k.j0 = 0;
+                k.w = a.g_w[k.e];  // e < e1: pairs remain
+            }
         }
+        return;
     }
     // the pass is done: the next pass of the output, or the next output
     k.c0 += 128;
     if (k.c0 < a.b) {
-        k.e = k.rec.e0;
-        k.j0 = 0;
-        k.w = k.e < k.rec.e1 ? a.g_w[k.e] : 0;
+        tc_pass_start(a, k);
         return;
     }
     k.wi += gridDim.x;
@@ -225,27 +232,36 @@ __device__ __forceinline__ void tc_advance(const RowArgs<float2> &a, const WideO
 }
 
 // the chunk's operands from global memory into registers (zeros outside the chunk, the rows and
-// the right-hand sides)
+// the right-hand sides): thread (warp w, lane l) takes pair kk = 4 w + (l & 3) of the chunk,
+// A rows m = 8 i + (l >> 2) and B rows n = 8 i + (l >> 2) of it
 __device__ __forceinline__ void tc_load(const RowArgs<float2> &a, const TcWalk &k, const TcChunk &ch, TcLoad &L) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kq = lane & 3, rq = lane >> 2;
-    const int64_t mo = a.g_moff[ch.e];
-    const float *M = reinterpret_cast<const float *>((mo >= 0 ? a.M + mo : a.M2 + (-1 - mo)) +
-                                                     int64_t(ch.j0) * k.rec.ld + k.rec.r0);
-    const float *V = reinterpret_cast<const float *>(a.src32 + (a.g_voff[ch.e] + ch.j0) * a.vs + ch.c0);
+    const int kk = 4 * w + kq;
+    const bool live = kk < ch.jn;
+    // the pair's segment and column: kk steps on from the chunk's start
+    int e = ch.e, j = ch.j0 + kk, we = k.w;
+    if (live)
+        while (j >= we) {
+            j -= we;
+            ++e;
+            we = a.g_w[e];
+        }
+    const int64_t mo = live ? a.g_moff[e] : 0;
+    const float *M = reinterpret_cast<const float *>((mo >= 0 ? a.M + mo : a.M2 + (-1 - mo)) + int64_t(j) * k.rec.ld +
+                                                     k.rec.r0);
+    const float *V = reinterpret_cast<const float *>(a.src32 + (live ? a.g_voff[e] + j : 0) * a.vs + ch.c0);
     const int nf = 2 * (a.b - ch.c0);  // floats of the right-hand sides of this pass
     const int nb = 2 * k.rec.R;
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
-        const int rest = 4 * i + w;
-        const int kk = 4 * (rest & 3) + kq, m = 8 * (rest >> 2) + rq;
-        L.a[i] = kk < ch.jn && m < nf ? V[int64_t(kk) * 2 * a.vs + m] : 0.f;
+        const int m = 8 * i + rq;
+        L.a[i] = live && m < nf ? V[m] : 0.f;
     }
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
-        const int rest = 4 * i + w;
-        const int kk = 4 * (rest & 3) + kq, n = 8 * (rest >> 2) + rq;
-        L.b[i] = kk < ch.jn && n < nb ? M[int64_t(kk) * 2 * k.rec.ld + n] : 0.f;
+        const int n = 8 * i + rq;
+        L.b[i] = live && n < nb ? M[n] : 0.f;
     }
 }
 
@@ -364,7 +380,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_gather_tc(RowArgs<float2> a, 
     k.wi = blockIdx.x;
     tc_start_output(a, outs, count, k);
     TcChunk ch;
-    bool have = tc_chunk(a, k, count, ch);
+    bool have = tc_chunk(k, count, ch);
     TcLoad L;
     if (have && ch.jn > 0) tc_load(a, k, ch, L);
     // the previous chunk, whose pass may still need its epilogue
@@ -434,7 +450,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_gather_tc(RowArgs<float2> a, 
         }
         if (ch.jn > 0) ++kc;
         tc_advance(a, outs, count, k);
-        have = tc_chunk(a, k, count, ch);
+        have = tc_chunk(k, count, ch);
         if (have && ch.jn > 0) tc_load(a, k, ch, L);
     }
     if (pend && !stop) {
