@@ -13,8 +13,9 @@
 // Rules fixed by this project where the reference's dependencies are not available
 // (AdaptiveCrossApproximation.jl, H2Trees.jl): 2-means splits seeded by the point farthest
 // from the centroid and the point farthest from that one, Lloyd iterations with ties to the
-// first cluster, stable partition; tree mimicry picks, for each pivot, the far node whose
-// centre maximises dmin^2/|y - c_t|^2 (dmin: distance to the pivots chosen so far), descends
+// first cluster, sums over a cluster taken in ordered chunks of 8192 points, stable partition;
+// tree mimicry picks, for each pivot, the far node whose centre maximises dmin^2/|y - c_t|^2
+// (dmin: distance to the pivots chosen so far), descends
 // by the same score to a leaf and takes the best untaken point there; ties go to the first
 // candidate. Compiled with -ffp-contract=off: every fused multiply-add is an explicit
 // std::fma, so results are reproducible bit for bit.
@@ -24,6 +25,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
+#include <mutex>
 #include <thread>
 
 #include <sched.h>
@@ -40,66 +43,185 @@ inline double dist2(const double *a, const double *b) {
 }
 
 constexpr int kLloydIterations = 50;
+// Sums over a cluster's points are taken in chunks of kChunk consecutive points: each chunk summed
+// in order from zero, the chunk sums added in chunk order (one chunk: the plain ordered sum).
+// Clusters of at least kTeamPoints points are split by a team of host threads over the chunks;
+// the fixed chunking makes the result independent of the team size.
+constexpr int kChunk = 8192;
+constexpr int kTeamPoints = 2 * kChunk;
+
+// reusable barrier of a fixed team of threads
+struct TeamBarrier {
+    std::mutex mu;
+    std::condition_variable cv;
+    int n, waiting = 0;
+    unsigned gen = 0;
+    explicit TeamBarrier(int count) : n(count) {}
+    void wait() {
+        std::unique_lock<std::mutex> lk(mu);
+        const unsigned g = gen;
+        if (++waiting == n) {
+            waiting = 0;
+            ++gen;
+            cv.notify_all();
+        } else {
+            cv.wait(lk, [&] { return gen != g; });
+        }
+    }
+};
 
 struct Splitter {
     const double *pts;
     std::vector<int32_t> side, scratch;
 
-    // Reorders ids[0:cnt) into two stable groups; returns the size of the first one.
-    int split(int32_t *ids, int cnt) {
+    // Reorders ids[0:cnt) into two stable groups; returns the size of the first one. nteam > 1
+    // spreads the chunks of one cluster over that many threads.
+    int split(int32_t *ids, int cnt, int nteam = 1) {
         side.assign(cnt, -1);
         scratch.resize(cnt);
-        double g[3] = {0.0, 0.0, 0.0};
-        for (int i = 0; i < cnt; ++i) {
-            const double *p = pts + 3 * int64_t(ids[i]);
-            g[0] += p[0];
-            g[1] += p[1];
-            g[2] += p[2];
-        }
-        for (double &v : g) v /= cnt;
-        auto farthest = [&](const double *from) {
-            int arg = 0;
-            double best = -1.0;
-            for (int i = 0; i < cnt; ++i) {
-                double d = dist2(pts + 3 * int64_t(ids[i]), from);
-                if (d > best) {
-                    best = d;
-                    arg = i;
-                }
-            }
-            return std::make_pair(arg, best);
+        const int nch = (cnt + kChunk - 1) / kChunk;
+        nteam = std::max(1, std::min(nteam, nch));
+        // per chunk: partial sums of both groups, their counts, the farthest point, changes
+        std::vector<double> part(size_t(nch) * 6);
+        std::vector<int> num(size_t(nch) * 2), far_arg(nch);
+        std::vector<double> far_d(nch);
+        std::vector<char> chg(nch);
+        double g[3] = {0.0, 0.0, 0.0}, from[3] = {0.0, 0.0, 0.0}, c[2][3];
+        int a = 0, bidx = 0, first = 0;
+        double spread = 0.0;
+        bool stop = false;
+        TeamBarrier bar(nteam);
+        auto chunk_range = [&](int q, int &i0, int &i1) {
+            i0 = q * kChunk;
+            i1 = std::min(cnt, i0 + kChunk);
         };
-        int a = farthest(g).first;
-        auto [b, spread] = farthest(pts + 3 * int64_t(ids[a]));
-        int first = 0;
-        if (spread > 0.0) {
-            double c[2][3];
-            std::memcpy(c[0], pts + 3 * int64_t(ids[a]), sizeof(c[0]));
-            std::memcpy(c[1], pts + 3 * int64_t(ids[b]), sizeof(c[1]));
-            for (int it = 0; it < kLloydIterations; ++it) {
-                bool changed = false;
-                for (int i = 0; i < cnt; ++i) {
-                    const double *p = pts + 3 * int64_t(ids[i]);
-                    int32_t s = dist2(p, c[1]) < dist2(p, c[0]) ? 1 : 0;
-                    if (s != side[i]) {
-                        side[i] = s;
-                        changed = true;
+        // the farthest point from `from` in every chunk of this thread (first on ties)
+        auto farthest_local = [&](int tid) {
+            for (int q = tid; q < nch; q += nteam) {
+                int i0, i1;
+                chunk_range(q, i0, i1);
+                int arg = i0;
+                double best = -1.0;
+                for (int i = i0; i < i1; ++i) {
+                    const double d = dist2(pts + 3 * int64_t(ids[i]), from);
+                    if (d > best) {
+                        best = d;
+                        arg = i;
                     }
                 }
-                if (!changed) break;
-                double sum[2][3] = {{0, 0, 0}, {0, 0, 0}};
-                int num[2] = {0, 0};
-                for (int i = 0; i < cnt; ++i) {
-                    const double *p = pts + 3 * int64_t(ids[i]);
-                    for (int d = 0; d < 3; ++d) sum[side[i]][d] += p[d];
-                    ++num[side[i]];
-                }
-                if (num[0] == 0 || num[1] == 0) break;
-                for (int k = 0; k < 2; ++k)
-                    for (int d = 0; d < 3; ++d) c[k][d] = sum[k][d] / num[k];
+                far_arg[q] = arg;
+                far_d[q] = best;
             }
-            first = int(std::count(side.begin(), side.end(), 0));
+        };
+        auto farthest_combine = [&](double &best) {
+            int arg = 0;
+            best = -1.0;
+            for (int q = 0; q < nch; ++q)
+                if (far_d[q] > best) {
+                    best = far_d[q];
+                    arg = far_arg[q];
+                }
+            return arg;
+        };
+        auto body = [&](int tid) {
+            // centroid of the cluster
+            for (int q = tid; q < nch; q += nteam) {
+                int i0, i1;
+                chunk_range(q, i0, i1);
+                double t[3] = {0.0, 0.0, 0.0};
+                for (int i = i0; i < i1; ++i) {
+                    const double *p = pts + 3 * int64_t(ids[i]);
+                    t[0] += p[0];
+                    t[1] += p[1];
+                    t[2] += p[2];
+                }
+                for (int d = 0; d < 3; ++d) part[6 * size_t(q) + d] = t[d];
+            }
+            bar.wait();
+            if (tid == 0) {
+                for (int q = 0; q < nch; ++q)
+                    for (int d = 0; d < 3; ++d) g[d] += part[6 * size_t(q) + d];
+                for (double &v : g) v /= cnt;
+                std::memcpy(from, g, sizeof(from));
+            }
+            bar.wait();
+            farthest_local(tid);
+            bar.wait();
+            if (tid == 0) {
+                double best;
+                a = farthest_combine(best);
+                std::memcpy(from, pts + 3 * int64_t(ids[a]), sizeof(from));
+            }
+            bar.wait();
+            farthest_local(tid);
+            bar.wait();
+            if (tid == 0) {
+                bidx = farthest_combine(spread);
+                if (spread > 0.0) {
+                    std::memcpy(c[0], pts + 3 * int64_t(ids[a]), sizeof(c[0]));
+                    std::memcpy(c[1], pts + 3 * int64_t(ids[bidx]), sizeof(c[1]));
+                }
+                stop = !(spread > 0.0);
+            }
+            bar.wait();
+            for (int it = 0; it < kLloydIterations && !stop; ++it) {
+                // assignment, and the groups' sums under the new assignment, chunk by chunk
+                for (int q = tid; q < nch; q += nteam) {
+                    int i0, i1;
+                    chunk_range(q, i0, i1);
+                    bool changed = false;
+                    double t[2][3] = {{0, 0, 0}, {0, 0, 0}};
+                    int m[2] = {0, 0};
+                    for (int i = i0; i < i1; ++i) {
+                        const double *p = pts + 3 * int64_t(ids[i]);
+                        const int32_t sd = dist2(p, c[1]) < dist2(p, c[0]) ? 1 : 0;
+                        if (sd != side[i]) {
+                            side[i] = sd;
+                            changed = true;
+                        }
+                        for (int d = 0; d < 3; ++d) t[sd][d] += p[d];
+                        ++m[sd];
+                    }
+                    chg[q] = changed;
+                    for (int k = 0; k < 2; ++k) {
+                        for (int d = 0; d < 3; ++d) part[6 * size_t(q) + 3 * k + d] = t[k][d];
+                        num[2 * size_t(q) + k] = m[k];
+                    }
+                }
+                bar.wait();
+                if (tid == 0) {
+                    bool changed = false;
+                    for (int q = 0; q < nch; ++q) changed = changed || chg[q];
+                    if (!changed) {
+                        stop = true;
+                    } else {
+                        double sum[2][3] = {{0, 0, 0}, {0, 0, 0}};
+                        int n2[2] = {0, 0};
+                        for (int q = 0; q < nch; ++q)
+                            for (int k = 0; k < 2; ++k) {
+                                for (int d = 0; d < 3; ++d) sum[k][d] += part[6 * size_t(q) + 3 * k + d];
+                                n2[k] += num[2 * size_t(q) + k];
+                            }
+                        if (n2[0] == 0 || n2[1] == 0) {
+                            stop = true;
+                        } else {
+                            for (int k = 0; k < 2; ++k)
+                                for (int d = 0; d < 3; ++d) c[k][d] = sum[k][d] / n2[k];
+                        }
+                    }
+                }
+                bar.wait();
+            }
+        };
+        if (nteam == 1) {
+            body(0);
+        } else {
+            std::vector<std::thread> team;
+            for (int t = 1; t < nteam; ++t) team.emplace_back(body, t);
+            body(0);
+            for (auto &th : team) th.join();
         }
+        if (spread > 0.0) first = int(std::count(side.begin(), side.end(), 0));
         if (first == 0 || first == cnt) {
             first = (cnt + 1) / 2;
             for (int i = 0; i < cnt; ++i) side[i] = i < first ? 0 : 1;
@@ -149,7 +271,9 @@ Tree build_kmeans_tree(const double *pts, int64_t n, int minvalues) {
             thread_local Splitter sp{nullptr, {}, {}};
             sp.pts = pts;
             const int b = T.begin[node], cnt = T.end[node] - b;
-            if (cnt > minvalues && cnt >= 2) first[node - lev0] = sp.split(T.perm.data() + b, cnt);
+            // a level of few nodes (the top of the tree) gives each large cluster a team of threads
+            const int team = cnt >= kTeamPoints ? std::max(1, nth / std::max(1, int(lev1 - lev0))) : 1;
+            if (cnt > minvalues && cnt >= 2) first[node - lev0] = sp.split(T.perm.data() + b, cnt, team);
         });
         for (size_t node = lev0; node < lev1; ++node) {
             const int b = T.begin[node], e = T.end[node];

@@ -182,14 +182,27 @@ static double d2pts(const double *a, const double *b) {
 #define KMEANS_MAXIT 50
 
 /* Split perm[b:e) into two stable parts; returns the size of the first part. */
+/* Sums over a cluster's points are taken in chunks of KMEANS_CHUNK consecutive points: each
+ * chunk summed in order from zero, the chunk sums added in chunk order (for clusters of at most
+ * one chunk this is the plain ordered sum). The library's planner splits large clusters across
+ * host threads by these chunks and gets the same bits. */
+#define KMEANS_CHUNK 8192
+
 static int kmeans_split(const double *pts, int *perm, int b, int e, int *assign, int *tmp) {
     int cnt = e - b;
     double g[3] = {0, 0, 0};
-    for (int i = b; i < e; ++i) {
-        const double *p = pts + 3 * (long)perm[i];
-        g[0] += p[0];
-        g[1] += p[1];
-        g[2] += p[2];
+    for (int c0 = b; c0 < e; c0 += KMEANS_CHUNK) {
+        const int c1 = c0 + KMEANS_CHUNK < e ? c0 + KMEANS_CHUNK : e;
+        double part[3] = {0, 0, 0};
+        for (int i = c0; i < c1; ++i) {
+            const double *p = pts + 3 * (long)perm[i];
+            part[0] += p[0];
+            part[1] += p[1];
+            part[2] += p[2];
+        }
+        g[0] += part[0];
+        g[1] += part[1];
+        g[2] += part[2];
     }
     g[0] /= cnt;
     g[1] /= cnt;
@@ -233,14 +246,22 @@ static int kmeans_split(const double *pts, int *perm, int b, int e, int *assign,
                 break;
             double s0[3] = {0, 0, 0}, s1[3] = {0, 0, 0};
             int m0 = 0, m1 = 0;
-            for (int i = 0; i < cnt; ++i) {
-                const double *p = pts + 3 * (long)perm[b + i];
-                if (assign[i] == 0) {
-                    s0[0] += p[0]; s0[1] += p[1]; s0[2] += p[2];
-                    ++m0;
-                } else {
-                    s1[0] += p[0]; s1[1] += p[1]; s1[2] += p[2];
-                    ++m1;
+            for (int q0 = 0; q0 < cnt; q0 += KMEANS_CHUNK) {
+                const int q1 = q0 + KMEANS_CHUNK < cnt ? q0 + KMEANS_CHUNK : cnt;
+                double t0[3] = {0, 0, 0}, t1[3] = {0, 0, 0};
+                for (int i = q0; i < q1; ++i) {
+                    const double *p = pts + 3 * (long)perm[b + i];
+                    if (assign[i] == 0) {
+                        t0[0] += p[0]; t0[1] += p[1]; t0[2] += p[2];
+                        ++m0;
+                    } else {
+                        t1[0] += p[0]; t1[1] += p[1]; t1[2] += p[2];
+                        ++m1;
+                    }
+                }
+                for (int d = 0; d < 3; ++d) {
+                    s0[d] += t0[d];
+                    s1[d] += t1[d];
                 }
             }
             if (m0 == 0 || m1 == 0)
