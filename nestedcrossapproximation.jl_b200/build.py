@@ -33,6 +33,7 @@ UNITS = [
     ("mimicry.cu", "nvcc", ["--fmad=false"]),
     ("apply_kernels.cu", "nvcc", []),
     ("tc_gather.cu", "nvcc", []),
+    ("tree_kernels.cu", "nvcc", ["--fmad=false"]),
     ("capi.cu", "nvcc", []),
 ]
 HEADERS = ["nca_internal.h", "entry.cuh", "build_kernels.cuh", "apply_kernels.cuh"]

@@ -13,7 +13,7 @@
 // Rules fixed by this project where the reference's dependencies are not available
 // (AdaptiveCrossApproximation.jl, H2Trees.jl): 2-means splits seeded by the point farthest
 // from the centroid and the point farthest from that one, Lloyd iterations with ties to the
-// first cluster, sums over a cluster taken in ordered chunks of 8192 points, stable partition;
+// first cluster, sums over a cluster taken in ordered chunks of 256 points, stable partition;
 // tree mimicry picks, for each pivot, the far node whose centre maximises dmin^2/|y - c_t|^2
 // (dmin: distance to the pivots chosen so far), descends
 // by the same score to a leaf and takes the best untaken point there; ties go to the first
@@ -47,8 +47,8 @@ constexpr int kLloydIterations = 50;
 // in order from zero, the chunk sums added in chunk order (one chunk: the plain ordered sum).
 // Clusters of at least kTeamPoints points are split by a team of host threads over the chunks;
 // the fixed chunking makes the result independent of the team size.
-constexpr int kChunk = 8192;
-constexpr int kTeamPoints = 2 * kChunk;
+constexpr int kChunk = 256;
+constexpr int kTeamPoints = 16384;
 
 // reusable barrier of a fixed team of threads
 struct TeamBarrier {
@@ -298,8 +298,13 @@ Tree build_kmeans_tree(const double *pts, int64_t n, int minvalues) {
     T.radius.resize(T.nnodes);
     parallel_for(0, T.nnodes, [&](int node) {
         double s[3] = {0, 0, 0};
-        for (int i = T.begin[node]; i < T.end[node]; ++i)
-            for (int d = 0; d < 3; ++d) s[d] += pts[3 * int64_t(T.perm[i]) + d];
+        for (int c0 = T.begin[node]; c0 < T.end[node]; c0 += kChunk) {
+            const int c1 = std::min(T.end[node], c0 + kChunk);
+            double part[3] = {0, 0, 0};
+            for (int i = c0; i < c1; ++i)
+                for (int d = 0; d < 3; ++d) part[d] += pts[3 * int64_t(T.perm[i]) + d];
+            for (int d = 0; d < 3; ++d) s[d] += part[d];
+        }
         int cnt = T.size(node);
         double *c = &T.center[3 * size_t(node)];
         for (int d = 0; d < 3; ++d) c[d] = cnt > 0 ? s[d] / cnt : 0.0;

@@ -27,6 +27,9 @@ struct Tree {
 };
 
 Tree build_kmeans_tree(const double *pts, int64_t n, int minvalues);
+// the same tree, bit for bit, built on the current CUDA device (tree_kernels.cu); `stream` is a
+// cudaStream_t
+Tree build_kmeans_tree_device(const double *pts, int64_t n, int minvalues, void *stream);
 
 // Near/far interaction lists over test nodes, plus the trial-side transposes.
 struct Partition {

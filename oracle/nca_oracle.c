@@ -184,9 +184,10 @@ static double d2pts(const double *a, const double *b) {
 /* Split perm[b:e) into two stable parts; returns the size of the first part. */
 /* Sums over a cluster's points are taken in chunks of KMEANS_CHUNK consecutive points: each
  * chunk summed in order from zero, the chunk sums added in chunk order (for clusters of at most
- * one chunk this is the plain ordered sum). The library's planner splits large clusters across
- * host threads by these chunks and gets the same bits. */
-#define KMEANS_CHUNK 8192
+ * one chunk this is the plain ordered sum); the same for the node centres. The library's planner
+ * splits large clusters across host threads, and its device tree across GPU threads, by these
+ * chunks and gets the same bits. */
+#define KMEANS_CHUNK 256
 
 static int kmeans_split(const double *pts, int *perm, int b, int e, int *assign, int *tmp) {
     int cnt = e - b;
@@ -292,11 +293,18 @@ static int kmeans_split(const double *pts, int *perm, int b, int e, int *assign,
 
 static void node_ball(const double *pts, const int *perm, int b, int e, double *c, double *r) {
     double s[3] = {0, 0, 0};
-    for (int i = b; i < e; ++i) {
-        const double *p = pts + 3 * (long)perm[i];
-        s[0] += p[0];
-        s[1] += p[1];
-        s[2] += p[2];
+    for (int c0 = b; c0 < e; c0 += KMEANS_CHUNK) {
+        const int c1 = c0 + KMEANS_CHUNK < e ? c0 + KMEANS_CHUNK : e;
+        double part[3] = {0, 0, 0};
+        for (int i = c0; i < c1; ++i) {
+            const double *p = pts + 3 * (long)perm[i];
+            part[0] += p[0];
+            part[1] += p[1];
+            part[2] += p[2];
+        }
+        s[0] += part[0];
+        s[1] += part[1];
+        s[2] += part[2];
     }
     int cnt = e - b;
     for (int d = 0; d < 3; ++d)
