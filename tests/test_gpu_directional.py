@@ -104,6 +104,7 @@ def test_directional_against_oracle(name, make, k, tol, minvalues):
         assert relerr(W @ X, A @ X) < 1e-5, b
         U = cgauss((nt, b), 40 + b)
         assert relerr(W.H @ U, A.H @ U) < 1e-5, b
+        assert relerr(W.T @ U, A.T @ U) < 1e-5, b
 
 
 def test_directional_structure_and_limits():
