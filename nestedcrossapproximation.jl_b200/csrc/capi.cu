@@ -112,6 +112,94 @@ struct PinnedBuf {
     }
 };
 
+// Page-locked staging blocks for the builds' plan uploads, kept for the process and handed out
+// to the threads of later builds (uploads from pageable vectors go through the driver's staging
+// at a few GB/s and serialise across threads; from page-locked memory they are DMA copies).
+// Blocks beyond kPinnedKeep bytes in total are freed when returned.
+class PinnedPool {
+  public:
+    struct Block {
+        unsigned char *p = nullptr;
+        size_t n = 0;
+    };
+    static PinnedPool &get() {
+        static PinnedPool pool;
+        return pool;
+    }
+    Block acquire(size_t n) {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            size_t best = free_.size();
+            for (size_t i = 0; i < free_.size(); ++i)
+                if (free_[i].n >= n && (best == free_.size() || free_[i].n < free_[best].n)) best = i;
+            if (best < free_.size()) {
+                const Block b = free_[best];
+                free_.erase(free_.begin() + long(best));
+                kept_ -= b.n;
+                return b;
+            }
+        }
+        Block b;
+        b.n = std::max<size_t>((n + (size_t(64) << 20) - 1) & ~((size_t(64) << 20) - 1), size_t(64) << 20);
+        if (cudaHostAlloc(reinterpret_cast<void **>(&b.p), b.n, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            b.n = 0;
+        }
+        return b;
+    }
+    void release(Block b) {
+        if (!b.p) return;
+        std::lock_guard<std::mutex> g(mu_);
+        if (kept_ + b.n > kPinnedKeep) {
+            cudaFreeHost(b.p);
+            return;
+        }
+        kept_ += b.n;
+        free_.push_back(b);
+    }
+
+  private:
+    static constexpr size_t kPinnedKeep = size_t(2) << 30;
+    std::mutex mu_;
+    std::vector<Block> free_;
+    size_t kept_ = 0;
+};
+
+// Uploads through one page-locked block (pageable copies when no block could be had); the block
+// goes back to the pool once the stream has finished the copies.
+class StagedUploads {
+  public:
+    StagedUploads(size_t bytes, cudaStream_t s) : s_(s), b_(PinnedPool::get().acquire(bytes + 256)) {}
+    ~StagedUploads() {
+        if (b_.p) {
+            cudaStreamSynchronize(s_);
+            PinnedPool::get().release(b_);
+        }
+    }
+    template <typename T>
+    void up(DBuf<T> &d, const std::vector<T> &v) {
+        d.alloc(v.size());
+        if (v.empty()) return;
+        const size_t bytes = sizeof(T) * v.size();
+        used_ = (used_ + 15) & ~size_t(15);
+        if (b_.p && used_ + bytes <= b_.n) {
+            std::memcpy(b_.p + used_, v.data(), bytes);
+            CK(cudaMemcpyAsync(d.p, b_.p + used_, bytes, cudaMemcpyHostToDevice, s_));
+            used_ += bytes;
+        } else {
+            CK(cudaMemcpyAsync(d.p, v.data(), bytes, cudaMemcpyHostToDevice, s_));
+        }
+    }
+    StagedUploads(const StagedUploads &) = delete;
+    StagedUploads &operator=(const StagedUploads &) = delete;
+
+  private:
+    cudaStream_t s_;
+    PinnedPool::Block b_;
+    size_t used_ = 0;
+};
+
 template <typename T>
 std::vector<T> download_now(const DBuf<T> &b, size_t n) {
     std::vector<T> h(n);
@@ -1314,16 +1402,26 @@ struct StageBuilder {
                 trec[i] = WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], rows[o], 0};
             }
         }
+        // records of the tensor-core gathers only if some group takes them
+        bool any_tc = false;
+        for (size_t g = 0; g + 1 < group_ptr.size(); ++g) any_tc = any_tc || !wide_group(group_maxrows[g], group_work[g]);
+        if (!any_tc) trec.clear();
         if (mark) mark("records");
-        G.outputs.upload(order, s);
-        G.wout.upload(rec, s);
-        G.tout.upload(trec, s);
-        G.rows.upload(rows, s);
-        G.out.upload(out, s);
-        G.segptr.upload(segptr, s);
-        G.moff.upload(moff, s);
-        G.w.upload(w, s);
-        G.voff.upload(voff, s);
+        const size_t bytes = sizeof(int32_t) * (order.size() + rows.size() + segptr.size() + w.size() + sld.size() +
+                                                crows.size() + ccols.size()) +
+                             sizeof(WideOut) * (rec.size() + trec.size()) +
+                             sizeof(int64_t) * (out.size() + moff.size() + voff.size() + soff.size() + doff.size()) +
+                             16 * 16;
+        StagedUploads up(bytes, s);
+        up.up(G.outputs, order);
+        up.up(G.wout, rec);
+        up.up(G.tout, trec);
+        up.up(G.rows, rows);
+        up.up(G.out, out);
+        up.up(G.segptr, segptr);
+        up.up(G.moff, moff);
+        up.up(G.w, w);
+        up.up(G.voff, voff);
         if (mark) mark("plan uploaded");
         if (!src) return;
         G.M.alloc(size_t(store));
@@ -1332,11 +1430,11 @@ struct StageBuilder {
         for (size_t i = 0; i < crows.size(); ++i) G.entries += int64_t(crows[i]) * ccols[i];
         G.ncopies = int64_t(crows.size());
         if (!crows.empty()) {
-            G.c_soff.upload(soff, s);
-            G.c_doff.upload(doff, s);
-            G.c_ld.upload(sld, s);
-            G.c_rows.upload(crows, s);
-            G.c_cols.upload(ccols, s);
+            up.up(G.c_soff, soff);
+            up.up(G.c_doff, doff);
+            up.up(G.c_ld, sld);
+            up.up(G.c_rows, crows);
+            up.up(G.c_cols, ccols);
             launch_copy_blocks<double2>(src, G.c_soff.p, G.c_ld.p, G.c_rows.p, G.c_cols.p, G.c_doff.p, G.ncopies,
                                         G.M.p, s);
             CK(cudaGetLastError());
