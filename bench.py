@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--nrhs", type=int, default=16)
     p.add_argument("--wideband-points", type=int, default=0, help="point count of the wideband workload")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--builds", type=int, default=3,
+                   help="timed builds of each wideband form; the median is reported")
     p.add_argument("--profile-stages", action="store_true", help="print per-stage times to stderr")
     p.add_argument("--profile-run", action="store_true",
                    help="wideband workload for profiler captures: one mixed-precision build and `steps` block "
@@ -617,6 +619,22 @@ def dir_stage_bytes(info, b, e):
     return e * xe + e * info["coupling_entries"] + e * info["near_entries"]
 
 
+def timed_builds(N, pts, k, local, mixed, reps):
+    """`reps` builds of the same wideband core, each freed before the next: the last core, the
+    median build time and every build time."""
+    import gc
+    import torch
+    times, core = [], None
+    for _ in range(max(reps, 1)):
+        if core is not None:
+            del core
+            gc.collect()
+            torch.cuda.synchronize()
+        core, t = wideband_core(N, pts, k, local, mixed)
+        times.append(t)
+    return core, float(np.median(times)), times
+
+
 def profile_wideband(args, N, L, pts, k, local, n, nvec, Xd, Yd):
     """--profile-run: the batched mixed form's build and `steps` block products of 100 columns
     (after `warmup` untimed ones), with the library's stage events; one JSON line. The command
@@ -668,7 +686,7 @@ def run_wideband(args):
     gc.collect()
     torch.cuda.synchronize()
     # plain FP64 form: FP64-only build, then 100 single-vector FP64 matvecs
-    core, build_plain = wideband_core(N, pts, k, local, False)
+    core, build_plain, plain_times = timed_builds(N, pts, k, local, False, args.builds)
     W64 = N.H2Workspace(core, max_nrhs=1)
 
     def seq():
@@ -690,7 +708,7 @@ def run_wideband(args):
     gc.collect()
     torch.cuda.synchronize()
     # batched mixed form: the build with complex-FP32 stores, the 100 vectors as one block
-    core, build_mixed = wideband_core(N, pts, k, local, True)
+    core, build_mixed, mixed_times = timed_builds(N, pts, k, local, True, args.builds)
     info = info_dict(core)
     W = N.H2Workspace(core, np.complex64, max_nrhs=16)
     W.set_profiling(True)
@@ -793,6 +811,8 @@ def run_wideband(args):
                                "small outputs on the FP32 pipe, leaf outputs on the tcgen05 tensor cores)",
                        "l2": "inputs larger than L2 (FP32 stores %.1f GB per step)" % (8 * store_entries(info) / 1e9),
                        "build_s": build_mixed, "build_s_plain_f64": build_plain,
+                       "build_s_samples": {"batched_mixed": mixed_times, "plain_f64": plain_times,
+                                           "reported": "median"},
                        "build_device_s": info["build_seconds"], "stored_gb_f64": E * store_entries(info) / 1e9,
                        "relerr_vs_dense_rows": {"plain_f64": err64, "batched_mixed": errmix, "bar_north_star": 1e-4,
                                                 "bar_reference_tests_10tol": 1e-3},

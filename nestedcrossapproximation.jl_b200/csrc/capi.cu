@@ -25,6 +25,8 @@
 #include <thread>
 #include <vector>
 
+#include <sys/mman.h>
+
 #include "apply_kernels.cuh"
 #include "build_kernels.cuh"
 #include "nca_internal.h"
@@ -166,6 +168,91 @@ class PinnedPool {
     size_t kept_ = 0;
 };
 
+// Host blocks for the builds' large transient arrays (gather plan lists and records), kept for
+// the process and handed to the threads of later builds. A fresh page costs a fault and a zero
+// fill on first touch: on the build host, 8 threads each filling 96 MB of fresh memory took 63-67
+// ms against 15 ms for memory already mapped. Blocks are mapped with transparent huge pages
+// requested (half the first-touch cost of 4 KB pages), sized in powers of two from 2 MiB and
+// kept on free lists by size, up to kHostKeep bytes; smaller requests go to operator new.
+class HostPool {
+  public:
+    static constexpr size_t kMin = size_t(2) << 20;
+    static HostPool &get() {
+        static HostPool *pool = new HostPool;  // never destroyed: blocks may outlive static teardown
+        return *pool;
+    }
+    static size_t block_size(size_t bytes) {
+        size_t c = kMin;
+        while (c < bytes) c <<= 1;
+        return c;
+    }
+    void *acquire(size_t cap) {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            auto it = free_.find(cap);
+            if (it != free_.end() && !it->second.empty()) {
+                void *p = it->second.back();
+                it->second.pop_back();
+                kept_ -= cap;
+                return p;
+            }
+        }
+        void *p = mmap(nullptr, cap, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+        if (p == MAP_FAILED) throw std::bad_alloc();
+        madvise(p, cap, MADV_HUGEPAGE);  // advice only: ignored where huge pages are off
+        return p;
+    }
+    void release(void *p, size_t cap) {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            if (kept_ + cap <= kHostKeep) {
+                free_[cap].push_back(p);
+                kept_ += cap;
+                return;
+            }
+        }
+        munmap(p, cap);
+    }
+
+  private:
+    static constexpr size_t kHostKeep = size_t(4) << 30;
+    std::mutex mu_;
+    std::unordered_map<size_t, std::vector<void *>> free_;
+    size_t kept_ = 0;
+};
+
+// std::vector allocator over HostPool for arrays of 2 MiB and more
+template <typename T>
+struct PoolAlloc {
+    using value_type = T;
+    PoolAlloc() = default;
+    template <typename U>
+    PoolAlloc(const PoolAlloc<U> &) {}
+    T *allocate(size_t n) {
+        const size_t bytes = n * sizeof(T);
+        if (bytes < HostPool::kMin) return static_cast<T *>(::operator new(bytes));
+        return static_cast<T *>(HostPool::get().acquire(HostPool::block_size(bytes)));
+    }
+    void deallocate(T *p, size_t n) {
+        const size_t bytes = n * sizeof(T);
+        if (bytes < HostPool::kMin) {
+            ::operator delete(p);
+            return;
+        }
+        HostPool::get().release(p, HostPool::block_size(bytes));
+    }
+    template <typename U>
+    bool operator==(const PoolAlloc<U> &) const {
+        return true;
+    }
+    template <typename U>
+    bool operator!=(const PoolAlloc<U> &) const {
+        return false;
+    }
+};
+template <typename T>
+using hvec = std::vector<T, PoolAlloc<T>>;
+
 // Uploads through one page-locked block (pageable copies when no block could be had); the block
 // goes back to the pool once the stream has finished the copies.
 class StagedUploads {
@@ -177,8 +264,8 @@ class StagedUploads {
             PinnedPool::get().release(b_);
         }
     }
-    template <typename T>
-    void up(DBuf<T> &d, const std::vector<T> &v) {
+    template <typename T, typename A>
+    void up(DBuf<T> &d, const std::vector<T, A> &v) {
         d.alloc(v.size());
         if (v.empty()) return;
         const size_t bytes = sizeof(T) * v.size();
@@ -1250,11 +1337,11 @@ struct StageBuilder {
     std::vector<int32_t> group_ptr{0};
     std::vector<int> group_maxrows;
     std::vector<double> group_work;
-    std::vector<int32_t> rows, segptr{0}, w;
-    std::vector<int64_t> out, moff, voff, work;
+    hvec<int32_t> rows, segptr{0}, w;
+    hvec<int64_t> out, moff, voff, work;
     // sub-matrix copies from the source store into the stage store
-    std::vector<int64_t> soff, doff;
-    std::vector<int32_t> sld, crows, ccols;
+    hvec<int64_t> soff, doff;
+    hvec<int32_t> sld, crows, ccols;
     int64_t store = 0;
     int cur_max = 0;
     // room for the outputs, segments and copies a stage is known to have at most
@@ -1340,7 +1427,7 @@ struct StageBuilder {
         if (tag && getenv("NCA_DIR_STATS")) print_stats(tag);
         // outputs of each group largest work first (shorter tail of the last wave): a stable
         // counting sort on the work, linear in the outputs
-        std::vector<int32_t> order(rows.size());
+        hvec<int32_t> order(rows.size());
         std::vector<int64_t> cnt;
         for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
             const int32_t b = group_ptr[g], e = group_ptr[g + 1];
@@ -1359,7 +1446,7 @@ struct StageBuilder {
         G.wide_begin.clear();
         G.wide_count.clear();
         G.wide_nr.clear();
-        std::vector<WideOut> rec;
+        hvec<WideOut> rec;
         rec.reserve(order.size());
         for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
             const int32_t b = group_ptr[g], e = group_ptr[g + 1];
@@ -1392,7 +1479,7 @@ struct StageBuilder {
         G.group_work = group_work;
         // records of the tensor-core gathers: the groups the all-column FP32 kernel does not take
         // (left zero elsewhere)
-        std::vector<WideOut> trec(order.size());
+        hvec<WideOut> trec(order.size());
         for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
             if (wide_group(group_maxrows[g], group_work[g])) continue;
             for (int32_t i = group_ptr[g]; i < group_ptr[g + 1]; ++i) {
@@ -1406,7 +1493,9 @@ struct StageBuilder {
         bool any_tc = false;
         for (size_t g = 0; g + 1 < group_ptr.size(); ++g) any_tc = any_tc || !wide_group(group_maxrows[g], group_work[g]);
         if (!any_tc) trec.clear();
-        if (mark) mark("records");
+        if (mark)
+            mark("records (" + std::to_string(rows.size()) + " outputs, " + std::to_string(w.size()) + " segments, " +
+                 std::to_string(crows.size()) + " copies)");
         const size_t bytes = sizeof(int32_t) * (order.size() + rows.size() + segptr.size() + w.size() + sld.size() +
                                                 crows.size() + ccols.size()) +
                              sizeof(WideOut) * (rec.size() + trec.size()) +
@@ -1422,7 +1511,7 @@ struct StageBuilder {
         up.up(G.moff, moff);
         up.up(G.w, w);
         up.up(G.voff, voff);
-        if (mark) mark("plan uploaded");
+        if (mark) mark("plan uploaded (" + std::to_string(bytes >> 20) + " MiB)");
         if (!src) return;
         G.M.alloc(size_t(store));
         if (mark) mark("store allocated");
@@ -1502,7 +1591,7 @@ struct PhaseTimer {
 // side's X, h_xoff, ranks and rows in d.
 void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
                        const std::vector<std::vector<int32_t>> &bylevel, cudaStream_t s, const nca_build_opts *o,
-                       PhaseTimer &timer, const std::string &side) {
+                       PhaseTimer &timer, const std::string &side, const std::function<void()> &ranks_known) {
     const int maxrank = c->maxrank;
     const nca::DirSide &pl = d.plan;
     const nca::Tree &T = c->tree[sd], &Ft = c->tree[1 - sd];
@@ -1701,6 +1790,7 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     d.h_xoff.assign(ni + 1, 0);
     for (int it = 0; it < ni; ++it) d.h_xoff[it] = cpos[it] >= 0 ? cpos[it] : 0;
     d.h_xoff[ni] = total;
+    ranks_known();  // the gather plans list from here while the levels are joined on the device
     d.X.alloc(size_t(std::max<int64_t>(total, 1)));
     {
         int64_t off = 0;
@@ -1818,8 +1908,12 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     }).share();
     std::vector<std::vector<int32_t>> bylevel[2];  // items per level, filled by each side's task
     int64_t basis_entries[2] = {0, 0}, transfer_entries[2] = {0, 0};
-    std::promise<void> sided[2];
+    // a side's ranks, rows, operator offsets and coefficient offsets are known (side_ranked) before
+    // its operators are joined and transposed on the device (side_done)
+    std::promise<void> sided[2], ranked[2];
     std::shared_future<void> side_done[2] = {sided[0].get_future().share(), sided[1].get_future().share()};
+    std::shared_future<void> side_ranked[2] = {ranked[0].get_future().share(), ranked[1].get_future().share()};
+    std::atomic<bool> ranked_set[2] = {false, false};
     auto side_task = [&](int sd) {
         const cudaStream_t s = ss[sd];
         DirItems &d = D->side[sd];
@@ -1842,6 +1936,17 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         d.nitems = ni;
         bylevel[sd].assign(T.nlevels, {});
         for (int it = 0; it < ni; ++it) bylevel[sd][T.level[pl.item_node[it]]].push_back(it);
+        auto known = [&]() {
+            d.h_cptr.assign(ni + 1, 0);
+            for (int it = 0; it < ni; ++it) {
+                d.h_cptr[it + 1] = d.h_cptr[it] + d.h_rank[it];
+                const int64_t e = int64_t(d.h_rank[it]) * d.h_nrows[it];
+                (pl.item_basis[it] ? basis_entries[sd] : transfer_entries[sd]) += e;
+            }
+            ranked_set[sd] = true;
+            ranked[sd].set_value();
+            timer.mark(side + "ranks known");
+        };
         if (sv) {
             // a saved skeleton: the items' operators and pivots as the build left them
             const SavedSide &v = sv->side[sd];
@@ -1856,17 +1961,12 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             d.h_rank = v.rank;
             d.h_nrows = v.nrows;
             d.h_xoff = v.xoff;
+            known();
             d.X.upload(v.X, s);
         } else {
-            compress_dir_side(c, d, sd, pts[sd], bylevel[sd], s, o, timer, side);
+            compress_dir_side(c, d, sd, pts[sd], bylevel[sd], s, o, timer, side, known);
         }
         d.xoff.upload(d.h_xoff, s);
-        d.h_cptr.assign(ni + 1, 0);
-        for (int it = 0; it < ni; ++it) {
-            d.h_cptr[it + 1] = d.h_cptr[it] + d.h_rank[it];
-            const int64_t e = int64_t(d.h_rank[it]) * d.h_nrows[it];
-            (pl.item_basis[it] ? basis_entries[sd] : transfer_entries[sd]) += e;
-        }
         d.XT.alloc(d.X.n);
         launch_transpose_blocks<double2>(d.X.p, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, ni, d.XT.p, s);
         CK(cudaGetLastError());
@@ -1965,12 +2065,12 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         const int64_t xin = TI.npoints;
         int64_t yo = 0;
         auto input_side_built = [&]() {
-            side_done[I].get();
+            side_ranked[I].get();
             yo = xin + di.h_cptr.back();
         };
         // up: input-side items, deepest level first
         if (stage == 0) {
-            side_done[I].get();
+            side_ranked[I].get();
             StageBuilder B;
             const size_t seg = size_t(di.nitems) + di.plan.item_chidx.size();
             B.reserve(size_t(di.nitems), seg, seg);
@@ -1997,6 +2097,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 B.end_group();
             }
             timer.mark("gather plan " + std::to_string(task) + ": up listed");
+            side_done[I].get();
             B.finish(pr.up, di.XT.p, s, m ? "T up" : "N up", plan_mark("up"));
             timer.mark("gather plan " + std::to_string(task) + ": up");
         }
@@ -2005,7 +2106,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             if (m == 0) {
                 // every way out of this block settles `coupled`, which the transposed plan awaits
                 try {
-                    side_done[O].get();
+                    side_ranked[O].get();
                     input_side_built();
                     pairs_f.get();
                     couplings();
@@ -2016,7 +2117,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 }
             } else {
                 coupled_done.get();
-                side_done[O].get();
+                side_ranked[O].get();
                 input_side_built();
             }
             StageBuilder B;
@@ -2044,11 +2145,11 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         if (stage == 2) {
             // listed with output rows relative to yo (the other side may still be compressing),
             // moved by yo once it is known
-            side_done[O].get();
+            side_ranked[O].get();
             // parents of every child item (CSR in parent order), with the child's row offset in
             // the parent's X
-            std::vector<int32_t> pptr(size_t(dout.nitems) + 1, 0), ppar;
-            std::vector<int64_t> prow;
+            hvec<int32_t> pptr(size_t(dout.nitems) + 1, 0), ppar;
+            hvec<int64_t> prow;
             auto each_child = [&](auto fn) {
                 for (int it = 0; it < dout.nitems; ++it) {
                     if (dout.h_rank[it] <= 0 || dout.plan.item_basis[it]) continue;
@@ -2064,7 +2165,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             for (int it = 0; it < dout.nitems; ++it) pptr[size_t(it) + 1] += pptr[it];
             ppar.resize(pptr.back());
             prow.resize(pptr.back());
-            std::vector<int32_t> fill(pptr.begin(), pptr.end() - 1);
+            hvec<int32_t> fill(pptr.begin(), pptr.end() - 1);
             each_child([&](int ch, int it, int64_t c0) {
                 ppar[fill[ch]] = it;
                 prow[fill[ch]++] = c0;
@@ -2088,12 +2189,13 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             timer.mark("gather plan " + std::to_string(task) + ": down listed");
             input_side_built();
             B.shift(yo, true);
+            side_done[O].get();
             B.finish(pr.down, dout.X.p, s, m ? "T down" : "N down", plan_mark("down"));
             timer.mark("gather plan " + std::to_string(task) + ": down");
         }
         // leaves: every basis item whose cluster contains the leaf, then the near blocks
         if (stage == 3) {
-            side_done[O].get();
+            side_ranked[O].get();
             near_f.get();
             StageBuilder B;
             const nca::DirSide &pl = dout.plan;
@@ -2121,6 +2223,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             timer.mark("gather plan " + std::to_string(task) + ": leaves listed");
             input_side_built();
             B.shift(yo, false);
+            side_done[O].get();
             B.finish(pr.leaves, dout.X.p, s, m ? "T leaves" : "N leaves", plan_mark("leaves"));
             timer.mark("gather plan " + std::to_string(task) + ": leaves");
         }
@@ -2135,6 +2238,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             try {
                 side_task(task);
             } catch (...) {
+                if (!ranked_set[task]) ranked[task].set_exception(std::current_exception());
                 sided[task].set_exception(std::current_exception());
                 throw;
             }
