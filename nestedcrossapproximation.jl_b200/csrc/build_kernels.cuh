@@ -121,7 +121,6 @@ struct IacaArgs {
     const int32_t *item_basis, *item_chptr, *item_chidx;          // item mode (mim.item_node set)
     const int32_t *items;  // the launch's items
     int nitems;
-    int32_t *cursor;       // zero at launch
     int32_t *rank, *nrows, *piv, *cpiv;  // piv, cpiv: maxrank per item (cpiv optional)
     double2 *X;            // item slots of rows x min(maxrank, rows, far points) entries at xoff
     const int64_t *xoff;   // indexed by item, or by position in `items` with xoff_by_position

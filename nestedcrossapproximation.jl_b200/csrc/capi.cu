@@ -90,10 +90,14 @@ struct DBuf {
     }
 };
 
-// uploads v into the scratch buffer b, reallocating only when b is too small
+// uploads v into the scratch buffer b, reallocating only when b is too small (the old array
+// goes to `later`)
 template <typename T>
-void upload_reuse(DBuf<T> &b, const std::vector<T> &v, cudaStream_t s) {
-    if (!b.p || v.size() > b.n) b.alloc(v.size());
+void upload_reuse(DBuf<T> &b, const std::vector<T> &v, cudaStream_t s, std::vector<void *> &later) {
+    if (!b.p || v.size() > b.n) {
+        b.defer(later);  // cudaFree here would wait for the work of every stream on the device
+        b.alloc(v.size());
+    }
     if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
 }
 
@@ -123,6 +127,7 @@ class PinnedPool {
     struct Block {
         unsigned char *p = nullptr;
         size_t n = 0;
+        bool fresh = false;  // allocated by this acquire (not taken from the pool)
     };
     static PinnedPool &get() {
         static PinnedPool pool;
@@ -143,6 +148,7 @@ class PinnedPool {
         }
         Block b;
         b.n = std::max<size_t>((n + (size_t(64) << 20) - 1) & ~((size_t(64) << 20) - 1), size_t(64) << 20);
+        b.fresh = true;
         if (cudaHostAlloc(reinterpret_cast<void **>(&b.p), b.n, cudaHostAllocDefault) != cudaSuccess) {
             cudaGetLastError();
             b.p = nullptr;
@@ -158,6 +164,7 @@ class PinnedPool {
             return;
         }
         kept_ += b.n;
+        b.fresh = false;
         free_.push_back(b);
     }
 
@@ -171,9 +178,10 @@ class PinnedPool {
 // Host blocks for the builds' large transient arrays (gather plan lists and records), kept for
 // the process and handed to the threads of later builds. A fresh page costs a fault and a zero
 // fill on first touch: on the build host, 8 threads each filling 96 MB of fresh memory took 63-67
-// ms against 15 ms for memory already mapped. Blocks are mapped with transparent huge pages
-// requested (half the first-touch cost of 4 KB pages), sized in powers of two from 2 MiB and
-// kept on free lists by size, up to kHostKeep bytes; smaller requests go to operator new.
+// ms against 15 ms for memory already mapped. Blocks are sized in powers of two from 2 MiB and
+// kept on free lists by size, up to kHostKeep bytes; smaller requests go to operator new. (No
+// huge-page advice: with the hosts' defrag=madvise setting a fault in an advised range may stall
+// on memory compaction, and the driver's own mappings wait behind it.)
 class HostPool {
   public:
     static constexpr size_t kMin = size_t(2) << 20;
@@ -199,7 +207,6 @@ class HostPool {
         }
         void *p = mmap(nullptr, cap, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
         if (p == MAP_FAILED) throw std::bad_alloc();
-        madvise(p, cap, MADV_HUGEPAGE);  // advice only: ignored where huge pages are off
         return p;
     }
     void release(void *p, size_t cap) {
@@ -280,6 +287,7 @@ class StagedUploads {
     }
     StagedUploads(const StagedUploads &) = delete;
     StagedUploads &operator=(const StagedUploads &) = delete;
+    bool fresh() const { return b_.fresh; }
 
   private:
     cudaStream_t s_;
@@ -1042,7 +1050,7 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
         }
     } eg{ev0, ev1};
     DBuf<int32_t> status;
-    status.alloc(5);  // [flag, node, a, b], IACA node cursor
+    status.alloc(4);  // [flag, node, a, b]
     CK(cudaEventRecord(ev0, s));
     for (int sd = 0; sd < 2; ++sd) {
         DevSide &d = c->side[sd];
@@ -1137,7 +1145,6 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
             ia.maxrank = maxrank;
             ia.tol = a.tol;
             ia.status = status.p;
-            ia.cursor = status.p + 4;
             for (size_t l = 0; l + 1 < lv_ptr.size(); ++l) {
                 const int cnt = lv_ptr[l + 1] - lv_ptr[l];
                 if (cnt == 0) continue;
@@ -1145,7 +1152,6 @@ void build_core(nca_core *c, const double *tp, int64_t nt, const double *sp, int
                     throw Failure(NCA_ERR_ARG, "a cluster block has up to " + std::to_string(lv_mcap[l]) +
                                                    " rows; the IACA kernel holds at most " +
                                                    std::to_string(nca::iaca_max_rows()) + " (reduce the leaf size)");
-                CK(cudaMemsetAsync(status.p + 4, 0, sizeof(int32_t), s));
                 ia.items = nodes.p + lv_ptr[l];
                 ia.nitems = cnt;
                 launch_iaca(ia, lv_mcap[l], s);
@@ -1502,6 +1508,7 @@ struct StageBuilder {
                              sizeof(int64_t) * (out.size() + moff.size() + voff.size() + soff.size() + doff.size()) +
                              16 * 16;
         StagedUploads up(bytes, s);
+        if (mark) mark(up.fresh() ? "staging block allocated" : "staging block reused");
         up.up(G.outputs, order);
         up.up(G.wout, rec);
         up.up(G.tout, trec);
@@ -1591,7 +1598,8 @@ struct PhaseTimer {
 // side's X, h_xoff, ranks and rows in d.
 void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
                        const std::vector<std::vector<int32_t>> &bylevel, cudaStream_t s, const nca_build_opts *o,
-                       PhaseTimer &timer, const std::string &side, const std::function<void()> &ranks_known) {
+                       PhaseTimer &timer, const std::string &side, const std::function<void()> &ranks_known,
+                       cudaStream_t hs) {
     const int maxrank = c->maxrank;
     const nca::DirSide &pl = d.plan;
     const nca::Tree &T = c->tree[sd], &Ft = c->tree[1 - sd];
@@ -1636,7 +1644,7 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     timer.mark(side + "centroids uploaded");
     // the side's items, level by level
     DBuf<int32_t> status;
-    status.alloc(5);  // [flag, item, a, b], item cursor
+    status.alloc(4);  // [flag, item, a, b]
     d.item_node.upload(pl.item_node, s);
     d.item_basis.upload(pl.item_basis, s);
     d.item_chptr.upload(pl.item_chptr, s);
@@ -1679,7 +1687,6 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     a.maxrank = maxrank;
     a.tol = sd == 0 ? o->tol_test : o->tol_trial;
     a.status = status.p;
-    a.cursor = status.p + 4;
     // Level by level, deepest first: the rows of a nested item are its children's actual
     // ranks, so each level's X is allocated for min(maxrank, rows, far points) columns, then
     // compacted to the ranks found before the next level runs.
@@ -1718,8 +1725,8 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
             mc = int(std::max<int64_t>(mc, m));
         }
         if (items.empty()) continue;
-        upload_reuse(dffptr, far.ptr, s);
-        upload_reuse(dffnodes, far.nodes, s);
+        upload_reuse(dffptr, far.ptr, s, d.later);
+        upload_reuse(dffnodes, far.nodes, s, d.later);
         a.mim.ffptr = dffptr.p;
         a.mim.ffnodes = dffnodes.p;
         if (mc > nca::iaca_max_rows())
@@ -1732,10 +1739,13 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
             timer.mark(side + "level " + std::to_string(lev) + " scratch of " + std::to_string(bound >> 16) +
                        " x 1 MiB allocated");
         }
-        upload_reuse(dlvoff, lvoff, s);
-        upload_reuse(nodes, items, s);
+        upload_reuse(dlvoff, lvoff, s, d.later);
+        upload_reuse(nodes, items, s, d.later);
         const int nl = int(items.size());
-        if (drk.n < 2 * size_t(nl)) drk.alloc(2 * size_t(nl));
+        if (drk.n < 2 * size_t(nl)) {
+            drk.defer(d.later);
+            drk.alloc(2 * size_t(nl));
+        }
         status.zero(s);
         a.X = chunk.p;
         a.xoff = dlvoff.p;
@@ -1774,11 +1784,12 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
         levelX.emplace_back(new DBuf<double2>());
         levelX.back()->alloc(size_t(std::max<int64_t>(lt, 1)));
         if (lt > 0) {
-            upload_reuse(ddo, doff, s);
+            // on the high-priority stream: its blocks start ahead of the other side's IACA blocks
+            upload_reuse(ddo, doff, hs, d.later);
             launch_copy_blocks<double2>(chunk.p, dlvoff.p, drk.p + nl, drk.p + nl, drk.p, ddo.p, int64_t(nl),
-                                        levelX.back()->p, s);
+                                        levelX.back()->p, hs);
             CK(cudaGetLastError());
-            CK(cudaStreamSynchronize(s));
+            CK(cudaStreamSynchronize(hs));
         }
         levelItems.push_back(items);
         for (int it : items) cpos[it] += total;
@@ -1835,6 +1846,16 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     CK(cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking));
     StreamGuard sg1{s1};
     const cudaStream_t ss[2] = {s, s1};
+    // high-priority streams for the short steps between a side's IACA levels (the compaction):
+    // their blocks are scheduled before the pending blocks of the other side's IACA launch
+    int prio_low = 0, prio_high = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    cudaStream_t h0s, h1s;
+    CK(cudaStreamCreateWithPriority(&h0s, cudaStreamNonBlocking, prio_high));
+    StreamGuard hg0{h0s};
+    CK(cudaStreamCreateWithPriority(&h1s, cudaStreamNonBlocking, prio_high));
+    StreamGuard hg1{h1s};
+    const cudaStream_t hs[2] = {h0s, h1s};
     CK(cudaStreamSynchronize(s));
     cudaEvent_t ev0, ev1;
     CK(cudaEventCreate(&ev0));
@@ -1964,7 +1985,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             known();
             d.X.upload(v.X, s);
         } else {
-            compress_dir_side(c, d, sd, pts[sd], bylevel[sd], s, o, timer, side, known);
+            compress_dir_side(c, d, sd, pts[sd], bylevel[sd], s, o, timer, side, known, hs[sd]);
         }
         d.xoff.upload(d.h_xoff, s);
         d.XT.alloc(d.X.n);

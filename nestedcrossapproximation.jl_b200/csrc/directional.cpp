@@ -22,6 +22,8 @@
 #include <stdexcept>
 #include <thread>
 
+#include <immintrin.h>
+
 #include "nca_internal.h"
 
 namespace nca {
@@ -107,7 +109,8 @@ void candidate_directions(double diam, double k, double gamma, std::vector<doubl
     }
 }
 
-// 0-based index of the direction with the largest dot product (first on ties).
+// 0-based index of the direction with the largest dot product (first on ties), one candidate
+// at a time: the reference form of the search (the checks compare the planner's search with it).
 int nearest_direction(const std::vector<double> &dirs, const double *v) {
     const size_t n = dirs.size() / 3;
     int best = 0;
@@ -122,33 +125,92 @@ int nearest_direction(const std::vector<double> &dirs, const double *v) {
     return best;
 }
 
-// nearest_direction over the spherical Fibonacci candidates of candidate_directions (z_i =
-// 1 - 2 (i + 1/2) / n, descending): only the indices whose z lies within an angle of
-// 4 sqrt(4 pi / n) of v's polar angle are searched. That band holds every candidate within twice
-// the lattice's covering radius of v, so the largest dot product lies inside it, ahead of every
-// candidate outside by about 75 / n of |v|, far above the rounding of a three-term dot product.
-// Inside the band the dots are formed and compared as in the full search (ascending index, first
-// on ties), so the result is the full search's.
-int nearest_candidate(const std::vector<double> &dirs, const double *v) {
-    const int64_t n = int64_t(dirs.size() / 3);
-    const double r = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-    const double band = 4.0 * std::sqrt(4.0 * M_PI / double(n));
-    if (!(r > 0.0) || !std::isfinite(r) || band >= 0.5 * M_PI) return nearest_direction(dirs, v);
-    const double theta = std::acos(std::max(-1.0, std::min(1.0, v[2] / r)));
-    const double zhi = std::cos(std::max(0.0, theta - band)), zlo = std::cos(std::min(M_PI, theta + band));
-    // z_i <= zhi  <=>  i >= (1 - zhi) n / 2 - 1/2;  z_i >= zlo  <=>  i <= (1 - zlo) n / 2 - 1/2
-    const int64_t i0 = std::max<int64_t>(0, int64_t(std::floor((1.0 - zhi) * double(n) / 2.0 - 0.5)) - 1);
-    const int64_t i1 = std::min<int64_t>(n - 1, int64_t(std::ceil((1.0 - zlo) * double(n) / 2.0 - 0.5)) + 1);
-    int64_t best = i0;
-    double bd = dirs[3 * i0] * v[0] + dirs[3 * i0 + 1] * v[1] + dirs[3 * i0 + 2] * v[2];
-    for (int64_t i = i0 + 1; i <= i1; ++i) {
-        const double d = dirs[3 * i] * v[0] + dirs[3 * i + 1] * v[1] + dirs[3 * i + 2] * v[2];
+// The candidates of one cluster as coordinate arrays (x[i], y[i], z[i]), i < n.
+struct Candidates {
+    std::vector<double> xyz;
+    const double *x = nullptr, *y = nullptr, *z = nullptr;
+    int64_t n = 0;
+    double band = 0.0, cb = 0.0, sb = 0.0;  // the search band's half angle, its cosine and sine
+    void set(const std::vector<double> &dirs) {
+        n = int64_t(dirs.size() / 3);
+        band = 4.0 * std::sqrt(4.0 * M_PI / double(n));
+        cb = std::cos(band);
+        sb = std::sin(band);
+        xyz.resize(3 * size_t(n));
+        for (int64_t i = 0; i < n; ++i) {
+            xyz[i] = dirs[3 * i];
+            xyz[n + i] = dirs[3 * i + 1];
+            xyz[2 * n + i] = dirs[3 * i + 2];
+        }
+        x = xyz.data();
+        y = x + n;
+        z = y + n;
+    }
+};
+
+// Index of the largest x_i v0 + y_i v1 + z_i v2 over i0 <= i <= i1, the first on ties. Every dot is
+// formed as (x v0 + y v1) + z v2 with each product and sum rounded (no fused multiply-add), four
+// candidates at a time: each lane keeps its largest dot and the first index reaching it, the lanes
+// are merged by value then index, and the tail follows in order.
+int64_t argmax_dot(const Candidates &c, int64_t i0, int64_t i1, const double *v) {
+    int64_t i = i0, best = i0;
+    double bd = -INFINITY;
+    if (i1 - i0 + 1 >= 8) {
+        const __m256d v0 = _mm256_set1_pd(v[0]), v1 = _mm256_set1_pd(v[1]), v2 = _mm256_set1_pd(v[2]);
+        const __m256d four = _mm256_set1_pd(4.0);
+        __m256d bv = _mm256_set1_pd(-INFINITY), bi = _mm256_setzero_pd();
+        __m256d idx = _mm256_setr_pd(double(i), double(i + 1), double(i + 2), double(i + 3));
+        for (; i + 3 <= i1; i += 4) {
+            const __m256d d = _mm256_add_pd(
+                _mm256_add_pd(_mm256_mul_pd(_mm256_loadu_pd(c.x + i), v0), _mm256_mul_pd(_mm256_loadu_pd(c.y + i), v1)),
+                _mm256_mul_pd(_mm256_loadu_pd(c.z + i), v2));
+            const __m256d gt = _mm256_cmp_pd(d, bv, _CMP_GT_OQ);
+            bv = _mm256_blendv_pd(bv, d, gt);
+            bi = _mm256_blendv_pd(bi, idx, gt);
+            idx = _mm256_add_pd(idx, four);
+        }
+        alignas(32) double lv[4], li[4];
+        _mm256_store_pd(lv, bv);
+        _mm256_store_pd(li, bi);
+        for (int l = 0; l < 4; ++l)
+            if (lv[l] > bd || (lv[l] == bd && int64_t(li[l]) < best)) {
+                bd = lv[l];
+                best = int64_t(li[l]);
+            }
+    }
+    for (; i <= i1; ++i) {
+        const double d = c.x[i] * v[0] + c.y[i] * v[1] + c.z[i] * v[2];
         if (d > bd) {
             bd = d;
             best = i;
         }
     }
-    return int(best);
+    return best;
+}
+
+// Index of the candidate nearest to direction v: the largest dot product, the first on ties
+// (nearest_direction). Over the spherical Fibonacci candidates of candidate_directions (z_i =
+// 1 - 2 (i + 1/2) / n, descending) only the indices whose z lies within an angle of
+// 4 sqrt(4 pi / n) of v's polar angle are searched. That band holds every candidate within twice
+// the lattice's covering radius of v, so the largest dot product lies inside it, ahead of every
+// candidate outside by about 75 / n of |v|, far above the rounding of a three-term dot product.
+// Inside the band the dots are formed and compared as in the full search, so the result is the
+// full search's.
+// The band's z limits cos(max(0, theta - band)) and cos(min(pi, theta + band)) are formed from
+// cos theta = v_z / |v| by the angle-sum formulas; their rounding (~1e-16) is far inside the one
+// index of slack added on each side (2 / n in z).
+int nearest_candidate(const Candidates &c, const double *v) {
+    const int64_t n = c.n;
+    const double r = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (!(r > 0.0) || !std::isfinite(r) || c.band >= 0.5 * M_PI) return int(argmax_dot(c, 0, n - 1, v));
+    const double ct = std::max(-1.0, std::min(1.0, v[2] / r));
+    const double st = std::sqrt(std::max(0.0, 1.0 - ct * ct));
+    const double zhi = ct >= c.cb ? 1.0 : ct * c.cb + st * c.sb;
+    const double zlo = ct <= -c.cb ? -1.0 : ct * c.cb - st * c.sb;
+    // z_i <= zhi  <=>  i >= (1 - zhi) n / 2 - 1/2;  z_i >= zlo  <=>  i <= (1 - zlo) n / 2 - 1/2
+    const int64_t i0 = std::max<int64_t>(0, int64_t(std::floor((1.0 - zhi) * double(n) / 2.0 - 0.5)) - 1);
+    const int64_t i1 = std::min<int64_t>(n - 1, int64_t(std::ceil((1.0 - zlo) * double(n) / 2.0 - 0.5)) + 1);
+    return int(argmax_dot(c, i0, i1, v));
 }
 
 }  // namespace
@@ -180,7 +242,8 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
     for (int node = 0; node < nn; ++node) lf[node] = is_lowfrequency(T, node, w);
     // the nodes of one level depend on their parents only: a level's nodes run on the host
     // threads, each writing its own entries (and its own range of the far-node list)
-    auto plan_node = [&](int level, int node, std::vector<double> &total, std::vector<int32_t> &slot) {
+    auto plan_node = [&](int level, int node, std::vector<double> &total, Candidates &cand,
+                         std::vector<int32_t> &slot) {
             const int p = T.parent[node];
             const bool hasfars = farptr[node + 1] > farptr[node];
             const bool hasparentvecs = p >= 0 && hasvec[p];
@@ -193,13 +256,14 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
             }
             if (!hasfars && !hasparentvecs) return;
             candidate_directions(2.0 * T.radius[node], w.k, w.gamma, total);
+            cand.set(total);
             const int b = farptr[node], nfar = farptr[node + 1] - b;
             std::vector<int32_t> nd(nfar);
             const double *c = &T.center[3 * size_t(node)];
             for (int i = 0; i < nfar; ++i) {
                 const double *cf = &F.center[3 * size_t(D.farnodes[b + i])];
                 const double v[3] = {c[0] - cf[0], c[1] - cf[1], c[2] - cf[2]};
-                nd[i] = nearest_candidate(total, v) + 1;
+                nd[i] = nearest_candidate(cand, v) + 1;
             }
             // far nodes grouped by direction (stable)
             std::vector<int32_t> order(nfar);
@@ -225,7 +289,7 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
                     const double *pv = &dirvec[p][3 * di];
                     const double v[3] = {c[0] - cp[0] + mult * pv[0], c[1] - cp[1] + mult * pv[1],
                                          c[2] - cp[2] + mult * pv[2]};
-                    map[di] = nearest_candidate(total, v) + 1;
+                    map[di] = nearest_candidate(cand, v) + 1;
                 }
                 // candidate -> 1-based position in uniq (0: not yet listed), instead of a search
                 // of uniq per parent direction
@@ -261,11 +325,12 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
         std::atomic<int> cursor{n0};
         auto work = [&]() {
             std::vector<double> total;
+            Candidates cand;
             std::vector<int32_t> slot;
             for (;;) {
                 const int node = cursor.fetch_add(1);
                 if (node >= n1) break;
-                plan_node(level, node, total, slot);
+                plan_node(level, node, total, cand, slot);
             }
         };
         const int use = std::max(1, std::min(nth, n1 - n0));

@@ -312,7 +312,7 @@ __device__ __noinline__ double2 oriented_entry(KernelParams K, bool own_is_test,
     return kernel_entry(K, qx, qy, qz, rx, ry, rz, qid, rid);
 }
 
-// IACA of every item of one level, one warp per item (items taken from an atomic cursor): tree
+// IACA of every item of one level, one warp per item: tree
 // mimicry picks the geometric columns one at a time, the column is evaluated on the item's rows
 // (lane l holds rows l + 32 q), eliminated against the accepted crosses, tested by the
 // extrapolated Frobenius stop (||r||^2 k <= tol^2 ||sampled block||_F^2; the build stops, rejecting
@@ -321,8 +321,10 @@ __device__ __noinline__ double2 oriented_entry(KernelParams K, bool own_is_test,
 // unit lower triangular in the eliminated columns, so X = U L^{-1} is solved in place in the
 // item's X slot. Status: [1, item, npivots, rank] singular cross matrix, [2, item, rows, limit]
 // more rows than the warp holds, [3, item, 0, 0] tree mimicry out of far points.
-// The CTA's warps take their items in rounds and run the pivot steps in lockstep (one CTA-wide
-// barrier per step), so that the warps of an SM execute the same part of the item loop at a time:
+// The CTA's warps take their items in rounds (one round per CTA as launched: CTAs retire as their
+// items end, so the kernels of other streams find room on the SMs between them) and run the pivot
+// steps in lockstep (one CTA-wide barrier per step), so that the warps of an SM execute the same
+// part of the item loop at a time:
 // instruction fetch bounded the free-running form (8 lockstep warps per CTA took 11 % less time
 // than 4 free-running ones; refilling a warp as soon as its item ends was slower still, as the
 // refill holds up the step barrier). Warps whose item is done, or that hold none, wait at the
@@ -341,11 +343,10 @@ __global__ void __launch_bounds__(kIacaWarps * 32) k_iaca(IacaArgs a) {
     int32_t *rp = ibase + mr;         // local pivot row of every accepted cross
     const MimicryArgs &F = a.mim;
     const bool items = F.item_node != nullptr;
-    for (;;) {
-        int idx = 0;
-        if (lane == 0) idx = atomicAdd(a.cursor, 1);
-        idx = __shfl_sync(kFull, idx, 0);
-        const bool valid = idx < a.nitems;
+    for (int64_t round = 0;; ++round) {
+        const int64_t at = (round * gridDim.x + blockIdx.x) * kIacaWarps + warp;
+        const int idx = int(at < a.nitems ? at : a.nitems);
+        const bool valid = at < a.nitems;
         if (__syncthreads_and(!valid)) break;  // every warp of the CTA is out of items
         const int item = valid ? a.items[idx] : 0;
         const int cl = items ? F.item_node[item] : item;
@@ -589,13 +590,8 @@ int iaca_max_rows() { return 256; }
 
 void launch_iaca(const IacaArgs &a, int mcap, cudaStream_t s) {
     if (a.nitems <= 0) return;
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const size_t sm = iaca_smem_bytes(a.maxrank);
-    const int need = (a.nitems + kIacaWarps - 1) / kIacaWarps;
-    const int cap = sms * 2;  // two resident CTAs per SM (about 128 registers a thread)
-    const int grid = need < cap ? need : cap;
+    const int grid = (a.nitems + kIacaWarps - 1) / kIacaWarps;  // one round of items per CTA
     auto go = [&](auto kern) {
         if (sm > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
         kern<<<grid, kIacaWarps * 32, sm, s>>>(a);

@@ -1,4 +1,5 @@
-// Randomised check of the banded nearest-direction search against the full search: the
+// Randomised check of the banded, four-wide nearest-direction search against the full
+// one-at-a-time search (and of the four-wide search over all candidates against it): the
 // candidate sets of candidate_directions for cluster diameters 0.01-3 and wavenumbers 1-120
 // (6 to ~680,000 spherical Fibonacci points), queried with Gaussian directions of magnitudes
 // 1e-30 to 1e30, many of them near the poles or on the equator. Both searches must return the
@@ -16,9 +17,11 @@ int main(int argc, char **argv) {
     std::uniform_real_distribution<double> ud(-30, 30);
     long bad = 0, total = 0;
     std::vector<double> dirs;
+    nca::Candidates cand;
     for (double diam = 0.01; diam < 3.0; diam *= 1.07) {
         for (double k : {1.0, 10.0, 50.0, 120.0}) {
             nca::candidate_directions(diam, k, 1.0, dirs);
+            cand.set(dirs);
             for (int t = 0; t < per_set; ++t) {
                 double v[3] = {nd(g), nd(g), nd(g)};
                 if (t % 5 == 0) {  // near the poles
@@ -29,7 +32,9 @@ int main(int argc, char **argv) {
                 const double scale = std::pow(10.0, ud(g));
                 for (double &x : v) x *= scale;
                 ++total;
-                if (nca::nearest_candidate(dirs, v) != nca::nearest_direction(dirs, v)) ++bad;
+                const int full = nca::nearest_direction(dirs, v);
+                if (nca::nearest_candidate(cand, v) != full) ++bad;
+                if (t % 3 == 0 && int(nca::argmax_dot(cand, 0, cand.n - 1, v)) != full) ++bad;
             }
         }
     }
