@@ -14,11 +14,13 @@
 #include <exception>
 #include <functional>
 #include <future>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
 #include <type_traits>
 #include <unordered_map>
+#include <unordered_set>
 #include <stdexcept>
 #include <string>
 #include <system_error>
@@ -51,18 +53,92 @@ void check(cudaError_t e, const char *what, int line) {
 }
 #define CK(call) check((call), #call, __LINE__)
 
+// Device blocks of the builds' large scratch (level buffers, transposed operators), kept for the
+// process and handed to later builds instead of freed: cudaFree of a multi-GB block waits for the
+// whole device and unmaps it (tens of ms at the end of every build, once 0.84 s). A request takes
+// the smallest kept block of at least its size and at most twice it; blocks beyond kKeep bytes
+// (NCA_SCRATCH_CACHE_GB, default 16) are freed when returned.
+class DeviceCache {
+  public:
+    static DeviceCache &get() {
+        static DeviceCache *cache = new DeviceCache;  // never destroyed: the driver frees at exit
+        return *cache;
+    }
+    // a block of at least `bytes` on the current device
+    void *acquire(size_t bytes) {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            std::multimap<size_t, void *> &fl = free_[dev];
+            auto it = fl.lower_bound(bytes);
+            if (it != fl.end() && it->first <= 2 * bytes) {
+                void *q = it->second;
+                kept_ -= it->first;
+                fl.erase(it);
+                return q;
+            }
+        }
+        void *q = nullptr;
+        CK(cudaMalloc(&q, bytes));
+        std::lock_guard<std::mutex> g(mu_);
+        block_[q] = Block{bytes, dev};
+        return q;
+    }
+    // takes back a block of this cache (false: not one of its blocks)
+    bool release(void *q) {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            auto it = block_.find(q);
+            if (it == block_.end()) return false;
+            const Block b = it->second;
+            if (kept_ + b.bytes <= keep_) {
+                free_[b.device].emplace(b.bytes, q);
+                kept_ += b.bytes;
+                return true;
+            }
+            block_.erase(it);
+        }
+        cudaFree(q);
+        return true;
+    }
+
+  private:
+    struct Block {
+        size_t bytes;
+        int device;
+    };
+    DeviceCache() {
+        const char *e = getenv("NCA_SCRATCH_CACHE_GB");
+        keep_ = size_t((e ? std::max(0.0, atof(e)) : 16.0) * double(size_t(1) << 30));
+    }
+    std::mutex mu_;
+    std::unordered_map<int, std::multimap<size_t, void *>> free_;  // kept blocks per device, by size
+    std::unordered_map<void *, Block> block_;                        // every block the cache made
+    size_t kept_ = 0, keep_ = 0;
+};
+
 template <typename T>
 struct DBuf {
     T *p = nullptr;
     size_t n = 0;
+    bool cached = false;  // from DeviceCache (alloc_scratch)
     DBuf() = default;
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
     ~DBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p && !(cached && DeviceCache::get().release(p))) cudaFree(p);
         p = nullptr;
         n = 0;
+        cached = false;
+    }
+    // build scratch: from the process's device cache, returned to it on release
+    void alloc_scratch(size_t count) {
+        release();
+        n = count;
+        p = static_cast<T *>(DeviceCache::get().acquire(sizeof(T) * std::max<size_t>(count, 1)));
+        cached = true;
     }
     void alloc(size_t count) {
         release();
@@ -75,6 +151,7 @@ struct DBuf {
         if (p) later.push_back(p);
         p = nullptr;
         n = 0;
+        cached = false;
     }
     void upload(const T *h, size_t count, cudaStream_t s) {
         alloc(count);
@@ -92,11 +169,11 @@ struct DBuf {
 
 // uploads v into the scratch buffer b, reallocating only when b is too small (the old array
 // goes to `later`)
-template <typename T>
-void upload_reuse(DBuf<T> &b, const std::vector<T> &v, cudaStream_t s, std::vector<void *> &later) {
+template <typename T, typename A>
+void upload_reuse(DBuf<T> &b, const std::vector<T, A> &v, cudaStream_t s, std::vector<void *> &later) {
     if (!b.p || v.size() > b.n) {
         b.defer(later);  // cudaFree here would wait for the work of every stream on the device
-        b.alloc(v.size());
+        b.alloc_scratch(v.size());
     }
     if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
 }
@@ -127,7 +204,6 @@ class PinnedPool {
     struct Block {
         unsigned char *p = nullptr;
         size_t n = 0;
-        bool fresh = false;  // allocated by this acquire (not taken from the pool)
     };
     static PinnedPool &get() {
         static PinnedPool pool;
@@ -148,7 +224,6 @@ class PinnedPool {
         }
         Block b;
         b.n = std::max<size_t>((n + (size_t(64) << 20) - 1) & ~((size_t(64) << 20) - 1), size_t(64) << 20);
-        b.fresh = true;
         if (cudaHostAlloc(reinterpret_cast<void **>(&b.p), b.n, cudaHostAllocDefault) != cudaSuccess) {
             cudaGetLastError();
             b.p = nullptr;
@@ -164,7 +239,6 @@ class PinnedPool {
             return;
         }
         kept_ += b.n;
-        b.fresh = false;
         free_.push_back(b);
     }
 
@@ -207,6 +281,14 @@ class HostPool {
         }
         void *p = mmap(nullptr, cap, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
         if (p == MAP_FAILED) throw std::bad_alloc();
+        // page-locked for the process (a block is registered once and reused), so uploads from it
+        // are DMA copies; a block that cannot be registered is used as it is
+        if (cudaHostRegister(p, cap, cudaHostRegisterPortable) == cudaSuccess) {
+            std::lock_guard<std::mutex> g(mu_);
+            registered_.insert(p);
+        } else {
+            cudaGetLastError();
+        }
         return p;
     }
     void release(void *p, size_t cap) {
@@ -217,14 +299,21 @@ class HostPool {
                 kept_ += cap;
                 return;
             }
+            if (registered_.erase(p)) cudaHostUnregister(p);
         }
         munmap(p, cap);
+    }
+    // whether p starts a block registered with the driver
+    bool registered(const void *p) {
+        std::lock_guard<std::mutex> g(mu_);
+        return registered_.count(const_cast<void *>(p)) != 0;
     }
 
   private:
     static constexpr size_t kHostKeep = size_t(4) << 30;
     std::mutex mu_;
     std::unordered_map<size_t, std::vector<void *>> free_;
+    std::unordered_set<void *> registered_;
     size_t kept_ = 0;
 };
 
@@ -264,18 +353,26 @@ using hvec = std::vector<T, PoolAlloc<T>>;
 // goes back to the pool once the stream has finished the copies.
 class StagedUploads {
   public:
-    StagedUploads(size_t bytes, cudaStream_t s) : s_(s), b_(PinnedPool::get().acquire(bytes + 256)) {}
+    // bytes: the most the staged arrays need; the block is taken at the first staged array
+    StagedUploads(size_t bytes, cudaStream_t s) : s_(s), want_(bytes + 256) {}
     ~StagedUploads() {
-        if (b_.p) {
-            cudaStreamSynchronize(s_);
-            PinnedPool::get().release(b_);
-        }
+        if (b_.p || direct_) cudaStreamSynchronize(s_);  // no source is reused before its copy
+        if (b_.p) PinnedPool::get().release(b_);
     }
     template <typename T, typename A>
     void up(DBuf<T> &d, const std::vector<T, A> &v) {
         d.alloc(v.size());
         if (v.empty()) return;
         const size_t bytes = sizeof(T) * v.size();
+        if (std::is_same<A, PoolAlloc<T>>::value && HostPool::get().registered(v.data())) {
+            CK(cudaMemcpyAsync(d.p, v.data(), bytes, cudaMemcpyHostToDevice, s_));  // page-locked already
+            direct_ = true;
+            return;
+        }
+        if (!b_.p && !tried_) {
+            b_ = PinnedPool::get().acquire(want_);
+            tried_ = true;
+        }
         used_ = (used_ + 15) & ~size_t(15);
         if (b_.p && used_ + bytes <= b_.n) {
             std::memcpy(b_.p + used_, v.data(), bytes);
@@ -287,11 +384,12 @@ class StagedUploads {
     }
     StagedUploads(const StagedUploads &) = delete;
     StagedUploads &operator=(const StagedUploads &) = delete;
-    bool fresh() const { return b_.fresh; }
 
   private:
     cudaStream_t s_;
+    size_t want_;
     PinnedPool::Block b_;
+    bool tried_ = false, direct_ = false;
     size_t used_ = 0;
 };
 
@@ -373,7 +471,8 @@ struct DirItems {
     // device and page-locked scratch of the build, freed once the build has synchronised
     std::vector<void *> later, later_host;
     void free_later() {
-        for (void *q : later) cudaFree(q);
+        for (void *q : later)
+            if (!DeviceCache::get().release(q)) cudaFree(q);
         for (void *q : later_host) cudaFreeHost(q);
         later.clear();
         later_host.clear();
@@ -563,11 +662,12 @@ void upload_tree(DevSide &d, const nca::Tree &T, const double *pts, cudaStream_t
 
 // CSR of n lists filled by fill(i, list) on the host's worker threads (contiguous item ranges
 // per thread, concatenated in item order).
-template <typename F>
-void parallel_csr(int n, F fill, std::vector<int64_t> &ptr, std::vector<int32_t> &idx) {
-    const int nth = std::max(1, std::min(nca::host_threads(), std::max(n, 1)));
-    std::vector<std::vector<int64_t>> lptr(nth);
-    std::vector<std::vector<int32_t>> lidx(nth);
+template <typename F, typename PV, typename IV>
+void parallel_csr(int n, F fill, PV &ptr, IV &idx) {
+    // a thread per 2,048 lists at least: short lists (the deepest levels) are not worth a pool
+    const int nth = std::max(1, std::min(nca::host_threads(), (n + 2047) / 2048));
+    std::vector<hvec<int64_t>> lptr(nth);  // pooled: the lists are rebuilt level by level
+    std::vector<hvec<int32_t>> lidx(nth);
     auto work = [&](int w) {
         const int i0 = int(int64_t(n) * w / nth), i1 = int(int64_t(n) * (w + 1) / nth);
         std::vector<int32_t> one;
@@ -591,7 +691,7 @@ void parallel_csr(int n, F fill, std::vector<int64_t> &ptr, std::vector<int32_t>
         const int i0 = int(int64_t(n) * w / nth);
         for (size_t k = 1; k < lptr[w].size(); ++k) ptr[size_t(i0) + k] = lptr[w][k] + off[w];
         std::copy(lidx[w].begin(), lidx[w].end(), idx.begin() + off[w]);
-        std::vector<int32_t>().swap(lidx[w]);
+        hvec<int32_t>().swap(lidx[w]);
     };
     pool.clear();
     for (int w = 1; w < nth; ++w) pool.emplace_back(place, w);
@@ -1448,6 +1548,14 @@ struct StageBuilder {
         // Records of the all-column FP32 kernel (groups of small outputs): inside a group the
         // records of one row class (the kernel's register tile) are contiguous, largest work
         // first inside a class: one launch per class
+        // the vector rows an output reads: its work over its rows (work = rows x widths, summed
+        // while listing), so the segments need not be visited again
+        auto width = [&](int32_t o) -> int32_t {
+            if (rows[o] > 0) return int32_t(work[o] / rows[o]);
+            int32_t W = 0;
+            for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
+            return W;
+        };
         G.wide_gptr.assign(1, 0);
         G.wide_begin.clear();
         G.wide_count.clear();
@@ -1472,8 +1580,7 @@ struct StageBuilder {
                 rec.resize(size_t(at));
                 for (int32_t i = b; i < e; ++i) {
                     const int32_t o = order[i];
-                    int32_t W = 0;
-                    for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
+                    const int32_t W = width(o);
                     rec[size_t(start[wide_rows_class(rows[o])]++)] =
                         WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], rows[o], 0};
                 }
@@ -1490,8 +1597,7 @@ struct StageBuilder {
             if (wide_group(group_maxrows[g], group_work[g])) continue;
             for (int32_t i = group_ptr[g]; i < group_ptr[g + 1]; ++i) {
                 const int32_t o = order[i];
-                int32_t W = 0;
-                for (int32_t k = segptr[o]; k < segptr[o + 1]; ++k) W += w[k];
+                const int32_t W = width(o);
                 trec[i] = WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], rows[o], 0};
             }
         }
@@ -1508,7 +1614,6 @@ struct StageBuilder {
                              sizeof(int64_t) * (out.size() + moff.size() + voff.size() + soff.size() + doff.size()) +
                              16 * 16;
         StagedUploads up(bytes, s);
-        if (mark) mark(up.fresh() ? "staging block allocated" : "staging block reused");
         up.up(G.outputs, order);
         up.up(G.wout, rec);
         up.up(G.tout, trec);
@@ -1612,13 +1717,13 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     // is not compressed; its empty range leaves the level's CSR over the remaining items intact.
     struct LevelFar {
         std::vector<int32_t> items, farpts;  // the level's items with far points, and their counts
-        std::vector<int64_t> ptr;             // CSR over those items (positional)
-        std::vector<int32_t> nodes;
+        hvec<int64_t> ptr;                    // CSR over those items (positional)
+        hvec<int32_t> nodes;
     };
     auto list_level = [&, maxrank](int lev) {
         LevelFar L;
         const std::vector<int32_t> &cand = bylevel[lev];
-        std::vector<int64_t> ptr;
+        hvec<int64_t> ptr;
         parallel_csr(
             int(cand.size()), [&](int i, std::vector<int32_t> &ff) { nca::item_farfield(T, pl, cand[i], ff); }, ptr,
             L.nodes);
@@ -1633,22 +1738,33 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
         }
         return L;
     };
-    std::future<LevelFar> next_far;
-    if (T.nlevels > 0) next_far = std::async(std::launch::async, list_level, T.nlevels - 1);
+    // two levels listed ahead: the deepest level is small, and the next one's list would
+    // otherwise hold up its launch
+    std::vector<std::future<LevelFar>> far_of(size_t(std::max(T.nlevels, 0)));
+    for (int lev = T.nlevels - 1; lev >= 0 && lev >= T.nlevels - 2; --lev)
+        far_of[size_t(lev)] = std::async(std::launch::async, list_level, lev);
     const std::vector<double> centroid = cluster_centroids(T, ownpts);
     DBuf<int64_t> dffptr;
     DBuf<int32_t> dffnodes;
     DBuf<double> dcent, dcenter;
-    dcent.upload(centroid, s);
-    dcenter.upload(Ft.center, s);
-    timer.mark(side + "centroids uploaded");
+    {
+        // through one page-locked block (pageable copies are staged by the driver, a few GB/s)
+        const size_t bytes = sizeof(double) * (centroid.size() + Ft.center.size()) +
+                             sizeof(int32_t) * (pl.item_node.size() + pl.item_basis.size() + pl.item_chptr.size() +
+                                                pl.item_chidx.size()) +
+                             6 * 16;
+        StagedUploads up(bytes, s);
+        up.up(dcent, centroid);
+        up.up(dcenter, Ft.center);
+        up.up(d.item_node, pl.item_node);
+        up.up(d.item_basis, pl.item_basis);
+        up.up(d.item_chptr, pl.item_chptr);
+        up.up(d.item_chidx, pl.item_chidx);
+    }
+    timer.mark(side + "centroids and items uploaded");
     // the side's items, level by level
     DBuf<int32_t> status;
     status.alloc(4);  // [flag, item, a, b]
-    d.item_node.upload(pl.item_node, s);
-    d.item_basis.upload(pl.item_basis, s);
-    d.item_chptr.upload(pl.item_chptr, s);
-    d.item_chidx.upload(pl.item_chidx, s);
     d.rank.alloc(std::max(ni, 1));
     d.rank.zero(s);
     d.nrows.alloc(std::max(ni, 1));
@@ -1684,6 +1800,7 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     a.piv = d.piv.p;
     d.cpiv.alloc(size_t(std::max(ni, 1)) * maxrank);
     a.cpiv = d.cpiv.p;
+    timer.mark(side + "item arrays allocated");
     a.maxrank = maxrank;
     a.tol = sd == 0 ? o->tol_test : o->tol_trial;
     a.status = status.p;
@@ -1700,13 +1817,26 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     DBuf<int64_t> dlvoff, ddo;
     DBuf<int32_t> nodes, drk;
     DBuf<double2> chunk;
-    PinnedBuf<int32_t> hrank(2 * size_t(std::max(ni, 1)));
+    // ranks and rows read back per level, through a block of the page-locked pool (returned
+    // below, once the side's stream has synchronised)
+    PinnedPool::Block hrank_block = PinnedPool::get().acquire(sizeof(int32_t) * 2 * size_t(std::max(ni, 1)));
+    if (!hrank_block.p) throw Failure(NCA_ERR_CUDA, "no page-locked host memory for the rank read-back");
+    struct BlockGuard {
+        PinnedPool::Block b;
+        cudaStream_t s;
+        ~BlockGuard() {
+            cudaStreamSynchronize(s);  // no read-back still lands in the block
+            PinnedPool::get().release(b);
+        }
+    } hrank_guard{hrank_block, s};
+    int32_t *const hrank = reinterpret_cast<int32_t *>(hrank_block.p);
     a.xoff_by_position = 1;
     int64_t total = 0;
     a.mim.ff_by_position = 1;
     for (int lev = T.nlevels - 1; lev >= 0; --lev) {
-        const LevelFar far = next_far.get();
-        if (lev > 0) next_far = std::async(std::launch::async, list_level, lev - 1);
+        const LevelFar far = far_of[size_t(lev)].get();
+        timer.mark(side + "level " + std::to_string(lev) + " far field listed");
+        if (lev >= 2) far_of[size_t(lev) - 2] = std::async(std::launch::async, list_level, lev - 2);
         const std::vector<int32_t> &items = far.items;
         std::vector<int64_t> lvoff;
         int mc = 0;
@@ -1735,7 +1865,7 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
                                            std::to_string(nca::iaca_max_rows()) + " (reduce the leaf size)");
         if (!chunk.p || size_t(bound) > chunk.n) {
             chunk.defer(d.later);
-            chunk.alloc(size_t(std::max<int64_t>(bound, 1)));
+            chunk.alloc_scratch(size_t(std::max<int64_t>(bound, 1)));
             timer.mark(side + "level " + std::to_string(lev) + " scratch of " + std::to_string(bound >> 16) +
                        " x 1 MiB allocated");
         }
@@ -1744,7 +1874,7 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
         const int nl = int(items.size());
         if (drk.n < 2 * size_t(nl)) {
             drk.defer(d.later);
-            drk.alloc(2 * size_t(nl));
+            drk.alloc_scratch(2 * size_t(nl));
         }
         status.zero(s);
         a.X = chunk.p;
@@ -1765,10 +1895,10 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
         }
         if (st[0] == 2) throw Failure(NCA_ERR_ARG, "internal: an item exceeds the IACA kernel's row capacity");
         if (st[0] == 3) throw Failure(NCA_ERR_CUDA, "internal: tree mimicry ran out of far points");
-        CK(cudaMemcpyAsync(hrank.p, drk.p, sizeof(int32_t) * 2 * nl, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hrank, drk.p, sizeof(int32_t) * 2 * nl, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         timer.mark(side + "level " + std::to_string(lev) + " IACA done");
-        const int32_t *rk = hrank.p, *nr = hrank.p + nl;
+        const int32_t *rk = hrank, *nr = hrank + nl;
         // compact this level: exact m x r blocks, back to back (one copy per item, rank-0 items
         // copy nothing; sources, rows and columns straight from the positional arrays)
         std::vector<int64_t> doff(nl);
@@ -1782,7 +1912,7 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
             lt += pad2(int64_t(nr[i]) * rk[i]);
         }
         levelX.emplace_back(new DBuf<double2>());
-        levelX.back()->alloc(size_t(std::max<int64_t>(lt, 1)));
+        levelX.back()->alloc_scratch(size_t(std::max<int64_t>(lt, 1)));
         if (lt > 0) {
             // on the high-priority stream: its blocks start ahead of the other side's IACA blocks
             upload_reuse(ddo, doff, hs, d.later);
@@ -1821,7 +1951,6 @@ void compress_dir_side(nca_core *c, DirItems &d, int sd, const double *ownpts,
     for (auto *b : {&dffnodes, &status, &nodes, &drk}) b->defer(d.later);
     for (auto *b : {&dcent, &dcenter}) b->defer(d.later);
     chunk.defer(d.later);
-    hrank.defer(d.later_host);
 }
 
 void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_build_opts *o, const nca::Wideband &wb,
@@ -1876,9 +2005,19 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     StreamGuard sg2{s2};
     std::vector<int64_t> h_ntoff;
     int64_t near_entries = 0;
+    // complex-FP32 copy of a store, made on the stream that filled it (by the thread that did), so
+    // that the copies overlap the rest of the build instead of following it
+    auto to_f32 = [&](DBuf<double2> &src, DBuf<float2> &dst, cudaStream_t st) {
+        if (!c->f32) return;
+        dst.alloc(src.n);
+        if (src.n) k_to_f32<<<launch_grid(int64_t(src.n) / 256 + 1, 8), 256, 0, st>>>(src.p, dst.p, int64_t(src.n));
+        CK(cudaGetLastError());
+    };
     std::shared_future<void> near_f = std::async(std::launch::async, [&]() {
         CK(cudaSetDevice(c->device));
         near_entries = build_near(c, s2, &h_ntoff);
+        to_f32(c->N, c->N32, s2);
+        to_f32(c->NT, c->NT32, s2);
         CK(cudaStreamSynchronize(s2));
         timer.mark("near field built");
     }).share();
@@ -1988,7 +2127,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             compress_dir_side(c, d, sd, pts[sd], bylevel[sd], s, o, timer, side, known, hs[sd]);
         }
         d.xoff.upload(d.h_xoff, s);
-        d.XT.alloc(d.X.n);
+        d.XT.alloc_scratch(d.X.n);
         launch_transpose_blocks<double2>(d.X.p, d.xoff.p, d.nrows.p, d.rank.p, d.xoff.p, ni, d.XT.p, s);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s));
@@ -2057,6 +2196,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             launch_transpose_blocks<double2>(CN.M.p, D->ctr_in.p, D->ctr_rows.p, D->ctr_cols.p, D->ctr_off.p, D->ntr,
                                              CTs.M.p, s);
             CK(cudaGetLastError());
+            to_f32(CN.M, CN.M32, s);
+            to_f32(CTs.M, CTs.M32, s);
         }
     };
     std::promise<void> coupled;
@@ -2120,6 +2261,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             timer.mark("gather plan " + std::to_string(task) + ": up listed");
             side_done[I].get();
             B.finish(pr.up, di.XT.p, s, m ? "T up" : "N up", plan_mark("up"));
+            to_f32(pr.up.M, pr.up.M32, s);
             timer.mark("gather plan " + std::to_string(task) + ": up");
         }
         // coupling: output-side items with a rank and their far pairs' blocks (store built above)
@@ -2212,6 +2354,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             B.shift(yo, true);
             side_done[O].get();
             B.finish(pr.down, dout.X.p, s, m ? "T down" : "N down", plan_mark("down"));
+            to_f32(pr.down.M, pr.down.M32, s);
             timer.mark("gather plan " + std::to_string(task) + ": down");
         }
         // leaves: every basis item whose cluster contains the leaf, then the near blocks
@@ -2246,6 +2389,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             B.shift(yo, false);
             side_done[O].get();
             B.finish(pr.leaves, dout.X.p, s, m ? "T leaves" : "N leaves", plan_mark("leaves"));
+            to_f32(pr.leaves.M, pr.leaves.M32, s);
             timer.mark("gather plan " + std::to_string(task) + ": leaves");
         }
         CK(cudaStreamSynchronize(s));
@@ -2282,21 +2426,11 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     // the stage stores hold the products' copies of the operators; X stays for nca_core_save
     for (DirItems &d : D->side) d.XT.release();
     timer.mark("transposed bases released");
-    if (c->f32) {
-        auto down = [&](DBuf<double2> &src, DBuf<float2> &dst) {
-            dst.alloc(src.n);
-            if (src.n) k_to_f32<<<launch_grid(int64_t(src.n) / 256 + 1, 8), 256, 0, s>>>(src.p, dst.p, int64_t(src.n));
-            CK(cudaGetLastError());
-        };
-        for (DirProduct &pr : D->prod)
-            for (GatherStage *G : {&pr.up, &pr.couple, &pr.down, &pr.leaves}) down(G->M, G->M32);
-        down(c->N, c->N32);
-        down(c->NT, c->NT32);
-    }
     CK(cudaEventRecord(ev1, s));
     CK(cudaStreamSynchronize(s));
-    timer.mark("complex-FP32 copies done, build complete");
+    timer.mark("build complete");
     for (DirItems &d : D->side) d.free_later();
+    timer.mark("scratch freed");
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
     auto h2 = std::chrono::steady_clock::now();

@@ -215,14 +215,70 @@ int nearest_candidate(const Candidates &c, const double *v) {
 
 }  // namespace
 
+// The lists of a node come out of csr sorted, so the pairs may be found in any order: the top of
+// the traversal is expanded breadth first (near leaf pairs and far pairs found there kept) until
+// it offers enough independent (test, trial) subtrees, which the host threads then traverse into
+// their own lists; the four CSR lists are made side by side.
 Partition build_partition_wideband(const Tree &test, const Tree &trial, const Wideband &w) {
     Pairs sink;
-    if (test.nnodes > 0 && trial.nnodes > 0) traverse_wideband(test, trial, 0, 0, w, sink);
+    std::vector<std::pair<int, int>> frontier, next;
+    if (test.nnodes > 0 && trial.nnodes > 0) frontier.emplace_back(0, 0);
+    const int nth = host_threads();
+    while (!frontier.empty() && frontier.size() < size_t(16) * nth) {
+        next.clear();
+        for (const auto &ts : frontier) {
+            const int t = ts.first, s = ts.second;
+            if (!isnear_wideband(test, trial, t, s, w)) {
+                sink.ft.push_back(t);
+                sink.fs.push_back(s);
+                continue;
+            }
+            const bool lt = test.isleaf(t), ls = trial.isleaf(s);
+            if (lt && ls) {
+                sink.nt.push_back(t);
+                sink.ns.push_back(s);
+            } else if (lt) {
+                for (int c = 0; c < trial.nchildren[s]; ++c) next.emplace_back(t, trial.firstchild[s] + c);
+            } else if (ls) {
+                for (int c = 0; c < test.nchildren[t]; ++c) next.emplace_back(test.firstchild[t] + c, s);
+            } else {
+                for (int c = 0; c < test.nchildren[t]; ++c)
+                    for (int d = 0; d < trial.nchildren[s]; ++d)
+                        next.emplace_back(test.firstchild[t] + c, trial.firstchild[s] + d);
+            }
+        }
+        frontier.swap(next);
+    }
+    const int use = std::max(1, std::min(nth, int(frontier.size())));
+    std::vector<Pairs> part(use);
+    std::atomic<size_t> cursor{0};
+    auto work = [&](int i) {
+        for (;;) {
+            const size_t f = cursor.fetch_add(1);
+            if (f >= frontier.size()) break;
+            traverse_wideband(test, trial, frontier[f].first, frontier[f].second, w, part[i]);
+        }
+    };
+    {
+        std::vector<std::thread> pool;
+        for (int i = 1; i < use; ++i) pool.emplace_back(work, i);
+        work(0);
+        for (auto &th : pool) th.join();
+    }
+    for (const Pairs &q : part) {
+        sink.nt.insert(sink.nt.end(), q.nt.begin(), q.nt.end());
+        sink.ns.insert(sink.ns.end(), q.ns.begin(), q.ns.end());
+        sink.ft.insert(sink.ft.end(), q.ft.begin(), q.ft.end());
+        sink.fs.insert(sink.fs.end(), q.fs.begin(), q.fs.end());
+    }
     Partition P;
-    csr(sink.nt, sink.ns, test.nnodes, P.nearptr, P.nearnodes);
-    csr(sink.ft, sink.fs, test.nnodes, P.farptr, P.farnodes);
-    csr(sink.ns, sink.nt, trial.nnodes, P.tnearptr, P.tnearnodes);
+    std::thread a([&] { csr(sink.nt, sink.ns, test.nnodes, P.nearptr, P.nearnodes); });
+    std::thread b([&] { csr(sink.ft, sink.fs, test.nnodes, P.farptr, P.farnodes); });
+    std::thread c([&] { csr(sink.ns, sink.nt, trial.nnodes, P.tnearptr, P.tnearnodes); });
     csr(sink.fs, sink.ft, trial.nnodes, P.tfarptr, P.tfarnodes);
+    a.join();
+    b.join();
+    c.join();
     return P;
 }
 
