@@ -281,14 +281,6 @@ class HostPool {
         }
         void *p = mmap(nullptr, cap, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
         if (p == MAP_FAILED) throw std::bad_alloc();
-        // page-locked for the process (a block is registered once and reused), so uploads from it
-        // are DMA copies; a block that cannot be registered is used as it is
-        if (cudaHostRegister(p, cap, cudaHostRegisterPortable) == cudaSuccess) {
-            std::lock_guard<std::mutex> g(mu_);
-            registered_.insert(p);
-        } else {
-            cudaGetLastError();
-        }
         return p;
     }
     void release(void *p, size_t cap) {
@@ -299,21 +291,14 @@ class HostPool {
                 kept_ += cap;
                 return;
             }
-            if (registered_.erase(p)) cudaHostUnregister(p);
         }
         munmap(p, cap);
-    }
-    // whether p starts a block registered with the driver
-    bool registered(const void *p) {
-        std::lock_guard<std::mutex> g(mu_);
-        return registered_.count(const_cast<void *>(p)) != 0;
     }
 
   private:
     static constexpr size_t kHostKeep = size_t(4) << 30;
     std::mutex mu_;
     std::unordered_map<size_t, std::vector<void *>> free_;
-    std::unordered_set<void *> registered_;
     size_t kept_ = 0;
 };
 
@@ -356,19 +341,16 @@ class StagedUploads {
     // bytes: the most the staged arrays need; the block is taken at the first staged array
     StagedUploads(size_t bytes, cudaStream_t s) : s_(s), want_(bytes + 256) {}
     ~StagedUploads() {
-        if (b_.p || direct_) cudaStreamSynchronize(s_);  // no source is reused before its copy
-        if (b_.p) PinnedPool::get().release(b_);
+        if (b_.p) {
+            cudaStreamSynchronize(s_);  // the block is not reused before its copies
+            PinnedPool::get().release(b_);
+        }
     }
     template <typename T, typename A>
     void up(DBuf<T> &d, const std::vector<T, A> &v) {
         d.alloc(v.size());
         if (v.empty()) return;
         const size_t bytes = sizeof(T) * v.size();
-        if (std::is_same<A, PoolAlloc<T>>::value && HostPool::get().registered(v.data())) {
-            CK(cudaMemcpyAsync(d.p, v.data(), bytes, cudaMemcpyHostToDevice, s_));  // page-locked already
-            direct_ = true;
-            return;
-        }
         if (!b_.p && !tried_) {
             b_ = PinnedPool::get().acquire(want_);
             tried_ = true;
@@ -389,7 +371,7 @@ class StagedUploads {
     cudaStream_t s_;
     size_t want_;
     PinnedPool::Block b_;
-    bool tried_ = false, direct_ = false;
+    bool tried_ = false;
     size_t used_ = 0;
 };
 
@@ -2074,16 +2056,64 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     std::shared_future<void> side_done[2] = {sided[0].get_future().share(), sided[1].get_future().share()};
     std::shared_future<void> side_ranked[2] = {ranked[0].get_future().share(), ranked[1].get_future().share()};
     std::atomic<bool> ranked_set[2] = {false, false};
+    // Galerkin inputs (one tree on both sides, a symmetric partition) give the trial side the test
+    // side's directional plan: it is made once and copied, instead of twice at once on the same
+    // host cores
+    const nca::Tree &T0 = c->tree[0], &T1 = c->tree[1];
+    const bool symmetric = !sv && T0.nnodes == T1.nnodes && T0.perm == T1.perm && T0.begin == T1.begin &&
+                           T0.end == T1.end && T0.parent == T1.parent && T0.firstchild == T1.firstchild &&
+                           T0.nchildren == T1.nchildren && T0.level == T1.level && T0.center == T1.center &&
+                           T0.radius == T1.radius && P.farptr == P.tfarptr && P.farnodes == P.tfarnodes;
+    // ... and, when moreover both sides hold the same points, the kernel depends on |x - y| only
+    // (Helmholtz, Laplace: K(x, y) and K(y, x) are formed from the same squared differences, bit for
+    // bit) and the tolerances agree, the trial side's IACA would repeat the test side's bit for bit
+    // (every entry, sum and pivot decision is the same): the trial side takes the test side's
+    // ranks, pivots and operators (device copies) instead of a second compression.
+    // NCA_MIRROR_TRIAL=0 compresses both sides.
+    const bool mirror = [&] {
+        const char *e = getenv("NCA_MIRROR_TRIAL");
+        if (e && e[0] == '0') return false;
+        return symmetric && (c->K.kind == 0 || c->K.kind == 1) && c->K.deriv == 0 && o->tol_test == o->tol_trial &&
+               T0.npoints == T1.npoints &&
+               std::memcmp(tp, sp, sizeof(double) * 3 * size_t(T0.npoints)) == 0;
+    }();
     auto side_task = [&](int sd) {
         const cudaStream_t s = ss[sd];
         DirItems &d = D->side[sd];
         const std::string side = sd == 0 ? "test: " : "trial: ";
         try {
-            if (sv)
+            if (sv) {
                 d.plan = sv->side[sd].plan;
-            else
+            } else if (symmetric && sd == 1) {
+                planned_f[0].get();
+                // member by member on threads of their own: the copy writes ~50 MB of fresh pages
+                const nca::DirSide &src = D->side[0].plan;
+                nca::DirSide &dst = d.plan;
+                std::vector<std::future<void>> parts;
+                auto copy = [&parts](auto &to, const auto &from) {
+                    parts.push_back(std::async(std::launch::async, [&to, &from] { to = from; }));
+                };
+                copy(dst.farptr, src.farptr);
+                copy(dst.farnodes, src.farnodes);
+                copy(dst.dirptr, src.dirptr);
+                copy(dst.dirs, src.dirs);
+                copy(dst.dirvec, src.dirvec);
+                copy(dst.dirfarptr, src.dirfarptr);
+                copy(dst.chdirptr, src.chdirptr);
+                copy(dst.chdirmap, src.chdirmap);
+                copy(dst.invptr, src.invptr);
+                copy(dst.invidx, src.invidx);
+                copy(dst.item_node, src.item_node);
+                copy(dst.item_basis, src.item_basis);
+                copy(dst.item_chptr, src.item_chptr);
+                copy(dst.item_chidx, src.item_chidx);
+                for (auto &f : parts) f.get();
+                static_assert(sizeof(nca::DirSide) == 14 * sizeof(std::vector<int32_t>),
+                              "every member of DirSide is copied above");
+            } else {
                 d.plan = directional_plan(c->tree[sd], c->tree[1 - sd], sd == 0 ? P.farptr : P.tfarptr,
                                           sd == 0 ? P.farnodes : P.tfarnodes, wb);
+            }
         } catch (...) {
             planned[sd].set_exception(std::current_exception());
             throw;
@@ -2123,6 +2153,37 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             d.h_xoff = v.xoff;
             known();
             d.X.upload(v.X, s);
+        } else if (mirror && sd == 1) {
+            // the test side's ranks and pivots are final once its ranks are known: copied before
+            // this side's ranks are announced (the couplings read them on the device)
+            side_ranked[0].get();
+            const DirItems &d0 = D->side[0];
+            auto dup = [&](auto &to, const auto &from) {
+                to.alloc(from.n);
+                if (from.n) CK(cudaMemcpyAsync(to.p, from.p, sizeof(*from.p) * from.n, cudaMemcpyDeviceToDevice, s));
+            };
+            dup(d.item_node, d0.item_node);
+            dup(d.item_basis, d0.item_basis);
+            dup(d.item_chptr, d0.item_chptr);
+            dup(d.item_chidx, d0.item_chidx);
+            dup(d.rank, d0.rank);
+            dup(d.nrows, d0.nrows);
+            dup(d.piv, d0.piv);
+            dup(d.cpiv, d0.cpiv);
+            CK(cudaStreamSynchronize(s));
+            d.h_rank = d0.h_rank;
+            d.h_nrows = d0.h_nrows;
+            d.h_xoff = d0.h_xoff;
+            known();
+            side_done[0].get();  // the test side's operators are joined and transposed
+            dup(d.xoff, d0.xoff);
+            dup(d.X, d0.X);
+            d.XT.alloc_scratch(d0.XT.n);
+            if (d0.XT.n)
+                CK(cudaMemcpyAsync(d.XT.p, d0.XT.p, sizeof(double2) * d0.XT.n, cudaMemcpyDeviceToDevice, s));
+            CK(cudaStreamSynchronize(s));
+            timer.mark(side + "operators taken from the test side");
+            return;
         } else {
             compress_dir_side(c, d, sd, pts[sd], bylevel[sd], s, o, timer, side, known, hs[sd]);
         }
@@ -2184,6 +2245,8 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             a.npairs = npairs;
             a.C = CN.M.p;
             a.C32 = nullptr;
+            if (npairs > 0 && !(a.rank_t && a.rank_s && a.piv_t && a.piv_s && a.C))
+                throw Failure(NCA_ERR_CUDA, "internal: the couplings were reached before both sides' pivots");
             if (npairs > 0) {
                 k_couplings<<<launch_grid(npairs, 16), 256, 0, s>>>(a);
                 CK(cudaGetLastError());
