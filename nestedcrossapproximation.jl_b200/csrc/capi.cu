@@ -491,6 +491,18 @@ struct GatherStage {
 struct DirProduct {
     int64_t nin = 0, nout = 0, cin = 0, cout = 0;
     GatherStage up, couple, down, leaves;
+    // a mirrored Galerkin core (both sides one skeleton): the transposed product's up, down and
+    // leaf stages are the forward product's (the same plans over the same stores); `same` points
+    // at that product and this product's own three stay empty
+    DirProduct *same = nullptr;
+    GatherStage &up_stage() { return same ? same->up : up; }
+    GatherStage &down_stage() { return same ? same->down : down; }
+    GatherStage &leaf_stage() { return same ? same->leaves : leaves; }
+    // the stages this product owns (the shared ones belong to `same`)
+    std::vector<GatherStage *> own_stages() {
+        if (same) return {&couple};
+        return {&up, &couple, &down, &leaves};
+    }
 };
 
 struct DirCore {
@@ -2201,7 +2213,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     int64_t npairs = 0;
     std::vector<int64_t> cfoff, ctoff;
     int64_t coupling_entries = 0;
-    auto couplings = [&]() {
+    auto couplings = [&](cudaStream_t st) {
         npairs = int64_t(pt.farnodes.size());
         const std::vector<int32_t> &rt = D->side[0].h_rank, &rs = D->side[1].h_rank;
         // coupling blocks S_e = K[tau_(t, dt), tau_(s, ds)] in test pair order, transposes in trial order
@@ -2226,9 +2238,20 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         CTs.M.alloc(size_t(ctoff.back()));
         CN.entries = CTs.entries = coupling_entries;
         {
-            D->cpair_it.upload(pair_it, s);
-            D->cpair_is.upload(pair_is, s);
-            D->ccoff.upload(cfoff, s);
+            // staged through page-locked memory on the coupling plan's stream (not behind the test
+            // side's work on the build stream)
+            {
+                StagedUploads up(sizeof(int32_t) * (pair_it.size() + pair_is.size() + tr_rows.size() + tr_cols.size()) +
+                                     sizeof(int64_t) * (cfoff.size() + tr_in.size() + ctoff.size()) + 8 * 16,
+                                 st);
+                up.up(D->cpair_it, pair_it);
+                up.up(D->cpair_is, pair_is);
+                up.up(D->ccoff, cfoff);
+                up.up(D->ctr_in, tr_in);
+                up.up(D->ctr_rows, tr_rows);
+                up.up(D->ctr_cols, tr_cols);
+                up.up(D->ctr_off, ctoff);
+            }  // the copies have landed (the staging block goes back to the pool)
             D->npairs = npairs;
             CouplingArgs a;
             a.K = c->K;
@@ -2248,19 +2271,15 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             if (npairs > 0 && !(a.rank_t && a.rank_s && a.piv_t && a.piv_s && a.C))
                 throw Failure(NCA_ERR_CUDA, "internal: the couplings were reached before both sides' pivots");
             if (npairs > 0) {
-                k_couplings<<<launch_grid(npairs, 16), 256, 0, s>>>(a);
+                k_couplings<<<launch_grid(npairs, 16), 256, 0, st>>>(a);
                 CK(cudaGetLastError());
             }
-            D->ctr_in.upload(tr_in, s);
-            D->ctr_rows.upload(tr_rows, s);
-            D->ctr_cols.upload(tr_cols, s);
-            D->ctr_off.upload(ctoff, s);
             D->ntr = int64_t(ps.farnodes.size());
             launch_transpose_blocks<double2>(CN.M.p, D->ctr_in.p, D->ctr_rows.p, D->ctr_cols.p, D->ctr_off.p, D->ntr,
-                                             CTs.M.p, s);
+                                             CTs.M.p, st);
             CK(cudaGetLastError());
-            to_f32(CN.M, CN.M32, s);
-            to_f32(CTs.M, CTs.M32, s);
+            to_f32(CN.M, CN.M32, st);
+            to_f32(CTs.M, CTs.M32, st);
         }
     };
     std::promise<void> coupled;
@@ -2285,6 +2304,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         const DirItems &di = D->side[I], &dout = D->side[O];
         const nca::Tree &TI = c->tree[I], &TO = c->tree[O];
         DirProduct &pr = D->prod[m];
+        if (pr.same && stage != 1) return;  // the forward product's stage serves this one
         // arena rows: [x of the input side; its coefficients; the output side's coefficients]: the
         // output rows start after the input side's coefficients, known once that side is built
         const int64_t xin = TI.npoints;
@@ -2335,7 +2355,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                     side_ranked[O].get();
                     input_side_built();
                     pairs_f.get();
-                    couplings();
+                    couplings(s);
                     coupled.set_value();
                 } catch (...) {
                     coupled.set_exception(std::current_exception());
@@ -2461,6 +2481,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     // stages x two orientations) on ten host threads and streams: a plan starts as soon as the
     // sides it reads are built (up: the input side; down, leaves: the output side, then the input
     // side's coefficient count; coupling: both sides and the couplings).
+    if (mirror) D->prod[1].same = &D->prod[0];
     on_threads(c->device, 10, [&](int task) {
         if (task < 2) {
             try {
@@ -2942,7 +2963,7 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
     const int I = mode == 0 ? 1 : 0, O = 1 - I;
     const int vs = vector_stride(b);
     const int cap = rows_capacity(std::min(b, 16));
-    for (const GatherStage *G : {&pr.up, &pr.couple, &pr.down, &pr.leaves})
+    for (const GatherStage *G : {&pr.up_stage(), &pr.couple, &pr.down_stage(), &pr.leaf_stage()})
         for (int r : G->group_maxrows)
             if (r > cap) return fail(NCA_ERR_ARG, "a leaf or basis block has more rows than one product CTA holds");
     // Complex-FP32 products keep the arena [x; coefficients] in complex FP32 too: the stages
@@ -2967,7 +2988,10 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
         using S = decltype(tag);
         constexpr bool f64 = std::is_same<S, double2>::value;
         using VT = S;  // FP64 stores with FP64 vectors, FP32 stores with FP32 vectors
-        const S *nearM = f64 ? (const S *)(mode == 0 ? c->N.p : c->NT.p) : (const S *)(mode == 0 ? c->N32.p : c->NT32.p);
+        // a shared leaf stage lists the forward near blocks (the mirrored core's transpose is the
+        // matrix itself)
+        const bool fwd = mode == 0 || pr.same;
+        const S *nearM = f64 ? (const S *)(fwd ? c->N.p : c->NT.p) : (const S *)(fwd ? c->N32.p : c->NT32.p);
         auto stage = [&](const GatherStage &G, bool accumulate, bool scatter, int sk) {
             const S *M = f64 ? (const S *)G.M.p : (const S *)G.M32.p;
             if (timer) timer->mark(sk, false, s);
@@ -3042,10 +3066,10 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
             }
             if (timer) timer->mark(sk, true, s);
         };
-        stage(pr.up, false, false, 1);
+        stage(pr.up_stage(), false, false, 1);
         stage(pr.couple, false, false, 2);
-        stage(pr.down, true, false, 3);
-        stage(pr.leaves, false, true, 5);
+        stage(pr.down_stage(), true, false, 3);
+        stage(pr.leaf_stage(), false, true, 5);
     };
     if (precision == NCA_PREC_F64)
         run(double2{});
@@ -3854,6 +3878,7 @@ void fill_dir_stores(nca_core *c, const KernelParams &K, double2 *const X[2], do
                                             dst.p, s);
             CK(cudaGetLastError());
         };
+        if (pr.same) continue;  // its stages are the forward product's, refilled above
         copy(pr.up, XT[I]);
         copy(pr.down, X[O]);
         copy(pr.leaves, X[O]);
@@ -3899,7 +3924,7 @@ void make_dir_f32(nca_core *c, cudaStream_t s) {
         CK(cudaGetLastError());
     };
     for (DirProduct &pr : c->dir->prod)
-        for (GatherStage *G : {&pr.up, &pr.couple, &pr.down, &pr.leaves}) down(G->M, G->M32);
+        for (GatherStage *G : pr.own_stages()) down(G->M, G->M32);
     down(c->N, c->N32);
     down(c->NT, c->NT32);
 }
@@ -3909,7 +3934,7 @@ void drop_dir_dk(nca_core *c) {
     c->dN.release();
     c->dNT.release();
     for (DirProduct &pr : c->dir->prod)
-        for (GatherStage *G : {&pr.up, &pr.couple, &pr.down, &pr.leaves}) G->dM.release();
+        for (GatherStage *G : pr.own_stages()) G->dM.release();
     c->has_dk = false;
 }
 
