@@ -194,3 +194,45 @@ def test_directional_parity_at_65536_points():
     rows = np.arange(0, n, n // 256)
     ref = O.dense_rows(O.Kernel(O.KIND_HELMHOLTZ, k=k, rmin=1e-12), pts, pts, rows, x[:, 0])
     assert relerr((A @ x[:, 0])[rows], ref) < 10 * tol
+
+
+def _mirror_env(on):
+    import os
+    if on:
+        os.environ.pop("NCA_MIRROR_TRIAL", None)
+    else:
+        os.environ["NCA_MIRROR_TRIAL"] = "0"
+
+
+@pytest.mark.parametrize("store_f32", [False, True])
+def test_mirrored_galerkin_build_equals_two_compressions(store_f32):
+    """A Galerkin core (one point set, one tree, a kernel of |x - y|) takes the trial side's
+    skeleton from the test side and shares the transposed product's up, down and leaf stages; it
+    must equal the core whose trial side is compressed on its own: ranks and pivots of both sides
+    bit for bit, products in the three modes to rounding."""
+    import os
+    pts = sphere(6000, 41)
+    old = os.environ.get("NCA_MIRROR_TRIAL")
+    try:
+        _mirror_env(False)
+        B = build(pts, pts, 2 * np.pi * 3, 1e-4, 32, store_f32)
+        _mirror_env(True)
+        A = build(pts, pts, 2 * np.pi * 3, 1e-4, 32, store_f32)
+    finally:
+        if old is None:
+            os.environ.pop("NCA_MIRROR_TRIAL", None)
+        else:
+            os.environ["NCA_MIRROR_TRIAL"] = old
+    for side in (0, 1):
+        ra, pa = items(A, side)
+        rb, pb = items(B, side)
+        assert np.array_equal(ra, rb), side
+        assert all(np.array_equal(p, q) for p, q in zip(pa, pb)), side
+    ra0, pa0 = items(A, 0)
+    ra1, pa1 = items(A, 1)
+    assert np.array_equal(ra0, ra1) and all(np.array_equal(p, q) for p, q in zip(pa0, pa1))
+    x = cgauss((len(pts), 4), 5)
+    rel = 1e-5 if store_f32 else 1e-13
+    for op in (lambda M: M @ x, lambda M: M.T @ x, lambda M: M.H @ x):
+        ya, yb = op(A), op(B)
+        assert np.linalg.norm(ya - yb) <= rel * np.linalg.norm(yb)
