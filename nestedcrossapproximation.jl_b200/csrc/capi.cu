@@ -2215,7 +2215,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
     int64_t coupling_entries = 0;
     auto couplings = [&](cudaStream_t st) {
         npairs = int64_t(pt.farnodes.size());
-        const std::vector<int32_t> &rt = D->side[0].h_rank, &rs = D->side[1].h_rank;
+        const std::vector<int32_t> &rt = D->side[0].h_rank, &rs = D->side[mirror ? 0 : 1].h_rank;
         // coupling blocks S_e = K[tau_(t, dt), tau_(s, ds)] in test pair order, transposes in trial order
         cfoff.assign(npairs + 1, 0);
         ctoff.assign(ps.farnodes.size() + 1, 0);
@@ -2260,9 +2260,9 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             a.pair_t = D->cpair_it.p;
             a.pair_s = D->cpair_is.p;
             a.rank_t = D->side[0].rank.p;
-            a.rank_s = D->side[1].rank.p;
+            a.rank_s = D->side[mirror ? 0 : 1].rank.p;
             a.piv_t = D->side[0].piv.p;
-            a.piv_s = D->side[1].piv.p;
+            a.piv_s = D->side[mirror ? 0 : 1].piv.p;
             a.maxrank = maxrank;
             a.coff = D->ccoff.p;
             a.npairs = npairs;
@@ -2301,7 +2301,10 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         };
         const int m = task / 4, stage = task % 4;
         const int I = m == 0 ? 1 : 0, O = 1 - I;
-        const DirItems &di = D->side[I], &dout = D->side[O];
+        // the sides whose host arrays (ranks, offsets, items) the plan reads: a mirrored trial
+        // side's are the test side's, read from there as soon as the test side's ranks are known
+        const int hI = mirror ? 0 : I, hO = mirror ? 0 : O;
+        const DirItems &di = D->side[hI], &dout = D->side[hO];
         const nca::Tree &TI = c->tree[I], &TO = c->tree[O];
         DirProduct &pr = D->prod[m];
         if (pr.same && stage != 1) return;  // the forward product's stage serves this one
@@ -2310,17 +2313,17 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         const int64_t xin = TI.npoints;
         int64_t yo = 0;
         auto input_side_built = [&]() {
-            side_ranked[I].get();
+            side_ranked[hI].get();
             yo = xin + di.h_cptr.back();
         };
         // up: input-side items, deepest level first
         if (stage == 0) {
-            side_ranked[I].get();
+            side_ranked[hI].get();
             StageBuilder B;
             const size_t seg = size_t(di.nitems) + di.plan.item_chidx.size();
             B.reserve(size_t(di.nitems), seg, seg);
             for (int lev = TI.nlevels - 1; lev >= 0; --lev) {
-                for (int it : bylevel[I][lev]) {
+                for (int it : bylevel[hI][lev]) {
                     const int r = di.h_rank[it];
                     if (r <= 0) continue;
                     B.begin_output(r, xin + di.h_cptr[it]);
@@ -2342,7 +2345,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 B.end_group();
             }
             timer.mark("gather plan " + std::to_string(task) + ": up listed");
-            side_done[I].get();
+            side_done[hI].get();
             B.finish(pr.up, di.XT.p, s, m ? "T up" : "N up", plan_mark("up"));
             to_f32(pr.up.M, pr.up.M32, s);
             timer.mark("gather plan " + std::to_string(task) + ": up");
@@ -2352,7 +2355,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             if (m == 0) {
                 // every way out of this block settles `coupled`, which the transposed plan awaits
                 try {
-                    side_ranked[O].get();
+                    side_ranked[hO].get();
                     input_side_built();
                     pairs_f.get();
                     couplings(s);
@@ -2363,7 +2366,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 }
             } else {
                 coupled_done.get();
-                side_ranked[O].get();
+                side_ranked[hO].get();
                 input_side_built();
             }
             StageBuilder B;
@@ -2391,7 +2394,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
         if (stage == 2) {
             // listed with output rows relative to yo (the other side may still be compressing),
             // moved by yo once it is known
-            side_ranked[O].get();
+            side_ranked[hO].get();
             // parents of every child item (CSR in parent order), with the child's row offset in
             // the parent's X
             hvec<int32_t> pptr(size_t(dout.nitems) + 1, 0), ppar;
@@ -2419,7 +2422,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             StageBuilder B;
             B.reserve(size_t(dout.nitems), ppar.size(), ppar.size());
             for (int lev = 1; lev < TO.nlevels; ++lev) {
-                for (int it : bylevel[O][lev]) {
+                for (int it : bylevel[hO][lev]) {
                     const int r = dout.h_rank[it];
                     if (r <= 0 || pptr[it + 1] == pptr[it]) continue;
                     B.begin_output(r, yo + dout.h_cptr[it]);
@@ -2435,14 +2438,14 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             timer.mark("gather plan " + std::to_string(task) + ": down listed");
             input_side_built();
             B.shift(yo, true);
-            side_done[O].get();
+            side_done[hO].get();
             B.finish(pr.down, dout.X.p, s, m ? "T down" : "N down", plan_mark("down"));
             to_f32(pr.down.M, pr.down.M32, s);
             timer.mark("gather plan " + std::to_string(task) + ": down");
         }
         // leaves: every basis item whose cluster contains the leaf, then the near blocks
         if (stage == 3) {
-            side_ranked[O].get();
+            side_ranked[hO].get();
             near_f.get();
             StageBuilder B;
             const nca::DirSide &pl = dout.plan;
@@ -2470,7 +2473,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             timer.mark("gather plan " + std::to_string(task) + ": leaves listed");
             input_side_built();
             B.shift(yo, false);
-            side_done[O].get();
+            side_done[hO].get();
             B.finish(pr.leaves, dout.X.p, s, m ? "T leaves" : "N leaves", plan_mark("leaves"));
             to_f32(pr.leaves.M, pr.leaves.M32, s);
             timer.mark("gather plan " + std::to_string(task) + ": leaves");
