@@ -1396,13 +1396,17 @@ template void launch_gather_rows<float2, float2>(const RowArgs<float2> &, const 
 
 namespace {
 template <typename S>
+// One warp per block (the blocks are small: a CTA per block left most of its threads idle and
+// had one block's index loads in flight at a time)
 __global__ void k_copy_blocks(const S *src, const int64_t *soff, const int32_t *sld, const int32_t *rows,
                               const int32_t *cols, const int64_t *doff, int64_t nblocks, S *dst) {
-    for (int64_t blk = blockIdx.x; blk < nblocks; blk += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = int64_t(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t blk = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); blk < nblocks; blk += nw) {
         const int R = rows[blk], Cc = cols[blk], ld = sld[blk];
         const S *in = src + soff[blk];
         S *out = dst + doff[blk];
-        for (int e = threadIdx.x; e < R * Cc; e += blockDim.x) {
+        for (int e = lane; e < R * Cc; e += 32) {
             const int i = e % R, j = e / R;
             out[e] = in[i + int64_t(j) * ld];
         }
@@ -1417,7 +1421,8 @@ void launch_copy_blocks(const S *src, const int64_t *soff, const int32_t *sld, c
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = int(nblocks < int64_t(sms) * 16 ? nblocks : int64_t(sms) * 16);
+    const int64_t need = (nblocks + 7) / 8;  // eight warps (blocks) per CTA
+    const int grid = int(need < int64_t(sms) * 16 ? need : int64_t(sms) * 16);
     k_copy_blocks<S><<<grid, 256, 0, s>>>(src, soff, sld, rows, cols, doff, nblocks, dst);
 }
 
@@ -1426,13 +1431,16 @@ template void launch_copy_blocks<double2>(const double2 *, const int64_t *, cons
 
 namespace {
 template <typename S>
+// One warp per block, as k_copy_blocks
 __global__ void k_transpose_blocks(const S *in, const int64_t *inoff, const int32_t *rows, const int32_t *cols,
                                    const int64_t *outoff, int64_t nblocks, S *out) {
-    for (int64_t blk = blockIdx.x; blk < nblocks; blk += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = int64_t(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t blk = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); blk < nblocks; blk += nw) {
         const int R = rows[blk], Cc = cols[blk];
         const S *src = in + inoff[blk];
         S *dst = out + outoff[blk];
-        for (int e = threadIdx.x; e < R * Cc; e += blockDim.x) {
+        for (int e = lane; e < R * Cc; e += 32) {
             const int i = e % R, j = e / R;
             dst[j + int64_t(i) * Cc] = src[e];
         }
@@ -1447,7 +1455,8 @@ void launch_transpose_blocks(const S *in, const int64_t *inoff, const int32_t *r
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = int(nblocks < int64_t(sms) * 16 ? nblocks : int64_t(sms) * 16);
+    const int64_t need = (nblocks + 7) / 8;  // eight warps (blocks) per CTA
+    const int grid = int(need < int64_t(sms) * 16 ? need : int64_t(sms) * 16);
     k_transpose_blocks<S><<<grid, 256, 0, s>>>(in, inoff, rows, cols, outoff, nblocks, out);
 }
 template void launch_transpose_blocks<double2>(const double2 *, const int64_t *, const int32_t *, const int32_t *,
