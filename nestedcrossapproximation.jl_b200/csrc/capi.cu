@@ -521,12 +521,14 @@ struct DirProduct {
     // leaf stages are the forward product's (the same plans over the same stores); `same` points
     // at that product and this product's own three stay empty
     DirProduct *same = nullptr;
+    bool same_couple = false;  // ... and the coupling stage too (the transposed blocks are the blocks)
     GatherStage &up_stage() { return same ? same->up : up; }
+    GatherStage &couple_stage() { return same && same_couple ? same->couple : couple; }
     GatherStage &down_stage() { return same ? same->down : down; }
     GatherStage &leaf_stage() { return same ? same->leaves : leaves; }
     // the stages this product owns (the shared ones belong to `same`)
     std::vector<GatherStage *> own_stages() {
-        if (same) return {&couple};
+        if (same) return same_couple ? std::vector<GatherStage *>{} : std::vector<GatherStage *>{&couple};
         return {&up, &couple, &down, &leaves};
     }
 };
@@ -1560,11 +1562,34 @@ struct StageBuilder {
             if (e <= b) continue;
             int64_t wmax = 0;
             for (int32_t i = b; i < e; ++i) wmax = std::max(wmax, work[i]);
+            if (wmax > 8 * int64_t(e - b) + 4096) {
+                // few outputs of large work (the leaves): a comparison sort, same order
+                for (int32_t i = b; i < e; ++i) order[i] = i;
+                std::stable_sort(order.begin() + b, order.begin() + e,
+                                 [&](int32_t x, int32_t y) { return work[x] > work[y]; });
+                continue;
+            }
             cnt.assign(size_t(wmax) + 2, 0);
             for (int32_t i = b; i < e; ++i) ++cnt[size_t(wmax - work[i]) + 1];
             for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
             for (int32_t i = b; i < e; ++i) order[size_t(b + cnt[size_t(wmax - work[i])]++)] = i;
         }
+        // fn(k, i0, i1) over nparts consecutive ranges of [b, e), on threads of their own when
+        // the range is long
+        auto in_parts = [](int32_t b, int32_t e, int nparts, auto fn) {
+            if (nparts <= 1) {
+                fn(0, b, e);
+                return;
+            }
+            std::vector<std::thread> pool;
+            for (int k = 1; k < nparts; ++k)
+                pool.emplace_back([&, k] {
+                    fn(k, int32_t(b + int64_t(e - b) * k / nparts), int32_t(b + int64_t(e - b) * (k + 1) / nparts));
+                });
+            fn(0, b, int32_t(b + int64_t(e - b) / nparts));
+            for (auto &th : pool) th.join();
+        };
+        auto parts_of = [](int32_t n) { return std::max(1, std::min(8, int(n / 65536))); };
         // Records of the all-column FP32 kernel (groups of small outputs): inside a group the
         // records of one row class (the kernel's register tile) are contiguous, largest work
         // first inside a class: one launch per class
@@ -1585,25 +1610,38 @@ struct StageBuilder {
         for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
             const int32_t b = group_ptr[g], e = group_ptr[g + 1];
             if (e > b && wide_group(group_maxrows[g], group_work[g])) {
-                int32_t ccount[34] = {0}, start[34];
-                for (int32_t i = b; i < e; ++i) ++ccount[wide_rows_class(rows[order[i]])];
+                // each part counts its classes; a part's records of a class follow those of the
+                // parts before it, so the records are those of one pass in order
+                const int np = parts_of(e - b);
+                std::vector<int32_t> pc(size_t(np) * 34, 0);  // [part][class]
+                in_parts(b, e, np, [&](int k, int32_t i0, int32_t i1) {
+                    int32_t *cc = pc.data() + size_t(k) * 34;
+                    for (int32_t i = i0; i < i1; ++i) ++cc[wide_rows_class(rows[order[i]])];
+                });
                 int32_t at = int32_t(rec.size());
                 for (int c = 0; c < 34; ++c) {
-                    start[c] = at;
-                    if (ccount[c]) {
+                    int32_t n = 0;
+                    for (int k = 0; k < np; ++k) {
+                        const int32_t q = pc[size_t(k) * 34 + c];
+                        pc[size_t(k) * 34 + c] = at + n;  // the part's first slot of the class
+                        n += q;
+                    }
+                    if (n) {
                         G.wide_begin.push_back(at);
-                        G.wide_count.push_back(ccount[c]);
+                        G.wide_count.push_back(n);
                         G.wide_nr.push_back(c);
                     }
-                    at += ccount[c];
+                    at += n;
                 }
                 rec.resize(size_t(at));
-                for (int32_t i = b; i < e; ++i) {
-                    const int32_t o = order[i];
-                    const int32_t W = width(o);
-                    rec[size_t(start[wide_rows_class(rows[o])]++)] =
-                        WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], rows[o], 0};
-                }
+                in_parts(b, e, np, [&](int k, int32_t i0, int32_t i1) {
+                    int32_t *slot = pc.data() + size_t(k) * 34;
+                    for (int32_t i = i0; i < i1; ++i) {
+                        const int32_t o = order[i];
+                        rec[size_t(slot[wide_rows_class(rows[o])]++)] =
+                            WideOut{rows[o], width(o), segptr[o], segptr[o + 1], out[o], rows[o], 0};
+                    }
+                });
             }
             G.wide_gptr.push_back(int32_t(G.wide_begin.size()));
         }
@@ -1612,19 +1650,20 @@ struct StageBuilder {
         G.group_work = group_work;
         // records of the tensor-core gathers: the groups the all-column FP32 kernel does not take
         // (left zero elsewhere)
-        hvec<WideOut> trec(order.size());
-        for (size_t g = 0; g + 1 < group_ptr.size(); ++g) {
-            if (wide_group(group_maxrows[g], group_work[g])) continue;
-            for (int32_t i = group_ptr[g]; i < group_ptr[g + 1]; ++i) {
-                const int32_t o = order[i];
-                const int32_t W = width(o);
-                trec[i] = WideOut{rows[o], W, segptr[o], segptr[o + 1], out[o], rows[o], 0};
-            }
-        }
-        // records of the tensor-core gathers only if some group takes them
+        // (only if some group takes them)
         bool any_tc = false;
         for (size_t g = 0; g + 1 < group_ptr.size(); ++g) any_tc = any_tc || !wide_group(group_maxrows[g], group_work[g]);
-        if (!any_tc) trec.clear();
+        hvec<WideOut> trec(any_tc ? order.size() : 0);
+        for (size_t g = 0; any_tc && g + 1 < group_ptr.size(); ++g) {
+            if (wide_group(group_maxrows[g], group_work[g])) continue;
+            const int32_t b = group_ptr[g], e = group_ptr[g + 1];
+            in_parts(b, e, parts_of(e - b), [&](int, int32_t i0, int32_t i1) {
+                for (int32_t i = i0; i < i1; ++i) {
+                    const int32_t o = order[i];
+                    trec[i] = WideOut{rows[o], width(o), segptr[o], segptr[o + 1], out[o], rows[o], 0};
+                }
+            });
+        }
         if (mark)
             mark("records (" + std::to_string(rows.size()) + " outputs, " + std::to_string(w.size()) + " segments, " +
                  std::to_string(crows.size()) + " copies)");
@@ -2262,9 +2301,19 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
             tr_cols[q] = rs[pair_is[e]];
             ctoff[q + 1] = ctoff[q] + pad2(int64_t(tr_rows[q]) * tr_cols[q]);
         }
+        // a mirrored core whose transposed block at every trial position is the forward block at
+        // the same test position (the partners swap places and the offsets agree) shares the
+        // forward coupling stage: the blocks are equal entry for entry (one point set, K(x, y) =
+        // K(y, x) bit for bit, the same pivots on both sides)
+        bool share = mirror && ctoff == cfoff;
+        for (size_t q = 0; share && q < ps.farnodes.size(); ++q) {
+            const int e = pair_of_pos[q];
+            share = pair_is[e] == pair_it[q] && pair_it[e] == pair_is[q];
+        }
+        D->prod[1].same_couple = share;
         GatherStage &CN = D->prod[0].couple, &CTs = D->prod[1].couple;
         CN.M.alloc(size_t(cfoff.back()));
-        CTs.M.alloc(size_t(ctoff.back()));
+        if (!share) CTs.M.alloc(size_t(ctoff.back()));
         CN.entries = CTs.entries = coupling_entries;
         {
             // staged through page-locked memory on the coupling plan's stream (not behind the test
@@ -2303,12 +2352,12 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 k_couplings<<<launch_grid(npairs, 16), 256, 0, st>>>(a);
                 CK(cudaGetLastError());
             }
-            D->ntr = int64_t(ps.farnodes.size());
+            D->ntr = share ? 0 : int64_t(ps.farnodes.size());  // no transposes when the stage is shared
             launch_transpose_blocks<double2>(CN.M.p, D->ctr_in.p, D->ctr_rows.p, D->ctr_cols.p, D->ctr_off.p, D->ntr,
                                              CTs.M.p, st);
             CK(cudaGetLastError());
             to_f32(CN.M, CN.M32, st);
-            to_f32(CTs.M, CTs.M32, st);
+            if (!share) to_f32(CTs.M, CTs.M32, st);
         }
     };
     std::promise<void> coupled;
@@ -2387,7 +2436,9 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                     side_ranked[hO].get();
                     input_side_built();
                     pairs_f.get();
+                    timer.mark("gather plan " + std::to_string(task) + ": couplings started");
                     couplings(s);
+                    timer.mark("gather plan " + std::to_string(task) + ": couplings enqueued");
                     coupled.set_value();
                 } catch (...) {
                     coupled.set_exception(std::current_exception());
@@ -2395,6 +2446,7 @@ void build_dir_core(nca_core *c, const double *tp, const double *sp, const nca_b
                 }
             } else {
                 coupled_done.get();
+                if (pr.same_couple) return;  // the forward coupling stage serves this product
                 side_ranked[hO].get();
                 input_side_built();
             }
@@ -2995,7 +3047,7 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
     const int I = mode == 0 ? 1 : 0, O = 1 - I;
     const int vs = vector_stride(b);
     const int cap = rows_capacity(std::min(b, 16));
-    for (const GatherStage *G : {&pr.up_stage(), &pr.couple, &pr.down_stage(), &pr.leaf_stage()})
+    for (const GatherStage *G : {&pr.up_stage(), &pr.couple_stage(), &pr.down_stage(), &pr.leaf_stage()})
         for (int r : G->group_maxrows)
             if (r > cap) return fail(NCA_ERR_ARG, "a leaf or basis block has more rows than one product CTA holds");
     // Complex-FP32 products keep the arena [x; coefficients] in complex FP32 too: the stages
@@ -3099,7 +3151,7 @@ int enqueue_dir_product(nca_core *c, int mode, int precision, const double2 *xd,
             if (timer) timer->mark(sk, true, s);
         };
         stage(pr.up_stage(), false, false, 1);
-        stage(pr.couple, false, false, 2);
+        stage(pr.couple_stage(), false, false, 2);
         stage(pr.down_stage(), true, false, 3);
         stage(pr.leaf_stage(), false, true, 5);
     };
