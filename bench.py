@@ -55,7 +55,7 @@ def parse():
     p.add_argument("--nrhs", type=int, default=16)
     p.add_argument("--wideband-points", type=int, default=0, help="point count of the wideband workload")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--builds", type=int, default=5,
+    p.add_argument("--builds", type=int, default=7,
                    help="timed builds of each wideband form; the median is reported")
     p.add_argument("--profile-stages", action="store_true", help="print per-stage times to stderr")
     p.add_argument("--profile-run", action="store_true",
