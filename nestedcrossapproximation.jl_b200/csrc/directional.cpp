@@ -93,11 +93,15 @@ double genradius(const Tree &T, int node) {
 // Candidate directions of a cluster of diameter diam: n = max(6, ceil(6 * 4^log2(
 // acos(1/sqrt 3) / asin(min(1, gamma / (k diam)))))) spherical Fibonacci points
 // (boundingballdirections.jl:12-29).
-void candidate_directions(double diam, double k, double gamma, std::vector<double> &out) {
+int64_t candidate_count(double diam, double k, double gamma) {
     const double kd = std::max(k * diam, 0x1p-52);
     const double ratio = std::acos(1.0 / std::sqrt(3.0)) / std::asin(std::min(1.0, gamma / kd));
-    int64_t n = int64_t(std::ceil(6.0 * std::pow(4.0, std::log(ratio) / std::log(2.0))));
-    n = std::max<int64_t>(6, n);
+    const int64_t n = int64_t(std::ceil(6.0 * std::pow(4.0, std::log(ratio) / std::log(2.0))));
+    return std::max<int64_t>(6, n);
+}
+
+// the n spherical Fibonacci points (a function of n alone)
+void fibonacci_points(int64_t n, std::vector<double> &out) {
     out.resize(3 * size_t(n));
     const double ga = M_PI * (3.0 - std::sqrt(5.0));
     for (int64_t i = 0; i < n; ++i) {
@@ -107,6 +111,10 @@ void candidate_directions(double diam, double k, double gamma, std::vector<doubl
         out[3 * i + 1] = r * std::sin(double(i) * ga);
         out[3 * i + 2] = z;
     }
+}
+
+void candidate_directions(double diam, double k, double gamma, std::vector<double> &out) {
+    fibonacci_points(candidate_count(diam, k, gamma), out);
 }
 
 // 0-based index of the direction with the largest dot product (first on ties), one candidate
@@ -311,8 +319,13 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
                 return;
             }
             if (!hasfars && !hasparentvecs) return;
-            candidate_directions(2.0 * T.radius[node], w.k, w.gamma, total);
-            cand.set(total);
+            // the candidates depend on their count alone: a thread keeps its last set, which the
+            // next nodes of the level (of about the same size) mostly share
+            const int64_t ncand = candidate_count(2.0 * T.radius[node], w.k, w.gamma);
+            if (int64_t(total.size()) != 3 * ncand) {
+                fibonacci_points(ncand, total);
+                cand.set(total);
+            }
             const int b = farptr[node], nfar = farptr[node + 1] - b;
             std::vector<int32_t> nd(nfar);
             const double *c = &T.center[3 * size_t(node)];
@@ -408,72 +421,103 @@ DirSide directional_plan(const Tree &T, const Tree &F, const std::vector<int32_t
         D.chdirptr[node + 1] = D.chdirptr[node] + pcount[node];
     }
     const int ni = D.dirptr[nn];
+    // The rest fills disjoint ranges per node or per item, on the host threads: fn(b, e) over
+    // consecutive ranges of [0, n)
+    auto in_ranges = [nth](int n, auto fn) {
+        const int use = std::max(1, std::min(nth, n / 4096));
+        std::vector<std::thread> pool;
+        for (int k = 1; k < use; ++k)
+            pool.emplace_back([&, k] { fn(int(int64_t(n) * k / use), int(int64_t(n) * (k + 1) / use)); });
+        fn(0, int(int64_t(n) / use));
+        for (auto &th : pool) th.join();
+    };
     D.dirs.resize(ni);
     D.dirvec.assign(3 * size_t(ni), 0.0);
     D.dirfarptr.resize(ni + 1);
     D.chdirmap.resize(D.chdirptr[nn]);
     D.item_node.resize(ni);
-    for (int node = 0; node < nn; ++node) {
-        int32_t off = farptr[node];
-        for (size_t u = 0; u < dirs[node].size(); ++u) {
-            const int item = D.dirptr[node] + int(u);
-            D.dirs[item] = dirs[node][u];
-            D.item_node[item] = node;
-            if (hasvec[node])
-                for (int d = 0; d < 3; ++d) D.dirvec[3 * size_t(item) + d] = dirvec[node][3 * u + d];
-            D.dirfarptr[item] = off;
-            off += dircount[node][u];
+    in_ranges(nn, [&](int n0, int n1) {
+        for (int node = n0; node < n1; ++node) {
+            int32_t off = farptr[node];
+            for (size_t u = 0; u < dirs[node].size(); ++u) {
+                const int item = D.dirptr[node] + int(u);
+                D.dirs[item] = dirs[node][u];
+                D.item_node[item] = node;
+                if (hasvec[node])
+                    for (int d = 0; d < 3; ++d) D.dirvec[3 * size_t(item) + d] = dirvec[node][3 * u + d];
+                D.dirfarptr[item] = off;
+                off += dircount[node][u];
+            }
+            std::copy(pmap[node].begin(), pmap[node].end(), D.chdirmap.begin() + D.chdirptr[node]);
         }
-        std::copy(pmap[node].begin(), pmap[node].end(), D.chdirmap.begin() + D.chdirptr[node]);
-    }
+    });
     D.dirfarptr[ni] = farptr[nn];
     // the inverse of the parent-to-child maps: for every item the parent directions mapped onto it
+    // (a node's map points at the node's own items only)
     D.invptr.assign(ni + 1, 0);
-    for (int node = 0; node < nn; ++node) {
-        const int nown = D.dirptr[node + 1] - D.dirptr[node];
-        for (int i = D.chdirptr[node]; i < D.chdirptr[node + 1]; ++i)
-            if (D.chdirmap[i] >= 1 && D.chdirmap[i] <= nown) ++D.invptr[D.dirptr[node] + D.chdirmap[i]];
-    }
+    in_ranges(nn, [&](int n0, int n1) {
+        for (int node = n0; node < n1; ++node) {
+            const int nown = D.dirptr[node + 1] - D.dirptr[node];
+            for (int i = D.chdirptr[node]; i < D.chdirptr[node + 1]; ++i)
+                if (D.chdirmap[i] >= 1 && D.chdirmap[i] <= nown) ++D.invptr[D.dirptr[node] + D.chdirmap[i]];
+        }
+    });
     for (int item = 0; item < ni; ++item) D.invptr[item + 1] += D.invptr[item];
     D.invidx.resize(D.invptr[ni]);
     {
         std::vector<int32_t> fill(D.invptr.begin(), D.invptr.end() - 1);
-        for (int node = 0; node < nn; ++node) {
-            const int nown = D.dirptr[node + 1] - D.dirptr[node];
-            for (int i = D.chdirptr[node]; i < D.chdirptr[node + 1]; ++i)
-                if (D.chdirmap[i] >= 1 && D.chdirmap[i] <= nown)
-                    D.invidx[fill[D.dirptr[node] + D.chdirmap[i] - 1]++] = i - D.chdirptr[node] + 1;
-        }
+        in_ranges(nn, [&](int n0, int n1) {
+            for (int node = n0; node < n1; ++node) {
+                const int nown = D.dirptr[node + 1] - D.dirptr[node];
+                for (int i = D.chdirptr[node]; i < D.chdirptr[node + 1]; ++i)
+                    if (D.chdirmap[i] >= 1 && D.chdirmap[i] <= nown)
+                        D.invidx[fill[D.dirptr[node] + D.chdirmap[i] - 1]++] = i - D.chdirptr[node] + 1;
+            }
+        });
     }
-    // basis items and the children's items of nested ones
+    // basis items and the children's items of nested ones: the basis flags and child counts per
+    // item, their prefix, then the children's items
     D.item_basis.resize(ni);
     D.item_chptr.assign(ni + 1, 0);
-    D.item_chidx.clear();
-    for (int item = 0; item < ni; ++item) {
-        const int node = D.item_node[item];
-        bool basis;
-        if (T.isleaf(node)) {
-            basis = true;
-        } else if (D.dirs[item] == 0) {
-            basis = false;
-        } else {
-            const int fc = T.firstchild[node];
-            basis = D.dirptr[fc + 1] == D.dirptr[fc] ||
-                    (D.dirptr[fc + 1] - D.dirptr[fc] == 1 && D.dirs[D.dirptr[fc]] == 0);
+    in_ranges(ni, [&](int i0, int i1) {
+        for (int item = i0; item < i1; ++item) {
+            const int node = D.item_node[item];
+            bool basis;
+            if (T.isleaf(node)) {
+                basis = true;
+            } else if (D.dirs[item] == 0) {
+                basis = false;
+            } else {
+                const int fc = T.firstchild[node];
+                basis = D.dirptr[fc + 1] == D.dirptr[fc] ||
+                        (D.dirptr[fc + 1] - D.dirptr[fc] == 1 && D.dirs[D.dirptr[fc]] == 0);
+            }
+            D.item_basis[item] = basis;
+            D.item_chptr[item + 1] = basis ? 0 : T.nchildren[node];
         }
-        D.item_basis[item] = basis;
-        if (!basis) {
+    });
+    for (int item = 0; item < ni; ++item) D.item_chptr[item + 1] += D.item_chptr[item];
+    D.item_chidx.assign(size_t(D.item_chptr[ni]), 0);
+    std::atomic<bool> missing{false};
+    in_ranges(ni, [&](int i0, int i1) {
+        for (int item = i0; item < i1; ++item) {
+            if (D.item_basis[item]) continue;
+            const int node = D.item_node[item];
             const int local = item - D.dirptr[node];  // 0-based local direction of the parent
+            int32_t at = D.item_chptr[item];
             for (int c = 0; c < T.nchildren[node]; ++c) {
                 const int ch = T.firstchild[node] + c;
                 const int cnt = D.chdirptr[ch + 1] - D.chdirptr[ch];
                 const int m = local < cnt ? D.chdirmap[D.chdirptr[ch] + local] : 0;  // 1-based local direction
-                if (m <= 0) throw std::runtime_error("directional plan: a child has no direction for its parent's");
-                D.item_chidx.push_back(D.dirptr[ch] + m - 1);
+                if (m <= 0) {
+                    missing = true;
+                    return;
+                }
+                D.item_chidx[at++] = D.dirptr[ch] + m - 1;
             }
         }
-        D.item_chptr[item + 1] = int32_t(D.item_chidx.size());
-    }
+    });
+    if (missing) throw std::runtime_error("directional plan: a child has no direction for its parent's");
     return D;
 }
 
