@@ -73,12 +73,16 @@ struct TeamBarrier {
 struct Splitter {
     const double *pts;
     std::vector<int32_t> side, scratch;
+    std::vector<double> px, py, pz;  // the cluster's points, gathered once per split (same values)
 
     // Reorders ids[0:cnt) into two stable groups; returns the size of the first one. nteam > 1
     // spreads the chunks of one cluster over that many threads.
     int split(int32_t *ids, int cnt, int nteam = 1) {
         side.assign(cnt, -1);
         scratch.resize(cnt);
+        px.resize(cnt);
+        py.resize(cnt);
+        pz.resize(cnt);
         const int nch = (cnt + kChunk - 1) / kChunk;
         nteam = std::max(1, std::min(nteam, nch));
         // per chunk: partial sums of both groups, their counts, the farthest point, changes
@@ -103,7 +107,8 @@ struct Splitter {
                 int arg = i0;
                 double best = -1.0;
                 for (int i = i0; i < i1; ++i) {
-                    const double d = dist2(pts + 3 * int64_t(ids[i]), from);
+                    const double p[3] = {px[i], py[i], pz[i]};
+                    const double d = dist2(p, from);
                     if (d > best) {
                         best = d;
                         arg = i;
@@ -131,6 +136,9 @@ struct Splitter {
                 double t[3] = {0.0, 0.0, 0.0};
                 for (int i = i0; i < i1; ++i) {
                     const double *p = pts + 3 * int64_t(ids[i]);
+                    px[i] = p[0];
+                    py[i] = p[1];
+                    pz[i] = p[2];
                     t[0] += p[0];
                     t[1] += p[1];
                     t[2] += p[2];
@@ -173,7 +181,7 @@ struct Splitter {
                     double t[2][3] = {{0, 0, 0}, {0, 0, 0}};
                     int m[2] = {0, 0};
                     for (int i = i0; i < i1; ++i) {
-                        const double *p = pts + 3 * int64_t(ids[i]);
+                        const double p[3] = {px[i], py[i], pz[i]};
                         const int32_t sd = dist2(p, c[1]) < dist2(p, c[0]) ? 1 : 0;
                         if (sd != side[i]) {
                             side[i] = sd;
