@@ -25,10 +25,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <condition_variable>
-#include <mutex>
 #include <thread>
 
+#include <immintrin.h>
 #include <sched.h>
 
 #include "nca_internal.h"
@@ -50,22 +49,26 @@ constexpr int kLloydIterations = 50;
 constexpr int kChunk = 256;
 constexpr int kTeamPoints = 16384;
 
-// reusable barrier of a fixed team of threads
+// reusable barrier of a fixed team of threads: arrivals counted atomically, the last one opens
+// the next generation; waiters spin briefly (a Lloyd step of a team is tens of microseconds, and a
+// sleeping wait through a condition variable cost about as much as the step), then yield
 struct TeamBarrier {
-    std::mutex mu;
-    std::condition_variable cv;
-    int n, waiting = 0;
-    unsigned gen = 0;
+    std::atomic<int> waiting{0};
+    std::atomic<unsigned> gen{0};
+    const int n;
     explicit TeamBarrier(int count) : n(count) {}
     void wait() {
-        std::unique_lock<std::mutex> lk(mu);
-        const unsigned g = gen;
-        if (++waiting == n) {
-            waiting = 0;
-            ++gen;
-            cv.notify_all();
-        } else {
-            cv.wait(lk, [&] { return gen != g; });
+        const unsigned g = gen.load(std::memory_order_acquire);
+        if (waiting.fetch_add(1, std::memory_order_acq_rel) + 1 == n) {
+            waiting.store(0, std::memory_order_relaxed);
+            gen.store(g + 1, std::memory_order_release);
+            return;
+        }
+        for (int spin = 0; gen.load(std::memory_order_acquire) == g; ++spin) {
+            if (spin < 4096)
+                _mm_pause();
+            else
+                std::this_thread::yield();
         }
     }
 };
