@@ -1,5 +1,5 @@
-// Randomised check of the banded, four-wide nearest-direction search against the full
-// one-at-a-time search (and of the four-wide search over all candidates against it): the
+// Randomised check of the banded, vectorised nearest-direction search against the full
+// one-at-a-time search (and of the four- and eight-wide scans over all candidates against it): the
 // candidate sets of candidate_directions for cluster diameters 0.01-3 and wavenumbers 1-120
 // (6 to ~680,000 spherical Fibonacci points), queried with Gaussian directions of magnitudes
 // 1e-30 to 1e30, many of them near the poles or on the equator. Both searches must return the
@@ -18,6 +18,7 @@ int main(int argc, char **argv) {
     long bad = 0, total = 0;
     std::vector<double> dirs;
     nca::Candidates cand;
+    const bool wide = __builtin_cpu_supports("avx512f");
     for (double diam = 0.01; diam < 3.0; diam *= 1.07) {
         for (double k : {1.0, 10.0, 50.0, 120.0}) {
             nca::candidate_directions(diam, k, 1.0, dirs);
@@ -34,7 +35,10 @@ int main(int argc, char **argv) {
                 ++total;
                 const int full = nca::nearest_direction(dirs, v);
                 if (nca::nearest_candidate(cand, v) != full) ++bad;
-                if (t % 3 == 0 && int(nca::argmax_dot(cand, 0, cand.n - 1, v)) != full) ++bad;
+                if (t % 3 == 0) {  // the four- and (where the host has it) eight-wide scans over all
+                    if (int(nca::argmax_dot4(cand, 0, cand.n - 1, v)) != full) ++bad;
+                    if (wide && int(nca::argmax_dot8(cand, 0, cand.n - 1, v)) != full) ++bad;
+                }
             }
         }
     }
